@@ -1,0 +1,1217 @@
+// CPU oracle for the HyTeG P1 matrix-free geometric-multigrid path.
+//
+// TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's CPU
+// baseline / reference arm load this library as the checker or the timed CPU
+// baseline. The product path never links, loads or calls it.
+//
+// Design: one value per unique micro-vertex (global DoF vector in the canonical
+// order documented in hyteg_oracle.h). Macro-cell closure points are mapped to
+// DoFs through exact integer barycentric keys, so no face/edge permutation
+// table is involved. Operators are evaluated row by row as the sum, over the
+// macro-cells containing the DoF, of that cell's partial row -- exactly how the
+// reference assembles its macro-face/edge/vertex stencils
+// (src/hyteg/p1functionspace/P1Elements.hpp:464-526 calculateStencilInMacroCellForm_new,
+//  P1Operator.hpp:1045-1175 apply_edge / apply_face3D).
+#include "hyteg_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <vector>
+
+namespace {
+
+using i64 = int64_t;
+
+// ---------------------------------------------------------------------------
+// Index space (src/hyteg/Levelinfo.hpp:35-105, indexing/MacroCellIndexing.hpp:37-54)
+// ---------------------------------------------------------------------------
+inline i64 tetSize( i64 w ) { return ( w + 2 ) * ( w + 1 ) * w / 6; }
+// linearMacroCellIndex( width, x, y, z )
+inline i64 cellIdx( i64 width, i64 x, i64 y, i64 z )
+{
+   const i64 wms = width - z;
+   return tetSize( width ) - tetSize( wms ) + y * ( wms + 1 ) - ( ( y + 1 ) * y ) / 2 + x;
+}
+
+// The 15 stencil offsets in the repository-wide order.
+const int kOff[15][3] = { { 0, 0, 0 },  { 1, 0, 0 },  { -1, 0, 0 }, { 0, 1, 0 },  { 0, -1, 0 },
+                          { 0, 0, 1 },  { 0, 0, -1 }, { -1, 1, 0 }, { 1, -1, 0 }, { -1, 0, 1 },
+                          { 1, 0, -1 }, { 0, -1, 1 }, { 0, 1, -1 }, { -1, 1, -1 }, { 1, -1, 1 } };
+
+int offsetId( int x, int y, int z )
+{
+   for ( int o = 0; o < 15; ++o )
+      if ( kOff[o][0] == x && kOff[o][1] == y && kOff[o][2] == z )
+         return o;
+   return -1;
+}
+
+// Micro-cell types and their micro-vertices
+// (src/hyteg/volumedofspace/CellDoFIndexing.hpp:38-46, 155-198).
+const int kMicro[6][4][3] = {
+    { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, // WHITE_UP
+    { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } }, // BLUE_UP
+    { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, // GREEN_UP
+    { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } }, // WHITE_DOWN
+    { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, // BLUE_DOWN
+    { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } }, // GREEN_DOWN
+};
+// Micro-cells per row of each type: WHITE_UP N, WHITE_DOWN N-2, others N-1
+// (CellDoFIndexing.hpp numCellsPerRowByType).
+inline i64 microWidth( int type, i64 N ) { return type == 0 ? N : ( type == 3 ? N - 2 : N - 1 ); }
+
+// The 24 micro-tets incident to a micro-vertex: (type, role k) -> vertex offsets
+// relative to the vertex (vertex j of the tet at offset kMicro[t][j]-kMicro[t][k]).
+struct Incident
+{
+   int t, k;
+   int rel[4][3];
+};
+std::vector< Incident > makeIncident()
+{
+   std::vector< Incident > v;
+   for ( int t = 0; t < 6; ++t )
+      for ( int k = 0; k < 4; ++k )
+      {
+         Incident in{ t, k, {} };
+         for ( int j = 0; j < 4; ++j )
+            for ( int d = 0; d < 3; ++d )
+               in.rel[j][d] = kMicro[t][j][d] - kMicro[t][k][d];
+         v.push_back( in );
+      }
+   return v;
+}
+const std::vector< Incident > kIncident = makeIncident();
+
+// Barycentric micro-coordinate change of an offset: db0 = -(x+y+z), db1 = x, db2 = y, db3 = z.
+// A point has "class mask" bit k set iff its barycentric coordinate b_k is zero; a micro-tet
+// incident to it lies in the closure iff db_k >= 0 for all its vertices and all k in the mask.
+inline int pointMask( i64 N, i64 x, i64 y, i64 z )
+{
+   int m = 0;
+   if ( N - x - y - z == 0 ) m |= 1;
+   if ( x == 0 ) m |= 2;
+   if ( y == 0 ) m |= 4;
+   if ( z == 0 ) m |= 8;
+   return m;
+}
+inline bool relAllowed( int mask, const int* r )
+{
+   if ( ( mask & 1 ) && -( r[0] + r[1] + r[2] ) < 0 ) return false;
+   if ( ( mask & 2 ) && r[0] < 0 ) return false;
+   if ( ( mask & 4 ) && r[1] < 0 ) return false;
+   if ( ( mask & 8 ) && r[2] < 0 ) return false;
+   return true;
+}
+inline bool inClosure( i64 N, i64 x, i64 y, i64 z ) { return x >= 0 && y >= 0 && z >= 0 && x + y + z <= N; }
+
+// P1 element stiffness  K_ij = |T| grad(phi_i).grad(phi_j)  for a tetrahedron.
+// (What src/hyteg/forms/form_fenics_generated/p1_tet_diffusion.h tabulate_tensor computes.)
+void p1Stiffness( const std::array< std::array< double, 3 >, 4 >& X, double K[4][4], double* absDetOut = nullptr )
+{
+   double J[3][3];
+   for ( int r = 0; r < 3; ++r )
+      for ( int c = 0; c < 3; ++c )
+         J[r][c] = X[c + 1][r] - X[0][r]; // columns = edge vectors
+   const double det = J[0][0] * ( J[1][1] * J[2][2] - J[1][2] * J[2][1] ) -
+                      J[0][1] * ( J[1][0] * J[2][2] - J[1][2] * J[2][0] ) +
+                      J[0][2] * ( J[1][0] * J[2][1] - J[1][1] * J[2][0] );
+   // inverse transpose rows = gradients of barycentric coords 1..3
+   double inv[3][3];
+   inv[0][0] = ( J[1][1] * J[2][2] - J[1][2] * J[2][1] ) / det;
+   inv[0][1] = ( J[0][2] * J[2][1] - J[0][1] * J[2][2] ) / det;
+   inv[0][2] = ( J[0][1] * J[1][2] - J[0][2] * J[1][1] ) / det;
+   inv[1][0] = ( J[1][2] * J[2][0] - J[1][0] * J[2][2] ) / det;
+   inv[1][1] = ( J[0][0] * J[2][2] - J[0][2] * J[2][0] ) / det;
+   inv[1][2] = ( J[0][2] * J[1][0] - J[0][0] * J[1][2] ) / det;
+   inv[2][0] = ( J[1][0] * J[2][1] - J[1][1] * J[2][0] ) / det;
+   inv[2][1] = ( J[0][1] * J[2][0] - J[0][0] * J[2][1] ) / det;
+   inv[2][2] = ( J[0][0] * J[1][1] - J[0][1] * J[1][0] ) / det;
+   double g[4][3];
+   for ( int i = 0; i < 3; ++i )
+      for ( int d = 0; d < 3; ++d )
+         g[i + 1][d] = inv[i][d]; // row i of J^-1 is grad(lambda_{i+1})
+   for ( int d = 0; d < 3; ++d )
+      g[0][d] = -g[1][d] - g[2][d] - g[3][d];
+   const double vol = std::fabs( det ) / 6.0;
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j )
+         K[i][j] = vol * ( g[i][0] * g[j][0] + g[i][1] * g[j][1] + g[i][2] * g[j][2] );
+   if ( absDetOut )
+      *absDetOut = std::fabs( det );
+}
+
+// ---------------------------------------------------------------------------
+// Topology
+// ---------------------------------------------------------------------------
+struct Level
+{
+   int                                 L;
+   i64                                 N, S, nDof;
+   i64                                 offE, offF, offC, nIntFace, nIntCell;
+   std::vector< std::vector< int32_t > > cellMap; // [cell][closure idx] -> DoF
+   std::vector< uint8_t >              kind, bc;
+   std::vector< int32_t >              owner;
+   // entries for non-cell-interior DoFs [0, offC): (cell, x, y, z)
+   std::vector< i64 >                  entOff;
+   std::vector< std::array< int32_t, 4 > > ent;
+};
+
+struct Op
+{
+   bool variable = false;
+   // constant: stencil[level][cell][mask][15]
+   std::vector< std::vector< std::array< std::array< double, 15 >, 16 > > > st;
+   // variable: nodal k per level, element matrices K[level][cell][type][4][4]
+   std::vector< std::vector< double > > k;
+   std::vector< std::vector< std::array< std::array< std::array< double, 4 >, 4 >, 6 > > > K;
+};
+
+struct Oracle
+{
+   std::vector< std::array< double, 3 > > V;
+   std::vector< std::array< int, 4 > >    T;
+   std::vector< std::array< int, 2 > >    E;
+   std::vector< std::array< int, 3 > >    F;
+   std::map< std::array< int, 2 >, int >  eId;
+   std::map< std::array< int, 3 >, int >  fId;
+   std::vector< uint8_t >                 vBc, eBc, fBc;
+   std::vector< std::vector< int > >      fEdges, fVerts, eVerts; // closures
+   int                                    maxLevel;
+   std::vector< Level >                   lv;
+   std::vector< Op >                      ops;
+};
+
+void buildTopology( Oracle& o )
+{
+   // edges/faces from cells (MeshInfo::addEdge/addFace keep sorted keys; mesh/MeshInfo.cpp:37-72)
+   std::set< std::array< int, 2 > > es;
+   std::set< std::array< int, 3 > > fs;
+   for ( auto& t : o.T )
+   {
+      for ( int a = 0; a < 4; ++a )
+         for ( int b = a + 1; b < 4; ++b )
+            es.insert( { std::min( t[a], t[b] ), std::max( t[a], t[b] ) } );
+      const int fl[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+      for ( auto& f : fl )
+      {
+         std::array< int, 3 > k = { t[f[0]], t[f[1]], t[f[2]] };
+         std::sort( k.begin(), k.end() );
+         fs.insert( k );
+      }
+   }
+   for ( auto& e : es )
+   {
+      o.eId[e] = int( o.E.size() );
+      o.E.push_back( e );
+   }
+   for ( auto& f : fs )
+   {
+      o.fId[f] = int( o.F.size() );
+      o.F.push_back( f );
+   }
+   // boundary: faces with one neighbour cell, and every edge/vertex of such a face
+   // (SetupPrimitiveStorage::setMeshBoundaryFlagsOnBoundary(1,0,true) + create0123BC:
+   //  flag 1 -> DirichletBoundary, 0 -> Inner)
+   std::vector< int > fCells( o.F.size(), 0 );
+   for ( auto& t : o.T )
+   {
+      const int fl[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+      for ( auto& f : fl )
+      {
+         std::array< int, 3 > k = { t[f[0]], t[f[1]], t[f[2]] };
+         std::sort( k.begin(), k.end() );
+         fCells[o.fId[k]]++;
+      }
+   }
+   o.vBc.assign( o.V.size(), ORC_INNER );
+   o.eBc.assign( o.E.size(), ORC_INNER );
+   o.fBc.assign( o.F.size(), ORC_INNER );
+   o.fEdges.resize( o.F.size() );
+   o.fVerts.resize( o.F.size() );
+   o.eVerts.resize( o.E.size() );
+   for ( size_t e = 0; e < o.E.size(); ++e )
+      o.eVerts[e] = { o.E[e][0], o.E[e][1] };
+   for ( size_t f = 0; f < o.F.size(); ++f )
+   {
+      auto& k       = o.F[f];
+      o.fVerts[f]   = { k[0], k[1], k[2] };
+      o.fEdges[f]   = { o.eId[{ k[0], k[1] }], o.eId[{ k[0], k[2] }], o.eId[{ k[1], k[2] }] };
+      if ( fCells[f] == 1 )
+      {
+         o.fBc[f] = ORC_DIRICHLET;
+         for ( int e : o.fEdges[f] )
+            o.eBc[e] = ORC_DIRICHLET;
+         for ( int v : o.fVerts[f] )
+            o.vBc[v] = ORC_DIRICHLET;
+      }
+   }
+}
+
+void buildLevel( Oracle& o, int L )
+{
+   Level lv;
+   lv.L           = L;
+   lv.N           = i64( 1 ) << L;
+   const i64 N    = lv.N;
+   lv.S           = tetSize( N + 1 );
+   const i64 nV   = i64( o.V.size() ), nE = i64( o.E.size() ), nF = i64( o.F.size() ), nC = i64( o.T.size() );
+   lv.nIntFace    = N >= 3 ? ( N - 1 ) * ( N - 2 ) / 2 : 0;
+   lv.nIntCell    = N >= 4 ? tetSize( N - 3 ) : 0;
+   lv.offE        = nV;
+   lv.offF        = lv.offE + nE * std::max< i64 >( N - 1, 0 );
+   lv.offC        = lv.offF + nF * lv.nIntFace;
+   lv.nDof        = lv.offC + nC * lv.nIntCell;
+   lv.kind.resize( lv.nDof );
+   lv.bc.resize( lv.nDof );
+   lv.owner.resize( lv.nDof );
+   for ( i64 v = 0; v < nV; ++v )
+   {
+      lv.kind[v]  = 0;
+      lv.bc[v]    = o.vBc[v];
+      lv.owner[v] = int32_t( v );
+   }
+   for ( i64 e = 0; e < nE; ++e )
+      for ( i64 i = 0; i < N - 1; ++i )
+      {
+         i64 d       = lv.offE + e * ( N - 1 ) + i;
+         lv.kind[d]  = 1;
+         lv.bc[d]    = o.eBc[e];
+         lv.owner[d] = int32_t( e );
+      }
+   for ( i64 f = 0; f < nF; ++f )
+      for ( i64 i = 0; i < lv.nIntFace; ++i )
+      {
+         i64 d       = lv.offF + f * lv.nIntFace + i;
+         lv.kind[d]  = 2;
+         lv.bc[d]    = o.fBc[f];
+         lv.owner[d] = int32_t( f );
+      }
+   for ( i64 c = 0; c < nC; ++c )
+      for ( i64 i = 0; i < lv.nIntCell; ++i )
+      {
+         i64 d       = lv.offC + c * lv.nIntCell + i;
+         lv.kind[d]  = 3;
+         lv.bc[d]    = ORC_INNER;
+         lv.owner[d] = int32_t( c );
+      }
+   // closure point -> DoF by exact barycentric key
+   lv.cellMap.assign( nC, std::vector< int32_t >( lv.S ) );
+   std::vector< std::vector< std::array< int32_t, 4 > > > entries( lv.offC );
+   for ( i64 c = 0; c < nC; ++c )
+   {
+      auto& t = o.T[c];
+      for ( i64 z = 0; z <= N; ++z )
+         for ( i64 y = 0; y <= N - z; ++y )
+            for ( i64 x = 0; x <= N - y - z; ++x )
+            {
+               const i64 b[4] = { N - x - y - z, x, y, z };
+               std::vector< std::pair< int, i64 > > nz;
+               for ( int k = 0; k < 4; ++k )
+                  if ( b[k] > 0 )
+                     nz.push_back( { t[k], b[k] } );
+               std::sort( nz.begin(), nz.end() );
+               i64 d = -1;
+               if ( nz.size() == 1 )
+                  d = nz[0].first;
+               else if ( nz.size() == 2 )
+               {
+                  const int e = o.eId.at( { nz[0].first, nz[1].first } );
+                  d           = lv.offE + e * ( N - 1 ) + ( nz[1].second - 1 );
+               }
+               else if ( nz.size() == 3 )
+               {
+                  const int f = o.fId.at( { nz[0].first, nz[1].first, nz[2].first } );
+                  const i64 i = nz[1].second, j = nz[2].second;
+                  d = lv.offF + f * lv.nIntFace + ( j - 1 ) * ( N - 1 ) - ( j - 1 ) * j / 2 + ( i - 1 );
+               }
+               else
+               {
+                  d = lv.offC + c * lv.nIntCell + cellIdx( N - 3, x - 1, y - 1, z - 1 );
+               }
+               lv.cellMap[c][cellIdx( N + 1, x, y, z )] = int32_t( d );
+               if ( d < lv.offC )
+                  entries[d].push_back( { int32_t( c ), int32_t( x ), int32_t( y ), int32_t( z ) } );
+            }
+   }
+   lv.entOff.assign( lv.offC + 1, 0 );
+   for ( i64 d = 0; d < lv.offC; ++d )
+      lv.entOff[d + 1] = lv.entOff[d] + i64( entries[d].size() );
+   lv.ent.reserve( lv.entOff[lv.offC] );
+   for ( i64 d = 0; d < lv.offC; ++d )
+      for ( auto& e : entries[d] )
+         lv.ent.push_back( e );
+   o.lv.push_back( std::move( lv ) );
+}
+
+std::array< double, 3 > microCoord( const Oracle& o, int c, i64 N, i64 x, i64 y, i64 z )
+{
+   // vertexdof::macrocell::coordinateFromIndex (src/hyteg/p1functionspace/VertexDoFMacroCell.hpp:68-75)
+   const auto& t = o.T[c];
+   std::array< double, 3 > p;
+   for ( int d = 0; d < 3; ++d )
+   {
+      const double v0 = o.V[t[0]][d];
+      p[d] = v0 + ( o.V[t[1]][d] - v0 ) / double( N ) * double( x ) + ( o.V[t[2]][d] - v0 ) / double( N ) * double( y ) +
+             ( o.V[t[3]][d] - v0 ) / double( N ) * double( z );
+   }
+   return p;
+}
+
+// Element matrices of the six micro-tet shapes of a cell at level L.
+void cellElementMatrices( const Oracle& o, int c, i64 N, std::array< std::array< std::array< double, 4 >, 4 >, 6 >& K )
+{
+   for ( int t = 0; t < 6; ++t )
+   {
+      std::array< std::array< double, 3 >, 4 > X;
+      for ( int j = 0; j < 4; ++j )
+         X[j] = microCoord( o, c, N, kMicro[t][j][0], kMicro[t][j][1], kMicro[t][j][2] );
+      double Km[4][4];
+      p1Stiffness( X, Km );
+      for ( int i = 0; i < 4; ++i )
+         for ( int j = 0; j < 4; ++j )
+            K[t][i][j] = Km[i][j];
+   }
+}
+
+// ---------------------------------------------------------------------------
+// Row evaluation: the partial row of DoF at closure point p of cell c.
+// val(d) supplies the value of DoF d (current or snapshot, see smooth_sor).
+// ---------------------------------------------------------------------------
+template < typename T, typename Val >
+inline void partialRow( const Oracle& o, const Op& op, const Level& lv, int c, i64 x, i64 y, i64 z, Val&& val, T& diag,
+                        T& off )
+{
+   const i64 N    = lv.N;
+   const int mask = pointMask( N, x, y, z );
+   const auto& map = lv.cellMap[c];
+   if ( !op.variable )
+   {
+      const auto& st = op.st[lv.L][c][mask];
+      diag += T( st[0] );
+      for ( int q = 1; q < 15; ++q )
+      {
+         const i64 xx = x + kOff[q][0], yy = y + kOff[q][1], zz = z + kOff[q][2];
+         if ( !inClosure( N, xx, yy, zz ) )
+            continue;
+         off += T( st[q] ) * val( map[cellIdx( N + 1, xx, yy, zz )] );
+      }
+   }
+   else
+   {
+      const auto& K  = op.K[lv.L][c];
+      const auto& kv = op.k[lv.L];
+      for ( const auto& in : kIncident )
+      {
+         bool ok = true;
+         for ( int j = 0; j < 4 && ok; ++j )
+            ok = relAllowed( mask, in.rel[j] );
+         if ( !ok )
+            continue;
+         i64 dof[4];
+         for ( int j = 0; j < 4; ++j )
+            dof[j] = map[cellIdx( N + 1, x + in.rel[j][0], y + in.rel[j][1], z + in.rel[j][2] )];
+         // 5-point degree-3 rule of p1_div_k_grad_affine_q3::integrateAll
+         // (src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_affine_q3.cpp:179+) with the
+         // coefficient callback = P1 interpolant of the nodal k: centroid weight -2/15, four
+         // points (1/2,1/6,1/6,1/6) with weight 3/40, all times |det J| = 6|T|.
+         double kq[5];
+         kq[0] = 0.25 * ( kv[dof[0]] + kv[dof[1]] + kv[dof[2]] + kv[dof[3]] );
+         for ( int a = 0; a < 4; ++a )
+         {
+            double s = 0;
+            for ( int j = 0; j < 4; ++j )
+               s += ( j == a ? 0.5 : 1.0 / 6.0 ) * kv[dof[j]];
+            kq[a + 1] = s;
+         }
+         const double quad = -2.0 / 15.0 * kq[0] + 3.0 / 40.0 * ( kq[1] + kq[2] + kq[3] + kq[4] );
+         const double scale = 6.0 * quad; // K holds |T| grad.grad = |detJ|/6 grad.grad
+         for ( int j = 0; j < 4; ++j )
+         {
+            const double a = scale * K[in.t][in.k][j];
+            if ( j == in.k )
+               diag += T( a );
+            else
+               off += T( a ) * val( dof[j] );
+         }
+      }
+   }
+}
+
+template < typename T, typename Val >
+inline void fullRow( const Oracle& o, const Op& op, const Level& lv, i64 d, Val&& val, T& diag, T& off )
+{
+   if ( d >= lv.offC )
+   {
+      const i64 c = ( d - lv.offC ) / lv.nIntCell;
+      // invert the interior tet index by scanning (used only for per-DoF access paths)
+      i64 r = ( d - lv.offC ) % lv.nIntCell;
+      const i64 W = lv.N - 3;
+      for ( i64 z = 0; z < W; ++z )
+      {
+         const i64 sl = ( W - z ) * ( W - z + 1 ) / 2;
+         if ( r >= sl )
+         {
+            r -= sl;
+            continue;
+         }
+         for ( i64 y = 0; y < W - z; ++y )
+         {
+            const i64 rl = W - z - y;
+            if ( r >= rl )
+            {
+               r -= rl;
+               continue;
+            }
+            partialRow( o, op, lv, int( c ), r + 1, y + 1, z + 1, val, diag, off );
+            return;
+         }
+      }
+      return;
+   }
+   for ( i64 e = lv.entOff[d]; e < lv.entOff[d + 1]; ++e )
+   {
+      const auto& en = lv.ent[e];
+      partialRow( o, op, lv, en[0], en[1], en[2], en[3], val, diag, off );
+   }
+}
+
+inline bool flagged( uint8_t bc, int flag ) { return ( bc & flag ) != 0; }
+
+// apply (P1Operator.hpp:196-324; P1ElementwiseOperator.cpp:64-221)
+template < typename T >
+void applyT( const Oracle& o, const Op& op, const Level& lv, const T* src, T* dst, int flag, bool add )
+{
+   auto val = [src]( i64 d ) { return src[d]; };
+#pragma omp parallel for schedule( dynamic, 64 )
+   for ( i64 d = 0; d < lv.offC; ++d )
+   {
+      if ( !flagged( lv.bc[d], flag ) )
+         continue;
+      T diag = 0, off = 0;
+      fullRow( o, op, lv, d, val, diag, off );
+      const T r = diag * src[d] + off;
+      dst[d]    = add ? dst[d] + r : r;
+   }
+   const i64 N = lv.N;
+#pragma omp parallel for schedule( dynamic, 1 )
+   for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+      for ( i64 z = 1; z <= N; ++z )
+         for ( i64 y = 1; y <= N - z; ++y )
+            for ( i64 x = 1; x <= N - y - z - 1; ++x )
+            {
+               const i64 d = lv.cellMap[c][cellIdx( N + 1, x, y, z )];
+               T diag = 0, off = 0;
+               partialRow( o, op, lv, int( c ), x, y, z, val, diag, off );
+               const T r = diag * src[d] + off;
+               dst[d]    = add ? dst[d] + r : r;
+            }
+}
+
+template < typename T >
+inline void sorUpdate( T& x, T b, T diag, T off, T relax )
+{
+   x = ( T( 1 ) - relax ) * x + relax * ( b - off ) / diag;
+}
+
+// smooth_sor (P1Operator.hpp:352-422): six-way ghost update, then forward sweeps
+// V -> E -> F -> C. Within a macro-face/edge/vertex the sweep is lexicographic and
+// reads current values only for DoFs of that primitive's closure; DoFs of other
+// primitives are read from the ghost layers filled before the sweep (VertexDoFPackInfo.hpp:
+// edge->face only refreshes the face's own boundary, not its ghost layers), i.e.
+// from the start-of-sweep snapshot. Macro-cells read their full (refreshed) closure.
+template < typename T >
+void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag )
+{
+   const i64 N = lv.N;
+   std::vector< T > xs( x, x + lv.nDof );
+   const T* snap = xs.data();
+   // vertices (VertexDoFMacroVertex.hpp:208-229)
+   for ( i64 v = 0; v < i64( o.V.size() ); ++v )
+   {
+      if ( !flagged( lv.bc[v], flag ) )
+         continue;
+      auto val = [&]( i64 d ) { return d == v ? x[d] : snap[d]; };
+      T diag = 0, off = 0;
+      fullRow( o, op, lv, v, val, diag, off );
+      sorUpdate( x[v], b[v], diag, off, relax );
+   }
+   if ( N >= 2 )
+   {
+      // edges (P1Operator.hpp:1353-1423), each independent given the snapshot
+#pragma omp parallel for schedule( dynamic, 1 )
+      for ( i64 e = 0; e < i64( o.E.size() ); ++e )
+      {
+         if ( !flagged( o.eBc[e], flag ) )
+            continue;
+         const int va = o.E[e][0], vb = o.E[e][1];
+         auto val = [&]( i64 d ) {
+            const bool mine = ( lv.kind[d] == 1 && lv.owner[d] == e ) || ( lv.kind[d] == 0 && ( d == va || d == vb ) );
+            return mine ? x[d] : snap[d];
+         };
+         for ( i64 i = 0; i < N - 1; ++i )
+         {
+            const i64 d = lv.offE + e * ( N - 1 ) + i;
+            T diag = 0, off = 0;
+            fullRow( o, op, lv, d, val, diag, off );
+            sorUpdate( x[d], b[d], diag, off, relax );
+         }
+      }
+   }
+   if ( N >= 3 )
+   {
+      // faces (P1ConstantOperator.cpp:372-534)
+#pragma omp parallel for schedule( dynamic, 1 )
+      for ( i64 f = 0; f < i64( o.F.size() ); ++f )
+      {
+         if ( !flagged( o.fBc[f], flag ) )
+            continue;
+         const auto& fe = o.fEdges[f];
+         const auto& fv = o.fVerts[f];
+         auto val = [&]( i64 d ) {
+            bool mine = false;
+            switch ( lv.kind[d] )
+            {
+            case 2: mine = lv.owner[d] == f; break;
+            case 1: mine = lv.owner[d] == fe[0] || lv.owner[d] == fe[1] || lv.owner[d] == fe[2]; break;
+            case 0: mine = d == fv[0] || d == fv[1] || d == fv[2]; break;
+            default: mine = false;
+            }
+            return mine ? x[d] : snap[d];
+         };
+         for ( i64 i = 0; i < lv.nIntFace; ++i )
+         {
+            const i64 d = lv.offF + f * lv.nIntFace + i;
+            T diag = 0, off = 0;
+            fullRow( o, op, lv, d, val, diag, off );
+            sorUpdate( x[d], b[d], diag, off, relax );
+         }
+      }
+   }
+   // cells (sor_3D_macrocell_P1.cpp:31-77): lexicographic, x fastest
+   auto cur = [x]( i64 d ) { return x[d]; };
+#pragma omp parallel for schedule( dynamic, 1 )
+   for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+      for ( i64 z = 1; z <= N; ++z )
+         for ( i64 y = 1; y <= N - z; ++y )
+            for ( i64 xx = 1; xx <= N - y - z - 1; ++xx )
+            {
+               const i64 d = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
+               T diag = 0, off = 0;
+               partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
+               sorUpdate( x[d], b[d], diag, off, relax );
+            }
+}
+
+int dofColour( const Oracle& o, const Level& lv, i64 d, const int* labels, int m )
+{
+   int32_t c;
+   i64     x, y, z;
+   if ( d >= lv.offC )
+   {
+      c = int32_t( ( d - lv.offC ) / lv.nIntCell );
+      // find by scanning the cell closure map (per-DoF path; small sizes only)
+      const auto& map = lv.cellMap[c];
+      const i64 N = lv.N;
+      for ( z = 0; z <= N; ++z )
+         for ( y = 0; y <= N - z; ++y )
+            for ( x = 0; x <= N - y - z; ++x )
+               if ( map[cellIdx( N + 1, x, y, z )] == d )
+                  goto found;
+      return -1;
+   }
+   else
+   {
+      const auto& en = lv.ent[lv.entOff[d]];
+      c = en[0];
+      x = en[1];
+      y = en[2];
+      z = en[3];
+   }
+found:
+   const auto& t = o.T[c];
+   const i64 b[4] = { lv.N - x - y - z, x, y, z };
+   i64 s = 0;
+   for ( int k = 0; k < 4; ++k )
+      s += i64( labels[t[k]] ) * b[k];
+   return int( ( ( s % m ) + m ) % m );
+}
+
+// Multicolour SOR: colour(p) = sum_k label(V_k) b_k mod m over the barycentric micro-
+// coordinates; within one colour no two DoFs are coupled, so the update order inside
+// a colour is irrelevant.
+template < typename T >
+void sorColoredT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag, const int* labels,
+                  int m )
+{
+   const i64 N = lv.N;
+   auto cur = [x]( i64 d ) { return x[d]; };
+   for ( int col = 0; col < m; ++col )
+   {
+#pragma omp parallel for schedule( dynamic, 64 )
+      for ( i64 d = 0; d < lv.offC; ++d )
+      {
+         if ( !flagged( lv.bc[d], flag ) )
+            continue;
+         if ( dofColour( o, lv, d, labels, m ) != col )
+            continue;
+         T diag = 0, off = 0;
+         fullRow( o, op, lv, d, cur, diag, off );
+         sorUpdate( x[d], b[d], diag, off, relax );
+      }
+#pragma omp parallel for schedule( dynamic, 1 )
+      for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+      {
+         const auto& t = o.T[c];
+         for ( i64 z = 1; z <= N; ++z )
+            for ( i64 y = 1; y <= N - z; ++y )
+               for ( i64 xx = 1; xx <= N - y - z - 1; ++xx )
+               {
+                  const i64 bb[4] = { N - xx - y - z, xx, y, z };
+                  i64 s = 0;
+                  for ( int k = 0; k < 4; ++k )
+                     s += i64( labels[t[k]] ) * bb[k];
+                  if ( int( ( ( s % m ) + m ) % m ) != col )
+                     continue;
+                  const i64 d = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
+                  T diag = 0, off = 0;
+                  partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
+                  sorUpdate( x[d], b[d], diag, off, relax );
+               }
+      }
+   }
+}
+
+// Weighted Jacobi (P1Operator.hpp smooth_jac / WeightedJacobiSmoother):
+// x <- x + relax * D^-1 (b - A x)
+template < typename T >
+void jacobiT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag )
+{
+   std::vector< T > xo( x, x + lv.nDof );
+   const T* xs = xo.data();
+   auto val = [xs]( i64 d ) { return xs[d]; };
+#pragma omp parallel for schedule( dynamic, 256 )
+   for ( i64 d = 0; d < lv.nDof; ++d )
+   {
+      if ( !flagged( lv.bc[d], flag ) )
+         continue;
+      T diag = 0, off = 0;
+      fullRow( o, op, lv, d, val, diag, off );
+      x[d] = xs[d] + relax * ( b[d] - off - diag * xs[d] ) / diag;
+   }
+}
+
+// first (cell, x, y, z) occurrence of every DoF of a level
+struct Where
+{
+   std::vector< std::array< int32_t, 4 > > w;
+};
+Where whereOf( const Oracle& o, const Level& lv )
+{
+   Where W;
+   W.w.assign( lv.nDof, { -1, 0, 0, 0 } );
+   const i64 N = lv.N;
+   for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+      for ( i64 z = 0; z <= N; ++z )
+         for ( i64 y = 0; y <= N - z; ++y )
+            for ( i64 x = 0; x <= N - y - z; ++x )
+            {
+               const i64 d = lv.cellMap[c][cellIdx( N + 1, x, y, z )];
+               if ( W.w[d][0] < 0 )
+                  W.w[d] = { int32_t( c ), int32_t( x ), int32_t( y ), int32_t( z ) };
+            }
+   return W;
+}
+
+// Linear interpolation of a fine micro-vertex from the coarse level: coincident
+// coarse vertex (weight 1) or the midpoint of a coarse micro-edge (1/2, 1/2).
+// (P1toP1LinearProlongation.cpp:194-410 with the generated push kernel.)
+template < typename T >
+T interpolateFine( const Oracle& o, const Level& cl, int c, i64 X, i64 Y, i64 Z, const T* coarse )
+{
+   const i64 Nc = cl.N;
+   const auto& map = cl.cellMap[c];
+   const int px = int( X & 1 ), py = int( Y & 1 ), pz = int( Z & 1 );
+   if ( !px && !py && !pz )
+      return coarse[map[cellIdx( Nc + 1, X / 2, Y / 2, Z / 2 )]];
+   int ox = 0, oy = 0, oz = 0;
+   const int pat = px | ( py << 1 ) | ( pz << 2 );
+   switch ( pat )
+   {
+   case 1: ox = 1; break;
+   case 2: oy = 1; break;
+   case 4: oz = 1; break;
+   case 3: ox = -1; oy = 1; break;
+   case 5: ox = -1; oz = 1; break;
+   case 6: oy = -1; oz = 1; break;
+   case 7: ox = -1; oy = 1; oz = -1; break;
+   }
+   const i64 a = map[cellIdx( Nc + 1, ( X - ox ) / 2, ( Y - oy ) / 2, ( Z - oz ) / 2 )];
+   const i64 b = map[cellIdx( Nc + 1, ( X + ox ) / 2, ( Y + oy ) / 2, ( Z + oz ) / 2 )];
+   return T( 0.5 ) * ( coarse[a] + coarse[b] );
+}
+
+template < typename T >
+void prolongateT( const Oracle& o, int coarseLevel, const T* coarse, T* fine, int flag, bool add )
+{
+   const Level& cl = o.lv[coarseLevel];
+   const Level& fl = o.lv[coarseLevel + 1];
+   Where W = whereOf( o, fl );
+#pragma omp parallel for schedule( static )
+   for ( i64 d = 0; d < fl.nDof; ++d )
+   {
+      if ( !flagged( fl.bc[d], flag ) )
+         continue;
+      const auto& w = W.w[d];
+      const T v = interpolateFine( o, cl, w[0], w[1], w[2], w[3], coarse );
+      fine[d]   = add ? fine[d] + v : v;
+   }
+}
+
+// Full-weighting restriction = transpose of the linear prolongation
+// (P1toP1LinearRestriction.cpp:168-345 with the generated pull kernel, whose
+//  1/#neighbour-cells factors make each fine point count exactly once).
+template < typename T >
+void restrictT( const Oracle& o, int fineLevel, const T* fine, T* coarse, int flag )
+{
+   const Level& fl = o.lv[fineLevel];
+   const Level& cl = o.lv[fineLevel - 1];
+   Where W = whereOf( o, cl );
+   const i64 Nf = fl.N;
+#pragma omp parallel for schedule( dynamic, 64 )
+   for ( i64 d = 0; d < cl.nDof; ++d )
+   {
+      if ( !flagged( cl.bc[d], flag ) )
+         continue;
+      // all cells containing the coarse DoF
+      std::vector< std::array< int32_t, 4 > > occ;
+      if ( d < cl.offC )
+         for ( i64 e = cl.entOff[d]; e < cl.entOff[d + 1]; ++e )
+            occ.push_back( cl.ent[e] );
+      else
+         occ.push_back( W.w[d] );
+      if ( occ.size() == 1 )
+      {
+         // a single cell: the fine neighbours inside it are distinct
+         const auto& en  = occ[0];
+         const i64   X   = 2 * en[1], Y = 2 * en[2], Z = 2 * en[3];
+         const auto& map = fl.cellMap[en[0]];
+         T           h   = 0;
+         for ( int q = 1; q < 15; ++q )
+         {
+            const i64 xx = X + kOff[q][0], yy = Y + kOff[q][1], zz = Z + kOff[q][2];
+            if ( inClosure( Nf, xx, yy, zz ) )
+               h += fine[map[cellIdx( Nf + 1, xx, yy, zz )]];
+         }
+         coarse[d] = fine[map[cellIdx( Nf + 1, X, Y, Z )]] + T( 0.5 ) * h;
+         continue;
+      }
+      std::set< i64 > nbr;
+      i64 centre = -1;
+      for ( auto& en : occ )
+      {
+         const i64 X = 2 * en[1], Y = 2 * en[2], Z = 2 * en[3];
+         const auto& map = fl.cellMap[en[0]];
+         centre = map[cellIdx( Nf + 1, X, Y, Z )];
+         for ( int q = 1; q < 15; ++q )
+         {
+            const i64 xx = X + kOff[q][0], yy = Y + kOff[q][1], zz = Z + kOff[q][2];
+            if ( inClosure( Nf, xx, yy, zz ) )
+               nbr.insert( map[cellIdx( Nf + 1, xx, yy, zz )] );
+         }
+      }
+      T s = fine[centre];
+      T h = 0;
+      for ( i64 q : nbr )
+         h += fine[q];
+      coarse[d] = s + T( 0.5 ) * h;
+   }
+}
+
+template < typename T >
+double dotT( const Level& lv, const T* a, const T* b, int flag )
+{
+   double s = 0;
+#pragma omp parallel for reduction( + : s ) schedule( static )
+   for ( i64 d = 0; d < lv.nDof; ++d )
+      if ( flagged( lv.bc[d], flag ) )
+         s += double( a[d] ) * double( b[d] );
+   return s;
+}
+
+// CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:66-135, init :237+), identity preconditioner,
+// absolute stopping test sqrt(r.r) < tol, flag Inner|Neumann|Freeslip.
+template < typename T >
+int cgT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, double tol, int maxIter )
+{
+   const int flag = ORC_INNER | ORC_NEUMANN | ORC_FREESLIP;
+   const i64 n    = lv.nDof;
+   std::vector< T > p( n, 0 ), ap( n, 0 ), r( n, 0 );
+   applyT( o, op, lv, x, p.data(), flag, false );
+   for ( i64 d = 0; d < n; ++d )
+      if ( flagged( lv.bc[d], flag ) )
+         r[d] = b[d] - p[d];
+   for ( i64 d = 0; d < n; ++d )
+      if ( flagged( lv.bc[d], flag ) )
+         p[d] = r[d];
+   double prsold = dotT( lv, r.data(), r.data(), flag );
+   if ( std::sqrt( prsold ) < tol )
+      return 0;
+   int it = 0;
+   for ( ; it < maxIter; ++it )
+   {
+      applyT( o, op, lv, p.data(), ap.data(), flag, false );
+      const double pAp   = dotT( lv, p.data(), ap.data(), flag );
+      const T      alpha = T( prsold / pAp );
+      for ( i64 d = 0; d < n; ++d )
+         if ( flagged( lv.bc[d], flag ) )
+         {
+            x[d] += alpha * p[d];
+            r[d] -= alpha * ap[d];
+         }
+      const double rsnew = dotT( lv, r.data(), r.data(), flag );
+      if ( std::sqrt( rsnew ) < tol )
+         break;
+      const T beta = T( rsnew / prsold );
+      for ( i64 d = 0; d < n; ++d )
+         if ( flagged( lv.bc[d], flag ) )
+            p[d] = r[d] + beta * p[d];
+      prsold = rsnew;
+   }
+   return it;
+}
+
+Oracle* H( void* h ) { return static_cast< Oracle* >( h ); }
+
+// ---------------------------------------------------------------------------
+// GMG (GeometricMultigridSolver.hpp:136-235)
+// ---------------------------------------------------------------------------
+template < typename T >
+struct Hier
+{
+   std::vector< std::vector< T > > x, b, tmp;
+};
+
+struct GmgCfg
+{
+   int         op, minL, maxL, pre, post, smoother, m;
+   double      relax, coarseTol;
+   const int*  labels;
+};
+
+template < typename T >
+void smoothT( const Oracle& o, const GmgCfg& g, int level, T* x, const T* b )
+{
+   const Op& op = o.ops[g.op];
+   const Level& lv = o.lv[level];
+   const int flag = ORC_INNER | ORC_NEUMANN;
+   if ( g.smoother == 0 )
+      sorRefT( o, op, lv, x, b, T( g.relax ), flag );
+   else if ( g.smoother == 1 )
+      sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m );
+   else
+      jacobiT( o, op, lv, x, b, T( g.relax ), flag );
+}
+
+template < typename T >
+void vcycleT( const Oracle& o, const GmgCfg& g, Hier< T >& h, int level )
+{
+   const int flag = ORC_INNER | ORC_NEUMANN;
+   const Op& op   = o.ops[g.op];
+   if ( level == g.minL )
+   {
+      // coarse grid solve in FP64 (the mixed-precision variant keeps it in FP64 too)
+      const Level& lv = o.lv[level];
+      std::vector< double > xd( h.x[level].begin(), h.x[level].end() ), bd( h.b[level].begin(), h.b[level].end() );
+      cgT< double >( o, op, lv, xd.data(), bd.data(), g.coarseTol, 100000 );
+      for ( i64 d = 0; d < lv.nDof; ++d )
+         h.x[level][d] = T( xd[d] );
+      return;
+   }
+   const Level& lv = o.lv[level];
+   for ( int i = 0; i < g.pre; ++i )
+      smoothT( o, g, level, h.x[level].data(), h.b[level].data() );
+   applyT( o, op, lv, h.x[level].data(), h.tmp[level].data(), flag, false );
+   for ( i64 d = 0; d < lv.nDof; ++d )
+      if ( flagged( lv.bc[d], flag ) )
+         h.tmp[level][d] = h.b[level][d] - h.tmp[level][d];
+   restrictT( o, level, h.tmp[level].data(), h.tmp[level - 1].data(), flag );
+   const Level& cl = o.lv[level - 1];
+   for ( i64 d = 0; d < cl.nDof; ++d )
+      if ( flagged( cl.bc[d], flag ) )
+         h.b[level - 1][d] = h.tmp[level - 1][d];
+   std::fill( h.x[level - 1].begin(), h.x[level - 1].end(), T( 0 ) ); // x.interpolate(0, level-1) on All
+   vcycleT( o, g, h, level - 1 );
+   prolongateT( o, level - 1, h.x[level - 1].data(), h.x[level].data(), flag, true );
+   for ( int i = 0; i < g.post; ++i )
+      smoothT( o, g, level, h.x[level].data(), h.b[level].data() );
+}
+
+template < typename T >
+void allocHier( const Oracle& o, Hier< T >& h, int maxL )
+{
+   h.x.resize( maxL + 1 );
+   h.b.resize( maxL + 1 );
+   h.tmp.resize( maxL + 1 );
+   for ( int l = 0; l <= maxL; ++l )
+   {
+      h.x[l].assign( o.lv[l].nDof, T( 0 ) );
+      h.b[l].assign( o.lv[l].nDof, T( 0 ) );
+      h.tmp[l].assign( o.lv[l].nDof, T( 0 ) );
+   }
+}
+
+double relResidual( const Oracle& o, const Op& op, int level, const double* x, const double* b, std::vector< double >& r )
+{
+   const int flag  = ORC_INNER | ORC_NEUMANN;
+   const Level& lv = o.lv[level];
+   applyT( o, op, lv, x, r.data(), flag, false );
+   for ( i64 d = 0; d < lv.nDof; ++d )
+      r[d] = flagged( lv.bc[d], flag ) ? b[d] - r[d] : 0.0;
+   const double nb = std::sqrt( dotT( lv, b, b, flag ) );
+   return std::sqrt( dotT( lv, r.data(), r.data(), flag ) ) / ( nb > 0 ? nb : 1.0 );
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// C API
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void* orc_create( const double* coords, int64_t nv, const int64_t* tets, int64_t nt, int maxLevel )
+{
+   auto* o = new Oracle;
+   o->V.resize( nv );
+   for ( int64_t i = 0; i < nv; ++i )
+      o->V[i] = { coords[3 * i], coords[3 * i + 1], coords[3 * i + 2] };
+   o->T.resize( nt );
+   for ( int64_t i = 0; i < nt; ++i )
+      o->T[i] = { int( tets[4 * i] ), int( tets[4 * i + 1] ), int( tets[4 * i + 2] ), int( tets[4 * i + 3] ) };
+   o->maxLevel = maxLevel;
+   buildTopology( *o );
+   for ( int l = 0; l <= maxLevel; ++l )
+      buildLevel( *o, l );
+   orc_op_laplace( o ); // op 0
+   return o;
+}
+
+void orc_destroy( void* h ) { delete H( h ); }
+
+int64_t orc_num_dofs( void* h, int level ) { return H( h )->lv[level].nDof; }
+
+int64_t orc_num_prims( void* h, int kind )
+{
+   auto* o = H( h );
+   switch ( kind )
+   {
+   case 0: return int64_t( o->V.size() );
+   case 1: return int64_t( o->E.size() );
+   case 2: return int64_t( o->F.size() );
+   default: return int64_t( o->T.size() );
+   }
+}
+
+void orc_dof_coords( void* h, int level, double* xyz )
+{
+   auto* o = H( h );
+   const Level& lv = o->lv[level];
+   const i64 N = lv.N;
+   for ( i64 c = 0; c < i64( o->T.size() ); ++c )
+      for ( i64 z = 0; z <= N; ++z )
+         for ( i64 y = 0; y <= N - z; ++y )
+            for ( i64 x = 0; x <= N - y - z; ++x )
+            {
+               const i64 d = lv.cellMap[c][cellIdx( N + 1, x, y, z )];
+               auto p = microCoord( *o, int( c ), N, x, y, z );
+               xyz[3 * d] = p[0];
+               xyz[3 * d + 1] = p[1];
+               xyz[3 * d + 2] = p[2];
+            }
+}
+
+void orc_dof_info( void* h, int level, uint8_t* kind, uint8_t* bc )
+{
+   const Level& lv = H( h )->lv[level];
+   std::memcpy( kind, lv.kind.data(), lv.nDof );
+   std::memcpy( bc, lv.bc.data(), lv.nDof );
+}
+
+void orc_cell_closure_map( void* h, int level, int cell, int32_t* out )
+{
+   const auto& m = H( h )->lv[level].cellMap[cell];
+   std::memcpy( out, m.data(), m.size() * sizeof( int32_t ) );
+}
+
+int orc_op_laplace( void* h )
+{
+   auto* o = H( h );
+   Op op;
+   op.variable = false;
+   op.st.resize( o->maxLevel + 1 );
+   for ( int L = 0; L <= o->maxLevel; ++L )
+   {
+      const i64 N = i64( 1 ) << L;
+      op.st[L].resize( o->T.size() );
+      for ( size_t c = 0; c < o->T.size(); ++c )
+      {
+         std::array< std::array< std::array< double, 4 >, 4 >, 6 > K;
+         cellElementMatrices( *o, int( c ), N, K );
+         for ( int mask = 0; mask < 16; ++mask )
+         {
+            auto& st = op.st[L][c][mask];
+            st.fill( 0.0 );
+            // sum of row "k" of every incident micro-tet inside the closure
+            // (P1Elements.hpp:215-302 getNeighboringElements, :464-526)
+            for ( const auto& in : kIncident )
+            {
+               bool ok = true;
+               for ( int j = 0; j < 4 && ok; ++j )
+                  ok = relAllowed( mask, in.rel[j] );
+               if ( !ok )
+                  continue;
+               for ( int j = 0; j < 4; ++j )
+                  st[offsetId( in.rel[j][0], in.rel[j][1], in.rel[j][2] )] += K[in.t][in.k][j];
+            }
+         }
+      }
+   }
+   o->ops.push_back( std::move( op ) );
+   return int( o->ops.size() - 1 );
+}
+
+int orc_op_divkgrad( void* h, const double* const* nodalK )
+{
+   auto* o = H( h );
+   Op op;
+   op.variable = true;
+   op.k.resize( o->maxLevel + 1 );
+   op.K.resize( o->maxLevel + 1 );
+   for ( int L = 0; L <= o->maxLevel; ++L )
+   {
+      op.k[L].assign( nodalK[L], nodalK[L] + o->lv[L].nDof );
+      op.K[L].resize( o->T.size() );
+      for ( size_t c = 0; c < o->T.size(); ++c )
+         cellElementMatrices( *o, int( c ), i64( 1 ) << L, op.K[L][c] );
+   }
+   o->ops.push_back( std::move( op ) );
+   return int( o->ops.size() - 1 );
+}
+
+void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 )
+{
+   const auto& st = H( h )->ops[op].st[level][cell][mask];
+   for ( int q = 0; q < 15; ++q )
+      out15[q] = st[q];
+}
+
+void orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add )
+{
+   auto* o = H( h );
+   applyT( *o, o->ops[op], o->lv[level], src, dst, flag, add != 0 );
+}
+
+void orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag )
+{
+   auto* o = H( h );
+   sorRefT( *o, o->ops[op], o->lv[level], x, b, relax, flag );
+}
+
+void orc_sor_colored( void* h, int op, int level, double* x, const double* b, double relax, int flag, const int* labels,
+                      int m )
+{
+   auto* o = H( h );
+   sorColoredT( *o, o->ops[op], o->lv[level], x, b, relax, flag, labels, m );
+}
+
+void orc_jacobi( void* h, int op, int level, double* x, const double* b, double relax, int flag )
+{
+   auto* o = H( h );
+   jacobiT( *o, o->ops[op], o->lv[level], x, b, relax, flag );
+}
+
+void orc_prolongate( void* h, int coarseLevel, const double* coarse, double* fine, int flag, int add )
+{
+   prolongateT( *H( h ), coarseLevel, coarse, fine, flag, add != 0 );
+}
+
+void orc_restrict( void* h, int fineLevel, const double* fine, double* coarse, int flag )
+{
+   restrictT( *H( h ), fineLevel, fine, coarse, flag );
+}
+
+double orc_dot( void* h, int level, const double* a, const double* b, int flag )
+{
+   return dotT( H( h )->lv[level], a, b, flag );
+}
+
+int orc_cg( void* h, int op, int level, double* x, const double* b, double tol, int maxIter )
+{
+   auto* o = H( h );
+   return cgT( *o, o->ops[op], o->lv[level], x, b, tol, maxIter );
+}
+
+int orc_gmg_solve( void* h, int op, int minLevel, int maxLevel, double* x, const double* b, int pre, int post,
+                   double relax, int smoother, const int* labels, int m, double coarseTol, int maxCycles, double relTol,
+                   int precision, double* history )
+{
+   auto* o = H( h );
+   GmgCfg g{ op, minLevel, maxLevel, pre, post, smoother, m, relax, coarseTol, labels };
+   const Op& A = o->ops[op];
+   const Level& lv = o->lv[maxLevel];
+   const int flag  = ORC_INNER | ORC_NEUMANN;
+   std::vector< double > r( lv.nDof );
+   double rel = relResidual( *o, A, maxLevel, x, b, r );
+   if ( history )
+      history[0] = rel;
+   int cyc = 0;
+   if ( precision == 64 )
+   {
+      Hier< double > hd;
+      allocHier( *o, hd, maxLevel );
+      hd.x[maxLevel].assign( x, x + lv.nDof );
+      hd.b[maxLevel].assign( b, b + lv.nDof );
+      while ( cyc < maxCycles && rel > relTol )
+      {
+         vcycleT( *o, g, hd, maxLevel );
+         hd.b[maxLevel].assign( b, b + lv.nDof ); // coarse levels of b are scratch; finest is restored
+         ++cyc;
+         rel = relResidual( *o, A, maxLevel, hd.x[maxLevel].data(), b, r );
+         if ( history )
+            history[cyc] = rel;
+      }
+      std::copy( hd.x[maxLevel].begin(), hd.x[maxLevel].end(), x );
+   }
+   else
+   {
+      // FP32 V-cycle on the residual equation inside FP64 iterative refinement
+      // (tests/hyteg/mixedPrecision/mixedPrecisionIterativeRefinement.cpp:162-171).
+      Hier< float > hf;
+      allocHier( *o, hf, maxLevel );
+      while ( cyc < maxCycles && rel > relTol )
+      {
+         for ( i64 d = 0; d < lv.nDof; ++d )
+         {
+            hf.b[maxLevel][d] = float( r[d] );
+            hf.x[maxLevel][d] = 0.0f;
+         }
+         vcycleT( *o, g, hf, maxLevel );
+         for ( i64 d = 0; d < lv.nDof; ++d )
+            if ( flagged( lv.bc[d], flag ) )
+               x[d] += double( hf.x[maxLevel][d] );
+         ++cyc;
+         rel = relResidual( *o, A, maxLevel, x, b, r );
+         if ( history )
+            history[cyc] = rel;
+      }
+   }
+   return cyc;
+}
+
+} // extern "C"

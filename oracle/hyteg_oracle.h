@@ -1,0 +1,69 @@
+// CPU oracle for the HyTeG P1 matrix-free geometric-multigrid path.
+//
+// TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference arm of bench.py may load this library, and only as
+// the checker or the timed CPU baseline. The product path never calls it.
+//
+// It is a plain, sequential-semantics restatement of the reference algorithm on
+// a global DoF vector (one value per micro-vertex). Every entry point cites the
+// reference function it follows (paths relative to the reference project root).
+//
+// Canonical DoF order of one level (shared with the product's upload/download):
+//   [macro-vertices in mesh order]
+//   [macro-edges (sorted vertex pairs, lexicographic), interior points i=1..N-1,
+//    i = micro-weight of the larger-id vertex]
+//   [macro-faces (sorted vertex triples, lexicographic), interior points (i,j),
+//    i/j = micro-weights of the 2nd/3rd vertex, j outer, i inner]
+//   [macro-cells in mesh order, interior points in tet-linear order (x fastest)]
+// with N = 2^level. This is the reference's per-primitive logical numbering
+// (src/hyteg/p1functionspace/VertexDoFIndexing.hpp, MeshInfo edge/face keys).
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// DoFType bit flags (src/hyteg/types/types.hpp:35-44)
+#define ORC_INNER 1
+#define ORC_DIRICHLET 2
+#define ORC_NEUMANN 4
+#define ORC_FREESLIP 8
+#define ORC_ALL 15
+
+void*   orc_create( const double* coords, int64_t nv, const int64_t* tets, int64_t nt, int maxLevel );
+void    orc_destroy( void* h );
+int64_t orc_num_dofs( void* h, int level );
+void    orc_dof_coords( void* h, int level, double* xyz );
+void    orc_dof_info( void* h, int level, uint8_t* kind, uint8_t* bc );
+// closure point (tet-linear index, reference cell layout) -> canonical DoF of one macro-cell
+void    orc_cell_closure_map( void* h, int level, int cell, int32_t* out );
+int64_t orc_num_prims( void* h, int kind );
+
+// operators: 0 = constant P1 Laplace; then div-k-grad with nodal k per level
+int  orc_op_laplace( void* h );
+int  orc_op_divkgrad( void* h, const double* const* nodalK );
+void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 );
+
+void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );
+void   orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag );
+void   orc_sor_colored( void* h, int op, int level, double* x, const double* b, double relax, int flag,
+                        const int* labels, int m );
+void   orc_jacobi( void* h, int op, int level, double* x, const double* b, double relax, int flag );
+void   orc_prolongate( void* h, int coarseLevel, const double* coarse, double* fine, int flag, int add );
+void   orc_restrict( void* h, int fineLevel, const double* fine, double* coarse, int flag );
+double orc_dot( void* h, int level, const double* a, const double* b, int flag );
+int    orc_cg( void* h, int op, int level, double* x, const double* b, double tol, int maxIter );
+
+// V-cycle GMG (src/hyteg/solvers/GeometricMultigridSolver.hpp:127-235).
+// smoother: 0 = reference-order SOR, 1 = multicolour SOR (labels, m), 2 = weighted Jacobi.
+// precision: 64 = plain FP64 cycles; 32 = FP32 inner V-cycles inside FP64 iterative refinement.
+// Runs until ||b-Ax||/||b|| <= relTol (Inner|Neumann DoFs) or maxCycles; history[k] =
+// relative residual after cycle k (history[0] = initial). Returns cycles done.
+int orc_gmg_solve( void* h, int op, int minLevel, int maxLevel, double* x, const double* b, int pre, int post,
+                   double relax, int smoother, const int* labels, int m, double coarseTol, int maxCycles,
+                   double relTol, int precision, double* history );
+
+#ifdef __cplusplus
+}
+#endif
