@@ -1,0 +1,338 @@
+"""Benchmark: time to relative residual 1e-8 and DoF-updates/s of the P1 geometric-
+multigrid solve on one B200, FP32-inner/FP64-refinement (mixed) against plain FP64.
+
+Workload (the reference configuration the metric is quoted on): Poisson -lap(u) = f
+on the unit cube split into a 2x2x2 macro-cube mesh (48 macro-tets), refinement
+level 7 (16.97M micro-vertices), Dirichlet u = 0, f ~ U[-1,1] per micro-vertex
+(seed 0), zero initial guess, V(3,3) cycles with SOR (omega = 1) and an FP64 CG
+coarse solve on level 0, each solve run to ||f - Au|| / ||f|| <= 1e-8.
+
+A step is one full solve from the zero initial guess with f resident in HBM. Each
+FP64 vector of the finest level is 140 MB, larger than the 126 MB L2, so no L2 flush
+is needed between steps. Under torchrun every rank solves its own replica of the
+problem (the path has no exchange step on one mesh: replicas only); the time is the
+maximum over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "hyteg-vara_b200")
+sys.path.insert(0, os.path.join(PKG, "python"))
+sys.path.insert(0, PKG)
+
+METRIC = "MG time-to-1e-8 & DoF-updates/s, mixed vs FP64 on 1 B200; p50/p99 solve latency"
+UNIT = "DoF-updates/s"
+TOL = 1e-8
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        except Exception:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import build as B
+    import hyb_inputs as I
+    import hyteg_b200 as H
+
+    B.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    L, nc = args.level, args.cubes
+
+    st = H.PrimitiveStorage.cuboid(nc, nc, nc, L)
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, coarse_tol=1e-12)
+    xyz = st.dof_coords(L)
+    f = I.uniform_rhs(xyz, 0, nc << L)
+    ndof = st.num_dofs(L)
+    u, b = H.P1Function("u", st, 0, L), H.P1Function("f", st, 0, L)
+    b.set(f, L, stream=sh)
+    m_col, _ = st.colouring()
+    # interior (non-Dirichlet) DoFs: the unknowns each V-cycle updates
+    mask = H.P1Function("mask", st, 0, L)
+    mask.interpolate(1.0, L, flag=H.INNER | H.NEUMANN)
+    n_unknowns = int(round(mask.dot_global(mask, L, H.INNER | H.NEUMANN)))
+    del mask
+
+    def solve(precision):
+        u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+        return gmg.solve_to_tolerance(u, b, L, TOL, max_cycles=60, precision=precision, stream=sh)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = [fn() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1)), out
+
+    for _ in range(args.warmup):
+        solve(32)
+        solve(64)
+    # headline: mixed precision solves, inputs resident
+    with Clocks(local_rank) as clk:
+        k0 = H.kernel_launch_count()
+        t_mixed, hist_mixed = timed(lambda: solve(32), args.steps)
+        launches = H.kernel_launch_count() - k0
+    clocks = clk.summary()
+    t_fp64, hist_fp64 = timed(lambda: solve(64), args.steps)
+    cyc_mixed = [len(h) - 1 for h in hist_mixed]
+    cyc_fp64 = [len(h) - 1 for h in hist_fp64]
+    ms_mixed = t_mixed / args.steps
+    ms_fp64 = t_fp64 / args.steps
+    value = world * n_unknowns * sum(cyc_mixed) / (t_mixed / 1e3)
+
+    # error of the mixed solution against a tightly converged FP64 solve of the same system
+    solve(32)
+    u_mixed = u.get(L, stream=sh)
+    u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+    gmg.solve_to_tolerance(u, b, L, 1e-13, max_cycles=80, precision=64, stream=sh)
+    u_ref = u.get(L, stream=sh)
+    err_mixed = float(np.abs(u_mixed - u_ref).max() / np.abs(u_ref).max())
+
+    # end to end through the C ABI with host buffers: H2D of f, solve, D2H of u
+    f_host = torch.from_numpy(f).pin_memory()
+    u_host = torch.empty(ndof, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        b.set_host_ptr(f_host.data_ptr(), L, stream=sh)
+        solve(32)
+        u.get_host_ptr(u_host.data_ptr(), L, stream=sh)
+
+    t_e2e, _ = timed(e2e_step, args.steps)
+    e2e = {"value": world * n_unknowns * sum(cyc_mixed) / args.steps * args.steps / (t_e2e / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8, "ms_per_step": t_e2e / args.steps}
+
+    # kernel rooflines (CUDA events on the launching stream, 20 launches each)
+    peak, peak_kind = peaks()
+
+    def kernel_time(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    y = H.P1Function("y", st, L, L)
+    t_apply = kernel_time(lambda: A.apply(b, y, L, H.INNER | H.NEUMANN, stream=sh))
+    t_sor = kernel_time(lambda: A.smooth_sor(u, b, 1.0, L, H.INNER | H.NEUMANN, stream=sh))
+    u32, b32 = H.P1Function("u32", st, L, L, H.F32), H.P1Function("b32", st, L, L, H.F32)
+    b32.copy_from(b, L, stream=sh)
+    t_sor32 = kernel_time(lambda: A.smooth_sor(u32, b32, 1.0, L, H.INNER | H.NEUMANN, stream=sh))
+    # algorithmic bytes: apply reads src and writes dst (16 B/DoF); an SOR sweep reads rhs,
+    # reads and writes u (24 B/DoF FP64, 12 B/DoF FP32)
+    apply_gbs = ndof * 16 / t_apply / 1e9
+    sor_gbs = ndof * 24 / t_sor / 1e9
+    sor32_gbs = ndof * 12 / t_sor32 / 1e9
+
+    def roof(a, t_bytes=None):
+        return {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 3),
+                "peak_source": peak_kind, "traffic": t_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 V-cycles in f64 refinement", "data": "synthetic",
+            "config": {"workload": f"Poisson, {nc}x{nc}x{nc} cuboid ({6 * nc ** 3} macro-tets), level {L}, "
+                                   f"V(3,3) multicolour SOR w=1, FP64 CG coarse on level 0, to rel. residual 1e-8",
+                       "dofs": ndof, "unknowns": n_unknowns, "colours": {"interface": m_col, "interior": 4},
+                       "l2": "inputs larger than L2 (FP64 finest vector 140 MB > 126 MB)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "time_to_tol_ms": {"mixed": ms_mixed, "fp64": ms_fp64},
+            "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
+            "cycles": {"mixed": cyc_mixed[-1], "fp64": cyc_fp64[-1]},
+            "final_rel_residual": {"mixed": float(hist_mixed[-1][-1]), "fp64": float(hist_fp64[-1][-1])},
+            "error_mixed_vs_fp64_solution": err_mixed,
+            "dof_updates_per_s_fp64": world * n_unknowns * sum(cyc_fp64) / (t_fp64 / 1e3),
+            "roofline": dict(roof(sor_gbs), kernel="k_sor (one FP64 multicolour SOR sweep, level 7)",
+                             ms=t_sor * 1e3),
+            "roofline_apply": dict(roof(apply_gbs), kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
+            "roofline_sor_fp32": dict(roof(sor32_gbs), kernel="k_sor (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args, steps=1):
+    """The CPU oracle (a restatement of the reference's algorithm) on the host cores:
+    FP64 V(3,3) cycles with the reference's SOR ordering on the same problem."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    c, t = O.mesh_cuboid(args.cubes, args.cubes, args.cubes)
+    orc = O.Oracle(c, t, args.level)
+    L = args.level
+    b = O.uniform_rhs(orc.coords_of(L), 0, args.cubes << L)
+    kind, bc = orc.info(L)
+    n_unknowns = int(np.sum((bc & (O.INNER | O.NEUMANN)) != 0))
+    x = np.zeros(orc.n(L))
+    t0 = time.perf_counter()
+    orc.gmg(x, b, 0, L, smoother=0, max_cycles=steps)
+    dt = time.perf_counter() - t0
+    return {"value": n_unknowns * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} FP64 V(3,3) cycle(s) at level {L} on the {6 * args.cubes ** 3}-tet mesh, "
+                      f"reference SOR ordering, {dt:.2f} s"}
+
+
+def reference(args, rank, world):
+    """The reference's algorithm on the host CPU (oracle port; the reference itself cannot be
+    built here: its waLBerla and Eigen submodules and MPI are absent). Each step is one FP64
+    V(3,3) cycle of the workload."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    c, t = O.mesh_cuboid(args.cubes, args.cubes, args.cubes)
+    L = args.level
+    orc = O.Oracle(c, t, L)
+    b = O.uniform_rhs(orc.coords_of(L), 0, args.cubes << L)
+    kind, bc = orc.info(L)
+    n_unknowns = int(np.sum((bc & (O.INNER | O.NEUMANN)) != 0))
+    x = np.zeros(orc.n(L))
+    for _ in range(args.warmup):
+        orc.gmg(x, b, 0, L, smoother=0, max_cycles=1)
+    x[:] = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.gmg(x, b, 0, L, smoother=0, max_cycles=1)
+    dt = time.perf_counter() - t0
+    value = n_unknowns * args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"Poisson, {args.cubes}^3 cuboid ({6 * args.cubes ** 3} macro-tets), level {L}, "
+                                   f"one FP64 V(3,3) cycle per step, reference SOR ordering"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} V-cycles at level {L}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--level", type=int, default=7)
+    ap.add_argument("--cubes", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference(args, rank, world)
+    else:
+        ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1535 @@
+// Host engine and C ABI of the B200 P1 multigrid path (declarations and the
+// reference interface each entry point replaces: include/hyteg_b200.h).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hyteg_b200.h"
+#include "hyb_kernels.cuh"
+#include "topology.hpp"
+
+namespace hyb {
+
+thread_local std::string g_lastError;
+
+struct Error : std::runtime_error
+{
+   int code;
+   Error( int c, const std::string& m ) : std::runtime_error( m ), code( c ) {}
+};
+
+#define HYB_CUDA( call )                                                                                              \
+   do                                                                                                                 \
+   {                                                                                                                  \
+      cudaError_t e_ = ( call );                                                                                      \
+      if ( e_ != cudaSuccess )                                                                                        \
+         throw Error( e_ == cudaErrorMemoryAllocation ? HYB_ENOMEM : HYB_EDEVICE,                                     \
+                      std::string( #call ) + ": " + cudaGetErrorString( e_ ) );                                       \
+   } while ( 0 )
+
+// Kernels enqueued by this library (graph replays add the kernel nodes they hold).
+std::atomic< long long > g_launches{ 0 };
+
+#define HYB_CHECK_LAUNCH()                                                                                            \
+   do                                                                                                                 \
+   {                                                                                                                  \
+      HYB_CUDA( cudaGetLastError() );                                                                                 \
+      g_launches.fetch_add( 1, std::memory_order_relaxed );                                                          \
+   } while ( 0 )
+
+inline void require( bool c, const std::string& msg )
+{
+   if ( !c )
+      throw Error( HYB_EINVAL, msg );
+}
+
+template < typename T >
+struct DevBuf
+{
+   T*     p = nullptr;
+   size_t n = 0;
+   DevBuf() = default;
+   DevBuf( const DevBuf& ) = delete;
+   DevBuf& operator=( const DevBuf& ) = delete;
+   ~DevBuf() { release(); }
+   void release()
+   {
+      if ( p )
+         cudaFree( p );
+      p = nullptr;
+      n = 0;
+   }
+   void alloc( size_t count )
+   {
+      release();
+      if ( count == 0 )
+         count = 1;
+      HYB_CUDA( cudaMalloc( &p, count * sizeof( T ) ) );
+      n = count;
+   }
+   void upload( const std::vector< T >& v )
+   {
+      alloc( v.size() );
+      if ( !v.empty() )
+         HYB_CUDA( cudaMemcpy( p, v.data(), v.size() * sizeof( T ), cudaMemcpyHostToDevice ) );
+   }
+};
+
+inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s ); }
+
+// ---------------------------------------------------------------------------
+// Storage
+// ---------------------------------------------------------------------------
+struct LevelHost
+{
+   LevelDev          dev{};
+   DevBuf< int32_t > seg, sorSeg, xyz;
+   int               blocksPerCell = 0, sorBlocksPerCell = 0;
+   int               slabBlocks    = 0; // blocks of 256 over one closure
+};
+
+struct Storage
+{
+   Topology                              topo;
+   int                                   maxLevel = 0;
+   DevBuf< ClassDev >                    cls;
+   DevBuf< int32_t >                     fEmb, eEmbOff, eEmb, vEmbOff, vEmb;
+   DevBuf< uint8_t >                     fBc, eBc, vBc;
+   DevBuf< int8_t >                      labels;
+   TopoDev                               td{};
+   std::vector< std::unique_ptr< LevelHost > > lv;
+   DevBuf< double >                      partial; // dot-product partials
+   DevBuf< double >                      scalars; // device scalars (dot results)
+   double*                               hostScalar = nullptr;
+   DevBuf< char >                        staging; // canonical-order transfer buffer (grow-only)
+
+   char* stage( size_t bytes )
+   {
+      if ( staging.n < bytes )
+      {
+         HYB_CUDA( cudaDeviceSynchronize() ); // the old buffer may still be in use by queued copies
+         staging.alloc( bytes );
+      }
+      return staging.p;
+   }
+
+   ~Storage()
+   {
+      if ( hostScalar )
+         cudaFreeHost( hostScalar );
+   }
+
+   const LevelHost& L( int l ) const { return *lv.at( l ); }
+};
+
+inline int stridePad( int s ) { return ( s + 31 ) / 32 * 32; }
+
+void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, const std::vector< std::array< int, 4 > >& T,
+                   int maxLevel )
+{
+   require( maxLevel >= 0 && maxLevel <= 9, "max_level must be in [0, 9]" );
+   require( !T.empty(), "mesh has no tetrahedra" );
+   s.maxLevel = maxLevel;
+   s.topo.build( V, T );
+   s.topo.computeColouring();
+   auto& tp = s.topo;
+   const int nC = int( tp.T.size() ), nF = int( tp.F.size() ), nE = int( tp.E.size() ), nV = int( tp.V.size() );
+   require( nC < ( 1 << 24 ), "too many macro-cells for the packed embedding format" );
+   // class table
+   std::vector< ClassDev > cls( size_t( nC ) * 16 );
+   for ( int c = 0; c < nC; ++c )
+      for ( int m = 0; m < 16; ++m )
+      {
+         const auto& ci = tp.cls[c][m];
+         ClassDev    d{};
+         d.id    = ci.id;
+         d.kind  = uint8_t( ci.kind < 0 ? 255 : ci.kind );
+         d.bc    = ci.bc;
+         d.owned = ci.owned ? 1 : 0;
+         d.invN  = ci.ncells > 0 ? 1.0f / float( ci.ncells ) : 0.0f;
+         // local vertex indices of the primitive's sorted vertices in this cell
+         std::vector< std::pair< int, int > > vs;
+         for ( int k = 0; k < 4; ++k )
+            if ( !( m & ( 1 << k ) ) )
+               vs.push_back( { tp.T[c][k], k } );
+         std::sort( vs.begin(), vs.end() );
+         d.k0 = vs.size() > 0 ? uint8_t( vs[0].second ) : 0;
+         d.k1 = vs.size() > 1 ? uint8_t( vs[1].second ) : 0;
+         d.k2 = vs.size() > 2 ? uint8_t( vs[2].second ) : 0;
+         cls[size_t( c ) * 16 + m] = d;
+      }
+   s.cls.upload( cls );
+   std::vector< int32_t > fEmb( size_t( nF ) * 2, -1 );
+   for ( int f = 0; f < nF; ++f )
+      for ( size_t e = 0; e < tp.fEmb[f].size(); ++e )
+         fEmb[2 * f + e] = packEmbedding( tp.fEmb[f][e] );
+   auto csr = []( const std::vector< std::vector< Embedding > >& emb, std::vector< int32_t >& off, std::vector< int32_t >& val ) {
+      off.assign( emb.size() + 1, 0 );
+      val.clear();
+      for ( size_t i = 0; i < emb.size(); ++i )
+      {
+         for ( auto& e : emb[i] )
+            val.push_back( packEmbedding( e ) );
+         off[i + 1] = int32_t( val.size() );
+      }
+   };
+   std::vector< int32_t > eOff, eVal, vOff, vVal;
+   csr( tp.eEmb, eOff, eVal );
+   csr( tp.vEmb, vOff, vVal );
+   s.fEmb.upload( fEmb );
+   s.eEmbOff.upload( eOff );
+   s.eEmb.upload( eVal );
+   s.vEmbOff.upload( vOff );
+   s.vEmb.upload( vVal );
+   s.fBc.upload( tp.fBc );
+   s.eBc.upload( tp.eBc );
+   s.vBc.upload( tp.vBc );
+   std::vector< int8_t > lab( size_t( nC ) * 4 );
+   for ( int c = 0; c < nC; ++c )
+      for ( int k = 0; k < 4; ++k )
+         lab[4 * c + k] = int8_t( tp.labels[tp.T[c][k]] );
+   s.labels.upload( lab );
+   s.td = TopoDev{ nC, nF, nE, nV, s.cls.p, s.fEmb.p, s.eEmbOff.p, s.eEmb.p, s.vEmbOff.p, s.vEmb.p,
+                   s.fBc.p, s.eBc.p, s.vBc.p, s.labels.p, tp.colours };
+   // per-level tables
+   size_t maxPartial = 1;
+   for ( int l = 0; l <= maxLevel; ++l )
+   {
+      auto      lh = std::make_unique< LevelHost >();
+      LevelDev& d  = lh->dev;
+      d.L          = l;
+      d.N          = 1 << l;
+      d.W          = d.N + 1;
+      d.S          = tetSize( d.W );
+      d.stride     = stridePad( d.S );
+      d.nIntFace   = d.N >= 3 ? ( d.N - 1 ) * ( d.N - 2 ) / 2 : 0;
+      d.nIntCell   = d.N >= 4 ? tetSize( d.N - 3 ) : 0;
+      d.nBdry      = nV + nE * ( d.N - 1 ) + nF * d.nIntFace;
+      std::vector< int32_t > seg, sorSeg, xyz( d.S );
+      for ( int z = 1; z <= d.N; ++z )
+         for ( int y = 1; y <= d.N - z; ++y )
+         {
+            const int len = d.N - 1 - y - z; // interior x in [1, len]
+            if ( len < 1 )
+               continue;
+            for ( int x0 = 1; x0 <= len; x0 += 32 )
+               seg.push_back( z | ( y << 10 ) | ( x0 << 20 ) );
+            const int groups = ( len + kInteriorColours - 1 ) / kInteriorColours;
+            for ( int g0 = 0; g0 < groups; g0 += 32 )
+               sorSeg.push_back( z | ( y << 10 ) | ( g0 << 20 ) );
+         }
+      for ( int z = 0; z <= d.N; ++z )
+         for ( int y = 0; y <= d.N - z; ++y )
+            for ( int x = 0; x <= d.N - y - z; ++x )
+               xyz[cidx( d.W, x, y, z )] = x | ( y << 10 ) | ( z << 20 );
+      lh->seg.upload( seg );
+      lh->sorSeg.upload( sorSeg );
+      lh->xyz.upload( xyz );
+      d.nSeg               = int( seg.size() );
+      d.nSorSeg            = int( sorSeg.size() );
+      d.seg                = lh->seg.p;
+      d.sorSeg             = lh->sorSeg.p;
+      d.xyz                = lh->xyz.p;
+      lh->blocksPerCell    = ( d.nSeg + kCellWarps - 1 ) / kCellWarps;
+      lh->sorBlocksPerCell = ( d.nSorSeg + kCellWarps - 1 ) / kCellWarps;
+      lh->slabBlocks       = ( d.S + 255 ) / 256;
+      maxPartial           = std::max( maxPartial, size_t( lh->slabBlocks ) * nC );
+      s.lv.push_back( std::move( lh ) );
+   }
+   s.partial.alloc( maxPartial );
+   s.scalars.alloc( 64 );
+   HYB_CUDA( cudaMallocHost( &s.hostScalar, 64 * sizeof( double ) ) );
+}
+
+// ---------------------------------------------------------------------------
+// Functions
+// ---------------------------------------------------------------------------
+struct Function
+{
+   Storage*            st;
+   int                 minL, maxL, dtype;
+   std::vector< void* > data; // per level, index l - minL
+
+   ~Function()
+   {
+      for ( void* p : data )
+         if ( p )
+            cudaFree( p );
+   }
+   size_t elem() const { return dtype == HYB_F64 ? 8 : 4; }
+   void*  at( int l ) const
+   {
+      require( l >= minL && l <= maxL, "level " + std::to_string( l ) + " outside the function's level range" );
+      return data[l - minL];
+   }
+   template < typename T >
+   T* ptr( int l ) const
+   {
+      return static_cast< T* >( at( l ) );
+   }
+   size_t levelBytes( int l ) const { return size_t( st->td.nC ) * st->L( l ).dev.stride * elem(); }
+};
+
+Function* makeFunction( Storage* s, int minL, int maxL, int dtype )
+{
+   require( minL >= 0 && minL <= maxL && maxL <= s->maxLevel, "invalid level range" );
+   require( dtype == HYB_F64 || dtype == HYB_F32, "dtype must be HYB_F64 or HYB_F32" );
+   auto f = std::make_unique< Function >();
+   f->st = s;
+   f->minL = minL;
+   f->maxL = maxL;
+   f->dtype = dtype;
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      void* p = nullptr;
+      HYB_CUDA( cudaMalloc( &p, f->levelBytes( l ) ) );
+      f->data.push_back( p );
+      HYB_CUDA( cudaMemset( p, 0, f->levelBytes( l ) ) );
+   }
+   return f.release();
+}
+
+// ---------------------------------------------------------------------------
+// Operators
+// ---------------------------------------------------------------------------
+namespace {
+const int kMicro[6][4][3] = {
+    { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
+    { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
+    { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
+
+// P1 stiffness  K_ij = |T| grad(phi_i).grad(phi_j)  of a tetrahedron
+void stiffness( const double X[4][3], double K[4][4] )
+{
+   double J[3][3];
+   for ( int r = 0; r < 3; ++r )
+      for ( int c = 0; c < 3; ++c )
+         J[r][c] = X[c + 1][r] - X[0][r];
+   const double det = J[0][0] * ( J[1][1] * J[2][2] - J[1][2] * J[2][1] ) - J[0][1] * ( J[1][0] * J[2][2] - J[1][2] * J[2][0] ) +
+                      J[0][2] * ( J[1][0] * J[2][1] - J[1][1] * J[2][0] );
+   require( std::fabs( det ) > 0, "degenerate macro-cell" );
+   // rows of J^-1 are the gradients of the barycentric coordinates 1..3
+   double g[4][3];
+   g[1][0] = ( J[1][1] * J[2][2] - J[1][2] * J[2][1] ) / det;
+   g[1][1] = ( J[0][2] * J[2][1] - J[0][1] * J[2][2] ) / det;
+   g[1][2] = ( J[0][1] * J[1][2] - J[0][2] * J[1][1] ) / det;
+   g[2][0] = ( J[1][2] * J[2][0] - J[1][0] * J[2][2] ) / det;
+   g[2][1] = ( J[0][0] * J[2][2] - J[0][2] * J[2][0] ) / det;
+   g[2][2] = ( J[0][2] * J[1][0] - J[0][0] * J[1][2] ) / det;
+   g[3][0] = ( J[1][0] * J[2][1] - J[1][1] * J[2][0] ) / det;
+   g[3][1] = ( J[0][1] * J[2][0] - J[0][0] * J[2][1] ) / det;
+   g[3][2] = ( J[0][0] * J[1][1] - J[0][1] * J[1][0] ) / det;
+   for ( int d = 0; d < 3; ++d )
+      g[0][d] = -g[1][d] - g[2][d] - g[3][d];
+   const double vol = std::fabs( det ) / 6.0;
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j )
+         K[i][j] = vol * ( g[i][0] * g[j][0] + g[i][1] * g[j][1] + g[i][2] * g[j][2] );
+}
+
+// element matrices of the six micro-tet shapes of a macro-cell at level L
+void microMatrices( const Topology& tp, int c, int N, double K[6][4][4] )
+{
+   const auto& t = tp.T[c];
+   for ( int ty = 0; ty < 6; ++ty )
+   {
+      double X[4][3];
+      for ( int j = 0; j < 4; ++j )
+         for ( int d = 0; d < 3; ++d )
+         {
+            const double v0 = tp.V[t[0]][d];
+            X[j][d] = v0 + ( tp.V[t[1]][d] - v0 ) / N * kMicro[ty][j][0] + ( tp.V[t[2]][d] - v0 ) / N * kMicro[ty][j][1] +
+                      ( tp.V[t[3]][d] - v0 ) / N * kMicro[ty][j][2];
+         }
+      stiffness( X, K[ty] );
+   }
+}
+
+bool tetAllowed( int mask, const IncidentTet& it )
+{
+   for ( int j = 0; j < 4; ++j )
+   {
+      const int q = it.q[j];
+      const int x = offX( q ), y = offY( q ), z = offZ( q );
+      if ( ( mask & 1 ) && -( x + y + z ) < 0 )
+         return false;
+      if ( ( mask & 2 ) && x < 0 )
+         return false;
+      if ( ( mask & 4 ) && y < 0 )
+         return false;
+      if ( ( mask & 8 ) && z < 0 )
+         return false;
+   }
+   return true;
+}
+} // namespace
+
+struct Operator
+{
+   Storage* st;
+   int      minL, maxL;
+   bool     variable = false;
+   // per level (index l - minL)
+   std::vector< std::unique_ptr< DevBuf< double > > > st64, K64;
+   std::vector< std::unique_ptr< DevBuf< float > > >  st32, K32;
+   std::vector< std::vector< double > >               stHost; // [nC*16*15]
+   std::unique_ptr< Function >                        kap64, kap32;
+
+   template < typename T >
+   OpDev< T > dev( int l ) const
+   {
+      require( l >= minL && l <= maxL, "level outside the operator's level range" );
+      OpDev< T > o{};
+      const int  i = l - minL;
+      if constexpr ( std::is_same< T, double >::value )
+      {
+         o.st = variable ? nullptr : st64[i]->p;
+         o.K  = variable ? K64[i]->p : nullptr;
+         o.kap = variable ? kap64->ptr< double >( l ) : nullptr;
+      }
+      else
+      {
+         o.st = variable ? nullptr : st32[i]->p;
+         o.K  = variable ? K32[i]->p : nullptr;
+         o.kap = variable ? kap32->ptr< float >( l ) : nullptr;
+      }
+      o.stride = st->L( l ).dev.stride;
+      return o;
+   }
+};
+
+Operator* makeLaplace( Storage* s, int minL, int maxL )
+{
+   require( minL >= 0 && minL <= maxL && maxL <= s->maxLevel, "invalid level range" );
+   auto op = std::make_unique< Operator >();
+   op->st = s;
+   op->minL = minL;
+   op->maxL = maxL;
+   const int nC = s->td.nC;
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      std::vector< double > st( size_t( nC ) * 16 * 15, 0.0 );
+      for ( int c = 0; c < nC; ++c )
+      {
+         double K[6][4][4];
+         microMatrices( s->topo, c, 1 << l, K );
+         // partial stencil of each class = sum over the incident micro-tets inside the closure
+         // (P1Elements.hpp:215-302, 464-526)
+         for ( int mask = 0; mask < 16; ++mask )
+            for ( int i = 0; i < 24; ++i )
+            {
+               const IncidentTet it = incidentTet( i );
+               if ( !tetAllowed( mask, it ) )
+                  continue;
+               for ( int j = 0; j < 4; ++j )
+                  st[( size_t( c ) * 16 + mask ) * 15 + it.q[j]] += K[it.t][it.k][j];
+            }
+      }
+      auto b64 = std::make_unique< DevBuf< double > >();
+      b64->upload( st );
+      std::vector< float > f( st.begin(), st.end() );
+      auto b32 = std::make_unique< DevBuf< float > >();
+      b32->upload( f );
+      op->st64.push_back( std::move( b64 ) );
+      op->st32.push_back( std::move( b32 ) );
+      op->stHost.push_back( std::move( st ) );
+   }
+   return op.release();
+}
+
+template < typename T >
+void launchFromDofs( const Storage& s, int l, T* slab, const T* dofs, cudaStream_t stream );
+
+Operator* makeDivKGrad( Storage* s, int minL, int maxL, const std::vector< std::vector< double > >& nodalK )
+{
+   require( minL >= 0 && minL <= maxL && maxL <= s->maxLevel, "invalid level range" );
+   require( int( nodalK.size() ) == maxL - minL + 1, "one nodal coefficient vector per level is required" );
+   auto op = std::make_unique< Operator >();
+   op->st = s;
+   op->minL = minL;
+   op->maxL = maxL;
+   op->variable = true;
+   op->kap64.reset( makeFunction( s, minL, maxL, HYB_F64 ) );
+   op->kap32.reset( makeFunction( s, minL, maxL, HYB_F32 ) );
+   const int nC = s->td.nC;
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      // micro-tet matrices with the 1/4 of the vertex average folded in: the reference form's
+      // 5-point degree-3 rule integrates the P1 interpolant of k exactly, giving
+      // A_e = mean_e(k) * K_e (p1_div_k_grad_affine_q3.cpp:179+)
+      std::vector< double > Km( size_t( nC ) * 96 );
+      for ( int c = 0; c < nC; ++c )
+      {
+         double K[6][4][4];
+         microMatrices( s->topo, c, 1 << l, K );
+         for ( int t = 0; t < 6; ++t )
+            for ( int i = 0; i < 4; ++i )
+               for ( int j = 0; j < 4; ++j )
+                  Km[size_t( c ) * 96 + t * 16 + i * 4 + j] = 0.25 * K[t][i][j];
+      }
+      auto b64 = std::make_unique< DevBuf< double > >();
+      b64->upload( Km );
+      std::vector< float > f( Km.begin(), Km.end() );
+      auto b32 = std::make_unique< DevBuf< float > >();
+      b32->upload( f );
+      op->K64.push_back( std::move( b64 ) );
+      op->K32.push_back( std::move( b32 ) );
+      const auto& kv = nodalK[l - minL];
+      require( int64_t( kv.size() ) == s->topo.numDofs( l ), "nodal coefficient vector has the wrong length" );
+      DevBuf< double > tmp;
+      tmp.upload( kv );
+      launchFromDofs< double >( *s, l, op->kap64->ptr< double >( l ), tmp.p, 0 );
+      const int n = s->td.nC * s->L( l ).dev.stride;
+      k_convert< float, double ><<< ( n + 255 ) / 256, 256 >>>( s->L( l ).dev, op->kap32->ptr< float >( l ),
+                                                                 op->kap64->ptr< double >( l ), s->td.nC );
+      HYB_CHECK_LAUNCH();
+      HYB_CUDA( cudaDeviceSynchronize() );
+   }
+   return op.release();
+}
+
+// Coordinates of every micro-vertex of a level in the canonical DoF order
+// (vertexdof::macrocell::coordinateFromIndex, VertexDoFMacroCell.hpp:68-75, and its
+// face/edge analogues), evaluated on the host.
+void dofCoords( const Topology& tp, int l, std::vector< double >& out )
+{
+   const int     N        = 1 << l;
+   const int64_t offE     = int64_t( tp.V.size() ), offF = offE + int64_t( tp.E.size() ) * ( N - 1 );
+   const int64_t nIntFace = N >= 3 ? ( N - 1 ) * ( N - 2 ) / 2 : 0;
+   const int64_t offC     = offF + int64_t( tp.F.size() ) * nIntFace;
+   const int64_t nIntCell = N >= 4 ? ( N - 3 ) * ( N - 2 ) * ( N - 1 ) / 6 : 0;
+   out.assign( size_t( tp.numDofs( l ) ) * 3, 0.0 );
+   auto put = [&]( int64_t d, const double* x ) {
+      for ( int k = 0; k < 3; ++k )
+         out[3 * d + k] = x[k];
+   };
+   double x[3];
+   for ( size_t v = 0; v < tp.V.size(); ++v )
+      put( int64_t( v ), tp.V[v].data() );
+   for ( size_t e = 0; e < tp.E.size(); ++e )
+      for ( int i = 1; i < N; ++i )
+      {
+         for ( int d = 0; d < 3; ++d )
+            x[d] = tp.V[tp.E[e][0]][d] + ( tp.V[tp.E[e][1]][d] - tp.V[tp.E[e][0]][d] ) / N * i;
+         put( offE + int64_t( e ) * ( N - 1 ) + ( i - 1 ), x );
+      }
+   for ( size_t f = 0; f < tp.F.size(); ++f )
+      for ( int j = 1; j <= N - 2; ++j )
+         for ( int i = 1; i <= N - 1 - j; ++i )
+         {
+            const auto& F = tp.F[f];
+            for ( int d = 0; d < 3; ++d )
+               x[d] = tp.V[F[0]][d] + ( tp.V[F[1]][d] - tp.V[F[0]][d] ) / N * i + ( tp.V[F[2]][d] - tp.V[F[0]][d] ) / N * j;
+            put( offF + int64_t( f ) * nIntFace + ( j - 1 ) * ( N - 1 ) - ( j - 1 ) * j / 2 + ( i - 1 ), x );
+         }
+   for ( size_t c = 0; c < tp.T.size(); ++c )
+      for ( int zz = 1; zz <= N; ++zz )
+         for ( int yy = 1; yy <= N - zz; ++yy )
+            for ( int xx = 1; xx <= N - 1 - yy - zz; ++xx )
+            {
+               const auto& t = tp.T[c];
+               for ( int d = 0; d < 3; ++d )
+               {
+                  const double v0 = tp.V[t[0]][d];
+                  x[d] = v0 + ( tp.V[t[1]][d] - v0 ) / N * xx + ( tp.V[t[2]][d] - v0 ) / N * yy + ( tp.V[t[3]][d] - v0 ) / N * zz;
+               }
+               put( offC + int64_t( c ) * nIntCell + cidx( N - 3, xx - 1, yy - 1, zz - 1 ), x );
+            }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+inline int bdryBlocks( const LevelDev& d ) { return ( d.nBdry + kBdryThreads - 1 ) / kBdryThreads; }
+
+template < typename T >
+void launchFromDofs( const Storage& s, int l, T* slab, const T* dofs, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   k_from_dofs< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, slab, dofs );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchToDofs( const Storage& s, int l, const T* slab, T* dofs, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   k_to_dofs< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, slab, dofs );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs, int flag, int mode, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.blocksPerCell * s.td.nC;
+   const int      nb = nc + bdryBlocks( L.dev );
+   if ( nb == 0 )
+      return;
+   const OpDev< T > od = op.dev< T >( l );
+#define HYB_APPLY( VAR, MODE )                                                                                         \
+   k_apply< T, VAR, MODE ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, flag, nc, L.blocksPerCell )
+   if ( op.variable )
+   {
+      if ( mode == kReplace )
+         HYB_APPLY( true, kReplace );
+      else if ( mode == kAdd )
+         HYB_APPLY( true, kAdd );
+      else
+         HYB_APPLY( true, kResidual );
+   }
+   else
+   {
+      if ( mode == kReplace )
+         HYB_APPLY( false, kReplace );
+      else if ( mode == kAdd )
+         HYB_APPLY( false, kAdd );
+      else
+         HYB_APPLY( false, kResidual );
+   }
+#undef HYB_APPLY
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream )
+{
+   const Storage&   s  = *op.st;
+   const auto&      L  = s.L( l );
+   const int        nc = L.sorBlocksPerCell * s.td.nC;
+   const int        nbd = bdryBlocks( L.dev );
+   const OpDev< T > od = op.dev< T >( l );
+   // interface passes: boundary blocks only (nCellBlocks = 0)
+   if ( nbd > 0 )
+      for ( int c = 0; c < s.td.m; ++c )
+      {
+         if ( op.variable )
+            k_sor< T, true ><<< nbd, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, 0, 1 );
+         else
+            k_sor< T, false ><<< nbd, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, 0, 1 );
+         HYB_CHECK_LAUNCH();
+      }
+   // interior passes: cell blocks only (no boundary blocks follow them)
+   if ( nc > 0 )
+      for ( int c = 0; c < kInteriorColours; ++c )
+      {
+         if ( op.variable )
+            k_sor< T, true ><<< nc, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, nc, L.sorBlocksPerCell );
+         else
+            k_sor< T, false ><<< nc, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, nc, L.sorBlocksPerCell );
+         HYB_CHECK_LAUNCH();
+      }
+}
+
+template < typename T >
+void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs, T relax, int flag, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.blocksPerCell * s.td.nC;
+   const int      nb = nc + bdryBlocks( L.dev );
+   if ( nb == 0 )
+      return;
+   const OpDev< T > od = op.dev< T >( l );
+   if ( op.variable )
+      k_jacobi< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc, L.blocksPerCell );
+   else
+      k_jacobi< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc, L.blocksPerCell );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchProlongate( const Storage& s, int coarseL, const T* coarse, T* fine, int flag, bool add, cudaStream_t stream )
+{
+   const auto& F  = s.L( coarseL + 1 );
+   const auto& C  = s.L( coarseL );
+   const int   nc = F.blocksPerCell * s.td.nC;
+   const int   nb = nc + bdryBlocks( F.dev );
+   if ( nb == 0 )
+      return;
+   if ( add )
+      k_prolongate< T, true ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc,
+                                                          F.blocksPerCell );
+   else
+      k_prolongate< T, false ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc,
+                                                           F.blocksPerCell );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchRestrict( const Storage& s, int fineL, const T* fine, T* coarse, int flag, cudaStream_t stream )
+{
+   const auto& F  = s.L( fineL );
+   const auto& C  = s.L( fineL - 1 );
+   const int   nc = C.blocksPerCell * s.td.nC;
+   const int   nb = nc + bdryBlocks( C.dev );
+   if ( nb == 0 )
+      return;
+   k_restrict< T ><<< nb, 128, 0, stream >>>( s.td, C.dev, F.dev.W, F.dev.stride, fine, coarse, flag, nc, C.blocksPerCell );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchLincomb( const Storage& s, int l, T* dst, int n, const double* sc, const T* const* src, bool add, int flag,
+                    cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   k_lincomb< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>(
+       s.td, L.dev, dst, n, T( n > 0 ? sc[0] : 0 ), n > 0 ? src[0] : nullptr, T( n > 1 ? sc[1] : 0 ),
+       n > 1 ? src[1] : nullptr, T( n > 2 ? sc[2] : 0 ), n > 2 ? src[2] : nullptr, add ? 1 : 0, flag );
+   HYB_CHECK_LAUNCH();
+}
+
+// dot product into the device scalar slot `slot`
+template < typename T >
+void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, int slot, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   k_dot_partial< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, a, b, flag, s.partial.p );
+   HYB_CHECK_LAUNCH();
+   k_reduce_final<<< 1, 1024, 0, stream >>>( s.partial.p, L.slabBlocks * s.td.nC, s.scalars.p + slot );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename TD, typename TS >
+void launchConvert( const Storage& s, int l, TD* dst, const TS* src, cudaStream_t stream )
+{
+   const auto&  L = s.L( l );
+   const size_t n = size_t( s.td.nC ) * L.dev.stride;
+   k_convert< TD, TS ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, stream >>>( L.dev, dst, src, s.td.nC );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchAddCorrection( const Storage& s, int l, double* x, const T* e, int flag, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   k_add_correction< double, T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, x, e, flag );
+   HYB_CHECK_LAUNCH();
+}
+
+// Coarse CG in FP64 on device scratch (x, b given; r, p, ap scratch)
+struct CgScratch
+{
+   std::unique_ptr< Function > r, p, ap;
+   DevBuf< int >               status;
+};
+
+void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch& cs, double tol, int maxIter,
+               cudaStream_t stream )
+{
+   const Storage& s = *op.st;
+   if ( !cs.r || cs.r->minL > l || cs.r->maxL < l )
+   {
+      cs.r.reset( makeFunction( op.st, l, l, HYB_F64 ) );
+      cs.p.reset( makeFunction( op.st, l, l, HYB_F64 ) );
+      cs.ap.reset( makeFunction( op.st, l, l, HYB_F64 ) );
+      cs.status.alloc( 4 );
+   }
+   const OpDev< double > od = op.dev< double >( l );
+   if ( op.variable )
+      k_cg< true ><<< 1, 256, 0, stream >>>( s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
+                                             cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p );
+   else
+      k_cg< false ><<< 1, 256, 0, stream >>>( s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
+                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p );
+   HYB_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Geometric multigrid (GeometricMultigridSolver.hpp:136-235)
+// ---------------------------------------------------------------------------
+struct Gmg
+{
+   Storage*  st;
+   Operator* op;
+   int       minL, maxL, pre, post, smoother, coarseMaxIter;
+   double    relax, coarseTol;
+   std::unique_ptr< Function > tmp64;         // gmg_tmp
+   std::unique_ptr< Function > x32, b32, t32; // FP32 inner hierarchy (mixed precision)
+   std::unique_ptr< Function > r64;           // FP64 residual (mixed precision)
+   std::unique_ptr< Function > cx64, cb64;    // FP64 coarse-solve copies of the FP32 hierarchy
+   CgScratch                   cg;
+   cudaStream_t                cap = nullptr; // capture stream
+   // captured graphs keyed by (x, b, level, kind)
+   struct G
+   {
+      const void* x;
+      const void* b;
+      int         level, kind;
+      cudaGraphExec_t exec;
+      long long       kernels; // kernel launches captured in the graph
+   };
+   std::vector< G > graphs;
+
+   ~Gmg()
+   {
+      for ( auto& g : graphs )
+         cudaGraphExecDestroy( g.exec );
+      if ( cap )
+         cudaStreamDestroy( cap );
+   }
+};
+
+constexpr int kGmgFlag = HYB_INNER | HYB_NEUMANN;
+
+template < typename T >
+void smooth( Gmg& g, int l, T* x, const T* b, T* scratch, cudaStream_t stream )
+{
+   if ( g.smoother == HYB_SMOOTHER_SOR )
+      launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
+   else
+   {
+      // Jacobi needs the old iterate: scratch = x, then x = scratch + relax D^-1 (b - A scratch)
+      HYB_CUDA( cudaMemcpyAsync( scratch, x, size_t( g.st->td.nC ) * g.st->L( l ).dev.stride * sizeof( T ),
+                                 cudaMemcpyDeviceToDevice, stream ) );
+      launchJacobi< T >( *g.op, l, scratch, x, b, T( g.relax ), kGmgFlag, stream );
+   }
+}
+
+// coarse solve: FP64 CG; an FP32 hierarchy is solved through FP64 copies
+void coarseSolve( Gmg& g, double* x, const double* b, cudaStream_t stream )
+{
+   launchCg( *g.op, g.minL, x, b, g.cg, g.coarseTol, g.coarseMaxIter, stream );
+}
+void coarseSolve( Gmg& g, float* x, const float* b, cudaStream_t stream )
+{
+   const int l = g.minL;
+   launchConvert< double, float >( *g.st, l, g.cx64->ptr< double >( l ), x, stream );
+   launchConvert< double, float >( *g.st, l, g.cb64->ptr< double >( l ), b, stream );
+   launchCg( *g.op, l, g.cx64->ptr< double >( l ), g.cb64->ptr< double >( l ), g.cg, g.coarseTol, g.coarseMaxIter, stream );
+   launchConvert< float, double >( *g.st, l, x, g.cx64->ptr< double >( l ), stream );
+}
+
+template < typename T >
+void vcycle( Gmg& g, Function& x, Function& b, Function& tmp, int l, cudaStream_t stream )
+{
+   if ( l == g.minL )
+   {
+      coarseSolve( g, x.ptr< T >( l ), b.ptr< T >( l ), stream );
+      return;
+   }
+   for ( int i = 0; i < g.pre; ++i )
+      smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
+   // tmp = b - A x ; restricted straight into b on the coarser level (b.assign(tmp) on flag)
+   launchApply< T >( *g.op, l, x.ptr< T >( l ), tmp.ptr< T >( l ), b.ptr< T >( l ), kGmgFlag, kResidual, stream );
+   launchRestrict< T >( *g.st, l, tmp.ptr< T >( l ), b.ptr< T >( l - 1 ), kGmgFlag, stream );
+   HYB_CUDA( cudaMemsetAsync( x.ptr< T >( l - 1 ), 0, x.levelBytes( l - 1 ), stream ) ); // x.interpolate(0, l-1)
+   vcycle< T >( g, x, b, tmp, l - 1, stream );
+   launchProlongate< T >( *g.st, l - 1, x.ptr< T >( l - 1 ), x.ptr< T >( l ), kGmgFlag, true, stream );
+   for ( int i = 0; i < g.post; ++i )
+      smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
+}
+
+// Graph-captured work units.
+enum GraphKind : int
+{
+   kCycle64      = 0, // one FP64 V-cycle
+   kCycle64Norm  = 1, // FP64 V-cycle, then r = b - A x and ||r||^2 into scalar slot 0
+   kMixedStep    = 2, // FP32 V-cycle on A e = r (r from the previous step), x += e, new r and ||r||^2
+   kNorm64       = 3, // r = b - A x into gmg_tmp and ||r||^2
+   kNormMixed    = 4, // r = b - A x into the FP64 residual of the mixed solver and ||r||^2
+};
+
+void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s )
+{
+   if ( kind == kCycle64 || kind == kCycle64Norm )
+      vcycle< double >( g, x, b, *g.tmp64, l, s );
+   if ( kind == kMixedStep )
+   {
+      // FP32 V-cycle on the residual equation (mixedPrecisionIterativeRefinement.cpp:162-171)
+      launchConvert< float, double >( *g.st, l, g.b32->ptr< float >( l ), g.r64->ptr< double >( l ), s );
+      HYB_CUDA( cudaMemsetAsync( g.x32->ptr< float >( l ), 0, g.x32->levelBytes( l ), s ) );
+      vcycle< float >( g, *g.x32, *g.b32, *g.t32, l, s );
+      launchAddCorrection< float >( *g.st, l, x.ptr< double >( l ), g.x32->ptr< float >( l ), kGmgFlag, s );
+   }
+   if ( kind != kCycle64 )
+   {
+      Function& r = ( kind == kCycle64Norm || kind == kNorm64 ) ? *g.tmp64 : *g.r64;
+      launchApply< double >( *g.op, l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ), kGmgFlag, kResidual, s );
+      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, 0, s );
+   }
+}
+
+// everything a captured graph needs is allocated before capture begins
+void prepare( Gmg& g )
+{
+   if ( !g.cg.r )
+   {
+      g.cg.r.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
+      g.cg.p.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
+      g.cg.ap.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
+      g.cg.status.alloc( 4 );
+   }
+}
+
+void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t stream )
+{
+   for ( auto& G : g.graphs )
+      if ( G.x == &x && G.b == &b && G.level == l && G.kind == kind )
+      {
+         HYB_CUDA( cudaGraphLaunch( G.exec, stream ) );
+         g_launches.fetch_add( G.kernels, std::memory_order_relaxed );
+         return;
+      }
+   prepare( g );
+   if ( !g.cap )
+      HYB_CUDA( cudaStreamCreateWithFlags( &g.cap, cudaStreamNonBlocking ) );
+   // make the capture stream wait for prior work on the caller's stream
+   cudaEvent_t ev;
+   HYB_CUDA( cudaEventCreateWithFlags( &ev, cudaEventDisableTiming ) );
+   HYB_CUDA( cudaEventRecord( ev, stream ) );
+   HYB_CUDA( cudaStreamWaitEvent( g.cap, ev, 0 ) );
+   HYB_CUDA( cudaStreamSynchronize( g.cap ) );
+   HYB_CUDA( cudaEventDestroy( ev ) );
+   cudaGraph_t     graph = nullptr;
+   const long long before = g_launches.load();
+   HYB_CUDA( cudaStreamBeginCapture( g.cap, cudaStreamCaptureModeThreadLocal ) );
+   try
+   {
+      enqueue( g, x, b, l, kind, g.cap );
+   }
+   catch ( ... )
+   {
+      cudaStreamEndCapture( g.cap, &graph );
+      if ( graph )
+         cudaGraphDestroy( graph );
+      throw;
+   }
+   HYB_CUDA( cudaStreamEndCapture( g.cap, &graph ) );
+   const long long captured = g_launches.load() - before;
+   g_launches.fetch_sub( captured ); // counted when the graph runs
+   cudaGraphExec_t exec;
+   HYB_CUDA( cudaGraphInstantiate( &exec, graph, 0 ) );
+   HYB_CUDA( cudaGraphDestroy( graph ) );
+   g.graphs.push_back( { &x, &b, l, kind, exec, captured } );
+   HYB_CUDA( cudaGraphLaunch( exec, stream ) );
+   g_launches.fetch_add( captured );
+}
+
+} // namespace hyb
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace hyb;
+
+struct hyb_storage_s : Storage
+{};
+struct hyb_function_s : Function
+{};
+struct hyb_operator_s : Operator
+{};
+struct hyb_gmg_s : Gmg
+{};
+
+#define HYB_API_BEGIN try {
+#define HYB_API_END                                                                                                   \
+   return HYB_OK;                                                                                                     \
+   }                                                                                                                  \
+   catch ( const Error& e )                                                                                           \
+   {                                                                                                                  \
+      g_lastError = e.what();                                                                                         \
+      return e.code;                                                                                                  \
+   }                                                                                                                  \
+   catch ( const std::invalid_argument& e )                                                                           \
+   {                                                                                                                  \
+      g_lastError = e.what();                                                                                         \
+      return HYB_EINVAL;                                                                                              \
+   }                                                                                                                  \
+   catch ( const std::exception& e )                                                                                  \
+   {                                                                                                                  \
+      g_lastError = e.what();                                                                                         \
+      return HYB_EUNSUPPORTED;                                                                                        \
+   }
+
+static Storage*  ST( hyb_storage* s ) { return static_cast< Storage* >( s ); }
+static Function* FN( hyb_function* f ) { return static_cast< Function* >( f ); }
+static Operator* OP( hyb_operator* o ) { return static_cast< Operator* >( o ); }
+
+static void sameStorage( const Function* a, const Function* b )
+{
+   require( a && b && a->st == b->st, "functions belong to different storages" );
+}
+
+extern "C" {
+
+const char* hyb_last_error( void ) { return g_lastError.c_str(); }
+
+long long hyb_kernel_launch_count( void ) { return g_launches.load(); }
+
+int hyb_storage_create( const double* coords, int64_t nv, const int64_t* tets, int64_t nt, int maxLevel, hyb_storage** out )
+{
+   HYB_API_BEGIN
+   require( coords && tets && out && nv >= 4 && nt >= 1, "invalid mesh arguments" );
+   std::vector< std::array< double, 3 > > V( nv );
+   for ( int64_t i = 0; i < nv; ++i )
+      V[i] = { coords[3 * i], coords[3 * i + 1], coords[3 * i + 2] };
+   std::vector< std::array< int, 4 > > T( nt );
+   for ( int64_t i = 0; i < nt; ++i )
+      for ( int k = 0; k < 4; ++k )
+         T[i][k] = int( tets[4 * i + k] );
+   auto s = std::make_unique< hyb_storage_s >();
+   buildStorage( *s, V, T, maxLevel );
+   *out = s.release();
+   HYB_API_END
+}
+
+int hyb_storage_create_cuboid( int nx, int ny, int nz, const double* lo, const double* hi, int maxLevel, hyb_storage** out )
+{
+   HYB_API_BEGIN
+   require( lo && hi && out, "null argument" );
+   std::vector< std::array< double, 3 > > V;
+   std::vector< std::array< int, 4 > >    T;
+   meshCuboid( nx, ny, nz, lo, hi, V, T );
+   auto s = std::make_unique< hyb_storage_s >();
+   buildStorage( *s, V, T, maxLevel );
+   *out = s.release();
+   HYB_API_END
+}
+
+int hyb_storage_destroy( hyb_storage* s )
+{
+   HYB_API_BEGIN
+   delete static_cast< hyb_storage_s* >( s );
+   HYB_API_END
+}
+
+int hyb_storage_counts( const hyb_storage* s, int64_t* c )
+{
+   HYB_API_BEGIN
+   require( s && c, "null argument" );
+   const auto& tp = s->topo;
+   c[0] = int64_t( tp.V.size() );
+   c[1] = int64_t( tp.E.size() );
+   c[2] = int64_t( tp.F.size() );
+   c[3] = int64_t( tp.T.size() );
+   HYB_API_END
+}
+
+int64_t hyb_storage_num_dofs( const hyb_storage* s, int level )
+{
+   if ( !s || level < 0 || level > s->maxLevel )
+      return -1;
+   return s->topo.numDofs( level );
+}
+
+int hyb_storage_mesh( const hyb_storage* s, double* coords, int64_t* tets )
+{
+   HYB_API_BEGIN
+   require( s && coords && tets, "null argument" );
+   for ( size_t i = 0; i < s->topo.V.size(); ++i )
+      for ( int d = 0; d < 3; ++d )
+         coords[3 * i + d] = s->topo.V[i][d];
+   for ( size_t i = 0; i < s->topo.T.size(); ++i )
+      for ( int k = 0; k < 4; ++k )
+         tets[4 * i + k] = s->topo.T[i][k];
+   HYB_API_END
+}
+
+int hyb_storage_colouring( const hyb_storage* s, int* m, int* labels )
+{
+   HYB_API_BEGIN
+   require( s && m, "null argument" );
+   *m = s->topo.colours;
+   if ( labels )
+      std::copy( s->topo.labels.begin(), s->topo.labels.end(), labels );
+   HYB_API_END
+}
+
+int hyb_function_create( hyb_storage* s, int minL, int maxL, int dtype, hyb_function** out )
+{
+   HYB_API_BEGIN
+   require( s && out, "null argument" );
+   Function* f = makeFunction( ST( s ), minL, maxL, dtype );
+   // re-home into the ABI type (same layout, no extra members)
+   *out = reinterpret_cast< hyb_function* >( f );
+   HYB_API_END
+}
+
+int hyb_function_destroy( hyb_function* f )
+{
+   HYB_API_BEGIN
+   delete FN( f );
+   HYB_API_END
+}
+
+static void checkLevel( const Function* f, int l ) { (void) f->at( l ); }
+
+int hyb_function_upload( hyb_function* fh, int level, const void* host, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f && host, "null argument" );
+   checkLevel( f, level );
+   const size_t n   = size_t( f->st->topo.numDofs( level ) ) * f->elem();
+   char*        tmp = f->st->stage( n );
+   HYB_CUDA( cudaMemcpyAsync( tmp, host, n, cudaMemcpyHostToDevice, S( stream ) ) );
+   if ( f->dtype == HYB_F64 )
+      launchFromDofs< double >( *f->st, level, f->ptr< double >( level ), reinterpret_cast< double* >( tmp ), S( stream ) );
+   else
+      launchFromDofs< float >( *f->st, level, f->ptr< float >( level ), reinterpret_cast< float* >( tmp ), S( stream ) );
+   HYB_CUDA( cudaStreamSynchronize( S( stream ) ) );
+   HYB_API_END
+}
+
+int hyb_function_download( hyb_function* fh, int level, void* host, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f && host, "null argument" );
+   checkLevel( f, level );
+   const size_t n   = size_t( f->st->topo.numDofs( level ) ) * f->elem();
+   char*        tmp = f->st->stage( n );
+   if ( f->dtype == HYB_F64 )
+      launchToDofs< double >( *f->st, level, f->ptr< double >( level ), reinterpret_cast< double* >( tmp ), S( stream ) );
+   else
+      launchToDofs< float >( *f->st, level, f->ptr< float >( level ), reinterpret_cast< float* >( tmp ), S( stream ) );
+   HYB_CUDA( cudaMemcpyAsync( host, tmp, n, cudaMemcpyDeviceToHost, S( stream ) ) );
+   HYB_CUDA( cudaStreamSynchronize( S( stream ) ) );
+   HYB_API_END
+}
+
+int hyb_function_upload_device( hyb_function* fh, int level, const void* dev, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f && dev, "null argument" );
+   checkLevel( f, level );
+   if ( f->dtype == HYB_F64 )
+      launchFromDofs< double >( *f->st, level, f->ptr< double >( level ), static_cast< const double* >( dev ), S( stream ) );
+   else
+      launchFromDofs< float >( *f->st, level, f->ptr< float >( level ), static_cast< const float* >( dev ), S( stream ) );
+   HYB_API_END
+}
+
+int hyb_function_download_device( hyb_function* fh, int level, void* dev, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f && dev, "null argument" );
+   checkLevel( f, level );
+   if ( f->dtype == HYB_F64 )
+      launchToDofs< double >( *f->st, level, f->ptr< double >( level ), static_cast< double* >( dev ), S( stream ) );
+   else
+      launchToDofs< float >( *f->st, level, f->ptr< float >( level ), static_cast< float* >( dev ), S( stream ) );
+   HYB_API_END
+}
+
+int hyb_function_interpolate_const( hyb_function* fh, int level, double value, int flag, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f, "null argument" );
+   checkLevel( f, level );
+   const auto& L = f->st->L( level );
+   if ( value == 0.0 && flag == HYB_ALL )
+      HYB_CUDA( cudaMemsetAsync( f->at( level ), 0, f->levelBytes( level ), S( stream ) ) );
+   else if ( f->dtype == HYB_F64 )
+      k_fill< double ><<< dim3( L.slabBlocks, f->st->td.nC ), 256, 0, S( stream ) >>>( f->st->td, L.dev,
+                                                                                      f->ptr< double >( level ), value, flag );
+   else
+      k_fill< float ><<< dim3( L.slabBlocks, f->st->td.nC ), 256, 0, S( stream ) >>>( f->st->td, L.dev,
+                                                                                     f->ptr< float >( level ), float( value ),
+                                                                                     flag );
+   HYB_CHECK_LAUNCH();
+   HYB_API_END
+}
+
+static int lincombApi( hyb_function* fh, int level, int n, const double* sc, hyb_function* const* srcs, int flag,
+                       void* stream, bool add )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f && ( n == 0 || ( sc && srcs ) ), "null argument" );
+   require( n >= 0 && n <= 3, "at most three source functions" );
+   checkLevel( f, level );
+   for ( int i = 0; i < n; ++i )
+   {
+      sameStorage( f, FN( srcs[i] ) );
+      require( FN( srcs[i] )->dtype == f->dtype, "source and destination dtypes differ" );
+      checkLevel( FN( srcs[i] ), level );
+   }
+   if ( f->dtype == HYB_F64 )
+   {
+      const double* p[3] = { nullptr, nullptr, nullptr };
+      for ( int i = 0; i < n; ++i )
+         p[i] = FN( srcs[i] )->ptr< double >( level );
+      launchLincomb< double >( *f->st, level, f->ptr< double >( level ), n, sc, p, add, flag, S( stream ) );
+   }
+   else
+   {
+      const float* p[3] = { nullptr, nullptr, nullptr };
+      for ( int i = 0; i < n; ++i )
+         p[i] = FN( srcs[i] )->ptr< float >( level );
+      launchLincomb< float >( *f->st, level, f->ptr< float >( level ), n, sc, p, add, flag, S( stream ) );
+   }
+   HYB_API_END
+}
+
+int hyb_function_assign( hyb_function* f, int level, int n, const double* sc, hyb_function* const* srcs, int flag,
+                         void* stream )
+{
+   return lincombApi( f, level, n, sc, srcs, flag, stream, false );
+}
+
+int hyb_function_add( hyb_function* f, int level, int n, const double* sc, hyb_function* const* srcs, int flag, void* stream )
+{
+   return lincombApi( f, level, n, sc, srcs, flag, stream, true );
+}
+
+int hyb_function_dot( hyb_function* ah, hyb_function* bh, int level, int flag, double* out, void* stream )
+{
+   HYB_API_BEGIN
+   Function *a = FN( ah ), *b = FN( bh );
+   require( out, "null argument" );
+   sameStorage( a, b );
+   require( a->dtype == b->dtype, "dtypes differ" );
+   checkLevel( a, level );
+   checkLevel( b, level );
+   if ( a->dtype == HYB_F64 )
+      launchDot< double >( *a->st, level, a->ptr< double >( level ), b->ptr< double >( level ), flag, 1, S( stream ) );
+   else
+      launchDot< float >( *a->st, level, a->ptr< float >( level ), b->ptr< float >( level ), flag, 1, S( stream ) );
+   HYB_CUDA( cudaMemcpyAsync( a->st->hostScalar, a->st->scalars.p + 1, sizeof( double ), cudaMemcpyDeviceToHost, S( stream ) ) );
+   HYB_CUDA( cudaStreamSynchronize( S( stream ) ) );
+   *out = a->st->hostScalar[0];
+   HYB_API_END
+}
+
+int hyb_function_copy_convert( hyb_function* dh, hyb_function* sh, int level, void* stream )
+{
+   HYB_API_BEGIN
+   Function *d = FN( dh ), *s = FN( sh );
+   sameStorage( d, s );
+   checkLevel( d, level );
+   checkLevel( s, level );
+   if ( d->dtype == HYB_F64 && s->dtype == HYB_F32 )
+      launchConvert< double, float >( *d->st, level, d->ptr< double >( level ), s->ptr< float >( level ), S( stream ) );
+   else if ( d->dtype == HYB_F32 && s->dtype == HYB_F64 )
+      launchConvert< float, double >( *d->st, level, d->ptr< float >( level ), s->ptr< double >( level ), S( stream ) );
+   else
+      HYB_CUDA( cudaMemcpyAsync( d->at( level ), s->at( level ), d->levelBytes( level ), cudaMemcpyDeviceToDevice,
+                                 S( stream ) ) );
+   HYB_API_END
+}
+
+int hyb_operator_create_laplace( hyb_storage* s, int minL, int maxL, hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && out, "null argument" );
+   *out = reinterpret_cast< hyb_operator* >( makeLaplace( ST( s ), minL, maxL ) );
+   HYB_API_END
+}
+
+int hyb_operator_create_divkgrad( hyb_storage* s, int minL, int maxL, const double* const* nodal, hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && out && nodal, "null argument" );
+   std::vector< std::vector< double > > k;
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      require( nodal[l - minL] != nullptr, "missing nodal coefficient level" );
+      const int64_t n = ST( s )->topo.numDofs( l );
+      k.emplace_back( nodal[l - minL], nodal[l - minL] + n );
+   }
+   *out = reinterpret_cast< hyb_operator* >( makeDivKGrad( ST( s ), minL, maxL, k ) );
+   HYB_API_END
+}
+
+int hyb_operator_create_divkgrad_callback( hyb_storage* s, int minL, int maxL, double ( *kfun )( const double*, void* ),
+                                           void* ctx, hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && out && kfun, "null argument" );
+   require( minL >= 0 && minL <= maxL && maxL <= ST( s )->maxLevel, "invalid level range" );
+   const Topology& tp = ST( s )->topo;
+   std::vector< std::vector< double > > k;
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      std::vector< double > xyz;
+      dofCoords( tp, l, xyz );
+      std::vector< double > kv( xyz.size() / 3 );
+      for ( size_t i = 0; i < kv.size(); ++i )
+         kv[i] = kfun( &xyz[3 * i], ctx );
+      k.push_back( std::move( kv ) );
+   }
+   *out = reinterpret_cast< hyb_operator* >( makeDivKGrad( ST( s ), minL, maxL, k ) );
+   HYB_API_END
+}
+
+int hyb_storage_dof_coords( const hyb_storage* s, int level, double* xyz )
+{
+   HYB_API_BEGIN
+   require( s && xyz, "null argument" );
+   require( level >= 0 && level <= s->maxLevel, "level out of range" );
+   std::vector< double > v;
+   dofCoords( s->topo, level, v );
+   std::copy( v.begin(), v.end(), xyz );
+   HYB_API_END
+}
+
+int hyb_operator_destroy( hyb_operator* op )
+{
+   HYB_API_BEGIN
+   delete OP( op );
+   HYB_API_END
+}
+
+static void checkOpFn( const Operator* op, const Function* f, int level )
+{
+   require( op && f, "null argument" );
+   require( op->st == f->st, "operator and function belong to different storages" );
+   require( level >= op->minL && level <= op->maxL, "level outside the operator's level range" );
+   checkLevel( f, level );
+}
+
+int hyb_operator_apply( hyb_operator* oh, hyb_function* sh, hyb_function* dh, int level, int flag, int update, void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *src = FN( sh ), *dst = FN( dh );
+   checkOpFn( op, src, level );
+   checkOpFn( op, dst, level );
+   require( src != dst, "apply needs distinct src and dst (reference: WALBERLA_ASSERT_NOT_IDENTICAL)" );
+   require( src->dtype == dst->dtype, "dtypes differ" );
+   require( update == HYB_REPLACE || update == HYB_ADD, "invalid update type" );
+   const int mode = update == HYB_ADD ? kAdd : kReplace;
+   if ( src->dtype == HYB_F64 )
+      launchApply< double >( *op, level, src->ptr< double >( level ), dst->ptr< double >( level ), nullptr, flag, mode, S( stream ) );
+   else
+      launchApply< float >( *op, level, src->ptr< float >( level ), dst->ptr< float >( level ), nullptr, flag, mode, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_operator_residual( hyb_operator* oh, hyb_function* xh, hyb_function* bh, hyb_function* rh, int level, int flag,
+                           void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *x = FN( xh ), *b = FN( bh ), *r = FN( rh );
+   checkOpFn( op, x, level );
+   checkOpFn( op, b, level );
+   checkOpFn( op, r, level );
+   require( x != r && b != r, "residual needs a separate output function" );
+   require( x->dtype == b->dtype && x->dtype == r->dtype, "dtypes differ" );
+   if ( x->dtype == HYB_F64 )
+      launchApply< double >( *op, level, x->ptr< double >( level ), r->ptr< double >( level ), b->ptr< double >( level ), flag,
+                             kResidual, S( stream ) );
+   else
+      launchApply< float >( *op, level, x->ptr< float >( level ), r->ptr< float >( level ), b->ptr< float >( level ), flag,
+                            kResidual, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_operator_smooth_sor( hyb_operator* oh, hyb_function* dh, hyb_function* rh, double relax, int level, int flag,
+                             void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *u = FN( dh ), *b = FN( rh );
+   checkOpFn( op, u, level );
+   checkOpFn( op, b, level );
+   require( u != b, "smooth_sor needs distinct dst and rhs" );
+   require( u->dtype == b->dtype, "dtypes differ" );
+   if ( u->dtype == HYB_F64 )
+      launchSor< double >( *op, level, u->ptr< double >( level ), b->ptr< double >( level ), relax, flag, S( stream ) );
+   else
+      launchSor< float >( *op, level, u->ptr< float >( level ), b->ptr< float >( level ), float( relax ), flag, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_operator_smooth_jac( hyb_operator* oh, hyb_function* dh, hyb_function* rh, hyb_function* sh, double relax, int level,
+                             int flag, void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *d = FN( dh ), *b = FN( rh ), *s = FN( sh );
+   checkOpFn( op, d, level );
+   checkOpFn( op, b, level );
+   checkOpFn( op, s, level );
+   require( d != s, "smooth_jac needs distinct dst and src" );
+   require( d->dtype == b->dtype && d->dtype == s->dtype, "dtypes differ" );
+   if ( d->dtype == HYB_F64 )
+      launchJacobi< double >( *op, level, s->ptr< double >( level ), d->ptr< double >( level ), b->ptr< double >( level ), relax,
+                              flag, S( stream ) );
+   else
+      launchJacobi< float >( *op, level, s->ptr< float >( level ), d->ptr< float >( level ), b->ptr< float >( level ),
+                             float( relax ), flag, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_operator_cell_stencil( const hyb_operator* oh, int level, int cell, int mask, double* out15 )
+{
+   HYB_API_BEGIN
+   const Operator* op = reinterpret_cast< const Operator* >( oh );
+   require( op && out15, "null argument" );
+   require( !op->variable, "stencils are stored for constant-coefficient operators only" );
+   require( level >= op->minL && level <= op->maxL && cell >= 0 && cell < op->st->td.nC && mask >= 0 && mask < 16,
+            "index out of range" );
+   const auto& st = op->stHost[level - op->minL];
+   std::copy( st.begin() + ( size_t( cell ) * 16 + mask ) * 15, st.begin() + ( size_t( cell ) * 16 + mask ) * 15 + 15, out15 );
+   HYB_API_END
+}
+
+int hyb_prolongate( hyb_function* fh, int src, int flag, int update, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f, "null argument" );
+   checkLevel( f, src );
+   checkLevel( f, src + 1 );
+   require( update == HYB_REPLACE || update == HYB_ADD, "invalid update type" );
+   if ( f->dtype == HYB_F64 )
+      launchProlongate< double >( *f->st, src, f->ptr< double >( src ), f->ptr< double >( src + 1 ), flag, update == HYB_ADD,
+                                  S( stream ) );
+   else
+      launchProlongate< float >( *f->st, src, f->ptr< float >( src ), f->ptr< float >( src + 1 ), flag, update == HYB_ADD,
+                                 S( stream ) );
+   HYB_API_END
+}
+
+int hyb_restrict( hyb_function* fh, int src, int flag, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f, "null argument" );
+   checkLevel( f, src );
+   checkLevel( f, src - 1 );
+   if ( f->dtype == HYB_F64 )
+      launchRestrict< double >( *f->st, src, f->ptr< double >( src ), f->ptr< double >( src - 1 ), flag, S( stream ) );
+   else
+      launchRestrict< float >( *f->st, src, f->ptr< float >( src ), f->ptr< float >( src - 1 ), flag, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_cg_solve( hyb_operator* oh, hyb_function* xh, hyb_function* bh, int level, double tol, int maxIter, int* iters,
+                  int* converged, void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *x = FN( xh ), *b = FN( bh );
+   checkOpFn( op, x, level );
+   checkOpFn( op, b, level );
+   require( x->dtype == HYB_F64 && b->dtype == HYB_F64, "the CG solver runs in FP64" );
+   require( maxIter >= 0, "max_iter must be non-negative" );
+   CgScratch cs;
+   launchCg( *op, level, x->ptr< double >( level ), b->ptr< double >( level ), cs, tol, maxIter, S( stream ) );
+   int st[2] = { 0, 0 };
+   HYB_CUDA( cudaMemcpyAsync( st, cs.status.p, 2 * sizeof( int ), cudaMemcpyDeviceToHost, S( stream ) ) );
+   HYB_CUDA( cudaStreamSynchronize( S( stream ) ) );
+   if ( iters )
+      *iters = st[0];
+   if ( converged )
+      *converged = st[1];
+   HYB_API_END
+}
+
+int hyb_gmg_create( hyb_storage* s, hyb_operator* oh, int minL, int maxL, int pre, int post, double relax, int smoother,
+                    double coarseTol, int coarseMaxIter, hyb_gmg** out )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   require( s && op && out, "null argument" );
+   require( op->st == ST( s ), "operator belongs to another storage" );
+   require( minL >= op->minL && maxL <= op->maxL && minL <= maxL, "GMG levels outside the operator's level range" );
+   require( pre >= 0 && post >= 0, "smoothing steps must be non-negative" );
+   require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI, "unknown smoother" );
+   auto g = std::make_unique< hyb_gmg_s >();
+   g->st = ST( s );
+   g->op = op;
+   g->minL = minL;
+   g->maxL = maxL;
+   g->pre = pre;
+   g->post = post;
+   g->relax = relax;
+   g->smoother = smoother;
+   g->coarseTol = coarseTol;
+   g->coarseMaxIter = coarseMaxIter;
+   g->tmp64.reset( makeFunction( ST( s ), minL, maxL, HYB_F64 ) );
+   *out = g.release();
+   HYB_API_END
+}
+
+int hyb_gmg_destroy( hyb_gmg* g )
+{
+   HYB_API_BEGIN
+   delete static_cast< hyb_gmg_s* >( g );
+   HYB_API_END
+}
+
+static void checkGmg( Gmg* g, Function* x, Function* b, int level )
+{
+   require( g && x && b, "null argument" );
+   require( x->st == g->st && b->st == g->st, "functions belong to another storage" );
+   require( x->dtype == HYB_F64 && b->dtype == HYB_F64, "GMG functions are FP64 (the FP32 hierarchy is internal)" );
+   require( level > g->minL - 1 && level <= g->maxL, "level outside the GMG level range" );
+   require( x->minL <= g->minL && b->minL <= g->minL && x->maxL >= level && b->maxL >= level,
+            "x and b must span the GMG levels" );
+}
+
+int hyb_gmg_solve( hyb_gmg* gh, hyb_function* xh, hyb_function* bh, int level, void* stream )
+{
+   HYB_API_BEGIN
+   Gmg*      g = gh;
+   Function *x = FN( xh ), *b = FN( bh );
+   checkGmg( g, x, b, level );
+   runGraph( *g, *x, *b, level, 0, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_gmg_solve_to_tolerance( hyb_gmg* gh, hyb_function* xh, hyb_function* bh, int level, double relTol, int maxCycles,
+                                int precision, double* history, int* cycles, void* stream )
+{
+   HYB_API_BEGIN
+   Gmg*      g = gh;
+   Function *x = FN( xh ), *b = FN( bh );
+   checkGmg( g, x, b, level );
+   require( precision == 64 || precision == 32, "precision must be 64 or 32" );
+   require( maxCycles >= 0, "max_cycles must be non-negative" );
+   cudaStream_t s = S( stream );
+   Storage&     st = *g->st;
+   if ( precision == 32 && !g->x32 )
+   {
+      g->x32.reset( makeFunction( &st, g->minL, g->maxL, HYB_F32 ) );
+      g->b32.reset( makeFunction( &st, g->minL, g->maxL, HYB_F32 ) );
+      g->t32.reset( makeFunction( &st, g->minL, g->maxL, HYB_F32 ) );
+      g->r64.reset( makeFunction( &st, g->minL, g->maxL, HYB_F64 ) );
+      g->cx64.reset( makeFunction( &st, g->minL, g->minL, HYB_F64 ) );
+      g->cb64.reset( makeFunction( &st, g->minL, g->minL, HYB_F64 ) );
+   }
+   // ||b|| and the initial residual
+   launchDot< double >( st, level, b->ptr< double >( level ), b->ptr< double >( level ), kGmgFlag, 2, s );
+   HYB_CUDA( cudaMemcpyAsync( st.hostScalar + 2, st.scalars.p + 2, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
+   runGraph( *g, *x, *b, level, precision == 64 ? kNorm64 : kNormMixed, s );
+   HYB_CUDA( cudaMemcpyAsync( st.hostScalar, st.scalars.p, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
+   HYB_CUDA( cudaStreamSynchronize( s ) );
+   const double nb  = std::sqrt( st.hostScalar[2] ) > 0 ? std::sqrt( st.hostScalar[2] ) : 1.0;
+   double       rel = std::sqrt( st.hostScalar[0] ) / nb;
+   if ( history )
+      history[0] = rel;
+   int cyc = 0;
+   while ( cyc < maxCycles && rel > relTol )
+   {
+      runGraph( *g, *x, *b, level, precision == 64 ? kCycle64Norm : kMixedStep, s );
+      HYB_CUDA( cudaMemcpyAsync( st.hostScalar, st.scalars.p, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
+      HYB_CUDA( cudaStreamSynchronize( s ) );
+      rel = std::sqrt( st.hostScalar[0] ) / nb;
+      ++cyc;
+      if ( history )
+         history[cyc] = rel;
+      if ( !std::isfinite( rel ) )
+         throw Error( HYB_ENOTCONVERGED, "residual is not finite: the iteration diverged" );
+   }
+   if ( cycles )
+      *cycles = cyc;
+   HYB_API_END
+}
+
+} // extern "C"

@@ -1,0 +1,242 @@
+// Device-side data layout and per-point arithmetic of the P1 multigrid path.
+//
+// Layout in HBM. A function on level L stores, for every macro-cell, the values
+// of its whole closure (interior, faces, edges, vertices: (N+1)(N+2)(N+3)/6
+// points, N = 2^L) in the reference's tetrahedral linear order
+// (src/hyteg/indexing/MacroCellIndexing.hpp:37-54, x fastest, then y, then z);
+// each cell slab is padded to a multiple of 32 values. A micro-vertex shared by
+// several cells has one replica per cell; every kernel that writes it writes all
+// replicas, so all replicas always agree. The reference's ghost-layer copies
+// (VertexDoFPackInfo) therefore never run: a "ghost update" is the replica write
+// fused into the kernel that produced the value.
+//
+// Point classes. A closure point's class mask has bit k set iff its barycentric
+// micro-coordinate b_k is zero (b = (N-x-y-z, x, y, z)). Mask 0 is the cell
+// interior; one bit = a macro-face, two = a macro-edge, three = a macro-vertex.
+// Per cell and mask the class table gives the owning primitive and its BC.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hyb {
+
+struct ClassDev
+{
+   int32_t id;    // primitive id within its kind
+   uint8_t kind;  // 0 vertex, 1 edge, 2 face, 3 cell
+   uint8_t bc;    // DoFType bits
+   uint8_t owned; // this cell holds the canonical replica
+   uint8_t k0, k1, k2; // cell-local indices of the primitive's vertices (sorted-id order)
+   uint8_t pad;
+   float   invN;  // 1 / #cells adjacent to the primitive
+};
+static_assert( sizeof( ClassDev ) == 16, "ClassDev layout" );
+
+struct TopoDev
+{
+   int             nC, nF, nE, nV;
+   const ClassDev* cls;     // [nC][16]
+   const int32_t*  fEmb;    // [nF][2] packed embeddings, -1 if absent
+   const int32_t*  eEmbOff; // [nE+1]
+   const int32_t*  eEmb;
+   const int32_t*  vEmbOff; // [nV+1]
+   const int32_t*  vEmb;
+   const uint8_t*  fBc;
+   const uint8_t*  eBc;
+   const uint8_t*  vBc;
+   const int8_t*   labels;  // [nC][4] colour labels of the cell's vertices
+   int             m;       // number of colours
+};
+
+struct LevelDev
+{
+   int     L, N, W, S, stride; // W = N+1 points per macro-edge, S = closure size
+   int     nIntFace, nIntCell;
+   int     nBdry;              // nV + nE (N-1) + nF nIntFace
+   int     nSeg;               // interior row segments (32 points each)
+   int     nSorSeg;            // interior row segments of 32 colour groups
+   const int32_t* seg;         // packed z | y<<10 | x0<<20
+   const int32_t* sorSeg;      // packed z | y<<10 | g0<<20
+   const int32_t* xyz;         // closure index -> x | y<<10 | z<<20
+};
+
+// 15 stencil offsets, order shared with the oracle and the C ABI
+__host__ __device__ constexpr int offX( int q )
+{
+   return q == 1 ? 1 : q == 2 ? -1 : q == 7 ? -1 : q == 8 ? 1 : q == 9 ? -1 : q == 10 ? 1 : q == 13 ? -1 : q == 14 ? 1 : 0;
+}
+__host__ __device__ constexpr int offY( int q )
+{
+   return q == 3 ? 1 : q == 4 ? -1 : q == 7 ? 1 : q == 8 ? -1 : q == 11 ? -1 : q == 12 ? 1 : q == 13 ? 1 : q == 14 ? -1 : 0;
+}
+__host__ __device__ constexpr int offZ( int q )
+{
+   return q == 5 ? 1 : q == 6 ? -1 : q == 9 ? 1 : q == 10 ? -1 : q == 11 ? 1 : q == 12 ? -1 : q == 13 ? -1 : q == 14 ? 1 : 0;
+}
+
+// valid offsets (bit q) of a point of class mask (offset stays inside the closure)
+__constant__ const uint16_t kValidOffsets[16] = { 0x7fff, 0x3fd5, 0x5d7b, 0x1d51, 0x36ef, 0x36c5, 0x146b, 0x1441,
+                                                  0x4bbf, 0x0b95, 0x493b, 0x0911, 0x02af, 0x0285, 0x002b, 0x0001 };
+// incident micro-tets (bit i of the 24 below) lying inside the closure, per class mask
+__constant__ const uint32_t kValidTets[16] = { 0xffffff, 0xe324ae, 0x9e4a4d, 0x82000c, 0x458d9b, 0x41048a,
+                                               0x040809, 0x000008, 0x381377, 0x200026, 0x180245, 0x000004,
+                                               0x000113, 0x000002, 0x000001, 0x000000 };
+
+// The 24 micro-tets incident to a micro-vertex: micro-cell type t (WHITE_UP, BLUE_UP,
+// GREEN_UP, WHITE_DOWN, BLUE_DOWN, GREEN_DOWN of src/hyteg/volumedofspace/CellDoFIndexing.hpp:
+// 155-198), the vertex's role k in it, and the stencil offset of each of its 4 vertices.
+struct IncidentTet
+{
+   int t, k, q[4];
+};
+__host__ __device__ constexpr IncidentTet incidentTet( int i )
+{
+   constexpr int tab[24][6] = { { 0, 0, 0, 1, 3, 5 },   { 0, 1, 2, 0, 7, 9 },    { 0, 2, 4, 8, 0, 11 },  { 0, 3, 6, 10, 12, 0 },
+                                { 1, 0, 0, 3, 7, 5 },   { 1, 1, 4, 0, 2, 11 },   { 1, 2, 8, 1, 0, 14 },  { 1, 3, 6, 12, 13, 0 },
+                                { 2, 0, 0, 7, 5, 9 },   { 2, 1, 8, 0, 14, 11 },  { 2, 2, 6, 13, 0, 2 },  { 2, 3, 10, 12, 1, 0 },
+                                { 3, 0, 0, 5, 9, 11 },  { 3, 1, 6, 0, 2, 4 },    { 3, 2, 10, 1, 0, 8 },  { 3, 3, 12, 3, 7, 0 },
+                                { 4, 0, 0, 7, 2, 13 },  { 4, 1, 8, 0, 4, 6 },    { 4, 2, 1, 3, 0, 12 },  { 4, 3, 14, 5, 11, 0 },
+                                { 5, 0, 0, 1, 14, 5 },  { 5, 1, 2, 0, 11, 9 },   { 5, 2, 13, 12, 0, 7 }, { 5, 3, 6, 10, 8, 0 } };
+   return IncidentTet{ tab[i][0], tab[i][1], { tab[i][2], tab[i][3], tab[i][4], tab[i][5] } };
+}
+
+__host__ __device__ __forceinline__ int tetSize( int w ) { return ( w + 2 ) * ( w + 1 ) * w / 6; }
+// first index of row (y, z) in a closure of width W
+__host__ __device__ __forceinline__ int rowStart( int W, int y, int z )
+{
+   const int wms = W - z;
+   return tetSize( W ) - tetSize( wms ) + y * ( wms + 1 ) - ( ( y + 1 ) * y ) / 2;
+}
+__host__ __device__ __forceinline__ int cidx( int W, int x, int y, int z ) { return rowStart( W, y, z ) + x; }
+
+__host__ __device__ __forceinline__ int classMask( int N, int x, int y, int z )
+{
+   return ( N - x - y - z == 0 ? 1 : 0 ) | ( x == 0 ? 2 : 0 ) | ( y == 0 ? 4 : 0 ) | ( z == 0 ? 8 : 0 );
+}
+
+// Index offsets of the 15 neighbours of closure point (*, y, z) relative to its own
+// index, from the row-start recurrences of the tetrahedral layout.
+struct NbrOff
+{
+   int d[15];
+};
+__host__ __device__ __forceinline__ NbrOff nbrOffsets( int W, int y, int z )
+{
+   NbrOff    o;
+   const int dyp = W - z - y;                         // (0,1,0)
+   const int dym = -( W - z - y + 1 );                // (0,-1,0)
+   const int slz = ( W - z ) * ( W - z + 1 ) / 2;      // points in slice z
+   const int slm = ( W - z + 1 ) * ( W - z + 2 ) / 2;  // points in slice z-1
+   const int dzp = slz - y;                           // (0,0,1)
+   const int dzm = -( slm - y );                      // (0,0,-1)
+   const int d11 = dym + slz - ( y - 1 );             // (0,-1,1)
+   const int d12 = dyp - slm + ( y + 1 );             // (0,1,-1)
+   o.d[0]  = 0;
+   o.d[1]  = 1;
+   o.d[2]  = -1;
+   o.d[3]  = dyp;
+   o.d[4]  = dym;
+   o.d[5]  = dzp;
+   o.d[6]  = dzm;
+   o.d[7]  = dyp - 1;
+   o.d[8]  = dym + 1;
+   o.d[9]  = dzp - 1;
+   o.d[10] = dzm + 1;
+   o.d[11] = d11;
+   o.d[12] = d12;
+   o.d[13] = d12 - 1;
+   o.d[14] = d11 + 1;
+   return o;
+}
+
+// Unpack a primitive embedding and place primitive-local barycentric weights
+// (weights of the primitive's vertices in sorted-id order) into the cell.
+__device__ __forceinline__ void embeddingCoords( int32_t packed, int kind, int N, int i, int j, int& cell, int& x, int& y,
+                                                 int& z )
+{
+   cell         = packed & 0xFFFFFF;
+   const int k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3, k2 = ( packed >> 28 ) & 3;
+   int       b[4] = { 0, 0, 0, 0 };
+   if ( kind == 0 )
+      b[k0] = N;
+   else if ( kind == 1 )
+   {
+      b[k0] = N - i;
+      b[k1] = i;
+   }
+   else
+   {
+      b[k0] = N - i - j;
+      b[k1] = i;
+      b[k2] = j;
+   }
+   x = b[1];
+   y = b[2];
+   z = b[3];
+}
+
+__device__ __forceinline__ int colourOf( const TopoDev& tp, int cell, int N, int x, int y, int z )
+{
+   const int8_t* l = tp.labels + 4 * cell;
+   const int     s = int( l[0] ) * ( N - x - y - z ) + int( l[1] ) * x + int( l[2] ) * y + int( l[3] ) * z;
+   return ( ( s % tp.m ) + tp.m ) % tp.m;
+}
+
+// Operator data of one level, in the compute type T.
+template < typename T >
+struct OpDev
+{
+   const T* st;  // constant coefficient: [nC][16][15] partial stencils per class
+   const T* K;   // variable coefficient: [nC][6][4][4] micro-tet matrices (1/4 folded in)
+   const T* kap; // variable coefficient: nodal k, function layout
+   int      stride;
+};
+
+// Partial row of the operator at closure point (x,y,z) of `cell`: the contributions
+// of the micro-tets of this cell only. u = the cell's slab.
+template < typename T, bool VAR >
+__device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* __restrict__ u, int cell, int W, int x, int y,
+                                            int z, T& diag, T& off )
+{
+   const int  N    = W - 1;
+   const int  mask = classMask( N, x, y, z );
+   const int  base = cidx( W, x, y, z );
+   const NbrOff no = nbrOffsets( W, y, z );
+   if constexpr ( !VAR )
+   {
+      const T*       st    = op.st + ( size_t( cell ) * 16 + mask ) * 15;
+      const uint32_t valid = kValidOffsets[mask];
+      diag += st[0];
+#pragma unroll
+      for ( int q = 1; q < 15; ++q )
+         if ( valid & ( 1u << q ) )
+            off += st[q] * u[base + no.d[q]];
+   }
+   else
+   {
+      const T*       kv    = op.kap + size_t( cell ) * op.stride;
+      const T*       K     = op.K + size_t( cell ) * 96;
+      const uint32_t valid = kValidTets[mask];
+#pragma unroll
+      for ( int i = 0; i < 24; ++i )
+      {
+         const IncidentTet it = incidentTet( i );
+         if ( !( valid & ( 1u << i ) ) )
+            continue;
+         const T ks = kv[base + no.d[it.q[0]]] + kv[base + no.d[it.q[1]]] + kv[base + no.d[it.q[2]]] +
+                      kv[base + no.d[it.q[3]]];
+         const T* Kr = K + it.t * 16 + it.k * 4;
+#pragma unroll
+         for ( int j = 0; j < 4; ++j )
+         {
+            if ( j == it.k )
+               diag += ks * Kr[j];
+            else
+               off += ks * Kr[j] * u[base + no.d[it.q[j]]];
+         }
+      }
+   }
+}
+
+} // namespace hyb

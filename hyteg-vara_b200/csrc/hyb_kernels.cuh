@@ -1,0 +1,764 @@
+// sm_100a kernels of the P1 multigrid path and their launchers.
+//
+// Every level operation is ONE launch whose first blocks sweep macro-cell
+// interiors (one warp per 32-point row segment of the tetrahedral layout, all
+// 15 neighbours at closed-form index offsets) and whose remaining blocks handle
+// the micro-vertices on macro-faces, -edges and -vertices (one thread per DoF,
+// summing the partial rows of all adjacent cells and writing every replica).
+// The work is HBM-bound integer-indexed stencil arithmetic on CUDA cores; no
+// tensor-core path applies.
+#pragma once
+
+#include "hyb_device.cuh"
+
+namespace hyb {
+
+enum ApplyMode : int
+{
+   kReplace  = 0,
+   kAdd      = 1,
+   kResidual = 2, // dst = rhs - A src
+};
+
+constexpr int kCellWarps  = 4; // warps (row segments) per cell block
+constexpr int kBdryThreads = 128;
+
+// ---------------------------------------------------------------------------
+// Boundary-DoF enumeration: [vertices | edge interiors | face interiors]
+// ---------------------------------------------------------------------------
+struct BdryPoint
+{
+   int kind, prim, i, j;
+};
+
+__device__ __forceinline__ BdryPoint decodeBdry( const TopoDev& tp, const LevelDev& lv, int t )
+{
+   BdryPoint p{ 0, 0, 0, 0 };
+   if ( t < tp.nV )
+   {
+      p.kind = 0;
+      p.prim = t;
+      return p;
+   }
+   t -= tp.nV;
+   const int ne = tp.nE * ( lv.N - 1 );
+   if ( t < ne )
+   {
+      p.kind = 1;
+      p.prim = t / ( lv.N - 1 );
+      p.i    = t % ( lv.N - 1 ) + 1;
+      return p;
+   }
+   t -= ne;
+   p.kind = 2;
+   p.prim = t / lv.nIntFace;
+   const int q  = t % lv.nIntFace;
+   const int rr = lv.nIntFace - 1 - q; // index counted from the short rows
+   int       k  = int( ( sqrtf( 8.0f * float( rr ) + 1.0f ) - 1.0f ) * 0.5f );
+   while ( ( k + 1 ) * ( k + 2 ) / 2 <= rr )
+      ++k;
+   while ( k * ( k + 1 ) / 2 > rr )
+      --k;
+   p.i = ( k + 1 ) * ( k + 2 ) / 2 - 1 - rr + 1;
+   p.j = lv.N - 2 - k;
+   return p;
+}
+
+__device__ __forceinline__ int numEmb( const TopoDev& tp, int kind, int prim )
+{
+   if ( kind == 2 )
+      return tp.fEmb[2 * prim + 1] >= 0 ? 2 : 1;
+   if ( kind == 1 )
+      return tp.eEmbOff[prim + 1] - tp.eEmbOff[prim];
+   return tp.vEmbOff[prim + 1] - tp.vEmbOff[prim];
+}
+__device__ __forceinline__ int32_t embAt( const TopoDev& tp, int kind, int prim, int e )
+{
+   if ( kind == 2 )
+      return tp.fEmb[2 * prim + e];
+   if ( kind == 1 )
+      return tp.eEmb[tp.eEmbOff[prim] + e];
+   return tp.vEmb[tp.vEmbOff[prim] + e];
+}
+__device__ __forceinline__ uint8_t primBc( const TopoDev& tp, int kind, int prim )
+{
+   return kind == 2 ? tp.fBc[prim] : kind == 1 ? tp.eBc[prim] : tp.vBc[prim];
+}
+
+// Full row (sum of partial rows over adjacent cells) of a boundary DoF.
+template < typename T, bool VAR >
+__device__ __forceinline__ void bdryRow( const TopoDev& tp, const LevelDev& lv, const OpDev< T >& op, const T* u,
+                                         const BdryPoint& p, T& diag, T& off )
+{
+   const int ne = numEmb( tp, p.kind, p.prim );
+   for ( int e = 0; e < ne; ++e )
+   {
+      int c, x, y, z;
+      embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+      partialRow< T, VAR >( op, u + size_t( c ) * lv.stride, c, lv.W, x, y, z, diag, off );
+   }
+}
+
+template < typename T >
+__device__ __forceinline__ size_t bdryReplica( const TopoDev& tp, const LevelDev& lv, const BdryPoint& p, int e )
+{
+   int c, x, y, z;
+   embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+   return size_t( c ) * lv.stride + cidx( lv.W, x, y, z );
+}
+
+template < typename T >
+__device__ __forceinline__ void bdryWriteAll( const TopoDev& tp, const LevelDev& lv, const BdryPoint& p, T* dst, T v )
+{
+   const int ne = numEmb( tp, p.kind, p.prim );
+   for ( int e = 0; e < ne; ++e )
+      dst[bdryReplica< T >( tp, lv, p, e )] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Interior stencil evaluation with all 15 neighbours inside the cell
+// ---------------------------------------------------------------------------
+template < typename T, bool VAR >
+struct InteriorOp
+{
+   T w[15];       // constant operator: the class-0 stencil of the cell
+   const T* K;    // variable operator: micro-tet matrices of the cell
+   const T* kv;   // variable operator: nodal k slab of the cell
+
+   __device__ __forceinline__ void load( const OpDev< T >& op, int cell )
+   {
+      if constexpr ( !VAR )
+      {
+         const T* st = op.st + size_t( cell ) * 16 * 15;
+#pragma unroll
+         for ( int q = 0; q < 15; ++q )
+            w[q] = st[q];
+      }
+      else
+      {
+         K  = op.K + size_t( cell ) * 96;
+         kv = op.kap + size_t( cell ) * op.stride;
+      }
+   }
+
+   // diag and off-diagonal sum at index `base` with neighbour offsets `no`
+   __device__ __forceinline__ void row( const T* __restrict__ u, int base, const NbrOff& no, T& diag, T& off ) const
+   {
+      if constexpr ( !VAR )
+      {
+         diag = w[0];
+         T s  = 0;
+#pragma unroll
+         for ( int q = 1; q < 15; ++q )
+            s += w[q] * u[base + no.d[q]];
+         off = s;
+      }
+      else
+      {
+         T kq[15], uq[15];
+#pragma unroll
+         for ( int q = 0; q < 15; ++q )
+         {
+            kq[q] = kv[base + no.d[q]];
+            uq[q] = u[base + no.d[q]];
+         }
+         T d = 0, s = 0;
+#pragma unroll
+         for ( int i = 0; i < 24; ++i )
+         {
+            const IncidentTet it = incidentTet( i );
+            const T ks = kq[it.q[0]] + kq[it.q[1]] + kq[it.q[2]] + kq[it.q[3]];
+            const T* Kr = K + it.t * 16 + it.k * 4;
+            T acc = 0;
+#pragma unroll
+            for ( int j = 0; j < 4; ++j )
+               if ( j == it.k )
+                  d += ks * Kr[j];
+               else
+                  acc += Kr[j] * uq[it.q[j]];
+            s += ks * acc;
+         }
+         diag = d;
+         off  = s;
+      }
+   }
+};
+
+// ---------------------------------------------------------------------------
+// apply / residual (P1Operator::apply, P1Operator.hpp:196-324;
+// P1ElementwiseOperator::apply, P1ElementwiseOperator.cpp:64-221)
+// ---------------------------------------------------------------------------
+template < typename T, bool VAR, int MODE >
+__global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
+                                                  T* __restrict__ dst, const T* __restrict__ rhs, int flag,
+                                                  int nCellBlocks, int blocksPerCell )
+{
+   if ( int( blockIdx.x ) < nCellBlocks )
+   {
+      const int cell = blockIdx.x / blocksPerCell;
+      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
+      if ( seg >= lv.nSeg )
+         return;
+      const int32_t sp = lv.seg[seg];
+      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+      if ( x + y + z > lv.N - 1 )
+         return;
+      InteriorOp< T, VAR > io;
+      io.load( op, cell );
+      const size_t co   = size_t( cell ) * lv.stride;
+      const int    base = cidx( lv.W, x, y, z );
+      const NbrOff no   = nbrOffsets( lv.W, y, z );
+      T            diag, off;
+      io.row( src + co, base, no, diag, off );
+      const T ax = diag * src[co + base] + off;
+      if constexpr ( MODE == kReplace )
+         dst[co + base] = ax;
+      else if constexpr ( MODE == kAdd )
+         dst[co + base] += ax;
+      else
+         dst[co + base] = rhs[co + base] - ax;
+      return;
+   }
+   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
+   if ( t >= lv.nBdry )
+      return;
+   const BdryPoint p = decodeBdry( tp, lv, t );
+   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
+      return;
+   T diag = 0, off = 0;
+   bdryRow< T, VAR >( tp, lv, op, src, p, diag, off );
+   const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+   const T      ax = diag * src[r0] + off;
+   T            v;
+   if constexpr ( MODE == kReplace )
+      v = ax;
+   else if constexpr ( MODE == kAdd )
+      v = dst[r0] + ax;
+   else
+      v = rhs[r0] - ax;
+   bdryWriteAll( tp, lv, p, dst, v );
+}
+
+// ---------------------------------------------------------------------------
+// Multicolour SOR: u <- (1-w) u + w (b - sum_{o!=0} a_o u_o) / a_0 (reference update
+// formula: P1Operator.hpp:1638, sor_3D_macrocell_P1.cpp:31-77). One sweep is
+//   interface passes: DoFs on macro-faces/-edges/-vertices of global colour
+//     sum_k label(V_k) b_k mod m, c = 0..m-1 (boundary blocks only), then
+//   interior passes: macro-cell interior points of local colour (x + 2y + 3z) mod 4,
+//     c = 0..3 (cell blocks only; interiors of different cells are not coupled).
+// Like the reference's V -> E -> F -> C staging, interfaces are relaxed before the
+// cell interiors. No two DoFs of one pass are coupled.
+// ---------------------------------------------------------------------------
+constexpr int kInteriorColours = 4;
+
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_sor( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                const T* __restrict__ rhs, T relax, int flag, int colour, int nCellBlocks,
+                                                int blocksPerCell )
+{
+   if ( int( blockIdx.x ) < nCellBlocks )
+   {
+      const int cell = blockIdx.x / blocksPerCell;
+      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
+      if ( seg >= lv.nSorSeg )
+         return;
+      const int32_t sp = lv.sorSeg[seg];
+      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, g = ( sp >> 20 ) + ( threadIdx.x & 31 );
+      // the one x of colour `colour` in the group [1 + 4g, 1 + 4g + 4)
+      const int x0 = 1 + kInteriorColours * g;
+      const int c0 = ( x0 + 2 * y + 3 * z ) & 3;
+      const int x  = x0 + ( ( colour - c0 ) & 3 );
+      if ( x + y + z > lv.N - 1 )
+         return;
+      InteriorOp< T, VAR > io;
+      io.load( op, cell );
+      const size_t co   = size_t( cell ) * lv.stride;
+      const int    base = cidx( lv.W, x, y, z );
+      const NbrOff no   = nbrOffsets( lv.W, y, z );
+      T            diag, off;
+      io.row( u + co, base, no, diag, off );
+      u[co + base] = ( T( 1 ) - relax ) * u[co + base] + relax * ( rhs[co + base] - off ) / diag;
+      return;
+   }
+   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
+   if ( t >= lv.nBdry )
+      return;
+   const BdryPoint p = decodeBdry( tp, lv, t );
+   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
+      return;
+   {
+      int c, x, y, z;
+      embeddingCoords( embAt( tp, p.kind, p.prim, 0 ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+      if ( colourOf( tp, c, lv.N, x, y, z ) != colour )
+         return;
+   }
+   T diag = 0, off = 0;
+   bdryRow< T, VAR >( tp, lv, op, u, p, diag, off );
+   const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+   const T      v  = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
+   bdryWriteAll( tp, lv, p, u, v );
+}
+
+// ---------------------------------------------------------------------------
+// Weighted Jacobi (P1Operator::smooth_jac, P1Operator.hpp:424-440):
+// dst = src + relax * (rhs - A src) / diag(A)
+// ---------------------------------------------------------------------------
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
+                                                   T* __restrict__ dst, const T* __restrict__ rhs, T relax, int flag,
+                                                   int nCellBlocks, int blocksPerCell )
+{
+   if ( int( blockIdx.x ) < nCellBlocks )
+   {
+      const int cell = blockIdx.x / blocksPerCell;
+      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
+      if ( seg >= lv.nSeg )
+         return;
+      const int32_t sp = lv.seg[seg];
+      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+      if ( x + y + z > lv.N - 1 )
+         return;
+      InteriorOp< T, VAR > io;
+      io.load( op, cell );
+      const size_t co   = size_t( cell ) * lv.stride;
+      const int    base = cidx( lv.W, x, y, z );
+      const NbrOff no   = nbrOffsets( lv.W, y, z );
+      T            diag, off;
+      io.row( src + co, base, no, diag, off );
+      const T s      = src[co + base];
+      dst[co + base] = s + relax * ( rhs[co + base] - off - diag * s ) / diag;
+      return;
+   }
+   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
+   if ( t >= lv.nBdry )
+      return;
+   const BdryPoint p = decodeBdry( tp, lv, t );
+   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
+      return;
+   T diag = 0, off = 0;
+   bdryRow< T, VAR >( tp, lv, op, src, p, diag, off );
+   const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+   const T      s  = src[r0];
+   bdryWriteAll( tp, lv, p, dst, T( s + relax * ( rhs[r0] - off - diag * s ) / diag ) );
+}
+
+// ---------------------------------------------------------------------------
+// Linear prolongation (P1toP1LinearProlongation.cpp:194-410): a fine micro-vertex
+// either coincides with a coarse one (weight 1) or bisects a coarse micro-edge
+// (weights 1/2, 1/2). Computed in gather form inside any one adjacent cell.
+// ---------------------------------------------------------------------------
+template < typename T >
+__device__ __forceinline__ T interpolateFine( const T* __restrict__ coarse, int Wc, int X, int Y, int Z )
+{
+   const int px = X & 1, py = Y & 1, pz = Z & 1;
+   if ( !( px | py | pz ) )
+      return coarse[cidx( Wc, X >> 1, Y >> 1, Z >> 1 )];
+   int       ox = 0, oy = 0, oz = 0;
+   const int pat = px | ( py << 1 ) | ( pz << 2 );
+   switch ( pat )
+   {
+   case 1: ox = 1; break;
+   case 2: oy = 1; break;
+   case 4: oz = 1; break;
+   case 3: ox = -1; oy = 1; break;
+   case 5: ox = -1; oz = 1; break;
+   case 6: oy = -1; oz = 1; break;
+   default: ox = -1; oy = 1; oz = -1; break;
+   }
+   return T( 0.5 ) * ( coarse[cidx( Wc, ( X - ox ) >> 1, ( Y - oy ) >> 1, ( Z - oz ) >> 1 )] +
+                       coarse[cidx( Wc, ( X + ox ) >> 1, ( Y + oy ) >> 1, ( Z + oz ) >> 1 )] );
+}
+
+template < typename T, bool ADD >
+__global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev fl, int Wc, int strideC,
+                                                       const T* __restrict__ coarse, T* __restrict__ fine, int flag,
+                                                       int nCellBlocks, int blocksPerCell )
+{
+   if ( int( blockIdx.x ) < nCellBlocks )
+   {
+      const int cell = blockIdx.x / blocksPerCell;
+      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
+      if ( seg >= fl.nSeg )
+         return;
+      const int32_t sp = fl.seg[seg];
+      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+      if ( x + y + z > fl.N - 1 )
+         return;
+      const T      v  = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
+      const size_t fi = size_t( cell ) * fl.stride + cidx( fl.W, x, y, z );
+      fine[fi]        = ADD ? fine[fi] + v : v;
+      return;
+   }
+   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
+   if ( t >= fl.nBdry )
+      return;
+   const BdryPoint p = decodeBdry( tp, fl, t );
+   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
+      return;
+   int c, x, y, z;
+   embeddingCoords( embAt( tp, p.kind, p.prim, 0 ), p.kind, fl.N, p.i, p.j, c, x, y, z );
+   T v = interpolateFine( coarse + size_t( c ) * strideC, Wc, x, y, z );
+   if ( ADD )
+      v += fine[size_t( c ) * fl.stride + cidx( fl.W, x, y, z )];
+   bdryWriteAll( tp, fl, p, fine, v );
+}
+
+// ---------------------------------------------------------------------------
+// Full-weighting restriction (P1toP1LinearRestriction.cpp:168-345 with the generated
+// pull kernel): r_c(P) = r_f(2P) + 1/2 sum of r_f over the fine neighbours of 2P. A
+// boundary coarse DoF gathers in every adjacent cell, each fine point scaled by
+// 1/#cells of the primitive it lies on, so every fine point counts exactly once.
+// ---------------------------------------------------------------------------
+template < typename T >
+__global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev cl, int Wf, int strideF, const T* __restrict__ fine,
+                                                     T* __restrict__ coarse, int flag, int nCellBlocks, int blocksPerCell )
+{
+   if ( int( blockIdx.x ) < nCellBlocks )
+   {
+      const int cell = blockIdx.x / blocksPerCell;
+      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
+      if ( seg >= cl.nSeg )
+         return;
+      const int32_t sp = cl.seg[seg];
+      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+      if ( x + y + z > cl.N - 1 )
+         return;
+      const T*     f    = fine + size_t( cell ) * strideF;
+      const int    base = cidx( Wf, 2 * x, 2 * y, 2 * z );
+      const NbrOff no   = nbrOffsets( Wf, 2 * y, 2 * z );
+      T            s    = 0;
+#pragma unroll
+      for ( int q = 1; q < 15; ++q )
+         s += f[base + no.d[q]];
+      coarse[size_t( cell ) * cl.stride + cidx( cl.W, x, y, z )] = f[base] + T( 0.5 ) * s;
+      return;
+   }
+   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
+   if ( t >= cl.nBdry )
+      return;
+   const BdryPoint p = decodeBdry( tp, cl, t );
+   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
+      return;
+   const int Nf = Wf - 1;
+   const int ne = numEmb( tp, p.kind, p.prim );
+   T         acc = 0;
+   for ( int e = 0; e < ne; ++e )
+   {
+      int c, x, y, z;
+      embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, cl.N, p.i, p.j, c, x, y, z );
+      const int       X = 2 * x, Y = 2 * y, Z = 2 * z;
+      const T*        f = fine + size_t( c ) * strideF;
+      const ClassDev* cc = tp.cls + size_t( c ) * 16;
+      const int       mask = classMask( Nf, X, Y, Z );
+      const uint32_t  valid = kValidOffsets[mask];
+      const int       base  = cidx( Wf, X, Y, Z );
+      const NbrOff    no    = nbrOffsets( Wf, Y, Z );
+      acc += T( cc[mask].invN ) * f[base];
+      for ( int q = 1; q < 15; ++q )
+         if ( valid & ( 1u << q ) )
+         {
+            const int mq = classMask( Nf, X + offX( q ), Y + offY( q ), Z + offZ( q ) );
+            acc += T( 0.5f * cc[mq].invN ) * f[base + no.d[q]];
+         }
+   }
+   bdryWriteAll( tp, cl, p, coarse, acc );
+}
+
+// ---------------------------------------------------------------------------
+// Pointwise vector kernels over whole cell slabs (all replicas; consistent by
+// construction). blockIdx.y = cell.
+// ---------------------------------------------------------------------------
+template < typename T >
+__global__ void k_lincomb( TopoDev tp, LevelDev lv, T* __restrict__ dst, int n, T s0, const T* a0, T s1, const T* a1, T s2,
+                           const T* a2, int add, int flag )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int p    = lv.xyz[idx];
+   const int mask = classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 );
+   if ( !( tp.cls[cell * 16 + mask].bc & flag ) )
+      return;
+   const size_t i = size_t( cell ) * lv.stride + idx;
+   T            v = add ? dst[i] : T( 0 );
+   if ( n > 0 )
+      v += s0 * a0[i];
+   if ( n > 1 )
+      v += s1 * a1[i];
+   if ( n > 2 )
+      v += s2 * a2[i];
+   dst[i] = v;
+}
+
+// VertexDoFFunction::interpolate(constant, level, flag)
+template < typename T >
+__global__ void k_fill( TopoDev tp, LevelDev lv, T* __restrict__ dst, T value, int flag )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int p    = lv.xyz[idx];
+   const int mask = classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 );
+   if ( tp.cls[cell * 16 + mask].bc & flag )
+      dst[size_t( cell ) * lv.stride + idx] = value;
+}
+
+template < typename TD, typename TS >
+__global__ void k_convert( LevelDev lv, TD* __restrict__ dst, const TS* __restrict__ src, int nCells )
+{
+   const size_t i = size_t( blockIdx.x ) * blockDim.x + threadIdx.x;
+   if ( i < size_t( nCells ) * lv.stride )
+      dst[i] = TD( src[i] );
+}
+
+// x64 += e (FP32 correction) on flagged points
+template < typename T, typename TE >
+__global__ void k_add_correction( TopoDev tp, LevelDev lv, T* __restrict__ x, const TE* __restrict__ e, int flag )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int p    = lv.xyz[idx];
+   const int mask = classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 );
+   if ( !( tp.cls[cell * 16 + mask].bc & flag ) )
+      return;
+   const size_t i = size_t( cell ) * lv.stride + idx;
+   x[i] += T( e[i] );
+}
+
+// Partial dot products over the canonical replica of every DoF whose BC is in flag.
+template < typename T >
+__global__ void k_dot_partial( TopoDev tp, LevelDev lv, const T* __restrict__ a, const T* __restrict__ b, int flag,
+                               double* __restrict__ partial )
+{
+   __shared__ double red[32];
+   const int idx  = blockIdx.x * blockDim.x + threadIdx.x;
+   const int cell = blockIdx.y;
+   double    v    = 0;
+   if ( idx < lv.S )
+   {
+      const int p    = lv.xyz[idx];
+      const int mask = classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 );
+      const ClassDev cd = tp.cls[cell * 16 + mask];
+      if ( cd.owned && ( cd.bc & flag ) )
+      {
+         const size_t i = size_t( cell ) * lv.stride + idx;
+         v              = double( a[i] ) * double( b[i] );
+      }
+   }
+   for ( int o = 16; o > 0; o >>= 1 )
+      v += __shfl_down_sync( 0xffffffffu, v, o );
+   if ( ( threadIdx.x & 31 ) == 0 )
+      red[threadIdx.x >> 5] = v;
+   __syncthreads();
+   if ( threadIdx.x < 32 )
+   {
+      v = threadIdx.x < ( blockDim.x >> 5 ) ? red[threadIdx.x] : 0.0;
+      for ( int o = 16; o > 0; o >>= 1 )
+         v += __shfl_down_sync( 0xffffffffu, v, o );
+      if ( threadIdx.x == 0 )
+         partial[size_t( blockIdx.y ) * gridDim.x + blockIdx.x] = v;
+   }
+}
+
+// Deterministic second pass: one block sums the partials in a fixed order.
+__global__ void k_reduce_final( const double* __restrict__ partial, int n, double* __restrict__ out )
+{
+   __shared__ double red[32];
+   double            v = 0;
+   for ( int i = threadIdx.x; i < n; i += blockDim.x )
+      v += partial[i];
+   for ( int o = 16; o > 0; o >>= 1 )
+      v += __shfl_down_sync( 0xffffffffu, v, o );
+   if ( ( threadIdx.x & 31 ) == 0 )
+      red[threadIdx.x >> 5] = v;
+   __syncthreads();
+   if ( threadIdx.x < 32 )
+   {
+      v = threadIdx.x < ( blockDim.x >> 5 ) ? red[threadIdx.x] : 0.0;
+      for ( int o = 16; o > 0; o >>= 1 )
+         v += __shfl_down_sync( 0xffffffffu, v, o );
+      if ( threadIdx.x == 0 )
+         *out = v;
+   }
+}
+
+// Canonical DoF order <-> cell slabs (see oracle/hyteg_oracle.h for the order).
+__device__ __forceinline__ int64_t canonicalDof( const TopoDev& tp, const LevelDev& lv, int cell, int x, int y, int z )
+{
+   const int       N    = lv.N;
+   const int       mask = classMask( N, x, y, z );
+   const ClassDev& cd   = tp.cls[cell * 16 + mask];
+   const int       b[4] = { N - x - y - z, x, y, z };
+   const int64_t   offE = tp.nV, offF = offE + int64_t( tp.nE ) * ( N - 1 ), offC = offF + int64_t( tp.nF ) * lv.nIntFace;
+   switch ( cd.kind )
+   {
+   case 0: return cd.id;
+   case 1: return offE + int64_t( cd.id ) * ( N - 1 ) + ( b[cd.k1] - 1 );
+   case 2: {
+      const int i = b[cd.k1], j = b[cd.k2];
+      return offF + int64_t( cd.id ) * lv.nIntFace + ( j - 1 ) * ( N - 1 ) - ( j - 1 ) * j / 2 + ( i - 1 );
+   }
+   default: return offC + int64_t( cell ) * lv.nIntCell + cidx( N - 3, x - 1, y - 1, z - 1 );
+   }
+}
+
+template < typename T >
+__global__ void k_from_dofs( TopoDev tp, LevelDev lv, T* __restrict__ slab, const T* __restrict__ dofs )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int p    = lv.xyz[idx];
+   slab[size_t( cell ) * lv.stride + idx] = dofs[canonicalDof( tp, lv, cell, p & 1023, ( p >> 10 ) & 1023, p >> 20 )];
+}
+
+template < typename T >
+__global__ void k_to_dofs( TopoDev tp, LevelDev lv, const T* __restrict__ slab, T* __restrict__ dofs )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int p    = lv.xyz[idx];
+   const int x = p & 1023, y = ( p >> 10 ) & 1023, z = p >> 20;
+   if ( !tp.cls[cell * 16 + classMask( lv.N, x, y, z )].owned )
+      return;
+   dofs[canonicalDof( tp, lv, cell, x, y, z )] = slab[size_t( cell ) * lv.stride + idx];
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-grid CG (CGSolver::solve, src/hyteg/solvers/CGSolver.hpp:66-135, init :237+),
+// identity preconditioner, absolute test sqrt(r.r) < tol, flag Inner|Neumann|Freeslip.
+// The whole iteration runs in ONE thread block (coarse levels hold at most a few
+// thousand DoFs); scalars stay on the device, so it can be captured in a CUDA graph.
+// status[0] = iterations, status[1] = 1 if converged, 2 if the budget ran out.
+// ---------------------------------------------------------------------------
+template < bool VAR >
+__device__ void cgApplyAll( const TopoDev& tp, const LevelDev& lv, const OpDev< double >& op, const double* src,
+                            double* dst, int flag )
+{
+   // interior points
+   const int nInt = lv.nIntCell;
+   for ( int t = threadIdx.x; t < tp.nC * lv.S; t += blockDim.x )
+   {
+      const int cell = t / lv.S, idx = t % lv.S;
+      const int p    = lv.xyz[idx];
+      const int x = p & 1023, y = ( p >> 10 ) & 1023, z = p >> 20;
+      if ( classMask( lv.N, x, y, z ) != 0 )
+         continue;
+      double d = 0, o = 0;
+      partialRow< double, VAR >( op, src + size_t( cell ) * lv.stride, cell, lv.W, x, y, z, d, o );
+      const size_t i = size_t( cell ) * lv.stride + idx;
+      dst[i]         = d * src[i] + o;
+   }
+   (void) nInt;
+   for ( int t = threadIdx.x; t < lv.nBdry; t += blockDim.x )
+   {
+      const BdryPoint pnt = decodeBdry( tp, lv, t );
+      if ( !( primBc( tp, pnt.kind, pnt.prim ) & flag ) )
+         continue;
+      double d = 0, o = 0;
+      bdryRow< double, VAR >( tp, lv, op, src, pnt, d, o );
+      bdryWriteAll( tp, lv, pnt, dst, d * src[bdryReplica< double >( tp, lv, pnt, 0 )] + o );
+   }
+}
+
+__device__ double blockSum( double v, double* red )
+{
+   for ( int o = 16; o > 0; o >>= 1 )
+      v += __shfl_down_sync( 0xffffffffu, v, o );
+   __syncthreads();
+   if ( ( threadIdx.x & 31 ) == 0 )
+      red[threadIdx.x >> 5] = v;
+   __syncthreads();
+   double s = 0;
+   for ( int w = 0; w < int( blockDim.x >> 5 ); ++w )
+      s += red[w];
+   return s;
+}
+
+__device__ double cgDot( const TopoDev& tp, const LevelDev& lv, const double* a, const double* b, int flag, double* red )
+{
+   double v = 0;
+   for ( int t = threadIdx.x; t < tp.nC * lv.S; t += blockDim.x )
+   {
+      const int cell = t / lv.S, idx = t % lv.S;
+      const int p    = lv.xyz[idx];
+      const ClassDev cd = tp.cls[cell * 16 + classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 )];
+      if ( cd.owned && ( cd.bc & flag ) )
+         v += a[size_t( cell ) * lv.stride + idx] * b[size_t( cell ) * lv.stride + idx];
+   }
+   return blockSum( v, red );
+}
+
+// y = a*x + b*y over flagged points of all replicas
+__device__ void cgAxpby( const TopoDev& tp, const LevelDev& lv, double a, const double* x, double b, double* y, int flag )
+{
+   for ( int t = threadIdx.x; t < tp.nC * lv.S; t += blockDim.x )
+   {
+      const int cell = t / lv.S, idx = t % lv.S;
+      const int p    = lv.xyz[idx];
+      if ( !( tp.cls[cell * 16 + classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 )].bc & flag ) )
+         continue;
+      const size_t i = size_t( cell ) * lv.stride + idx;
+      y[i]           = a * x[i] + b * y[i];
+   }
+}
+
+template < bool VAR >
+__global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
+                                                double* r, double* p, double* ap, double tol, int maxIter, int* status )
+{
+   __shared__ double red[32];
+   const int flag = 1 | 4 | 8;
+   cgApplyAll< VAR >( tp, lv, op, x, p, flag );
+   __syncthreads();
+   // r = b - A x ; p = r
+   for ( int t = threadIdx.x; t < tp.nC * lv.S; t += blockDim.x )
+   {
+      const int cell = t / lv.S, idx = t % lv.S;
+      const int pp   = lv.xyz[idx];
+      if ( !( tp.cls[cell * 16 + classMask( lv.N, pp & 1023, ( pp >> 10 ) & 1023, pp >> 20 )].bc & flag ) )
+         continue;
+      const size_t i = size_t( cell ) * lv.stride + idx;
+      r[i]           = b[i] - p[i];
+      p[i]           = r[i];
+   }
+   __syncthreads();
+   double prsold = cgDot( tp, lv, r, r, flag, red );
+   int    it     = 0;
+   int    conv   = sqrt( prsold ) < tol ? 1 : 0;
+   while ( !conv && it < maxIter )
+   {
+      cgApplyAll< VAR >( tp, lv, op, p, ap, flag );
+      __syncthreads();
+      const double pAp   = cgDot( tp, lv, p, ap, flag, red );
+      const double alpha = prsold / pAp;
+      cgAxpby( tp, lv, alpha, p, 1.0, x, flag );
+      cgAxpby( tp, lv, -alpha, ap, 1.0, r, flag );
+      __syncthreads();
+      const double rsnew = cgDot( tp, lv, r, r, flag, red );
+      ++it;
+      if ( sqrt( rsnew ) < tol )
+      {
+         conv = 1;
+         break;
+      }
+      const double beta = rsnew / prsold;
+      cgAxpby( tp, lv, 1.0, r, beta, p, flag );
+      __syncthreads();
+      prsold = rsnew;
+   }
+   if ( threadIdx.x == 0 )
+   {
+      status[0] = it;
+      status[1] = conv ? 1 : 2;
+   }
+}
+
+} // namespace hyb

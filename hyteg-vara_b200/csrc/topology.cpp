@@ -1,0 +1,310 @@
+// Host-side macro-mesh topology (see topology.hpp).
+#include "topology.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <queue>
+#include <set>
+#include <stdexcept>
+
+namespace hyb {
+
+namespace {
+const int kFaceLocal[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+}
+
+void Topology::build( const std::vector< std::array< double, 3 > >& coords, const std::vector< std::array< int, 4 > >& tets )
+{
+   V = coords;
+   T = tets;
+   E.clear();
+   F.clear();
+   edgeId.clear();
+   faceId.clear();
+   for ( auto& t : T )
+      for ( int k = 0; k < 4; ++k )
+      {
+         if ( t[k] < 0 || t[k] >= int( V.size() ) )
+            throw std::invalid_argument( "tetrahedron references a vertex id outside the vertex list" );
+         for ( int j = k + 1; j < 4; ++j )
+            if ( t[j] == t[k] )
+               throw std::invalid_argument( "tetrahedron with repeated vertex" );
+      }
+   // edges and faces keyed by sorted vertex ids, numbered in key order
+   std::set< std::array< int, 2 > > es;
+   std::set< std::array< int, 3 > > fs;
+   for ( auto& t : T )
+   {
+      for ( int a = 0; a < 4; ++a )
+         for ( int b = a + 1; b < 4; ++b )
+            es.insert( { std::min( t[a], t[b] ), std::max( t[a], t[b] ) } );
+      for ( auto& f : kFaceLocal )
+      {
+         std::array< int, 3 > key = { t[f[0]], t[f[1]], t[f[2]] };
+         std::sort( key.begin(), key.end() );
+         fs.insert( key );
+      }
+   }
+   for ( auto& e : es )
+   {
+      edgeId[e] = int( E.size() );
+      E.push_back( e );
+   }
+   for ( auto& f : fs )
+   {
+      faceId[f] = int( F.size() );
+      F.push_back( f );
+   }
+   // embeddings of every lower-dimensional primitive into its adjacent cells,
+   // cells visited in order, so the first embedding is the owning cell
+   vEmb.assign( V.size(), {} );
+   eEmb.assign( E.size(), {} );
+   fEmb.assign( F.size(), {} );
+   for ( int c = 0; c < int( T.size() ); ++c )
+   {
+      const auto& t     = T[c];
+      auto        local = [&]( int v ) {
+         for ( int k = 0; k < 4; ++k )
+            if ( t[k] == v )
+               return uint8_t( k );
+         return uint8_t( 255 );
+      };
+      for ( int k = 0; k < 4; ++k )
+         vEmb[t[k]].push_back( { c, { uint8_t( k ), 0, 0 } } );
+      for ( int a = 0; a < 4; ++a )
+         for ( int b = a + 1; b < 4; ++b )
+         {
+            std::array< int, 2 > key = { std::min( t[a], t[b] ), std::max( t[a], t[b] ) };
+            eEmb[edgeId[key]].push_back( { c, { local( key[0] ), local( key[1] ), 0 } } );
+         }
+      for ( auto& f : kFaceLocal )
+      {
+         std::array< int, 3 > key = { t[f[0]], t[f[1]], t[f[2]] };
+         std::sort( key.begin(), key.end() );
+         fEmb[faceId[key]].push_back( { c, { local( key[0] ), local( key[1] ), local( key[2] ) } } );
+      }
+   }
+   for ( auto& fe : fEmb )
+      if ( fe.size() > 2 )
+         throw std::invalid_argument( "non-manifold mesh: a face with more than two cells" );
+   // boundary flags (SetupPrimitiveStorage::onBoundary, 3D branch: a face with one cell is on
+   // the boundary, and so is every edge and vertex of such a face)
+   vBc.assign( V.size(), kInner );
+   eBc.assign( E.size(), kInner );
+   fBc.assign( F.size(), kInner );
+   for ( size_t f = 0; f < F.size(); ++f )
+      if ( fEmb[f].size() == 1 )
+      {
+         fBc[f] = kDirichlet;
+         const auto& k = F[f];
+         eBc[edgeId[{ k[0], k[1] }]] = kDirichlet;
+         eBc[edgeId[{ k[0], k[2] }]] = kDirichlet;
+         eBc[edgeId[{ k[1], k[2] }]] = kDirichlet;
+         for ( int v : k )
+            vBc[v] = kDirichlet;
+      }
+   // class table
+   cls.assign( T.size(), {} );
+   for ( int c = 0; c < int( T.size() ); ++c )
+   {
+      const auto& t = T[c];
+      for ( int mask = 0; mask < 16; ++mask )
+      {
+         ClassInfo ci{ -1, -1, 0, 0, false };
+         std::vector< int > vs;
+         for ( int k = 0; k < 4; ++k )
+            if ( !( mask & ( 1 << k ) ) )
+               vs.push_back( t[k] );
+         std::sort( vs.begin(), vs.end() );
+         switch ( vs.size() )
+         {
+         case 4:
+            ci = { 3, c, kInner, 1, true };
+            break;
+         case 3: {
+            const int f = faceId.at( { vs[0], vs[1], vs[2] } );
+            ci          = { 2, f, fBc[f], int32_t( fEmb[f].size() ), fEmb[f][0].cell == c };
+            break;
+         }
+         case 2: {
+            const int e = edgeId.at( { vs[0], vs[1] } );
+            ci          = { 1, e, eBc[e], int32_t( eEmb[e].size() ), eEmb[e][0].cell == c };
+            break;
+         }
+         case 1:
+            ci = { 0, vs[0], vBc[vs[0]], int32_t( vEmb[vs[0]].size() ), vEmb[vs[0]][0].cell == c };
+            break;
+         default:
+            break;
+         }
+         cls[c][mask] = ci;
+      }
+   }
+}
+
+int64_t Topology::numDofs( int level ) const
+{
+   const int64_t N = int64_t( 1 ) << level;
+   const int64_t nIntFace = N >= 3 ? ( N - 1 ) * ( N - 2 ) / 2 : 0;
+   const int64_t nIntCell = N >= 4 ? ( N - 3 ) * ( N - 2 ) * ( N - 1 ) / 6 : 0;
+   return int64_t( V.size() ) + int64_t( E.size() ) * std::max< int64_t >( N - 1, 0 ) + int64_t( F.size() ) * nIntFace +
+          int64_t( T.size() ) * nIntCell;
+}
+
+namespace {
+inline int mod( int a, int m ) { return ( ( a % m ) + m ) % m; }
+
+// Constraint of one cell given (possibly partial) labels; -1 = unassigned.
+bool cellOk( const std::array< int, 4 >& l, int m )
+{
+   for ( int a = 0; a < 4; ++a )
+      for ( int b = a + 1; b < 4; ++b )
+         if ( l[a] >= 0 && l[b] >= 0 && mod( l[a] - l[b], m ) == 0 )
+            return false;
+   // the octahedron diagonal (-1,1,-1) couples b0+b2 against b1+b3
+   if ( l[0] >= 0 && l[1] >= 0 && l[2] >= 0 && l[3] >= 0 && mod( l[0] + l[2] - l[1] - l[3], m ) == 0 )
+      return false;
+   return true;
+}
+} // namespace
+
+void Topology::computeColouring( int maxColours )
+{
+   const int nv = int( V.size() );
+   std::vector< std::vector< int > > vCells( nv );
+   for ( int c = 0; c < int( T.size() ); ++c )
+      for ( int k = 0; k < 4; ++k )
+         vCells[T[c][k]].push_back( c );
+   // BFS order over the vertex graph keeps constraints local during backtracking
+   std::vector< std::vector< int > > adj( nv );
+   for ( auto& e : E )
+   {
+      adj[e[0]].push_back( e[1] );
+      adj[e[1]].push_back( e[0] );
+   }
+   std::vector< int > order;
+   std::vector< char > seen( nv, 0 );
+   for ( int s = 0; s < nv; ++s )
+   {
+      if ( seen[s] )
+         continue;
+      std::queue< int > q;
+      q.push( s );
+      seen[s] = 1;
+      while ( !q.empty() )
+      {
+         int v = q.front();
+         q.pop();
+         order.push_back( v );
+         for ( int w : adj[v] )
+            if ( !seen[w] )
+            {
+               seen[w] = 1;
+               q.push( w );
+            }
+      }
+   }
+   for ( int m = 4; m <= maxColours; ++m )
+   {
+      std::vector< int > lab( nv, -1 );
+      std::vector< int > next( nv, 0 );
+      long               budget = 4000000;
+      int                pos    = 0;
+      bool               ok     = false;
+      while ( budget-- > 0 )
+      {
+         if ( pos == nv )
+         {
+            ok = true;
+            break;
+         }
+         if ( pos < 0 )
+            break;
+         const int v = order[pos];
+         bool placed = false;
+         while ( next[pos] < m )
+         {
+            lab[v] = next[pos]++;
+            bool good = true;
+            for ( int c : vCells[v] )
+            {
+               std::array< int, 4 > l = { lab[T[c][0]], lab[T[c][1]], lab[T[c][2]], lab[T[c][3]] };
+               if ( !cellOk( l, m ) )
+               {
+                  good = false;
+                  break;
+               }
+            }
+            if ( good )
+            {
+               placed = true;
+               break;
+            }
+         }
+         if ( placed )
+         {
+            ++pos;
+            if ( pos < nv )
+               next[pos] = 0;
+         }
+         else
+         {
+            lab[v] = -1;
+            next[pos] = 0;
+            --pos;
+         }
+      }
+      if ( ok )
+      {
+         labels  = lab;
+         colours = m;
+         return;
+      }
+   }
+   throw std::runtime_error( "no valid multicolour labelling found" );
+}
+
+bool Topology::colouringValid() const
+{
+   if ( colours < 2 || labels.size() != V.size() )
+      return false;
+   for ( auto& t : T )
+      if ( !cellOk( { labels[t[0]], labels[t[1]], labels[t[2]], labels[t[3]] }, colours ) )
+         return false;
+   return true;
+}
+
+// MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:34-160): vertices with x fastest,
+// six tetrahedra per cube from the hexahedron node table, cells in the lexicographic order
+// of their vertex-id lists (the std::map order in which SetupPrimitiveStorage numbers them).
+void meshCuboid( int nx, int ny, int nz, const double lo[3], const double hi[3], std::vector< std::array< double, 3 > >& V,
+                 std::vector< std::array< int, 4 > >& T )
+{
+   if ( nx < 1 || ny < 1 || nz < 1 )
+      throw std::invalid_argument( "meshCuboid: need at least one cube per direction" );
+   const double hx = ( hi[0] - lo[0] ) / nx, hy = ( hi[1] - lo[1] ) / ny, hz = ( hi[2] - lo[2] ) / nz;
+   V.clear();
+   T.clear();
+   for ( int iz = 0; iz <= nz; ++iz )
+      for ( int iy = 0; iy <= ny; ++iy )
+         for ( int ix = 0; ix <= nx; ++ix )
+            V.push_back( { lo[0] + ix * hx, lo[1] + iy * hy, lo[2] + iz * hz } );
+   const int tNode[6][4] = { { 4, 5, 7, 3 }, { 0, 3, 1, 4 }, { 4, 1, 5, 3 }, { 5, 6, 7, 2 }, { 1, 3, 2, 5 }, { 7, 2, 3, 5 } };
+   const int off[8][3]   = { { 0, 0, 0 }, { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 0, 0, 1 }, { 1, 0, 1 }, { 1, 1, 1 }, { 0, 1, 1 } };
+   auto      vid         = [&]( int i, int j, int k ) { return k * ( nx + 1 ) * ( ny + 1 ) + j * ( nx + 1 ) + i; };
+   std::set< std::array< int, 4 > > cells;
+   for ( int iz = 0; iz < nz; ++iz )
+      for ( int iy = 0; iy < ny; ++iy )
+         for ( int ix = 0; ix < nx; ++ix )
+            for ( auto& tn : tNode )
+            {
+               std::array< int, 4 > c;
+               for ( int m = 0; m < 4; ++m )
+                  c[m] = vid( ix + off[tn[m]][0], iy + off[tn[m]][1], iz + off[tn[m]][2] );
+               cells.insert( c );
+            }
+   T.assign( cells.begin(), cells.end() );
+}
+
+} // namespace hyb

@@ -1,0 +1,349 @@
+"""Python binding of the B200 P1 multigrid C ABI (include/hyteg_b200.h).
+
+Thin ctypes layer over hyteg-vara_b200/libhyteg_b200.so. Class and method names
+follow the reference's C++ API (P1Function, P1ConstantLaplaceOperator,
+P1ElementwiseDivKGradOperator, P1toP1LinearProlongation/Restriction, CGSolver,
+GeometricMultigridSolver). There is no CPU fallback: if the shared library is
+missing or no CUDA device is present, constructing any object raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libhyteg_b200.so")
+
+INNER, DIRICHLET, NEUMANN, FREESLIP, ALL = 1, 2, 4, 8, 15
+REPLACE, ADD = 0, 1
+F64, F32 = 0, 1
+SMOOTHER_SOR, SMOOTHER_JACOBI = 0, 1
+
+# the C ABI symbols (include/hyteg_b200.h); tests check that the library exports all of them
+SYMBOLS = [
+    "hyb_last_error", "hyb_kernel_launch_count", "hyb_storage_create", "hyb_storage_create_cuboid", "hyb_storage_destroy", "hyb_storage_counts",
+    "hyb_storage_num_dofs", "hyb_storage_mesh", "hyb_storage_dof_coords", "hyb_storage_colouring", "hyb_function_create",
+    "hyb_function_destroy", "hyb_function_upload", "hyb_function_download", "hyb_function_upload_device",
+    "hyb_function_download_device", "hyb_function_interpolate_const", "hyb_function_assign", "hyb_function_add",
+    "hyb_function_dot", "hyb_function_copy_convert", "hyb_operator_create_laplace", "hyb_operator_create_divkgrad",
+    "hyb_operator_create_divkgrad_callback", "hyb_operator_destroy", "hyb_operator_apply", "hyb_operator_residual",
+    "hyb_operator_smooth_sor", "hyb_operator_smooth_jac", "hyb_operator_cell_stencil", "hyb_prolongate",
+    "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
+    "hyb_gmg_solve_to_tolerance",
+]
+
+_lib = None
+
+
+class HybError(RuntimeError):
+    pass
+
+
+def load(path=LIB_PATH):
+    """Load the shared library and declare the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise HybError(f"{path} is missing: build it with `python __graft_entry__.py build`")
+    L = ctypes.CDLL(path)
+    P, I, I64, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+    PP = ctypes.POINTER(ctypes.c_void_p)
+    sig = {
+        "hyb_last_error": (ctypes.c_char_p, []),
+        "hyb_kernel_launch_count": (ctypes.c_longlong, []),
+        "hyb_storage_create": (I, [P, I64, P, I64, I, PP]),
+        "hyb_storage_create_cuboid": (I, [I, I, I, P, P, I, PP]),
+        "hyb_storage_destroy": (I, [P]),
+        "hyb_storage_counts": (I, [P, P]),
+        "hyb_storage_num_dofs": (I64, [P, I]),
+        "hyb_storage_mesh": (I, [P, P, P]),
+        "hyb_storage_colouring": (I, [P, P, P]),
+        "hyb_storage_dof_coords": (I, [P, I, P]),
+        "hyb_function_create": (I, [P, I, I, I, PP]),
+        "hyb_function_destroy": (I, [P]),
+        "hyb_function_upload": (I, [P, I, P, P]),
+        "hyb_function_download": (I, [P, I, P, P]),
+        "hyb_function_upload_device": (I, [P, I, P, P]),
+        "hyb_function_download_device": (I, [P, I, P, P]),
+        "hyb_function_interpolate_const": (I, [P, I, D, I, P]),
+        "hyb_function_assign": (I, [P, I, I, P, P, I, P]),
+        "hyb_function_add": (I, [P, I, I, P, P, I, P]),
+        "hyb_function_dot": (I, [P, P, I, I, P, P]),
+        "hyb_function_copy_convert": (I, [P, P, I, P]),
+        "hyb_operator_create_laplace": (I, [P, I, I, PP]),
+        "hyb_operator_create_divkgrad": (I, [P, I, I, P, PP]),
+        "hyb_operator_create_divkgrad_callback": (I, [P, I, I, P, P, PP]),
+        "hyb_operator_destroy": (I, [P]),
+        "hyb_operator_apply": (I, [P, P, P, I, I, I, P]),
+        "hyb_operator_residual": (I, [P, P, P, P, I, I, P]),
+        "hyb_operator_smooth_sor": (I, [P, P, P, D, I, I, P]),
+        "hyb_operator_smooth_jac": (I, [P, P, P, P, D, I, I, P]),
+        "hyb_operator_cell_stencil": (I, [P, I, I, I, P]),
+        "hyb_prolongate": (I, [P, I, I, I, P]),
+        "hyb_restrict": (I, [P, I, I, P]),
+        "hyb_cg_solve": (I, [P, P, P, I, D, I, P, P, P]),
+        "hyb_gmg_create": (I, [P, P, I, I, I, I, D, I, D, I, PP]),
+        "hyb_gmg_destroy": (I, [P]),
+        "hyb_gmg_solve": (I, [P, P, P, I, P]),
+        "hyb_gmg_solve_to_tolerance": (I, [P, P, P, I, D, I, I, P, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def kernel_launch_count():
+    return int(load().hyb_kernel_launch_count())
+
+
+def _check(code):
+    if code != 0:
+        msg = load().hyb_last_error().decode()
+        raise HybError(f"hyteg_b200 error {code}: {msg}")
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _stream(stream):
+    return ctypes.c_void_p(int(stream) if stream else 0)
+
+
+class PrimitiveStorage:
+    """Macro-mesh (vertices, tetrahedra) plus the level hierarchy, resident on the GPU."""
+
+    def __init__(self, coords=None, tets=None, max_level=0, cuboid=None):
+        L = load()
+        h = ctypes.c_void_p()
+        if cuboid is not None:
+            nx, ny, nz, lo, hi = cuboid
+            lo = np.asarray(lo, np.float64)
+            hi = np.asarray(hi, np.float64)
+            _check(L.hyb_storage_create_cuboid(nx, ny, nz, _p(lo), _p(hi), max_level, ctypes.byref(h)))
+        else:
+            c = np.ascontiguousarray(coords, np.float64)
+            t = np.ascontiguousarray(tets, np.int64)
+            _check(L.hyb_storage_create(_p(c), len(c), _p(t), len(t), max_level, ctypes.byref(h)))
+        self.h = h
+        self.max_level = max_level
+
+    @classmethod
+    def cuboid(cls, nx, ny, nz, max_level, lo=(0, 0, 0), hi=(1, 1, 1)):
+        return cls(cuboid=(nx, ny, nz, lo, hi), max_level=max_level)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().hyb_storage_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def counts(self):
+        c = np.zeros(4, np.int64)
+        _check(load().hyb_storage_counts(self.h, _p(c)))
+        return c
+
+    def num_dofs(self, level):
+        return int(load().hyb_storage_num_dofs(self.h, level))
+
+    def mesh(self):
+        c = self.counts()
+        coords = np.zeros((c[0], 3))
+        tets = np.zeros((c[3], 4), np.int64)
+        _check(load().hyb_storage_mesh(self.h, _p(coords), _p(tets)))
+        return coords, tets
+
+    def dof_coords(self, level):
+        out = np.zeros((self.num_dofs(level), 3))
+        _check(load().hyb_storage_dof_coords(self.h, level, _p(out)))
+        return out
+
+    def colouring(self):
+        m = ctypes.c_int()
+        lab = np.zeros(self.counts()[0], np.int32)
+        _check(load().hyb_storage_colouring(self.h, ctypes.byref(m), _p(lab)))
+        return m.value, lab
+
+
+class P1Function:
+    """P1Function<double|float>(name, storage, minLevel, maxLevel)."""
+
+    def __init__(self, name, storage, min_level, max_level, dtype=F64):
+        self.name, self.storage, self.dtype = name, storage, dtype
+        self.min_level, self.max_level = min_level, max_level
+        h = ctypes.c_void_p()
+        _check(load().hyb_function_create(storage.h, min_level, max_level, dtype, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().hyb_function_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def np_dtype(self):
+        return np.float64 if self.dtype == F64 else np.float32
+
+    def set(self, values, level, stream=None):
+        v = np.ascontiguousarray(values, self.np_dtype)
+        assert v.size == self.storage.num_dofs(level)
+        _check(load().hyb_function_upload(self.h, level, _p(v), _stream(stream)))
+
+    def get(self, level, stream=None):
+        out = np.zeros(self.storage.num_dofs(level), self.np_dtype)
+        _check(load().hyb_function_download(self.h, level, _p(out), _stream(stream)))
+        return out
+
+    def set_host_ptr(self, ptr, level, stream=None):
+        """Upload from a raw host pointer (e.g. pinned memory) in the canonical DoF order."""
+        _check(load().hyb_function_upload(self.h, level, ctypes.c_void_p(ptr), _stream(stream)))
+
+    def get_host_ptr(self, ptr, level, stream=None):
+        _check(load().hyb_function_download(self.h, level, ctypes.c_void_p(ptr), _stream(stream)))
+
+    def set_device(self, ptr, level, stream=None):
+        _check(load().hyb_function_upload_device(self.h, level, ctypes.c_void_p(ptr), _stream(stream)))
+
+    def get_device(self, ptr, level, stream=None):
+        _check(load().hyb_function_download_device(self.h, level, ctypes.c_void_p(ptr), _stream(stream)))
+
+    def interpolate(self, value, level, flag=ALL, stream=None):
+        _check(load().hyb_function_interpolate_const(self.h, level, float(value), flag, _stream(stream)))
+
+    def _lincomb(self, fn, scalars, funcs, level, flag, stream):
+        n = len(funcs)
+        sc = np.ascontiguousarray(scalars, np.float64)
+        arr = (ctypes.c_void_p * max(n, 1))(*[f.h.value for f in funcs])
+        _check(fn(self.h, level, n, _p(sc), ctypes.cast(arr, ctypes.c_void_p), flag, _stream(stream)))
+
+    def assign(self, scalars, funcs, level, flag=ALL, stream=None):
+        self._lincomb(load().hyb_function_assign, scalars, funcs, level, flag, stream)
+
+    def add(self, scalars, funcs, level, flag=ALL, stream=None):
+        self._lincomb(load().hyb_function_add, scalars, funcs, level, flag, stream)
+
+    def dot_global(self, other, level, flag=ALL, stream=None):
+        out = ctypes.c_double()
+        _check(load().hyb_function_dot(self.h, other.h, level, flag, ctypes.byref(out), _stream(stream)))
+        return out.value
+
+    def copy_from(self, other, level, stream=None):
+        _check(load().hyb_function_copy_convert(self.h, other.h, level, _stream(stream)))
+
+
+class _Operator:
+    def close(self):
+        if getattr(self, "h", None):
+            load().hyb_operator_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def apply(self, src, dst, level, flag, update=REPLACE, stream=None):
+        _check(load().hyb_operator_apply(self.h, src.h, dst.h, level, flag, update, _stream(stream)))
+
+    def residual(self, x, b, r, level, flag, stream=None):
+        _check(load().hyb_operator_residual(self.h, x.h, b.h, r.h, level, flag, _stream(stream)))
+
+    def smooth_sor(self, dst, rhs, relax, level, flag, stream=None):
+        _check(load().hyb_operator_smooth_sor(self.h, dst.h, rhs.h, float(relax), level, flag, _stream(stream)))
+
+    def smooth_gs(self, dst, rhs, level, flag, stream=None):
+        self.smooth_sor(dst, rhs, 1.0, level, flag, stream)
+
+    def smooth_jac(self, dst, rhs, src, relax, level, flag, stream=None):
+        _check(load().hyb_operator_smooth_jac(self.h, dst.h, rhs.h, src.h, float(relax), level, flag,
+                                              _stream(stream)))
+
+    def cell_stencil(self, level, cell, mask=0):
+        out = np.zeros(15)
+        _check(load().hyb_operator_cell_stencil(self.h, level, cell, mask, _p(out)))
+        return out
+
+
+class P1ConstantLaplaceOperator(_Operator):
+    def __init__(self, storage, min_level, max_level):
+        self.storage = storage
+        h = ctypes.c_void_p()
+        _check(load().hyb_operator_create_laplace(storage.h, min_level, max_level, ctypes.byref(h)))
+        self.h = h
+
+
+class P1ElementwiseDivKGradOperator(_Operator):
+    """P1ElementwiseOperator<p1_div_k_grad_affine_q3>; the coefficient is given by its nodal
+    values on every level (canonical DoF order), i.e. its P1 interpolant."""
+
+    def __init__(self, storage, min_level, max_level, nodal_k):
+        self.storage = storage
+        arrs = [np.ascontiguousarray(k, np.float64) for k in nodal_k]
+        ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        h = ctypes.c_void_p()
+        _check(load().hyb_operator_create_divkgrad(storage.h, min_level, max_level, ctypes.cast(ptrs, ctypes.c_void_p),
+                                                   ctypes.byref(h)))
+        self.h = h
+
+
+class P1toP1LinearProlongation:
+    def prolongate(self, f, source_level, flag, stream=None):
+        _check(load().hyb_prolongate(f.h, source_level, flag, REPLACE, _stream(stream)))
+
+    def prolongate_and_add(self, f, source_level, flag, stream=None):
+        _check(load().hyb_prolongate(f.h, source_level, flag, ADD, _stream(stream)))
+
+
+class P1toP1LinearRestriction:
+    def restrict(self, f, source_level, flag, stream=None):
+        _check(load().hyb_restrict(f.h, source_level, flag, _stream(stream)))
+
+
+class CGSolver:
+    def __init__(self, tolerance=1e-16, max_iter=100000):
+        self.tolerance, self.max_iter = tolerance, max_iter
+
+    def solve(self, A, x, b, level, stream=None):
+        it, conv = ctypes.c_int(), ctypes.c_int()
+        _check(load().hyb_cg_solve(A.h, x.h, b.h, level, self.tolerance, self.max_iter, ctypes.byref(it),
+                                   ctypes.byref(conv), _stream(stream)))
+        return it.value, conv.value == 1
+
+
+class GeometricMultigridSolver:
+    """GeometricMultigridSolver(storage, smoother, coarseSolver, restriction, prolongation,
+    minLevel, maxLevel, preSmooth, postSmooth): solve() performs one V-cycle."""
+
+    def __init__(self, storage, A, min_level, max_level, pre=3, post=3, relax=1.0, smoother=SMOOTHER_SOR,
+                 coarse_tol=1e-12, coarse_max_iter=10000):
+        self.storage, self.A = storage, A
+        h = ctypes.c_void_p()
+        _check(load().hyb_gmg_create(storage.h, A.h, min_level, max_level, pre, post, float(relax), smoother,
+                                     float(coarse_tol), coarse_max_iter, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().hyb_gmg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def solve(self, x, b, level, stream=None):
+        _check(load().hyb_gmg_solve(self.h, x.h, b.h, level, _stream(stream)))
+
+    def solve_to_tolerance(self, x, b, level, rel_tol, max_cycles=100, precision=64, stream=None):
+        hist = np.zeros(max_cycles + 1)
+        cyc = ctypes.c_int()
+        _check(load().hyb_gmg_solve_to_tolerance(self.h, x.h, b.h, level, float(rel_tol), max_cycles, precision,
+                                                 _p(hist), ctypes.byref(cyc), _stream(stream)))
+        return hist[: cyc.value + 1]

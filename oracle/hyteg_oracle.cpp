@@ -643,9 +643,11 @@ found:
    return int( ( ( s % m ) + m ) % m );
 }
 
-// Multicolour SOR: colour(p) = sum_k label(V_k) b_k mod m over the barycentric micro-
-// coordinates; within one colour no two DoFs are coupled, so the update order inside
-// a colour is irrelevant.
+// Multicolour SOR, the ordering the GPU path uses. First the DoFs on macro-faces,
+// -edges and -vertices, by global colour colour(p) = sum_k label(V_k) b_k mod m over the
+// barycentric micro-coordinates (c = 0..m-1); then the macro-cell interiors by the local
+// colour (x + 2y + 3z) mod 4 (c = 0..3). Within one pass no two DoFs are coupled, so the
+// update order inside a pass is irrelevant.
 template < typename T >
 void sorColoredT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag, const int* labels,
                   int m )
@@ -665,26 +667,22 @@ void sorColoredT( const Oracle& o, const Op& op, const Level& lv, T* x, const T*
          fullRow( o, op, lv, d, cur, diag, off );
          sorUpdate( x[d], b[d], diag, off, relax );
       }
+   }
+   for ( int col = 0; col < 4; ++col )
+   {
 #pragma omp parallel for schedule( dynamic, 1 )
       for ( i64 c = 0; c < i64( o.T.size() ); ++c )
-      {
-         const auto& t = o.T[c];
          for ( i64 z = 1; z <= N; ++z )
             for ( i64 y = 1; y <= N - z; ++y )
                for ( i64 xx = 1; xx <= N - y - z - 1; ++xx )
                {
-                  const i64 bb[4] = { N - xx - y - z, xx, y, z };
-                  i64 s = 0;
-                  for ( int k = 0; k < 4; ++k )
-                     s += i64( labels[t[k]] ) * bb[k];
-                  if ( int( ( ( s % m ) + m ) % m ) != col )
+                  if ( ( xx + 2 * y + 3 * z ) % 4 != col )
                      continue;
                   const i64 d = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
                   T diag = 0, off = 0;
                   partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
                   sorUpdate( x[d], b[d], diag, off, relax );
                }
-      }
    }
 }
 

@@ -1,0 +1,268 @@
+"""GPU parity: every operation of the sm_100a path, called through the C ABI, against
+the CPU oracle on the same seeded inputs. FP64 apply / residual / transfers /
+smoothers must agree within 1e-12 relative (max-norm relative to the oracle's
+result); CG and V-cycles within 1e-10."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def H():
+    import hyteg_b200 as H
+
+    H.load()
+    return H
+
+
+def meshes(O):
+    g = np.load(os.path.join(GOLD, "reference_meshes.npz"))
+    out = {
+        "tet_1el": (g["tet_1el_coords"], g["tet_1el_tets"]),
+        "octahedron": (g["regular_octahedron_8el_coords"], g["regular_octahedron_8el_tets"]),
+        "cube1": O.mesh_cuboid(1, 1, 1),
+        "cube211": O.mesh_cuboid(2, 1, 1, hi=(2.0, 1.0, 1.0)),
+    }
+    return out
+
+
+def close(a, b, rtol=RTOL):
+    scale = max(np.abs(b).max(), 1e-300)
+    err = np.abs(a - b).max() / scale
+    assert err <= rtol, f"max relative error {err:.3e} > {rtol:.1e}"
+
+
+@pytest.fixture(scope="module")
+def setups(H, oracle_mod):
+    O = oracle_mod
+    res = {}
+    for name, (c, t) in meshes(O).items():
+        L = 4
+        st = H.PrimitiveStorage(c, t, L)
+        orc = O.Oracle(c, t, L)
+        res[name] = (st, orc, L)
+    return res
+
+
+MESHES = ["tet_1el", "octahedron", "cube1", "cube211"]
+
+
+@pytest.mark.parametrize("name", MESHES)
+def test_roundtrip_and_counts(H, oracle_mod, setups, name):
+    st, orc, L = setups[name]
+    for l in range(L + 1):
+        assert st.num_dofs(l) == orc.n(l)
+    f = H.P1Function("f", st, 0, L)
+    v = np.random.default_rng(1).uniform(-1, 1, orc.n(L))
+    f.set(v, L)
+    assert np.array_equal(f.get(L), v)
+
+
+@pytest.mark.parametrize("name", MESHES)
+@pytest.mark.parametrize("flag", [1, 15, 1 | 4])
+@pytest.mark.parametrize("update", [0, 1])
+def test_apply_matches_oracle(H, oracle_mod, setups, name, flag, update):
+    O = oracle_mod
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    rng = np.random.default_rng(2)
+    for level in range(L + 1):
+        x = rng.uniform(-1, 1, orc.n(level))
+        y0 = rng.uniform(-1, 1, orc.n(level))
+        src, dst = H.P1Function("s", st, 0, L), H.P1Function("d", st, 0, L)
+        src.set(x, level)
+        dst.set(y0, level)
+        A.apply(src, dst, level, flag, update)
+        ref = orc.apply(x, level, flag=flag, dst=y0.copy(), add=bool(update))
+        close(dst.get(level), ref)
+
+
+@pytest.mark.parametrize("name", MESHES)
+def test_stencils_match_oracle(H, setups, name):
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    for level in (1, 3, 4):
+        for c in range(len(st.mesh()[1])):
+            for mask in range(15):
+                close(A.cell_stencil(level, c, mask), orc.cell_stencil(level, c, mask), 1e-13)
+
+
+@pytest.mark.parametrize("name", MESHES)
+def test_residual_matches_oracle(H, setups, name):
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    rng = np.random.default_rng(3)
+    x, b = rng.uniform(-1, 1, orc.n(L)), rng.uniform(-1, 1, orc.n(L))
+    fx, fb, fr = (H.P1Function(n, st, 0, L) for n in "xbr")
+    fx.set(x, L)
+    fb.set(b, L)
+    A.residual(fx, fb, fr, L, 1 | 4)
+    ax = orc.apply(x, L, flag=1 | 4)
+    kind, bc = orc.info(L)
+    ref = np.where((bc & (1 | 4)) != 0, b - ax, 0.0)
+    close(fr.get(L), ref)
+
+
+@pytest.mark.parametrize("name", MESHES)
+@pytest.mark.parametrize("relax", [1.0, 1.3])
+def test_multicolour_sor_matches_oracle(H, oracle_mod, setups, name, relax):
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    m, labels = st.colouring()
+    rng = np.random.default_rng(4)
+    for level in range(1, L + 1):
+        x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+        fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+        fx.set(x, level)
+        fb.set(b, level)
+        for _ in range(2):
+            A.smooth_sor(fx, fb, relax, level, 1 | 4)
+            orc.sor_colored(x, b, level, labels, m, relax=relax, flag=1 | 4)
+        close(fx.get(level), x, 1e-11)
+
+
+@pytest.mark.parametrize("name", MESHES)
+def test_jacobi_matches_oracle(H, setups, name):
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    rng = np.random.default_rng(5)
+    x, b = rng.uniform(-1, 1, orc.n(L)), rng.uniform(-1, 1, orc.n(L))
+    fs, fd, fb = (H.P1Function(n, st, 0, L) for n in "sdb")
+    fs.set(x, L)
+    fd.set(x, L)
+    fb.set(b, L)
+    A.smooth_jac(fd, fb, fs, 0.7, L, 1 | 4)
+    ref = orc.jacobi(x.copy(), b, L, relax=0.7, flag=1 | 4)
+    close(fd.get(L), ref)
+
+
+@pytest.mark.parametrize("name", MESHES)
+@pytest.mark.parametrize("flag", [1 | 4, 15])
+def test_transfers_match_oracle(H, setups, name, flag):
+    st, orc, L = setups[name]
+    P, R = H.P1toP1LinearProlongation(), H.P1toP1LinearRestriction()
+    rng = np.random.default_rng(6)
+    f = H.P1Function("f", st, 0, L)
+    for lc in range(L):
+        coarse, fine0 = rng.uniform(-1, 1, orc.n(lc)), rng.uniform(-1, 1, orc.n(lc + 1))
+        for add in (False, True):
+            f.set(coarse, lc)
+            f.set(fine0, lc + 1)
+            (P.prolongate_and_add if add else P.prolongate)(f, lc, flag)
+            close(f.get(lc + 1), orc.prolongate(coarse, lc, fine=fine0.copy(), flag=flag, add=add))
+        fine, coarse0 = rng.uniform(-1, 1, orc.n(lc + 1)), rng.uniform(-1, 1, orc.n(lc))
+        f.set(fine, lc + 1)
+        f.set(coarse0, lc)
+        R.restrict(f, lc + 1, flag)
+        close(f.get(lc), orc.restrict(fine, lc + 1, coarse=coarse0.copy(), flag=flag))
+
+
+@pytest.mark.parametrize("name", MESHES)
+def test_vector_ops(H, setups, name):
+    st, orc, L = setups[name]
+    kind, bc = orc.info(L)
+    rng = np.random.default_rng(7)
+    a, b, c = (rng.uniform(-1, 1, orc.n(L)) for _ in range(3))
+    fa, fb, fc = (H.P1Function(n, st, 0, L) for n in "abc")
+    fa.set(a, L)
+    fb.set(b, L)
+    fc.set(c, L)
+    for flag in (1, 15, 2):
+        m = (bc & flag) != 0
+        assert abs(fa.dot_global(fb, L, flag) - float(np.sum(a[m] * b[m]))) <= 1e-12 * max(1, np.abs(a * b).sum())
+    fc.assign([2.0, -0.5], [fa, fb], L, flag=1)
+    close(fc.get(L), np.where(bc & 1, 2 * a - 0.5 * b, c))
+    fc.add([3.0], [fa], L, flag=15)
+    close(fc.get(L), np.where(bc & 1, 2 * a - 0.5 * b, c) + 3 * a)
+    fc.interpolate(1.25, L, flag=2)
+    ref = np.where(bc & 1, 2 * a - 0.5 * b, c) + 3 * a
+    ref[(bc & 2) != 0] = 1.25
+    close(fc.get(L), ref)
+
+
+@pytest.mark.parametrize("name", ["octahedron", "cube211"])
+def test_cg_matches_oracle(H, setups, name):
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    level = 2
+    rng = np.random.default_rng(8)
+    b = rng.uniform(-1, 1, orc.n(level))
+    x0 = np.zeros(orc.n(level))
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fx.set(x0, level)
+    fb.set(b, level)
+    it, conv = H.CGSolver(tolerance=1e-12, max_iter=1000).solve(A, fx, fb, level)
+    xr = x0.copy()
+    it_ref = orc.cg(xr, b, level, tol=1e-12, max_iter=1000)
+    assert conv and abs(it - it_ref) <= 2
+    close(fx.get(level), xr, 1e-9)
+
+
+@pytest.mark.parametrize("name", ["octahedron", "cube1", "cube211"])
+def test_vcycle_matches_oracle_multicolour(H, oracle_mod, setups, name):
+    """One GPU V(3,3) cycle == the oracle's V-cycle with the same multicolour SOR."""
+    O = oracle_mod
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    m, labels = st.colouring()
+    xyz = orc.coords_of(L)
+    b = O.uniform_rhs(xyz, 0, 1 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fx.set(np.zeros(orc.n(L)), L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, coarse_tol=1e-14)
+    x = np.zeros(orc.n(L))
+    for cyc in range(2):
+        gmg.solve(fx, fb, L)
+        fb.set(b, L)  # the coarser levels of b are scratch; the finest is untouched
+        orc.gmg(x, b, 0, L, pre=3, post=3, relax=1.0, smoother=1, labels=labels, m=m, coarse_tol=1e-14,
+                max_cycles=1)
+        close(fx.get(L), x, 1e-10)
+
+
+def test_divkgrad_apply_and_sor_match_oracle(H, oracle_mod, setups):
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    kv = [O.grf_coefficient(orc.coords_of(l), seed=1) for l in range(L + 1)]
+    A = H.P1ElementwiseDivKGradOperator(st, 0, L, kv)
+    op = orc.op_divkgrad(kv)
+    m, labels = st.colouring()
+    rng = np.random.default_rng(9)
+    for level in range(L + 1):
+        x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+        fs, fd, fb = (H.P1Function(n, st, 0, L) for n in "sdb")
+        fs.set(x, level)
+        fb.set(b, level)
+        A.apply(fs, fd, level, 15)
+        close(fd.get(level), orc.apply(x, level, flag=15, op=op))
+        if level >= 1:
+            A.smooth_sor(fs, fb, 1.0, level, 1 | 4)
+            xr = orc.sor_colored(x.copy(), b, level, labels, m, flag=1 | 4, op=op)
+            close(fs.get(level), xr, 1e-11)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_gmg_to_tolerance_error_vs_oracle(H, oracle_mod, setups, precision):
+    """Solve to 1e-8 relative residual (plain FP64 and FP32-inner / FP64 refinement) and
+    compare the solution with the oracle's FP64 solve of the same system."""
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    xyz = orc.coords_of(L)
+    b = O.uniform_rhs(xyz, 0, 1 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    hist = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=30, precision=precision)
+    assert hist[-1] <= 1e-8 and len(hist) <= 15
+    x = np.zeros(orc.n(L))
+    _, href = orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=30, rel_tol=1e-12)
+    err = np.abs(fx.get(L) - x).max() / np.abs(x).max()
+    assert err < 1e-6, err

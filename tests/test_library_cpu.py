@@ -1,0 +1,157 @@
+"""CPU-side checks of the product library: it builds for sm_100a, loads, and exports
+every entry point include/hyteg_b200.h declares; the host topology (multicolour
+labelling) is valid on the reference's meshes. No GPU compute is called here."""
+import ctypes
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "hyteg-vara_b200")
+HEADER = os.path.join(ROOT, "include", "hyteg_b200.h")
+
+
+def header_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(hyb_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    sys.path.insert(0, PKG)
+    import build as B
+
+    B.build()
+    import hyteg_b200 as H
+
+    return H.load()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    import hyteg_b200 as H
+
+    syms = header_symbols()
+    assert syms, "no declarations parsed"
+    assert sorted(H.SYMBOLS) == syms
+    for s in syms:
+        assert hasattr(lib, s), s
+    out = subprocess.run(["nm", "-D", "--defined-only", os.path.join(PKG, "libhyteg_b200.so")], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (hyb_[a-z0-9_]+)", out))
+    assert set(syms) <= exported
+
+
+def test_library_is_built_for_sm100a(lib):
+    import build as B
+
+    assert "arch=compute_100a,code=sm_100a" in B.FLAGS
+    assert B.up_to_date()
+
+
+def test_last_error_without_device(lib):
+    # no compute call: only the error channel is exercised
+    assert isinstance(lib.hyb_last_error(), bytes)
+
+
+TOPO_CHECK = r"""
+#include "topology.hpp"
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+using namespace hyb;
+int main( int argc, char** argv )
+{
+   // stdin: nv nt, coords, tets; stdout: colours, valid, nE, nF, then labels
+   long nv, nt;
+   if ( scanf( "%ld %ld", &nv, &nt ) != 2 ) return 2;
+   std::vector< std::array< double, 3 > > V( nv );
+   std::vector< std::array< int, 4 > > T( nt );
+   for ( auto& v : V ) if ( scanf( "%lf %lf %lf", &v[0], &v[1], &v[2] ) != 3 ) return 2;
+   for ( auto& t : T ) if ( scanf( "%d %d %d %d", &t[0], &t[1], &t[2], &t[3] ) != 4 ) return 2;
+   Topology tp;
+   tp.build( V, T );
+   tp.computeColouring();
+   printf( "%d %d %zu %zu\n", tp.colours, tp.colouringValid() ? 1 : 0, tp.E.size(), tp.F.size() );
+   for ( int l : tp.labels ) printf( "%d ", l );
+   printf( "\n" );
+   return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def topo_exe(tmp_path_factory):
+    d = tmp_path_factory.mktemp("topo")
+    src = d / "topo_check.cpp"
+    src.write_text(TOPO_CHECK)
+    exe = d / "topo_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(PKG, "csrc"), str(src),
+                    os.path.join(PKG, "csrc", "topology.cpp"), "-o", str(exe)], check=True)
+    return str(exe)
+
+
+def run_topo(exe, coords, tets):
+    inp = f"{len(coords)} {len(tets)}\n" + "\n".join(" ".join(map(repr, map(float, c))) for c in coords) + "\n" + \
+        "\n".join(" ".join(map(str, t)) for t in tets) + "\n"
+    out = subprocess.run([exe], input=inp, capture_output=True, text=True, check=True).stdout.split("\n")
+    m, valid, ne, nf = map(int, out[0].split())
+    labels = np.array(list(map(int, out[1].split())))
+    return m, valid, ne, nf, labels
+
+
+def colouring_separates_couplings(oracle_mod, coords, tets, labels, m, level=2):
+    """Every pair of micro-vertices coupled by the operator gets different colours."""
+    O = oracle_mod
+    o = O.Oracle(coords, tets, level)
+    n = o.n(level)
+    xyz = o.coords_of(level)
+    # colour of every DoF from its barycentric key in its first cell
+    col = np.full(n, -1)
+    N = 1 << level
+    for c, t in enumerate(tets):
+        cm = o.closure_map(level, c)
+        idx = 0
+        for z in range(N + 1):
+            for y in range(N + 1 - z):
+                for x in range(N + 1 - y - z):
+                    b = (N - x - y - z, x, y, z)
+                    col[cm[idx]] = sum(labels[t[k]] * b[k] for k in range(4)) % m
+                    idx += 1
+    # couplings from the operator: A e_j has nonzeros at the coupled rows
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1.0
+        y = o.apply(e, level, flag=O.ALL)
+        nz = np.nonzero(np.abs(y) > 1e-14)[0]
+        for i in nz:
+            if i != j:
+                assert col[i] != col[j], (i, j)
+    return True
+
+
+@pytest.mark.parametrize("mesh", ["cube1", "cube2", "octahedron", "pyramid"])
+def test_multicolour_labelling_is_valid(topo_exe, oracle_mod, mesh):
+    O = oracle_mod
+    if mesh == "cube1":
+        c, t = O.mesh_cuboid(1, 1, 1)
+    elif mesh == "cube2":
+        c, t = O.mesh_cuboid(2, 2, 2)
+    else:
+        g = np.load(os.path.join(ROOT, "tests", "golden", "reference_meshes.npz"))
+        name = "regular_octahedron_8el" if mesh == "octahedron" else "pyramid_4el"
+        c, t = g[name + "_coords"], g[name + "_tets"]
+    m, valid, ne, nf, labels = run_topo(topo_exe, c, t)
+    assert valid == 1 and m >= 4
+    assert colouring_separates_couplings(O, c, t, labels, m, level=2)
+
+
+def test_topology_counts_match_oracle(topo_exe, oracle_mod):
+    O = oracle_mod
+    c, t = O.mesh_cuboid(2, 2, 2)
+    m, valid, ne, nf, labels = run_topo(topo_exe, c, t)
+    o = O.Oracle(c, t, 0)
+    assert ne == o.num_prims(1) and nf == o.num_prims(2)
