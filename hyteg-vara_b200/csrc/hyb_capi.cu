@@ -129,6 +129,9 @@ struct Storage
 
 inline int stridePad( int s ) { return ( s + 31 ) / 32 * 32; }
 
+template < typename T, bool VAR >
+void initClusterCfg();
+
 void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, const std::vector< std::array< int, 4 > >& T,
                    int maxLevel )
 {
@@ -151,7 +154,7 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
          d.kind  = uint8_t( ci.kind < 0 ? 255 : ci.kind );
          d.bc    = ci.bc;
          d.owned = ci.owned ? 1 : 0;
-         d.invN  = ci.ncells > 0 ? 1.0f / float( ci.ncells ) : 0.0f;
+         d.invN  = ci.ncells > 0 ? 1.0 / double( ci.ncells ) : 0.0;
          // local vertex indices of the primitive's sorted vertices in this cell
          std::vector< std::pair< int, int > > vs;
          for ( int k = 0; k < 4; ++k )
@@ -244,6 +247,10 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
    s.partial.alloc( maxPartial );
    s.scalars.alloc( 64 );
    HYB_CUDA( cudaMallocHost( &s.hostScalar, 64 * sizeof( double ) ) );
+   initClusterCfg< double, false >();
+   initClusterCfg< double, true >();
+   initClusterCfg< float, false >();
+   initClusterCfg< float, true >();
 }
 
 // ---------------------------------------------------------------------------
@@ -597,6 +604,81 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
    HYB_CHECK_LAUNCH();
 }
 
+// Cluster shape of the fused interior SOR kernel, chosen once per instantiation
+// (outside any stream capture): 16 CTAs per cluster where the device allows
+// non-portable sizes, else 8; maxClusters = clusters that fit at once.
+struct ClusterCfg
+{
+   int csize = 0, maxClusters = 0;
+};
+template < typename T, bool VAR >
+ClusterCfg& clusterCfg()
+{
+   static ClusterCfg c;
+   return c;
+}
+constexpr int kClusterThreads = 256;
+
+template < typename T, bool VAR >
+void initClusterCfg()
+{
+   ClusterCfg& cfg = clusterCfg< T, VAR >();
+   if ( cfg.csize != 0 )
+      return;
+   auto kern = k_sor_interior_cluster< T, VAR >;
+   for ( int cs : { 16, 8 } )
+   {
+      if ( cs > 8 && cudaFuncSetAttribute( kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1 ) != cudaSuccess )
+      {
+         cudaGetLastError();
+         continue;
+      }
+      cudaLaunchConfig_t  c{};
+      cudaLaunchAttribute a{};
+      a.id               = cudaLaunchAttributeClusterDimension;
+      a.val.clusterDim.x = cs;
+      a.val.clusterDim.y = 1;
+      a.val.clusterDim.z = 1;
+      c.gridDim          = dim3( cs );
+      c.blockDim         = dim3( kClusterThreads );
+      c.attrs            = &a;
+      c.numAttrs         = 1;
+      int n              = 0;
+      if ( cudaOccupancyMaxActiveClusters( &n, kern, &c ) == cudaSuccess && n > 0 )
+      {
+         cfg.csize       = cs;
+         cfg.maxClusters = n;
+         return;
+      }
+      cudaGetLastError();
+   }
+   cfg.csize = -1; // clusters unavailable: per-colour launches are used
+}
+
+template < typename T, bool VAR >
+bool launchSorInteriorCluster( const Storage& s, const LevelHost& L, const OpDev< T >& od, T* u, const T* rhs, T relax,
+                               cudaStream_t stream )
+{
+   const ClusterCfg& cfg = clusterCfg< T, VAR >();
+   if ( cfg.csize <= 0 )
+      return false;
+   const int           nClusters = std::min( s.td.nC, cfg.maxClusters );
+   cudaLaunchConfig_t  c{};
+   cudaLaunchAttribute a{};
+   a.id               = cudaLaunchAttributeClusterDimension;
+   a.val.clusterDim.x = cfg.csize;
+   a.val.clusterDim.y = 1;
+   a.val.clusterDim.z = 1;
+   c.gridDim          = dim3( nClusters * cfg.csize );
+   c.blockDim         = dim3( kClusterThreads );
+   c.stream           = stream;
+   c.attrs            = &a;
+   c.numAttrs         = 1;
+   HYB_CUDA( cudaLaunchKernelEx( &c, k_sor_interior_cluster< T, VAR >, s.td, L.dev, od, u, rhs, relax ) );
+   HYB_CHECK_LAUNCH();
+   return true;
+}
+
 template < typename T >
 void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream )
 {
@@ -615,7 +697,15 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
             k_sor< T, false ><<< nbd, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, 0, 1 );
          HYB_CHECK_LAUNCH();
       }
-   // interior passes: cell blocks only (no boundary blocks follow them)
+   // interior passes: all four colours in one cluster launch, else one launch per colour
+   // (cell blocks only, no boundary blocks follow them)
+   if ( nc > 0 )
+   {
+      const bool fused = op.variable ? launchSorInteriorCluster< T, true >( s, L, od, u, rhs, relax, stream ) :
+                                       launchSorInteriorCluster< T, false >( s, L, od, u, rhs, relax, stream );
+      if ( fused )
+         return;
+   }
    if ( nc > 0 )
       for ( int c = 0; c < kInteriorColours; ++c )
       {

@@ -29,9 +29,9 @@ struct ClassDev
    uint8_t owned; // this cell holds the canonical replica
    uint8_t k0, k1, k2; // cell-local indices of the primitive's vertices (sorted-id order)
    uint8_t pad;
-   float   invN;  // 1 / #cells adjacent to the primitive
+   double  invN;  // 1 / #cells adjacent to the primitive (exact in FP64 restriction weights)
 };
-static_assert( sizeof( ClassDev ) == 16, "ClassDev layout" );
+static_assert( sizeof( ClassDev ) == 24, "ClassDev layout" );
 
 struct TopoDev
 {

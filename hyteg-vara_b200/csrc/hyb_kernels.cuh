@@ -9,6 +9,8 @@
 // tensor-core path applies.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "hyb_device.cuh"
 
 namespace hyb {
@@ -141,7 +143,19 @@ struct InteriorOp
       }
    }
 
+   // load of u: through L1, or (L2ONLY) straight from L2 for data other CTAs of a
+   // cluster rewrite between cluster barriers
+   template < bool L2ONLY >
+   __device__ __forceinline__ static T ld( const T* p )
+   {
+      if constexpr ( L2ONLY )
+         return __ldcg( p );
+      else
+         return *p;
+   }
+
    // diag and off-diagonal sum at index `base` with neighbour offsets `no`
+   template < bool L2ONLY = false >
    __device__ __forceinline__ void row( const T* __restrict__ u, int base, const NbrOff& no, T& diag, T& off ) const
    {
       if constexpr ( !VAR )
@@ -150,7 +164,7 @@ struct InteriorOp
          T s  = 0;
 #pragma unroll
          for ( int q = 1; q < 15; ++q )
-            s += w[q] * u[base + no.d[q]];
+            s += w[q] * ld< L2ONLY >( u + base + no.d[q] );
          off = s;
       }
       else
@@ -160,7 +174,7 @@ struct InteriorOp
          for ( int q = 0; q < 15; ++q )
          {
             kq[q] = kv[base + no.d[q]];
-            uq[q] = u[base + no.d[q]];
+            uq[q] = ld< L2ONLY >( u + base + no.d[q] );
          }
          T d = 0, s = 0;
 #pragma unroll
@@ -297,6 +311,51 @@ __global__ void __launch_bounds__( 128 ) k_sor( TopoDev tp, LevelDev lv, OpDev< 
    const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
    const T      v  = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
    bdryWriteAll( tp, lv, p, u, v );
+}
+
+// All four interior colour passes of a sweep in ONE launch: a thread-block cluster
+// owns a macro-cell at a time and runs its colours 0..3 with a cluster barrier in
+// between (barrier.cluster arrive.release / wait.acquire), so the cell's slab stays
+// in L2 across the passes and three launches per sweep disappear. Neighbour values
+// are read from L2 (ld.global.cg): other CTAs of the cluster rewrite them between
+// barriers. Clusters never wait on each other.
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 256 ) k_sor_interior_cluster( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                                 const T* __restrict__ rhs, T relax )
+{
+   cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+   const int csize     = int( cluster.num_blocks() );
+   const int crank     = int( cluster.block_rank() );
+   const int nClusters = int( gridDim.x ) / csize;
+   const int clusterId = int( blockIdx.x ) / csize;
+   const int nw        = csize * int( blockDim.x >> 5 );
+   const int gw        = crank * int( blockDim.x >> 5 ) + int( threadIdx.x >> 5 );
+   const int lane      = threadIdx.x & 31;
+   for ( int cell = clusterId; cell < tp.nC; cell += nClusters )
+   {
+      InteriorOp< T, VAR > io;
+      io.load( op, cell );
+      T* __restrict__ uc       = u + size_t( cell ) * lv.stride;
+      const T* __restrict__ bc = rhs + size_t( cell ) * lv.stride;
+      for ( int colour = 0; colour < kInteriorColours; ++colour )
+      {
+         for ( int seg = gw; seg < lv.nSorSeg; seg += nw )
+         {
+            const int32_t sp = lv.sorSeg[seg];
+            const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, g = ( sp >> 20 ) + lane;
+            const int     x0 = 1 + kInteriorColours * g;
+            const int     x  = x0 + ( ( colour - ( ( x0 + 2 * y + 3 * z ) & 3 ) ) & 3 );
+            if ( x + y + z > lv.N - 1 )
+               continue;
+            const int    base = cidx( lv.W, x, y, z );
+            const NbrOff no   = nbrOffsets( lv.W, y, z );
+            T            diag, off;
+            io.template row< true >( uc, base, no, diag, off );
+            uc[base] = ( T( 1 ) - relax ) * __ldcg( uc + base ) + relax * ( bc[base] - off ) / diag;
+         }
+         cluster.sync();
+      }
+   }
 }
 
 // ---------------------------------------------------------------------------
@@ -458,7 +517,7 @@ __global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev cl, in
          if ( valid & ( 1u << q ) )
          {
             const int mq = classMask( Nf, X + offX( q ), Y + offY( q ), Z + offZ( q ) );
-            acc += T( 0.5f * cc[mq].invN ) * f[base + no.d[q]];
+            acc += T( 0.5 * cc[mq].invN ) * f[base + no.d[q]];
          }
    }
    bdryWriteAll( tp, cl, p, coarse, acc );

@@ -261,8 +261,17 @@ def test_gmg_to_tolerance_error_vs_oracle(H, oracle_mod, setups, precision):
     fb.set(b, L)
     gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
     hist = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=30, precision=precision)
-    assert hist[-1] <= 1e-8 and len(hist) <= 15
+    assert hist[-1] <= 1e-8
+    # the reference's SOR ordering (oracle) needs the same number of cycles within one
+    x_ref_order = np.zeros(orc.n(L))
+    _, h_ref = orc.gmg(x_ref_order, b, 0, L, pre=3, post=3, smoother=0, max_cycles=30, rel_tol=1e-8)
+    assert abs((len(hist) - 1) - (len(h_ref) - 1)) <= 1, (hist, h_ref)
+    # per-cycle convergence factors agree with the reference ordering's within 25%
+    f_gpu, f_ref = hist[2:] / hist[1:-1], h_ref[2:] / h_ref[1:-1]
+    k = min(len(f_gpu), len(f_ref))
+    assert np.all(np.abs(f_gpu[:k] - f_ref[:k]) <= 0.25 * f_ref[:k] + 1e-3), (f_gpu, f_ref)
+    # final error against the oracle's FP64 solution of the same system
     x = np.zeros(orc.n(L))
-    _, href = orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=30, rel_tol=1e-12)
+    orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=60, rel_tol=1e-13)
     err = np.abs(fx.get(L) - x).max() / np.abs(x).max()
     assert err < 1e-6, err
