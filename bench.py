@@ -315,6 +315,44 @@ def reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def single_op(args):
+    """Run one level operation repeatedly (for ncu captures of a single kernel):
+    --op apply|residual|sor|sor32|restrict|prolong at --level on the bench mesh."""
+    import torch
+
+    import build as B
+    import hyb_inputs as I
+    import hyteg_b200 as H
+
+    B.build()
+    L, nc = args.level, args.cubes
+    st = H.PrimitiveStorage.cuboid(nc, nc, nc, L)
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    dt = H.F32 if args.op == "sor32" else H.F64
+    u, b, y = (H.P1Function(n, st, 0, L, dt) for n in "uby")
+    for lv in range(L + 1):
+        f = I.uniform_rhs(st.dof_coords(lv), 0, nc << lv)
+        if dt == H.F64:
+            b.set(f, lv)
+            u.set(0.1 * f, lv)
+        else:
+            b.set(f.astype("float32"), lv)
+            u.set((0.1 * f).astype("float32"), lv)
+    F = H.INNER | H.NEUMANN
+    P, R = H.P1toP1LinearProlongation(), H.P1toP1LinearRestriction()
+    ops = {"apply": lambda: A.apply(b, y, L, F), "residual": lambda: A.residual(u, b, y, L, F),
+           "sor": lambda: A.smooth_sor(u, b, 1.0, L, F), "sor32": lambda: A.smooth_sor(u, b, 1.0, L, F),
+           "restrict": lambda: R.restrict(y, L, F), "prolong": lambda: P.prolongate_and_add(u, L - 1, F)}
+    fn = ops[args.op]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fn()
+    torch.cuda.synchronize()
+    print(json.dumps({"op": args.op, "level": L, "dofs": st.num_dofs(L), "reps": args.steps,
+                      "us_per_call_wall": (time.perf_counter() - t0) / args.steps * 1e6}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -324,11 +362,15 @@ def main():
     ap.add_argument("--level", type=int, default=7)
     ap.add_argument("--cubes", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong"],
+                    help="profiling mode: repeat one level operation --steps times")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.op:
+        single_op(args)
+    elif args.impl == "reference":
         reference(args, rank, world)
     else:
         ours(args, rank, world, local_rank)

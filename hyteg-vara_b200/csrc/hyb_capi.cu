@@ -87,16 +87,26 @@ inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s );
 // ---------------------------------------------------------------------------
 struct LevelHost
 {
-   LevelDev          dev{};
-   DevBuf< int32_t > seg, sorSeg, xyz;
-   int               blocksPerCell = 0, sorBlocksPerCell = 0;
-   int               slabBlocks    = 0; // blocks of 256 over one closure
+   LevelDev           dev{};
+   DevBuf< int32_t >  seg, sorSeg, xyz;
+   DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
+   std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
+   int                cellBlocks   = 0;  // grid of the cell-interior loops
+   int                sorCellBlocks = 0;
+   int                bdryBlocks   = 0;  // grid of the surface-DoF loops
+   int                slabBlocks   = 0;  // blocks of 256 over one closure
 };
 
 struct Storage
 {
    Topology                              topo;
    int                                   maxLevel = 0;
+   int                                   numSMs   = 148;
+   // levels up to this one run the four interior SOR colours in one cluster launch;
+   // larger levels use one launch per colour (tuning: HYB_SOR_FUSED_MAX_LEVEL). Measured
+   // on B200 (48 cells, levels 1-7) the per-colour launches are as fast or faster at
+   // every level, so the cluster path is off unless requested.
+   int                                   sorFusedMaxLevel = -1;
    DevBuf< ClassDev >                    cls;
    DevBuf< int32_t >                     fEmb, eEmbOff, eEmb, vEmbOff, vEmb;
    DevBuf< uint8_t >                     fBc, eBc, vBc;
@@ -138,6 +148,13 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
    require( maxLevel >= 0 && maxLevel <= 9, "max_level must be in [0, 9]" );
    require( !T.empty(), "mesh has no tetrahedra" );
    s.maxLevel = maxLevel;
+   {
+      int dev = 0;
+      HYB_CUDA( cudaGetDevice( &dev ) );
+      HYB_CUDA( cudaDeviceGetAttribute( &s.numSMs, cudaDevAttrMultiProcessorCount, dev ) );
+      if ( const char* e = std::getenv( "HYB_SOR_FUSED_MAX_LEVEL" ) )
+         s.sorFusedMaxLevel = std::atoi( e );
+   }
    s.topo.build( V, T );
    s.topo.computeColouring();
    auto& tp = s.topo;
@@ -233,15 +250,56 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       lh->seg.upload( seg );
       lh->sorSeg.upload( sorSeg );
       lh->xyz.upload( xyz );
-      d.nSeg               = int( seg.size() );
-      d.nSorSeg            = int( sorSeg.size() );
-      d.seg                = lh->seg.p;
-      d.sorSeg             = lh->sorSeg.p;
-      d.xyz                = lh->xyz.p;
-      lh->blocksPerCell    = ( d.nSeg + kCellWarps - 1 ) / kCellWarps;
-      lh->sorBlocksPerCell = ( d.nSorSeg + kCellWarps - 1 ) / kCellWarps;
-      lh->slabBlocks       = ( d.S + 255 ) / 256;
-      maxPartial           = std::max( maxPartial, size_t( lh->slabBlocks ) * nC );
+      d.nSeg    = int( seg.size() );
+      d.nSorSeg = int( sorSeg.size() );
+      d.seg     = lh->seg.p;
+      d.sorSeg  = lh->sorSeg.p;
+      d.xyz     = lh->xyz.p;
+      // grids: the loops are grid-stride, so a few resident blocks per SM suffice
+      auto grid = [&]( long work, int perBlock, int perSM ) {
+         return int( std::max< long >( 0, std::min< long >( ( work + perBlock - 1 ) / perBlock, long( s.numSMs ) * perSM ) ) );
+      };
+      lh->cellBlocks    = grid( long( d.nSeg ) * nC, kCellWarps, 16 );
+      lh->sorCellBlocks = grid( long( d.nSorSeg ) * nC, kCellWarps, 16 );
+      lh->bdryBlocks    = grid( bdryLaneCount( nV, nE * ( d.N - 1 ), nF * d.nIntFace ), kBdryThreads, 8 );
+      lh->slabBlocks    = ( d.S + 255 ) / 256;
+      maxPartial        = std::max( maxPartial, size_t( lh->slabBlocks ) * nC );
+      // surface DoFs grouped by SOR colour: colour = sum of label(v) * micro-weight(v) over
+      // the primitive's vertices (the same value in every adjacent cell)
+      {
+         const int                        m = tp.colours, N = d.N;
+         std::vector< std::vector< int > > byColour( m );
+         auto                             col = [&]( long s ) { return int( ( ( s % m ) + m ) % m ); };
+         int                              t   = 0;
+         for ( int v = 0; v < nV; ++v, ++t )
+            byColour[col( long( tp.labels[v] ) * N )].push_back( t );
+         for ( int e = 0; e < nE; ++e )
+            for ( int i = 1; i < N; ++i, ++t )
+               byColour[col( long( tp.labels[tp.E[e][0]] ) * ( N - i ) + long( tp.labels[tp.E[e][1]] ) * i )].push_back( t );
+         for ( int f = 0; f < nF; ++f )
+            for ( int j = 1; j <= N - 2; ++j )
+               for ( int i = 1; i <= N - 1 - j; ++i, ++t )
+                  byColour[col( long( tp.labels[tp.F[f][0]] ) * ( N - i - j ) + long( tp.labels[tp.F[f][1]] ) * i +
+                                long( tp.labels[tp.F[f][2]] ) * j )]
+                      .push_back( t );
+         require( t == d.nBdry, "surface DoF enumeration mismatch" );
+         // per colour: [vertex DoFs | edge DoFs | face DoFs] (ascending t keeps the kinds apart)
+         std::vector< int32_t > flat;
+         lh->colourOff.clear();
+         const int tE = nV, tF = nV + nE * ( N - 1 );
+         for ( auto& v : byColour )
+         {
+            int nv = 0, ne = 0, nf = 0;
+            for ( int tt : v )
+               ( tt < tE ? nv : tt < tF ? ne : nf )++;
+            lh->colourOff.push_back( int( flat.size() ) );
+            lh->colourOff.push_back( nv );
+            lh->colourOff.push_back( ne );
+            lh->colourOff.push_back( nf );
+            flat.insert( flat.end(), v.begin(), v.end() );
+         }
+         lh->colourList.upload( flat );
+      }
       s.lv.push_back( std::move( lh ) );
    }
    s.partial.alloc( maxPartial );
@@ -575,13 +633,12 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
 {
    const Storage& s  = *op.st;
    const auto&    L  = s.L( l );
-   const int      nc = L.blocksPerCell * s.td.nC;
-   const int      nb = nc + bdryBlocks( L.dev );
+   const int      nc = L.dev.nSeg > 0 ? L.cellBlocks : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
    const OpDev< T > od = op.dev< T >( l );
-#define HYB_APPLY( VAR, MODE )                                                                                         \
-   k_apply< T, VAR, MODE ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, flag, nc, L.blocksPerCell )
+#define HYB_APPLY( VAR, MODE ) k_apply< T, VAR, MODE ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, flag, nc )
    if ( op.variable )
    {
       if ( mode == kReplace )
@@ -684,37 +741,43 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
 {
    const Storage&   s  = *op.st;
    const auto&      L  = s.L( l );
-   const int        nc = L.sorBlocksPerCell * s.td.nC;
-   const int        nbd = bdryBlocks( L.dev );
    const OpDev< T > od = op.dev< T >( l );
-   // interface passes: boundary blocks only (nCellBlocks = 0)
-   if ( nbd > 0 )
-      for ( int c = 0; c < s.td.m; ++c )
-      {
-         if ( op.variable )
-            k_sor< T, true ><<< nbd, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, 0, 1 );
-         else
-            k_sor< T, false ><<< nbd, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, 0, 1 );
-         HYB_CHECK_LAUNCH();
-      }
-   // interior passes: all four colours in one cluster launch, else one launch per colour
-   // (cell blocks only, no boundary blocks follow them)
-   if ( nc > 0 )
+   // interface passes: one launch per colour over that colour's surface DoFs
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      const int* co = &L.colourOff[4 * c];
+      const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+      if ( lanes == 0 )
+         continue;
+      const int       nb   = int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) );
+      const int32_t*  list = L.colourList.p + co[0];
+      const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+      if ( op.variable )
+         k_sor_iface< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, bl );
+      else
+         k_sor_iface< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, bl );
+      HYB_CHECK_LAUNCH();
+   }
+   if ( L.dev.nSorSeg == 0 )
+      return;
+   // interior passes: all four colours in one cluster launch on small levels, else one
+   // launch per colour
+   if ( l <= s.sorFusedMaxLevel )
    {
       const bool fused = op.variable ? launchSorInteriorCluster< T, true >( s, L, od, u, rhs, relax, stream ) :
                                        launchSorInteriorCluster< T, false >( s, L, od, u, rhs, relax, stream );
       if ( fused )
          return;
    }
-   if ( nc > 0 )
-      for ( int c = 0; c < kInteriorColours; ++c )
-      {
-         if ( op.variable )
-            k_sor< T, true ><<< nc, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, nc, L.sorBlocksPerCell );
-         else
-            k_sor< T, false ><<< nc, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, c, nc, L.sorBlocksPerCell );
-         HYB_CHECK_LAUNCH();
-      }
+   for ( int c = 0; c < kInteriorColours; ++c )
+   {
+      if ( op.variable )
+         k_sor_interior< T, true ><<< L.sorCellBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c, L.sorCellBlocks );
+      else
+         k_sor_interior< T, false ><<< L.sorCellBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c,
+                                                                            L.sorCellBlocks );
+      HYB_CHECK_LAUNCH();
+   }
 }
 
 template < typename T >
@@ -722,15 +785,15 @@ void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs
 {
    const Storage& s  = *op.st;
    const auto&    L  = s.L( l );
-   const int      nc = L.blocksPerCell * s.td.nC;
-   const int      nb = nc + bdryBlocks( L.dev );
+   const int      nc = L.dev.nSeg > 0 ? L.cellBlocks : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
    const OpDev< T > od = op.dev< T >( l );
    if ( op.variable )
-      k_jacobi< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc, L.blocksPerCell );
+      k_jacobi< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
    else
-      k_jacobi< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc, L.blocksPerCell );
+      k_jacobi< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
    HYB_CHECK_LAUNCH();
 }
 
@@ -739,16 +802,14 @@ void launchProlongate( const Storage& s, int coarseL, const T* coarse, T* fine, 
 {
    const auto& F  = s.L( coarseL + 1 );
    const auto& C  = s.L( coarseL );
-   const int   nc = F.blocksPerCell * s.td.nC;
-   const int   nb = nc + bdryBlocks( F.dev );
+   const int   nc = F.dev.nSeg > 0 ? F.cellBlocks : 0;
+   const int   nb = nc + ( F.dev.nBdry > 0 ? F.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
    if ( add )
-      k_prolongate< T, true ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc,
-                                                          F.blocksPerCell );
+      k_prolongate< T, true ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
    else
-      k_prolongate< T, false ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc,
-                                                           F.blocksPerCell );
+      k_prolongate< T, false ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
    HYB_CHECK_LAUNCH();
 }
 
@@ -757,11 +818,11 @@ void launchRestrict( const Storage& s, int fineL, const T* fine, T* coarse, int 
 {
    const auto& F  = s.L( fineL );
    const auto& C  = s.L( fineL - 1 );
-   const int   nc = C.blocksPerCell * s.td.nC;
-   const int   nb = nc + bdryBlocks( C.dev );
+   const int   nc = C.dev.nSeg > 0 ? C.cellBlocks : 0;
+   const int   nb = nc + ( C.dev.nBdry > 0 ? C.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
-   k_restrict< T ><<< nb, 128, 0, stream >>>( s.td, C.dev, F.dev.W, F.dev.stride, fine, coarse, flag, nc, C.blocksPerCell );
+   k_restrict< T ><<< nb, 128, 0, stream >>>( s.td, C.dev, F.dev.W, F.dev.stride, fine, coarse, flag, nc );
    HYB_CHECK_LAUNCH();
 }
 

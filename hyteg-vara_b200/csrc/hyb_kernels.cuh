@@ -118,6 +118,112 @@ __device__ __forceinline__ void bdryWriteAll( const TopoDev& tp, const LevelDev&
 }
 
 // ---------------------------------------------------------------------------
+// Lane groups for surface DoFs. A DoF on a macro-vertex gets 32 lanes, on a
+// macro-edge 8, on a macro-face 2; lane `sub` of the group handles the adjacent
+// cells e = sub, sub + G, ... and the group reduces with warp shuffles. Each kind's
+// lane range is padded to whole warps, so all lanes of a warp share G and every
+// shuffle is executed by the full warp.
+// ---------------------------------------------------------------------------
+struct BdryLists
+{
+   const int32_t* v; // surface-DoF indices of each kind, or nullptr for the full range
+   const int32_t* e;
+   const int32_t* f;
+   int            nv, ne, nf;
+};
+
+__device__ __forceinline__ BdryLists fullBdryLists( const TopoDev& tp, const LevelDev& lv )
+{
+   return BdryLists{ nullptr, nullptr, nullptr, tp.nV, tp.nE * ( lv.N - 1 ), tp.nF * lv.nIntFace };
+}
+
+__host__ __device__ __forceinline__ long bdryLaneCount( int nv, int ne, int nf )
+{
+   return long( nv ) * 32 + ( long( ne ) * 8 + 31 ) / 32 * 32 + ( long( nf ) * 2 + 31 ) / 32 * 32;
+}
+
+struct LaneTask
+{
+   int  t;      // surface-DoF index in [vertices | edge interiors | face interiors]
+   int  G, sub; // group size and lane within the group
+   bool valid;  // false for padding lanes
+};
+
+__device__ __forceinline__ LaneTask laneTask( const TopoDev& tp, const LevelDev& lv, const BdryLists& bl, long gt )
+{
+   LaneTask  tk{ 0, 32, 0, false };
+   const long nvl = long( bl.nv ) * 32, nel = ( long( bl.ne ) * 8 + 31 ) / 32 * 32;
+   if ( gt < nvl )
+   {
+      const int idx = int( gt >> 5 );
+      tk            = { bl.v ? bl.v[idx] : idx, 32, int( gt & 31 ), true };
+   }
+   else if ( ( gt -= nvl ) < nel )
+   {
+      const int idx = int( gt >> 3 );
+      tk.G          = 8;
+      tk.sub        = int( gt & 7 );
+      tk.valid      = idx < bl.ne;
+      tk.t          = tk.valid ? ( bl.e ? bl.e[idx] : tp.nV + idx ) : 0;
+   }
+   else
+   {
+      gt -= nel;
+      const int idx = int( gt >> 1 );
+      tk.G          = 2;
+      tk.sub        = int( gt & 1 );
+      tk.valid      = idx < bl.nf;
+      tk.t          = tk.valid ? ( bl.f ? bl.f[idx] : tp.nV + tp.nE * ( lv.N - 1 ) + idx ) : 0;
+   }
+   return tk;
+}
+
+template < typename T >
+__device__ __forceinline__ T groupSum( T v, int G )
+{
+   for ( int o = G >> 1; o > 0; o >>= 1 )
+      v += __shfl_xor_sync( 0xffffffffu, v, o );
+   return v;
+}
+
+// Partial rows of the group's adjacent cells, summed over the group (all lanes get it).
+template < typename T, bool VAR >
+__device__ __forceinline__ void bdryRowGroup( const TopoDev& tp, const LevelDev& lv, const OpDev< T >& op, const T* u,
+                                              const BdryPoint& p, const LaneTask& tk, bool active, T& diag, T& off )
+{
+   diag = 0;
+   off  = 0;
+   if ( active )
+   {
+      const int ne = numEmb( tp, p.kind, p.prim );
+      for ( int e = tk.sub; e < ne; e += tk.G )
+      {
+         int c, x, y, z;
+         embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+         partialRow< T, VAR >( op, u + size_t( c ) * lv.stride, c, lv.W, x, y, z, diag, off );
+      }
+   }
+   diag = groupSum( diag, tk.G );
+   off  = groupSum( off, tk.G );
+}
+
+template < typename T >
+__device__ __forceinline__ void bdryWriteGroup( const TopoDev& tp, const LevelDev& lv, const BdryPoint& p,
+                                                const LaneTask& tk, T* dst, T v )
+{
+   const int ne = numEmb( tp, p.kind, p.prim );
+   for ( int e = tk.sub; e < ne; e += tk.G )
+      dst[bdryReplica< T >( tp, lv, p, e )] = v;
+}
+
+// Warp-uniform grid-stride loop over the lanes of the surface-DoF blocks.
+#define HYB_BDRY_LANES( BL )                                                                                         \
+   const long total_ = bdryLaneCount( ( BL ).nv, ( BL ).ne, ( BL ).nf );                                             \
+   const int  nbb_   = int( gridDim.x ) - nCellBlocks;                                                               \
+   for ( long gt = long( int( blockIdx.x ) - nCellBlocks ) * blockDim.x + threadIdx.x;                               \
+         gt - ( threadIdx.x & 31 ) < total_; gt += long( nbb_ ) * blockDim.x )
+
+// ---------------------------------------------------------------------------
 // Interior stencil evaluation with all 15 neighbours inside the cell
 // ---------------------------------------------------------------------------
 template < typename T, bool VAR >
@@ -199,91 +305,134 @@ struct InteriorOp
 };
 
 // ---------------------------------------------------------------------------
+// Work decomposition shared by the level kernels. A launch has nCellBlocks blocks
+// that loop over cell-interior row segments (item = cell * nSeg + seg, one warp per
+// item, consecutive items in the same cell) and gridDim.x - nCellBlocks blocks that
+// loop over surface DoFs (one thread per DoF). Both loops are grid-stride, and the
+// host sizes the grid to a few blocks per SM.
+// ---------------------------------------------------------------------------
+#define HYB_CELL_LOOP( NSEG )                                                                                        \
+   const int wpb_    = int( blockDim.x >> 5 );                                                                       \
+   const int nItems_ = tp.nC * ( NSEG );                                                                             \
+   for ( int it_ = int( blockIdx.x ) * wpb_ + int( threadIdx.x >> 5 ); it_ < nItems_; it_ += nCellBlocks * wpb_ )
+
+// ---------------------------------------------------------------------------
 // apply / residual (P1Operator::apply, P1Operator.hpp:196-324;
 // P1ElementwiseOperator::apply, P1ElementwiseOperator.cpp:64-221)
 // ---------------------------------------------------------------------------
 template < typename T, bool VAR, int MODE >
 __global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
                                                   T* __restrict__ dst, const T* __restrict__ rhs, int flag,
-                                                  int nCellBlocks, int blocksPerCell )
+                                                  int nCellBlocks )
 {
    if ( int( blockIdx.x ) < nCellBlocks )
    {
-      const int cell = blockIdx.x / blocksPerCell;
-      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
-      if ( seg >= lv.nSeg )
-         return;
-      const int32_t sp = lv.seg[seg];
-      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-      if ( x + y + z > lv.N - 1 )
-         return;
-      InteriorOp< T, VAR > io;
-      io.load( op, cell );
-      const size_t co   = size_t( cell ) * lv.stride;
-      const int    base = cidx( lv.W, x, y, z );
-      const NbrOff no   = nbrOffsets( lv.W, y, z );
-      T            diag, off;
-      io.row( src + co, base, no, diag, off );
-      const T ax = diag * src[co + base] + off;
-      if constexpr ( MODE == kReplace )
-         dst[co + base] = ax;
-      else if constexpr ( MODE == kAdd )
-         dst[co + base] += ax;
-      else
-         dst[co + base] = rhs[co + base] - ax;
+      HYB_CELL_LOOP( lv.nSeg )
+      {
+         const int     cell = it_ / lv.nSeg;
+         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
+         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+         if ( x + y + z > lv.N - 1 )
+            continue;
+         InteriorOp< T, VAR > io;
+         io.load( op, cell );
+         const size_t co   = size_t( cell ) * lv.stride;
+         const int    base = cidx( lv.W, x, y, z );
+         const NbrOff no   = nbrOffsets( lv.W, y, z );
+         T            diag, off;
+         io.row( src + co, base, no, diag, off );
+         const T ax = diag * src[co + base] + off;
+         if constexpr ( MODE == kReplace )
+            dst[co + base] = ax;
+         else if constexpr ( MODE == kAdd )
+            dst[co + base] += ax;
+         else
+            dst[co + base] = rhs[co + base] - ax;
+      }
       return;
    }
-   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
-   if ( t >= lv.nBdry )
-      return;
-   const BdryPoint p = decodeBdry( tp, lv, t );
-   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
-      return;
-   T diag = 0, off = 0;
-   bdryRow< T, VAR >( tp, lv, op, src, p, diag, off );
-   const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
-   const T      ax = diag * src[r0] + off;
-   T            v;
-   if constexpr ( MODE == kReplace )
-      v = ax;
-   else if constexpr ( MODE == kAdd )
-      v = dst[r0] + ax;
-   else
-      v = rhs[r0] - ax;
-   bdryWriteAll( tp, lv, p, dst, v );
+   const BdryLists bl = fullBdryLists( tp, lv );
+   HYB_BDRY_LANES( bl )
+   {
+      const LaneTask  tk     = laneTask( tp, lv, bl, gt );
+      const BdryPoint p      = decodeBdry( tp, lv, tk.t );
+      const bool      active = tk.valid && ( primBc( tp, p.kind, p.prim ) & flag );
+      T               diag, off;
+      bdryRowGroup< T, VAR >( tp, lv, op, src, p, tk, active, diag, off );
+      if ( !active )
+         continue;
+      const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+      const T      ax = diag * src[r0] + off;
+      T            v;
+      if constexpr ( MODE == kReplace )
+         v = ax;
+      else if constexpr ( MODE == kAdd )
+         v = dst[r0] + ax;
+      else
+         v = rhs[r0] - ax;
+      // every lane of the group has read dst[r0] before any replica is written
+      __syncwarp( __activemask() );
+      bdryWriteGroup( tp, lv, p, tk, dst, v );
+   }
 }
 
 // ---------------------------------------------------------------------------
 // Multicolour SOR: u <- (1-w) u + w (b - sum_{o!=0} a_o u_o) / a_0 (reference update
 // formula: P1Operator.hpp:1638, sor_3D_macrocell_P1.cpp:31-77). One sweep is
 //   interface passes: DoFs on macro-faces/-edges/-vertices of global colour
-//     sum_k label(V_k) b_k mod m, c = 0..m-1 (boundary blocks only), then
+//     sum_k label(V_k) b_k mod m, c = 0..m-1 (each pass walks a precomputed list of
+//     the surface DoFs of its colour), then
 //   interior passes: macro-cell interior points of local colour (x + 2y + 3z) mod 4,
-//     c = 0..3 (cell blocks only; interiors of different cells are not coupled).
+//     c = 0..3 (interiors of different cells are not coupled).
 // Like the reference's V -> E -> F -> C staging, interfaces are relaxed before the
 // cell interiors. No two DoFs of one pass are coupled.
 // ---------------------------------------------------------------------------
 constexpr int kInteriorColours = 4;
 
 template < typename T, bool VAR >
-__global__ void __launch_bounds__( 128 ) k_sor( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                const T* __restrict__ rhs, T relax, int flag, int colour, int nCellBlocks,
-                                                int blocksPerCell )
+__global__ void __launch_bounds__( 128 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                      const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
 {
-   if ( int( blockIdx.x ) < nCellBlocks )
+   const int nCellBlocks = 0;
+   HYB_BDRY_LANES( bl )
    {
-      const int cell = blockIdx.x / blocksPerCell;
-      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
-      if ( seg >= lv.nSorSeg )
-         return;
-      const int32_t sp = lv.sorSeg[seg];
-      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, g = ( sp >> 20 ) + ( threadIdx.x & 31 );
-      // the one x of colour `colour` in the group [1 + 4g, 1 + 4g + 4)
-      const int x0 = 1 + kInteriorColours * g;
-      const int c0 = ( x0 + 2 * y + 3 * z ) & 3;
-      const int x  = x0 + ( ( colour - c0 ) & 3 );
+      const LaneTask  tk     = laneTask( tp, lv, bl, gt );
+      const BdryPoint p      = decodeBdry( tp, lv, tk.t );
+      const bool      active = tk.valid && ( primBc( tp, p.kind, p.prim ) & flag );
+      T               diag, off;
+      bdryRowGroup< T, VAR >( tp, lv, op, u, p, tk, active, diag, off );
+      if ( !active )
+         continue;
+      const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+      const T      v  = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
+      // all lanes of the group read u[r0] before any replica is written
+      __syncwarp( __activemask() );
+      bdryWriteGroup( tp, lv, p, tk, u, v );
+   }
+}
+
+// the one interior x of colour `colour` in the group [1 + 4g, 1 + 4g + 4) of row (y, z)
+__device__ __forceinline__ int colourX( int g, int y, int z, int colour )
+{
+   const int x0 = 1 + kInteriorColours * g;
+   return x0 + ( ( colour - ( ( x0 + 2 * y + 3 * z ) & 3 ) ) & 3 );
+}
+
+// One interior colour over all cells. Odd colours walk the cells in reverse order, so a
+// pass starts on the data the previous pass touched last (still in L2).
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                         const T* __restrict__ rhs, T relax, int colour, int nCellBlocks )
+{
+   HYB_CELL_LOOP( lv.nSorSeg )
+   {
+      const int     item = ( colour & 1 ) ? nItems_ - 1 - it_ : it_;
+      const int     cell = item / lv.nSorSeg;
+      const int32_t sp   = lv.sorSeg[item - cell * lv.nSorSeg];
+      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023;
+      const int     x = colourX( ( sp >> 20 ) + ( threadIdx.x & 31 ), y, z, colour );
       if ( x + y + z > lv.N - 1 )
-         return;
+         continue;
       InteriorOp< T, VAR > io;
       io.load( op, cell );
       const size_t co   = size_t( cell ) * lv.stride;
@@ -292,25 +441,7 @@ __global__ void __launch_bounds__( 128 ) k_sor( TopoDev tp, LevelDev lv, OpDev< 
       T            diag, off;
       io.row( u + co, base, no, diag, off );
       u[co + base] = ( T( 1 ) - relax ) * u[co + base] + relax * ( rhs[co + base] - off ) / diag;
-      return;
    }
-   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
-   if ( t >= lv.nBdry )
-      return;
-   const BdryPoint p = decodeBdry( tp, lv, t );
-   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
-      return;
-   {
-      int c, x, y, z;
-      embeddingCoords( embAt( tp, p.kind, p.prim, 0 ), p.kind, lv.N, p.i, p.j, c, x, y, z );
-      if ( colourOf( tp, c, lv.N, x, y, z ) != colour )
-         return;
-   }
-   T diag = 0, off = 0;
-   bdryRow< T, VAR >( tp, lv, op, u, p, diag, off );
-   const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
-   const T      v  = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
-   bdryWriteAll( tp, lv, p, u, v );
 }
 
 // All four interior colour passes of a sweep in ONE launch: a thread-block cluster
@@ -342,9 +473,8 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cluster( TopoDev tp, Lev
          for ( int seg = gw; seg < lv.nSorSeg; seg += nw )
          {
             const int32_t sp = lv.sorSeg[seg];
-            const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, g = ( sp >> 20 ) + lane;
-            const int     x0 = 1 + kInteriorColours * g;
-            const int     x  = x0 + ( ( colour - ( ( x0 + 2 * y + 3 * z ) & 3 ) ) & 3 );
+            const int     z = sp & 1023, y = ( sp >> 10 ) & 1023;
+            const int     x = colourX( ( sp >> 20 ) + lane, y, z, colour );
             if ( x + y + z > lv.N - 1 )
                continue;
             const int    base = cidx( lv.W, x, y, z );
@@ -365,40 +495,43 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cluster( TopoDev tp, Lev
 template < typename T, bool VAR >
 __global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
                                                    T* __restrict__ dst, const T* __restrict__ rhs, T relax, int flag,
-                                                   int nCellBlocks, int blocksPerCell )
+                                                   int nCellBlocks )
 {
    if ( int( blockIdx.x ) < nCellBlocks )
    {
-      const int cell = blockIdx.x / blocksPerCell;
-      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
-      if ( seg >= lv.nSeg )
-         return;
-      const int32_t sp = lv.seg[seg];
-      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-      if ( x + y + z > lv.N - 1 )
-         return;
-      InteriorOp< T, VAR > io;
-      io.load( op, cell );
-      const size_t co   = size_t( cell ) * lv.stride;
-      const int    base = cidx( lv.W, x, y, z );
-      const NbrOff no   = nbrOffsets( lv.W, y, z );
-      T            diag, off;
-      io.row( src + co, base, no, diag, off );
-      const T s      = src[co + base];
-      dst[co + base] = s + relax * ( rhs[co + base] - off - diag * s ) / diag;
+      HYB_CELL_LOOP( lv.nSeg )
+      {
+         const int     cell = it_ / lv.nSeg;
+         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
+         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+         if ( x + y + z > lv.N - 1 )
+            continue;
+         InteriorOp< T, VAR > io;
+         io.load( op, cell );
+         const size_t co   = size_t( cell ) * lv.stride;
+         const int    base = cidx( lv.W, x, y, z );
+         const NbrOff no   = nbrOffsets( lv.W, y, z );
+         T            diag, off;
+         io.row( src + co, base, no, diag, off );
+         const T s      = src[co + base];
+         dst[co + base] = s + relax * ( rhs[co + base] - off - diag * s ) / diag;
+      }
       return;
    }
-   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
-   if ( t >= lv.nBdry )
-      return;
-   const BdryPoint p = decodeBdry( tp, lv, t );
-   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
-      return;
-   T diag = 0, off = 0;
-   bdryRow< T, VAR >( tp, lv, op, src, p, diag, off );
-   const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
-   const T      s  = src[r0];
-   bdryWriteAll( tp, lv, p, dst, T( s + relax * ( rhs[r0] - off - diag * s ) / diag ) );
+   const BdryLists bl = fullBdryLists( tp, lv );
+   HYB_BDRY_LANES( bl )
+   {
+      const LaneTask  tk     = laneTask( tp, lv, bl, gt );
+      const BdryPoint p      = decodeBdry( tp, lv, tk.t );
+      const bool      active = tk.valid && ( primBc( tp, p.kind, p.prim ) & flag );
+      T               diag, off;
+      bdryRowGroup< T, VAR >( tp, lv, op, src, p, tk, active, diag, off );
+      if ( !active )
+         continue;
+      const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+      const T      s  = src[r0];
+      bdryWriteGroup( tp, lv, p, tk, dst, T( s + relax * ( rhs[r0] - off - diag * s ) / diag ) );
+   }
 }
 
 // ---------------------------------------------------------------------------
@@ -429,37 +562,41 @@ __device__ __forceinline__ T interpolateFine( const T* __restrict__ coarse, int 
 }
 
 template < typename T, bool ADD >
-__global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev fl, int Wc, int strideC,
+__global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, int Wc, int strideC,
                                                        const T* __restrict__ coarse, T* __restrict__ fine, int flag,
-                                                       int nCellBlocks, int blocksPerCell )
+                                                       int nCellBlocks )
 {
    if ( int( blockIdx.x ) < nCellBlocks )
    {
-      const int cell = blockIdx.x / blocksPerCell;
-      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
-      if ( seg >= fl.nSeg )
-         return;
-      const int32_t sp = fl.seg[seg];
-      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-      if ( x + y + z > fl.N - 1 )
-         return;
-      const T      v  = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
-      const size_t fi = size_t( cell ) * fl.stride + cidx( fl.W, x, y, z );
-      fine[fi]        = ADD ? fine[fi] + v : v;
+      HYB_CELL_LOOP( lv.nSeg )
+      {
+         const int     cell = it_ / lv.nSeg;
+         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
+         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+         if ( x + y + z > lv.N - 1 )
+            continue;
+         const T      v  = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
+         const size_t fi = size_t( cell ) * lv.stride + cidx( lv.W, x, y, z );
+         fine[fi]        = ADD ? fine[fi] + v : v;
+      }
       return;
    }
-   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
-   if ( t >= fl.nBdry )
-      return;
-   const BdryPoint p = decodeBdry( tp, fl, t );
-   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
-      return;
-   int c, x, y, z;
-   embeddingCoords( embAt( tp, p.kind, p.prim, 0 ), p.kind, fl.N, p.i, p.j, c, x, y, z );
-   T v = interpolateFine( coarse + size_t( c ) * strideC, Wc, x, y, z );
-   if ( ADD )
-      v += fine[size_t( c ) * fl.stride + cidx( fl.W, x, y, z )];
-   bdryWriteAll( tp, fl, p, fine, v );
+   const BdryLists bl = fullBdryLists( tp, lv );
+   HYB_BDRY_LANES( bl )
+   {
+      const LaneTask  tk = laneTask( tp, lv, bl, gt );
+      const BdryPoint p  = decodeBdry( tp, lv, tk.t );
+      if ( !tk.valid || !( primBc( tp, p.kind, p.prim ) & flag ) )
+         continue;
+      int c, x, y, z;
+      embeddingCoords( embAt( tp, p.kind, p.prim, 0 ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+      T v = interpolateFine( coarse + size_t( c ) * strideC, Wc, x, y, z );
+      if ( ADD )
+         v += fine[size_t( c ) * lv.stride + cidx( lv.W, x, y, z )];
+      // every lane of the group has read the old value before any replica is written
+      __syncwarp( __activemask() );
+      bdryWriteGroup( tp, lv, p, tk, fine, v );
+   }
 }
 
 // ---------------------------------------------------------------------------
@@ -469,58 +606,64 @@ __global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev fl, 
 // 1/#cells of the primitive it lies on, so every fine point counts exactly once.
 // ---------------------------------------------------------------------------
 template < typename T >
-__global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev cl, int Wf, int strideF, const T* __restrict__ fine,
-                                                     T* __restrict__ coarse, int flag, int nCellBlocks, int blocksPerCell )
+__global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, int Wf, int strideF, const T* __restrict__ fine,
+                                                     T* __restrict__ coarse, int flag, int nCellBlocks )
 {
    if ( int( blockIdx.x ) < nCellBlocks )
    {
-      const int cell = blockIdx.x / blocksPerCell;
-      const int seg  = ( blockIdx.x % blocksPerCell ) * kCellWarps + ( threadIdx.x >> 5 );
-      if ( seg >= cl.nSeg )
-         return;
-      const int32_t sp = cl.seg[seg];
-      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-      if ( x + y + z > cl.N - 1 )
-         return;
-      const T*     f    = fine + size_t( cell ) * strideF;
-      const int    base = cidx( Wf, 2 * x, 2 * y, 2 * z );
-      const NbrOff no   = nbrOffsets( Wf, 2 * y, 2 * z );
-      T            s    = 0;
+      HYB_CELL_LOOP( lv.nSeg )
+      {
+         const int     cell = it_ / lv.nSeg;
+         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
+         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
+         if ( x + y + z > lv.N - 1 )
+            continue;
+         const T*     f    = fine + size_t( cell ) * strideF;
+         const int    base = cidx( Wf, 2 * x, 2 * y, 2 * z );
+         const NbrOff no   = nbrOffsets( Wf, 2 * y, 2 * z );
+         T            s    = 0;
 #pragma unroll
-      for ( int q = 1; q < 15; ++q )
-         s += f[base + no.d[q]];
-      coarse[size_t( cell ) * cl.stride + cidx( cl.W, x, y, z )] = f[base] + T( 0.5 ) * s;
+         for ( int q = 1; q < 15; ++q )
+            s += f[base + no.d[q]];
+         coarse[size_t( cell ) * lv.stride + cidx( lv.W, x, y, z )] = f[base] + T( 0.5 ) * s;
+      }
       return;
    }
-   const int t = ( blockIdx.x - nCellBlocks ) * blockDim.x + threadIdx.x;
-   if ( t >= cl.nBdry )
-      return;
-   const BdryPoint p = decodeBdry( tp, cl, t );
-   if ( !( primBc( tp, p.kind, p.prim ) & flag ) )
-      return;
-   const int Nf = Wf - 1;
-   const int ne = numEmb( tp, p.kind, p.prim );
-   T         acc = 0;
-   for ( int e = 0; e < ne; ++e )
+   const int       Nf = Wf - 1;
+   const BdryLists bl = fullBdryLists( tp, lv );
+   HYB_BDRY_LANES( bl )
    {
-      int c, x, y, z;
-      embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, cl.N, p.i, p.j, c, x, y, z );
-      const int       X = 2 * x, Y = 2 * y, Z = 2 * z;
-      const T*        f = fine + size_t( c ) * strideF;
-      const ClassDev* cc = tp.cls + size_t( c ) * 16;
-      const int       mask = classMask( Nf, X, Y, Z );
-      const uint32_t  valid = kValidOffsets[mask];
-      const int       base  = cidx( Wf, X, Y, Z );
-      const NbrOff    no    = nbrOffsets( Wf, Y, Z );
-      acc += T( cc[mask].invN ) * f[base];
-      for ( int q = 1; q < 15; ++q )
-         if ( valid & ( 1u << q ) )
+      const LaneTask  tk     = laneTask( tp, lv, bl, gt );
+      const BdryPoint p      = decodeBdry( tp, lv, tk.t );
+      const bool      active = tk.valid && ( primBc( tp, p.kind, p.prim ) & flag );
+      T               acc    = 0;
+      if ( active )
+      {
+         const int ne = numEmb( tp, p.kind, p.prim );
+         for ( int e = tk.sub; e < ne; e += tk.G )
          {
-            const int mq = classMask( Nf, X + offX( q ), Y + offY( q ), Z + offZ( q ) );
-            acc += T( 0.5 * cc[mq].invN ) * f[base + no.d[q]];
+            int c, x, y, z;
+            embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+            const int       X = 2 * x, Y = 2 * y, Z = 2 * z;
+            const T*        f     = fine + size_t( c ) * strideF;
+            const ClassDev* cc    = tp.cls + size_t( c ) * 16;
+            const int       mask  = classMask( Nf, X, Y, Z );
+            const uint32_t  valid = kValidOffsets[mask];
+            const int       base  = cidx( Wf, X, Y, Z );
+            const NbrOff    no    = nbrOffsets( Wf, Y, Z );
+            acc += T( cc[mask].invN ) * f[base];
+            for ( int q = 1; q < 15; ++q )
+               if ( valid & ( 1u << q ) )
+               {
+                  const int mq = classMask( Nf, X + offX( q ), Y + offY( q ), Z + offZ( q ) );
+                  acc += T( 0.5 * cc[mq].invN ) * f[base + no.d[q]];
+               }
          }
+      }
+      acc = groupSum( acc, tk.G );
+      if ( active )
+         bdryWriteGroup( tp, lv, p, tk, coarse, acc );
    }
-   bdryWriteAll( tp, cl, p, coarse, acc );
 }
 
 // ---------------------------------------------------------------------------

@@ -139,7 +139,10 @@ class PrimitiveStorage:
 
     def close(self):
         if getattr(self, "h", None):
-            load().hyb_storage_destroy(self.h)
+            try:
+                load().hyb_storage_destroy(self.h)
+            except Exception:  # interpreter shutdown: module globals already gone
+                pass
             self.h = None
 
     def __del__(self):
@@ -184,7 +187,10 @@ class P1Function:
 
     def close(self):
         if getattr(self, "h", None):
-            load().hyb_function_destroy(self.h)
+            try:
+                load().hyb_function_destroy(self.h)
+            except Exception:  # interpreter shutdown: module globals already gone
+                pass
             self.h = None
 
     def __del__(self):
@@ -244,7 +250,10 @@ class P1Function:
 class _Operator:
     def close(self):
         if getattr(self, "h", None):
-            load().hyb_operator_destroy(self.h)
+            try:
+                load().hyb_operator_destroy(self.h)
+            except Exception:  # interpreter shutdown: module globals already gone
+                pass
             self.h = None
 
     def __del__(self):
@@ -332,7 +341,10 @@ class GeometricMultigridSolver:
 
     def close(self):
         if getattr(self, "h", None):
-            load().hyb_gmg_destroy(self.h)
+            try:
+                load().hyb_gmg_destroy(self.h)
+            except Exception:  # interpreter shutdown: module globals already gone
+                pass
             self.h = None
 
     def __del__(self):
