@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1680,6 +1681,76 @@ int hyb_gmg_solve_to_tolerance( hyb_gmg* gh, hyb_function* xh, hyb_function* bh,
    }
    if ( cycles )
       *cycles = cyc;
+   HYB_API_END
+}
+
+} // extern "C"
+
+// ===========================================================================
+// Dot product that allocates nothing
+// ===========================================================================
+// For callers that cannot allocate device memory while they run: a serving loop that
+// admitted its solves against a fixed HBM budget, or a host framework that owns the
+// device allocator and forbids allocations behind its back. The first pass writes one
+// partial sum per thread block into a file-scope device array instead of a buffer the
+// library allocates; the caller passes the inputs and a device pointer for the result.
+namespace hyb {
+
+// 131072 partial sums = 1 MiB. Every GPU that loads this library holds the array until
+// the process exits. A call needs (closure size / 256, rounded up) x (#macro-cells)
+// slots; larger problems are rejected.
+constexpr int kNoAllocSlots = 131072;
+static __device__ __align__( 256 ) double g_noAllocPartial[kNoAllocSlots];
+
+// In host code the array's name is only a host-side stand-in, not a device address: the
+// address is looked up once per device, with that device current.
+double* noAllocScratch()
+{
+   static std::mutex mu;
+   static double*    addr[256] = {};
+   int               dev       = 0;
+   HYB_CUDA( cudaGetDevice( &dev ) );
+   require( dev >= 0 && dev < 256, "device ordinal out of range" );
+   std::lock_guard< std::mutex > lock( mu );
+   if ( !addr[dev] )
+   {
+      void* p = nullptr;
+      HYB_CUDA( cudaGetSymbolAddress( &p, g_noAllocPartial ) );
+      addr[dev] = static_cast< double* >( p );
+   }
+   return addr[dev];
+}
+
+} // namespace hyb
+
+extern "C" {
+
+int hyb_function_dot_noalloc( hyb_function* ah, hyb_function* bh, int level, int flag, double* out_device, void* stream )
+{
+   HYB_API_BEGIN
+   Function *a = FN( ah ), *b = FN( bh );
+   require( out_device, "null result pointer" );
+   sameStorage( a, b );
+   require( a->dtype == b->dtype, "dtypes differ" );
+   checkLevel( a, level );
+   checkLevel( b, level );
+   const Storage& st    = *a->st;
+   const auto&    L     = st.L( level );
+   const long     slots = long( L.slabBlocks ) * st.td.nC;
+   require( slots <= kNoAllocSlots, "problem too large for the no-allocation dot product: needs " +
+                                        std::to_string( slots ) + " scratch slots, the maximum is " +
+                                        std::to_string( kNoAllocSlots ) );
+   double* scratch = noAllocScratch();
+   // every slot the reduction reads is rewritten by the first pass, so nothing is cleared
+   if ( a->dtype == HYB_F64 )
+      k_dot_partial< double ><<< dim3( L.slabBlocks, st.td.nC ), 256, 0, S( stream ) >>>(
+          st.td, L.dev, a->ptr< double >( level ), b->ptr< double >( level ), flag, scratch );
+   else
+      k_dot_partial< float ><<< dim3( L.slabBlocks, st.td.nC ), 256, 0, S( stream ) >>>(
+          st.td, L.dev, a->ptr< float >( level ), b->ptr< float >( level ), flag, scratch );
+   HYB_CHECK_LAUNCH();
+   k_reduce_final<<< 1, 1024, 0, S( stream ) >>>( scratch, int( slots ), out_device );
+   HYB_CHECK_LAUNCH();
    HYB_API_END
 }
 

@@ -30,7 +30,7 @@ SYMBOLS = [
     "hyb_operator_create_divkgrad_callback", "hyb_operator_destroy", "hyb_operator_apply", "hyb_operator_residual",
     "hyb_operator_smooth_sor", "hyb_operator_smooth_jac", "hyb_operator_cell_stencil", "hyb_prolongate",
     "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
-    "hyb_gmg_solve_to_tolerance",
+    "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc",
 ]
 
 _lib = None
@@ -88,6 +88,7 @@ def load(path=LIB_PATH):
         "hyb_gmg_destroy": (I, [P]),
         "hyb_gmg_solve": (I, [P, P, P, I, P]),
         "hyb_gmg_solve_to_tolerance": (I, [P, P, P, I, D, I, I, P, P, P]),
+        "hyb_function_dot_noalloc": (I, [P, P, I, I, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -115,6 +115,17 @@ int hyb_function_add( hyb_function* f, int level, int n, const double* scalars, 
 /* blocking: returns the dot product over the DoFs whose BC is in flag */
 int hyb_function_dot( hyb_function* a, hyb_function* b, int level, int flag, double* out, void* stream );
 int hyb_function_copy_convert( hyb_function* dst, hyb_function* src, int level, void* stream );
+/* Same dot product as hyb_function_dot, for callers that cannot allocate device memory
+ * while they run (a serving loop bound to a fixed HBM budget, a host framework that owns
+ * the allocator). No counterpart in the reference. It allocates nothing: its scratch is
+ * a 1 MiB file-scope device array that every GPU loading this library holds until exit,
+ * so problems needing more than 131072 partial sums ((closure size / 256, rounded up) x
+ * #macro-cells) are rejected with HYB_EINVAL. Asynchronous on `stream`; the result is
+ * written to the device double `out_device`. The first call on a device looks up the
+ * array's device address with that device current; make that first call before any
+ * stream capture. All calls share the array and it keeps the last call's contents:
+ * calls that overlap on the GPU (other streams, other host threads) race. */
+int hyb_function_dot_noalloc( hyb_function* a, hyb_function* b, int level, int flag, double* out_device, void* stream );
 
 /* ---- operators ---- */
 int hyb_operator_create_laplace( hyb_storage* s, int min_level, int max_level, hyb_operator** out );
