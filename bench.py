@@ -223,6 +223,19 @@ def ours(args, rank, world, local_rank):
         return {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 3),
                 "peak_source": peak_kind, "traffic": t_bytes}
 
+    serve = None
+    if not args.no_serve:
+        del y, u32, b32
+        torch.cuda.synchronize()
+        serve = serving(args, H)
+        if world > 1:
+            t = torch.tensor([serve["solves_per_s"], serve["p99_ms"]], dtype=torch.float64, device=dev)
+            s_sum, s_max = t.clone(), t.clone()
+            dist.all_reduce(s_sum, op=dist.ReduceOp.SUM)
+            dist.all_reduce(s_max, op=dist.ReduceOp.MAX)
+            serve["solves_per_s"] = float(s_sum[0].item())
+            serve["p99_ms_max_over_ranks"] = float(s_max[1].item())
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args)
@@ -248,10 +261,69 @@ def ours(args, rank, world, local_rank):
             "roofline_apply": dict(roof(apply_gbs), kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
             "roofline_sor_fp32": dict(roof(sor32_gbs), kernel="k_sor (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def serve_stream(n, rate, seed, levels=(3, 7), cubes=(1, 4)):
+    """Open-loop request stream: Poisson arrivals at `rate` per second; per request a
+    cuboid mesh of c x c x c macro-cubes (c uniform in `cubes`), a level uniform in
+    `levels`, a constant or lognormal coefficient with equal odds, its own seed for f and
+    k; mixed precision to 1e-8."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    t -= t[0]
+    out = []
+    for i in range(n):
+        c = int(rng.integers(cubes[0], cubes[1] + 1))
+        out.append((float(t[i]), (c, c, c, int(rng.integers(levels[0], levels[1] + 1)), int(rng.integers(0, 2)), 32,
+                                  int(rng.integers(1, 1 << 62)))))
+    return out
+
+
+def serving(args, H):
+    """Serving stream at --rate requests/s through the continuous-batching loop. Warm-up:
+    one request of every shape the stream holds, so that hierarchies are resident and
+    their graphs captured before the timed stream (as in a long-running server)."""
+    import numpy as np
+
+    stream = serve_stream(args.serve_requests, args.rate, 1234)
+    sv = H.Server(int(args.serve_budget_gb * (1 << 30)), max_active=args.serve_slots, max_level=7)
+    t0 = time.perf_counter()
+    shapes = sorted({q[:6] for _, q in stream})
+    for i, sh in enumerate(shapes):
+        sv.submit(H.Server.request(*sh, seed=10_000 + i), arrival_s=0.0)
+    sv.run(600)
+    warm_s = time.perf_counter() - t0
+    ids = [sv.submit(H.Server.request(*q), arrival_s=a) for a, q in stream]
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        sv.run(900)
+    res = [sv.result(i) for i in ids]
+    ok = [r for r in res if r.status == 0]
+    lat = np.array([(r.done_s - r.arrival_s) * 1e3 for r in ok])
+    wait = np.array([(r.admit_s - r.arrival_s) * 1e3 for r in ok])
+    makespan = max(r.done_s for r in res) - min(r.arrival_s for r in res)
+    # unknowns (interior micro-vertices) x cycles of the completed solves
+    work = sum((q[0] * (1 << q[3]) - 1) ** 3 * r.cycles for (a, q), r in zip(stream, res) if r.status == 0)
+    stats = sv.stats()
+    sv.close()
+    return {"rate_req_per_s": args.rate, "requests": len(res), "completed": len(ok),
+            "statuses": sorted({r.status for r in res}),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "p50_queue_ms": float(np.percentile(wait, 50)),
+            "solves_per_s": len(ok) / makespan, "makespan_s": makespan,
+            "dof_updates_per_s": work / makespan, "max_rel_residual": max(r.rel_residual for r in ok),
+            "slots": args.serve_slots, "budget_gb": args.serve_budget_gb, "warmup_s": warm_s,
+            "peak_gb": stats["peak_bytes"] / 2 ** 30, "hierarchies_built": stats["hierarchies_built"],
+            "graphs_captured": stats["graphs_captured"], "clocks": clk.summary(),
+            "workload": "Poisson arrivals; c x c x c cubes c~U{1..4}, level~U{3..7}, k constant or lognormal "
+                        "(exp of GRF, corr. 0.2, sigma 1), seeded f, mixed V(3,3) to 1e-8; latency = arrival "
+                        "to result on the host"}
 
 
 def cpu_baseline(args, steps=1):
@@ -362,6 +434,12 @@ def main():
     ap.add_argument("--level", type=int, default=7)
     ap.add_argument("--cubes", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--serve-only", action="store_true", help="run only the serving-stream leg")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving arrival rate, requests/s")
+    ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--serve-slots", type=int, default=16)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong"],
                     help="profiling mode: repeat one level operation --steps times")
     args = ap.parse_args()
@@ -370,6 +448,15 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.op:
         single_op(args)
+    elif args.serve_only:
+        import torch
+
+        import build as B
+        import hyteg_b200 as H
+
+        B.build()
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(serving(args, H)), flush=True)
     elif args.impl == "reference":
         reference(args, rank, world)
     else:

@@ -43,6 +43,9 @@ std::atomic< long long > g_launches{ 0 };
       g_launches.fetch_add( 1, std::memory_order_relaxed );                                                          \
    } while ( 0 )
 
+// Device bytes currently held by this library's buffers and functions (footprint accounting).
+std::atomic< long long > g_deviceBytes{ 0 };
+
 inline void require( bool c, const std::string& msg )
 {
    if ( !c )
@@ -61,7 +64,10 @@ struct DevBuf
    void release()
    {
       if ( p )
+      {
          cudaFree( p );
+         g_deviceBytes.fetch_sub( (long long) ( n * sizeof( T ) ) );
+      }
       p = nullptr;
       n = 0;
    }
@@ -72,6 +78,7 @@ struct DevBuf
          count = 1;
       HYB_CUDA( cudaMalloc( &p, count * sizeof( T ) ) );
       n = count;
+      g_deviceBytes.fetch_add( (long long) ( n * sizeof( T ) ) );
    }
    void upload( const std::vector< T >& v )
    {
@@ -112,6 +119,8 @@ struct Storage
    DevBuf< int32_t >                     fEmb, eEmbOff, eEmb, vEmbOff, vEmb;
    DevBuf< uint8_t >                     fBc, eBc, vBc;
    DevBuf< int8_t >                      labels;
+   DevBuf< double >                      cellCoords; // [nC][4][3] macro-cell vertex coordinates
+   DevBuf< int32_t >                     cellOrder;  // [nC] local vertex indices sorted by global id, 2 bits each
    TopoDev                               td{};
    std::vector< std::unique_ptr< LevelHost > > lv;
    DevBuf< double >                      partial; // dot-product partials
@@ -215,6 +224,20 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       for ( int k = 0; k < 4; ++k )
          lab[4 * c + k] = int8_t( tp.labels[tp.T[c][k]] );
    s.labels.upload( lab );
+   std::vector< double > cc( size_t( nC ) * 12 );
+   for ( int c = 0; c < nC; ++c )
+      for ( int k = 0; k < 4; ++k )
+         for ( int d = 0; d < 3; ++d )
+            cc[size_t( c ) * 12 + 3 * k + d] = tp.V[tp.T[c][k]][d];
+   s.cellCoords.upload( cc );
+   std::vector< int32_t > order( nC );
+   for ( int c = 0; c < nC; ++c )
+   {
+      int k[4] = { 0, 1, 2, 3 };
+      std::sort( k, k + 4, [&]( int a, int b ) { return tp.T[c][a] < tp.T[c][b]; } );
+      order[c] = k[0] | k[1] << 2 | k[2] << 4 | k[3] << 6;
+   }
+   s.cellOrder.upload( order );
    s.td = TopoDev{ nC, nF, nE, nV, s.cls.p, s.fEmb.p, s.eEmbOff.p, s.eEmb.p, s.vEmbOff.p, s.vEmb.p,
                    s.fBc.p, s.eBc.p, s.vBc.p, s.labels.p, tp.colours };
    // per-level tables
@@ -319,13 +342,17 @@ struct Function
 {
    Storage*            st;
    int                 minL, maxL, dtype;
-   std::vector< void* > data; // per level, index l - minL
+   std::vector< void* > data;  // per level, index l - minL
+   std::vector< size_t > bytes; // allocation size per level
 
    ~Function()
    {
-      for ( void* p : data )
-         if ( p )
-            cudaFree( p );
+      for ( size_t i = 0; i < data.size(); ++i )
+         if ( data[i] )
+         {
+            cudaFree( data[i] );
+            g_deviceBytes.fetch_sub( (long long) bytes[i] );
+         }
    }
    size_t elem() const { return dtype == HYB_F64 ? 8 : 4; }
    void*  at( int l ) const
@@ -355,6 +382,8 @@ Function* makeFunction( Storage* s, int minL, int maxL, int dtype )
       void* p = nullptr;
       HYB_CUDA( cudaMalloc( &p, f->levelBytes( l ) ) );
       f->data.push_back( p );
+      f->bytes.push_back( f->levelBytes( l ) );
+      g_deviceBytes.fetch_add( (long long) f->levelBytes( l ) );
       HYB_CUDA( cudaMemset( p, 0, f->levelBytes( l ) ) );
    }
    return f.release();
@@ -510,11 +539,14 @@ Operator* makeLaplace( Storage* s, int minL, int maxL )
 
 template < typename T >
 void launchFromDofs( const Storage& s, int l, T* slab, const T* dofs, cudaStream_t stream );
+template < typename TD, typename TS >
+void launchConvert( const Storage& s, int l, TD* dst, const TS* src, cudaStream_t stream );
 
-Operator* makeDivKGrad( Storage* s, int minL, int maxL, const std::vector< std::vector< double > >& nodalK )
+// The nodal coefficient of level l is written into the FP64 slab by fillK( l, slab ).
+template < typename FillK >
+Operator* makeDivKGradWith( Storage* s, int minL, int maxL, FillK&& fillK )
 {
    require( minL >= 0 && minL <= maxL && maxL <= s->maxLevel, "invalid level range" );
-   require( int( nodalK.size() ) == maxL - minL + 1, "one nodal coefficient vector per level is required" );
    auto op = std::make_unique< Operator >();
    op->st = s;
    op->minL = minL;
@@ -545,17 +577,54 @@ Operator* makeDivKGrad( Storage* s, int minL, int maxL, const std::vector< std::
       b32->upload( f );
       op->K64.push_back( std::move( b64 ) );
       op->K32.push_back( std::move( b32 ) );
-      const auto& kv = nodalK[l - minL];
-      require( int64_t( kv.size() ) == s->topo.numDofs( l ), "nodal coefficient vector has the wrong length" );
-      DevBuf< double > tmp;
-      tmp.upload( kv );
-      launchFromDofs< double >( *s, l, op->kap64->ptr< double >( l ), tmp.p, 0 );
+      fillK( l, op->kap64->ptr< double >( l ) );
       const int n = s->td.nC * s->L( l ).dev.stride;
       k_convert< float, double ><<< ( n + 255 ) / 256, 256 >>>( s->L( l ).dev, op->kap32->ptr< float >( l ),
                                                                  op->kap64->ptr< double >( l ), s->td.nC );
       HYB_CHECK_LAUNCH();
       HYB_CUDA( cudaDeviceSynchronize() );
    }
+   return op.release();
+}
+
+Operator* makeDivKGrad( Storage* s, int minL, int maxL, const std::vector< std::vector< double > >& nodalK )
+{
+   require( int( nodalK.size() ) == maxL - minL + 1, "one nodal coefficient vector per level is required" );
+   return makeDivKGradWith( s, minL, maxL, [&]( int l, double* slab ) {
+      const auto& kv = nodalK[l - minL];
+      require( int64_t( kv.size() ) == s->topo.numDofs( l ), "nodal coefficient vector has the wrong length" );
+      DevBuf< double > tmp;
+      tmp.upload( kv );
+      launchFromDofs< double >( *s, l, slab, tmp.p, 0 );
+   } );
+}
+
+// k = exp( sigma sqrt(2/M) sum_m cos( w_m . x + phase_m ) ) (random Fourier features of a
+// Gaussian random field) written into the operator's nodal coefficient on every level, FP64
+// and its FP32 copy; dW (modes x 3) and dPhase are device arrays. Asynchronous on `stream`;
+// the slabs keep their addresses, so graphs captured with the operator stay valid.
+void fillRff( Operator& op, const double* dW, const double* dPhase, int modes, double sigma, cudaStream_t stream )
+{
+   const Storage& s = *op.st;
+   for ( int l = op.minL; l <= op.maxL; ++l )
+   {
+      const auto& L = s.L( l );
+      k_fill_rff_coefficient< double ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>(
+          s.td, L.dev, s.cellCoords.p, s.cellOrder.p, op.kap64->ptr< double >( l ), dW, dPhase, modes, sigma );
+      HYB_CHECK_LAUNCH();
+      launchConvert< float, double >( s, l, op.kap32->ptr< float >( l ), op.kap64->ptr< double >( l ), stream );
+   }
+}
+
+Operator* makeDivKGradRff( Storage* s, int minL, int maxL, const double* w, const double* phase, int modes, double sigma )
+{
+   require( modes > 0 && w && phase, "random-feature parameters missing" );
+   DevBuf< double > dw, dp;
+   dw.upload( std::vector< double >( w, w + 3 * modes ) );
+   dp.upload( std::vector< double >( phase, phase + modes ) );
+   std::unique_ptr< Operator > op( makeDivKGradWith( s, minL, maxL, []( int, double* ) {} ) );
+   fillRff( *op, dw.p, dp.p, modes, sigma, 0 );
+   HYB_CUDA( cudaDeviceSynchronize() );
    return op.release();
 }
 
@@ -838,15 +907,24 @@ void launchLincomb( const Storage& s, int l, T* dst, int n, const double* sc, co
    HYB_CHECK_LAUNCH();
 }
 
-// dot product into the device scalar slot `slot`
+// dot product into the device double `result`, with one partial sum per block in `partial`
+// (at least maxPartialSlots( s ) doubles)
+template < typename T >
+void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, double* partial, double* result,
+                cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   k_dot_partial< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, a, b, flag, partial );
+   HYB_CHECK_LAUNCH();
+   k_reduce_final<<< 1, 1024, 0, stream >>>( partial, L.slabBlocks * s.td.nC, result );
+   HYB_CHECK_LAUNCH();
+}
+
+// dot product into the storage's device scalar slot `slot`
 template < typename T >
 void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, int slot, cudaStream_t stream )
 {
-   const auto& L = s.L( l );
-   k_dot_partial< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, a, b, flag, s.partial.p );
-   HYB_CHECK_LAUNCH();
-   k_reduce_final<<< 1, 1024, 0, stream >>>( s.partial.p, L.slabBlocks * s.td.nC, s.scalars.p + slot );
-   HYB_CHECK_LAUNCH();
+   launchDot< T >( s, l, a, b, flag, s.partial.p, s.scalars.p + slot, stream );
 }
 
 template < typename TD, typename TS >
@@ -908,6 +986,10 @@ struct Gmg
    std::unique_ptr< Function > r64;           // FP64 residual (mixed precision)
    std::unique_ptr< Function > cx64, cb64;    // FP64 coarse-solve copies of the FP32 hierarchy
    CgScratch                   cg;
+   // reduction scratch of this solver, so that solvers sharing a storage can run on
+   // different streams at the same time: scalars[0] = ||r||^2, scalars[1] = ||b||^2
+   DevBuf< double >            partial, scalars;
+   double*                     hostScalar = nullptr; // pinned, 2 doubles
    cudaStream_t                cap = nullptr; // capture stream
    // captured graphs keyed by (x, b, level, kind)
    struct G
@@ -926,6 +1008,8 @@ struct Gmg
          cudaGraphExecDestroy( g.exec );
       if ( cap )
          cudaStreamDestroy( cap );
+      if ( hostScalar )
+         cudaFreeHost( hostScalar );
    }
 };
 
@@ -1005,7 +1089,7 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
    {
       Function& r = ( kind == kCycle64Norm || kind == kNorm64 ) ? *g.tmp64 : *g.r64;
       launchApply< double >( *g.op, l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ), kGmgFlag, kResidual, s );
-      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, 0, s );
+      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, g.partial.p, g.scalars.p, s );
    }
 }
 
@@ -1019,6 +1103,39 @@ void prepare( Gmg& g )
       g.cg.ap.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
       g.cg.status.alloc( 4 );
    }
+}
+
+void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int post, double relax, int smoother,
+              double coarseTol, int coarseMaxIter )
+{
+   g.st            = s;
+   g.op            = op;
+   g.minL          = minL;
+   g.maxL          = maxL;
+   g.pre           = pre;
+   g.post          = post;
+   g.relax         = relax;
+   g.smoother      = smoother;
+   g.coarseTol     = coarseTol;
+   g.coarseMaxIter = coarseMaxIter;
+   g.tmp64.reset( makeFunction( s, minL, maxL, HYB_F64 ) );
+   g.partial.alloc( s->partial.n );
+   g.scalars.alloc( 2 );
+   HYB_CUDA( cudaMallocHost( &g.hostScalar, 2 * sizeof( double ) ) );
+}
+
+// the FP32 hierarchy and FP64 residual of the mixed-precision solver
+void ensureMixed( Gmg& g )
+{
+   if ( g.x32 )
+      return;
+   Storage* s = g.st;
+   g.x32.reset( makeFunction( s, g.minL, g.maxL, HYB_F32 ) );
+   g.b32.reset( makeFunction( s, g.minL, g.maxL, HYB_F32 ) );
+   g.t32.reset( makeFunction( s, g.minL, g.maxL, HYB_F32 ) );
+   g.r64.reset( makeFunction( s, g.minL, g.maxL, HYB_F64 ) );
+   g.cx64.reset( makeFunction( s, g.minL, g.minL, HYB_F64 ) );
+   g.cb64.reset( makeFunction( s, g.minL, g.minL, HYB_F64 ) );
 }
 
 void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t stream )
@@ -1294,6 +1411,25 @@ int hyb_function_interpolate_const( hyb_function* fh, int level, double value, i
    HYB_API_END
 }
 
+int hyb_function_fill_uniform_random( hyb_function* fh, int level, uint64_t seed, double lattice, void* stream )
+{
+   HYB_API_BEGIN
+   Function* f = FN( fh );
+   require( f, "null argument" );
+   require( lattice > 0.0, "lattice must be positive" );
+   checkLevel( f, level );
+   const Storage& st = *f->st;
+   const auto&    L  = st.L( level );
+   if ( f->dtype == HYB_F64 )
+      k_fill_uniform_hash< double ><<< dim3( L.slabBlocks, st.td.nC ), 256, 0, S( stream ) >>>(
+          st.td, L.dev, st.cellCoords.p, st.cellOrder.p, f->ptr< double >( level ), seed, lattice );
+   else
+      k_fill_uniform_hash< float ><<< dim3( L.slabBlocks, st.td.nC ), 256, 0, S( stream ) >>>(
+          st.td, L.dev, st.cellCoords.p, st.cellOrder.p, f->ptr< float >( level ), seed, lattice );
+   HYB_CHECK_LAUNCH();
+   HYB_API_END
+}
+
 static int lincombApi( hyb_function* fh, int level, int n, const double* sc, hyb_function* const* srcs, int flag,
                        void* stream, bool add )
 {
@@ -1413,6 +1549,16 @@ int hyb_operator_create_divkgrad_callback( hyb_storage* s, int minL, int maxL, d
       k.push_back( std::move( kv ) );
    }
    *out = reinterpret_cast< hyb_operator* >( makeDivKGrad( ST( s ), minL, maxL, k ) );
+   HYB_API_END
+}
+
+int hyb_operator_create_divkgrad_rff( hyb_storage* s, int minL, int maxL, const double* w, const double* phase,
+                                      int modes, double sigma, hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && w && phase && out, "null argument" );
+   require( modes > 0 && modes <= 4096, "modes must be in [1, 4096]" );
+   *out = reinterpret_cast< hyb_operator* >( makeDivKGradRff( ST( s ), minL, maxL, w, phase, modes, sigma ) );
    HYB_API_END
 }
 
@@ -1594,17 +1740,7 @@ int hyb_gmg_create( hyb_storage* s, hyb_operator* oh, int minL, int maxL, int pr
    require( pre >= 0 && post >= 0, "smoothing steps must be non-negative" );
    require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI, "unknown smoother" );
    auto g = std::make_unique< hyb_gmg_s >();
-   g->st = ST( s );
-   g->op = op;
-   g->minL = minL;
-   g->maxL = maxL;
-   g->pre = pre;
-   g->post = post;
-   g->relax = relax;
-   g->smoother = smoother;
-   g->coarseTol = coarseTol;
-   g->coarseMaxIter = coarseMaxIter;
-   g->tmp64.reset( makeFunction( ST( s ), minL, maxL, HYB_F64 ) );
+   initGmg( *g, ST( s ), op, minL, maxL, pre, post, relax, smoother, coarseTol, coarseMaxIter );
    *out = g.release();
    HYB_API_END
 }
@@ -1647,32 +1783,25 @@ int hyb_gmg_solve_to_tolerance( hyb_gmg* gh, hyb_function* xh, hyb_function* bh,
    require( maxCycles >= 0, "max_cycles must be non-negative" );
    cudaStream_t s = S( stream );
    Storage&     st = *g->st;
-   if ( precision == 32 && !g->x32 )
-   {
-      g->x32.reset( makeFunction( &st, g->minL, g->maxL, HYB_F32 ) );
-      g->b32.reset( makeFunction( &st, g->minL, g->maxL, HYB_F32 ) );
-      g->t32.reset( makeFunction( &st, g->minL, g->maxL, HYB_F32 ) );
-      g->r64.reset( makeFunction( &st, g->minL, g->maxL, HYB_F64 ) );
-      g->cx64.reset( makeFunction( &st, g->minL, g->minL, HYB_F64 ) );
-      g->cb64.reset( makeFunction( &st, g->minL, g->minL, HYB_F64 ) );
-   }
+   if ( precision == 32 )
+      ensureMixed( *g );
    // ||b|| and the initial residual
-   launchDot< double >( st, level, b->ptr< double >( level ), b->ptr< double >( level ), kGmgFlag, 2, s );
-   HYB_CUDA( cudaMemcpyAsync( st.hostScalar + 2, st.scalars.p + 2, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
+   launchDot< double >( st, level, b->ptr< double >( level ), b->ptr< double >( level ), kGmgFlag, g->partial.p,
+                        g->scalars.p + 1, s );
    runGraph( *g, *x, *b, level, precision == 64 ? kNorm64 : kNormMixed, s );
-   HYB_CUDA( cudaMemcpyAsync( st.hostScalar, st.scalars.p, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
+   HYB_CUDA( cudaMemcpyAsync( g->hostScalar, g->scalars.p, 2 * sizeof( double ), cudaMemcpyDeviceToHost, s ) );
    HYB_CUDA( cudaStreamSynchronize( s ) );
-   const double nb  = std::sqrt( st.hostScalar[2] ) > 0 ? std::sqrt( st.hostScalar[2] ) : 1.0;
-   double       rel = std::sqrt( st.hostScalar[0] ) / nb;
+   const double nb  = std::sqrt( g->hostScalar[1] ) > 0 ? std::sqrt( g->hostScalar[1] ) : 1.0;
+   double       rel = std::sqrt( g->hostScalar[0] ) / nb;
    if ( history )
       history[0] = rel;
    int cyc = 0;
    while ( cyc < maxCycles && rel > relTol )
    {
       runGraph( *g, *x, *b, level, precision == 64 ? kCycle64Norm : kMixedStep, s );
-      HYB_CUDA( cudaMemcpyAsync( st.hostScalar, st.scalars.p, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
+      HYB_CUDA( cudaMemcpyAsync( g->hostScalar, g->scalars.p, sizeof( double ), cudaMemcpyDeviceToHost, s ) );
       HYB_CUDA( cudaStreamSynchronize( s ) );
-      rel = std::sqrt( st.hostScalar[0] ) / nb;
+      rel = std::sqrt( g->hostScalar[0] ) / nb;
       ++cyc;
       if ( history )
          history[cyc] = rel;
@@ -1755,3 +1884,8 @@ int hyb_function_dot_noalloc( hyb_function* ah, hyb_function* bh, int level, int
 }
 
 } // extern "C"
+
+// ===========================================================================
+// Serving loop
+// ===========================================================================
+#include "hyb_server.inl"

@@ -693,6 +693,84 @@ __global__ void k_lincomb( TopoDev tp, LevelDev lv, T* __restrict__ dst, int n, 
    dst[i] = v;
 }
 
+// ---------------------------------------------------------------------------
+// Seeded synthetic inputs evaluated on the device at every closure point (replicas get
+// identical values: they depend on the position only).
+//   * uniform right-hand side: f ~ U[-1,1] from a SplitMix64 hash of the point's integer
+//     position on the lattice of spacing 1/lattice and the seed;
+//   * random-Fourier-feature coefficient: k = exp( sigma sqrt(2/M) sum_m cos(w_m . x + p_m) ).
+// Cell geometry: cellCoords[c] = 4 vertices x 3 in the cell's local order; cellOrder[c] packs
+// the local indices of the vertices sorted by global id (2 bits each). The position is the
+// barycentric sum taken in global vertex order, so every replica of a shared point (whose
+// weights on the other vertices are exactly zero) evaluates the same expression and gets
+// the same bits.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void closurePosition( const double* __restrict__ cellCoords,
+                                                 const int32_t* __restrict__ cellOrder, int cell, int N, int x, int y,
+                                                 int z, double p[3] )
+{
+   const double* v     = cellCoords + size_t( cell ) * 12;
+   const int     order = cellOrder[cell];
+   const double  b[4]  = { double( N - x - y - z ), double( x ), double( y ), double( z ) };
+   for ( int d = 0; d < 3; ++d )
+   {
+      double acc = 0.0;
+      for ( int j = 0; j < 4; ++j )
+      {
+         const int k = ( order >> ( 2 * j ) ) & 3;
+         acc += b[k] * v[3 * k + d];
+      }
+      p[d] = acc / N;
+   }
+}
+
+__device__ __forceinline__ uint64_t splitmix64( uint64_t x )
+{
+   x += 0x9E3779B97F4A7C15ull;
+   uint64_t z = x;
+   z          = ( z ^ ( z >> 30 ) ) * 0xBF58476D1CE4E5B9ull;
+   z          = ( z ^ ( z >> 27 ) ) * 0x94D049BB133111EBull;
+   return z ^ ( z >> 31 );
+}
+
+template < typename T >
+__global__ void k_fill_uniform_hash( TopoDev tp, LevelDev lv, const double* __restrict__ cellCoords,
+                                     const int32_t* __restrict__ cellOrder, T* __restrict__ dst, uint64_t seed,
+                                     double lattice )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int pk   = lv.xyz[idx];
+   double    p[3];
+   closurePosition( cellCoords, cellOrder, cell, lv.N, pk & 1023, ( pk >> 10 ) & 1023, pk >> 20, p );
+   const uint64_t kx = uint64_t( llrint( p[0] * lattice ) ), ky = uint64_t( llrint( p[1] * lattice ) ),
+                  kz = uint64_t( llrint( p[2] * lattice ) );
+   const uint64_t key = ( kx * 1000003ull + ky ) * 1000033ull + kz;
+   const uint64_t h   = splitmix64( key ^ ( seed * 0xD1B54A32D192ED03ull ) );
+   dst[size_t( cell ) * lv.stride + idx] = T( double( h >> 11 ) / 9007199254740992.0 * 2.0 - 1.0 );
+}
+
+template < typename T >
+__global__ void k_fill_rff_coefficient( TopoDev tp, LevelDev lv, const double* __restrict__ cellCoords,
+                                        const int32_t* __restrict__ cellOrder, T* __restrict__ dst,
+                                        const double* __restrict__ w, const double* __restrict__ phase, int modes,
+                                        double sigma )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int pk   = lv.xyz[idx];
+   double    p[3];
+   closurePosition( cellCoords, cellOrder, cell, lv.N, pk & 1023, ( pk >> 10 ) & 1023, pk >> 20, p );
+   double g = 0;
+   for ( int m = 0; m < modes; ++m )
+      g += cos( w[3 * m] * p[0] + w[3 * m + 1] * p[1] + w[3 * m + 2] * p[2] + phase[m] );
+   dst[size_t( cell ) * lv.stride + idx] = T( exp( sigma * sqrt( 2.0 / modes ) * g ) );
+}
+
 // VertexDoFFunction::interpolate(constant, level, flag)
 template < typename T >
 __global__ void k_fill( TopoDev tp, LevelDev lv, T* __restrict__ dst, T value, int flag )

@@ -56,9 +56,16 @@ def uniform_rhs(xyz, seed, lattice):
     return (h >> np.uint64(11)).astype(np.float64) / float(1 << 53) * 2.0 - 1.0
 
 
-def grf_coefficient(xyz, corr_len=0.2, sigma=1.0, seed=1, modes=64):
+def grf_features(corr_len=0.2, seed=1, modes=64):
+    """Random Fourier features (wave vectors ~ N(0, 1/corr_len^2), phases ~ U[0, 2 pi)) of a
+    Gaussian random field with a squared-exponential covariance of length corr_len."""
     rng = np.random.default_rng(seed)
     w = rng.normal(0.0, 1.0 / corr_len, size=(modes, 3))
     ph = rng.uniform(0.0, 2.0 * np.pi, size=modes)
+    return w, ph
+
+
+def grf_coefficient(xyz, corr_len=0.2, sigma=1.0, seed=1, modes=64):
+    w, ph = grf_features(corr_len, seed, modes)
     g = sigma * np.sqrt(2.0 / modes) * np.cos(np.asarray(xyz) @ w.T + ph).sum(axis=1)
     return np.exp(g)

@@ -30,8 +30,25 @@ SYMBOLS = [
     "hyb_operator_create_divkgrad_callback", "hyb_operator_destroy", "hyb_operator_apply", "hyb_operator_residual",
     "hyb_operator_smooth_sor", "hyb_operator_smooth_jac", "hyb_operator_cell_stencil", "hyb_prolongate",
     "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
-    "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc",
+    "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
+    "hyb_operator_create_divkgrad_rff", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
+    "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
 ]
+
+COEFF_CONSTANT, COEFF_LOGNORMAL = 0, 1
+
+
+class Request(ctypes.Structure):
+    """hyb_request: one Poisson solve on the unit cube split into nx x ny x nz macro-cubes."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("level", ctypes.c_int),
+                ("coefficient", ctypes.c_int), ("precision", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("rel_tol", ctypes.c_double), ("max_cycles", ctypes.c_int)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("cycles", ctypes.c_int), ("rel_residual", ctypes.c_double),
+                ("arrival_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("footprint_bytes", ctypes.c_size_t)]
 
 _lib = None
 
@@ -89,6 +106,16 @@ def load(path=LIB_PATH):
         "hyb_gmg_solve": (I, [P, P, P, I, P]),
         "hyb_gmg_solve_to_tolerance": (I, [P, P, P, I, D, I, I, P, P, P]),
         "hyb_function_dot_noalloc": (I, [P, P, I, I, P, P]),
+        "hyb_function_fill_uniform_random": (I, [P, I, ctypes.c_uint64, D, P]),
+        "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, PP]),
+        "hyb_server_create": (I, [ctypes.c_size_t, I, I, PP]),
+        "hyb_server_destroy": (I, [P]),
+        "hyb_server_footprint": (I, [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
+        "hyb_server_submit": (I, [P, ctypes.POINTER(Request), D, P, ctypes.POINTER(I)]),
+        "hyb_server_run": (I, [P, D]),
+        "hyb_server_result": (I, [P, I, ctypes.POINTER(RequestResult)]),
+        "hyb_server_stats": (I, [P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "hyb_rff_features": (I, [ctypes.c_uint64, D, I, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -227,6 +254,11 @@ class P1Function:
     def interpolate(self, value, level, flag=ALL, stream=None):
         _check(load().hyb_function_interpolate_const(self.h, level, float(value), flag, _stream(stream)))
 
+    def fill_uniform_random(self, level, seed, lattice, stream=None):
+        """Seeded U[-1,1) values from a hash of each DoF's lattice position (device side;
+        equals hyb_inputs.uniform_rhs on the DoF coordinates)."""
+        _check(load().hyb_function_fill_uniform_random(self.h, level, int(seed), float(lattice), _stream(stream)))
+
     def _lincomb(self, fn, scalars, funcs, level, flag, stream):
         n = len(funcs)
         sc = np.ascontiguousarray(scalars, np.float64)
@@ -303,6 +335,20 @@ class P1ElementwiseDivKGradOperator(_Operator):
                                                    ctypes.byref(h)))
         self.h = h
 
+    @classmethod
+    def random_features(cls, storage, min_level, max_level, w, phase, sigma):
+        """k(x) = exp(sigma sqrt(2/M) sum_m cos(w_m . x + phase_m)), evaluated on the device."""
+        w = np.ascontiguousarray(w, np.float64).reshape(-1, 3)
+        phase = np.ascontiguousarray(phase, np.float64).ravel()
+        assert w.shape[0] == phase.shape[0]
+        op = cls.__new__(cls)
+        op.storage = storage
+        h = ctypes.c_void_p()
+        _check(load().hyb_operator_create_divkgrad_rff(storage.h, min_level, max_level, w.ctypes.data,
+                                                       phase.ctypes.data, w.shape[0], float(sigma), ctypes.byref(h)))
+        op.h = h
+        return op
+
 
 class P1toP1LinearProlongation:
     def prolongate(self, f, source_level, flag, stream=None):
@@ -360,3 +406,70 @@ class GeometricMultigridSolver:
         _check(load().hyb_gmg_solve_to_tolerance(self.h, x.h, b.h, level, float(rel_tol), max_cycles, precision,
                                                  _p(hist), ctypes.byref(cyc), _stream(stream)))
         return hist[: cyc.value + 1]
+
+
+def rff_features(seed, corr_len=0.2, modes=64):
+    """The random Fourier features the server draws for a lognormal request of this seed."""
+    w, ph = np.zeros((modes, 3)), np.zeros(modes)
+    _check(load().hyb_rff_features(int(seed), float(corr_len), modes, w.ctypes.data, ph.ctypes.data))
+    return w, ph
+
+
+class Server:
+    """Continuous-batching serving loop (hyb_server_*): submit requests with arrival times,
+    run, read per-request results."""
+
+    def __init__(self, budget_bytes, max_active=16, max_level=7):
+        h = ctypes.c_void_p()
+        _check(load().hyb_server_create(int(budget_bytes), max_active, max_level, ctypes.byref(h)))
+        self.h = h
+        self._solutions = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            try:
+                load().hyb_server_destroy(self.h)
+            except Exception:  # interpreter shutdown: module globals already gone
+                pass
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @staticmethod
+    def request(nx, ny, nz, level, coefficient=COEFF_CONSTANT, precision=32, seed=0, rel_tol=1e-8, max_cycles=100):
+        return Request(nx, ny, nz, level, coefficient, precision, seed, rel_tol, max_cycles)
+
+    def footprint(self, req):
+        n = ctypes.c_size_t()
+        _check(load().hyb_server_footprint(self.h, ctypes.byref(req), ctypes.byref(n)))
+        return n.value
+
+    def submit(self, req, arrival_s=0.0, keep_solution=False, num_dofs=None):
+        """Returns the request id. keep_solution needs num_dofs (hyb_storage_num_dofs of the
+        request's mesh and level)."""
+        buf = None
+        if keep_solution:
+            buf = np.zeros(int(num_dofs))
+        i = ctypes.c_int()
+        _check(load().hyb_server_submit(self.h, ctypes.byref(req), float(arrival_s),
+                                        buf.ctypes.data if buf is not None else None, ctypes.byref(i)))
+        if buf is not None:
+            self._solutions[i.value] = buf
+        return i.value
+
+    def run(self, time_limit_s=600.0):
+        _check(load().hyb_server_run(self.h, float(time_limit_s)))
+
+    def result(self, rid):
+        r = RequestResult()
+        _check(load().hyb_server_result(self.h, rid, ctypes.byref(r)))
+        return r
+
+    def solution(self, rid):
+        return self._solutions[rid]
+
+    def stats(self):
+        peak, built, graphs = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int()
+        _check(load().hyb_server_stats(self.h, ctypes.byref(peak), ctypes.byref(built), ctypes.byref(graphs)))
+        return {"peak_bytes": peak.value, "hierarchies_built": built.value, "graphs_captured": graphs.value}

@@ -26,6 +26,10 @@
  *   hyb_cg_solve                  CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:66-135)
  *   hyb_gmg_create / hyb_gmg_solve  GeometricMultigridSolver ctor / solve (GeometricMultigridSolver.hpp:42-235)
  *
+ *   hyb_server_*                  no reference counterpart (the reference runs one solve per
+ *                                 MPI job): a continuous-batching loop that serves many
+ *                                 GeometricMultigridSolver solves on one GPU
+ *
  * Conventions: plain pointers and sizes; every call that enqueues GPU work
  * takes a cudaStream_t passed as void* (NULL = legacy default stream) and is
  * asynchronous unless documented as blocking. Every call returns an hyb_status;
@@ -35,6 +39,7 @@
 #ifndef HYTEG_B200_H
 #define HYTEG_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -107,6 +112,12 @@ int hyb_function_download( hyb_function* f, int level, void* host_dofs, void* st
 int hyb_function_upload_device( hyb_function* f, int level, const void* device_dofs, void* stream );
 int hyb_function_download_device( hyb_function* f, int level, void* device_dofs, void* stream );
 int hyb_function_interpolate_const( hyb_function* f, int level, double value, int flag, void* stream );
+/* Seeded synthetic input on the device (no reference counterpart: the reference's
+ * benchmarks interpolate analytic right-hand sides): every DoF gets a value in [-1, 1)
+ * from a SplitMix64 hash of its position on the lattice of spacing 1/lattice and of the
+ * seed, so replicas and repeated calls agree bit for bit and the values do not depend
+ * on the mesh partition. */
+int hyb_function_fill_uniform_random( hyb_function* f, int level, uint64_t seed, double lattice, void* stream );
 /* f = sum_i scalars[i] * srcs[i]   (n <= 3)  /  f += sum_i ... */
 int hyb_function_assign( hyb_function* f, int level, int n, const double* scalars, hyb_function* const* srcs, int flag,
                          void* stream );
@@ -138,6 +149,11 @@ int hyb_operator_create_divkgrad( hyb_storage* s, int min_level, int max_level, 
 int hyb_operator_create_divkgrad_callback( hyb_storage* s, int min_level, int max_level,
                                            double ( *k )( const double* xyz, void* ctx ), void* ctx,
                                            hyb_operator** out );
+/* the coefficient k(x) = exp( sigma sqrt(2/modes) sum_m cos( w_m . x + phase_m ) ) (random
+ * Fourier features of a Gaussian random field; w is modes x 3, phase has modes entries),
+ * evaluated on the device at every micro-vertex of every level; blocking */
+int hyb_operator_create_divkgrad_rff( hyb_storage* s, int min_level, int max_level, const double* w,
+                                      const double* phase, int modes, double sigma, hyb_operator** out );
 int hyb_operator_destroy( hyb_operator* op );
 int hyb_operator_apply( hyb_operator* op, hyb_function* src, hyb_function* dst, int level, int flag, int update,
                         void* stream );
@@ -172,6 +188,73 @@ int hyb_gmg_solve( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, void
  * history[0..cycles] (optional) receives the relative residuals. */
 int hyb_gmg_solve_to_tolerance( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, double rel_tol,
                                 int max_cycles, int precision, double* history, int* cycles, void* stream );
+
+/* ---- serving loop ----
+ * Poisson solves -div(k grad u) = f, u = 0 on the boundary, on the unit cube split into
+ * nx x ny x nz macro-cubes of 6 macro-tets each, arrive at stated times. The server
+ * admits a request when an active slot and its device footprint (hyb_server_footprint)
+ * fit the byte budget, keeps each admitted hierarchy resident (an idle hierarchy of the
+ * same shape is reused; idle ones are evicted least recently used when memory is needed),
+ * and runs every admitted solve on its own stream as captured CUDA graphs, one
+ * V-cycle (FP64) or one refinement step (FP32 V-cycle in FP64 refinement) per graph, so
+ * the solves in flight overlap on the GPU. New requests join between any two steps of
+ * the others. Each solve is V(3,3) with multicolour SOR (omega 1) and a level-0 FP64 CG
+ * coarse solve to 1e-12; f is hyb_function_fill_uniform_random( seed, lattice =
+ * lcm(nx,ny,nz) 2^level ) and, for the lognormal coefficient, k is exp of the random
+ * field of hyb_rff_features( seed, 0.2, 64 ) with sigma 1. Results do not depend on
+ * which other requests share the GPU. */
+typedef struct hyb_server_s hyb_server;
+
+enum
+{
+   HYB_COEFF_CONSTANT  = 0, /* k = 1 (P1ConstantLaplaceOperator) */
+   HYB_COEFF_LOGNORMAL = 1  /* k = exp(g), g a Gaussian random field (P1ElementwiseOperator) */
+};
+
+typedef struct hyb_request
+{
+   int      nx, ny, nz;   /* macro-cubes per direction */
+   int      level;        /* refinement level of the solve */
+   int      coefficient;  /* HYB_COEFF_* */
+   int      precision;    /* 64: FP64 V-cycles; 32: FP32 V-cycles in FP64 iterative refinement */
+   uint64_t seed;         /* right-hand side and coefficient seed */
+   double   rel_tol;      /* stop when ||b - A x|| / ||b|| <= rel_tol */
+   int      max_cycles;   /* give up (HYB_ENOTCONVERGED) after this many cycles */
+} hyb_request;
+
+typedef struct hyb_request_result
+{
+   int    status;          /* HYB_OK; HYB_ENOMEM if it can never fit the budget; HYB_ENOTCONVERGED; ... */
+   int    cycles;          /* V-cycles (FP64) or refinement steps (mixed) run */
+   double rel_residual;    /* final FP64 ||b - A x|| / ||b|| over inner and Neumann DoFs */
+   double arrival_s;       /* host clock, seconds from the start of the hyb_server_run call */
+   double admit_s;
+   double done_s;          /* the result (and the solution, if requested) is on the host */
+   size_t footprint_bytes; /* device bytes held by the hierarchy that served the request */
+} hyb_request_result;
+
+/* Host only (no device call): budget_bytes bounds the device memory of all resident
+ * hierarchies and meshes; at most max_active solves run at a time; meshes are built up
+ * to max_level. */
+int hyb_server_create( size_t budget_bytes, int max_active, int max_level, hyb_server** out );
+int hyb_server_destroy( hyb_server* s );
+/* device bytes that the request's resident hierarchy takes (host only) */
+int hyb_server_footprint( const hyb_server* s, const hyb_request* r, size_t* bytes );
+/* Queue a request arriving arrival_s seconds after the start of the next hyb_server_run.
+ * solution_host, if not NULL, receives the solution on the request's level in the
+ * canonical DoF order (hyb_storage_num_dofs doubles). Invalid requests are refused with
+ * HYB_EINVAL and requests larger than the whole budget with HYB_ENOMEM; neither is queued. */
+int hyb_server_submit( hyb_server* s, const hyb_request* r, double arrival_s, double* solution_host, int* id );
+/* Serve the queued requests until all are done or time_limit_s has passed (then the
+ * unfinished ones end with HYB_ETIMEOUT); blocking. */
+int hyb_server_run( hyb_server* s, double time_limit_s );
+int hyb_server_result( const hyb_server* s, int id, hyb_request_result* out );
+/* peak device bytes held by the server, hierarchies built, graphs captured */
+int hyb_server_stats( const hyb_server* s, size_t* peak_bytes, int* hierarchies_built, int* graphs_captured );
+/* The random Fourier features the server draws for a lognormal request of this seed:
+ * w (modes x 3) ~ N(0, 1/corr_len^2), phase (modes) ~ U[0, 2 pi), from a SplitMix64
+ * stream and the Box-Muller transform (host only). */
+int hyb_rff_features( uint64_t seed, double corr_len, int modes, double* w, double* phase );
 
 #ifdef __cplusplus
 }

@@ -275,3 +275,38 @@ def test_gmg_to_tolerance_error_vs_oracle(H, oracle_mod, setups, precision):
     orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=60, rel_tol=1e-13)
     err = np.abs(fx.get(L) - x).max() / np.abs(x).max()
     assert err < 1e-6, err
+
+
+@pytest.mark.parametrize("name", ["octahedron", "cube211"])
+def test_device_uniform_fill_matches_host_hash(H, oracle_mod, setups, name):
+    """hyb_function_fill_uniform_random equals the host hash on the DoF coordinates bit for bit."""
+    O = oracle_mod
+    st, orc, L = setups[name]
+    for level in (2, L):
+        lattice = float(2 << level)
+        f64, f32 = H.P1Function("a", st, 0, L), H.P1Function("b", st, 0, L, dtype=H.F32)
+        f64.fill_uniform_random(level, 7, lattice)
+        f32.fill_uniform_random(level, 7, lattice)
+        expect = O.uniform_rhs(orc.coords_of(level), 7, lattice)
+        assert np.array_equal(f64.get(level), expect)
+        assert np.array_equal(f32.get(level), expect.astype(np.float32))
+
+
+def test_device_rff_coefficient_matches_nodal_operator(H, oracle_mod, setups):
+    """The div-k-grad operator whose coefficient is evaluated on the device (random Fourier
+    features) applies like the one built from host nodal values of the same field."""
+    import hyb_inputs as I
+
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    w, ph = I.grf_features(0.2, 1, 64)
+    A_dev = H.P1ElementwiseDivKGradOperator.random_features(st, 0, L, w, ph, 1.0)
+    kv = [O.grf_coefficient(orc.coords_of(l), seed=1) for l in range(L + 1)]
+    op = orc.op_divkgrad(kv)
+    rng = np.random.default_rng(5)
+    for level in range(L + 1):
+        x = rng.uniform(-1, 1, orc.n(level))
+        fs, fd = H.P1Function("s", st, 0, L), H.P1Function("d", st, 0, L)
+        fs.set(x, level)
+        A_dev.apply(fs, fd, level, 15)
+        close(fd.get(level), orc.apply(x, level, flag=15, op=op), 1e-12)
