@@ -96,11 +96,12 @@ inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s );
 struct LevelHost
 {
    LevelDev           dev{};
-   DevBuf< int32_t >  seg, sorSeg, xyz;
+   DevBuf< int32_t >  seg, xyz, blk, pts, ptsC;
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
    std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
-   int                cellBlocks   = 0;  // grid of the cell-interior loops
-   int                sorCellBlocks = 0;
+   int                cellBlocks   = 0;  // grid of the cell-interior row-segment loops
+   int                ptsBlocks    = 0;  // grid of the loops over all interior points
+   int                colourBlocks = 0;  // grid of the loops over one interior colour
    int                bdryBlocks   = 0;  // grid of the surface-DoF loops
    int                slabBlocks   = 0;  // blocks of 256 over one closure
 };
@@ -110,11 +111,6 @@ struct Storage
    Topology                              topo;
    int                                   maxLevel = 0;
    int                                   numSMs   = 148;
-   // levels up to this one run the four interior SOR colours in one cluster launch;
-   // larger levels use one launch per colour (tuning: HYB_SOR_FUSED_MAX_LEVEL). Measured
-   // on B200 (48 cells, levels 1-7) the per-colour launches are as fast or faster at
-   // every level, so the cluster path is off unless requested.
-   int                                   sorFusedMaxLevel = -1;
    DevBuf< ClassDev >                    cls;
    DevBuf< int32_t >                     fEmb, eEmbOff, eEmb, vEmbOff, vEmb;
    DevBuf< uint8_t >                     fBc, eBc, vBc;
@@ -149,9 +145,6 @@ struct Storage
 
 inline int stridePad( int s ) { return ( s + 31 ) / 32 * 32; }
 
-template < typename T, bool VAR >
-void initClusterCfg();
-
 void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, const std::vector< std::array< int, 4 > >& T,
                    int maxLevel )
 {
@@ -162,8 +155,6 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       int dev = 0;
       HYB_CUDA( cudaGetDevice( &dev ) );
       HYB_CUDA( cudaDeviceGetAttribute( &s.numSMs, cudaDevAttrMultiProcessorCount, dev ) );
-      if ( const char* e = std::getenv( "HYB_SOR_FUSED_MAX_LEVEL" ) )
-         s.sorFusedMaxLevel = std::atoi( e );
    }
    s.topo.build( V, T );
    s.topo.computeColouring();
@@ -254,7 +245,8 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       d.nIntFace   = d.N >= 3 ? ( d.N - 1 ) * ( d.N - 2 ) / 2 : 0;
       d.nIntCell   = d.N >= 4 ? tetSize( d.N - 3 ) : 0;
       d.nBdry      = nV + nE * ( d.N - 1 ) + nF * d.nIntFace;
-      std::vector< int32_t > seg, sorSeg, xyz( d.S );
+      std::vector< int32_t >                seg, xyz( d.S ), blk, pts;
+      std::vector< std::vector< int32_t > > ptsC( kInteriorColours );
       for ( int z = 1; z <= d.N; ++z )
          for ( int y = 1; y <= d.N - z; ++y )
          {
@@ -263,28 +255,57 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
                continue;
             for ( int x0 = 1; x0 <= len; x0 += 32 )
                seg.push_back( z | ( y << 10 ) | ( x0 << 20 ) );
-            const int groups = ( len + kInteriorColours - 1 ) / kInteriorColours;
-            for ( int g0 = 0; g0 < groups; g0 += 32 )
-               sorSeg.push_back( z | ( y << 10 ) | ( g0 << 20 ) );
+            // residue blocks of the row in storage order: r = 0..3, g ascending
+            for ( int r = 0; r < 4; ++r )
+            {
+               const int b = int( blk.size() / 16 );
+               require( b < ( 1 << 23 ), "too many residue blocks for the point-table encoding" );
+               const NbrOff no = residueNbr( d.W, y, z, r );
+               for ( int q = 0; q < 16; ++q )
+                  blk.push_back( q < 15 ? no.d[q] : 0 );
+               const int c = ( r + 2 * y + 3 * z ) & 3;
+               for ( int g = 0; 4 * g + r <= len; ++g )
+               {
+                  if ( 4 * g + r < 1 )
+                     continue;
+                  pts.push_back( g | ( b << 8 ) );
+                  ptsC[c].push_back( g | ( b << 8 ) );
+               }
+            }
          }
+      std::vector< int32_t > ptsFlat;
+      for ( int c = 0; c < kInteriorColours; ++c )
+      {
+         d.ptsOff[c] = int( ptsFlat.size() );
+         ptsFlat.insert( ptsFlat.end(), ptsC[c].begin(), ptsC[c].end() );
+      }
+      d.ptsOff[kInteriorColours] = int( ptsFlat.size() );
+      d.nPts                     = int( pts.size() );
+      lh->blk.upload( blk );
+      lh->pts.upload( pts );
+      lh->ptsC.upload( ptsFlat );
+      d.blk  = lh->blk.p;
+      d.pts  = lh->pts.p;
+      d.ptsC = lh->ptsC.p;
       for ( int z = 0; z <= d.N; ++z )
          for ( int y = 0; y <= d.N - z; ++y )
             for ( int x = 0; x <= d.N - y - z; ++x )
-               xyz[cidx( d.W, x, y, z )] = x | ( y << 10 ) | ( z << 20 );
+               xyz[sidx( d.W, x, y, z )] = x | ( y << 10 ) | ( z << 20 );
       lh->seg.upload( seg );
-      lh->sorSeg.upload( sorSeg );
       lh->xyz.upload( xyz );
-      d.nSeg    = int( seg.size() );
-      d.nSorSeg = int( sorSeg.size() );
-      d.seg     = lh->seg.p;
-      d.sorSeg  = lh->sorSeg.p;
-      d.xyz     = lh->xyz.p;
+      d.nSeg = int( seg.size() );
+      d.seg  = lh->seg.p;
+      d.xyz  = lh->xyz.p;
       // grids: the loops are grid-stride, so a few resident blocks per SM suffice
       auto grid = [&]( long work, int perBlock, int perSM ) {
          return int( std::max< long >( 0, std::min< long >( ( work + perBlock - 1 ) / perBlock, long( s.numSMs ) * perSM ) ) );
       };
-      lh->cellBlocks    = grid( long( d.nSeg ) * nC, kCellWarps, 16 );
-      lh->sorCellBlocks = grid( long( d.nSorSeg ) * nC, kCellWarps, 16 );
+      lh->cellBlocks = grid( long( d.nSeg ) * nC, kCellWarps, 16 );
+      lh->ptsBlocks  = grid( long( ( d.nPts + 31 ) / 32 ) * nC, kCellWarps, 16 );
+      int maxColour  = 0;
+      for ( int c = 0; c < kInteriorColours; ++c )
+         maxColour = std::max( maxColour, d.ptsOff[c + 1] - d.ptsOff[c] );
+      lh->colourBlocks = grid( long( ( maxColour + 31 ) / 32 ) * nC, kCellWarps, 16 );
       lh->bdryBlocks    = grid( bdryLaneCount( nV, nE * ( d.N - 1 ), nF * d.nIntFace ), kBdryThreads, 8 );
       lh->slabBlocks    = ( d.S + 255 ) / 256;
       maxPartial        = std::max( maxPartial, size_t( lh->slabBlocks ) * nC );
@@ -329,10 +350,6 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
    s.partial.alloc( maxPartial );
    s.scalars.alloc( 64 );
    HYB_CUDA( cudaMallocHost( &s.hostScalar, 64 * sizeof( double ) ) );
-   initClusterCfg< double, false >();
-   initClusterCfg< double, true >();
-   initClusterCfg< float, false >();
-   initClusterCfg< float, true >();
 }
 
 // ---------------------------------------------------------------------------
@@ -703,7 +720,7 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
 {
    const Storage& s  = *op.st;
    const auto&    L  = s.L( l );
-   const int      nc = L.dev.nSeg > 0 ? L.cellBlocks : 0;
+   const int      nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
@@ -731,81 +748,6 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
    HYB_CHECK_LAUNCH();
 }
 
-// Cluster shape of the fused interior SOR kernel, chosen once per instantiation
-// (outside any stream capture): 16 CTAs per cluster where the device allows
-// non-portable sizes, else 8; maxClusters = clusters that fit at once.
-struct ClusterCfg
-{
-   int csize = 0, maxClusters = 0;
-};
-template < typename T, bool VAR >
-ClusterCfg& clusterCfg()
-{
-   static ClusterCfg c;
-   return c;
-}
-constexpr int kClusterThreads = 256;
-
-template < typename T, bool VAR >
-void initClusterCfg()
-{
-   ClusterCfg& cfg = clusterCfg< T, VAR >();
-   if ( cfg.csize != 0 )
-      return;
-   auto kern = k_sor_interior_cluster< T, VAR >;
-   for ( int cs : { 16, 8 } )
-   {
-      if ( cs > 8 && cudaFuncSetAttribute( kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1 ) != cudaSuccess )
-      {
-         cudaGetLastError();
-         continue;
-      }
-      cudaLaunchConfig_t  c{};
-      cudaLaunchAttribute a{};
-      a.id               = cudaLaunchAttributeClusterDimension;
-      a.val.clusterDim.x = cs;
-      a.val.clusterDim.y = 1;
-      a.val.clusterDim.z = 1;
-      c.gridDim          = dim3( cs );
-      c.blockDim         = dim3( kClusterThreads );
-      c.attrs            = &a;
-      c.numAttrs         = 1;
-      int n              = 0;
-      if ( cudaOccupancyMaxActiveClusters( &n, kern, &c ) == cudaSuccess && n > 0 )
-      {
-         cfg.csize       = cs;
-         cfg.maxClusters = n;
-         return;
-      }
-      cudaGetLastError();
-   }
-   cfg.csize = -1; // clusters unavailable: per-colour launches are used
-}
-
-template < typename T, bool VAR >
-bool launchSorInteriorCluster( const Storage& s, const LevelHost& L, const OpDev< T >& od, T* u, const T* rhs, T relax,
-                               cudaStream_t stream )
-{
-   const ClusterCfg& cfg = clusterCfg< T, VAR >();
-   if ( cfg.csize <= 0 )
-      return false;
-   const int           nClusters = std::min( s.td.nC, cfg.maxClusters );
-   cudaLaunchConfig_t  c{};
-   cudaLaunchAttribute a{};
-   a.id               = cudaLaunchAttributeClusterDimension;
-   a.val.clusterDim.x = cfg.csize;
-   a.val.clusterDim.y = 1;
-   a.val.clusterDim.z = 1;
-   c.gridDim          = dim3( nClusters * cfg.csize );
-   c.blockDim         = dim3( kClusterThreads );
-   c.stream           = stream;
-   c.attrs            = &a;
-   c.numAttrs         = 1;
-   HYB_CUDA( cudaLaunchKernelEx( &c, k_sor_interior_cluster< T, VAR >, s.td, L.dev, od, u, rhs, relax ) );
-   HYB_CHECK_LAUNCH();
-   return true;
-}
-
 template < typename T >
 void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream )
 {
@@ -828,24 +770,20 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
          k_sor_iface< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, bl );
       HYB_CHECK_LAUNCH();
    }
-   if ( L.dev.nSorSeg == 0 )
+   if ( L.dev.nPts == 0 )
       return;
-   // interior passes: all four colours in one cluster launch on small levels, else one
-   // launch per colour
-   if ( l <= s.sorFusedMaxLevel )
-   {
-      const bool fused = op.variable ? launchSorInteriorCluster< T, true >( s, L, od, u, rhs, relax, stream ) :
-                                       launchSorInteriorCluster< T, false >( s, L, od, u, rhs, relax, stream );
-      if ( fused )
-         return;
-   }
+   // interior passes: one launch per colour
    for ( int c = 0; c < kInteriorColours; ++c )
    {
+      const int begin = L.dev.ptsOff[c], count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
+      if ( count == 0 )
+         continue;
       if ( op.variable )
-         k_sor_interior< T, true ><<< L.sorCellBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c, L.sorCellBlocks );
+         k_sor_interior< T, true ><<< L.colourBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c, begin, count,
+                                                                          L.colourBlocks );
       else
-         k_sor_interior< T, false ><<< L.sorCellBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c,
-                                                                            L.sorCellBlocks );
+         k_sor_interior< T, false ><<< L.colourBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c, begin,
+                                                                           count, L.colourBlocks );
       HYB_CHECK_LAUNCH();
    }
 }
@@ -855,7 +793,7 @@ void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs
 {
    const Storage& s  = *op.st;
    const auto&    L  = s.L( l );
-   const int      nc = L.dev.nSeg > 0 ? L.cellBlocks : 0;
+   const int      nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;

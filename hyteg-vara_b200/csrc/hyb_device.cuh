@@ -55,10 +55,18 @@ struct LevelDev
    int     nIntFace, nIntCell;
    int     nBdry;              // nV + nE (N-1) + nF nIntFace
    int     nSeg;               // interior row segments (32 points each)
-   int     nSorSeg;            // interior row segments of 32 colour groups
    const int32_t* seg;         // packed z | y<<10 | x0<<20
-   const int32_t* sorSeg;      // packed z | y<<10 | g0<<20
    const int32_t* xyz;         // closure index -> x | y<<10 | z<<20
+   // Cell-interior points, the same for every cell of the level. A residue block is the
+   // run of points x = 4g + r (fixed r) of one row; blk[16 b + q] is the position of
+   // stencil neighbour q of point g of block b, minus g (residueNbr). pts lists every
+   // interior point as g | b << 8 in storage order; ptsC lists the points of interior SOR
+   // colour c in [ptsOff[c], ptsOff[c + 1]), also in storage order.
+   int            nPts;
+   int            ptsOff[5];
+   const int32_t* blk;
+   const int32_t* pts;
+   const int32_t* ptsC;
 };
 
 // 15 stencil offsets, order shared with the oracle and the C ABI
@@ -108,45 +116,85 @@ __host__ __device__ __forceinline__ int rowStart( int W, int y, int z )
    const int wms = W - z;
    return tetSize( W ) - tetSize( wms ) + y * ( wms + 1 ) - ( ( y + 1 ) * y ) / 2;
 }
+// tet-linear index (vertexdof::macrocell::index): the canonical numbering of a tetrahedral
+// point set, used for the canonical DoF order of cell interiors
 __host__ __device__ __forceinline__ int cidx( int W, int x, int y, int z ) { return rowStart( W, y, z ) + x; }
+
+// Storage layout of a closure slab: rows (y, z) in tet-linear order at their tet-linear
+// start, but inside a row of length n the points are grouped by x mod 4 -- all x = 0 mod 4
+// first, then 1, 2, 3 -- so that one interior SOR colour ((x + 2y + 3z) mod 4 is fixed in a
+// row) is one contiguous run of every row.
+__host__ __device__ __forceinline__ int resOff( int r, int n )
+{
+   const int m = n & 3;
+   return r * ( n >> 2 ) + ( r < m ? r : m );
+}
+__host__ __device__ __forceinline__ int resCarry( int v ) { return v < 0 ? -1 : ( v > 3 ? 1 : 0 ); }
+// storage position of closure point (x, y, z)
+__host__ __device__ __forceinline__ int sidx( int W, int x, int y, int z )
+{
+   return rowStart( W, y, z ) + resOff( x & 3, W - y - z ) + ( x >> 2 );
+}
 
 __host__ __device__ __forceinline__ int classMask( int N, int x, int y, int z )
 {
    return ( N - x - y - z == 0 ? 1 : 0 ) | ( x == 0 ? 2 : 0 ) | ( y == 0 ? 4 : 0 ) | ( z == 0 ? 8 : 0 );
 }
 
-// Index offsets of the 15 neighbours of closure point (*, y, z) relative to its own
-// index, from the row-start recurrences of the tetrahedral layout.
+// The seven rows a 15-point stencil at row (y, z) touches: start (tet-linear recurrences)
+// and length. Order: (y,z), (y+1,z), (y-1,z), (y,z+1), (y,z-1), (y-1,z+1), (y+1,z-1).
+// Rows outside the closure (y = 0 or z = 0) get meaningless values and must not be read.
+struct StencilRows
+{
+   int start[7], len[7];
+};
+__host__ __device__ __forceinline__ StencilRows stencilRows( int W, int y, int z )
+{
+   StencilRows R;
+   const int   n   = W - z - y;
+   const int   rs  = rowStart( W, y, z );
+   const int   slz = ( W - z ) * ( W - z + 1 ) / 2;     // points in slice z
+   const int   slm = ( W - z + 1 ) * ( W - z + 2 ) / 2; // points in slice z-1
+   R.start[0] = rs;
+   R.len[0]   = n;
+   R.start[1] = rs + n;
+   R.len[1]   = n - 1;
+   R.start[2] = rs - ( n + 1 );
+   R.len[2]   = n + 1;
+   R.start[3] = rs + slz - y;
+   R.len[3]   = n - 1;
+   R.start[4] = rs - ( slm - y );
+   R.len[4]   = n + 1;
+   R.start[5] = R.start[2] + slz - ( y - 1 );
+   R.len[5]   = n;
+   R.start[6] = R.start[1] - slm + ( y + 1 );
+   R.len[6]   = n;
+   return R;
+}
+// stencil offset q -> its row in StencilRows
+__host__ __device__ __forceinline__ int offRow( int q )
+{
+   constexpr int t[15] = { 0, 0, 0, 1, 2, 3, 4, 1, 2, 3, 4, 5, 6, 6, 5 };
+   return t[q];
+}
+
+// Positions of the 15 neighbours of interior point x = 4g + r of row (y, z), relative to
+// g: neighbour q sits at d[q] + g.
 struct NbrOff
 {
    int d[15];
 };
-__host__ __device__ __forceinline__ NbrOff nbrOffsets( int W, int y, int z )
+__host__ __device__ __forceinline__ NbrOff residueNbr( int W, int y, int z, int r )
 {
-   NbrOff    o;
-   const int dyp = W - z - y;                         // (0,1,0)
-   const int dym = -( W - z - y + 1 );                // (0,-1,0)
-   const int slz = ( W - z ) * ( W - z + 1 ) / 2;      // points in slice z
-   const int slm = ( W - z + 1 ) * ( W - z + 2 ) / 2;  // points in slice z-1
-   const int dzp = slz - y;                           // (0,0,1)
-   const int dzm = -( slm - y );                      // (0,0,-1)
-   const int d11 = dym + slz - ( y - 1 );             // (0,-1,1)
-   const int d12 = dyp - slm + ( y + 1 );             // (0,1,-1)
-   o.d[0]  = 0;
-   o.d[1]  = 1;
-   o.d[2]  = -1;
-   o.d[3]  = dyp;
-   o.d[4]  = dym;
-   o.d[5]  = dzp;
-   o.d[6]  = dzm;
-   o.d[7]  = dyp - 1;
-   o.d[8]  = dym + 1;
-   o.d[9]  = dzp - 1;
-   o.d[10] = dzm + 1;
-   o.d[11] = d11;
-   o.d[12] = d12;
-   o.d[13] = d12 - 1;
-   o.d[14] = d11 + 1;
+   const StencilRows R = stencilRows( W, y, z );
+   NbrOff            o;
+#pragma unroll
+   for ( int q = 0; q < 15; ++q )
+   {
+      const int v = r + offX( q );
+      const int k = offRow( q );
+      o.d[q]      = R.start[k] + resOff( v & 3, R.len[k] ) + resCarry( v );
+   }
    return o;
 }
 
@@ -199,33 +247,39 @@ template < typename T, bool VAR >
 __device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* __restrict__ u, int cell, int W, int x, int y,
                                             int z, T& diag, T& off )
 {
-   const int  N    = W - 1;
-   const int  mask = classMask( N, x, y, z );
-   const int  base = cidx( W, x, y, z );
-   const NbrOff no = nbrOffsets( W, y, z );
+   const int         N     = W - 1;
+   const int         mask  = classMask( N, x, y, z );
+   const uint32_t    valid = kValidOffsets[mask];
+   const StencilRows R     = stencilRows( W, y, z );
+   // positions of the neighbours inside the closure (the others are never read)
+   int pos[15];
+#pragma unroll
+   for ( int q = 0; q < 15; ++q )
+   {
+      const int xq = x + offX( q ), k = offRow( q );
+      pos[q]       = ( valid & ( 1u << q ) ) ? R.start[k] + resOff( xq & 3, R.len[k] ) + ( xq >> 2 ) : 0;
+   }
    if constexpr ( !VAR )
    {
-      const T*       st    = op.st + ( size_t( cell ) * 16 + mask ) * 15;
-      const uint32_t valid = kValidOffsets[mask];
+      const T* st = op.st + ( size_t( cell ) * 16 + mask ) * 15;
       diag += st[0];
 #pragma unroll
       for ( int q = 1; q < 15; ++q )
          if ( valid & ( 1u << q ) )
-            off += st[q] * u[base + no.d[q]];
+            off += st[q] * u[pos[q]];
    }
    else
    {
       const T*       kv    = op.kap + size_t( cell ) * op.stride;
       const T*       K     = op.K + size_t( cell ) * 96;
-      const uint32_t valid = kValidTets[mask];
+      const uint32_t validT = kValidTets[mask];
 #pragma unroll
       for ( int i = 0; i < 24; ++i )
       {
          const IncidentTet it = incidentTet( i );
-         if ( !( valid & ( 1u << i ) ) )
+         if ( !( validT & ( 1u << i ) ) )
             continue;
-         const T ks = kv[base + no.d[it.q[0]]] + kv[base + no.d[it.q[1]]] + kv[base + no.d[it.q[2]]] +
-                      kv[base + no.d[it.q[3]]];
+         const T ks = kv[pos[it.q[0]]] + kv[pos[it.q[1]]] + kv[pos[it.q[2]]] + kv[pos[it.q[3]]];
          const T* Kr = K + it.t * 16 + it.k * 4;
 #pragma unroll
          for ( int j = 0; j < 4; ++j )
@@ -233,7 +287,7 @@ __device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* __res
             if ( j == it.k )
                diag += ks * Kr[j];
             else
-               off += ks * Kr[j] * u[base + no.d[it.q[j]]];
+               off += ks * Kr[j] * u[pos[it.q[j]]];
          }
       }
    }

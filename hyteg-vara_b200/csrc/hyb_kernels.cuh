@@ -9,7 +9,6 @@
 // tensor-core path applies.
 #pragma once
 
-#include <cooperative_groups.h>
 
 #include "hyb_device.cuh"
 
@@ -106,7 +105,7 @@ __device__ __forceinline__ size_t bdryReplica( const TopoDev& tp, const LevelDev
 {
    int c, x, y, z;
    embeddingCoords( embAt( tp, p.kind, p.prim, e ), p.kind, lv.N, p.i, p.j, c, x, y, z );
-   return size_t( c ) * lv.stride + cidx( lv.W, x, y, z );
+   return size_t( c ) * lv.stride + sidx( lv.W, x, y, z );
 }
 
 template < typename T >
@@ -249,20 +248,9 @@ struct InteriorOp
       }
    }
 
-   // load of u: through L1, or (L2ONLY) straight from L2 for data other CTAs of a
-   // cluster rewrite between cluster barriers
-   template < bool L2ONLY >
-   __device__ __forceinline__ static T ld( const T* p )
-   {
-      if constexpr ( L2ONLY )
-         return __ldcg( p );
-      else
-         return *p;
-   }
-
-   // diag and off-diagonal sum at index `base` with neighbour offsets `no`
-   template < bool L2ONLY = false >
-   __device__ __forceinline__ void row( const T* __restrict__ u, int base, const NbrOff& no, T& diag, T& off ) const
+   // diag and off-diagonal sum at interior point x = 4g + r whose neighbours sit at
+   // no.d[q] + g (residueNbr)
+   __device__ __forceinline__ void row( const T* __restrict__ u, int g, const NbrOff& no, T& diag, T& off ) const
    {
       if constexpr ( !VAR )
       {
@@ -270,7 +258,7 @@ struct InteriorOp
          T s  = 0;
 #pragma unroll
          for ( int q = 1; q < 15; ++q )
-            s += w[q] * ld< L2ONLY >( u + base + no.d[q] );
+            s += w[q] * u[no.d[q] + g];
          off = s;
       }
       else
@@ -279,8 +267,8 @@ struct InteriorOp
 #pragma unroll
          for ( int q = 0; q < 15; ++q )
          {
-            kq[q] = kv[base + no.d[q]];
-            uq[q] = ld< L2ONLY >( u + base + no.d[q] );
+            kq[q] = kv[no.d[q] + g];
+            uq[q] = u[no.d[q] + g];
          }
          T d = 0, s = 0;
 #pragma unroll
@@ -317,6 +305,66 @@ struct InteriorOp
    for ( int it_ = int( blockIdx.x ) * wpb_ + int( threadIdx.x >> 5 ); it_ < nItems_; it_ += nCellBlocks * wpb_ )
 
 // ---------------------------------------------------------------------------
+// Cell-interior loops run over the level's interior point table: a warp takes 32
+// consecutive entries (consecutive storage positions, so every neighbour read is a
+// contiguous run across the warp) and reads the neighbour positions of each entry's
+// residue block from the block table (one broadcast per block).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ NbrOff blockNbr( const int32_t* __restrict__ blk, int b )
+{
+   const int4* p = reinterpret_cast< const int4* >( blk + 16 * size_t( b ) );
+   const int4  a = __ldg( p ), c = __ldg( p + 1 ), e = __ldg( p + 2 ), f = __ldg( p + 3 );
+   NbrOff      o;
+   o.d[0]  = a.x;
+   o.d[1]  = a.y;
+   o.d[2]  = a.z;
+   o.d[3]  = a.w;
+   o.d[4]  = c.x;
+   o.d[5]  = c.y;
+   o.d[6]  = c.z;
+   o.d[7]  = c.w;
+   o.d[8]  = e.x;
+   o.d[9]  = e.y;
+   o.d[10] = e.z;
+   o.d[11] = e.w;
+   o.d[12] = f.x;
+   o.d[13] = f.y;
+   o.d[14] = f.z;
+   return o;
+}
+
+// Interior points per lane and item: independent load chains that the warp keeps in
+// flight together (the loops are latency bound, not bandwidth bound, at one point per lane).
+template < typename T, bool VAR >
+__host__ __device__ constexpr int interiorBatch()
+{
+   return VAR ? 1 : ( sizeof( T ) == 8 ? 2 : 4 );
+}
+
+// The K table entries i0 + 32 k of a point table. Entries past the end are clamped to the
+// last one, so every read stays in bounds; valid[k] tells the caller not to store them.
+template < int K >
+struct PointBatch
+{
+   int    g[K];
+   NbrOff no[K];
+   bool   valid[K];
+   __device__ __forceinline__ void load( const int32_t* __restrict__ pts, const int32_t* __restrict__ blk, int nPts,
+                                         int i0 )
+   {
+#pragma unroll
+      for ( int k = 0; k < K; ++k )
+      {
+         const int i     = i0 + 32 * k;
+         valid[k]        = i < nPts;
+         const int32_t e = __ldg( pts + ( valid[k] ? i : nPts - 1 ) );
+         g[k]            = e & 255;
+         no[k]           = blockNbr( blk, e >> 8 );
+      }
+   }
+};
+
+// ---------------------------------------------------------------------------
 // apply / residual (P1Operator::apply, P1Operator.hpp:196-324;
 // P1ElementwiseOperator::apply, P1ElementwiseOperator.cpp:64-221)
 // ---------------------------------------------------------------------------
@@ -327,27 +375,38 @@ __global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev
 {
    if ( int( blockIdx.x ) < nCellBlocks )
    {
-      HYB_CELL_LOOP( lv.nSeg )
+      constexpr int K       = interiorBatch< T, VAR >();
+      const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
+      HYB_CELL_LOOP( nChunks )
       {
-         const int     cell = it_ / lv.nSeg;
-         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
-         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-         if ( x + y + z > lv.N - 1 )
-            continue;
+         const int     cell = it_ / nChunks;
+         PointBatch< K > pb;
+         pb.load( lv.pts, lv.blk, lv.nPts, ( it_ - cell * nChunks ) * 32 * K + int( threadIdx.x & 31 ) );
          InteriorOp< T, VAR > io;
          io.load( op, cell );
-         const size_t co   = size_t( cell ) * lv.stride;
-         const int    base = cidx( lv.W, x, y, z );
-         const NbrOff no   = nbrOffsets( lv.W, y, z );
-         T            diag, off;
-         io.row( src + co, base, no, diag, off );
-         const T ax = diag * src[co + base] + off;
-         if constexpr ( MODE == kReplace )
-            dst[co + base] = ax;
-         else if constexpr ( MODE == kAdd )
-            dst[co + base] += ax;
-         else
-            dst[co + base] = rhs[co + base] - ax;
+         const size_t co = size_t( cell ) * lv.stride;
+         const T* __restrict__ su = src + co;
+         T ax[K];
+#pragma unroll
+         for ( int k = 0; k < K; ++k )
+         {
+            T diag, off;
+            io.row( su, pb.g[k], pb.no[k], diag, off );
+            ax[k] = diag * su[pb.no[k].d[0] + pb.g[k]] + off;
+         }
+#pragma unroll
+         for ( int k = 0; k < K; ++k )
+         {
+            if ( !pb.valid[k] )
+               continue;
+            const size_t idx = co + pb.no[k].d[0] + pb.g[k];
+            if constexpr ( MODE == kReplace )
+               dst[idx] = ax[k];
+            else if constexpr ( MODE == kAdd )
+               dst[idx] += ax[k];
+            else
+               dst[idx] = rhs[idx] - ax[k];
+         }
       }
       return;
    }
@@ -411,80 +470,42 @@ __global__ void __launch_bounds__( 128 ) k_sor_iface( TopoDev tp, LevelDev lv, O
    }
 }
 
-// the one interior x of colour `colour` in the group [1 + 4g, 1 + 4g + 4) of row (y, z)
-__device__ __forceinline__ int colourX( int g, int y, int z, int colour )
-{
-   const int x0 = 1 + kInteriorColours * g;
-   return x0 + ( ( colour - ( ( x0 + 2 * y + 3 * z ) & 3 ) ) & 3 );
-}
-
-// One interior colour over all cells. Odd colours walk the cells in reverse order, so a
+// One interior colour over all cells: in row (y, z) the points of colour c are the
+// residue block r = (c - 2y - 3z) mod 4, one contiguous run of the row; the colour's point
+// table lists them in storage order. Odd colours walk the cells in reverse order, so a
 // pass starts on the data the previous pass touched last (still in L2).
 template < typename T, bool VAR >
 __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                         const T* __restrict__ rhs, T relax, int colour, int nCellBlocks )
+                                                         const T* __restrict__ rhs, T relax, int colour, int begin,
+                                                         int nPts, int nCellBlocks )
 {
-   HYB_CELL_LOOP( lv.nSorSeg )
+   constexpr int  K       = interiorBatch< T, VAR >();
+   const int32_t* pts     = lv.ptsC + begin;
+   const int      nChunks = ( nPts + 32 * K - 1 ) / ( 32 * K );
+   HYB_CELL_LOOP( nChunks )
    {
-      const int     item = ( colour & 1 ) ? nItems_ - 1 - it_ : it_;
-      const int     cell = item / lv.nSorSeg;
-      const int32_t sp   = lv.sorSeg[item - cell * lv.nSorSeg];
-      const int     z = sp & 1023, y = ( sp >> 10 ) & 1023;
-      const int     x = colourX( ( sp >> 20 ) + ( threadIdx.x & 31 ), y, z, colour );
-      if ( x + y + z > lv.N - 1 )
-         continue;
-      InteriorOp< T, VAR > io;
-      io.load( op, cell );
-      const size_t co   = size_t( cell ) * lv.stride;
-      const int    base = cidx( lv.W, x, y, z );
-      const NbrOff no   = nbrOffsets( lv.W, y, z );
-      T            diag, off;
-      io.row( u + co, base, no, diag, off );
-      u[co + base] = ( T( 1 ) - relax ) * u[co + base] + relax * ( rhs[co + base] - off ) / diag;
-   }
-}
-
-// All four interior colour passes of a sweep in ONE launch: a thread-block cluster
-// owns a macro-cell at a time and runs its colours 0..3 with a cluster barrier in
-// between (barrier.cluster arrive.release / wait.acquire), so the cell's slab stays
-// in L2 across the passes and three launches per sweep disappear. Neighbour values
-// are read from L2 (ld.global.cg): other CTAs of the cluster rewrite them between
-// barriers. Clusters never wait on each other.
-template < typename T, bool VAR >
-__global__ void __launch_bounds__( 256 ) k_sor_interior_cluster( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                                 const T* __restrict__ rhs, T relax )
-{
-   cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
-   const int csize     = int( cluster.num_blocks() );
-   const int crank     = int( cluster.block_rank() );
-   const int nClusters = int( gridDim.x ) / csize;
-   const int clusterId = int( blockIdx.x ) / csize;
-   const int nw        = csize * int( blockDim.x >> 5 );
-   const int gw        = crank * int( blockDim.x >> 5 ) + int( threadIdx.x >> 5 );
-   const int lane      = threadIdx.x & 31;
-   for ( int cell = clusterId; cell < tp.nC; cell += nClusters )
-   {
+      const int       item = ( colour & 1 ) ? nItems_ - 1 - it_ : it_;
+      const int       cell = item / nChunks;
+      PointBatch< K > pb;
+      pb.load( pts, lv.blk, nPts, ( item - cell * nChunks ) * 32 * K + int( threadIdx.x & 31 ) );
       InteriorOp< T, VAR > io;
       io.load( op, cell );
       T* __restrict__ uc       = u + size_t( cell ) * lv.stride;
       const T* __restrict__ bc = rhs + size_t( cell ) * lv.stride;
-      for ( int colour = 0; colour < kInteriorColours; ++colour )
+      T v[K];
+#pragma unroll
+      for ( int k = 0; k < K; ++k )
       {
-         for ( int seg = gw; seg < lv.nSorSeg; seg += nw )
-         {
-            const int32_t sp = lv.sorSeg[seg];
-            const int     z = sp & 1023, y = ( sp >> 10 ) & 1023;
-            const int     x = colourX( ( sp >> 20 ) + lane, y, z, colour );
-            if ( x + y + z > lv.N - 1 )
-               continue;
-            const int    base = cidx( lv.W, x, y, z );
-            const NbrOff no   = nbrOffsets( lv.W, y, z );
-            T            diag, off;
-            io.template row< true >( uc, base, no, diag, off );
-            uc[base] = ( T( 1 ) - relax ) * __ldcg( uc + base ) + relax * ( bc[base] - off ) / diag;
-         }
-         cluster.sync();
+         T         diag, off;
+         const int idx = pb.no[k].d[0] + pb.g[k];
+         io.row( uc, pb.g[k], pb.no[k], diag, off );
+         v[k] = ( T( 1 ) - relax ) * uc[idx] + relax * ( bc[idx] - off ) / diag;
       }
+      // the K points of a batch have one colour, so none reads another's new value
+#pragma unroll
+      for ( int k = 0; k < K; ++k )
+         if ( pb.valid[k] )
+            uc[pb.no[k].d[0] + pb.g[k]] = v[k];
    }
 }
 
@@ -499,22 +520,31 @@ __global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDe
 {
    if ( int( blockIdx.x ) < nCellBlocks )
    {
-      HYB_CELL_LOOP( lv.nSeg )
+      constexpr int K       = interiorBatch< T, VAR >();
+      const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
+      HYB_CELL_LOOP( nChunks )
       {
-         const int     cell = it_ / lv.nSeg;
-         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
-         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-         if ( x + y + z > lv.N - 1 )
-            continue;
+         const int       cell = it_ / nChunks;
+         PointBatch< K > pb;
+         pb.load( lv.pts, lv.blk, lv.nPts, ( it_ - cell * nChunks ) * 32 * K + int( threadIdx.x & 31 ) );
          InteriorOp< T, VAR > io;
          io.load( op, cell );
-         const size_t co   = size_t( cell ) * lv.stride;
-         const int    base = cidx( lv.W, x, y, z );
-         const NbrOff no   = nbrOffsets( lv.W, y, z );
-         T            diag, off;
-         io.row( src + co, base, no, diag, off );
-         const T s      = src[co + base];
-         dst[co + base] = s + relax * ( rhs[co + base] - off - diag * s ) / diag;
+         const size_t co = size_t( cell ) * lv.stride;
+         const T* __restrict__ su = src + co;
+         T v[K];
+#pragma unroll
+         for ( int k = 0; k < K; ++k )
+         {
+            T         diag, off;
+            const int idx = pb.no[k].d[0] + pb.g[k];
+            io.row( su, pb.g[k], pb.no[k], diag, off );
+            const T s = su[idx];
+            v[k]      = s + relax * ( rhs[co + idx] - off - diag * s ) / diag;
+         }
+#pragma unroll
+         for ( int k = 0; k < K; ++k )
+            if ( pb.valid[k] )
+               dst[co + pb.no[k].d[0] + pb.g[k]] = v[k];
       }
       return;
    }
@@ -544,7 +574,7 @@ __device__ __forceinline__ T interpolateFine( const T* __restrict__ coarse, int 
 {
    const int px = X & 1, py = Y & 1, pz = Z & 1;
    if ( !( px | py | pz ) )
-      return coarse[cidx( Wc, X >> 1, Y >> 1, Z >> 1 )];
+      return coarse[sidx( Wc, X >> 1, Y >> 1, Z >> 1 )];
    int       ox = 0, oy = 0, oz = 0;
    const int pat = px | ( py << 1 ) | ( pz << 2 );
    switch ( pat )
@@ -557,8 +587,8 @@ __device__ __forceinline__ T interpolateFine( const T* __restrict__ coarse, int 
    case 6: oy = -1; oz = 1; break;
    default: ox = -1; oy = 1; oz = -1; break;
    }
-   return T( 0.5 ) * ( coarse[cidx( Wc, ( X - ox ) >> 1, ( Y - oy ) >> 1, ( Z - oz ) >> 1 )] +
-                       coarse[cidx( Wc, ( X + ox ) >> 1, ( Y + oy ) >> 1, ( Z + oz ) >> 1 )] );
+   return T( 0.5 ) * ( coarse[sidx( Wc, ( X - ox ) >> 1, ( Y - oy ) >> 1, ( Z - oz ) >> 1 )] +
+                       coarse[sidx( Wc, ( X + ox ) >> 1, ( Y + oy ) >> 1, ( Z + oz ) >> 1 )] );
 }
 
 template < typename T, bool ADD >
@@ -576,7 +606,7 @@ __global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, 
          if ( x + y + z > lv.N - 1 )
             continue;
          const T      v  = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
-         const size_t fi = size_t( cell ) * lv.stride + cidx( lv.W, x, y, z );
+         const size_t fi = size_t( cell ) * lv.stride + sidx( lv.W, x, y, z );
          fine[fi]        = ADD ? fine[fi] + v : v;
       }
       return;
@@ -592,7 +622,7 @@ __global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, 
       embeddingCoords( embAt( tp, p.kind, p.prim, 0 ), p.kind, lv.N, p.i, p.j, c, x, y, z );
       T v = interpolateFine( coarse + size_t( c ) * strideC, Wc, x, y, z );
       if ( ADD )
-         v += fine[size_t( c ) * lv.stride + cidx( lv.W, x, y, z )];
+         v += fine[size_t( c ) * lv.stride + sidx( lv.W, x, y, z )];
       // every lane of the group has read the old value before any replica is written
       __syncwarp( __activemask() );
       bdryWriteGroup( tp, lv, p, tk, fine, v );
@@ -618,14 +648,15 @@ __global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, in
          const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
          if ( x + y + z > lv.N - 1 )
             continue;
-         const T*     f    = fine + size_t( cell ) * strideF;
-         const int    base = cidx( Wf, 2 * x, 2 * y, 2 * z );
-         const NbrOff no   = nbrOffsets( Wf, 2 * y, 2 * z );
-         T            s    = 0;
+         // the fine point 2P = (4g' + r', 2y, 2z) with r' = 2x mod 4, g' = 2x div 4
+         const T*     f  = fine + size_t( cell ) * strideF;
+         const int    gf = ( 2 * x ) >> 2;
+         const NbrOff no = residueNbr( Wf, 2 * y, 2 * z, ( 2 * x ) & 3 );
+         T            s  = 0;
 #pragma unroll
          for ( int q = 1; q < 15; ++q )
-            s += f[base + no.d[q]];
-         coarse[size_t( cell ) * lv.stride + cidx( lv.W, x, y, z )] = f[base] + T( 0.5 ) * s;
+            s += f[no.d[q] + gf];
+         coarse[size_t( cell ) * lv.stride + sidx( lv.W, x, y, z )] = f[no.d[0] + gf] + T( 0.5 ) * s;
       }
       return;
    }
@@ -649,14 +680,13 @@ __global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, in
             const ClassDev* cc    = tp.cls + size_t( c ) * 16;
             const int       mask  = classMask( Nf, X, Y, Z );
             const uint32_t  valid = kValidOffsets[mask];
-            const int       base  = cidx( Wf, X, Y, Z );
-            const NbrOff    no    = nbrOffsets( Wf, Y, Z );
-            acc += T( cc[mask].invN ) * f[base];
+            acc += T( cc[mask].invN ) * f[sidx( Wf, X, Y, Z )];
             for ( int q = 1; q < 15; ++q )
                if ( valid & ( 1u << q ) )
                {
-                  const int mq = classMask( Nf, X + offX( q ), Y + offY( q ), Z + offZ( q ) );
-                  acc += T( 0.5 * cc[mq].invN ) * f[base + no.d[q]];
+                  const int xq = X + offX( q ), yq = Y + offY( q ), zq = Z + offZ( q );
+                  const int mq = classMask( Nf, xq, yq, zq );
+                  acc += T( 0.5 * cc[mq].invN ) * f[sidx( Wf, xq, yq, zq )];
                }
          }
       }
