@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -12,6 +13,7 @@
 
 #include "../../include/hyteg_b200.h"
 #include "hyb_kernels.cuh"
+#include "hyb_program.cuh"
 #include "topology.hpp"
 
 namespace hyb {
@@ -119,6 +121,7 @@ struct Storage
    DevBuf< int32_t >                     cellOrder;  // [nC] local vertex indices sorted by global id, 2 bits each
    TopoDev                               td{};
    std::vector< std::unique_ptr< LevelHost > > lv;
+   DevBuf< LevelDev >                    lvTable; // LevelDev of every level, for the program kernel
    DevBuf< double >                      partial; // dot-product partials
    DevBuf< double >                      scalars; // device scalars (dot results)
    double*                               hostScalar = nullptr;
@@ -346,6 +349,12 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
          lh->colourList.upload( flat );
       }
       s.lv.push_back( std::move( lh ) );
+   }
+   {
+      std::vector< LevelDev > t;
+      for ( auto& lh : s.lv )
+         t.push_back( lh->dev );
+      s.lvTable.upload( t );
    }
    s.partial.alloc( maxPartial );
    s.scalars.alloc( 64 );
@@ -928,6 +937,17 @@ struct Gmg
    // different streams at the same time: scalars[0] = ||r||^2, scalars[1] = ||b||^2
    DevBuf< double >            partial, scalars;
    double*                     hostScalar = nullptr; // pinned, 2 doubles
+   // Levels <= progTop of a V-cycle run as one program-kernel launch (-1: none), with one
+   // recorded phase list per (x, b, compute type, top level).
+   int progTop = -1;
+   struct Program
+   {
+      const void*     x;
+      const void*     b;
+      int             dtype, top, n;
+      DevBuf< Phase > phases;
+   };
+   std::vector< std::unique_ptr< Program > > programs;
    cudaStream_t                cap = nullptr; // capture stream
    // captured graphs keyed by (x, b, level, kind)
    struct G
@@ -981,9 +1001,217 @@ void coarseSolve( Gmg& g, float* x, const float* b, cudaStream_t stream )
    launchConvert< float, double >( *g.st, l, x, g.cx64->ptr< double >( l ), stream );
 }
 
+// ---------------------------------------------------------------------------
+// Program-kernel V-cycle for the small levels: the phases mirror vcycle() below, launch
+// for launch, with each launch's grid as the phase's virtual grid.
+// ---------------------------------------------------------------------------
+// levels whose slabs hold at most this many points (all cells) run in the program kernel;
+// HYB_PROGRAM_MAX_POINTS overrides it (0: never)
+constexpr long kProgramMaxPoints = 4096;
+
+struct PhaseList
+{
+   const Gmg&           g;
+   std::vector< Phase > ph;
+
+   // one thread block runs the program: a phase has one virtual block for its cell-interior
+   // loop (if the launch it replaces has one) and one for its surface or flat loop
+   Phase& add( int kind, int level, int blocks, int cellBlocks )
+   {
+      Phase P{};
+      P.kind       = kind;
+      P.level      = level;
+      P.cellBlocks = cellBlocks > 0 ? 1 : 0;
+      P.blocks     = std::max( P.cellBlocks + ( blocks > cellBlocks ? 1 : 0 ), 1 );
+      P.op32       = g.op->dev< float >( level );
+      P.op64       = g.op->dev< double >( level );
+      ph.push_back( P );
+      return ph.back();
+   }
+   long slabElems( int l ) const { return long( g.st->td.nC ) * g.st->L( l ).dev.stride; }
+   int  flatBlocks( long n ) const
+   {
+      return int( std::min< long >( ( n + 127 ) / 128, long( g.st->numSMs ) * 8 ) );
+   }
+
+   template < typename T >
+   void smooth( int l, T* x, const T* b, T* scratch )
+   {
+      const Storage& s = *g.st;
+      const auto&    L = s.L( l );
+      if ( g.smoother == HYB_SMOOTHER_SOR )
+      {
+         for ( int c = 0; c < s.td.m; ++c )
+         {
+            const int* co    = &L.colourOff[4 * c];
+            const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+            if ( lanes == 0 )
+               continue;
+            const int32_t* list = L.colourList.p + co[0];
+            Phase&         P    = add( kPhSorIface, l, int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) ), 0 );
+            P.p0                = x;
+            P.p1                = const_cast< T* >( b );
+            P.relax             = g.relax;
+            P.flag              = kGmgFlag;
+            P.bl                = BdryLists{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+         }
+         for ( int c = 0; c < kInteriorColours; ++c )
+         {
+            const int count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
+            if ( count == 0 )
+               continue;
+            Phase& P = add( kPhSorInterior, l, L.colourBlocks, L.colourBlocks );
+            P.p0     = x;
+            P.p1     = const_cast< T* >( b );
+            P.relax  = g.relax;
+            P.a0     = c;
+            P.a1     = L.dev.ptsOff[c];
+            P.a2     = count;
+         }
+      }
+      else
+      {
+         Phase& C = add( kPhCopy, l, flatBlocks( slabElems( l ) ), 0 );
+         C.p0     = scratch;
+         C.p1     = x;
+         C.n      = slabElems( l );
+         const int nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+         Phase&    P  = add( kPhJacobi, l, nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 ), nc );
+         P.p0         = scratch;
+         P.p1         = x;
+         P.p2         = const_cast< T* >( b );
+         P.relax      = g.relax;
+         P.flag       = kGmgFlag;
+      }
+   }
+
+   void cg( int l, double* x, const double* b )
+   {
+      Phase& P = add( kPhCg, l, 1, 0 );
+      P.p0     = x;
+      P.p1     = const_cast< double* >( b );
+      P.p2     = g.cg.r->ptr< double >( l );
+      P.p3     = g.cg.p->ptr< double >( l );
+      P.p4     = g.cg.ap->ptr< double >( l );
+      P.status = g.cg.status.p;
+      P.relax  = g.coarseTol;
+      P.a0     = g.coarseMaxIter;
+   }
+
+   void coarse( double* x, const double* b ) { cg( g.minL, x, b ); }
+   void coarse( float* x, const float* b )
+   {
+      const int  l = g.minL;
+      const long n = slabElems( l );
+      Phase&     A = add( kPhToF64, l, flatBlocks( n ), 0 );
+      A.p0         = g.cx64->ptr< double >( l );
+      A.p1         = x;
+      A.n          = n;
+      Phase& B     = add( kPhToF64, l, flatBlocks( n ), 0 );
+      B.p0         = g.cb64->ptr< double >( l );
+      B.p1         = const_cast< float* >( b );
+      B.n          = n;
+      cg( l, g.cx64->ptr< double >( l ), g.cb64->ptr< double >( l ) );
+      Phase& C = add( kPhToF32, l, flatBlocks( n ), 0 );
+      C.p0     = x;
+      C.p1     = g.cx64->ptr< double >( l );
+      C.n      = n;
+   }
+
+   template < typename T >
+   void vcycle( Function& x, Function& b, Function& tmp, int l )
+   {
+      if ( l == g.minL )
+      {
+         coarse( x.ptr< T >( l ), b.ptr< T >( l ) );
+         return;
+      }
+      const Storage& s = *g.st;
+      for ( int i = 0; i < g.pre; ++i )
+         smooth< T >( l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ) );
+      {
+         const auto& L  = s.L( l );
+         const int   nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+         Phase&      P  = add( kPhResidual, l, nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 ), nc );
+         P.p0           = x.ptr< T >( l );
+         P.p1           = tmp.ptr< T >( l );
+         P.p2           = b.ptr< T >( l );
+         P.flag         = kGmgFlag;
+      }
+      {
+         const auto& C  = s.L( l - 1 );
+         const int   nc = C.dev.nSeg > 0 ? C.cellBlocks : 0;
+         Phase&      P  = add( kPhRestrict, l - 1, nc + ( C.dev.nBdry > 0 ? C.bdryBlocks : 0 ), nc );
+         P.p0           = tmp.ptr< T >( l );
+         P.p1           = b.ptr< T >( l - 1 );
+         P.flag         = kGmgFlag;
+      }
+      {
+         Phase& P = add( kPhZero, l - 1, flatBlocks( slabElems( l - 1 ) ), 0 );
+         P.p0     = x.ptr< T >( l - 1 );
+         P.n      = slabElems( l - 1 );
+      }
+      vcycle< T >( x, b, tmp, l - 1 );
+      {
+         const auto& F  = s.L( l );
+         const int   nc = F.dev.nSeg > 0 ? F.cellBlocks : 0;
+         Phase&      P  = add( kPhProlongAdd, l, nc + ( F.dev.nBdry > 0 ? F.bdryBlocks : 0 ), nc );
+         P.p0           = x.ptr< T >( l - 1 );
+         P.p1           = x.ptr< T >( l );
+         P.flag         = kGmgFlag;
+      }
+      for ( int i = 0; i < g.post; ++i )
+         smooth< T >( l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ) );
+   }
+};
+
+// Record (once, outside any stream capture) the program of the sub-cycle at level `top`
+// for the V-cycle on (x, b, tmp) in type T.
+template < typename T >
+void ensureProgram( Gmg& g, Function& x, Function& b, Function& tmp, int top )
+{
+   const int dtype = std::is_same< T, double >::value ? HYB_F64 : HYB_F32;
+   for ( auto& p : g.programs )
+      if ( p->x == &x && p->b == &b && p->dtype == dtype && p->top == top )
+         return;
+   PhaseList pl{ g, {} };
+   pl.vcycle< T >( x, b, tmp, top );
+   auto prog   = std::make_unique< Gmg::Program >();
+   prog->x     = &x;
+   prog->b     = &b;
+   prog->dtype = dtype;
+   prog->top   = top;
+   prog->n     = int( pl.ph.size() );
+   prog->phases.upload( pl.ph );
+   g.programs.push_back( std::move( prog ) );
+}
+
+template < typename T >
+void launchProgram( Gmg& g, Function& x, Function& b, int top, cudaStream_t stream )
+{
+   const int           dtype = std::is_same< T, double >::value ? HYB_F64 : HYB_F32;
+   const Gmg::Program* prog  = nullptr;
+   for ( auto& p : g.programs )
+      if ( p->x == &x && p->b == &b && p->dtype == dtype && p->top == top )
+         prog = p.get();
+   require( prog != nullptr, "program of the coarse V-cycle was not recorded" );
+   const Phase* ph = prog->phases.p;
+   const auto*  lt = (const LevelDev*) g.st->lvTable.p;
+   if ( g.op->variable )
+      k_program< T, true ><<< 1, kProgramThreads, 0, stream >>>( g.st->td, lt, ph, prog->n );
+   else
+      k_program< T, false ><<< 1, kProgramThreads, 0, stream >>>( g.st->td, lt, ph, prog->n );
+   HYB_CHECK_LAUNCH();
+}
+
 template < typename T >
 void vcycle( Gmg& g, Function& x, Function& b, Function& tmp, int l, cudaStream_t stream )
 {
+   if ( l <= g.progTop )
+   {
+      launchProgram< T >( g, x, b, l, stream );
+      return;
+   }
    if ( l == g.minL )
    {
       coarseSolve( g, x.ptr< T >( l ), b.ptr< T >( l ), stream );
@@ -1060,7 +1288,15 @@ void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int
    g.partial.alloc( s->partial.n );
    g.scalars.alloc( 2 );
    HYB_CUDA( cudaMallocHost( &g.hostScalar, 2 * sizeof( double ) ) );
+   long maxPoints = kProgramMaxPoints;
+   if ( const char* e = std::getenv( "HYB_PROGRAM_MAX_POINTS" ) )
+      maxPoints = std::atol( e );
+   g.progTop = -1;
+   for ( int l = minL; l <= maxL; ++l )
+      if ( long( s->td.nC ) * s->L( l ).dev.stride <= maxPoints )
+         g.progTop = l;
 }
+
 
 // the FP32 hierarchy and FP64 residual of the mixed-precision solver
 void ensureMixed( Gmg& g )
@@ -1086,6 +1322,14 @@ void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s
          return;
       }
    prepare( g );
+   if ( g.progTop >= g.minL )
+   {
+      const int top = std::min( l, g.progTop );
+      if ( kind == kCycle64 || kind == kCycle64Norm )
+         ensureProgram< double >( g, x, b, *g.tmp64, top );
+      if ( kind == kMixedStep )
+         ensureProgram< float >( g, *g.x32, *g.b32, *g.t32, top );
+   }
    if ( !g.cap )
       HYB_CUDA( cudaStreamCreateWithFlags( &g.cap, cudaStreamNonBlocking ) );
    // make the capture stream wait for prior work on the caller's stream

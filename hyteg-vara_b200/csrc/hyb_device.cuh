@@ -244,7 +244,7 @@ struct OpDev
 // Partial row of the operator at closure point (x,y,z) of `cell`: the contributions
 // of the micro-tets of this cell only. u = the cell's slab.
 template < typename T, bool VAR >
-__device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* __restrict__ u, int cell, int W, int x, int y,
+__device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* u, int cell, int W, int x, int y,
                                             int z, T& diag, T& off )
 {
    const int         N     = W - 1;

@@ -215,11 +215,19 @@ __device__ __forceinline__ void bdryWriteGroup( const TopoDev& tp, const LevelDe
       dst[bdryReplica< T >( tp, lv, p, e )] = v;
 }
 
+// Block index of a grid-stride loop: the block of a kernel launch, or a virtual block of a
+// phase of the program kernel (which runs many level operations in one launch).
+struct Blk
+{
+   int x, n;
+};
+__device__ __forceinline__ Blk launchBlk() { return Blk{ int( blockIdx.x ), int( gridDim.x ) }; }
+
 // Warp-uniform grid-stride loop over the lanes of the surface-DoF blocks.
 #define HYB_BDRY_LANES( BL )                                                                                         \
    const long total_ = bdryLaneCount( ( BL ).nv, ( BL ).ne, ( BL ).nf );                                             \
-   const int  nbb_   = int( gridDim.x ) - nCellBlocks;                                                               \
-   for ( long gt = long( int( blockIdx.x ) - nCellBlocks ) * blockDim.x + threadIdx.x;                               \
+   const int  nbb_   = vb.n - nCellBlocks;                                                                           \
+   for ( long gt = long( vb.x - nCellBlocks ) * blockDim.x + threadIdx.x;                                            \
          gt - ( threadIdx.x & 31 ) < total_; gt += long( nbb_ ) * blockDim.x )
 
 // ---------------------------------------------------------------------------
@@ -250,7 +258,7 @@ struct InteriorOp
 
    // diag and off-diagonal sum at interior point x = 4g + r whose neighbours sit at
    // no.d[q] + g (residueNbr)
-   __device__ __forceinline__ void row( const T* __restrict__ u, int g, const NbrOff& no, T& diag, T& off ) const
+   __device__ __forceinline__ void row( const T* u, int g, const NbrOff& no, T& diag, T& off ) const
    {
       if constexpr ( !VAR )
       {
@@ -302,7 +310,7 @@ struct InteriorOp
 #define HYB_CELL_LOOP( NSEG )                                                                                        \
    const int wpb_    = int( blockDim.x >> 5 );                                                                       \
    const int nItems_ = tp.nC * ( NSEG );                                                                             \
-   for ( int it_ = int( blockIdx.x ) * wpb_ + int( threadIdx.x >> 5 ); it_ < nItems_; it_ += nCellBlocks * wpb_ )
+   for ( int it_ = vb.x * wpb_ + int( threadIdx.x >> 5 ); it_ < nItems_; it_ += nCellBlocks * wpb_ )
 
 // ---------------------------------------------------------------------------
 // Cell-interior loops run over the level's interior point table: a warp takes 32
@@ -335,10 +343,12 @@ __device__ __forceinline__ NbrOff blockNbr( const int32_t* __restrict__ blk, int
 
 // Interior points per lane and item: independent load chains that the warp keeps in
 // flight together (the loops are latency bound, not bandwidth bound, at one point per lane).
+// Measured on B200 at level 7, two beat one by 1.2-1.3x and beat four for FP32 (four cost
+// registers and with them resident warps).
 template < typename T, bool VAR >
 __host__ __device__ constexpr int interiorBatch()
 {
-   return VAR ? 1 : ( sizeof( T ) == 8 ? 2 : 4 );
+   return VAR ? 1 : 2;
 }
 
 // The K table entries i0 + 32 k of a point table. Entries past the end are clamped to the
@@ -369,11 +379,11 @@ struct PointBatch
 // P1ElementwiseOperator::apply, P1ElementwiseOperator.cpp:64-221)
 // ---------------------------------------------------------------------------
 template < typename T, bool VAR, int MODE >
-__global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
-                                                  T* __restrict__ dst, const T* __restrict__ rhs, int flag,
+__device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, const T* src,
+                                                  T* dst, const T* rhs, int flag,
                                                   int nCellBlocks )
 {
-   if ( int( blockIdx.x ) < nCellBlocks )
+   if ( vb.x < nCellBlocks )
    {
       constexpr int K       = interiorBatch< T, VAR >();
       const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
@@ -385,7 +395,7 @@ __global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev
          InteriorOp< T, VAR > io;
          io.load( op, cell );
          const size_t co = size_t( cell ) * lv.stride;
-         const T* __restrict__ su = src + co;
+         const T* su = src + co;
          T ax[K];
 #pragma unroll
          for ( int k = 0; k < K; ++k )
@@ -435,6 +445,14 @@ __global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev
    }
 }
 
+template < typename T, bool VAR, int MODE >
+__global__ void __launch_bounds__( 128, 8 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
+                                                  T* __restrict__ dst, const T* __restrict__ rhs, int flag,
+                                                  int nCellBlocks )
+{
+   applyBody< T, VAR, MODE >( launchBlk(), tp, lv, op, src, dst, rhs, flag, nCellBlocks );
+}
+
 // ---------------------------------------------------------------------------
 // Multicolour SOR: u <- (1-w) u + w (b - sum_{o!=0} a_o u_o) / a_0 (reference update
 // formula: P1Operator.hpp:1638, sor_3D_macrocell_P1.cpp:31-77). One sweep is
@@ -449,8 +467,8 @@ __global__ void __launch_bounds__( 128 ) k_apply( TopoDev tp, LevelDev lv, OpDev
 constexpr int kInteriorColours = 4;
 
 template < typename T, bool VAR >
-__global__ void __launch_bounds__( 128 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                      const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
+__device__ __forceinline__ void sorIfaceBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, T* u,
+                                                      const T* rhs, T relax, int flag, BdryLists bl )
 {
    const int nCellBlocks = 0;
    HYB_BDRY_LANES( bl )
@@ -470,13 +488,20 @@ __global__ void __launch_bounds__( 128 ) k_sor_iface( TopoDev tp, LevelDev lv, O
    }
 }
 
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                      const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
+{
+   sorIfaceBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, flag, bl );
+}
+
 // One interior colour over all cells: in row (y, z) the points of colour c are the
 // residue block r = (c - 2y - 3z) mod 4, one contiguous run of the row; the colour's point
 // table lists them in storage order. Odd colours walk the cells in reverse order, so a
 // pass starts on the data the previous pass touched last (still in L2).
 template < typename T, bool VAR >
-__global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                         const T* __restrict__ rhs, T relax, int colour, int begin,
+__device__ __forceinline__ void sorInteriorBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, T* u,
+                                                         const T* rhs, T relax, int colour, int begin,
                                                          int nPts, int nCellBlocks )
 {
    constexpr int  K       = interiorBatch< T, VAR >();
@@ -490,8 +515,8 @@ __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv
       pb.load( pts, lv.blk, nPts, ( item - cell * nChunks ) * 32 * K + int( threadIdx.x & 31 ) );
       InteriorOp< T, VAR > io;
       io.load( op, cell );
-      T* __restrict__ uc       = u + size_t( cell ) * lv.stride;
-      const T* __restrict__ bc = rhs + size_t( cell ) * lv.stride;
+      T*       uc = u + size_t( cell ) * lv.stride;
+      const T* bc = rhs + size_t( cell ) * lv.stride;
       T v[K];
 #pragma unroll
       for ( int k = 0; k < K; ++k )
@@ -509,16 +534,24 @@ __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv
    }
 }
 
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                         const T* __restrict__ rhs, T relax, int colour, int begin,
+                                                         int nPts, int nCellBlocks )
+{
+   sorInteriorBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, colour, begin, nPts, nCellBlocks );
+}
+
 // ---------------------------------------------------------------------------
 // Weighted Jacobi (P1Operator::smooth_jac, P1Operator.hpp:424-440):
 // dst = src + relax * (rhs - A src) / diag(A)
 // ---------------------------------------------------------------------------
 template < typename T, bool VAR >
-__global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
-                                                   T* __restrict__ dst, const T* __restrict__ rhs, T relax, int flag,
+__device__ __forceinline__ void jacobiBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, const T* src,
+                                                   T* dst, const T* rhs, T relax, int flag,
                                                    int nCellBlocks )
 {
-   if ( int( blockIdx.x ) < nCellBlocks )
+   if ( vb.x < nCellBlocks )
    {
       constexpr int K       = interiorBatch< T, VAR >();
       const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
@@ -530,7 +563,7 @@ __global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDe
          InteriorOp< T, VAR > io;
          io.load( op, cell );
          const size_t co = size_t( cell ) * lv.stride;
-         const T* __restrict__ su = src + co;
+         const T* su = src + co;
          T v[K];
 #pragma unroll
          for ( int k = 0; k < K; ++k )
@@ -564,13 +597,21 @@ __global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDe
    }
 }
 
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
+                                                   T* __restrict__ dst, const T* __restrict__ rhs, T relax, int flag,
+                                                   int nCellBlocks )
+{
+   jacobiBody< T, VAR >( launchBlk(), tp, lv, op, src, dst, rhs, relax, flag, nCellBlocks );
+}
+
 // ---------------------------------------------------------------------------
 // Linear prolongation (P1toP1LinearProlongation.cpp:194-410): a fine micro-vertex
 // either coincides with a coarse one (weight 1) or bisects a coarse micro-edge
 // (weights 1/2, 1/2). Computed in gather form inside any one adjacent cell.
 // ---------------------------------------------------------------------------
 template < typename T >
-__device__ __forceinline__ T interpolateFine( const T* __restrict__ coarse, int Wc, int X, int Y, int Z )
+__device__ __forceinline__ T interpolateFine( const T* coarse, int Wc, int X, int Y, int Z )
 {
    const int px = X & 1, py = Y & 1, pz = Z & 1;
    if ( !( px | py | pz ) )
@@ -592,11 +633,11 @@ __device__ __forceinline__ T interpolateFine( const T* __restrict__ coarse, int 
 }
 
 template < typename T, bool ADD >
-__global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, int Wc, int strideC,
-                                                       const T* __restrict__ coarse, T* __restrict__ fine, int flag,
+__device__ __forceinline__ void prolongateBody( Blk vb, TopoDev tp, LevelDev lv, int Wc, int strideC,
+                                                       const T* coarse, T* fine, int flag,
                                                        int nCellBlocks )
 {
-   if ( int( blockIdx.x ) < nCellBlocks )
+   if ( vb.x < nCellBlocks )
    {
       HYB_CELL_LOOP( lv.nSeg )
       {
@@ -629,6 +670,14 @@ __global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, 
    }
 }
 
+template < typename T, bool ADD >
+__global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, int Wc, int strideC,
+                                                       const T* __restrict__ coarse, T* __restrict__ fine, int flag,
+                                                       int nCellBlocks )
+{
+   prolongateBody< T, ADD >( launchBlk(), tp, lv, Wc, strideC, coarse, fine, flag, nCellBlocks );
+}
+
 // ---------------------------------------------------------------------------
 // Full-weighting restriction (P1toP1LinearRestriction.cpp:168-345 with the generated
 // pull kernel): r_c(P) = r_f(2P) + 1/2 sum of r_f over the fine neighbours of 2P. A
@@ -636,10 +685,10 @@ __global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, 
 // 1/#cells of the primitive it lies on, so every fine point counts exactly once.
 // ---------------------------------------------------------------------------
 template < typename T >
-__global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, int Wf, int strideF, const T* __restrict__ fine,
-                                                     T* __restrict__ coarse, int flag, int nCellBlocks )
+__device__ __forceinline__ void restrictBody( Blk vb, TopoDev tp, LevelDev lv, int Wf, int strideF, const T* fine,
+                                                     T* coarse, int flag, int nCellBlocks )
 {
-   if ( int( blockIdx.x ) < nCellBlocks )
+   if ( vb.x < nCellBlocks )
    {
       HYB_CELL_LOOP( lv.nSeg )
       {
@@ -694,6 +743,13 @@ __global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, in
       if ( active )
          bdryWriteGroup( tp, lv, p, tk, coarse, acc );
    }
+}
+
+template < typename T >
+__global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, int Wf, int strideF, const T* __restrict__ fine,
+                                                     T* __restrict__ coarse, int flag, int nCellBlocks )
+{
+   restrictBody< T >( launchBlk(), tp, lv, Wf, strideF, fine, coarse, flag, nCellBlocks );
 }
 
 // ---------------------------------------------------------------------------
@@ -1020,11 +1076,11 @@ __device__ void cgAxpby( const TopoDev& tp, const LevelDev& lv, double a, const 
    }
 }
 
+// the whole CG in the calling thread block; red = 32 doubles of shared memory
 template < bool VAR >
-__global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
-                                                double* r, double* p, double* ap, double tol, int maxIter, int* status )
+__device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< double >& op, double* x, const double* b,
+                        double* r, double* p, double* ap, double tol, int maxIter, int* status, double* red )
 {
-   __shared__ double red[32];
    const int flag = 1 | 4 | 8;
    cgApplyAll< VAR >( tp, lv, op, x, p, flag );
    __syncthreads();
@@ -1069,6 +1125,14 @@ __global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< d
       status[0] = it;
       status[1] = conv ? 1 : 2;
    }
+}
+
+template < bool VAR >
+__global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
+                                                double* r, double* p, double* ap, double tol, int maxIter, int* status )
+{
+   __shared__ double red[32];
+   cgBody< VAR >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red );
 }
 
 } // namespace hyb

@@ -1,0 +1,139 @@
+// Program kernel: the small levels of a V-cycle in ONE launch of ONE thread block.
+//
+// On coarse levels every smoother pass, residual and transfer is a launch of a few
+// microseconds, so a V-cycle's coarse part is bound by launch latency, not by work. The
+// host records those level operations as a list of phases (the same bodies the separate
+// kernels run) and a single thread block executes the list, separating consecutive phases
+// by __syncthreads(): within one block that is both the execution and the memory barrier
+// (measured on B200, a grid-wide barrier across blocks costs 1-2.5 us, a kernel node of a
+// CUDA graph about 4 us, __syncthreads a few tens of ns). The small levels' data stays in
+// the multiprocessor's L1.
+#pragma once
+
+#include "hyb_kernels.cuh"
+
+namespace hyb {
+
+enum PhaseKind : int
+{
+   kPhSorIface    = 0, // one interface colour: p0 = u, p1 = rhs, bl, flag, relax
+   kPhSorInterior = 1, // one interior colour: p0 = u, p1 = rhs, a0 = colour, a1 = begin, a2 = count, relax
+   kPhJacobi      = 2, // p0 = src (old iterate), p1 = dst, p2 = rhs, flag, relax
+   kPhCopy        = 3, // p0 = dst, p1 = src, n elements of T
+   kPhResidual    = 4, // p0 = x, p1 = r, p2 = b, flag
+   kPhRestrict    = 5, // p0 = fine, p1 = coarse (level = coarse level), flag
+   kPhProlongAdd  = 6, // p0 = coarse, p1 = fine (level = fine level), flag
+   kPhZero        = 7, // p0 = dst, n elements of T
+   kPhToF64       = 8, // p0 = double dst, p1 = float src, n elements
+   kPhToF32       = 9, // p0 = float dst, p1 = double src, n elements
+   kPhCg          = 10 // FP64 CG on the level: p0 = x, p1 = b, p2 = r, p3 = p, p4 = ap, status, relax = tol, a0 = maxIter
+};
+
+struct Phase
+{
+   int             kind;
+   int             level;      // index into the level table
+   int             blocks;     // virtual blocks: the cell-interior loop's, then the surface loop's
+   int             cellBlocks; // of which the cell-interior loop's
+   int             a0, a1, a2;
+   int             flag;
+   double          relax;
+   long long       n;
+   void*           p0;
+   void*           p1;
+   void*           p2;
+   void*           p3;
+   void*           p4;
+   int*            status;
+   BdryLists       bl;
+   OpDev< float >  op32; // operator of the phase's level in both types
+   OpDev< double > op64;
+};
+
+template < typename T >
+__device__ __forceinline__ const OpDev< T >& phaseOp( const Phase& P );
+template <>
+__device__ __forceinline__ const OpDev< float >& phaseOp< float >( const Phase& P )
+{
+   return P.op32;
+}
+template <>
+__device__ __forceinline__ const OpDev< double >& phaseOp< double >( const Phase& P )
+{
+   return P.op64;
+}
+
+constexpr int kProgramThreads = 512;
+
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, const LevelDev* __restrict__ lvs,
+                                                                const Phase* __restrict__ prog, int nPhases )
+{
+   __shared__ double red[32];
+   for ( int ph = 0; ph < nPhases; ++ph )
+   {
+      const Phase&   P      = prog[ph];
+      const int      kind   = P.kind;
+      const int      blocks = P.blocks;
+      const LevelDev lv     = lvs[P.level];
+      for ( int b = int( blockIdx.x ); b < blocks; b += int( gridDim.x ) )
+      {
+         const Blk       vb{ b, blocks };
+         const long long t0 = (long long) b * blockDim.x + threadIdx.x, step = (long long) blocks * blockDim.x;
+         switch ( kind )
+         {
+         case kPhSorIface:
+            sorIfaceBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.flag, P.bl );
+            break;
+         case kPhSorInterior:
+            sorInteriorBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.a0, P.a1,
+                                       P.a2, P.cellBlocks );
+            break;
+         case kPhJacobi:
+            jacobiBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1, (const T*) P.p2, T( P.relax ),
+                                  P.flag, P.cellBlocks );
+            break;
+         case kPhCopy:
+            for ( long long i = t0; i < P.n; i += step )
+               ( (T*) P.p0 )[i] = ( (const T*) P.p1 )[i];
+            break;
+         case kPhResidual:
+            applyBody< T, VAR, kResidual >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1, (const T*) P.p2,
+                                            P.flag, P.cellBlocks );
+            break;
+         case kPhRestrict:
+         {
+            const LevelDev& F = lvs[P.level + 1];
+            restrictBody< T >( vb, tp, lv, F.W, F.stride, (const T*) P.p0, (T*) P.p1, P.flag, P.cellBlocks );
+            break;
+         }
+         case kPhProlongAdd:
+         {
+            const LevelDev& C = lvs[P.level - 1];
+            prolongateBody< T, true >( vb, tp, lv, C.W, C.stride, (const T*) P.p0, (T*) P.p1, P.flag, P.cellBlocks );
+            break;
+         }
+         case kPhZero:
+            for ( long long i = t0; i < P.n; i += step )
+               ( (T*) P.p0 )[i] = T( 0 );
+            break;
+         case kPhToF64:
+            for ( long long i = t0; i < P.n; i += step )
+               ( (double*) P.p0 )[i] = double( ( (const float*) P.p1 )[i] );
+            break;
+         case kPhToF32:
+            for ( long long i = t0; i < P.n; i += step )
+               ( (float*) P.p0 )[i] = float( ( (const double*) P.p1 )[i] );
+            break;
+         case kPhCg:
+            cgBody< VAR >( tp, lv, P.op64, (double*) P.p0, (const double*) P.p1, (double*) P.p2, (double*) P.p3,
+                           (double*) P.p4, P.relax, P.a0, P.status, red );
+            break;
+         default: break;
+         }
+      }
+      __syncthreads();
+   }
+}
+
+} // namespace hyb

@@ -102,6 +102,9 @@ size_t serveFootprint( const ServeKey& k, int meshMaxLevel )
       maxPartial     = std::max( maxPartial, ( S + 255 ) / 256 * nC );
    }
    bytes += maxPartial * 8 + 2 * 8 + 4 * sizeof( int ) + 4 * kServeModes * 8;
+   // an allowance of 64 KiB per level for the recorded phase list of the coarse-level
+   // program kernel
+   bytes += size_t( k.level + 1 ) * 65536;
    return bytes;
 }
 
@@ -247,6 +250,16 @@ struct Server
       prepare( *in->gmg );
       in->x.reset( makeFunction( st, 0, k.level, HYB_F64 ) );
       in->b.reset( makeFunction( st, 0, k.level, HYB_F64 ) );
+      // record the coarse-level program now, so that the hierarchy's footprint includes it
+      Gmg& g = *in->gmg;
+      if ( g.progTop >= 0 )
+      {
+         const int top = std::min( k.level, g.progTop );
+         if ( k.precision == 32 )
+            ensureProgram< float >( g, *g.x32, *g.b32, *g.t32, top );
+         else
+            ensureProgram< double >( g, *in->x, *in->b, *g.tmp64, top );
+      }
       in->feat.alloc( 4 * kServeModes );
       HYB_CUDA( cudaMallocHost( &in->featHost, 4 * kServeModes * sizeof( double ) ) );
       HYB_CUDA( cudaStreamCreateWithFlags( &in->stream, cudaStreamNonBlocking ) );

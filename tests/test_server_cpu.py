@@ -15,7 +15,8 @@ def H():
 
 def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes=64):
     """Independent restatement of the per-request device bytes (the hierarchy's vectors per
-    level, coefficient storage, coarse CG scratch, dot-product partials, features)."""
+    level, coefficient storage, coarse CG scratch, dot-product partials, features, the
+    coarse-level program kernel's phase list)."""
     nC = 6 * nx * ny * nz
     pad = lambda s: (s + 31) // 32 * 32
     closure = lambda l: ((1 << l) + 1) * ((1 << l) + 2) * ((1 << l) + 3) // 6
@@ -23,6 +24,7 @@ def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes
     b = sum(nC * pad(closure(l)) * per + (nC * 96 * 12 if coeff == 1 else 0) for l in range(level + 1))
     b += nC * pad(4) * 8 * (5 if precision == 32 else 3)
     b += max(-(-closure(l) // 256) * nC for l in range(mesh_max_level + 1)) * 8
+    b += (level + 1) * 65536  # phase-list allowance of the coarse-level program kernel
     return b + 16 + 16 + 4 * modes * 8
 
 
