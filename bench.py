@@ -223,9 +223,19 @@ def ours(args, rank, world, local_rank):
         return {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 3),
                 "peak_source": peak_kind, "traffic": t_bytes}
 
+    varcoef = None
+    if not args.no_varcoef:
+        del y, u32, b32
+        torch.cuda.synchronize()
+        varcoef = variable_coefficient(args, H, I, stream)
+
+    shell = None
+    if not args.no_shell:
+        torch.cuda.synchronize()
+        shell = spherical_shell(args, H, I, stream)
+
     serve = None
     if not args.no_serve:
-        del y, u32, b32
         torch.cuda.synchronize()
         serve = serving(args, H)
         if world > 1:
@@ -261,11 +271,111 @@ def ours(args, rank, world, local_rank):
             "roofline_apply": dict(roof(apply_gbs), kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
             "roofline_sor_fp32": dict(roof(sor32_gbs), kernel="k_sor (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
-            "serving": serve,
+            "variable_coefficient": varcoef, "spherical_shell": shell, "serving": serve,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def variable_coefficient(args, H, I, stream, nc=4, L=6, steps=2):
+    """-div(k grad u) = f with the P1 elementwise operator on the 4x4x4 cuboid (384
+    macro-tets) at level 6; k = exp(g), g a Gaussian random field (correlation length 0.2,
+    sigma 1, seed 1; 64 random Fourier features, evaluated on the device); f ~ U[-1,1]
+    seeded; V(3,3) multicolour SOR, FP64 and FP32-inner/FP64-refinement, each to 1e-8."""
+    import numpy as np
+    import torch
+
+    sh = stream.cuda_stream
+    st = H.PrimitiveStorage.cuboid(nc, nc, nc, L)
+    w, ph = I.grf_features(0.2, 1, 64)
+    A = H.P1ElementwiseDivKGradOperator.random_features(st, 0, L, w, ph, 1.0)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, coarse_tol=1e-12)
+    u, b = H.P1Function("u", st, 0, L), H.P1Function("f", st, 0, L)
+    b.fill_uniform_random(L, 0, float(nc << L), stream=sh)
+    n_unknowns = (nc * (1 << L) - 1) ** 3
+
+    def solve(precision, tol=TOL):
+        u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+        return gmg.solve_to_tolerance(u, b, L, tol, max_cycles=200, precision=precision, stream=sh)
+
+    out = {}
+    for prec in (32, 64):
+        solve(prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hist = [solve(prec) for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[prec] = (ms, len(hist[-1]) - 1, float(hist[-1][-1]))
+    solve(32)
+    u_mixed = u.get(L, stream=sh)
+    solve(64, 1e-13)
+    u_ref = u.get(L, stream=sh)
+    return {"workload": f"-div(k grad u)=f, {nc}x{nc}x{nc} cuboid ({6 * nc ** 3} macro-tets), level {L}, k=exp(GRF "
+                        f"corr 0.2 sigma 1 seed 1), V(3,3) multicolour SOR, to rel. residual 1e-8",
+            "dofs": st.num_dofs(L), "time_to_tol_ms": {"mixed": out[32][0], "fp64": out[64][0]},
+            "speedup_mixed_vs_fp64": out[64][0] / out[32][0], "cycles": {"mixed": out[32][1], "fp64": out[64][1]},
+            "final_rel_residual": {"mixed": out[32][2], "fp64": out[64][2]},
+            "dof_updates_per_s": {"mixed": n_unknowns * out[32][1] / (out[32][0] / 1e3),
+                                  "fp64": n_unknowns * out[64][1] / (out[64][0] / 1e3)},
+            "error_mixed_vs_fp64_solution": float(np.abs(u_mixed - u_ref).max() / np.abs(u_ref).max())}
+
+
+def spherical_shell(args, H, I, stream, ntan=5, nrad=4, L=6):
+    """Thick spherical shell, radii 0.55..1.0, icosahedral tangential resolution ntan = 5,
+    nrad = 4 radii (3 radial layers), affine macro-tets, level 6; -div(k grad u) = f with
+    k = exp(5 (1 - r)) times lognormal noise exp(0.5 g), g a Gaussian random field
+    (correlation length 0.2, seed 2); f ~ U[-1,1] seeded; V(2,2) cycles, mixed precision
+    and FP64, each to 1e-8."""
+    import numpy as np
+    import torch
+
+    sh = stream.cuda_stream
+    t0 = time.perf_counter()
+    st = H.PrimitiveStorage.spherical_shell(ntan, nrad, 0.55, 1.0, L)
+    setup_s = time.perf_counter() - t0
+    w, ph = I.grf_features(0.2, 2, 64)
+    A = H.P1ElementwiseDivKGradOperator.random_features(st, 0, L, w, ph, 0.5, radial=5.0)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, coarse_tol=1e-12)
+    u, b = H.P1Function("u", st, 0, L), H.P1Function("f", st, 0, L)
+    b.fill_uniform_random(L, 0, float(1 << 20), stream=sh)  # points are not on a lattice: a fine one
+    mask = H.P1Function("mask", st, L, L)
+    mask.interpolate(1.0, L, flag=H.INNER | H.NEUMANN)
+    n_unknowns = int(round(mask.dot_global(mask, L, H.INNER | H.NEUMANN)))
+    del mask
+
+    def solve(precision, tol=TOL):
+        u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+        return gmg.solve_to_tolerance(u, b, L, tol, max_cycles=300, precision=precision, stream=sh)
+
+    out = {}
+    for prec in (32, 64):
+        solve(prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hist = solve(prec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[prec] = (e0.elapsed_time(e1), len(hist) - 1, float(hist[-1]))
+    solve(32)
+    u_mixed = u.get(L, stream=sh)
+    solve(64, 1e-12)
+    u_ref = u.get(L, stream=sh)
+    m_col, _ = st.colouring()
+    return {"workload": f"spherical shell ntan={ntan} nrad={nrad} (3 radial layers) r in [0.55, 1], "
+                        f"{int(st.counts()[3])} macro-tets, level {L}, "
+                        f"k=exp(5(1-r))*exp(0.5 GRF corr 0.2 seed 2), V(2,2) multicolour SOR, to rel. residual 1e-8",
+            "dofs": st.num_dofs(L), "unknowns": n_unknowns, "interface_colours": m_col, "setup_s": setup_s,
+            "time_to_tol_ms": {"mixed": out[32][0], "fp64": out[64][0]},
+            "speedup_mixed_vs_fp64": out[64][0] / out[32][0], "cycles": {"mixed": out[32][1], "fp64": out[64][1]},
+            "final_rel_residual": {"mixed": out[32][2], "fp64": out[64][2]},
+            "dof_updates_per_s": {"mixed": n_unknowns * out[32][1] / (out[32][0] / 1e3),
+                                  "fp64": n_unknowns * out[64][1] / (out[64][0] / 1e3)},
+            "error_mixed_vs_fp64_solution": float(np.abs(u_mixed - u_ref).max() / np.abs(u_ref).max())}
 
 
 def serve_stream(n, rate, seed, levels=(3, 7), cubes=(1, 4)):
@@ -435,6 +545,8 @@ def main():
     ap.add_argument("--cubes", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--no-varcoef", action="store_true", help="skip the variable-coefficient leg")
+    ap.add_argument("--no-shell", action="store_true", help="skip the spherical-shell leg")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving-stream leg")
     ap.add_argument("--rate", type=float, default=200.0, help="serving arrival rate, requests/s")
     ap.add_argument("--serve-requests", type=int, default=100)

@@ -629,27 +629,29 @@ Operator* makeDivKGrad( Storage* s, int minL, int maxL, const std::vector< std::
 // Gaussian random field) written into the operator's nodal coefficient on every level, FP64
 // and its FP32 copy; dW (modes x 3) and dPhase are device arrays. Asynchronous on `stream`;
 // the slabs keep their addresses, so graphs captured with the operator stay valid.
-void fillRff( Operator& op, const double* dW, const double* dPhase, int modes, double sigma, cudaStream_t stream )
+void fillRff( Operator& op, const double* dW, const double* dPhase, int modes, double sigma, double radial,
+              cudaStream_t stream )
 {
    const Storage& s = *op.st;
    for ( int l = op.minL; l <= op.maxL; ++l )
    {
       const auto& L = s.L( l );
       k_fill_rff_coefficient< double ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>(
-          s.td, L.dev, s.cellCoords.p, s.cellOrder.p, op.kap64->ptr< double >( l ), dW, dPhase, modes, sigma );
+          s.td, L.dev, s.cellCoords.p, s.cellOrder.p, op.kap64->ptr< double >( l ), dW, dPhase, modes, sigma, radial );
       HYB_CHECK_LAUNCH();
       launchConvert< float, double >( s, l, op.kap32->ptr< float >( l ), op.kap64->ptr< double >( l ), stream );
    }
 }
 
-Operator* makeDivKGradRff( Storage* s, int minL, int maxL, const double* w, const double* phase, int modes, double sigma )
+Operator* makeDivKGradRff( Storage* s, int minL, int maxL, const double* w, const double* phase, int modes, double sigma,
+                           double radial )
 {
    require( modes > 0 && w && phase, "random-feature parameters missing" );
    DevBuf< double > dw, dp;
    dw.upload( std::vector< double >( w, w + 3 * modes ) );
    dp.upload( std::vector< double >( phase, phase + modes ) );
    std::unique_ptr< Operator > op( makeDivKGradWith( s, minL, maxL, []( int, double* ) {} ) );
-   fillRff( *op, dw.p, dp.p, modes, sigma, 0 );
+   fillRff( *op, dw.p, dp.p, modes, sigma, radial, 0 );
    HYB_CUDA( cudaDeviceSynchronize() );
    return op.release();
 }
@@ -1432,6 +1434,19 @@ int hyb_storage_create( const double* coords, int64_t nv, const int64_t* tets, i
    HYB_API_END
 }
 
+int hyb_storage_create_spherical_shell( int ntan, int nrad, double rmin, double rmax, int maxLevel, hyb_storage** out )
+{
+   HYB_API_BEGIN
+   require( out, "null argument" );
+   std::vector< std::array< double, 3 > > V;
+   std::vector< std::array< int, 4 > >    T;
+   meshSphericalShell( ntan, nrad, rmin, rmax, V, T );
+   auto s = std::make_unique< hyb_storage_s >();
+   buildStorage( *s, V, T, maxLevel );
+   *out = s.release();
+   HYB_API_END
+}
+
 int hyb_storage_create_cuboid( int nx, int ny, int nz, const double* lo, const double* hi, int maxLevel, hyb_storage** out )
 {
    HYB_API_BEGIN
@@ -1735,12 +1750,12 @@ int hyb_operator_create_divkgrad_callback( hyb_storage* s, int minL, int maxL, d
 }
 
 int hyb_operator_create_divkgrad_rff( hyb_storage* s, int minL, int maxL, const double* w, const double* phase,
-                                      int modes, double sigma, hyb_operator** out )
+                                      int modes, double sigma, double radial, hyb_operator** out )
 {
    HYB_API_BEGIN
    require( s && w && phase && out, "null argument" );
    require( modes > 0 && modes <= 4096, "modes must be in [1, 4096]" );
-   *out = reinterpret_cast< hyb_operator* >( makeDivKGradRff( ST( s ), minL, maxL, w, phase, modes, sigma ) );
+   *out = reinterpret_cast< hyb_operator* >( makeDivKGradRff( ST( s ), minL, maxL, w, phase, modes, sigma, radial ) );
    HYB_API_END
 }
 

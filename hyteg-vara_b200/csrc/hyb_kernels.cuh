@@ -784,7 +784,7 @@ __global__ void k_lincomb( TopoDev tp, LevelDev lv, T* __restrict__ dst, int n, 
 // identical values: they depend on the position only).
 //   * uniform right-hand side: f ~ U[-1,1] from a SplitMix64 hash of the point's integer
 //     position on the lattice of spacing 1/lattice and the seed;
-//   * random-Fourier-feature coefficient: k = exp( sigma sqrt(2/M) sum_m cos(w_m . x + p_m) ).
+//   * random-Fourier-feature coefficient: k = exp( radial (1 - |x|) + sigma sqrt(2/M) sum_m cos(w_m . x + p_m) ).
 // Cell geometry: cellCoords[c] = 4 vertices x 3 in the cell's local order; cellOrder[c] packs
 // the local indices of the vertices sorted by global id (2 bits each). The position is the
 // barycentric sum taken in global vertex order, so every replica of a shared point (whose
@@ -842,7 +842,7 @@ template < typename T >
 __global__ void k_fill_rff_coefficient( TopoDev tp, LevelDev lv, const double* __restrict__ cellCoords,
                                         const int32_t* __restrict__ cellOrder, T* __restrict__ dst,
                                         const double* __restrict__ w, const double* __restrict__ phase, int modes,
-                                        double sigma )
+                                        double sigma, double radial )
 {
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
@@ -854,7 +854,8 @@ __global__ void k_fill_rff_coefficient( TopoDev tp, LevelDev lv, const double* _
    double g = 0;
    for ( int m = 0; m < modes; ++m )
       g += cos( w[3 * m] * p[0] + w[3 * m + 1] * p[1] + w[3 * m + 2] * p[2] + phase[m] );
-   dst[size_t( cell ) * lv.stride + idx] = T( exp( sigma * sqrt( 2.0 / modes ) * g ) );
+   const double r = sqrt( p[0] * p[0] + p[1] * p[1] + p[2] * p[2] );
+   dst[size_t( cell ) * lv.stride + idx] = T( exp( radial * ( 1.0 - r ) + sigma * sqrt( 2.0 / modes ) * g ) );
 }
 
 // VertexDoFFunction::interpolate(constant, level, flag)

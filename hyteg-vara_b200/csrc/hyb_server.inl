@@ -332,7 +332,7 @@ void startRequest( Server& sv, ServeRequest& r, Instance& in )
    {
       rffFeatures( r.d.seed, kServeCorrLen, kServeModes, in.featHost, in.featHost + 3 * kServeModes );
       HYB_CUDA( cudaMemcpyAsync( in.feat.p, in.featHost, 4 * kServeModes * sizeof( double ), cudaMemcpyHostToDevice, s ) );
-      fillRff( *in.ownOp, in.feat.p, in.feat.p + 3 * kServeModes, kServeModes, kServeSigma, s );
+      fillRff( *in.ownOp, in.feat.p, in.feat.p + 3 * kServeModes, kServeModes, kServeSigma, 0.0, s );
    }
    const auto& Lh = st.L( L );
    k_fill_uniform_hash< double ><<< dim3( Lh.slabBlocks, st.td.nC ), 256, 0, s >>>(

@@ -1,5 +1,6 @@
 // Host-side macro-mesh topology (see topology.hpp).
 #include "topology.hpp"
+#include <map>
 
 #include <algorithm>
 #include <cmath>
@@ -305,6 +306,123 @@ void meshCuboid( int nx, int ny, int nz, const double lo[3], const double hi[3],
                cells.insert( c );
             }
    T.assign( cells.begin(), cells.end() );
+}
+
+// Thick spherical shell (the mesh family of MeshInfo::meshSphericalShell,
+// src/hyteg/mesh/MeshGenSphericalShell.cpp:579-690): the 20 faces of the icosahedron are
+// each cut into (ntan - 1)^2 triangles, projected onto the unit sphere, and the sphere is
+// repeated on nrad radii evenly spaced in [rmin, rmax]; every prism between two radii is
+// split into three tetrahedra. This gives the reference's cell count,
+// 60 (ntan - 1)^2 (nrad - 1), and vertex count, (10 (ntan - 1)^2 + 2) nrad, with affine
+// macro-cells, but the triangulation of the sphere is this function's own (uniform
+// barycentric subdivision of the icosahedron faces), not the reference's diamond meshing.
+// Shared sphere points are computed once, from a canonical key, so coincident vertices
+// are bitwise equal. Prism split: with the triangle's vertices in ascending id order
+// (0, 1, 2) and b/t its bottom/top copies, the tetrahedra (b0 b1 b2 t2), (b0 b1 t1 t2),
+// (b0 t0 t1 t2) cut every quadrilateral side from its lower-id bottom vertex to its
+// higher-id top vertex, so neighbouring prisms agree on the shared diagonal.
+void meshSphericalShell( int ntan, int nrad, double rmin, double rmax, std::vector< std::array< double, 3 > >& V,
+                         std::vector< std::array< int, 4 > >& T )
+{
+   if ( ntan < 2 || nrad < 2 )
+      throw std::invalid_argument( "meshSphericalShell: need ntan >= 2 and nrad >= 2" );
+   if ( !( rmin > 0 ) || !( rmin < rmax ) )
+      throw std::invalid_argument( "meshSphericalShell: need 0 < rmin < rmax" );
+   const int    n   = ntan - 1;
+   const double phi = ( 1.0 + std::sqrt( 5.0 ) ) / 2.0;
+   // icosahedron: cyclic permutations of (0, +-1, +-phi)
+   std::vector< std::array< double, 3 > > ico;
+   for ( int a : { -1, 1 } )
+      for ( int b : { -1, 1 } )
+      {
+         ico.push_back( { 0.0, double( a ), b * phi } );
+         ico.push_back( { double( a ), b * phi, 0.0 } );
+         ico.push_back( { b * phi, 0.0, double( a ) } );
+      }
+   auto dist2 = [&]( int i, int j ) {
+      double d = 0;
+      for ( int k = 0; k < 3; ++k )
+         d += ( ico[i][k] - ico[j][k] ) * ( ico[i][k] - ico[j][k] );
+      return d;
+   };
+   // faces: triples of mutually adjacent vertices (edge length 2)
+   std::vector< std::array< int, 3 > > faces;
+   for ( int i = 0; i < 12; ++i )
+      for ( int j = i + 1; j < 12; ++j )
+         for ( int k = j + 1; k < 12; ++k )
+            if ( std::fabs( dist2( i, j ) - 4 ) < 1e-9 && std::fabs( dist2( i, k ) - 4 ) < 1e-9 &&
+                 std::fabs( dist2( j, k ) - 4 ) < 1e-9 )
+               faces.push_back( { i, j, k } );
+   if ( faces.size() != 20 )
+      throw std::logic_error( "meshSphericalShell: icosahedron construction failed" );
+   // sphere points by canonical key: (kind, a, b, c) with kind 0 vertex (a), 1 edge point
+   // (a < b, c steps from a), 2 face point (face a, i = b, j = c)
+   std::map< std::array< int, 4 >, int >  key2id;
+   std::vector< std::array< double, 3 > > S;
+   auto point = [&]( const std::array< int, 4 >& key, const std::array< double, 3 >& x ) {
+      auto it = key2id.find( key );
+      if ( it != key2id.end() )
+         return it->second;
+      const double r = std::sqrt( x[0] * x[0] + x[1] * x[1] + x[2] * x[2] );
+      S.push_back( { x[0] / r, x[1] / r, x[2] / r } );
+      key2id[key] = int( S.size() ) - 1;
+      return int( S.size() ) - 1;
+   };
+   auto mix = [&]( int a, double wa, int b, double wb, int c, double wc ) {
+      std::array< double, 3 > x;
+      for ( int k = 0; k < 3; ++k )
+         x[k] = ( ico[a][k] * wa + ico[b][k] * wb + ico[c][k] * wc ) / n;
+      return x;
+   };
+   std::vector< std::array< int, 3 > > tris;
+   for ( int f = 0; f < 20; ++f )
+   {
+      const int a = faces[f][0], b = faces[f][1], c = faces[f][2]; // ascending
+      auto      P = [&]( int i, int j ) {
+         const int wa = n - i - j, wb = i, wc = j;
+         if ( wb == 0 && wc == 0 )
+            return point( { 0, a, 0, 0 }, ico[a] );
+         if ( wa == 0 && wc == 0 )
+            return point( { 0, b, 0, 0 }, ico[b] );
+         if ( wa == 0 && wb == 0 )
+            return point( { 0, c, 0, 0 }, ico[c] );
+         if ( wc == 0 )
+            return point( { 1, a, b, wb }, mix( a, wa, b, wb, c, 0 ) );
+         if ( wb == 0 )
+            return point( { 1, a, c, wc }, mix( a, wa, c, wc, b, 0 ) );
+         if ( wa == 0 )
+            return point( { 1, b, c, wc }, mix( b, wb, c, wc, a, 0 ) );
+         return point( { 2, f, i, j }, mix( a, wa, b, wb, c, wc ) );
+      };
+      for ( int j = 0; j < n; ++j )
+         for ( int i = 0; i + j < n; ++i )
+         {
+            tris.push_back( { P( i, j ), P( i + 1, j ), P( i, j + 1 ) } );
+            if ( i + j + 1 < n )
+               tris.push_back( { P( i + 1, j ), P( i + 1, j + 1 ), P( i, j + 1 ) } );
+         }
+   }
+   const int nS = int( S.size() );
+   V.clear();
+   T.clear();
+   for ( int l = 0; l < nrad; ++l )
+   {
+      const double r = rmin + ( rmax - rmin ) * l / ( nrad - 1 );
+      for ( const auto& x : S )
+         V.push_back( { r * x[0], r * x[1], r * x[2] } );
+   }
+   for ( auto t : tris )
+   {
+      std::sort( t.begin(), t.end() );
+      for ( int l = 0; l + 1 < nrad; ++l )
+      {
+         const int b0 = l * nS + t[0], b1 = l * nS + t[1], b2 = l * nS + t[2];
+         const int t0 = b0 + nS, t1 = b1 + nS, t2 = b2 + nS;
+         T.push_back( { b0, b1, b2, t2 } );
+         T.push_back( { b0, b1, t1, t2 } );
+         T.push_back( { b0, t0, t1, t2 } );
+      }
+   }
 }
 
 } // namespace hyb

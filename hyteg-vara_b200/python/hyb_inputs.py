@@ -69,3 +69,13 @@ def grf_coefficient(xyz, corr_len=0.2, sigma=1.0, seed=1, modes=64):
     w, ph = grf_features(corr_len, seed, modes)
     g = sigma * np.sqrt(2.0 / modes) * np.cos(np.asarray(xyz) @ w.T + ph).sum(axis=1)
     return np.exp(g)
+
+
+def shell_coefficient(xyz, radial=5.0, sigma=0.5, seed=2, corr_len=0.2, modes=64):
+    """k = exp(radial (1 - r)) times lognormal noise exp(sigma g), g a Gaussian random field
+    (random Fourier features of correlation length corr_len)."""
+    w, ph = grf_features(corr_len, seed, modes)
+    x = np.asarray(xyz)
+    r = np.sqrt((x * x).sum(axis=1))
+    g = sigma * np.sqrt(2.0 / modes) * np.cos(x @ w.T + ph).sum(axis=1)
+    return np.exp(radial * (1.0 - r) + g)

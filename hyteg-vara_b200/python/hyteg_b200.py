@@ -33,6 +33,7 @@ SYMBOLS = [
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
     "hyb_operator_create_divkgrad_rff", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
+    "hyb_storage_create_spherical_shell",
 ]
 
 COEFF_CONSTANT, COEFF_LOGNORMAL = 0, 1
@@ -107,7 +108,8 @@ def load(path=LIB_PATH):
         "hyb_gmg_solve_to_tolerance": (I, [P, P, P, I, D, I, I, P, P, P]),
         "hyb_function_dot_noalloc": (I, [P, P, I, I, P, P]),
         "hyb_function_fill_uniform_random": (I, [P, I, ctypes.c_uint64, D, P]),
-        "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, PP]),
+        "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, D, PP]),
+        "hyb_storage_create_spherical_shell": (I, [I, I, D, D, I, PP]),
         "hyb_server_create": (I, [ctypes.c_size_t, I, I, PP]),
         "hyb_server_destroy": (I, [P]),
         "hyb_server_footprint": (I, [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
@@ -164,6 +166,16 @@ class PrimitiveStorage:
     @classmethod
     def cuboid(cls, nx, ny, nz, max_level, lo=(0, 0, 0), hi=(1, 1, 1)):
         return cls(cuboid=(nx, ny, nz, lo, hi), max_level=max_level)
+
+    @classmethod
+    def spherical_shell(cls, ntan, nrad, rmin, rmax, max_level):
+        """MeshInfo::meshSphericalShell(ntan, nrad, rmin, rmax) family (own sphere triangulation)."""
+        st = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        _check(load().hyb_storage_create_spherical_shell(ntan, nrad, float(rmin), float(rmax), max_level,
+                                                         ctypes.byref(h)))
+        st.h, st.max_level = h, max_level
+        return st
 
     def close(self):
         if getattr(self, "h", None):
@@ -336,8 +348,9 @@ class P1ElementwiseDivKGradOperator(_Operator):
         self.h = h
 
     @classmethod
-    def random_features(cls, storage, min_level, max_level, w, phase, sigma):
-        """k(x) = exp(sigma sqrt(2/M) sum_m cos(w_m . x + phase_m)), evaluated on the device."""
+    def random_features(cls, storage, min_level, max_level, w, phase, sigma, radial=0.0):
+        """k(x) = exp(radial (1 - |x|) + sigma sqrt(2/M) sum_m cos(w_m . x + phase_m)),
+        evaluated on the device."""
         w = np.ascontiguousarray(w, np.float64).reshape(-1, 3)
         phase = np.ascontiguousarray(phase, np.float64).ravel()
         assert w.shape[0] == phase.shape[0]
@@ -345,7 +358,8 @@ class P1ElementwiseDivKGradOperator(_Operator):
         op.storage = storage
         h = ctypes.c_void_p()
         _check(load().hyb_operator_create_divkgrad_rff(storage.h, min_level, max_level, w.ctypes.data,
-                                                       phase.ctypes.data, w.shape[0], float(sigma), ctypes.byref(h)))
+                                                       phase.ctypes.data, w.shape[0], float(sigma), float(radial),
+                                                       ctypes.byref(h)))
         op.h = h
         return op
 

@@ -8,6 +8,8 @@
  *                                 setMeshBoundaryFlagsOnBoundary(1,0,true) + PrimitiveStorage
  *                                 (src/hyteg/primitivestorage/SetupPrimitiveStorage.hpp:52,136)
  *   hyb_storage_create_cuboid     MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:34-160)
+ *   hyb_storage_create_spherical_shell  MeshInfo::meshSphericalShell (MeshGenSphericalShell.cpp:579-690;
+ *                                 same cell and vertex counts, own sphere triangulation)
  *   hyb_function_create           P1Function<V>(name, storage, minLevel, maxLevel)
  *                                 (src/hyteg/p1functionspace/P1Function.hpp:26-27)
  *   hyb_function_interpolate_const  VertexDoFFunction::interpolate(constant, level, flag)
@@ -86,6 +88,9 @@ long long   hyb_kernel_launch_count( void );
 /* ---- storage (macro-mesh + level hierarchy metadata on the device) ---- */
 int     hyb_storage_create( const double* coords, int64_t num_vertices, const int64_t* tets, int64_t num_tets,
                             int max_level, hyb_storage** out );
+/* thick spherical shell: icosahedral sphere with (ntan - 1)^2 triangles per icosahedron
+ * face on nrad radii in [rmin, rmax], prisms split into three tetrahedra */
+int     hyb_storage_create_spherical_shell( int ntan, int nrad, double rmin, double rmax, int max_level, hyb_storage** out );
 int     hyb_storage_create_cuboid( int nx, int ny, int nz, const double* lo3, const double* hi3, int max_level,
                                    hyb_storage** out );
 int     hyb_storage_destroy( hyb_storage* s );
@@ -149,11 +154,12 @@ int hyb_operator_create_divkgrad( hyb_storage* s, int min_level, int max_level, 
 int hyb_operator_create_divkgrad_callback( hyb_storage* s, int min_level, int max_level,
                                            double ( *k )( const double* xyz, void* ctx ), void* ctx,
                                            hyb_operator** out );
-/* the coefficient k(x) = exp( sigma sqrt(2/modes) sum_m cos( w_m . x + phase_m ) ) (random
- * Fourier features of a Gaussian random field; w is modes x 3, phase has modes entries),
- * evaluated on the device at every micro-vertex of every level; blocking */
+/* the coefficient k(x) = exp( radial (1 - |x|) + sigma sqrt(2/modes) sum_m cos( w_m . x + phase_m ) )
+ * (a radial profile times the exponential of random Fourier features of a Gaussian random
+ * field; w is modes x 3, phase has modes entries), evaluated on the device at every
+ * micro-vertex of every level; blocking */
 int hyb_operator_create_divkgrad_rff( hyb_storage* s, int min_level, int max_level, const double* w,
-                                      const double* phase, int modes, double sigma, hyb_operator** out );
+                                      const double* phase, int modes, double sigma, double radial, hyb_operator** out );
 int hyb_operator_destroy( hyb_operator* op );
 int hyb_operator_apply( hyb_operator* op, hyb_function* src, hyb_function* dst, int level, int flag, int update,
                         void* stream );

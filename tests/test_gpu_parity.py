@@ -310,3 +310,33 @@ def test_device_rff_coefficient_matches_nodal_operator(H, oracle_mod, setups):
         fs.set(x, level)
         A_dev.apply(fs, fd, level, 15)
         close(fd.get(level), orc.apply(x, level, flag=15, op=op), 1e-12)
+
+
+def test_divkgrad_vcycle_and_solve_match_oracle(H, oracle_mod, setups):
+    """Variable-coefficient multigrid: one V(3,3) cycle equals the oracle's multicolour
+    V-cycle with the same coefficient (1e-10), and the mixed-precision solve to 1e-8 agrees
+    with the oracle's FP64 solution (1e-6) in a cycle count within one of the oracle's."""
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    kv = [O.grf_coefficient(orc.coords_of(l), seed=1) for l in range(L + 1)]
+    A = H.P1ElementwiseDivKGradOperator(st, 0, L, kv)
+    op = orc.op_divkgrad(kv)
+    m, labels = st.colouring()
+    b = O.uniform_rhs(orc.coords_of(L), 3, 2 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    gmg.solve(fx, fb, L)
+    x = np.zeros(orc.n(L))
+    orc.gmg(x, b, 0, L, pre=3, post=3, relax=1.0, smoother=1, labels=labels, m=m, coarse_tol=1e-12, max_cycles=1, op=op)
+    close(fx.get(L), x, 1e-10)
+    fx.interpolate(0.0, L, flag=H.ALL)
+    hist = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=60, precision=32)
+    assert hist[-1] <= 1e-8
+    x_oc = np.zeros(orc.n(L))
+    _, h_oc = orc.gmg(x_oc, b, 0, L, pre=3, post=3, smoother=1, labels=labels, m=m, max_cycles=60, rel_tol=1e-8, op=op)
+    assert abs((len(hist) - 1) - (len(h_oc) - 1)) <= 1, (hist, h_oc)
+    xr = np.zeros(orc.n(L))
+    orc.gmg(xr, b, 0, L, pre=3, post=3, smoother=0, max_cycles=100, rel_tol=1e-13, op=op)
+    err = np.abs(fx.get(L) - xr).max() / np.abs(xr).max()
+    assert err < 1e-6, err

@@ -155,3 +155,83 @@ def test_topology_counts_match_oracle(topo_exe, oracle_mod):
     m, valid, ne, nf, labels = run_topo(topo_exe, c, t)
     o = O.Oracle(c, t, 0)
     assert ne == o.num_prims(1) and nf == o.num_prims(2)
+
+
+SHELL_CHECK = r"""
+#include "topology.hpp"
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+using namespace hyb;
+int main( int argc, char** argv )
+{
+   // prints: vertices cells over-shared-faces boundary-faces boundary-off-sphere min-volume total-volume
+   const int ntan = atoi( argv[1] ), nrad = atoi( argv[2] );
+   const double rmin = 0.55, rmax = 1.0;
+   std::vector< std::array< double, 3 > > V;
+   std::vector< std::array< int, 4 > >    T;
+   meshSphericalShell( ntan, nrad, rmin, rmax, V, T );
+   std::map< std::array< int, 3 >, int > fc;
+   double vmin = 1e300, vtot = 0;
+   for ( auto& t : T )
+   {
+      double a[3][3];
+      for ( int k = 0; k < 3; ++k )
+         for ( int d = 0; d < 3; ++d )
+            a[k][d] = V[t[k + 1]][d] - V[t[0]][d];
+      const double det = a[0][0] * ( a[1][1] * a[2][2] - a[1][2] * a[2][1] ) - a[0][1] * ( a[1][0] * a[2][2] - a[1][2] * a[2][0] ) +
+                         a[0][2] * ( a[1][0] * a[2][1] - a[1][1] * a[2][0] );
+      vmin = std::min( vmin, std::fabs( det ) / 6 );
+      vtot += std::fabs( det ) / 6;
+      const int f[4][3] = { { t[0], t[1], t[2] }, { t[0], t[1], t[3] }, { t[0], t[2], t[3] }, { t[1], t[2], t[3] } };
+      for ( auto& ff : f )
+      {
+         std::array< int, 3 > k = { ff[0], ff[1], ff[2] };
+         std::sort( k.begin(), k.end() );
+         fc[k]++;
+      }
+   }
+   int over = 0, bdry = 0, off = 0;
+   for ( auto& kv : fc )
+   {
+      if ( kv.second > 2 ) ++over;
+      if ( kv.second == 1 )
+      {
+         ++bdry;
+         for ( int v : kv.first )
+         {
+            const double r = std::sqrt( V[v][0] * V[v][0] + V[v][1] * V[v][1] + V[v][2] * V[v][2] );
+            if ( std::fabs( r - rmin ) > 1e-12 && std::fabs( r - rmax ) > 1e-12 ) ++off;
+         }
+      }
+   }
+   printf( "%zu %zu %d %d %d %.17g %.17g\n", V.size(), T.size(), over, bdry, off, vmin, vtot );
+   return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("ntan,nrad", [(2, 2), (3, 2), (5, 4)])
+def test_spherical_shell_mesh(tmp_path, ntan, nrad):
+    """meshSphericalShell: the reference's cell and vertex counts, a conforming
+    tetrahedralisation (no face shared by more than two cells), boundary faces only on the
+    two spheres, no degenerate cell, and a volume close to the shell's (it grows towards the
+    exact one as the sphere is refined)."""
+    src = tmp_path / "shell_check.cpp"
+    src.write_text(SHELL_CHECK)
+    exe = tmp_path / "shell_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(PKG, "csrc"), str(src),
+                    os.path.join(PKG, "csrc", "topology.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe), str(ntan), str(nrad)], capture_output=True, text=True, check=True).stdout.split()
+    nv, nc, over, bdry, off = map(int, out[:5])
+    vmin, vtot = map(float, out[5:])
+    n = ntan - 1
+    assert nc == 60 * n * n * (nrad - 1)
+    assert nv == (10 * n * n + 2) * nrad
+    assert over == 0 and off == 0
+    assert bdry == 2 * 20 * n * n
+    assert vmin > 0
+    exact = 4.0 / 3.0 * np.pi * (1.0 - 0.55 ** 3)
+    assert 0.5 * exact < vtot < exact
