@@ -258,24 +258,39 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
                continue;
             for ( int x0 = 1; x0 <= len; x0 += 32 )
                seg.push_back( z | ( y << 10 ) | ( x0 << 20 ) );
-            // residue blocks of the row in storage order: r = 0..3, g ascending
-            for ( int r = 0; r < 4; ++r )
-            {
-               const int b = int( blk.size() / 16 );
-               require( b < ( 1 << 23 ), "too many residue blocks for the point-table encoding" );
-               const NbrOff no = residueNbr( d.W, y, z, r );
-               for ( int q = 0; q < 16; ++q )
-                  blk.push_back( q < 15 ? no.d[q] : 0 );
-               const int c = ( r + 2 * y + 3 * z ) & 3;
-               for ( int g = 0; 4 * g + r <= len; ++g )
-               {
-                  if ( 4 * g + r < 1 )
-                     continue;
-                  pts.push_back( g | ( b << 8 ) );
-                  ptsC[c].push_back( g | ( b << 8 ) );
-               }
-            }
          }
+      // interior point tables: points in storage order, cut into blocks of consecutive
+      // positions whose neighbour offsets agree (checked, not assumed from the layout)
+      {
+         std::vector< std::array< int, 2 > > order; // (position, packed x | y << 10 | z << 20)
+         for ( int z = 1; z <= d.N; ++z )
+            for ( int y = 1; y + z <= d.N - 2; ++y )
+               for ( int x = 1; x + y + z <= d.N - 1; ++x )
+                  order.push_back( { sidx( d.W, x, y, z ), x | ( y << 10 ) | ( z << 20 ) } );
+         std::sort( order.begin(), order.end() );
+         int prevPos = -2, start = 0;
+         int prevD[15] = {};
+         for ( const auto& o : order )
+         {
+            const int x = o[1] & 1023, y = ( o[1] >> 10 ) & 1023, z = o[1] >> 20;
+            int       D[15];
+            for ( int q = 0; q < 15; ++q )
+               D[q] = sidx( d.W, x + offX( q ), y + offY( q ), z + offZ( q ) ) - o[0];
+            const bool same = o[0] == prevPos + 1 && o[0] - start < 256 && std::equal( D, D + 15, prevD );
+            if ( !same )
+            {
+               start = o[0];
+               require( blk.size() / 16 < ( 1u << 23 ), "too many blocks for the point-table encoding" );
+               for ( int q = 0; q < 16; ++q )
+                  blk.push_back( q < 15 ? start + D[q] : 0 );
+            }
+            const int32_t e = ( o[0] - start ) | ( int32_t( blk.size() / 16 - 1 ) << 8 );
+            pts.push_back( e );
+            ptsC[( x + 2 * y + 3 * z ) & 3].push_back( e );
+            prevPos = o[0];
+            std::copy( D, D + 15, prevD );
+         }
+      }
       std::vector< int32_t > ptsFlat;
       for ( int c = 0; c < kInteriorColours; ++c )
       {

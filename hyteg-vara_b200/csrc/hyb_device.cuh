@@ -57,9 +57,10 @@ struct LevelDev
    int     nSeg;               // interior row segments (32 points each)
    const int32_t* seg;         // packed z | y<<10 | x0<<20
    const int32_t* xyz;         // closure index -> x | y<<10 | z<<20
-   // Cell-interior points, the same for every cell of the level. A residue block is the
-   // run of points x = 4g + r (fixed r) of one row; blk[16 b + q] is the position of
-   // stencil neighbour q of point g of block b, minus g (residueNbr). pts lists every
+   // Cell-interior points, the same for every cell of the level. A block is a run of
+   // interior points at consecutive storage positions whose 15 neighbours sit at the same
+   // offsets (a residue group x = 4g + r of one row, r fixed); blk[16 b + q] is the
+   // position of stencil neighbour q of point g of block b, minus g. pts lists every
    // interior point as g | b << 8 in storage order; ptsC lists the points of interior SOR
    // colour c in [ptsOff[c], ptsOff[c + 1]), also in storage order.
    int            nPts;
@@ -179,7 +180,8 @@ __host__ __device__ __forceinline__ int offRow( int q )
 }
 
 // Positions of the 15 neighbours of interior point x = 4g + r of row (y, z), relative to
-// g: neighbour q sits at d[q] + g.
+// g: neighbour q sits at d[q] + g. (The host builds the point tables from sidx and checks
+// them against this; the kernels read the tables.)
 struct NbrOff
 {
    int d[15];

@@ -256,8 +256,8 @@ struct InteriorOp
       }
    }
 
-   // diag and off-diagonal sum at interior point x = 4g + r whose neighbours sit at
-   // no.d[q] + g (residueNbr)
+   // diag and off-diagonal sum at the interior point of table entry g whose neighbours
+   // sit at no.d[q] + g
    __device__ __forceinline__ void row( const T* u, int g, const NbrOff& no, T& diag, T& off ) const
    {
       if constexpr ( !VAR )
@@ -446,7 +446,7 @@ __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDe
 }
 
 template < typename T, bool VAR, int MODE >
-__global__ void __launch_bounds__( 128, 8 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
+__global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
                                                   T* __restrict__ dst, const T* __restrict__ rhs, int flag,
                                                   int nCellBlocks )
 {

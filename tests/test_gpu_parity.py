@@ -340,3 +340,31 @@ def test_divkgrad_vcycle_and_solve_match_oracle(H, oracle_mod, setups):
     orc.gmg(xr, b, 0, L, pre=3, post=3, smoother=0, max_cycles=100, rel_tol=1e-13, op=op)
     err = np.abs(fx.get(L) - xr).max() / np.abs(xr).max()
     assert err < 1e-6, err
+
+
+def test_config1_ten_cycles_residual_history(H, oracle_mod):
+    """The reference's CPU-runnable case: Poisson on the 1x1x1 cube (6 macro-tets), levels
+    0..5, f ~ U[-1,1] seeded, zero initial guess, V(3,3) SOR (omega 1) with a CG coarse
+    solve to 1e-12, ten cycles: the GPU's residual history (relative to the initial one)
+    equals the oracle's with the same multicolour order to 1e-9, and its per-cycle
+    convergence factors stay within 25% of the reference ordering's."""
+    O = oracle_mod
+    L = 5
+    c, t = O.mesh_cuboid(1, 1, 1)
+    st = H.PrimitiveStorage(c, t, L)
+    orc = O.Oracle(c, t, L)
+    b = O.uniform_rhs(orc.coords_of(L), 0, 1 << L)
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, coarse_tol=1e-12)
+    hist = gmg.solve_to_tolerance(fx, fb, L, 0.0, max_cycles=10, precision=64)
+    assert len(hist) == 11
+    m, labels = st.colouring()
+    _, h_col = orc.gmg(np.zeros(orc.n(L)), b, 0, L, pre=3, post=3, smoother=1, labels=labels, m=m, coarse_tol=1e-12,
+                       max_cycles=10, rel_tol=0.0)
+    assert np.allclose(hist / hist[0], h_col / h_col[0], rtol=1e-9, atol=1e-15), (hist, h_col)
+    _, h_ref = orc.gmg(np.zeros(orc.n(L)), b, 0, L, pre=3, post=3, smoother=0, coarse_tol=1e-12, max_cycles=10,
+                       rel_tol=0.0)
+    f_gpu, f_ref = hist[1:] / hist[:-1], h_ref[1:] / h_ref[:-1]
+    assert np.all(np.abs(f_gpu - f_ref) <= 0.25 * f_ref + 1e-3), (f_gpu, f_ref)
