@@ -98,11 +98,12 @@ inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s );
 struct LevelHost
 {
    LevelDev           dev{};
-   DevBuf< int32_t >  seg, xyz, blk, pts, ptsC;
+   DevBuf< int32_t >  seg, xyz, blk, pts, ptsC, quads, rowYZ;
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
    std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
    int                cellBlocks   = 0;  // grid of the cell-interior row-segment loops
    int                ptsBlocks    = 0;  // grid of the loops over all interior points
+   int                quadBlocks   = 0;  // grid of the loops over interior quads
    int                colourBlocks = 0;  // grid of the loops over one interior colour
    int                bdryBlocks   = 0;  // grid of the surface-DoF loops
    int                slabBlocks   = 0;  // blocks of 256 over one closure
@@ -248,7 +249,7 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       d.nIntFace   = d.N >= 3 ? ( d.N - 1 ) * ( d.N - 2 ) / 2 : 0;
       d.nIntCell   = d.N >= 4 ? tetSize( d.N - 3 ) : 0;
       d.nBdry      = nV + nE * ( d.N - 1 ) + nF * d.nIntFace;
-      std::vector< int32_t >                seg, xyz( d.S ), blk, pts;
+      std::vector< int32_t >                seg, xyz( d.S ), blk, pts, quads, rowYZ;
       std::vector< std::vector< int32_t > > ptsC( kInteriorColours );
       for ( int z = 1; z <= d.N; ++z )
          for ( int y = 1; y <= d.N - z; ++y )
@@ -258,6 +259,11 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
                continue;
             for ( int x0 = 1; x0 <= len; x0 += 32 )
                seg.push_back( z | ( y << 10 ) | ( x0 << 20 ) );
+            const int row = int( rowYZ.size() );
+            require( row < ( 1 << 23 ), "too many rows for the quad-table encoding" );
+            rowYZ.push_back( y | ( z << 16 ) );
+            for ( int g = 0; 4 * g <= len; ++g )
+               quads.push_back( g | ( row << 8 ) );
          }
       // interior point tables: points in storage order, cut into blocks of consecutive
       // positions whose neighbour offsets agree (checked, not assumed from the layout)
@@ -299,6 +305,11 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       }
       d.ptsOff[kInteriorColours] = int( ptsFlat.size() );
       d.nPts                     = int( pts.size() );
+      d.nQuads = int( quads.size() );
+      lh->quads.upload( quads );
+      lh->rowYZ.upload( rowYZ );
+      d.quads = lh->quads.p;
+      d.rowYZ = lh->rowYZ.p;
       lh->blk.upload( blk );
       lh->pts.upload( pts );
       lh->ptsC.upload( ptsFlat );
@@ -319,7 +330,8 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
          return int( std::max< long >( 0, std::min< long >( ( work + perBlock - 1 ) / perBlock, long( s.numSMs ) * perSM ) ) );
       };
       lh->cellBlocks = grid( long( d.nSeg ) * nC, kCellWarps, 16 );
-      lh->ptsBlocks  = grid( long( ( d.nPts + 31 ) / 32 ) * nC, kCellWarps, 16 );
+      lh->ptsBlocks  = grid( long( ( d.nPts + 63 ) / 64 ) * nC, kCellWarps, 16 );
+      lh->quadBlocks = grid( long( ( d.nQuads + 31 ) / 32 ) * nC, kCellWarps, 16 );
       int maxColour  = 0;
       for ( int c = 0; c < kInteriorColours; ++c )
          maxColour = std::max( maxColour, d.ptsOff[c + 1] - d.ptsOff[c] );
@@ -746,7 +758,7 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
 {
    const Storage& s  = *op.st;
    const auto&    L  = s.L( l );
-   const int      nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+   const int      nc = L.dev.nPts > 0 ? ( op.variable ? L.ptsBlocks : L.quadBlocks ) : 0;
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;

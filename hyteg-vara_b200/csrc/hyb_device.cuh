@@ -68,6 +68,12 @@ struct LevelDev
    const int32_t* blk;
    const int32_t* pts;
    const int32_t* ptsC;
+   // Interior quads for the constant-coefficient apply: entry g | row << 8 stands for the
+   // points x = 4g .. 4g + 3 of interior row `row` (rowYZ[row] = y | z << 16), in storage
+   // order; a quad holds at least one interior point.
+   int            nQuads;
+   const int32_t* quads;
+   const int32_t* rowYZ;
 };
 
 // 15 stencil offsets, order shared with the oracle and the C ABI

@@ -374,6 +374,55 @@ struct PointBatch
    }
 };
 
+// Constant-stencil quad: the points x = 4g + r, r = 0..3, of row (y, z). Each of the seven
+// rows the stencil touches is read once for the four points: rows whose offsets have dx in
+// {-1, 0} need x' = 4g-1 .. 4g+3, rows with dx in {0, +1} need 4g .. 4g+4, the centre row
+// 4g-1 .. 4g+4 (36 reads for 4 points instead of 60). Reads outside the row give 0 and
+// are only used for points that are not interior.
+template < typename T >
+__device__ __forceinline__ T rowValue( const T* u, const StencilRows& R, int k, int g, int v )
+{
+   const int len = R.len[k];
+   const int xq  = 4 * g + v;
+   return ( xq >= 0 && xq < len ) ? u[R.start[k] + resOff( v & 3, len ) + g + resCarry( v )] : T( 0 );
+}
+
+// ax[r] = (A u) at the quad's points (constant stencil w)
+template < typename T >
+__device__ __forceinline__ void quadApply( const T* u, const T w[15], const StencilRows& R, int g, T ax[4] )
+{
+   {
+      T c[6];
+#pragma unroll
+      for ( int v = -1; v <= 4; ++v )
+         c[v + 1] = rowValue( u, R, 0, g, v );
+#pragma unroll
+      for ( int r = 0; r < 4; ++r )
+         ax[r] = w[0] * c[r + 1] + w[1] * c[r + 2] + w[2] * c[r];
+   }
+   // dx = 0 offset and the other offset of row k: rows 1, 3, 6 pair dx 0 with dx -1, rows
+   // 2, 4, 5 pair dx 0 with dx +1
+   constexpr int qa[7] = { 0, 3, 4, 5, 6, 11, 12 };
+   constexpr int qb[7] = { 0, 7, 8, 9, 10, 14, 13 };
+#pragma unroll
+   for ( int k = 1; k < 7; ++k )
+   {
+      const bool minus = ( k == 1 || k == 3 || k == 6 );
+      T          a[5];
+#pragma unroll
+      for ( int i = 0; i < 5; ++i )
+         a[i] = rowValue( u, R, k, g, minus ? i - 1 : i );
+#pragma unroll
+      for ( int r = 0; r < 4; ++r )
+      {
+         if ( minus ) // a[i] holds v = i - 1: dx 0 -> a[r + 1], dx -1 -> a[r]
+            ax[r] += w[qa[k]] * a[r + 1] + w[qb[k]] * a[r];
+         else // a[i] holds v = i: dx 0 -> a[r], dx +1 -> a[r + 1]
+            ax[r] += w[qa[k]] * a[r] + w[qb[k]] * a[r + 1];
+      }
+   }
+}
+
 // ---------------------------------------------------------------------------
 // apply / residual (P1Operator::apply, P1Operator.hpp:196-324;
 // P1ElementwiseOperator::apply, P1ElementwiseOperator.cpp:64-221)
@@ -383,7 +432,47 @@ __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDe
                                                   T* dst, const T* rhs, int flag,
                                                   int nCellBlocks )
 {
-   if ( vb.x < nCellBlocks )
+   if constexpr ( !VAR )
+   {
+      if ( vb.x < nCellBlocks )
+      {
+         const int nChunks = ( lv.nQuads + 31 ) >> 5;
+         HYB_CELL_LOOP( nChunks )
+         {
+            const int cell = it_ / nChunks;
+            const int i    = ( ( it_ - cell * nChunks ) << 5 ) + int( threadIdx.x & 31 );
+            if ( i >= lv.nQuads )
+               continue;
+            const int32_t     e  = __ldg( lv.quads + i );
+            const int         g  = e & 255;
+            const int32_t     yz = __ldg( lv.rowYZ + ( e >> 8 ) );
+            const int         y = yz & 0xffff, z = yz >> 16;
+            const StencilRows R  = stencilRows( lv.W, y, z );
+            InteriorOp< T, VAR > io;
+            io.load( op, cell );
+            const size_t co = size_t( cell ) * lv.stride;
+            T            ax[4];
+            quadApply( src + co, io.w, R, g, ax );
+            const int len = lv.N - 1 - y - z; // interior x in [1, len]
+#pragma unroll
+            for ( int r = 0; r < 4; ++r )
+            {
+               const int x = 4 * g + r;
+               if ( x < 1 || x > len )
+                  continue;
+               const size_t idx = co + R.start[0] + resOff( r, R.len[0] ) + g;
+               if constexpr ( MODE == kReplace )
+                  dst[idx] = ax[r];
+               else if constexpr ( MODE == kAdd )
+                  dst[idx] += ax[r];
+               else
+                  dst[idx] = rhs[idx] - ax[r];
+            }
+         }
+         return;
+      }
+   }
+   else if ( vb.x < nCellBlocks )
    {
       constexpr int K       = interiorBatch< T, VAR >();
       const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
