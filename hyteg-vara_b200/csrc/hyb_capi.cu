@@ -98,7 +98,7 @@ inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s );
 struct LevelHost
 {
    LevelDev           dev{};
-   DevBuf< int32_t >  seg, xyz, blk, pts, ptsC, quads, rowYZ;
+   DevBuf< int32_t >  seg, xyz, blk, blkXYZ, pts, ptsC, quads, rowYZ;
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
    std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
    int                cellBlocks   = 0;  // grid of the cell-interior row-segment loops
@@ -249,7 +249,7 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       d.nIntFace   = d.N >= 3 ? ( d.N - 1 ) * ( d.N - 2 ) / 2 : 0;
       d.nIntCell   = d.N >= 4 ? tetSize( d.N - 3 ) : 0;
       d.nBdry      = nV + nE * ( d.N - 1 ) + nF * d.nIntFace;
-      std::vector< int32_t >                seg, xyz( d.S ), blk, pts, quads, rowYZ;
+      std::vector< int32_t >                seg, xyz( d.S ), blk, blkXYZ, pts, quads, rowYZ;
       std::vector< std::vector< int32_t > > ptsC( kInteriorColours );
       for ( int z = 1; z <= d.N; ++z )
          for ( int y = 1; y <= d.N - z; ++y )
@@ -274,7 +274,7 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
                for ( int x = 1; x + y + z <= d.N - 1; ++x )
                   order.push_back( { sidx( d.W, x, y, z ), x | ( y << 10 ) | ( z << 20 ) } );
          std::sort( order.begin(), order.end() );
-         int prevPos = -2, start = 0;
+         int prevPos = -2, start = 0, prevXYZ = -1;
          int prevD[15] = {};
          for ( const auto& o : order )
          {
@@ -282,18 +282,21 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
             int       D[15];
             for ( int q = 0; q < 15; ++q )
                D[q] = sidx( d.W, x + offX( q ), y + offY( q ), z + offZ( q ) ) - o[0];
-            const bool same = o[0] == prevPos + 1 && o[0] - start < 256 && std::equal( D, D + 15, prevD );
+            const bool same = o[0] == prevPos + 1 && o[0] - start < 256 && std::equal( D, D + 15, prevD ) &&
+                              o[1] == prevXYZ + 4;
             if ( !same )
             {
                start = o[0];
                require( blk.size() / 16 < ( 1u << 23 ), "too many blocks for the point-table encoding" );
                for ( int q = 0; q < 16; ++q )
                   blk.push_back( q < 15 ? start + D[q] : 0 );
+               blkXYZ.push_back( o[1] );
             }
             const int32_t e = ( o[0] - start ) | ( int32_t( blk.size() / 16 - 1 ) << 8 );
             pts.push_back( e );
             ptsC[( x + 2 * y + 3 * z ) & 3].push_back( e );
             prevPos = o[0];
+            prevXYZ = o[1];
             std::copy( D, D + 15, prevD );
          }
       }
@@ -311,6 +314,8 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       d.quads = lh->quads.p;
       d.rowYZ = lh->rowYZ.p;
       lh->blk.upload( blk );
+      lh->blkXYZ.upload( blkXYZ );
+      d.blkXYZ = lh->blkXYZ.p;
       lh->pts.upload( pts );
       lh->ptsC.upload( ptsFlat );
       d.blk  = lh->blk.p;
@@ -848,7 +853,7 @@ void launchProlongate( const Storage& s, int coarseL, const T* coarse, T* fine, 
 {
    const auto& F  = s.L( coarseL + 1 );
    const auto& C  = s.L( coarseL );
-   const int   nc = F.dev.nSeg > 0 ? F.cellBlocks : 0;
+   const int   nc = F.dev.nPts > 0 ? F.ptsBlocks : 0;
    const int   nb = nc + ( F.dev.nBdry > 0 ? F.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
@@ -1183,7 +1188,7 @@ struct PhaseList
       vcycle< T >( x, b, tmp, l - 1 );
       {
          const auto& F  = s.L( l );
-         const int   nc = F.dev.nSeg > 0 ? F.cellBlocks : 0;
+         const int   nc = F.dev.nPts > 0 ? F.ptsBlocks : 0;
          Phase&      P  = add( kPhProlongAdd, l, nc + ( F.dev.nBdry > 0 ? F.bdryBlocks : 0 ), nc );
          P.p0           = x.ptr< T >( l - 1 );
          P.p1           = x.ptr< T >( l );

@@ -66,6 +66,7 @@ struct LevelDev
    int            nPts;
    int            ptsOff[5];
    const int32_t* blk;
+   const int32_t* blkXYZ; // per block: x | y << 10 | z << 20 of its g = 0 point (x steps by 4)
    const int32_t* pts;
    const int32_t* ptsC;
    // Interior quads for the constant-coefficient apply: entry g | row << 8 stands for the

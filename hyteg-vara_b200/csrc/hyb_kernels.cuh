@@ -578,7 +578,7 @@ __device__ __forceinline__ void sorIfaceBody( Blk vb, TopoDev tp, LevelDev lv, O
 }
 
 template < typename T, bool VAR >
-__global__ void __launch_bounds__( 128 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+__global__ void __launch_bounds__( 128, 8 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                       const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
 {
    sorIfaceBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, flag, bl );
@@ -728,16 +728,33 @@ __device__ __forceinline__ void prolongateBody( Blk vb, TopoDev tp, LevelDev lv,
 {
    if ( vb.x < nCellBlocks )
    {
-      HYB_CELL_LOOP( lv.nSeg )
+      // fine interior points from the point table: the points of one block share the
+      // parity pattern (x steps by 4), so the lanes of a block take one branch
+      constexpr int K       = 2;
+      const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
+      HYB_CELL_LOOP( nChunks )
       {
-         const int     cell = it_ / lv.nSeg;
-         const int32_t sp   = lv.seg[it_ - cell * lv.nSeg];
-         const int     z = sp & 1023, y = ( sp >> 10 ) & 1023, x = ( sp >> 20 ) + ( threadIdx.x & 31 );
-         if ( x + y + z > lv.N - 1 )
-            continue;
-         const T      v  = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
-         const size_t fi = size_t( cell ) * lv.stride + sidx( lv.W, x, y, z );
-         fine[fi]        = ADD ? fine[fi] + v : v;
+         const int cell = it_ / nChunks;
+         const int i0   = ( it_ - cell * nChunks ) * 32 * K + int( threadIdx.x & 31 );
+         T         v[K];
+         size_t    fi[K];
+         bool      ok[K];
+#pragma unroll
+         for ( int k = 0; k < K; ++k )
+         {
+            const int i     = i0 + 32 * k;
+            ok[k]           = i < lv.nPts;
+            const int32_t e = __ldg( lv.pts + ( ok[k] ? i : lv.nPts - 1 ) );
+            const int     g = e & 255, b = e >> 8;
+            const int32_t p = __ldg( lv.blkXYZ + b );
+            const int     x = ( p & 1023 ) + 4 * g, y = ( p >> 10 ) & 1023, z = p >> 20;
+            fi[k]           = size_t( cell ) * lv.stride + __ldg( lv.blk + 16 * size_t( b ) ) + g;
+            v[k]            = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
+         }
+#pragma unroll
+         for ( int k = 0; k < K; ++k )
+            if ( ok[k] )
+               fine[fi[k]] = ADD ? fine[fi[k]] + v[k] : v[k];
       }
       return;
    }
