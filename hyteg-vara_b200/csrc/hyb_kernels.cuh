@@ -237,8 +237,16 @@ template < typename T, bool VAR >
 struct InteriorOp
 {
    T w[15];       // constant operator: the class-0 stencil of the cell
-   const T* K;    // variable operator: micro-tet matrices of the cell
+   T ku[36];      // variable operator: the 6 off-diagonal entries (pairs 01 02 03 12 13 23)
+                  // of each of the cell's 6 micro-tet matrices, held in registers
    const T* kv;   // variable operator: nodal k slab of the cell
+
+   // index of the unordered vertex pair (a, b), a != b, in the order 01 02 03 12 13 23
+   __host__ __device__ static constexpr int pairIdx( int a, int b )
+   {
+      const int lo = a < b ? a : b, hi = a < b ? b : a;
+      return lo == 0 ? hi - 1 : ( lo == 1 ? hi + 1 : 5 );
+   }
 
    __device__ __forceinline__ void load( const OpDev< T >& op, int cell )
    {
@@ -251,7 +259,14 @@ struct InteriorOp
       }
       else
       {
-         K  = op.K + size_t( cell ) * 96;
+         const T* K = op.K + size_t( cell ) * 96;
+#pragma unroll
+         for ( int t = 0; t < 6; ++t )
+#pragma unroll
+            for ( int a = 0; a < 4; ++a )
+#pragma unroll
+               for ( int b = a + 1; b < 4; ++b )
+                  ku[6 * t + pairIdx( a, b )] = K[t * 16 + a * 4 + b];
          kv = op.kap + size_t( cell ) * op.stride;
       }
    }
@@ -278,20 +293,24 @@ struct InteriorOp
             kq[q] = kv[no.d[q] + g];
             uq[q] = u[no.d[q] + g];
          }
+         // element matrices of P1 stiffness have zero row sums, so the diagonal entry is
+         // minus the sum of the row's off-diagonal entries (symmetric: one value per pair)
          T d = 0, s = 0;
 #pragma unroll
          for ( int i = 0; i < 24; ++i )
          {
             const IncidentTet it = incidentTet( i );
             const T ks = kq[it.q[0]] + kq[it.q[1]] + kq[it.q[2]] + kq[it.q[3]];
-            const T* Kr = K + it.t * 16 + it.k * 4;
-            T acc = 0;
+            T       rowsum = 0, acc = 0;
 #pragma unroll
             for ( int j = 0; j < 4; ++j )
-               if ( j == it.k )
-                  d += ks * Kr[j];
-               else
-                  acc += Kr[j] * uq[it.q[j]];
+               if ( j != it.k )
+               {
+                  const T c = ku[6 * it.t + pairIdx( it.k, j )];
+                  rowsum += c;
+                  acc += c * uq[it.q[j]];
+               }
+            d -= ks * rowsum;
             s += ks * acc;
          }
          diag = d;
@@ -578,7 +597,7 @@ __device__ __forceinline__ void sorIfaceBody( Blk vb, TopoDev tp, LevelDev lv, O
 }
 
 template < typename T, bool VAR >
-__global__ void __launch_bounds__( 128, 8 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+__global__ void __launch_bounds__( 128, VAR ? 4 : 8 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                       const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
 {
    sorIfaceBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, flag, bl );
