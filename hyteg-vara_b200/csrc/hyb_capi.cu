@@ -9,6 +9,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/hyteg_b200.h"
@@ -52,6 +53,25 @@ inline void require( bool c, const std::string& msg )
 {
    if ( !c )
       throw Error( HYB_EINVAL, msg );
+}
+
+// Launch with programmatic stream serialization (the kernels' prologue waits for the
+// predecessor): consecutive kernels of a stream or a captured graph overlap their launch
+// latency with the predecessor's tail.
+template < typename... KArgs, typename... Args >
+void pdlLaunch( void ( *kernel )( KArgs... ), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args&&... args )
+{
+   cudaLaunchConfig_t  c{};
+   cudaLaunchAttribute a{};
+   a.id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
+   a.val.programmaticStreamSerializationAllowed = 1;
+   c.gridDim                                    = grid;
+   c.blockDim                                   = block;
+   c.dynamicSmemBytes                           = smem;
+   c.stream                                     = stream;
+   c.attrs                                      = &a;
+   c.numAttrs                                   = 1;
+   HYB_CUDA( cudaLaunchKernelEx( &c, kernel, std::forward< Args >( args )... ) );
 }
 
 template < typename T >
@@ -637,7 +657,7 @@ Operator* makeDivKGradWith( Storage* s, int minL, int maxL, FillK&& fillK )
       op->K32.push_back( std::move( b32 ) );
       fillK( l, op->kap64->ptr< double >( l ) );
       const int n = s->td.nC * s->L( l ).dev.stride;
-      k_convert< float, double ><<< ( n + 255 ) / 256, 256 >>>( s->L( l ).dev, op->kap32->ptr< float >( l ),
+      pdlLaunch( k_convert< float, double >, dim3( ( n + 255 ) / 256 ), dim3( 256 ), 0, 0, s->L( l ).dev, op->kap32->ptr< float >( l ),
                                                                  op->kap64->ptr< double >( l ), s->td.nC );
       HYB_CHECK_LAUNCH();
       HYB_CUDA( cudaDeviceSynchronize() );
@@ -668,8 +688,7 @@ void fillRff( Operator& op, const double* dW, const double* dPhase, int modes, d
    for ( int l = op.minL; l <= op.maxL; ++l )
    {
       const auto& L = s.L( l );
-      k_fill_rff_coefficient< double ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>(
-          s.td, L.dev, s.cellCoords.p, s.cellOrder.p, op.kap64->ptr< double >( l ), dW, dPhase, modes, sigma, radial );
+      pdlLaunch( k_fill_rff_coefficient< double >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, s.cellCoords.p, s.cellOrder.p, op.kap64->ptr< double >( l ), dW, dPhase, modes, sigma, radial );
       HYB_CHECK_LAUNCH();
       launchConvert< float, double >( s, l, op.kap32->ptr< float >( l ), op.kap64->ptr< double >( l ), stream );
    }
@@ -746,7 +765,7 @@ template < typename T >
 void launchFromDofs( const Storage& s, int l, T* slab, const T* dofs, cudaStream_t stream )
 {
    const auto& L = s.L( l );
-   k_from_dofs< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, slab, dofs );
+   pdlLaunch( k_from_dofs< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, slab, dofs );
    HYB_CHECK_LAUNCH();
 }
 
@@ -754,7 +773,7 @@ template < typename T >
 void launchToDofs( const Storage& s, int l, const T* slab, T* dofs, cudaStream_t stream )
 {
    const auto& L = s.L( l );
-   k_to_dofs< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, slab, dofs );
+   pdlLaunch( k_to_dofs< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, slab, dofs );
    HYB_CHECK_LAUNCH();
 }
 
@@ -768,7 +787,7 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
    if ( nb == 0 )
       return;
    const OpDev< T > od = op.dev< T >( l );
-#define HYB_APPLY( VAR, MODE ) k_apply< T, VAR, MODE ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, flag, nc )
+#define HYB_APPLY( VAR, MODE ) pdlLaunch( k_apply< T, VAR, MODE >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, flag, nc )
    if ( op.variable )
    {
       if ( mode == kReplace )
@@ -808,9 +827,9 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       const int32_t*  list = L.colourList.p + co[0];
       const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
       if ( op.variable )
-         k_sor_iface< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, bl );
+         pdlLaunch( k_sor_iface< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
       else
-         k_sor_iface< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, flag, bl );
+         pdlLaunch( k_sor_iface< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
       HYB_CHECK_LAUNCH();
    }
    if ( L.dev.nPts == 0 )
@@ -822,10 +841,10 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       if ( count == 0 )
          continue;
       if ( op.variable )
-         k_sor_interior< T, true ><<< L.colourBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c, begin, count,
+         pdlLaunch( k_sor_interior< T, true >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, c, begin, count,
                                                                           L.colourBlocks );
       else
-         k_sor_interior< T, false ><<< L.colourBlocks, 128, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, c, begin,
+         pdlLaunch( k_sor_interior< T, false >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, c, begin,
                                                                            count, L.colourBlocks );
       HYB_CHECK_LAUNCH();
    }
@@ -842,9 +861,9 @@ void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs
       return;
    const OpDev< T > od = op.dev< T >( l );
    if ( op.variable )
-      k_jacobi< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
+      pdlLaunch( k_jacobi< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
    else
-      k_jacobi< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
+      pdlLaunch( k_jacobi< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
    HYB_CHECK_LAUNCH();
 }
 
@@ -858,9 +877,9 @@ void launchProlongate( const Storage& s, int coarseL, const T* coarse, T* fine, 
    if ( nb == 0 )
       return;
    if ( add )
-      k_prolongate< T, true ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
+      pdlLaunch( k_prolongate< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
    else
-      k_prolongate< T, false ><<< nb, 128, 0, stream >>>( s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
+      pdlLaunch( k_prolongate< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
    HYB_CHECK_LAUNCH();
 }
 
@@ -873,7 +892,7 @@ void launchRestrict( const Storage& s, int fineL, const T* fine, T* coarse, int 
    const int   nb = nc + ( C.dev.nBdry > 0 ? C.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
-   k_restrict< T ><<< nb, 128, 0, stream >>>( s.td, C.dev, F.dev.W, F.dev.stride, fine, coarse, flag, nc );
+   pdlLaunch( k_restrict< T >, dim3( nb ), dim3( 128 ), 0, stream, s.td, C.dev, F.dev.W, F.dev.stride, fine, coarse, flag, nc );
    HYB_CHECK_LAUNCH();
 }
 
@@ -882,8 +901,7 @@ void launchLincomb( const Storage& s, int l, T* dst, int n, const double* sc, co
                     cudaStream_t stream )
 {
    const auto& L = s.L( l );
-   k_lincomb< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>(
-       s.td, L.dev, dst, n, T( n > 0 ? sc[0] : 0 ), n > 0 ? src[0] : nullptr, T( n > 1 ? sc[1] : 0 ),
+   pdlLaunch( k_lincomb< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, dst, n, T( n > 0 ? sc[0] : 0 ), n > 0 ? src[0] : nullptr, T( n > 1 ? sc[1] : 0 ),
        n > 1 ? src[1] : nullptr, T( n > 2 ? sc[2] : 0 ), n > 2 ? src[2] : nullptr, add ? 1 : 0, flag );
    HYB_CHECK_LAUNCH();
 }
@@ -895,9 +913,9 @@ void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, doubl
                 cudaStream_t stream )
 {
    const auto& L = s.L( l );
-   k_dot_partial< T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, a, b, flag, partial );
+   pdlLaunch( k_dot_partial< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, a, b, flag, partial );
    HYB_CHECK_LAUNCH();
-   k_reduce_final<<< 1, 1024, 0, stream >>>( partial, L.slabBlocks * s.td.nC, result );
+   pdlLaunch( k_reduce_final, dim3( 1 ), dim3( 1024 ), 0, stream, partial, L.slabBlocks * s.td.nC, result );
    HYB_CHECK_LAUNCH();
 }
 
@@ -913,7 +931,7 @@ void launchConvert( const Storage& s, int l, TD* dst, const TS* src, cudaStream_
 {
    const auto&  L = s.L( l );
    const size_t n = size_t( s.td.nC ) * L.dev.stride;
-   k_convert< TD, TS ><<< unsigned( ( n + 255 ) / 256 ), 256, 0, stream >>>( L.dev, dst, src, s.td.nC );
+   pdlLaunch( k_convert< TD, TS >, dim3( unsigned( ( n + 255 ) / 256 ) ), dim3( 256 ), 0, stream, L.dev, dst, src, s.td.nC );
    HYB_CHECK_LAUNCH();
 }
 
@@ -921,7 +939,7 @@ template < typename T >
 void launchAddCorrection( const Storage& s, int l, double* x, const T* e, int flag, cudaStream_t stream )
 {
    const auto& L = s.L( l );
-   k_add_correction< double, T ><<< dim3( L.slabBlocks, s.td.nC ), 256, 0, stream >>>( s.td, L.dev, x, e, flag );
+   pdlLaunch( k_add_correction< double, T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, x, e, flag );
    HYB_CHECK_LAUNCH();
 }
 
@@ -945,10 +963,10 @@ void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch&
    }
    const OpDev< double > od = op.dev< double >( l );
    if ( op.variable )
-      k_cg< true ><<< 1, 256, 0, stream >>>( s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
+      pdlLaunch( k_cg< true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p );
    else
-      k_cg< false ><<< 1, 256, 0, stream >>>( s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
+      pdlLaunch( k_cg< false >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
                                               cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p );
    HYB_CHECK_LAUNCH();
 }
@@ -1232,9 +1250,9 @@ void launchProgram( Gmg& g, Function& x, Function& b, int top, cudaStream_t stre
    const Phase* ph = prog->phases.p;
    const auto*  lt = (const LevelDev*) g.st->lvTable.p;
    if ( g.op->variable )
-      k_program< T, true ><<< 1, kProgramThreads, 0, stream >>>( g.st->td, lt, ph, prog->n );
+      pdlLaunch( k_program< T, true >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n );
    else
-      k_program< T, false ><<< 1, kProgramThreads, 0, stream >>>( g.st->td, lt, ph, prog->n );
+      pdlLaunch( k_program< T, false >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n );
    HYB_CHECK_LAUNCH();
 }
 

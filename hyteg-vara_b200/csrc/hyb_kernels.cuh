@@ -21,6 +21,14 @@ enum ApplyMode : int
    kResidual = 2, // dst = rhs - A src
 };
 
+// Programmatic dependent launch: a kernel lets the next kernel of its stream be scheduled
+// as soon as all its blocks run (launch_dependents), and every kernel waits for the
+// previous one to complete and its memory to be visible before touching any data (wait).
+// Launches with cudaLaunchAttributeProgrammaticStreamSerialization thus overlap the launch
+// latency of a kernel with the tail of its predecessor; without the attribute both
+// instructions do nothing.
+#define HYB_PDL_PROLOGUE() asm volatile( "griddepcontrol.launch_dependents;\n\tgriddepcontrol.wait;" ::: "memory" )
+
 constexpr int kCellWarps  = 4; // warps (row segments) per cell block
 constexpr int kBdryThreads = 128;
 
@@ -558,6 +566,7 @@ __global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_apply( TopoDev tp, Level
                                                   T* __restrict__ dst, const T* __restrict__ rhs, int flag,
                                                   int nCellBlocks )
 {
+   HYB_PDL_PROLOGUE();
    applyBody< T, VAR, MODE >( launchBlk(), tp, lv, op, src, dst, rhs, flag, nCellBlocks );
 }
 
@@ -600,6 +609,7 @@ template < typename T, bool VAR >
 __global__ void __launch_bounds__( 128, VAR ? 4 : 8 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                       const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
 {
+   HYB_PDL_PROLOGUE();
    sorIfaceBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, flag, bl );
 }
 
@@ -647,6 +657,7 @@ __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv
                                                          const T* __restrict__ rhs, T relax, int colour, int begin,
                                                          int nPts, int nCellBlocks )
 {
+   HYB_PDL_PROLOGUE();
    sorInteriorBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, colour, begin, nPts, nCellBlocks );
 }
 
@@ -710,6 +721,7 @@ __global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDe
                                                    T* __restrict__ dst, const T* __restrict__ rhs, T relax, int flag,
                                                    int nCellBlocks )
 {
+   HYB_PDL_PROLOGUE();
    jacobiBody< T, VAR >( launchBlk(), tp, lv, op, src, dst, rhs, relax, flag, nCellBlocks );
 }
 
@@ -800,6 +812,7 @@ __global__ void __launch_bounds__( 128 ) k_prolongate( TopoDev tp, LevelDev lv, 
                                                        const T* __restrict__ coarse, T* __restrict__ fine, int flag,
                                                        int nCellBlocks )
 {
+   HYB_PDL_PROLOGUE();
    prolongateBody< T, ADD >( launchBlk(), tp, lv, Wc, strideC, coarse, fine, flag, nCellBlocks );
 }
 
@@ -874,6 +887,7 @@ template < typename T >
 __global__ void __launch_bounds__( 128 ) k_restrict( TopoDev tp, LevelDev lv, int Wf, int strideF, const T* __restrict__ fine,
                                                      T* __restrict__ coarse, int flag, int nCellBlocks )
 {
+   HYB_PDL_PROLOGUE();
    restrictBody< T >( launchBlk(), tp, lv, Wf, strideF, fine, coarse, flag, nCellBlocks );
 }
 
@@ -885,6 +899,7 @@ template < typename T >
 __global__ void k_lincomb( TopoDev tp, LevelDev lv, T* __restrict__ dst, int n, T s0, const T* a0, T s1, const T* a1, T s2,
                            const T* a2, int add, int flag )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -949,6 +964,7 @@ __global__ void k_fill_uniform_hash( TopoDev tp, LevelDev lv, const double* __re
                                      const int32_t* __restrict__ cellOrder, T* __restrict__ dst, uint64_t seed,
                                      double lattice )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -969,6 +985,7 @@ __global__ void k_fill_rff_coefficient( TopoDev tp, LevelDev lv, const double* _
                                         const double* __restrict__ w, const double* __restrict__ phase, int modes,
                                         double sigma, double radial )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -987,6 +1004,7 @@ __global__ void k_fill_rff_coefficient( TopoDev tp, LevelDev lv, const double* _
 template < typename T >
 __global__ void k_fill( TopoDev tp, LevelDev lv, T* __restrict__ dst, T value, int flag )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -1000,6 +1018,7 @@ __global__ void k_fill( TopoDev tp, LevelDev lv, T* __restrict__ dst, T value, i
 template < typename TD, typename TS >
 __global__ void k_convert( LevelDev lv, TD* __restrict__ dst, const TS* __restrict__ src, int nCells )
 {
+   HYB_PDL_PROLOGUE();
    const size_t i = size_t( blockIdx.x ) * blockDim.x + threadIdx.x;
    if ( i < size_t( nCells ) * lv.stride )
       dst[i] = TD( src[i] );
@@ -1009,6 +1028,7 @@ __global__ void k_convert( LevelDev lv, TD* __restrict__ dst, const TS* __restri
 template < typename T, typename TE >
 __global__ void k_add_correction( TopoDev tp, LevelDev lv, T* __restrict__ x, const TE* __restrict__ e, int flag )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -1026,6 +1046,7 @@ template < typename T >
 __global__ void k_dot_partial( TopoDev tp, LevelDev lv, const T* __restrict__ a, const T* __restrict__ b, int flag,
                                double* __restrict__ partial )
 {
+   HYB_PDL_PROLOGUE();
    __shared__ double red[32];
    const int idx  = blockIdx.x * blockDim.x + threadIdx.x;
    const int cell = blockIdx.y;
@@ -1059,6 +1080,7 @@ __global__ void k_dot_partial( TopoDev tp, LevelDev lv, const T* __restrict__ a,
 // Deterministic second pass: one block sums the partials in a fixed order.
 __global__ void k_reduce_final( const double* __restrict__ partial, int n, double* __restrict__ out )
 {
+   HYB_PDL_PROLOGUE();
    __shared__ double red[32];
    double            v = 0;
    for ( int i = threadIdx.x; i < n; i += blockDim.x )
@@ -1101,6 +1123,7 @@ __device__ __forceinline__ int64_t canonicalDof( const TopoDev& tp, const LevelD
 template < typename T >
 __global__ void k_from_dofs( TopoDev tp, LevelDev lv, T* __restrict__ slab, const T* __restrict__ dofs )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -1112,6 +1135,7 @@ __global__ void k_from_dofs( TopoDev tp, LevelDev lv, T* __restrict__ slab, cons
 template < typename T >
 __global__ void k_to_dofs( TopoDev tp, LevelDev lv, const T* __restrict__ slab, T* __restrict__ dofs )
 {
+   HYB_PDL_PROLOGUE();
    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
    if ( idx >= lv.S )
       return;
@@ -1257,6 +1281,7 @@ template < bool VAR >
 __global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
                                                 double* r, double* p, double* ap, double tol, int maxIter, int* status )
 {
+   HYB_PDL_PROLOGUE();
    __shared__ double red[32];
    cgBody< VAR >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red );
 }

@@ -69,6 +69,7 @@ template < typename T, bool VAR >
 __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, const LevelDev* __restrict__ lvs,
                                                                 const Phase* __restrict__ prog, int nPhases )
 {
+   HYB_PDL_PROLOGUE();
    __shared__ double red[32];
    for ( int ph = 0; ph < nPhases; ++ph )
    {
