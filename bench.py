@@ -219,9 +219,16 @@ def ours(args, rank, world, local_rank):
     sor_gbs = ndof * 24 / t_sor / 1e9
     sor32_gbs = ndof * 12 / t_sor32 / 1e9
 
-    def roof(a, t_bytes=None):
+    def roof(a, t_bytes=None, t_src=None):
         return {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 3),
-                "peak_source": peak_kind, "traffic": t_bytes}
+                "peak_source": peak_kind, "traffic": t_bytes, "traffic_source": t_src}
+
+    # DRAM bytes (read + write) per launch from ncu captures of the same kernels and workload
+    # (the sum over the ten launches of one sweep): profiles/k_sor_fp64_fp32_level7_cube48.md,
+    # profiles/k_apply_fp64_level7_cube48.md
+    sweep64_traffic, sweep32_traffic, apply_traffic = 1516.7e6, 900.5e6, 429.7e6
+    if (L, nc) != (7, 2):
+        sweep64_traffic = sweep32_traffic = apply_traffic = None
 
     varcoef = None
     if not args.no_varcoef:
@@ -266,10 +273,13 @@ def ours(args, rank, world, local_rank):
             "final_rel_residual": {"mixed": float(hist_mixed[-1][-1]), "fp64": float(hist_fp64[-1][-1])},
             "error_mixed_vs_fp64_solution": err_mixed,
             "dof_updates_per_s_fp64": world * n_unknowns * sum(cyc_fp64) / (t_fp64 / 1e3),
-            "roofline": dict(roof(sor_gbs), kernel="k_sor (one FP64 multicolour SOR sweep, level 7)",
+            "roofline": dict(roof(sor_gbs, sweep64_traffic, "ncu, profiles/k_sor_fp64_fp32_level7_cube48.md"),
+                             kernel="k_sor_iface + k_sor_interior (one FP64 multicolour SOR sweep, 10 launches, level 7)",
                              ms=t_sor * 1e3),
-            "roofline_apply": dict(roof(apply_gbs), kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
-            "roofline_sor_fp32": dict(roof(sor32_gbs), kernel="k_sor (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
+            "roofline_apply": dict(roof(apply_gbs, apply_traffic, "ncu, profiles/k_apply_fp64_level7_cube48.md"),
+                                   kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
+            "roofline_sor_fp32": dict(roof(sor32_gbs, sweep32_traffic, "ncu, profiles/k_sor_fp64_fp32_level7_cube48.md"),
+                                      kernel="k_sor_iface + k_sor_interior (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "variable_coefficient": varcoef, "spherical_shell": shell, "serving": serve,
         }
@@ -366,16 +376,35 @@ def spherical_shell(args, H, I, stream, ntan=5, nrad=4, L=6):
     solve(64, 1e-12)
     u_ref = u.get(L, stream=sh)
     m_col, _ = st.colouring()
+    err = float(np.abs(u_mixed - u_ref).max() / np.abs(u_ref).max())
+    ndofs = st.num_dofs(L)
+    del gmg, A, u, b, st
+    torch.cuda.synchronize()
+    # the same shape as serving requests: four solves, 0.1 s apart, after a warm-up round
+    # that leaves four resident hierarchies
+    sv = H.Server(int(args.serve_budget_gb * (1 << 30)), max_active=4, max_level=L)
+    for i in range(4):
+        sv.submit(H.Server.request(ntan, nrad, 1, L, H.COEFF_RADIAL, 32, 500 + i, mesh=H.MESH_SHELL))
+    sv.run(600)
+    ids = [sv.submit(H.Server.request(ntan, nrad, 1, L, H.COEFF_RADIAL, 32, 600 + i, mesh=H.MESH_SHELL),
+                     arrival_s=0.1 * i) for i in range(4)]
+    sv.run(600)
+    res = [sv.result(i) for i in ids]
+    lat = [(r.done_s - r.arrival_s) * 1e3 for r in res]
+    served = {"requests": 4, "arrivals_s": [0.0, 0.1, 0.2, 0.3], "statuses": sorted({r.status for r in res}),
+              "latency_ms": lat, "cycles": [r.cycles for r in res],
+              "solves_per_s": 4 / (max(r.done_s for r in res) - min(r.arrival_s for r in res))}
+    sv.close()
     return {"workload": f"spherical shell ntan={ntan} nrad={nrad} (3 radial layers) r in [0.55, 1], "
-                        f"{int(st.counts()[3])} macro-tets, level {L}, "
+                        f"{60 * (ntan - 1) ** 2 * (nrad - 1)} macro-tets, level {L}, "
                         f"k=exp(5(1-r))*exp(0.5 GRF corr 0.2 seed 2), V(2,2) multicolour SOR, to rel. residual 1e-8",
-            "dofs": st.num_dofs(L), "unknowns": n_unknowns, "interface_colours": m_col, "setup_s": setup_s,
+            "dofs": ndofs, "unknowns": n_unknowns, "interface_colours": m_col, "setup_s": setup_s,
             "time_to_tol_ms": {"mixed": out[32][0], "fp64": out[64][0]},
             "speedup_mixed_vs_fp64": out[64][0] / out[32][0], "cycles": {"mixed": out[32][1], "fp64": out[64][1]},
             "final_rel_residual": {"mixed": out[32][2], "fp64": out[64][2]},
             "dof_updates_per_s": {"mixed": n_unknowns * out[32][1] / (out[32][0] / 1e3),
                                   "fp64": n_unknowns * out[64][1] / (out[64][0] / 1e3)},
-            "error_mixed_vs_fp64_solution": float(np.abs(u_mixed - u_ref).max() / np.abs(u_ref).max())}
+            "error_mixed_vs_fp64_solution": err, "as_serving_requests": served}
 
 
 def serve_stream(n, rate, seed, levels=(3, 7), cubes=(1, 4)):

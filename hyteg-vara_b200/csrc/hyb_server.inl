@@ -52,8 +52,12 @@ void rffFeatures( uint64_t seed, double corrLen, int modes, double* w, double* p
 
 struct ServeKey
 {
-   int  nx, ny, nz, level, coeff, precision;
-   bool sameMesh( const ServeKey& o ) const { return nx == o.nx && ny == o.ny && nz == o.nz; }
+   int  nx, ny, nz, level, coeff, precision, mesh;
+   bool sameMesh( const ServeKey& o ) const { return mesh == o.mesh && nx == o.nx && ny == o.ny && nz == o.nz; }
+   long cells() const
+   {
+      return mesh == HYB_MESH_SHELL ? 60l * ( nx - 1 ) * ( nx - 1 ) * ( ny - 1 ) : 6l * nx * ny * nz;
+   }
    bool operator==( const ServeKey& o ) const
    {
       return sameMesh( o ) && level == o.level && coeff == o.coeff && precision == o.precision;
@@ -64,6 +68,8 @@ inline long long gcdll( long long a, long long b ) { return b == 0 ? a : gcdll( 
 
 inline double serveLattice( const ServeKey& k )
 {
+   if ( k.mesh == HYB_MESH_SHELL )
+      return double( 1 << 20 ); // shell points are not on a lattice: a fine one
    long long l = k.nx;
    l           = l / gcdll( l, k.ny ) * k.ny;
    l           = l / gcdll( l, k.nz ) * k.nz;
@@ -78,11 +84,11 @@ inline double serveLattice( const ServeKey& k )
 // its own partial-sum array for dot products.
 size_t serveFootprint( const ServeKey& k, int meshMaxLevel )
 {
-   const size_t nC  = size_t( 6 ) * k.nx * k.ny * k.nz;
+   const size_t nC  = size_t( k.cells() );
    size_t       per = 3 * 8;
    if ( k.precision == 32 )
       per += 8 + 3 * 4;
-   if ( k.coeff == HYB_COEFF_LOGNORMAL )
+   if ( k.coeff != HYB_COEFF_CONSTANT )
       per += 8 + 4;
    size_t bytes = 0;
    for ( int l = 0; l <= k.level; ++l )
@@ -90,7 +96,7 @@ size_t serveFootprint( const ServeKey& k, int meshMaxLevel )
       const size_t N = size_t( 1 ) << l;
       const size_t S = ( N + 1 ) * ( N + 2 ) * ( N + 3 ) / 6;
       bytes += nC * size_t( stridePad( int( S ) ) ) * per;
-      if ( k.coeff == HYB_COEFF_LOGNORMAL )
+      if ( k.coeff != HYB_COEFF_CONSTANT )
          bytes += nC * 96 * ( 8 + 4 );
    }
    bytes += nC * size_t( stridePad( 4 ) ) * 8 * ( k.precision == 32 ? 5 : 3 );
@@ -110,7 +116,7 @@ size_t serveFootprint( const ServeKey& k, int meshMaxLevel )
 
 struct MeshEntry
 {
-   int                         nx, ny, nz;
+   int                         nx, ny, nz, kind;
    std::unique_ptr< Storage >  st;
    std::unique_ptr< Operator > laplace;
    size_t                      bytes = 0;
@@ -194,17 +200,21 @@ struct Server
    MeshEntry& mesh( const ServeKey& k )
    {
       for ( auto& m : meshes )
-         if ( m->nx == k.nx && m->ny == k.ny && m->nz == k.nz )
+         if ( m->kind == k.mesh && m->nx == k.nx && m->ny == k.ny && m->nz == k.nz )
             return *m;
       const long long before = g_deviceBytes.load();
       auto            m      = std::make_unique< MeshEntry >();
       m->nx                  = k.nx;
       m->ny                  = k.ny;
       m->nz                  = k.nz;
+      m->kind                = k.mesh;
       std::vector< std::array< double, 3 > > V;
       std::vector< std::array< int, 4 > >    T;
       const double                           lo[3] = { 0, 0, 0 }, hi[3] = { 1, 1, 1 };
-      meshCuboid( k.nx, k.ny, k.nz, lo, hi, V, T );
+      if ( k.mesh == HYB_MESH_SHELL )
+         meshSphericalShell( k.nx, k.ny, 0.55, 1.0, V, T );
+      else
+         meshCuboid( k.nx, k.ny, k.nz, lo, hi, V, T );
       m->st = std::make_unique< Storage >();
       buildStorage( *m->st, V, T, maxLevel );
       m->laplace.reset( makeLaplace( m->st.get(), 0, maxLevel ) );
@@ -235,7 +245,7 @@ struct Server
       in->key                = k;
       in->mesh               = &me;
       Storage* st            = me.st.get();
-      if ( k.coeff == HYB_COEFF_LOGNORMAL )
+      if ( k.coeff != HYB_COEFF_CONSTANT )
       {
          in->ownOp.reset( makeDivKGradWith( st, 0, k.level, []( int, double* ) {} ) );
          in->op = in->ownOp.get();
@@ -307,16 +317,26 @@ struct Server
 
 void validateRequest( const Server& sv, const hyb_request& d )
 {
-   require( d.nx >= 1 && d.ny >= 1 && d.nz >= 1 && d.nx <= 64 && d.ny <= 64 && d.nz <= 64,
-            "macro-cubes per direction must be in [1, 64]" );
+   require( d.mesh == HYB_MESH_CUBOID || d.mesh == HYB_MESH_SHELL, "unknown mesh kind" );
+   if ( d.mesh == HYB_MESH_CUBOID )
+      require( d.nx >= 1 && d.ny >= 1 && d.nz >= 1 && d.nx <= 64 && d.ny <= 64 && d.nz <= 64,
+               "macro-cubes per direction must be in [1, 64]" );
+   else
+      require( d.nx >= 2 && d.ny >= 2 && d.nx <= 64 && d.ny <= 64, "shell ntan and nrad must be in [2, 64]" );
    require( d.level >= 1 && d.level <= sv.maxLevel, "level must be in [1, the server's max_level]" );
-   require( d.coefficient == HYB_COEFF_CONSTANT || d.coefficient == HYB_COEFF_LOGNORMAL, "unknown coefficient kind" );
+   require( d.coefficient == HYB_COEFF_CONSTANT || d.coefficient == HYB_COEFF_LOGNORMAL ||
+                d.coefficient == HYB_COEFF_RADIAL,
+            "unknown coefficient kind" );
    require( d.precision == 64 || d.precision == 32, "precision must be 64 or 32" );
    require( d.rel_tol > 0 && std::isfinite( d.rel_tol ), "rel_tol must be positive" );
    require( d.max_cycles >= 1, "max_cycles must be at least 1" );
 }
 
-ServeKey keyOf( const hyb_request& d ) { return ServeKey{ d.nx, d.ny, d.nz, d.level, d.coefficient, d.precision }; }
+ServeKey keyOf( const hyb_request& d )
+{
+   const bool shell = d.mesh == HYB_MESH_SHELL;
+   return ServeKey{ d.nx, d.ny, shell ? 1 : d.nz, d.level, d.coefficient, d.precision, d.mesh };
+}
 
 // right-hand side, coefficient, x = 0, ||b||^2 and the initial residual norm
 void startRequest( Server& sv, ServeRequest& r, Instance& in )
@@ -328,11 +348,13 @@ void startRequest( Server& sv, ServeRequest& r, Instance& in )
    in.lastUse      = ++sv.tick;
    r.inst          = &in;
    r.served        = in.bytes;
-   if ( r.key.coeff == HYB_COEFF_LOGNORMAL )
+   if ( r.key.coeff != HYB_COEFF_CONSTANT )
    {
+      const bool radial = r.key.coeff == HYB_COEFF_RADIAL;
       rffFeatures( r.d.seed, kServeCorrLen, kServeModes, in.featHost, in.featHost + 3 * kServeModes );
       HYB_CUDA( cudaMemcpyAsync( in.feat.p, in.featHost, 4 * kServeModes * sizeof( double ), cudaMemcpyHostToDevice, s ) );
-      fillRff( *in.ownOp, in.feat.p, in.feat.p + 3 * kServeModes, kServeModes, kServeSigma, 0.0, s );
+      fillRff( *in.ownOp, in.feat.p, in.feat.p + 3 * kServeModes, kServeModes, radial ? 0.5 : kServeSigma,
+               radial ? 5.0 : 0.0, s );
    }
    const auto& Lh = st.L( L );
    k_fill_uniform_hash< double ><<< dim3( Lh.slabBlocks, st.td.nC ), 256, 0, s >>>(

@@ -36,14 +36,16 @@ SYMBOLS = [
     "hyb_storage_create_spherical_shell",
 ]
 
-COEFF_CONSTANT, COEFF_LOGNORMAL = 0, 1
+COEFF_CONSTANT, COEFF_LOGNORMAL, COEFF_RADIAL = 0, 1, 2
+MESH_CUBOID, MESH_SHELL = 0, 1
 
 
 class Request(ctypes.Structure):
-    """hyb_request: one Poisson solve on the unit cube split into nx x ny x nz macro-cubes."""
+    """hyb_request: one Poisson solve on the unit cube split into nx x ny x nz macro-cubes, or
+    on the spherical shell with ntan = nx, nrad = ny (mesh = MESH_SHELL)."""
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("level", ctypes.c_int),
                 ("coefficient", ctypes.c_int), ("precision", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("rel_tol", ctypes.c_double), ("max_cycles", ctypes.c_int)]
+                ("rel_tol", ctypes.c_double), ("max_cycles", ctypes.c_int), ("mesh", ctypes.c_int)]
 
 
 class RequestResult(ctypes.Structure):
@@ -451,8 +453,9 @@ class Server:
         self.close()
 
     @staticmethod
-    def request(nx, ny, nz, level, coefficient=COEFF_CONSTANT, precision=32, seed=0, rel_tol=1e-8, max_cycles=100):
-        return Request(nx, ny, nz, level, coefficient, precision, seed, rel_tol, max_cycles)
+    def request(nx, ny, nz, level, coefficient=COEFF_CONSTANT, precision=32, seed=0, rel_tol=1e-8, max_cycles=100,
+                mesh=MESH_CUBOID):
+        return Request(nx, ny, nz, level, coefficient, precision, seed, rel_tol, max_cycles, mesh)
 
     def footprint(self, req):
         n = ctypes.c_size_t()

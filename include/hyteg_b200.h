@@ -207,25 +207,34 @@ int hyb_gmg_solve_to_tolerance( hyb_gmg* g, hyb_function* x, hyb_function* b, in
  * the others. Each solve is V(3,3) with multicolour SOR (omega 1) and a level-0 FP64 CG
  * coarse solve to 1e-12; f is hyb_function_fill_uniform_random( seed, lattice =
  * lcm(nx,ny,nz) 2^level ) and, for the lognormal coefficient, k is exp of the random
- * field of hyb_rff_features( seed, 0.2, 64 ) with sigma 1. Results do not depend on
- * which other requests share the GPU. */
+ * field of hyb_rff_features( seed, 0.2, 64 ) with sigma 1 (the radial coefficient: the same
+ * field with sigma 0.5 times exp(5 (1 - |x|))). Spherical-shell requests (mesh
+ * HYB_MESH_SHELL) use the lattice 2^20 for f. Results do not depend on which other
+ * requests share the GPU. */
 typedef struct hyb_server_s hyb_server;
 
 enum
 {
    HYB_COEFF_CONSTANT  = 0, /* k = 1 (P1ConstantLaplaceOperator) */
-   HYB_COEFF_LOGNORMAL = 1  /* k = exp(g), g a Gaussian random field (P1ElementwiseOperator) */
+   HYB_COEFF_LOGNORMAL = 1, /* k = exp(g), g a Gaussian random field (P1ElementwiseOperator) */
+   HYB_COEFF_RADIAL    = 2  /* k = exp(5 (1 - |x|)) exp(0.5 g): the shell benchmark's coefficient */
+};
+enum
+{
+   HYB_MESH_CUBOID = 0, /* unit cube split into nx x ny x nz macro-cubes */
+   HYB_MESH_SHELL  = 1  /* spherical shell, radii 0.55..1: ntan = nx, nrad = ny (nz unused) */
 };
 
 typedef struct hyb_request
 {
-   int      nx, ny, nz;   /* macro-cubes per direction */
+   int      nx, ny, nz;   /* macro-cubes per direction (shell: ntan, nrad, unused) */
    int      level;        /* refinement level of the solve */
    int      coefficient;  /* HYB_COEFF_* */
    int      precision;    /* 64: FP64 V-cycles; 32: FP32 V-cycles in FP64 iterative refinement */
    uint64_t seed;         /* right-hand side and coefficient seed */
    double   rel_tol;      /* stop when ||b - A x|| / ||b|| <= rel_tol */
    int      max_cycles;   /* give up (HYB_ENOTCONVERGED) after this many cycles */
+   int      mesh;         /* HYB_MESH_*; zero-initialised requests are cuboids */
 } hyb_request;
 
 typedef struct hyb_request_result

@@ -126,3 +126,26 @@ def test_not_converged_and_time_limit_status(H):
     sv.run(120)
     res = sv.result(a)
     assert res.status == 6 and res.cycles == 2  # HYB_ENOTCONVERGED after max_cycles
+
+
+def test_shell_request_matches_standalone_solver(H):
+    """A spherical-shell request with the radial coefficient gives the solution of the same
+    problem built through the public API (shell storage, device coefficient with radial
+    profile and sigma 0.5, right-hand side on the lattice 2^20)."""
+    ntan, nrad, L, seed = 3, 2, 3, 21
+    sv = H.Server(4 << 30, max_level=L)
+    st = H.PrimitiveStorage.spherical_shell(ntan, nrad, 0.55, 1.0, L)
+    n = st.num_dofs(L)
+    req = H.Server.request(ntan, nrad, 1, L, H.COEFF_RADIAL, 32, seed, mesh=H.MESH_SHELL)
+    rid = sv.submit(req, keep_solution=True, num_dofs=n)
+    sv.run(120)
+    res = sv.result(rid)
+    assert res.status == 0 and res.rel_residual <= 1e-8
+    w, ph = H.rff_features(seed, 0.2, 64)
+    A = H.P1ElementwiseDivKGradOperator.random_features(st, 0, L, w, ph, 0.5, radial=5.0)
+    x, b = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    b.fill_uniform_random(L, seed, float(1 << 20))
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    hist = gmg.solve_to_tolerance(x, b, L, 1e-8, max_cycles=100, precision=32)
+    assert len(hist) - 1 == res.cycles
+    assert rel_diff(sv.solution(rid), x.get(L)) <= TOL

@@ -13,15 +13,15 @@ def H():
     return H
 
 
-def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes=64):
+def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes=64, mesh=0):
     """Independent restatement of the per-request device bytes (the hierarchy's vectors per
     level, coefficient storage, coarse CG scratch, dot-product partials, features, the
     coarse-level program kernel's phase list)."""
-    nC = 6 * nx * ny * nz
+    nC = 60 * (nx - 1) ** 2 * (ny - 1) if mesh == 1 else 6 * nx * ny * nz
     pad = lambda s: (s + 31) // 32 * 32
     closure = lambda l: ((1 << l) + 1) * ((1 << l) + 2) * ((1 << l) + 3) // 6
-    per = 24 + (20 if precision == 32 else 0) + (12 if coeff == 1 else 0)
-    b = sum(nC * pad(closure(l)) * per + (nC * 96 * 12 if coeff == 1 else 0) for l in range(level + 1))
+    per = 24 + (20 if precision == 32 else 0) + (12 if coeff != 0 else 0)
+    b = sum(nC * pad(closure(l)) * per + (nC * 96 * 12 if coeff != 0 else 0) for l in range(level + 1))
     b += nC * pad(4) * 8 * (5 if precision == 32 else 3)
     b += max(-(-closure(l) // 256) * nC for l in range(mesh_max_level + 1)) * 8
     b += (level + 1) * 65536  # phase-list allowance of the coarse-level program kernel
@@ -36,12 +36,21 @@ def test_footprint_matches_formula(H, shape):
     assert sv.footprint(req) == footprint_formula(nx, ny, nz, L, coeff, prec, 7)
 
 
+@pytest.mark.parametrize("shape", [(5, 4, 6, 2, 32), (3, 2, 3, 0, 64)])
+def test_shell_footprint_matches_formula(H, shape):
+    sv = H.Server(1 << 40, max_level=7)
+    ntan, nrad, L, coeff, prec = shape
+    req = H.Server.request(ntan, nrad, 1, L, coeff, prec, mesh=H.MESH_SHELL)
+    assert sv.footprint(req) == footprint_formula(ntan, nrad, 1, L, coeff, prec, 7, mesh=1)
+
+
 def test_invalid_requests_are_refused(H):
     sv = H.Server(1 << 40, max_level=7)
     bad = [H.Server.request(0, 1, 1, 3), H.Server.request(1, 1, 1, 8), H.Server.request(1, 1, 1, 0),
            H.Server.request(1, 1, 1, 3, coefficient=5), H.Server.request(1, 1, 1, 3, precision=16),
            H.Server.request(1, 1, 1, 3, rel_tol=0.0), H.Server.request(1, 1, 1, 3, max_cycles=0),
-           H.Server.request(1, 1, 1, 3, rel_tol=float("nan"))]
+           H.Server.request(1, 1, 1, 3, rel_tol=float("nan")), H.Server.request(1, 1, 1, 3, mesh=7),
+           H.Server.request(1, 2, 1, 3, mesh=H.MESH_SHELL), H.Server.request(1, 1, 1, 3, coefficient=3)]
     for req in bad:
         with pytest.raises(H.HybError, match="error 1:"):
             sv.submit(req)
