@@ -810,6 +810,13 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
    HYB_CHECK_LAUNCH();
 }
 
+// levels whose cells hold at most this many interior points run the four interior SOR
+// colours in one launch (a block per cell); HYB_FUSED_INTERIOR_MAX overrides it
+static const int kFusedInteriorMaxPoints = [] {
+   const char* e = std::getenv( "HYB_FUSED_INTERIOR_MAX" );
+   return e ? std::atoi( e ) : 4096;
+}();
+
 template < typename T >
 void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream )
 {
@@ -834,6 +841,19 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
    }
    if ( L.dev.nPts == 0 )
       return;
+   // small levels: the four interior colours in one launch, a block per cell
+   if ( L.dev.nPts <= kFusedInteriorMaxPoints )
+   {
+      const int* o = L.dev.ptsOff;
+      if ( op.variable )
+         pdlLaunch( k_sor_interior_cells< T, true >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
+                    relax, o[0], o[1], o[2], o[3], o[4] );
+      else
+         pdlLaunch( k_sor_interior_cells< T, false >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
+                    relax, o[0], o[1], o[2], o[3], o[4] );
+      HYB_CHECK_LAUNCH();
+      return;
+   }
    // interior passes: one launch per colour
    for ( int c = 0; c < kInteriorColours; ++c )
    {

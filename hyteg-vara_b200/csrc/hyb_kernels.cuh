@@ -661,6 +661,39 @@ __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv
    sorInteriorBody< T, VAR >( launchBlk(), tp, lv, op, u, rhs, relax, colour, begin, nPts, nCellBlocks );
 }
 
+// All four interior colour passes of a sweep in ONE launch for small levels: a block per
+// cell runs the colours one after the other with __syncthreads() in between. Interior
+// points of different cells are never coupled, so no other block's progress matters; on
+// small levels, where a colour pass has little work, this saves three launches per sweep.
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                               const T* __restrict__ rhs, T relax, int o0, int o1, int o2,
+                                                               int o3, int o4 )
+{
+   HYB_PDL_PROLOGUE();
+   const int            cell = blockIdx.x;
+   InteriorOp< T, VAR > io;
+   io.load( op, cell );
+   T*       uc = u + size_t( cell ) * lv.stride;
+   const T* bc = rhs + size_t( cell ) * lv.stride;
+   const int off[5] = { o0, o1, o2, o3, o4 };
+#pragma unroll
+   for ( int c = 0; c < kInteriorColours; ++c )
+   {
+      for ( int i = off[c] + int( threadIdx.x ); i < off[c + 1]; i += int( blockDim.x ) )
+      {
+         const int32_t e  = __ldg( lv.ptsC + i );
+         const int     g  = e & 255;
+         const NbrOff  no = blockNbr( lv.blk, e >> 8 );
+         T             diag, offd;
+         io.row( uc, g, no, diag, offd );
+         const int idx = no.d[0] + g;
+         uc[idx]       = ( T( 1 ) - relax ) * uc[idx] + relax * ( bc[idx] - offd ) / diag;
+      }
+      __syncthreads();
+   }
+}
+
 // ---------------------------------------------------------------------------
 // Weighted Jacobi (P1Operator::smooth_jac, P1Operator.hpp:424-440):
 // dst = src + relax * (rhs - A src) / diag(A)
