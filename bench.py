@@ -93,6 +93,26 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def rank_reduce(vals, op, world, device):
+    """All-reduce floats over the ranks of the default process group ("max" for times,
+    "sum" for throughputs); identity on a single rank. Every rank calls it in the same
+    order."""
+    if world == 1:
+        return [float(v) for v in vals]
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_value(world, unknowns, cycles, max_ms):
+    """Whole-job DoF-updates/s of N replicas: every rank solves its own copy, the time is the
+    slowest rank's."""
+    return world * unknowns * cycles / (max_ms / 1e3)
+
+
 def ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -137,11 +157,7 @@ def ours(args, rank, world, local_rank):
             dist.barrier()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_reduce([v], "max", world, dev)[0]
 
     def timed(fn, steps):
         torch.cuda.synchronize()
@@ -169,7 +185,7 @@ def ours(args, rank, world, local_rank):
     cyc_fp64 = [len(h) - 1 for h in hist_fp64]
     ms_mixed = t_mixed / args.steps
     ms_fp64 = t_fp64 / args.steps
-    value = world * n_unknowns * sum(cyc_mixed) / (t_mixed / 1e3)
+    value = replica_value(world, n_unknowns, sum(cyc_mixed), t_mixed)
 
     # error of the mixed solution against a tightly converged FP64 solve of the same system
     solve(32)
@@ -246,12 +262,8 @@ def ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         serve = serving(args, H)
         if world > 1:
-            t = torch.tensor([serve["solves_per_s"], serve["p99_ms"]], dtype=torch.float64, device=dev)
-            s_sum, s_max = t.clone(), t.clone()
-            dist.all_reduce(s_sum, op=dist.ReduceOp.SUM)
-            dist.all_reduce(s_max, op=dist.ReduceOp.MAX)
-            serve["solves_per_s"] = float(s_sum[0].item())
-            serve["p99_ms_max_over_ranks"] = float(s_max[1].item())
+            serve["solves_per_s"] = rank_reduce([serve["solves_per_s"]], "sum", world, dev)[0]
+            serve["p99_ms_max_over_ranks"] = rank_reduce([serve["p99_ms"]], "max", world, dev)[0]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
