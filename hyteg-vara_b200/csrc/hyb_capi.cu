@@ -1309,6 +1309,7 @@ enum GraphKind : int
    kMixedStep    = 2, // FP32 V-cycle on A e = r (r from the previous step), x += e, new r and ||r||^2
    kNorm64       = 3, // r = b - A x into gmg_tmp and ||r||^2
    kNormMixed    = 4, // r = b - A x into the FP64 residual of the mixed solver and ||r||^2
+   kFmg64        = 8, // full multigrid, kFmg64 + c: c FP64 V-cycles per level (1 <= c <= 8)
 };
 
 void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s )
@@ -1322,6 +1323,19 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
       HYB_CUDA( cudaMemsetAsync( g.x32->ptr< float >( l ), 0, g.x32->levelBytes( l ), s ) );
       vcycle< float >( g, *g.x32, *g.b32, *g.t32, l, s );
       launchAddCorrection< float >( *g.st, l, x.ptr< double >( l ), g.x32->ptr< float >( l ), kGmgFlag, s );
+   }
+   if ( kind > kFmg64 && kind <= kFmg64 + 8 )
+   {
+      // FullMultigridSolver::solve (FullMultigridSolver.hpp:51-75) with linear FMG
+      // prolongation on inner and Neumann DoFs
+      for ( int lc = g.minL; lc <= l; ++lc )
+      {
+         for ( int c = 0; c < kind - kFmg64; ++c )
+            vcycle< double >( g, x, b, *g.tmp64, lc, s );
+         if ( lc < l )
+            launchProlongate< double >( *g.st, lc, x.ptr< double >( lc ), x.ptr< double >( lc + 1 ), kGmgFlag, false, s );
+      }
+      return;
    }
    if ( kind != kCycle64 )
    {
@@ -1399,6 +1413,9 @@ void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s
       const int top = std::min( l, g.progTop );
       if ( kind == kCycle64 || kind == kCycle64Norm )
          ensureProgram< double >( g, x, b, *g.tmp64, top );
+      if ( kind > kFmg64 && kind <= kFmg64 + 8 )
+         for ( int t = g.minL; t <= top; ++t )
+            ensureProgram< double >( g, x, b, *g.tmp64, t );
       if ( kind == kMixedStep )
          ensureProgram< float >( g, *g.x32, *g.b32, *g.t32, top );
    }
@@ -2036,6 +2053,17 @@ int hyb_gmg_solve( hyb_gmg* gh, hyb_function* xh, hyb_function* bh, int level, v
    Function *x = FN( xh ), *b = FN( bh );
    checkGmg( g, x, b, level );
    runGraph( *g, *x, *b, level, 0, S( stream ) );
+   HYB_API_END
+}
+
+int hyb_gmg_solve_fmg( hyb_gmg* gh, hyb_function* xh, hyb_function* bh, int level, int cyclesPerLevel, void* stream )
+{
+   HYB_API_BEGIN
+   Gmg*      g = gh;
+   Function *x = FN( xh ), *b = FN( bh );
+   checkGmg( g, x, b, level );
+   require( cyclesPerLevel >= 1 && cyclesPerLevel <= 8, "cycles per level must be in [1, 8]" );
+   runGraph( *g, *x, *b, level, kFmg64 + cyclesPerLevel, S( stream ) );
    HYB_API_END
 }
 

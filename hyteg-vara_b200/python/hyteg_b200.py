@@ -33,7 +33,7 @@ SYMBOLS = [
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
     "hyb_operator_create_divkgrad_rff", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
-    "hyb_storage_create_spherical_shell",
+    "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg",
 ]
 
 COEFF_CONSTANT, COEFF_LOGNORMAL, COEFF_RADIAL = 0, 1, 2
@@ -112,6 +112,7 @@ def load(path=LIB_PATH):
         "hyb_function_fill_uniform_random": (I, [P, I, ctypes.c_uint64, D, P]),
         "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, D, PP]),
         "hyb_storage_create_spherical_shell": (I, [I, I, D, D, I, PP]),
+        "hyb_gmg_solve_fmg": (I, [P, P, P, I, I, P]),
         "hyb_server_create": (I, [ctypes.c_size_t, I, I, PP]),
         "hyb_server_destroy": (I, [P]),
         "hyb_server_footprint": (I, [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
@@ -415,6 +416,10 @@ class GeometricMultigridSolver:
 
     def solve(self, x, b, level, stream=None):
         _check(load().hyb_gmg_solve(self.h, x.h, b.h, level, _stream(stream)))
+
+    def solve_fmg(self, x, b, level, cycles_per_level=1, stream=None):
+        """FullMultigridSolver::solve: b must hold the right-hand side on every level."""
+        _check(load().hyb_gmg_solve_fmg(self.h, x.h, b.h, level, cycles_per_level, _stream(stream)))
 
     def solve_to_tolerance(self, x, b, level, rel_tol, max_cycles=100, precision=64, stream=None):
         hist = np.zeros(max_cycles + 1)

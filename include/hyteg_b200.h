@@ -27,6 +27,7 @@
  *   hyb_restrict                  P1toP1LinearRestriction::restrict (P1toP1LinearRestriction.cpp:168-345)
  *   hyb_cg_solve                  CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:66-135)
  *   hyb_gmg_create / hyb_gmg_solve  GeometricMultigridSolver ctor / solve (GeometricMultigridSolver.hpp:42-235)
+ *   hyb_gmg_solve_fmg             FullMultigridSolver::solve (src/hyteg/solvers/FullMultigridSolver.hpp)
  *
  *   hyb_server_*                  no reference counterpart (the reference runs one solve per
  *                                 MPI job): a continuous-batching loop that serves many
@@ -192,6 +193,13 @@ int hyb_gmg_solve( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, void
  * precision 64: plain FP64 V-cycles; 32: FP32 V-cycles on the residual equation inside
  * FP64 iterative refinement (FP64 residual, update and coarse solve).
  * history[0..cycles] (optional) receives the relative residuals. */
+/* FullMultigridSolver::solve (src/hyteg/solvers/FullMultigridSolver.hpp:51-75) with linear
+ * FMG prolongation: for l = min_level .. level, cycles_per_level V-cycles on l, then
+ * x(l+1) = P x(l) on inner and Neumann DoFs. As in the reference, b must hold the
+ * right-hand side on every level, x's coarsest level is the start of the coarse solve, and
+ * the V-cycles use b's levels below the current one as scratch. Captured as one CUDA graph
+ * per (x, b, level, cycles_per_level); asynchronous. */
+int hyb_gmg_solve_fmg( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, int cycles_per_level, void* stream );
 int hyb_gmg_solve_to_tolerance( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, double rel_tol,
                                 int max_cycles, int precision, double* history, int* cycles, void* stream );
 

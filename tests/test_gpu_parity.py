@@ -368,3 +368,39 @@ def test_config1_ten_cycles_residual_history(H, oracle_mod):
                        rel_tol=0.0)
     f_gpu, f_ref = hist[1:] / hist[:-1], h_ref[1:] / h_ref[:-1]
     assert np.all(np.abs(f_gpu - f_ref) <= 0.25 * f_ref + 1e-3), (f_gpu, f_ref)
+
+
+def test_full_multigrid_start(H, oracle_mod, setups):
+    """FullMultigridSolver: one FMG pass (b restricted to every level, one V(3,3) cycle per
+    level, linear FMG prolongation) equals the same sequence of solver calls made one by one
+    (1e-12), leaves a smaller residual than one V-cycle from zero, and the refinement loop
+    from it needs no more cycles to 1e-8."""
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    R, P = H.P1toP1LinearRestriction(), H.P1toP1LinearProlongation()
+    b = O.uniform_rhs(orc.coords_of(L), 2, 2 << L)
+
+    def fresh():
+        fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+        fb.set(b, L)
+        for l in range(L, 0, -1):
+            R.restrict(fb, l, H.INNER | H.NEUMANN)
+        return fx, fb
+
+    x1, b1 = fresh()
+    gmg.solve_fmg(x1, b1, L, 1)
+    x2, b2 = fresh()
+    for l in range(0, L + 1):
+        gmg.solve(x2, b2, l)
+        if l < L:
+            P.prolongate(x2, l, H.INNER | H.NEUMANN)
+    close(x1.get(L), x2.get(L), 1e-12)
+    # residual after FMG vs after one V-cycle from zero
+    r_fmg = gmg.solve_to_tolerance(x1, b1, L, 1.0, max_cycles=0)[0]
+    x0, b0 = fresh()
+    h0 = gmg.solve_to_tolerance(x0, b0, L, 1e-8, max_cycles=60, precision=32)
+    assert r_fmg < h0[1], (r_fmg, h0[:3])
+    h1 = gmg.solve_to_tolerance(x1, b1, L, 1e-8, max_cycles=60, precision=32)
+    assert h1[-1] <= 1e-8 and len(h1) <= len(h0), (h1, h0)
