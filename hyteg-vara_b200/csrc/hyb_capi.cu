@@ -818,18 +818,17 @@ static const int kFusedInteriorMaxPoints = [] {
 }();
 
 template < typename T >
-void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream )
+void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream, bool backwards = false )
 {
    const Storage&   s  = *op.st;
    const auto&      L  = s.L( l );
    const OpDev< T > od = op.dev< T >( l );
    // interface passes: one launch per colour over that colour's surface DoFs
-   for ( int c = 0; c < s.td.m; ++c )
-   {
+   auto iface = [&]( int c ) {
       const int* co = &L.colourOff[4 * c];
       const long lanes = bdryLaneCount( co[1], co[2], co[3] );
       if ( lanes == 0 )
-         continue;
+         return;
       const int       nb   = int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) );
       const int32_t*  list = L.colourList.p + co[0];
       const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
@@ -838,35 +837,54 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       else
          pdlLaunch( k_sor_iface< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
       HYB_CHECK_LAUNCH();
-   }
-   if ( L.dev.nPts == 0 )
-      return;
-   // small levels: the four interior colours in one launch, a block per cell
-   if ( L.dev.nPts <= kFusedInteriorMaxPoints )
+   };
+   // interior passes
+   auto interior = [&]() {
+      if ( L.dev.nPts == 0 )
+         return;
+      // small levels: the four interior colours in one launch, a block per cell
+      if ( L.dev.nPts <= kFusedInteriorMaxPoints )
+      {
+         const int* o  = L.dev.ptsOff;
+         const int  bw = backwards ? 1 : 0;
+         if ( op.variable )
+            pdlLaunch( k_sor_interior_cells< T, true >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, o[0], o[1], o[2], o[3], o[4], bw );
+         else
+            pdlLaunch( k_sor_interior_cells< T, false >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, o[0], o[1], o[2], o[3], o[4], bw );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
+      // one launch per colour
+      for ( int k = 0; k < kInteriorColours; ++k )
+      {
+         const int c     = backwards ? kInteriorColours - 1 - k : k;
+         const int begin = L.dev.ptsOff[c], count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
+         if ( count == 0 )
+            continue;
+         if ( op.variable )
+            pdlLaunch( k_sor_interior< T, true >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, c, begin, count, L.colourBlocks );
+         else
+            pdlLaunch( k_sor_interior< T, false >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, c, begin, count, L.colourBlocks );
+         HYB_CHECK_LAUNCH();
+      }
+   };
+   // forward: surface colours 0..m-1, then the interior colours 0..3; backwards (the
+   // multicolour smooth_sor_backwards, P1Operator.hpp:385-400): the same passes reversed
+   if ( !backwards )
    {
-      const int* o = L.dev.ptsOff;
-      if ( op.variable )
-         pdlLaunch( k_sor_interior_cells< T, true >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
-                    relax, o[0], o[1], o[2], o[3], o[4] );
-      else
-         pdlLaunch( k_sor_interior_cells< T, false >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
-                    relax, o[0], o[1], o[2], o[3], o[4] );
-      HYB_CHECK_LAUNCH();
-      return;
+      for ( int c = 0; c < s.td.m; ++c )
+         iface( c );
+      interior();
    }
-   // interior passes: one launch per colour
-   for ( int c = 0; c < kInteriorColours; ++c )
+   else
    {
-      const int begin = L.dev.ptsOff[c], count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
-      if ( count == 0 )
-         continue;
-      if ( op.variable )
-         pdlLaunch( k_sor_interior< T, true >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, c, begin, count,
-                                                                          L.colourBlocks );
-      else
-         pdlLaunch( k_sor_interior< T, false >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, c, begin,
-                                                                           count, L.colourBlocks );
-      HYB_CHECK_LAUNCH();
+      interior();
+      for ( int c = s.td.m - 1; c >= 0; --c )
+         iface( c );
    }
 }
 
@@ -999,6 +1017,7 @@ struct Gmg
    Storage*  st;
    Operator* op;
    int       minL, maxL, pre, post, smoother, coarseMaxIter;
+   int       cycleType = HYB_CYCLE_V;
    double    relax, coarseTol;
    std::unique_ptr< Function > tmp64;         // gmg_tmp
    std::unique_ptr< Function > x32, b32, t32; // FP32 inner hierarchy (mixed precision)
@@ -1050,6 +1069,12 @@ void smooth( Gmg& g, int l, T* x, const T* b, T* scratch, cudaStream_t stream )
 {
    if ( g.smoother == HYB_SMOOTHER_SOR )
       launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
+   else if ( g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR )
+   {
+      // SymmetricSORSmoother::solve (SymmetricSORSmoother.hpp:38-57): forward, then backwards
+      launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
+      launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream, true );
+   }
    else
    {
       // Jacobi needs the old iterate: scratch = x, then x = scratch + relax D^-1 (b - A scratch)
@@ -1111,14 +1136,13 @@ struct PhaseList
    {
       const Storage& s = *g.st;
       const auto&    L = s.L( l );
-      if ( g.smoother == HYB_SMOOTHER_SOR )
+      if ( g.smoother == HYB_SMOOTHER_SOR || g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR )
       {
-         for ( int c = 0; c < s.td.m; ++c )
-         {
+         auto iface = [&]( int c ) {
             const int* co    = &L.colourOff[4 * c];
             const long lanes = bdryLaneCount( co[1], co[2], co[3] );
             if ( lanes == 0 )
-               continue;
+               return;
             const int32_t* list = L.colourList.p + co[0];
             Phase&         P    = add( kPhSorIface, l, int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) ), 0 );
             P.p0                = x;
@@ -1126,12 +1150,11 @@ struct PhaseList
             P.relax             = g.relax;
             P.flag              = kGmgFlag;
             P.bl                = BdryLists{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
-         }
-         for ( int c = 0; c < kInteriorColours; ++c )
-         {
+         };
+         auto interior = [&]( int c ) {
             const int count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
             if ( count == 0 )
-               continue;
+               return;
             Phase& P = add( kPhSorInterior, l, L.colourBlocks, L.colourBlocks );
             P.p0     = x;
             P.p1     = const_cast< T* >( b );
@@ -1139,6 +1162,17 @@ struct PhaseList
             P.a0     = c;
             P.a1     = L.dev.ptsOff[c];
             P.a2     = count;
+         };
+         for ( int c = 0; c < s.td.m; ++c )
+            iface( c );
+         for ( int c = 0; c < kInteriorColours; ++c )
+            interior( c );
+         if ( g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR )
+         {
+            for ( int c = kInteriorColours - 1; c >= 0; --c )
+               interior( c );
+            for ( int c = s.td.m - 1; c >= 0; --c )
+               iface( c );
          }
       }
       else
@@ -1224,6 +1258,8 @@ struct PhaseList
          P.n      = slabElems( l - 1 );
       }
       vcycle< T >( x, b, tmp, l - 1 );
+      if ( g.cycleType == HYB_CYCLE_W )
+         vcycle< T >( x, b, tmp, l - 1 );
       {
          const auto& F  = s.L( l );
          const int   nc = F.dev.nPts > 0 ? F.ptsBlocks : 0;
@@ -1296,6 +1332,8 @@ void vcycle( Gmg& g, Function& x, Function& b, Function& tmp, int l, cudaStream_
    launchRestrict< T >( *g.st, l, tmp.ptr< T >( l ), b.ptr< T >( l - 1 ), kGmgFlag, stream );
    HYB_CUDA( cudaMemsetAsync( x.ptr< T >( l - 1 ), 0, x.levelBytes( l - 1 ), stream ) ); // x.interpolate(0, l-1)
    vcycle< T >( g, x, b, tmp, l - 1, stream );
+   if ( g.cycleType == HYB_CYCLE_W ) // GeometricMultigridSolver.hpp:201-204
+      vcycle< T >( g, x, b, tmp, l - 1, stream );
    launchProlongate< T >( *g.st, l - 1, x.ptr< T >( l - 1 ), x.ptr< T >( l ), kGmgFlag, true, stream );
    for ( int i = 0; i < g.post; ++i )
       smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
@@ -1515,6 +1553,19 @@ int hyb_storage_create( const double* coords, int64_t nv, const int64_t* tets, i
    for ( int64_t i = 0; i < nt; ++i )
       for ( int k = 0; k < 4; ++k )
          T[i][k] = int( tets[4 * i + k] );
+   auto s = std::make_unique< hyb_storage_s >();
+   buildStorage( *s, V, T, maxLevel );
+   *out = s.release();
+   HYB_API_END
+}
+
+int hyb_storage_create_from_gmsh( const char* path, int maxLevel, hyb_storage** out )
+{
+   HYB_API_BEGIN
+   require( path && out, "null argument" );
+   std::vector< std::array< double, 3 > > V;
+   std::vector< std::array< int, 4 > >    T;
+   readGmsh( path, V, T );
    auto s = std::make_unique< hyb_storage_s >();
    buildStorage( *s, V, T, maxLevel );
    *out = s.release();
@@ -1927,6 +1978,24 @@ int hyb_operator_smooth_sor( hyb_operator* oh, hyb_function* dh, hyb_function* r
    HYB_API_END
 }
 
+int hyb_operator_smooth_sor_backwards( hyb_operator* oh, hyb_function* dh, hyb_function* rh, double relax, int level,
+                                       int flag, void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *u = FN( dh ), *b = FN( rh );
+   checkOpFn( op, u, level );
+   checkOpFn( op, b, level );
+   require( u != b, "smooth_sor_backwards needs distinct dst and rhs" );
+   require( u->dtype == b->dtype, "dtypes differ" );
+   if ( u->dtype == HYB_F64 )
+      launchSor< double >( *op, level, u->ptr< double >( level ), b->ptr< double >( level ), relax, flag, S( stream ), true );
+   else
+      launchSor< float >( *op, level, u->ptr< float >( level ), b->ptr< float >( level ), float( relax ), flag, S( stream ),
+                          true );
+   HYB_API_END
+}
+
 int hyb_operator_smooth_jac( hyb_operator* oh, hyb_function* dh, hyb_function* rh, hyb_function* sh, double relax, int level,
                              int flag, void* stream )
 {
@@ -2022,7 +2091,8 @@ int hyb_gmg_create( hyb_storage* s, hyb_operator* oh, int minL, int maxL, int pr
    require( op->st == ST( s ), "operator belongs to another storage" );
    require( minL >= op->minL && maxL <= op->maxL && minL <= maxL, "GMG levels outside the operator's level range" );
    require( pre >= 0 && post >= 0, "smoothing steps must be non-negative" );
-   require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI, "unknown smoother" );
+   require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI || smoother == HYB_SMOOTHER_SYMMETRIC_SOR,
+            "unknown smoother" );
    auto g = std::make_unique< hyb_gmg_s >();
    initGmg( *g, ST( s ), op, minL, maxL, pre, post, relax, smoother, coarseTol, coarseMaxIter );
    *out = g.release();
@@ -2033,6 +2103,25 @@ int hyb_gmg_destroy( hyb_gmg* g )
 {
    HYB_API_BEGIN
    delete static_cast< hyb_gmg_s* >( g );
+   HYB_API_END
+}
+
+int hyb_gmg_set_cycle_type( hyb_gmg* gh, int cycleType )
+{
+   HYB_API_BEGIN
+   Gmg* g = static_cast< Gmg* >( static_cast< hyb_gmg_s* >( gh ) );
+   require( g != nullptr, "null argument" );
+   require( cycleType == HYB_CYCLE_V || cycleType == HYB_CYCLE_W, "unknown cycle type" );
+   if ( cycleType == g->cycleType )
+      return HYB_OK;
+   // the recorded graphs and coarse-level programs encode the old cycle; drop them once
+   // no work that uses them is in flight
+   HYB_CUDA( cudaDeviceSynchronize() );
+   for ( auto& gr : g->graphs )
+      cudaGraphExecDestroy( gr.exec );
+   g->graphs.clear();
+   g->programs.clear();
+   g->cycleType = cycleType;
    HYB_API_END
 }
 

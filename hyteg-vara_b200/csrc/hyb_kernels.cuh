@@ -665,10 +665,11 @@ __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv
 // cell runs the colours one after the other with __syncthreads() in between. Interior
 // points of different cells are never coupled, so no other block's progress matters; on
 // small levels, where a colour pass has little work, this saves three launches per sweep.
+// backwards != 0 runs the colours 3..0 (the backward sweep of a symmetric SOR step).
 template < typename T, bool VAR >
 __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                                const T* __restrict__ rhs, T relax, int o0, int o1, int o2,
-                                                               int o3, int o4 )
+                                                               int o3, int o4, int backwards )
 {
    HYB_PDL_PROLOGUE();
    const int            cell = blockIdx.x;
@@ -678,8 +679,9 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, Level
    const T* bc = rhs + size_t( cell ) * lv.stride;
    const int off[5] = { o0, o1, o2, o3, o4 };
 #pragma unroll
-   for ( int c = 0; c < kInteriorColours; ++c )
+   for ( int k = 0; k < kInteriorColours; ++k )
    {
+      const int c = backwards ? kInteriorColours - 1 - k : k;
       for ( int i = off[c] + int( threadIdx.x ); i < off[c + 1]; i += int( blockDim.x ) )
       {
          const int32_t e  = __ldg( lv.ptsC + i );

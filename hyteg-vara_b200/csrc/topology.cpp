@@ -1,6 +1,8 @@
 // Host-side macro-mesh topology (see topology.hpp).
 #include "topology.hpp"
+#include <fstream>
 #include <map>
+#include <string>
 
 #include <algorithm>
 #include <cmath>
@@ -305,6 +307,91 @@ void meshCuboid( int nx, int ny, int nz, const double lo[3], const double hi[3],
                   c[m] = vid( ix + off[tn[m]][0], iy + off[tn[m]][1], iz + off[tn[m]][2] );
                cells.insert( c );
             }
+   T.assign( cells.begin(), cells.end() );
+}
+
+// MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp:36-190): Gmsh 2.2 ASCII.
+// Vertices in ascending file id (made 0-based), tetrahedra (element type 4) in the
+// lexicographic order of their vertex-index lists (the reference keeps them in a std::map
+// keyed by that list); points (15), edges (1) and triangles (2) are read and skipped (their
+// boundary tags are superseded by setMeshBoundaryFlagsOnBoundary). Any other element type
+// is an error, as in the reference.
+void readGmsh( const std::string& path, std::vector< std::array< double, 3 > >& V, std::vector< std::array< int, 4 > >& T )
+{
+   std::ifstream f( path );
+   if ( !f )
+      throw std::invalid_argument( "readGmsh: cannot open " + path );
+   std::string tok;
+   auto        expect = [&]( const char* want ) {
+      if ( !( f >> tok ) || tok != want )
+         throw std::invalid_argument( std::string( "readGmsh: expected " ) + want + " in " + path );
+   };
+   expect( "$MeshFormat" );
+   if ( !( f >> tok ) || tok != "2.2" )
+      throw std::invalid_argument( "readGmsh: only the Gmsh 2.2 ASCII format is supported" );
+   int fileType = 0, dataSize = 0;
+   f >> fileType >> dataSize;
+   if ( fileType != 0 )
+      throw std::invalid_argument( "readGmsh: binary Gmsh files are not supported" );
+   expect( "$EndMeshFormat" );
+   expect( "$Nodes" );
+   long nNodes = 0;
+   f >> nNodes;
+   if ( !f || nNodes < 4 )
+      throw std::invalid_argument( "readGmsh: bad node count" );
+   std::map< long, std::array< double, 3 > > nodes;
+   for ( long i = 0; i < nNodes; ++i )
+   {
+      long                    id;
+      std::array< double, 3 > x;
+      if ( !( f >> id >> x[0] >> x[1] >> x[2] ) )
+         throw std::invalid_argument( "readGmsh: truncated $Nodes" );
+      nodes[id] = x;
+   }
+   expect( "$EndNodes" );
+   std::map< long, int > index;
+   V.clear();
+   for ( const auto& kv : nodes )
+   {
+      index[kv.first] = int( V.size() );
+      V.push_back( kv.second );
+   }
+   expect( "$Elements" );
+   long nElem = 0;
+   f >> nElem;
+   std::set< std::array< int, 4 > > cells;
+   for ( long e = 0; e < nElem; ++e )
+   {
+      long id;
+      int  type, ntags;
+      if ( !( f >> id >> type >> ntags ) || ntags < 0 )
+         throw std::invalid_argument( "readGmsh: truncated $Elements" );
+      for ( int t = 0; t < ntags; ++t )
+      {
+         long tag;
+         f >> tag;
+      }
+      const int nv = type == 15 ? 1 : type == 1 ? 2 : type == 2 ? 3 : type == 4 ? 4 : -1;
+      if ( nv < 0 )
+         throw std::invalid_argument( "readGmsh: unsupported element type " + std::to_string( type ) );
+      std::array< int, 4 > c{};
+      for ( int k = 0; k < nv; ++k )
+      {
+         long v;
+         if ( !( f >> v ) )
+            throw std::invalid_argument( "readGmsh: truncated element" );
+         auto it = index.find( v );
+         if ( it == index.end() )
+            throw std::invalid_argument( "readGmsh: element refers to an unknown node" );
+         if ( type == 4 )
+            c[k] = it->second;
+      }
+      if ( type == 4 )
+         cells.insert( c );
+   }
+   expect( "$EndElements" );
+   if ( cells.empty() )
+      throw std::invalid_argument( "readGmsh: no tetrahedra in " + path );
    T.assign( cells.begin(), cells.end() );
 }
 

@@ -90,5 +90,6 @@ void meshCuboid( int nx, int ny, int nz, const double lo[3], const double hi[3],
                  std::vector< std::array< int, 4 > >& T );
 void meshSphericalShell( int ntan, int nrad, double rmin, double rmax, std::vector< std::array< double, 3 > >& V,
                          std::vector< std::array< int, 4 > >& T );
+void readGmsh( const std::string& path, std::vector< std::array< double, 3 > >& V, std::vector< std::array< int, 4 > >& T );
 
 } // namespace hyb

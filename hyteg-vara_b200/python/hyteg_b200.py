@@ -18,7 +18,8 @@ LIB_PATH = os.path.join(PKG, "libhyteg_b200.so")
 INNER, DIRICHLET, NEUMANN, FREESLIP, ALL = 1, 2, 4, 8, 15
 REPLACE, ADD = 0, 1
 F64, F32 = 0, 1
-SMOOTHER_SOR, SMOOTHER_JACOBI = 0, 1
+SMOOTHER_SOR, SMOOTHER_JACOBI, SMOOTHER_SYMMETRIC_SOR = 0, 1, 2
+CYCLE_V, CYCLE_W = 0, 1
 
 # the C ABI symbols (include/hyteg_b200.h); tests check that the library exports all of them
 SYMBOLS = [
@@ -33,7 +34,8 @@ SYMBOLS = [
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
     "hyb_operator_create_divkgrad_rff", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
-    "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg",
+    "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
+    "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type",
 ]
 
 COEFF_CONSTANT, COEFF_LOGNORMAL, COEFF_RADIAL = 0, 1, 2
@@ -113,6 +115,9 @@ def load(path=LIB_PATH):
         "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, D, PP]),
         "hyb_storage_create_spherical_shell": (I, [I, I, D, D, I, PP]),
         "hyb_gmg_solve_fmg": (I, [P, P, P, I, I, P]),
+        "hyb_storage_create_from_gmsh": (I, [ctypes.c_char_p, I, PP]),
+        "hyb_operator_smooth_sor_backwards": (I, [P, P, P, D, I, I, P]),
+        "hyb_gmg_set_cycle_type": (I, [P, I]),
         "hyb_server_create": (I, [ctypes.c_size_t, I, I, PP]),
         "hyb_server_destroy": (I, [P]),
         "hyb_server_footprint": (I, [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
@@ -169,6 +174,15 @@ class PrimitiveStorage:
     @classmethod
     def cuboid(cls, nx, ny, nz, max_level, lo=(0, 0, 0), hi=(1, 1, 1)):
         return cls(cuboid=(nx, ny, nz, lo, hi), max_level=max_level)
+
+    @classmethod
+    def from_gmsh(cls, path, max_level):
+        """MeshInfo::fromGmshFile: a Gmsh 2.2 ASCII tetrahedral mesh."""
+        st = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        _check(load().hyb_storage_create_from_gmsh(os.fsencode(path), max_level, ctypes.byref(h)))
+        st.h, st.max_level = h, max_level
+        return st
 
     @classmethod
     def spherical_shell(cls, ntan, nrad, rmin, rmax, max_level):
@@ -316,8 +330,15 @@ class _Operator:
     def smooth_sor(self, dst, rhs, relax, level, flag, stream=None):
         _check(load().hyb_operator_smooth_sor(self.h, dst.h, rhs.h, float(relax), level, flag, _stream(stream)))
 
+    def smooth_sor_backwards(self, dst, rhs, relax, level, flag, stream=None):
+        _check(load().hyb_operator_smooth_sor_backwards(self.h, dst.h, rhs.h, float(relax), level, flag,
+                                                        _stream(stream)))
+
     def smooth_gs(self, dst, rhs, level, flag, stream=None):
         self.smooth_sor(dst, rhs, 1.0, level, flag, stream)
+
+    def smooth_gs_backwards(self, dst, rhs, level, flag, stream=None):
+        self.smooth_sor_backwards(dst, rhs, 1.0, level, flag, stream)
 
     def smooth_jac(self, dst, rhs, src, relax, level, flag, stream=None):
         _check(load().hyb_operator_smooth_jac(self.h, dst.h, rhs.h, src.h, float(relax), level, flag,
@@ -396,12 +417,14 @@ class GeometricMultigridSolver:
     minLevel, maxLevel, preSmooth, postSmooth): solve() performs one V-cycle."""
 
     def __init__(self, storage, A, min_level, max_level, pre=3, post=3, relax=1.0, smoother=SMOOTHER_SOR,
-                 coarse_tol=1e-12, coarse_max_iter=10000):
+                 coarse_tol=1e-12, coarse_max_iter=10000, cycle_type=CYCLE_V):
         self.storage, self.A = storage, A
         h = ctypes.c_void_p()
         _check(load().hyb_gmg_create(storage.h, A.h, min_level, max_level, pre, post, float(relax), smoother,
                                      float(coarse_tol), coarse_max_iter, ctypes.byref(h)))
         self.h = h
+        if cycle_type != CYCLE_V:
+            _check(load().hyb_gmg_set_cycle_type(self.h, cycle_type))
 
     def close(self):
         if getattr(self, "h", None):

@@ -21,13 +21,16 @@
  *                                 (src/hyteg/elementwiseoperators/P1ElementwiseOperator.cpp:64-302)
  *   hyb_operator_apply            Operator::apply(src, dst, level, flag, updateType) (P1Operator.hpp:196)
  *   hyb_operator_smooth_sor       SORSmoothable::smooth_sor(dst, rhs, relax, level, flag) (P1Operator.hpp:343-422)
+ *   hyb_operator_smooth_sor_backwards  SORBackwardsSmoothable::smooth_sor_backwards (P1Operator.hpp:424-431)
  *   hyb_operator_smooth_jac       WeightedJacobiSmoothable::smooth_jac (P1Operator.hpp:424-440)
  *   hyb_prolongate                P1toP1LinearProlongation::prolongate / prolongateAndAdd
  *                                 (src/hyteg/gridtransferoperators/P1toP1LinearProlongation.cpp:194-410)
  *   hyb_restrict                  P1toP1LinearRestriction::restrict (P1toP1LinearRestriction.cpp:168-345)
  *   hyb_cg_solve                  CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:66-135)
  *   hyb_gmg_create / hyb_gmg_solve  GeometricMultigridSolver ctor / solve (GeometricMultigridSolver.hpp:42-235)
+ *   hyb_gmg_set_cycle_type        the CycleType argument of the GeometricMultigridSolver ctor (V or W)
  *   hyb_gmg_solve_fmg             FullMultigridSolver::solve (src/hyteg/solvers/FullMultigridSolver.hpp)
+ *   hyb_storage_create_from_gmsh  MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp)
  *
  *   hyb_server_*                  no reference counterpart (the reference runs one solve per
  *                                 MPI job): a continuous-batching loop that serves many
@@ -72,9 +75,14 @@ typedef enum
 /* value types */
 #define HYB_F64 0
 #define HYB_F32 1
-/* smoothers of the V-cycle */
+/* smoothers of the V-cycle: SORSmoother, WeightedJacobiSmoother, SymmetricSORSmoother
+ * (src/hyteg/solvers/SymmetricSORSmoother.hpp: a forward, then a backward sweep) */
 #define HYB_SMOOTHER_SOR 0
 #define HYB_SMOOTHER_JACOBI 1
+#define HYB_SMOOTHER_SYMMETRIC_SOR 2
+/* multigrid cycle types (GeometricMultigridSolver.hpp CycleType) */
+#define HYB_CYCLE_V 0
+#define HYB_CYCLE_W 1
 
 typedef struct hyb_storage_s  hyb_storage;
 typedef struct hyb_function_s hyb_function;
@@ -89,6 +97,9 @@ long long   hyb_kernel_launch_count( void );
 /* ---- storage (macro-mesh + level hierarchy metadata on the device) ---- */
 int     hyb_storage_create( const double* coords, int64_t num_vertices, const int64_t* tets, int64_t num_tets,
                             int max_level, hyb_storage** out );
+/* MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp): a Gmsh 2.2 ASCII file,
+ * vertices in file-id order, tetrahedra in the reference's cell order */
+int     hyb_storage_create_from_gmsh( const char* path, int max_level, hyb_storage** out );
 /* thick spherical shell: icosahedral sphere with (ntan - 1)^2 triangles per icosahedron
  * face on nrad radii in [rmin, rmax], prisms split into three tetrahedra */
 int     hyb_storage_create_spherical_shell( int ntan, int nrad, double rmin, double rmax, int max_level, hyb_storage** out );
@@ -170,6 +181,10 @@ int hyb_operator_residual( hyb_operator* op, hyb_function* x, hyb_function* b, h
 /* one multicolour SOR sweep (colours in increasing order) */
 int hyb_operator_smooth_sor( hyb_operator* op, hyb_function* dst, hyb_function* rhs, double relax, int level, int flag,
                              void* stream );
+/* one backward multicolour SOR sweep: the passes of hyb_operator_smooth_sor in reverse
+ * order (interior colours 3..0, then the surface colours m-1..0) */
+int hyb_operator_smooth_sor_backwards( hyb_operator* op, hyb_function* dst, hyb_function* rhs, double relax, int level,
+                                       int flag, void* stream );
 /* dst = src + relax * diag(A)^-1 (rhs - A src) */
 int hyb_operator_smooth_jac( hyb_operator* op, hyb_function* dst, hyb_function* rhs, hyb_function* src, double relax,
                              int level, int flag, void* stream );
@@ -187,6 +202,9 @@ int hyb_cg_solve( hyb_operator* op, hyb_function* x, hyb_function* b, int level,
 int hyb_gmg_create( hyb_storage* s, hyb_operator* op, int min_level, int max_level, int pre_smooth, int post_smooth,
                     double relax, int smoother, double coarse_tol, int coarse_max_iter, hyb_gmg** out );
 int hyb_gmg_destroy( hyb_gmg* g );
+/* HYB_CYCLE_V (default) or HYB_CYCLE_W: with W the coarse-grid correction recurses twice
+ * (GeometricMultigridSolver.hpp:201-204); applies to every later solve of this solver */
+int hyb_gmg_set_cycle_type( hyb_gmg* g, int cycle_type );
 /* one V-cycle on level (GeometricMultigridSolver::solve); b's coarser levels are scratch */
 int hyb_gmg_solve( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, void* stream );
 /* blocking: cycles until ||b - Ax|| / ||b|| <= rel_tol (Inner|Neumann DoFs) or max_cycles.

@@ -58,6 +58,16 @@ class PrimitiveStorage
    {
       hybCheck( hyb_storage_create_cuboid( nx, ny, nz, lo, hi, maxLevel, &h_ ) );
    }
+   // MeshInfo::fromGmshFile: a Gmsh 2.2 ASCII tetrahedral mesh
+   PrimitiveStorage( const std::string& gmshFile, int maxLevel )
+   {
+      hybCheck( hyb_storage_create_from_gmsh( gmshFile.c_str(), maxLevel, &h_ ) );
+   }
+   // MeshInfo::meshSphericalShell( ntan, nrad, rmin, rmax ), affine macro-tets
+   PrimitiveStorage( int ntan, int nrad, double rmin, double rmax, int maxLevel )
+   {
+      hybCheck( hyb_storage_create_spherical_shell( ntan, nrad, rmin, rmax, maxLevel, &h_ ) );
+   }
    ~PrimitiveStorage() { hyb_storage_destroy( h_ ); }
    PrimitiveStorage( const PrimitiveStorage& )            = delete;
    PrimitiveStorage& operator=( const PrimitiveStorage& ) = delete;
@@ -174,9 +184,19 @@ class P1OperatorBase
       hybCheck( hyb_operator_smooth_sor( h_, dst.handle(), rhs.handle(), double( relax ), level, flag, nullptr ) );
    }
    template < typename V >
+   void smooth_sor_backwards( const P1Function< V >& dst, const P1Function< V >& rhs, V relax, int level, DoFType flag ) const
+   {
+      hybCheck( hyb_operator_smooth_sor_backwards( h_, dst.handle(), rhs.handle(), double( relax ), level, flag, nullptr ) );
+   }
+   template < typename V >
    void smooth_gs( const P1Function< V >& dst, const P1Function< V >& rhs, int level, DoFType flag ) const
    {
       smooth_sor( dst, rhs, V( 1 ), level, flag );
+   }
+   template < typename V >
+   void smooth_gs_backwards( const P1Function< V >& dst, const P1Function< V >& rhs, int level, DoFType flag ) const
+   {
+      smooth_sor_backwards( dst, rhs, V( 1 ), level, flag );
    }
    template < typename V >
    void smooth_jac( const P1Function< V >& dst, const P1Function< V >& rhs, const P1Function< V >& src, V relax, int level,
@@ -257,26 +277,42 @@ class CGSolver
    int    iterations_ = 0;
 };
 
-// V-cycle with SOR smoothing (SORSmoother, relax) and an FP64 CG coarse solve.
+enum class CycleType
+{
+   VCYCLE = HYB_CYCLE_V,
+   WCYCLE = HYB_CYCLE_W
+};
+
+// V- or W-cycle with SOR smoothing (SORSmoother, relax; HYB_SMOOTHER_SYMMETRIC_SOR for
+// SymmetricSORSmoother, HYB_SMOOTHER_JACOBI for WeightedJacobiSmoother) and an FP64 CG
+// coarse solve.
 template < typename OperatorType >
 class GeometricMultigridSolver
 {
  public:
    GeometricMultigridSolver( const std::shared_ptr< PrimitiveStorage >& storage, const OperatorType& A, int minLevel,
                              int maxLevel, int preSmoothSteps = 3, int postSmoothSteps = 3, double sorRelax = 1.0,
-                             double coarseTolerance = 1e-12, int coarseMaxIter = 10000 )
+                             double coarseTolerance = 1e-12, int coarseMaxIter = 10000, CycleType cycleType = CycleType::VCYCLE,
+                             int smoother = HYB_SMOOTHER_SOR )
    {
       hybCheck( hyb_gmg_create( storage->handle(), A.handle(), minLevel, maxLevel, preSmoothSteps, postSmoothSteps, sorRelax,
-                                HYB_SMOOTHER_SOR, coarseTolerance, coarseMaxIter, &h_ ) );
+                                smoother, coarseTolerance, coarseMaxIter, &h_ ) );
+      if ( cycleType != CycleType::VCYCLE )
+         hybCheck( hyb_gmg_set_cycle_type( h_, int( cycleType ) ) );
    }
    ~GeometricMultigridSolver() { hyb_gmg_destroy( h_ ); }
    GeometricMultigridSolver( const GeometricMultigridSolver& )            = delete;
    GeometricMultigridSolver& operator=( const GeometricMultigridSolver& ) = delete;
 
-   // one V-cycle (GeometricMultigridSolver::solve); the coarser levels of b are scratch
+   // one cycle (GeometricMultigridSolver::solve); the coarser levels of b are scratch
    void solve( const OperatorType&, const P1Function< double >& x, const P1Function< double >& b, int level )
    {
       hybCheck( hyb_gmg_solve( h_, x.handle(), b.handle(), level, nullptr ) );
+   }
+   // FullMultigridSolver::solve with cyclesPerLevel cycles per level; b is needed on every level
+   void solveFullMultigrid( const P1Function< double >& x, const P1Function< double >& b, int level, int cyclesPerLevel = 1 )
+   {
+      hybCheck( hyb_gmg_solve_fmg( h_, x.handle(), b.handle(), level, cyclesPerLevel, nullptr ) );
    }
    // cycles until ||b - Ax|| / ||b|| <= relTol; precision 64 (FP64) or 32 (FP32 inner cycles)
    std::vector< double > solveToTolerance( const P1Function< double >& x, const P1Function< double >& b, int level,

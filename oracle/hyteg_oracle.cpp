@@ -526,25 +526,36 @@ inline void sorUpdate( T& x, T b, T diag, T off, T relax )
 // primitives are read from the ghost layers filled before the sweep (VertexDoFPackInfo.hpp:
 // edge->face only refreshes the face's own boundary, not its ghost layers), i.e.
 // from the start-of-sweep snapshot. Macro-cells read their full (refreshed) closure.
+//
+// smooth_sor_backwards (P1Operator.hpp:385-400, backwards = true): the stages run
+// C -> F -> E -> V with a ghost update (cell->face, face->edge, edge->vertex) before each
+// of the last three, so a stage reads its own closure current and everything else from
+// the state at the start of that stage; inside each primitive the lexicographic order is
+// reversed (sor_3D_macrocell_P1_backwards.cpp:52-57, sor_3D_macroface_P1_backwards.cpp).
 template < typename T >
-void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag )
+void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag, bool backwards )
 {
    const i64 N = lv.N;
    std::vector< T > xs( x, x + lv.nDof );
    const T* snap = xs.data();
+   auto refresh = [&]() { std::copy( x, x + lv.nDof, xs.begin() ); };
    // vertices (VertexDoFMacroVertex.hpp:208-229)
-   for ( i64 v = 0; v < i64( o.V.size() ); ++v )
-   {
-      if ( !flagged( lv.bc[v], flag ) )
-         continue;
-      auto val = [&]( i64 d ) { return d == v ? x[d] : snap[d]; };
-      T diag = 0, off = 0;
-      fullRow( o, op, lv, v, val, diag, off );
-      sorUpdate( x[v], b[v], diag, off, relax );
-   }
-   if ( N >= 2 )
-   {
-      // edges (P1Operator.hpp:1353-1423), each independent given the snapshot
+   auto vertices = [&]() {
+      for ( i64 k = 0; k < i64( o.V.size() ); ++k )
+      {
+         const i64 v = backwards ? i64( o.V.size() ) - 1 - k : k;
+         if ( !flagged( lv.bc[v], flag ) )
+            continue;
+         auto val = [&]( i64 d ) { return d == v ? x[d] : snap[d]; };
+         T diag = 0, off = 0;
+         fullRow( o, op, lv, v, val, diag, off );
+         sorUpdate( x[v], b[v], diag, off, relax );
+      }
+   };
+   // edges (P1Operator.hpp:1353-1423), each independent given the snapshot
+   auto edges = [&]() {
+      if ( N < 2 )
+         return;
 #pragma omp parallel for schedule( dynamic, 1 )
       for ( i64 e = 0; e < i64( o.E.size() ); ++e )
       {
@@ -555,18 +566,19 @@ void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, 
             const bool mine = ( lv.kind[d] == 1 && lv.owner[d] == e ) || ( lv.kind[d] == 0 && ( d == va || d == vb ) );
             return mine ? x[d] : snap[d];
          };
-         for ( i64 i = 0; i < N - 1; ++i )
+         for ( i64 k = 0; k < N - 1; ++k )
          {
-            const i64 d = lv.offE + e * ( N - 1 ) + i;
+            const i64 d = lv.offE + e * ( N - 1 ) + ( backwards ? N - 2 - k : k );
             T diag = 0, off = 0;
             fullRow( o, op, lv, d, val, diag, off );
             sorUpdate( x[d], b[d], diag, off, relax );
          }
       }
-   }
-   if ( N >= 3 )
-   {
-      // faces (P1ConstantOperator.cpp:372-534)
+   };
+   // faces (P1ConstantOperator.cpp:372-534)
+   auto faces = [&]() {
+      if ( N < 3 )
+         return;
 #pragma omp parallel for schedule( dynamic, 1 )
       for ( i64 f = 0; f < i64( o.F.size() ); ++f )
       {
@@ -585,28 +597,55 @@ void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, 
             }
             return mine ? x[d] : snap[d];
          };
-         for ( i64 i = 0; i < lv.nIntFace; ++i )
+         for ( i64 k = 0; k < lv.nIntFace; ++k )
          {
-            const i64 d = lv.offF + f * lv.nIntFace + i;
+            const i64 d = lv.offF + f * lv.nIntFace + ( backwards ? lv.nIntFace - 1 - k : k );
             T diag = 0, off = 0;
             fullRow( o, op, lv, d, val, diag, off );
             sorUpdate( x[d], b[d], diag, off, relax );
          }
       }
-   }
-   // cells (sor_3D_macrocell_P1.cpp:31-77): lexicographic, x fastest
-   auto cur = [x]( i64 d ) { return x[d]; };
+   };
+   // cells (sor_3D_macrocell_P1.cpp:31-77): lexicographic, x fastest; backwards from the
+   // last interior point
+   auto cells = [&]() {
+      auto cur = [x]( i64 d ) { return x[d]; };
 #pragma omp parallel for schedule( dynamic, 1 )
-   for ( i64 c = 0; c < i64( o.T.size() ); ++c )
-      for ( i64 z = 1; z <= N; ++z )
-         for ( i64 y = 1; y <= N - z; ++y )
-            for ( i64 xx = 1; xx <= N - y - z - 1; ++xx )
+      for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+         for ( i64 zk = 1; zk <= N; ++zk )
+         {
+            const i64 z = backwards ? N + 1 - zk : zk;
+            for ( i64 yk = 1; yk <= N - z; ++yk )
             {
-               const i64 d = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
-               T diag = 0, off = 0;
-               partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
-               sorUpdate( x[d], b[d], diag, off, relax );
+               const i64 y = backwards ? N - z + 1 - yk : yk;
+               for ( i64 xk = 1; xk <= N - y - z - 1; ++xk )
+               {
+                  const i64 xx = backwards ? N - y - z - xk : xk;
+                  const i64 d  = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
+                  T diag = 0, off = 0;
+                  partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
+                  sorUpdate( x[d], b[d], diag, off, relax );
+               }
             }
+         }
+   };
+   if ( !backwards )
+   {
+      vertices();
+      edges();
+      faces();
+      cells();
+   }
+   else
+   {
+      cells();
+      refresh();
+      faces();
+      refresh();
+      edges();
+      refresh();
+      vertices();
+   }
 }
 
 int dofColour( const Oracle& o, const Level& lv, i64 d, const int* labels, int m )
@@ -643,47 +682,69 @@ found:
    return int( ( ( s % m ) + m ) % m );
 }
 
+template < typename T >
+void surfaceColourPass( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag,
+                        const int* labels, int m, int col )
+{
+   auto cur = [x]( i64 d ) { return x[d]; };
+#pragma omp parallel for schedule( dynamic, 64 )
+   for ( i64 d = 0; d < lv.offC; ++d )
+   {
+      if ( !flagged( lv.bc[d], flag ) )
+         continue;
+      if ( dofColour( o, lv, d, labels, m ) != col )
+         continue;
+      T diag = 0, off = 0;
+      fullRow( o, op, lv, d, cur, diag, off );
+      sorUpdate( x[d], b[d], diag, off, relax );
+   }
+}
+
+template < typename T >
+void interiorColourPass( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int col )
+{
+   const i64 N = lv.N;
+   auto cur = [x]( i64 d ) { return x[d]; };
+#pragma omp parallel for schedule( dynamic, 1 )
+   for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+      for ( i64 z = 1; z <= N; ++z )
+         for ( i64 y = 1; y <= N - z; ++y )
+            for ( i64 xx = 1; xx <= N - y - z - 1; ++xx )
+            {
+               if ( ( xx + 2 * y + 3 * z ) % 4 != col )
+                  continue;
+               const i64 d = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
+               T diag = 0, off = 0;
+               partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
+               sorUpdate( x[d], b[d], diag, off, relax );
+            }
+}
+
 // Multicolour SOR, the ordering the GPU path uses. First the DoFs on macro-faces,
 // -edges and -vertices, by global colour colour(p) = sum_k label(V_k) b_k mod m over the
 // barycentric micro-coordinates (c = 0..m-1); then the macro-cell interiors by the local
 // colour (x + 2y + 3z) mod 4 (c = 0..3). Within one pass no two DoFs are coupled, so the
 // update order inside a pass is irrelevant.
+//
+// Backwards (the multicolour counterpart of smooth_sor_backwards): the same passes in
+// the reverse order, interior colours 3..0 first, then the surface colours m-1..0, so a
+// forward sweep followed by a backward one is a symmetric SOR step.
 template < typename T >
 void sorColoredT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag, const int* labels,
-                  int m )
+                  int m, bool backwards )
 {
-   const i64 N = lv.N;
-   auto cur = [x]( i64 d ) { return x[d]; };
+   if ( backwards )
+   {
+      for ( int col = 3; col >= 0; --col )
+         interiorColourPass( o, op, lv, x, b, relax, col );
+      for ( int col = m - 1; col >= 0; --col )
+         surfaceColourPass( o, op, lv, x, b, relax, flag, labels, m, col );
+      return;
+   }
    for ( int col = 0; col < m; ++col )
-   {
-#pragma omp parallel for schedule( dynamic, 64 )
-      for ( i64 d = 0; d < lv.offC; ++d )
-      {
-         if ( !flagged( lv.bc[d], flag ) )
-            continue;
-         if ( dofColour( o, lv, d, labels, m ) != col )
-            continue;
-         T diag = 0, off = 0;
-         fullRow( o, op, lv, d, cur, diag, off );
-         sorUpdate( x[d], b[d], diag, off, relax );
-      }
-   }
+      surfaceColourPass( o, op, lv, x, b, relax, flag, labels, m, col );
    for ( int col = 0; col < 4; ++col )
-   {
-#pragma omp parallel for schedule( dynamic, 1 )
-      for ( i64 c = 0; c < i64( o.T.size() ); ++c )
-         for ( i64 z = 1; z <= N; ++z )
-            for ( i64 y = 1; y <= N - z; ++y )
-               for ( i64 xx = 1; xx <= N - y - z - 1; ++xx )
-               {
-                  if ( ( xx + 2 * y + 3 * z ) % 4 != col )
-                     continue;
-                  const i64 d = lv.cellMap[c][cellIdx( N + 1, xx, y, z )];
-                  T diag = 0, off = 0;
-                  partialRow( o, op, lv, int( c ), xx, y, z, cur, diag, off );
-                  sorUpdate( x[d], b[d], diag, off, relax );
-               }
-   }
+      interiorColourPass( o, op, lv, x, b, relax, col );
 }
 
 // Weighted Jacobi (P1Operator.hpp smooth_jac / WeightedJacobiSmoother):
@@ -901,6 +962,7 @@ struct GmgCfg
    int         op, minL, maxL, pre, post, smoother, m;
    double      relax, coarseTol;
    const int*  labels;
+   int         cycleType; // 0 = V-cycle, 1 = W-cycle (GeometricMultigridSolver.hpp:201-204)
 };
 
 template < typename T >
@@ -909,12 +971,20 @@ void smoothT( const Oracle& o, const GmgCfg& g, int level, T* x, const T* b )
    const Op& op = o.ops[g.op];
    const Level& lv = o.lv[level];
    const int flag = ORC_INNER | ORC_NEUMANN;
-   if ( g.smoother == 0 )
-      sorRefT( o, op, lv, x, b, T( g.relax ), flag );
-   else if ( g.smoother == 1 )
-      sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m );
-   else
-      jacobiT( o, op, lv, x, b, T( g.relax ), flag );
+   switch ( g.smoother )
+   {
+   case 0: sorRefT( o, op, lv, x, b, T( g.relax ), flag, false ); break;
+   case 1: sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m, false ); break;
+   case 2: jacobiT( o, op, lv, x, b, T( g.relax ), flag ); break;
+   // SymmetricSORSmoother::solve (SymmetricSORSmoother.hpp:38-57): forward, then backwards
+   case 3:
+      sorRefT( o, op, lv, x, b, T( g.relax ), flag, false );
+      sorRefT( o, op, lv, x, b, T( g.relax ), flag, true );
+      break;
+   default:
+      sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m, false );
+      sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m, true );
+   }
 }
 
 template < typename T >
@@ -946,6 +1016,8 @@ void vcycleT( const Oracle& o, const GmgCfg& g, Hier< T >& h, int level )
          h.b[level - 1][d] = h.tmp[level - 1][d];
    std::fill( h.x[level - 1].begin(), h.x[level - 1].end(), T( 0 ) ); // x.interpolate(0, level-1) on All
    vcycleT( o, g, h, level - 1 );
+   if ( g.cycleType == 1 )
+      vcycleT( o, g, h, level - 1 );
    prolongateT( o, level - 1, h.x[level - 1].data(), h.x[level].data(), flag, true );
    for ( int i = 0; i < g.post; ++i )
       smoothT( o, g, level, h.x[level].data(), h.b[level].data() );
@@ -1115,17 +1187,17 @@ void orc_apply( void* h, int op, int level, const double* src, double* dst, int 
    applyT( *o, o->ops[op], o->lv[level], src, dst, flag, add != 0 );
 }
 
-void orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag )
+void orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag, int backwards )
 {
    auto* o = H( h );
-   sorRefT( *o, o->ops[op], o->lv[level], x, b, relax, flag );
+   sorRefT( *o, o->ops[op], o->lv[level], x, b, relax, flag, backwards != 0 );
 }
 
 void orc_sor_colored( void* h, int op, int level, double* x, const double* b, double relax, int flag, const int* labels,
-                      int m )
+                      int m, int backwards )
 {
    auto* o = H( h );
-   sorColoredT( *o, o->ops[op], o->lv[level], x, b, relax, flag, labels, m );
+   sorColoredT( *o, o->ops[op], o->lv[level], x, b, relax, flag, labels, m, backwards != 0 );
 }
 
 void orc_jacobi( void* h, int op, int level, double* x, const double* b, double relax, int flag )
@@ -1157,10 +1229,10 @@ int orc_cg( void* h, int op, int level, double* x, const double* b, double tol, 
 
 int orc_gmg_solve( void* h, int op, int minLevel, int maxLevel, double* x, const double* b, int pre, int post,
                    double relax, int smoother, const int* labels, int m, double coarseTol, int maxCycles, double relTol,
-                   int precision, double* history )
+                   int precision, double* history, int cycleType )
 {
    auto* o = H( h );
-   GmgCfg g{ op, minLevel, maxLevel, pre, post, smoother, m, relax, coarseTol, labels };
+   GmgCfg g{ op, minLevel, maxLevel, pre, post, smoother, m, relax, coarseTol, labels, cycleType };
    const Op& A = o->ops[op];
    const Level& lv = o->lv[maxLevel];
    const int flag  = ORC_INNER | ORC_NEUMANN;

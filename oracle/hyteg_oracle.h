@@ -46,9 +46,10 @@ int  orc_op_divkgrad( void* h, const double* const* nodalK );
 void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 );
 
 void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );
-void   orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag );
+// backwards != 0: smooth_sor_backwards (P1Operator.hpp:424-431)
+void   orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag, int backwards );
 void   orc_sor_colored( void* h, int op, int level, double* x, const double* b, double relax, int flag,
-                        const int* labels, int m );
+                        const int* labels, int m, int backwards );
 void   orc_jacobi( void* h, int op, int level, double* x, const double* b, double relax, int flag );
 void   orc_prolongate( void* h, int coarseLevel, const double* coarse, double* fine, int flag, int add );
 void   orc_restrict( void* h, int fineLevel, const double* fine, double* coarse, int flag );
@@ -56,13 +57,15 @@ double orc_dot( void* h, int level, const double* a, const double* b, int flag )
 int    orc_cg( void* h, int op, int level, double* x, const double* b, double tol, int maxIter );
 
 // V-cycle GMG (src/hyteg/solvers/GeometricMultigridSolver.hpp:127-235).
-// smoother: 0 = reference-order SOR, 1 = multicolour SOR (labels, m), 2 = weighted Jacobi.
+// smoother: 0 = reference-order SOR, 1 = multicolour SOR (labels, m), 2 = weighted Jacobi,
+// 3 = reference-order symmetric SOR, 4 = multicolour symmetric SOR (SymmetricSORSmoother).
+// cycleType: 0 = V-cycle, 1 = W-cycle.
 // precision: 64 = plain FP64 cycles; 32 = FP32 inner V-cycles inside FP64 iterative refinement.
 // Runs until ||b-Ax||/||b|| <= relTol (Inner|Neumann DoFs) or maxCycles; history[k] =
 // relative residual after cycle k (history[0] = initial). Returns cycles done.
 int orc_gmg_solve( void* h, int op, int minLevel, int maxLevel, double* x, const double* b, int pre, int post,
                    double relax, int smoother, const int* labels, int m, double coarseTol, int maxCycles,
-                   double relTol, int precision, double* history );
+                   double relTol, int precision, double* history, int cycleType );
 
 #ifdef __cplusplus
 }

@@ -53,8 +53,8 @@ def lib():
         L.orc_op_divkgrad.argtypes = [P, P]
         L.orc_cell_stencil.argtypes = [P, I, I, I, I, P]
         L.orc_apply.argtypes = [P, I, I, P, P, I, I]
-        L.orc_sor_ref.argtypes = [P, I, I, P, P, D, I]
-        L.orc_sor_colored.argtypes = [P, I, I, P, P, D, I, P, I]
+        L.orc_sor_ref.argtypes = [P, I, I, P, P, D, I, I]
+        L.orc_sor_colored.argtypes = [P, I, I, P, P, D, I, P, I, I]
         L.orc_jacobi.argtypes = [P, I, I, P, P, D, I]
         L.orc_prolongate.argtypes = [P, I, P, P, I, I]
         L.orc_restrict.argtypes = [P, I, P, P, I]
@@ -63,7 +63,7 @@ def lib():
         L.orc_cg.restype = I
         L.orc_cg.argtypes = [P, I, I, P, P, D, I]
         L.orc_gmg_solve.restype = I
-        L.orc_gmg_solve.argtypes = [P, I, I, I, P, P, I, I, D, I, P, I, D, I, D, I, P]
+        L.orc_gmg_solve.argtypes = [P, I, I, I, P, P, I, I, D, I, P, I, D, I, D, I, P, I]
         _lib = L
     return _lib
 
@@ -120,14 +120,15 @@ class Oracle:
         lib().orc_apply(self.h, op, level, _p(src), _p(dst), flag, int(add))
         return dst
 
-    def sor_ref(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0):
-        lib().orc_sor_ref(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), relax, flag)
+    def sor_ref(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0, backwards=False):
+        lib().orc_sor_ref(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), relax, flag,
+                          int(backwards))
         return x
 
-    def sor_colored(self, x, b, level, labels, m, relax=1.0, flag=INNER | NEUMANN, op=0):
+    def sor_colored(self, x, b, level, labels, m, relax=1.0, flag=INNER | NEUMANN, op=0, backwards=False):
         lab = np.ascontiguousarray(labels, dtype=np.int32)
         lib().orc_sor_colored(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), relax, flag,
-                              _p(lab), m)
+                              _p(lab), m, int(backwards))
         return x
 
     def jacobi(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0):
@@ -153,12 +154,14 @@ class Oracle:
         return int(lib().orc_cg(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), tol, max_iter))
 
     def gmg(self, x, b, min_level, max_level, pre=3, post=3, relax=1.0, smoother=0, labels=None, m=0,
-            coarse_tol=1e-12, max_cycles=10, rel_tol=0.0, precision=64, op=0):
+            coarse_tol=1e-12, max_cycles=10, rel_tol=0.0, precision=64, op=0, cycle="V"):
+        """smoother: 0 reference-order SOR, 1 multicolour SOR, 2 weighted Jacobi, 3 and 4 their
+        symmetric SOR counterparts (forward then backwards); cycle "V" or "W"."""
         hist = np.zeros(max_cycles + 1)
         lab = np.ascontiguousarray(labels if labels is not None else np.zeros(1), dtype=np.int32)
         cyc = lib().orc_gmg_solve(self.h, op, min_level, max_level, _p(x), _p(np.ascontiguousarray(b, np.float64)),
                                   pre, post, relax, smoother, _p(lab), m, coarse_tol, max_cycles, rel_tol, precision,
-                                  _p(hist))
+                                  _p(hist), {"V": 0, "W": 1}[cycle])
         return x, hist[: cyc + 1]
 
 

@@ -404,3 +404,133 @@ def test_full_multigrid_start(H, oracle_mod, setups):
     assert r_fmg < h0[1], (r_fmg, h0[:3])
     h1 = gmg.solve_to_tolerance(x1, b1, L, 1e-8, max_cycles=60, precision=32)
     assert h1[-1] <= 1e-8 and len(h1) <= len(h0), (h1, h0)
+
+
+@pytest.mark.parametrize("name", ["pyramid_4el", "regular_octahedron_8el", "cube_6el"])
+def test_gmsh_storage_apply_and_vcycle_match_oracle(H, oracle_mod, tmp_path, write_gmsh, name):
+    """MeshInfo::fromGmshFile: a reference test mesh written as a Gmsh 2.2 file (shuffled
+    node ids and element order) loads into the same storage as the mesh given directly, and
+    the constant apply and one V-cycle on it match the oracle."""
+    O = oracle_mod
+    g = np.load(os.path.join(GOLD, "reference_meshes.npz"))
+    c, t = g[name + "_coords"], g[name + "_tets"]
+    path = tmp_path / (name + ".msh")
+    write_gmsh(path, c, t, seed=3)
+    L = 4
+    st = H.PrimitiveStorage.from_gmsh(str(path), L)
+    orc = O.Oracle(c, t, L)
+    assert st.num_dofs(L) == orc.n(L)
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, orc.n(L))
+    src, dst = H.P1Function("s", st, 0, L), H.P1Function("d", st, 0, L)
+    src.set(x, L)
+    A.apply(src, dst, L, 1 | 4, 0)
+    close(dst.get(L), orc.apply(x, L, 1 | 4))
+    m, labels = st.colouring()
+    b = O.uniform_rhs(orc.coords_of(L), 0, 1 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fx.set(np.zeros(orc.n(L)), L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, coarse_tol=1e-14)
+    gmg.solve(fx, fb, L)
+    xr = np.zeros(orc.n(L))
+    orc.gmg(xr, b, 0, L, pre=3, post=3, relax=1.0, smoother=1, labels=labels, m=m, coarse_tol=1e-14, max_cycles=1)
+    close(fx.get(L), xr, 1e-10)
+
+
+@pytest.mark.parametrize("name", MESHES)
+@pytest.mark.parametrize("relax", [1.0, 1.3])
+def test_backward_and_symmetric_sor_match_oracle(H, oracle_mod, setups, name, relax):
+    """smooth_sor_backwards (the passes of a forward sweep in reverse order) and the
+    symmetric step (forward, then backwards) against the oracle's multicolour sweeps."""
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    m, labels = st.colouring()
+    rng = np.random.default_rng(6)
+    for level in range(1, L + 1):
+        x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+        fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+        fx.set(x, level)
+        fb.set(b, level)
+        A.smooth_sor_backwards(fx, fb, relax, level, 1 | 4)
+        orc.sor_colored(x, b, level, labels, m, relax=relax, flag=1 | 4, backwards=True)
+        close(fx.get(level), x, 1e-11)
+        A.smooth_sor(fx, fb, relax, level, 1 | 4)
+        A.smooth_sor_backwards(fx, fb, relax, level, 1 | 4)
+        orc.sor_colored(x, b, level, labels, m, relax=relax, flag=1 | 4)
+        orc.sor_colored(x, b, level, labels, m, relax=relax, flag=1 | 4, backwards=True)
+        close(fx.get(level), x, 1e-11)
+
+
+def test_backward_sor_variable_coefficient_and_fp32(H, oracle_mod, setups):
+    """The backward sweep with the elementwise div-k-grad operator (FP64, against the
+    oracle) and in FP32 (against the FP64 oracle, FP32 rounding)."""
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    m, labels = st.colouring()
+    k = [O.grf_coefficient(orc.coords_of(l), seed=3) for l in range(L + 1)]
+    A = H.P1ElementwiseDivKGradOperator(st, 0, L, k)
+    op = orc.op_divkgrad(k)
+    rng = np.random.default_rng(7)
+    level = L
+    x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fx.set(x, level)
+    fb.set(b, level)
+    A.smooth_sor_backwards(fx, fb, 1.0, level, 1 | 4)
+    xr = orc.sor_colored(x.copy(), b, level, labels, m, relax=1.0, flag=1 | 4, op=op, backwards=True)
+    close(fx.get(level), xr, 1e-11)
+    L32 = H.P1ConstantLaplaceOperator(st, 0, L)
+    gx, gb = H.P1Function("x", st, 0, L, dtype=H.F32), H.P1Function("b", st, 0, L, dtype=H.F32)
+    gx.set(x, level)
+    gb.set(b, level)
+    L32.smooth_sor_backwards(gx, gb, 1.0, level, 1 | 4)
+    xr = orc.sor_colored(x.copy(), b, level, labels, m, relax=1.0, flag=1 | 4, backwards=True)
+    close(gx.get(level), xr, 1e-5)
+
+
+@pytest.mark.parametrize("name", ["octahedron", "cube1", "cube211"])
+@pytest.mark.parametrize("smoother,cycle", [(2, "V"), (0, "W"), (2, "W")])
+def test_symmetric_sor_and_w_cycles_match_oracle(H, oracle_mod, setups, name, smoother, cycle):
+    """Cycles with SymmetricSORSmoother (smoother 2) and/or W-cycles == the oracle's cycles
+    with the same multicolour sweeps (oracle smoother 4 = multicolour symmetric SOR)."""
+    O = oracle_mod
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    m, labels = st.colouring()
+    b = O.uniform_rhs(orc.coords_of(L), 0, 1 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fx.set(np.zeros(orc.n(L)), L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, smoother=smoother, coarse_tol=1e-14,
+                                     cycle_type=H.CYCLE_W if cycle == "W" else H.CYCLE_V)
+    x = np.zeros(orc.n(L))
+    for _ in range(2):
+        gmg.solve(fx, fb, L)
+        fb.set(b, L)
+        orc.gmg(x, b, 0, L, pre=2, post=2, relax=1.0, smoother=4 if smoother == 2 else 1, labels=labels, m=m,
+                coarse_tol=1e-14, max_cycles=1, cycle=cycle)
+        close(fx.get(L), x, 1e-10)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_w_cycle_symmetric_sor_to_tolerance(H, oracle_mod, setups, precision):
+    """W-cycles with symmetric SOR reach 1e-8 in no more cycles than V-cycles with SOR, and
+    the solution matches the oracle's FP64 solve."""
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    b = O.uniform_rhs(orc.coords_of(L), 0, 1 << L)
+    hists = {}
+    for smoother, cyc in ((0, H.CYCLE_V), (2, H.CYCLE_W)):
+        fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+        fb.set(b, L)
+        gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, smoother=smoother, cycle_type=cyc)
+        hists[smoother] = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=30, precision=precision)
+        assert hists[smoother][-1] <= 1e-8
+    assert len(hists[2]) <= len(hists[0])
+    x = np.zeros(orc.n(L))
+    orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=60, rel_tol=1e-13)
+    err = np.abs(fx.get(L) - x).max() / np.abs(x).max()
+    assert err < 1e-6, err

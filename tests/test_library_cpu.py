@@ -235,3 +235,79 @@ def test_spherical_shell_mesh(tmp_path, ntan, nrad):
     assert vmin > 0
     exact = 4.0 / 3.0 * np.pi * (1.0 - 0.55 ** 3)
     assert 0.5 * exact < vtot < exact
+
+
+GMSH_CHECK = r"""
+#include "topology.hpp"
+#include <cstdio>
+#include <stdexcept>
+using namespace hyb;
+int main( int argc, char** argv )
+{
+   std::vector< std::array< double, 3 > > V;
+   std::vector< std::array< int, 4 > >    T;
+   try
+   {
+      readGmsh( argv[1], V, T );
+   } catch ( const std::exception& e )
+   {
+      printf( "error %s\n", e.what() );
+      return 0;
+   }
+   printf( "%zu %zu\n", V.size(), T.size() );
+   for ( auto& v : V )
+      printf( "%.17g %.17g %.17g\n", v[0], v[1], v[2] );
+   for ( auto& t : T )
+      printf( "%d %d %d %d\n", t[0], t[1], t[2], t[3] );
+   return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def gmsh_exe(tmp_path_factory):
+    d = tmp_path_factory.mktemp("gmsh")
+    src = d / "gmsh_check.cpp"
+    src.write_text(GMSH_CHECK)
+    exe = d / "gmsh_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(PKG, "csrc"), str(src),
+                    os.path.join(PKG, "csrc", "topology.cpp"), "-o", str(exe)], check=True)
+    return str(exe)
+
+
+@pytest.mark.parametrize("name", ["tet_1el", "pyramid_4el", "regular_octahedron_8el", "cube_6el"])
+def test_gmsh_reader_matches_reference_order(tmp_path, gmsh_exe, write_gmsh, name):
+    """readGmsh (MeshInfo::fromGmshFile): vertices in file-id order, tetrahedra in the
+    lexicographic order of their vertex lists, whatever the order in the file. The golden
+    arrays are the reference's meshes in exactly that order; here the vertices of each
+    tetrahedron are permuted in the file, so the check is on the sorted lists."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "reference_meshes.npz"))
+    coords, tets = g[name + "_coords"], g[name + "_tets"]
+    path = tmp_path / (name + ".msh")
+    write_gmsh(path, coords, tets, seed=len(tets), permute_cells=True)
+    out = subprocess.run([gmsh_exe, str(path)], capture_output=True, text=True, check=True).stdout.split("\n")
+    nv, nt = map(int, out[0].split())
+    assert (nv, nt) == (len(coords), len(tets))
+    V = np.array([list(map(float, l.split())) for l in out[1:1 + nv]])
+    T = np.array([list(map(int, l.split())) for l in out[1 + nv:1 + nv + nt]])
+    assert np.array_equal(V, coords)
+    want = sorted(tuple(sorted(t)) for t in tets)
+    assert sorted(tuple(sorted(t)) for t in T) == want
+    assert [tuple(t) for t in T] == sorted(tuple(t) for t in T)
+
+
+def test_gmsh_reader_rejects_unsupported_files(tmp_path, gmsh_exe):
+    """The reference reader accepts only format 2.2 ASCII and element types 1, 2, 4, 15."""
+    cases = {
+        "v4.msh": "$MeshFormat\n4.1 0 8\n$EndMeshFormat\n",
+        "binary.msh": "$MeshFormat\n2.2 1 8\n$EndMeshFormat\n",
+        "hex.msh": "$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n4\n1 0 0 0\n2 1 0 0\n3 0 1 0\n4 0 0 1\n"
+                   "$EndNodes\n$Elements\n1\n1 5 0 1 2 3 4 1 2 3 4\n$EndElements\n",
+        "unknown_node.msh": "$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n4\n1 0 0 0\n2 1 0 0\n3 0 1 0\n"
+                            "4 0 0 1\n$EndNodes\n$Elements\n1\n1 4 0 1 2 3 9\n$EndElements\n",
+    }
+    for fname, text in cases.items():
+        p = tmp_path / fname
+        p.write_text(text)
+        out = subprocess.run([gmsh_exe, str(p)], capture_output=True, text=True, check=True).stdout
+        assert out.startswith("error"), (fname, out)

@@ -54,10 +54,12 @@ def test_cell_apply_matches_generated_kernel(oracle_mod):
             assert abs(y[cm[i]] - g[key][i]) <= 1e-13 * (1 + abs(g[key][i]))
 
 
+@pytest.mark.parametrize("backwards", [False, True])
 @pytest.mark.parametrize("relax", [1.0, 0.8])
-def test_cell_sor_matches_generated_kernel(oracle_mod, relax):
+def test_cell_sor_matches_generated_kernel(oracle_mod, relax, backwards):
     """Single macro-tet: every face/edge/vertex is Dirichlet, so the reference-order SOR
-    reduces to the generated lexicographic cell sweep."""
+    reduces to the generated lexicographic cell sweep (sor_3D_macrocell_P1.cpp, and
+    sor_3D_macrocell_P1_backwards.cpp for the backward sweep)."""
     O = oracle_mod
     g = np.load(os.path.join(GOLD, "cell_kernels_L4.npz"))
     s = np.load(os.path.join(GOLD, "stencils_cube1.npz"))
@@ -70,8 +72,8 @@ def test_cell_sor_matches_generated_kernel(oracle_mod, relax):
     b = np.zeros(o.n(L))
     x[cm] = g["src"]
     b[cm] = g["rhs"]
-    o.sor_ref(x, b, L, relax=relax, flag=O.INNER)
-    ref = g[f"sor_relax{relax}_bw0"]
+    o.sor_ref(x, b, L, relax=relax, flag=O.INNER, backwards=backwards)
+    ref = g[f"sor_relax{relax}_bw{int(backwards)}"]
     got = x[cm]
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-13)
 
@@ -173,3 +175,61 @@ def test_gmg_convergence_rate_reference_order_sor(oracle_mod):
     _, hist = o.gmg(x, b, 0, 3, pre=3, post=3, relax=1.0, smoother=0, max_cycles=4)
     ratios = (hist[1:] / hist[:-1]) ** 2
     assert np.all(ratios < 3.2e-2), ratios
+
+
+def test_symmetric_multicolour_sor_is_a_symmetric_operator(oracle_mod):
+    """A forward multicolour sweep followed by the backward one (the passes in reverse
+    order) from a zero start is b -> M^-1 b with M symmetric (symmetric SOR), because the
+    stiffness matrix is symmetric: <S b1, b2> == <b1, S b2> over the inner DoFs."""
+    O = oracle_mod
+    c, t = O.mesh_cuboid(2, 1, 1, hi=(2.0, 1.0, 1.0))
+    L = 3
+    o = O.Oracle(c, t, L)
+    kind, bc = o.info(L)
+    inner = bc == O.INNER
+    labels, m = np.arange(len(c)), len(c)  # distinct vertex labels: a valid multicolouring
+    rng = np.random.default_rng(5)
+    for relax in (1.0, 1.3):
+        S = []
+        bs = []
+        for _ in range(2):
+            b = rng.uniform(-1, 1, o.n(L)) * inner
+            x = np.zeros(o.n(L))
+            o.sor_colored(x, b, L, labels, m, relax=relax)
+            o.sor_colored(x, b, L, labels, m, relax=relax, backwards=True)
+            S.append(x)
+            bs.append(b)
+        lhs, rhs = S[0] @ bs[1], bs[0] @ S[1]
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (relax, lhs, rhs)
+        # the forward sweep alone is not symmetric
+        x0, x1 = np.zeros(o.n(L)), np.zeros(o.n(L))
+        o.sor_colored(x0, bs[0], L, labels, m, relax=relax)
+        o.sor_colored(x1, bs[1], L, labels, m, relax=relax)
+        assert abs(x0 @ bs[1] - bs[0] @ x1) > 1e-8 * abs(x0 @ bs[1])
+
+
+@pytest.mark.parametrize("smoother", [3, 4])
+@pytest.mark.parametrize("cycle", ["V", "W"])
+def test_gmg_convergence_symmetric_sor_and_w_cycles(oracle_mod, smoother, cycle):
+    """P1GMG3DConvergenceTest.cpp's setting (regular_octahedron_8el, levels 0..3, V(3,3)) with
+    SymmetricSORSmoother, as V- and W-cycles: every cycle must beat the reference test's
+    bound 3.2e-2 on the squared residual ratio, and the W-cycle must not converge slower
+    than the V-cycle."""
+    O = oracle_mod
+    g = np.load(os.path.join(GOLD, "reference_meshes.npz"))
+    c, t = g["regular_octahedron_8el_coords"], g["regular_octahedron_8el_tets"]
+    o = O.Oracle(c, t, 3)
+    labels, m = np.arange(len(c)), len(c)  # distinct vertex labels: a valid multicolouring
+    xyz = o.coords_of(3)
+    kind, bc = o.info(3)
+    x0 = np.random.default_rng(0).uniform(0, 1, o.n(3))
+    exact = np.sin(xyz[:, 0]) * np.sinh(xyz[:, 1]) * xyz[:, 2]
+    x0[bc == O.DIRICHLET] = exact[bc == O.DIRICHLET]
+    b = np.zeros(o.n(3))
+    rates = {}
+    for cyc in ("V", cycle):
+        _, hist = o.gmg(x0.copy(), b, 0, 3, pre=3, post=3, relax=1.0, smoother=smoother, labels=labels, m=m,
+                        max_cycles=4, cycle=cyc)
+        rates[cyc] = (hist[1:] / hist[:-1]) ** 2
+        assert np.all(rates[cyc] < 3.2e-2), (cyc, rates[cyc])
+    assert rates[cycle].max() <= rates["V"].max() * (1 + 1e-9)
