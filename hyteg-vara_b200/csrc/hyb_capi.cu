@@ -115,9 +115,21 @@ inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s );
 // ---------------------------------------------------------------------------
 // Storage
 // ---------------------------------------------------------------------------
+// Row tables of a small level (SlabRow, constant operator): the surface lanes of each SOR
+// colour, the interior points of each interior colour (cell-major), and all DoFs (the
+// surface lanes of the full lists, then every interior point) for residuals and CG.
+struct RowTables
+{
+   DevBuf< SlabRow >   iface, interior, all;
+   std::vector< long > ifaceOff; // per surface colour: first row
+   long                allN = 0, allB1 = 0, allB2 = 0, allB3 = 0;
+};
+
 struct LevelHost
 {
    LevelDev           dev{};
+   std::unique_ptr< RowTables > rows; // built on first use (ensureRows)
+   bool                         rowsTried = false;
    DevBuf< int32_t >  seg, xyz, blk, blkXYZ, pts, ptsC, quads, rowYZ;
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
    std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
@@ -988,6 +1000,103 @@ struct CgScratch
    DevBuf< int >               status;
 };
 
+// Levels whose closure slabs hold at most this many points (all cells) get row tables;
+// HYB_ROW_TABLE_MAX_POINTS overrides it (0: none).
+constexpr long kRowTableMaxPoints = 20000;
+
+long rowTableMaxPoints()
+{
+   static const long v = [] {
+      const char* e = std::getenv( "HYB_ROW_TABLE_MAX_POINTS" );
+      return e ? std::atol( e ) : kRowTableMaxPoints;
+   }();
+   return v;
+}
+
+// The row tables of level l, built on first use (not inside a stream capture); nullptr if
+// the level is too large, or if a DoF has more embeddings than its lane group (then the
+// passes keep the lane-group path).
+const RowTables* ensureRows( Storage& s, int l )
+{
+   LevelHost& L = *s.lv[size_t( l )];
+   if ( L.rowsTried )
+      return L.rows.get();
+   L.rowsTried = true;
+   const LevelDev& d = L.dev;
+   if ( long( s.td.nC ) * d.stride > rowTableMaxPoints() || d.stride >= 65536 )
+      return nullptr;
+   auto             R = std::make_unique< RowTables >();
+   DevBuf< int >    err;
+   err.alloc( 1 );
+   HYB_CUDA( cudaMemset( err.p, 0, sizeof( int ) ) );
+   auto grid = [&]( long n ) { return dim3( unsigned( std::max< long >( 1, std::min< long >( ( n + 255 ) / 256, 4096 ) ) ) ); };
+   // surface colours
+   long total = 0;
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      R->ifaceOff.push_back( total );
+      const int* co = &L.colourOff[4 * c];
+      total += bdryLaneCount( co[1], co[2], co[3] );
+   }
+   R->iface.alloc( size_t( std::max< long >( total, 1 ) ) );
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      const int* co    = &L.colourOff[4 * c];
+      const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+      if ( lanes == 0 )
+         continue;
+      const int32_t*  list = L.colourList.p + co[0];
+      const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+      k_rows_surface<<< grid( lanes ), 256 >>>( s.td, d, bl, lanes, R->iface.p + R->ifaceOff[size_t( c )], err.p );
+      HYB_CHECK_LAUNCH();
+   }
+   // interior colours
+   const long nInt = long( s.td.nC ) * d.nPts;
+   R->interior.alloc( size_t( std::max< long >( nInt, 1 ) ) );
+   for ( int c = 0; c < kInteriorColours; ++c )
+   {
+      const int count = d.ptsOff[c + 1] - d.ptsOff[c];
+      if ( count == 0 )
+         continue;
+      k_rows_interior<<< grid( long( s.td.nC ) * count ), 256 >>>( s.td, d, d.ptsC + d.ptsOff[c], count,
+                                                                  R->interior.p + long( s.td.nC ) * d.ptsOff[c] );
+      HYB_CHECK_LAUNCH();
+   }
+   // all DoFs
+   const int       nv = s.td.nV, ne = s.td.nE * ( d.N - 1 ), nf = s.td.nF * d.nIntFace;
+   const BdryLists full{ nullptr, nullptr, nullptr, nv, ne, nf };
+   const long      surf = bdryLaneCount( nv, ne, nf );
+   R->allB1             = long( nv ) * 32;
+   R->allB2             = R->allB1 + ( long( ne ) * 8 + 31 ) / 32 * 32;
+   R->allB3             = surf;
+   R->allN              = surf + nInt;
+   R->all.alloc( size_t( std::max< long >( R->allN, 1 ) ) );
+   if ( surf > 0 )
+   {
+      k_rows_surface<<< grid( surf ), 256 >>>( s.td, d, full, surf, R->all.p, err.p );
+      HYB_CHECK_LAUNCH();
+   }
+   if ( nInt > 0 )
+   {
+      k_rows_interior<<< grid( nInt ), 256 >>>( s.td, d, d.pts, d.nPts, R->all.p + surf );
+      HYB_CHECK_LAUNCH();
+   }
+   int bad = 0;
+   HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
+   if ( bad )
+      return nullptr;
+   L.rows = std::move( R );
+   return L.rows.get();
+}
+
+// the row table of level l if it has been built (usable inside a capture)
+const RowTables* rowsIf( const Storage& s, int l ) { return s.lv[size_t( l )]->rows.get(); }
+
+RowPass rowPassAll( const RowTables* R )
+{
+   return R ? RowPass{ R->all.p, R->allN, R->allB1, R->allB2, R->allB3 } : RowPass{ nullptr, 0, 0, 0, 0 };
+}
+
 void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch& cs, double tol, int maxIter,
                cudaStream_t stream )
 {
@@ -1000,12 +1109,13 @@ void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch&
       cs.status.alloc( 4 );
    }
    const OpDev< double > od = op.dev< double >( l );
+   const RowPass         rp = op.variable ? RowPass{ nullptr, 0, 0, 0, 0 } : rowPassAll( rowsIf( s, l ) );
    if ( op.variable )
       pdlLaunch( k_cg< true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
-                                             cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p );
+                                             cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
    else
       pdlLaunch( k_cg< false >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
-                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p );
+                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
    HYB_CHECK_LAUNCH();
 }
 
@@ -1126,6 +1236,8 @@ struct PhaseList
       return ph.back();
    }
    long slabElems( int l ) const { return long( g.st->td.nC ) * g.st->L( l ).dev.stride; }
+   // the row table of level l for the passes of this (constant) operator, built on first use
+   const RowTables* rows( int l ) const { return g.op->variable ? nullptr : ensureRows( *g.st, l ); }
    int  flatBlocks( long n ) const
    {
       return int( std::min< long >( ( n + 127 ) / 128, long( g.st->numSMs ) * 8 ) );
@@ -1150,6 +1262,13 @@ struct PhaseList
             P.relax             = g.relax;
             P.flag              = kGmgFlag;
             P.bl                = BdryLists{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+            if ( const RowTables* R = rows( l ) )
+            {
+               const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
+               P.rp          = RowPass{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes };
+               P.blocks      = 1;
+               P.cellBlocks  = 0;
+            }
          };
          auto interior = [&]( int c ) {
             const int count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
@@ -1162,6 +1281,13 @@ struct PhaseList
             P.a0     = c;
             P.a1     = L.dev.ptsOff[c];
             P.a2     = count;
+            if ( const RowTables* R = rows( l ) )
+            {
+               const long n = long( s.td.nC ) * count;
+               P.rp         = RowPass{ R->interior.p + long( s.td.nC ) * L.dev.ptsOff[c], n, 0, 0, 0 };
+               P.blocks     = 1;
+               P.cellBlocks = 0;
+            }
          };
          for ( int c = 0; c < s.td.m; ++c )
             iface( c );
@@ -1202,6 +1328,7 @@ struct PhaseList
       P.status = g.cg.status.p;
       P.relax  = g.coarseTol;
       P.a0     = g.coarseMaxIter;
+      P.rp     = rowPassAll( rows( l ) );
    }
 
    void coarse( double* x, const double* b ) { cg( g.minL, x, b ); }
@@ -1243,6 +1370,12 @@ struct PhaseList
          P.p1           = tmp.ptr< T >( l );
          P.p2           = b.ptr< T >( l );
          P.flag         = kGmgFlag;
+         if ( const RowTables* R = rows( l ) )
+         {
+            P.rp         = rowPassAll( R );
+            P.blocks     = 1;
+            P.cellBlocks = 0;
+         }
       }
       {
          const auto& C  = s.L( l - 1 );
@@ -1386,6 +1519,8 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
 // everything a captured graph needs is allocated before capture begins
 void prepare( Gmg& g )
 {
+   if ( !g.op->variable )
+      ensureRows( *g.st, g.minL );
    if ( !g.cg.r )
    {
       g.cg.r.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );

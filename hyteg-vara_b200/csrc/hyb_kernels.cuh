@@ -401,6 +401,159 @@ struct PointBatch
    }
 };
 
+// ---------------------------------------------------------------------------
+// Row tables of small levels (constant operator). On coarse levels a pass has little
+// work, and its time is the length of one lane's dependent chain: the DoF from the list,
+// its embedding, class and stencil positions, then the loads. A row table stores the end
+// of that chain per lane -- the cell, the partial-stencil class, the DoF's boundary flag
+// and the slab positions of the 15 neighbours -- so a pass reads one row (three 16-byte
+// loads), gathers, and sums the group as before.
+// ---------------------------------------------------------------------------
+struct SlabRow
+{
+   int32_t  base;    // cell * stride; -1: no row (padding lane)
+   int32_t  wsel;    // (cell * 16 + class) * 15: the partial stencil of the row
+   uint16_t valid;   // neighbour mask of the class
+   uint8_t  bc;      // boundary flag of the DoF
+   uint8_t  pad0;
+   uint16_t pos[15]; // slab positions of the neighbours within the cell, pos[0] = the point
+   uint16_t pad1[3];
+};
+static_assert( sizeof( SlabRow ) == 48, "three 16-byte loads per row" );
+
+__device__ __forceinline__ SlabRow noRow()
+{
+   SlabRow R{};
+   R.base = -1;
+   return R;
+}
+
+__device__ __forceinline__ SlabRow makeRow( const LevelDev& lv, int c, int x, int y, int z, uint8_t bc )
+{
+   SlabRow           R{};
+   const int         mask  = classMask( lv.N, x, y, z );
+   const uint32_t    valid = kValidOffsets[mask];
+   const StencilRows S     = stencilRows( lv.W, y, z );
+   const int         self  = S.start[offRow( 0 )] + resOff( x & 3, S.len[offRow( 0 )] ) + ( x >> 2 );
+   for ( int q = 0; q < 15; ++q )
+   {
+      const int xq = x + offX( q ), k = offRow( q );
+      R.pos[q]     = uint16_t( ( valid & ( 1u << q ) ) ? S.start[k] + resOff( xq & 3, S.len[k] ) + ( xq >> 2 ) : self );
+   }
+   R.base  = c * lv.stride;
+   R.wsel  = ( c * 16 + mask ) * 15;
+   R.valid = uint16_t( valid );
+   R.bc    = bc;
+   return R;
+}
+
+// one row per lane of the surface lists bl, in the lane order of HYB_BDRY_LANES; *err is
+// set when a lane's DoF has more embeddings than its group has lanes
+__global__ void k_rows_surface( TopoDev tp, LevelDev lv, BdryLists bl, long n, SlabRow* out, int* err )
+{
+   for ( long gt = long( blockIdx.x ) * blockDim.x + threadIdx.x; gt < n; gt += long( gridDim.x ) * blockDim.x )
+   {
+      SlabRow        R  = noRow();
+      const LaneTask tk = laneTask( tp, lv, bl, gt );
+      if ( tk.valid )
+      {
+         const BdryPoint p  = decodeBdry( tp, lv, tk.t );
+         const int       ne = numEmb( tp, p.kind, p.prim );
+         if ( tk.sub + tk.G < ne )
+            atomicExch( err, 1 );
+         if ( tk.sub < ne )
+         {
+            int c, x, y, z;
+            embeddingCoords( embAt( tp, p.kind, p.prim, tk.sub ), p.kind, lv.N, p.i, p.j, c, x, y, z );
+            R = makeRow( lv, c, x, y, z, primBc( tp, p.kind, p.prim ) );
+         }
+      }
+      out[gt] = R;
+   }
+}
+
+// one row per (cell, entry) of an interior point list, cell-major; interior points are Inner
+__global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, int nList, SlabRow* out )
+{
+   const long n = long( tp.nC ) * nList;
+   for ( long t = long( blockIdx.x ) * blockDim.x + threadIdx.x; t < n; t += long( gridDim.x ) * blockDim.x )
+   {
+      const int     cell = int( t / nList );
+      const int32_t e    = list[t - long( cell ) * nList];
+      const int     g    = e & 255;
+      const NbrOff  no   = blockNbr( lv.blk, e >> 8 );
+      SlabRow       R{};
+      R.base  = cell * lv.stride;
+      R.wsel  = cell * 16 * 15;
+      R.valid = 0x7fff;
+      R.bc    = 1; // Inner
+      for ( int q = 0; q < 15; ++q )
+         R.pos[q] = uint16_t( no.d[q] + g );
+      out[t] = R;
+   }
+}
+
+// the rows of a pass: lanes [0, b1) in groups of 32, [b1, b2) of 8, [b2, b3) of 2, the rest
+// single (b1, b2, b3 are multiples of 32, so a warp has one group size)
+struct RowPass
+{
+   const SlabRow* rows;
+   long long      n, b1, b2, b3;
+};
+
+enum RowMode : int
+{
+   kRowSor      = 0, // u = (1 - relax) u + relax (b - off) / diag
+   kRowResidual = 1, // r = b - A u
+   kRowApply    = 2  // r = A u
+};
+
+// one pass over the rows with the block's threads (the rows of one DoF are adjacent lanes)
+template < typename T, int MODE >
+__device__ __forceinline__ void rowPassBody( const RowPass& rp, const T* __restrict__ st, T* u, const T* b, T* r, T relax,
+                                             int flag )
+{
+   for ( long long gt = threadIdx.x; gt - ( threadIdx.x & 31 ) < rp.n; gt += blockDim.x )
+   {
+      int4 A = make_int4( -1, 0, 0, 0 ), B = make_int4( 0, 0, 0, 0 ), C = make_int4( 0, 0, 0, 0 );
+      if ( gt < rp.n )
+      {
+         const int4* p = reinterpret_cast< const int4* >( rp.rows + gt );
+         A             = __ldg( p );
+         B             = __ldg( p + 1 );
+         C             = __ldg( p + 2 );
+      }
+      const bool active = A.x >= 0 && ( ( A.z >> 16 ) & flag );
+      T          diag = 0, off = 0;
+      if ( active )
+      {
+         const T*       uc    = u + A.x;
+         const T*       w     = st + A.y;
+         const uint32_t valid = uint32_t( A.z ) & 0xffffu;
+         // pos[q] of the row: 16-bit halves of A.w, B.xyzw, C.xyz
+         const uint32_t h[8] = { uint32_t( A.w ), uint32_t( B.x ), uint32_t( B.y ), uint32_t( B.z ),
+                                 uint32_t( B.w ), uint32_t( C.x ), uint32_t( C.y ), uint32_t( C.z ) };
+         diag += w[0];
+#pragma unroll
+         for ( int q = 1; q < 15; ++q )
+            if ( valid & ( 1u << q ) )
+               off += w[q] * uc[( q & 1 ) ? ( h[q >> 1] >> 16 ) : ( h[q >> 1] & 0xffffu )];
+      }
+      const int G = gt < rp.b1 ? 32 : gt < rp.b2 ? 8 : gt < rp.b3 ? 2 : 1;
+      diag        = groupSum( diag, G );
+      off         = groupSum( off, G );
+      if ( !active )
+         continue;
+      const size_t i = size_t( A.x ) + ( uint32_t( A.w ) & 0xffffu );
+      if constexpr ( MODE == kRowSor )
+         u[i] = ( T( 1 ) - relax ) * u[i] + relax * ( b[i] - off ) / diag;
+      else if constexpr ( MODE == kRowResidual )
+         r[i] = b[i] - ( diag * u[i] + off );
+      else
+         r[i] = diag * u[i] + off;
+   }
+}
+
 // Constant-stencil quad: the points x = 4g + r, r = 0..3, of row (y, z). Each of the seven
 // rows the stencil touches is read once for the four points: rows whose offsets have dx in
 // {-1, 0} need x' = 4g-1 .. 4g+3, rows with dx in {0, +1} need 4g .. 4g+4, the centre row
@@ -1264,10 +1417,18 @@ __device__ void cgAxpby( const TopoDev& tp, const LevelDev& lv, double a, const 
 // the whole CG in the calling thread block; red = 32 doubles of shared memory
 template < bool VAR >
 __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< double >& op, double* x, const double* b,
-                        double* r, double* p, double* ap, double tol, int maxIter, int* status, double* red )
+                        double* r, double* p, double* ap, double tol, int maxIter, int* status, double* red,
+                        const RowPass& rp )
 {
    const int flag = 1 | 4 | 8;
-   cgApplyAll< VAR >( tp, lv, op, x, p, flag );
+   // the operator through the level's row table when there is one
+   auto applyA = [&]( const double* src, double* dst ) {
+      if ( rp.rows )
+         rowPassBody< double, kRowApply >( rp, op.st, const_cast< double* >( src ), nullptr, dst, 0.0, flag );
+      else
+         cgApplyAll< VAR >( tp, lv, op, src, dst, flag );
+   };
+   applyA( x, p );
    __syncthreads();
    // r = b - A x ; p = r
    for ( int t = threadIdx.x; t < tp.nC * lv.S; t += blockDim.x )
@@ -1286,7 +1447,7 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
    int    conv   = sqrt( prsold ) < tol ? 1 : 0;
    while ( !conv && it < maxIter )
    {
-      cgApplyAll< VAR >( tp, lv, op, p, ap, flag );
+      applyA( p, ap );
       __syncthreads();
       const double pAp   = cgDot( tp, lv, p, ap, flag, red );
       const double alpha = prsold / pAp;
@@ -1314,11 +1475,12 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
 
 template < bool VAR >
 __global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
-                                                double* r, double* p, double* ap, double tol, int maxIter, int* status )
+                                                double* r, double* p, double* ap, double tol, int maxIter, int* status,
+                                                RowPass rp )
 {
    HYB_PDL_PROLOGUE();
    __shared__ double red[32];
-   cgBody< VAR >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red );
+   cgBody< VAR >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red, rp );
 }
 
 } // namespace hyb

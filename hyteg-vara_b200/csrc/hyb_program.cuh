@@ -48,6 +48,7 @@ struct Phase
    BdryLists       bl;
    OpDev< float >  op32; // operator of the phase's level in both types
    OpDev< double > op64;
+   RowPass         rp;   // row table of the pass (constant operator, small levels) or rows = nullptr
 };
 
 template < typename T >
@@ -84,11 +85,20 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
          switch ( kind )
          {
          case kPhSorIface:
-            sorIfaceBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.flag, P.bl );
+            if ( P.rp.rows )
+               rowPassBody< T, kRowSor >( P.rp, phaseOp< T >( P ).st, (T*) P.p0, (const T*) P.p1, nullptr, T( P.relax ),
+                                          P.flag );
+            else
+               sorIfaceBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.flag,
+                                       P.bl );
             break;
          case kPhSorInterior:
-            sorInteriorBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.a0, P.a1,
-                                       P.a2, P.cellBlocks );
+            if ( P.rp.rows )
+               rowPassBody< T, kRowSor >( P.rp, phaseOp< T >( P ).st, (T*) P.p0, (const T*) P.p1, nullptr, T( P.relax ),
+                                          0xff );
+            else
+               sorInteriorBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.a0,
+                                          P.a1, P.a2, P.cellBlocks );
             break;
          case kPhJacobi:
             jacobiBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1, (const T*) P.p2, T( P.relax ),
@@ -99,8 +109,12 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
                ( (T*) P.p0 )[i] = ( (const T*) P.p1 )[i];
             break;
          case kPhResidual:
-            applyBody< T, VAR, kResidual >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1, (const T*) P.p2,
-                                            P.flag, P.cellBlocks );
+            if ( P.rp.rows )
+               rowPassBody< T, kRowResidual >( P.rp, phaseOp< T >( P ).st, (T*) P.p0, (const T*) P.p2, (T*) P.p1, T( 0 ),
+                                               P.flag );
+            else
+               applyBody< T, VAR, kResidual >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1,
+                                               (const T*) P.p2, P.flag, P.cellBlocks );
             break;
          case kPhRestrict:
          {
@@ -128,7 +142,7 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
             break;
          case kPhCg:
             cgBody< VAR >( tp, lv, P.op64, (double*) P.p0, (const double*) P.p1, (double*) P.p2, (double*) P.p3,
-                           (double*) P.p4, P.relax, P.a0, P.status, red );
+                           (double*) P.p4, P.relax, P.a0, P.status, red, P.rp );
             break;
          default: break;
          }

@@ -111,6 +111,20 @@ size_t serveFootprint( const ServeKey& k, int meshMaxLevel )
    // an allowance of 64 KiB per level for the recorded phase list of the coarse-level
    // program kernel
    bytes += size_t( k.level + 1 ) * 65536;
+   // row tables of the small levels (constant coefficient): an upper bound from the cell
+   // count (at most 4 vertices, 6 edges and 4 faces per cell, lane padding per colour)
+   if ( k.coeff == HYB_COEFF_CONSTANT )
+      for ( int l = 0; l <= k.level; ++l )
+      {
+         const size_t N = size_t( 1 ) << l;
+         const size_t S = ( N + 1 ) * ( N + 2 ) * ( N + 3 ) / 6;
+         if ( long( nC * size_t( stridePad( int( S ) ) ) ) > rowTableMaxPoints() )
+            continue;
+         const size_t nIntFace = N >= 3 ? ( N - 1 ) * ( N - 2 ) / 2 : 0;
+         const size_t nPts     = N >= 4 ? ( N - 1 ) * ( N - 2 ) * ( N - 3 ) / 6 : 0;
+         const size_t surf     = nC * ( 128 + 48 * ( N - 1 ) + 8 * nIntFace ) + 3 * 32 * 16;
+         bytes += sizeof( SlabRow ) * ( 2 * surf + 2 * nC * nPts ) + 4096;
+      }
    return bytes;
 }
 

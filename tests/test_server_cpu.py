@@ -25,6 +25,15 @@ def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes
     b += nC * pad(4) * 8 * (5 if precision == 32 else 3)
     b += max(-(-closure(l) // 256) * nC for l in range(mesh_max_level + 1)) * 8
     b += (level + 1) * 65536  # phase-list allowance of the coarse-level program kernel
+    if coeff == 0:  # row tables (48-byte rows) of the small levels of a constant operator
+        for l in range(level + 1):
+            N = 1 << l
+            if nC * pad(closure(l)) > 20000:
+                continue
+            n_int_face = (N - 1) * (N - 2) // 2 if N >= 3 else 0
+            n_pts = (N - 1) * (N - 2) * (N - 3) // 6 if N >= 4 else 0
+            surf = nC * (128 + 48 * (N - 1) + 8 * n_int_face) + 3 * 32 * 16
+            b += 48 * (2 * surf + 2 * nC * n_pts) + 4096
     return b + 16 + 16 + 4 * modes * 8
 
 
