@@ -123,6 +123,7 @@ struct RowTables
    DevBuf< SlabRow >   iface, interior, all;
    std::vector< long > ifaceOff; // per surface colour: first row
    long                allN = 0, allB1 = 0, allB2 = 0, allB3 = 0;
+   bool                full = true; // false: only the surface colours' rows (large levels)
 };
 
 struct LevelHost
@@ -789,6 +790,124 @@ void launchToDofs( const Storage& s, int l, const T* slab, T* dofs, cudaStream_t
    HYB_CHECK_LAUNCH();
 }
 
+// Levels whose closure slabs hold at most this many points (all cells) get full row tables
+// (HYB_ROW_TABLE_MAX_POINTS overrides it, 0: none); larger levels up to the second bound
+// get the surface colours' rows only (HYB_ROW_IFACE_MAX_POINTS): their interior passes
+// are bandwidth bound and keep the interior point tables.
+constexpr long kRowTableMaxPoints = 400000;
+constexpr long kRowIfaceMaxPoints = 4000000;
+
+long envLong( const char* name, long dflt )
+{
+   const char* e = std::getenv( name );
+   return e ? std::atol( e ) : dflt;
+}
+long rowTableMaxPoints()
+{
+   static const long v = envLong( "HYB_ROW_TABLE_MAX_POINTS", kRowTableMaxPoints );
+   return v;
+}
+long rowIfaceMaxPoints()
+{
+   static const long v = envLong( "HYB_ROW_IFACE_MAX_POINTS", kRowIfaceMaxPoints );
+   return v;
+}
+
+// The row tables of level l, built on first use (not inside a stream capture); nullptr if
+// the level is too large, or if a DoF has more embeddings than its lane group (then the
+// passes keep the lane-group path).
+const RowTables* ensureRows( Storage& s, int l )
+{
+   LevelHost& L = *s.lv[size_t( l )];
+   if ( L.rowsTried )
+      return L.rows.get();
+   L.rowsTried = true;
+   const LevelDev& d      = L.dev;
+   const long      points = long( s.td.nC ) * d.stride;
+   if ( points > std::max( rowTableMaxPoints(), rowIfaceMaxPoints() ) || d.stride >= 65536 )
+      return nullptr;
+   auto R  = std::make_unique< RowTables >();
+   R->full = points <= rowTableMaxPoints();
+   DevBuf< int >    err;
+   err.alloc( 1 );
+   HYB_CUDA( cudaMemset( err.p, 0, sizeof( int ) ) );
+   auto grid = [&]( long n ) { return dim3( unsigned( std::max< long >( 1, std::min< long >( ( n + 255 ) / 256, 4096 ) ) ) ); };
+   // surface colours
+   long total = 0;
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      R->ifaceOff.push_back( total );
+      const int* co = &L.colourOff[4 * c];
+      total += bdryLaneCount( co[1], co[2], co[3] );
+   }
+   R->iface.alloc( size_t( std::max< long >( total, 1 ) ) );
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      const int* co    = &L.colourOff[4 * c];
+      const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+      if ( lanes == 0 )
+         continue;
+      const int32_t*  list = L.colourList.p + co[0];
+      const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+      k_rows_surface<<< grid( lanes ), 256 >>>( s.td, d, bl, lanes, R->iface.p + R->ifaceOff[size_t( c )], err.p );
+      HYB_CHECK_LAUNCH();
+   }
+   if ( !R->full )
+   {
+      int bad = 0;
+      HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
+      if ( bad )
+         return nullptr;
+      L.rows = std::move( R );
+      return L.rows.get();
+   }
+   // interior colours
+   const long nInt = long( s.td.nC ) * d.nPts;
+   R->interior.alloc( size_t( std::max< long >( nInt, 1 ) ) );
+   for ( int c = 0; c < kInteriorColours; ++c )
+   {
+      const int count = d.ptsOff[c + 1] - d.ptsOff[c];
+      if ( count == 0 )
+         continue;
+      k_rows_interior<<< grid( long( s.td.nC ) * count ), 256 >>>( s.td, d, d.ptsC + d.ptsOff[c], count,
+                                                                  R->interior.p + long( s.td.nC ) * d.ptsOff[c] );
+      HYB_CHECK_LAUNCH();
+   }
+   // all DoFs
+   const int       nv = s.td.nV, ne = s.td.nE * ( d.N - 1 ), nf = s.td.nF * d.nIntFace;
+   const BdryLists full{ nullptr, nullptr, nullptr, nv, ne, nf };
+   const long      surf = bdryLaneCount( nv, ne, nf );
+   R->allB1             = long( nv ) * 32;
+   R->allB2             = R->allB1 + ( long( ne ) * 8 + 31 ) / 32 * 32;
+   R->allB3             = surf;
+   R->allN              = surf + nInt;
+   R->all.alloc( size_t( std::max< long >( R->allN, 1 ) ) );
+   if ( surf > 0 )
+   {
+      k_rows_surface<<< grid( surf ), 256 >>>( s.td, d, full, surf, R->all.p, err.p );
+      HYB_CHECK_LAUNCH();
+   }
+   if ( nInt > 0 )
+   {
+      k_rows_interior<<< grid( nInt ), 256 >>>( s.td, d, d.pts, d.nPts, R->all.p + surf );
+      HYB_CHECK_LAUNCH();
+   }
+   int bad = 0;
+   HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
+   if ( bad )
+      return nullptr;
+   L.rows = std::move( R );
+   return L.rows.get();
+}
+
+// the row table of level l if it has been built (usable inside a capture)
+const RowTables* rowsIf( const Storage& s, int l ) { return s.lv[size_t( l )]->rows.get(); }
+
+RowPass rowPassAll( const RowTables* R )
+{
+   return R && R->full ? RowPass{ R->all.p, R->allN, R->allB1, R->allB2, R->allB3 } : RowPass{ nullptr, 0, 0, 0, 0 };
+}
+
 template < typename T >
 void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs, int flag, int mode, cudaStream_t stream )
 {
@@ -799,6 +918,21 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
    if ( nb == 0 )
       return;
    const OpDev< T > od = op.dev< T >( l );
+   if ( !op.variable && ( mode == kResidual || mode == kReplace ) )
+      if ( const RowTables* R = rowsIf( s, l ); R && R->full )
+      {
+         // small and middle levels: the precomputed rows (residual r = b - A u, or r = A u)
+         const RowPass rp = rowPassAll( R );
+         const int     g  = int( std::max< long >( 1, std::min< long >( ( rp.n + 127 ) / 128, long( s.numSMs ) * 8 ) ) );
+         if ( mode == kResidual )
+            pdlLaunch( k_row_pass< T, kRowResidual >, dim3( g ), dim3( 128 ), 0, stream, rp, od.st, const_cast< T* >( src ),
+                       rhs, dst, T( 0 ), flag );
+         else
+            pdlLaunch( k_row_pass< T, kRowApply >, dim3( g ), dim3( 128 ), 0, stream, rp, od.st, const_cast< T* >( src ),
+                       rhs, dst, T( 0 ), flag );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
 #define HYB_APPLY( VAR, MODE ) pdlLaunch( k_apply< T, VAR, MODE >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, flag, nc )
    if ( op.variable )
    {
@@ -836,12 +970,22 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
    const auto&      L  = s.L( l );
    const OpDev< T > od = op.dev< T >( l );
    // interface passes: one launch per colour over that colour's surface DoFs
+   const RowTables* R = op.variable ? nullptr : rowsIf( s, l );
    auto iface = [&]( int c ) {
       const int* co = &L.colourOff[4 * c];
       const long lanes = bdryLaneCount( co[1], co[2], co[3] );
       if ( lanes == 0 )
          return;
       const int       nb   = int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) );
+      if ( R )
+      {
+         const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
+         pdlLaunch( k_row_pass< T, kRowSor >, dim3( nb ), dim3( 128 ), 0, stream,
+                    RowPass{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes }, od.st, u, rhs, (T*) nullptr,
+                    relax, flag );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
       const int32_t*  list = L.colourList.p + co[0];
       const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
       if ( op.variable )
@@ -1000,102 +1144,6 @@ struct CgScratch
    DevBuf< int >               status;
 };
 
-// Levels whose closure slabs hold at most this many points (all cells) get row tables;
-// HYB_ROW_TABLE_MAX_POINTS overrides it (0: none).
-constexpr long kRowTableMaxPoints = 20000;
-
-long rowTableMaxPoints()
-{
-   static const long v = [] {
-      const char* e = std::getenv( "HYB_ROW_TABLE_MAX_POINTS" );
-      return e ? std::atol( e ) : kRowTableMaxPoints;
-   }();
-   return v;
-}
-
-// The row tables of level l, built on first use (not inside a stream capture); nullptr if
-// the level is too large, or if a DoF has more embeddings than its lane group (then the
-// passes keep the lane-group path).
-const RowTables* ensureRows( Storage& s, int l )
-{
-   LevelHost& L = *s.lv[size_t( l )];
-   if ( L.rowsTried )
-      return L.rows.get();
-   L.rowsTried = true;
-   const LevelDev& d = L.dev;
-   if ( long( s.td.nC ) * d.stride > rowTableMaxPoints() || d.stride >= 65536 )
-      return nullptr;
-   auto             R = std::make_unique< RowTables >();
-   DevBuf< int >    err;
-   err.alloc( 1 );
-   HYB_CUDA( cudaMemset( err.p, 0, sizeof( int ) ) );
-   auto grid = [&]( long n ) { return dim3( unsigned( std::max< long >( 1, std::min< long >( ( n + 255 ) / 256, 4096 ) ) ) ); };
-   // surface colours
-   long total = 0;
-   for ( int c = 0; c < s.td.m; ++c )
-   {
-      R->ifaceOff.push_back( total );
-      const int* co = &L.colourOff[4 * c];
-      total += bdryLaneCount( co[1], co[2], co[3] );
-   }
-   R->iface.alloc( size_t( std::max< long >( total, 1 ) ) );
-   for ( int c = 0; c < s.td.m; ++c )
-   {
-      const int* co    = &L.colourOff[4 * c];
-      const long lanes = bdryLaneCount( co[1], co[2], co[3] );
-      if ( lanes == 0 )
-         continue;
-      const int32_t*  list = L.colourList.p + co[0];
-      const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
-      k_rows_surface<<< grid( lanes ), 256 >>>( s.td, d, bl, lanes, R->iface.p + R->ifaceOff[size_t( c )], err.p );
-      HYB_CHECK_LAUNCH();
-   }
-   // interior colours
-   const long nInt = long( s.td.nC ) * d.nPts;
-   R->interior.alloc( size_t( std::max< long >( nInt, 1 ) ) );
-   for ( int c = 0; c < kInteriorColours; ++c )
-   {
-      const int count = d.ptsOff[c + 1] - d.ptsOff[c];
-      if ( count == 0 )
-         continue;
-      k_rows_interior<<< grid( long( s.td.nC ) * count ), 256 >>>( s.td, d, d.ptsC + d.ptsOff[c], count,
-                                                                  R->interior.p + long( s.td.nC ) * d.ptsOff[c] );
-      HYB_CHECK_LAUNCH();
-   }
-   // all DoFs
-   const int       nv = s.td.nV, ne = s.td.nE * ( d.N - 1 ), nf = s.td.nF * d.nIntFace;
-   const BdryLists full{ nullptr, nullptr, nullptr, nv, ne, nf };
-   const long      surf = bdryLaneCount( nv, ne, nf );
-   R->allB1             = long( nv ) * 32;
-   R->allB2             = R->allB1 + ( long( ne ) * 8 + 31 ) / 32 * 32;
-   R->allB3             = surf;
-   R->allN              = surf + nInt;
-   R->all.alloc( size_t( std::max< long >( R->allN, 1 ) ) );
-   if ( surf > 0 )
-   {
-      k_rows_surface<<< grid( surf ), 256 >>>( s.td, d, full, surf, R->all.p, err.p );
-      HYB_CHECK_LAUNCH();
-   }
-   if ( nInt > 0 )
-   {
-      k_rows_interior<<< grid( nInt ), 256 >>>( s.td, d, d.pts, d.nPts, R->all.p + surf );
-      HYB_CHECK_LAUNCH();
-   }
-   int bad = 0;
-   HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
-   if ( bad )
-      return nullptr;
-   L.rows = std::move( R );
-   return L.rows.get();
-}
-
-// the row table of level l if it has been built (usable inside a capture)
-const RowTables* rowsIf( const Storage& s, int l ) { return s.lv[size_t( l )]->rows.get(); }
-
-RowPass rowPassAll( const RowTables* R )
-{
-   return R ? RowPass{ R->all.p, R->allN, R->allB1, R->allB2, R->allB3 } : RowPass{ nullptr, 0, 0, 0, 0 };
-}
 
 void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch& cs, double tol, int maxIter,
                cudaStream_t stream )
@@ -1237,7 +1285,11 @@ struct PhaseList
    }
    long slabElems( int l ) const { return long( g.st->td.nC ) * g.st->L( l ).dev.stride; }
    // the row table of level l for the passes of this (constant) operator, built on first use
-   const RowTables* rows( int l ) const { return g.op->variable ? nullptr : ensureRows( *g.st, l ); }
+   const RowTables* rows( int l ) const
+   {
+      const RowTables* R = g.op->variable ? nullptr : ensureRows( *g.st, l );
+      return R && R->full ? R : nullptr;
+   }
    int  flatBlocks( long n ) const
    {
       return int( std::min< long >( ( n + 127 ) / 128, long( g.st->numSMs ) * 8 ) );
@@ -1520,7 +1572,8 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
 void prepare( Gmg& g )
 {
    if ( !g.op->variable )
-      ensureRows( *g.st, g.minL );
+      for ( int l = g.minL; l <= g.maxL; ++l )
+         ensureRows( *g.st, l );
    if ( !g.cg.r )
    {
       g.cg.r.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );

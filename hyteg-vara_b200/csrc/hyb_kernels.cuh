@@ -508,12 +508,13 @@ enum RowMode : int
    kRowApply    = 2  // r = A u
 };
 
-// one pass over the rows with the block's threads (the rows of one DoF are adjacent lanes)
+// one pass over the rows, lanes start, start + step, ... (start - lane and step multiples
+// of 32; the rows of one DoF are adjacent lanes of one warp)
 template < typename T, int MODE >
 __device__ __forceinline__ void rowPassBody( const RowPass& rp, const T* __restrict__ st, T* u, const T* b, T* r, T relax,
-                                             int flag )
+                                             int flag, long long start, long long step )
 {
-   for ( long long gt = threadIdx.x; gt - ( threadIdx.x & 31 ) < rp.n; gt += blockDim.x )
+   for ( long long gt = start; gt - ( threadIdx.x & 31 ) < rp.n; gt += step )
    {
       int4 A = make_int4( -1, 0, 0, 0 ), B = make_int4( 0, 0, 0, 0 ), C = make_int4( 0, 0, 0, 0 );
       if ( gt < rp.n )
@@ -552,6 +553,16 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const T* __restr
       else
          r[i] = diag * u[i] + off;
    }
+}
+
+// a row pass as its own launch (levels between the program kernel's and the large ones)
+template < typename T, int MODE >
+__global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, const T* __restrict__ st, T* u, const T* b, T* r, T relax,
+                                                     int flag )
+{
+   HYB_PDL_PROLOGUE();
+   rowPassBody< T, MODE >( rp, st, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
+                           (long long) gridDim.x * blockDim.x );
 }
 
 // Constant-stencil quad: the points x = 4g + r, r = 0..3, of row (y, z). Each of the seven
@@ -1424,7 +1435,8 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
    // the operator through the level's row table when there is one
    auto applyA = [&]( const double* src, double* dst ) {
       if ( rp.rows )
-         rowPassBody< double, kRowApply >( rp, op.st, const_cast< double* >( src ), nullptr, dst, 0.0, flag );
+         rowPassBody< double, kRowApply >( rp, op.st, const_cast< double* >( src ), nullptr, dst, 0.0, flag, threadIdx.x,
+                                           blockDim.x );
       else
          cgApplyAll< VAR >( tp, lv, op, src, dst, flag );
    };

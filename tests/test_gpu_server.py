@@ -53,7 +53,8 @@ def test_result_same_alone_and_in_mix(H):
     ids = []
     for i, q in enumerate(MIX):
         # the last one arrives after the first probe has finished and reuses its hierarchy
-        arrival = 1.0 if i == len(MIX) - 1 else 0.002 * i
+        # (the loop's clock starts before the first mesh is built, which takes about a second)
+        arrival = 5.0 if i == len(MIX) - 1 else 0.002 * i
         ids.append(mix.submit(H.Server.request(*q), arrival_s=arrival, keep_solution=True,
                               num_dofs=ndofs(H, *q[:4])))
     mix.run(300)
@@ -98,10 +99,25 @@ def test_server_matches_standalone_solver(H, coefficient):
     assert rel_diff(sv.solution(rid), x.get(L)) <= TOL
 
 
+def test_footprint_is_an_upper_bound(H):
+    """The device bytes a resident hierarchy really holds never exceed its estimate, for the
+    constant (row tables) and the lognormal coefficient, mixed and plain FP64."""
+    reqs = [H.Server.request(*q) for q in [(2, 2, 2, 5, 0, 32, 1), (3, 3, 3, 4, 0, 64, 2), (1, 1, 1, 6, 0, 32, 3),
+                                           (2, 2, 2, 5, 1, 32, 4), (2, 2, 2, 4, 1, 64, 5)]]
+    sv = H.Server(8 << 30, max_active=8, max_level=6)
+    ids = [sv.submit(q) for q in reqs]
+    sv.run(120)
+    for i, q in zip(ids, reqs):
+        res = sv.result(i)
+        assert res.status == 0, res.status
+        assert 0 < res.footprint_bytes <= sv.footprint(q)
+
+
 def test_footprint_bound_and_tight_budget(H):
     """A budget that holds one level-5 hierarchy at a time: requests wait for memory,
-    idle hierarchies are evicted, and every request still completes."""
-    reqs = [H.Server.request(2, 2, 2, 5, c, 32, s) for s, c in [(1, 0), (2, 1), (3, 0), (4, 1)]]
+    idle hierarchies are evicted, and every request still completes. The shapes alternate
+    between FP32-inner (the larger) and FP64 hierarchies, so that no two fit together."""
+    reqs = [H.Server.request(2, 2, 2, 5, 1, p, s) for s, p in [(1, 32), (2, 64), (3, 32), (4, 64)]]
     probe = H.Server(1 << 40, max_level=5)
     need = max(probe.footprint(q) for q in reqs)
     # room for the mesh (a few MB) and one hierarchy, not two
