@@ -1167,6 +1167,66 @@ void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch&
    HYB_CHECK_LAUNCH();
 }
 
+// ChebyshevSmoother::setupCoefficients (src/hyteg/solvers/ChebyshevSmoother.hpp:98-188):
+// the power-basis coefficients w_0 .. w_{k-1} of p with 1 - l p(l) = T_k((th - l) / de) /
+// T_k(th / de) on the eigenvalue interval [lower, upper] of D^-1 A (th, de its midpoint and
+// half width, T_k the Chebyshev polynomial of the first kind, expanded by its three-term
+// recurrence); the smoother adds p(D^-1 A) D^-1 (b - A x) to x. Orders 1 to 5.
+std::vector< double > chebyshevCoefficients( int order, double lower, double upper )
+{
+   require( order >= 1 && order <= 5, "Chebyshev order must be in [1, 5]" );
+   require( std::isfinite( lower ) && std::isfinite( upper ) && 0 < lower && lower < upper,
+            "Chebyshev bounds must satisfy 0 < lower < upper" );
+   const double th = 0.5 * ( upper + lower ), de = 0.5 * ( upper - lower );
+   const double a = th / de, c = -1.0 / de; // T_k's argument a + c l
+   std::vector< double > prev( order + 1, 0.0 ), cur( order + 1, 0.0 ), next( order + 1, 0.0 );
+   prev[0] = 1.0;
+   cur[0]  = a;
+   cur[1]  = c;
+   for ( int n = 1; n < order; ++n )
+   {
+      std::fill( next.begin(), next.end(), 0.0 );
+      for ( int i = 0; i <= n; ++i )
+      {
+         next[i] += 2 * a * cur[i] - prev[i];
+         next[i + 1] += 2 * c * cur[i];
+      }
+      prev.swap( cur );
+      cur.swap( next );
+   }
+   std::vector< double > w( order );
+   for ( int i = 1; i <= order; ++i )
+      w[i - 1] = -cur[i] / cur[0];
+   return w;
+}
+
+// diag(A)^-1 of level l into out (every replica)
+template < typename T >
+void launchInvDiag( const Operator& op, int l, const T* zeros, T* out, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
+   if ( nb == 0 )
+      return;
+   const OpDev< T > od = op.dev< T >( l );
+   if ( op.variable )
+      k_inv_diag< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
+   else
+      k_inv_diag< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchChebUpdate( const Storage& s, int l, const T* inv, T* t, T* x, T w, cudaStream_t stream )
+{
+   const long long n = (long long) s.td.nC * s.L( l ).dev.stride;
+   const int       g = int( std::max< long long >( 1, std::min< long long >( ( n + 255 ) / 256, (long long) s.numSMs * 8 ) ) );
+   pdlLaunch( k_cheb_update< T >, dim3( g ), dim3( 256 ), 0, stream, n, inv, t, x, w );
+   HYB_CHECK_LAUNCH();
+}
+
 // ---------------------------------------------------------------------------
 // Geometric multigrid (GeometricMultigridSolver.hpp:136-235)
 // ---------------------------------------------------------------------------
@@ -1181,6 +1241,9 @@ struct Gmg
    std::unique_ptr< Function > x32, b32, t32; // FP32 inner hierarchy (mixed precision)
    std::unique_ptr< Function > r64;           // FP64 residual (mixed precision)
    std::unique_ptr< Function > cx64, cb64;    // FP64 coarse-solve copies of the FP32 hierarchy
+   std::vector< double >       cheb;          // Chebyshev smoother: omega_0 .. omega_{order-1}
+   std::unique_ptr< Function > inv64, inv32;  // Chebyshev smoother: diag(A)^-1 per level
+   std::unique_ptr< Function > ch64, ch32;    // Chebyshev smoother: second temporary
    CgScratch                   cg;
    // reduction scratch of this solver, so that solvers sharing a storage can run on
    // different streams at the same time: scalars[0] = ||r||^2, scalars[1] = ||b||^2
@@ -1232,6 +1295,24 @@ void smooth( Gmg& g, int l, T* x, const T* b, T* scratch, cudaStream_t stream )
       // SymmetricSORSmoother::solve (SymmetricSORSmoother.hpp:38-57): forward, then backwards
       launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
       launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream, true );
+   }
+   else if ( g.smoother == HYB_SMOOTHER_CHEBYSHEV )
+   {
+      // ChebyshevSmoother::solve (ChebyshevSmoother.hpp:49-96): t = D^-1 (b - A x), x += w_0 t,
+      // then t = D^-1 A t, x += w_k t. scratch (the solver's residual vector) and the second
+      // temporary are only written on Inner|Neumann DoFs, so they hold 0 elsewhere.
+      const bool      f64 = std::is_same< T, double >::value;
+      const T*        inv = ( f64 ? g.inv64 : g.inv32 )->template ptr< T >( l );
+      T*              t   = scratch;
+      T*              t2  = ( f64 ? g.ch64 : g.ch32 )->template ptr< T >( l );
+      launchApply< T >( *g.op, l, x, t, b, kGmgFlag, kResidual, stream );
+      launchChebUpdate< T >( *g.st, l, inv, t, x, T( g.cheb[0] ), stream );
+      for ( size_t k = 1; k < g.cheb.size(); ++k )
+      {
+         launchApply< T >( *g.op, l, t, t2, nullptr, kGmgFlag, kReplace, stream );
+         launchChebUpdate< T >( *g.st, l, inv, t2, x, T( g.cheb[k] ), stream );
+         std::swap( t, t2 );
+      }
    }
    else
    {
@@ -1569,8 +1650,32 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
 }
 
 // everything a captured graph needs is allocated before capture begins
+// the Chebyshev smoother's inverse diagonals and temporaries for the hierarchies in use
+void ensureChebyshev( Gmg& g )
+{
+   if ( g.smoother != HYB_SMOOTHER_CHEBYSHEV )
+      return;
+   require( !g.cheb.empty(), "the Chebyshev smoother needs its coefficients (hyb_gmg_setup_chebyshev)" );
+   auto fill = [&]( std::unique_ptr< Function >& inv, std::unique_ptr< Function >& t2, int dtype ) {
+      if ( inv )
+         return;
+      inv.reset( makeFunction( g.st, g.minL, g.maxL, dtype ) );
+      t2.reset( makeFunction( g.st, g.minL, g.maxL, dtype ) );
+      for ( int l = g.minL; l <= g.maxL; ++l )
+         if ( dtype == HYB_F64 )
+            launchInvDiag< double >( *g.op, l, t2->ptr< double >( l ), inv->ptr< double >( l ), nullptr );
+         else
+            launchInvDiag< float >( *g.op, l, t2->ptr< float >( l ), inv->ptr< float >( l ), nullptr );
+      HYB_CUDA( cudaDeviceSynchronize() );
+   };
+   fill( g.inv64, g.ch64, HYB_F64 );
+   if ( g.x32 )
+      fill( g.inv32, g.ch32, HYB_F32 );
+}
+
 void prepare( Gmg& g )
 {
+   ensureChebyshev( g );
    if ( !g.op->variable )
       for ( int l = g.minL; l <= g.maxL; ++l )
          ensureRows( *g.st, l );
@@ -1607,6 +1712,8 @@ void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int
    for ( int l = minL; l <= maxL; ++l )
       if ( long( s->td.nC ) * s->L( l ).dev.stride <= maxPoints )
          g.progTop = l;
+   if ( smoother == HYB_SMOOTHER_CHEBYSHEV )
+      g.progTop = -1; // the program kernel has no Chebyshev phases
 }
 
 
@@ -2279,7 +2386,8 @@ int hyb_gmg_create( hyb_storage* s, hyb_operator* oh, int minL, int maxL, int pr
    require( op->st == ST( s ), "operator belongs to another storage" );
    require( minL >= op->minL && maxL <= op->maxL && minL <= maxL, "GMG levels outside the operator's level range" );
    require( pre >= 0 && post >= 0, "smoothing steps must be non-negative" );
-   require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI || smoother == HYB_SMOOTHER_SYMMETRIC_SOR,
+   require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI || smoother == HYB_SMOOTHER_SYMMETRIC_SOR ||
+                smoother == HYB_SMOOTHER_CHEBYSHEV,
             "unknown smoother" );
    auto g = std::make_unique< hyb_gmg_s >();
    initGmg( *g, ST( s ), op, minL, maxL, pre, post, relax, smoother, coarseTol, coarseMaxIter );
@@ -2310,6 +2418,83 @@ int hyb_gmg_set_cycle_type( hyb_gmg* gh, int cycleType )
    g->graphs.clear();
    g->programs.clear();
    g->cycleType = cycleType;
+   HYB_API_END
+}
+
+int hyb_chebyshev_coefficients( int order, double lower, double upper, double* out )
+{
+   HYB_API_BEGIN
+   require( out, "null argument" );
+   const auto w = chebyshevCoefficients( order, lower, upper );
+   std::copy( w.begin(), w.end(), out );
+   HYB_API_END
+}
+
+int hyb_gmg_setup_chebyshev( hyb_gmg* gh, int order, double lower, double upper )
+{
+   HYB_API_BEGIN
+   Gmg* g = gh;
+   require( g != nullptr, "null argument" );
+   require( g->smoother == HYB_SMOOTHER_CHEBYSHEV, "the solver was not created with the Chebyshev smoother" );
+   g->cheb = chebyshevCoefficients( order, lower, upper );
+   // captured graphs hold the old coefficients
+   HYB_CUDA( cudaDeviceSynchronize() );
+   for ( auto& gr : g->graphs )
+      cudaGraphExecDestroy( gr.exec );
+   g->graphs.clear();
+   HYB_API_END
+}
+
+int hyb_operator_estimate_spectral_radius( hyb_operator* oh, hyb_function* xh, hyb_function* th, int level, int iterations,
+                                           double* radius )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *x = FN( xh ), *t = FN( th );
+   require( radius && iterations >= 1, "null argument or no iteration" );
+   checkOpFn( op, x, level );
+   checkOpFn( op, t, level );
+   require( x != t && x->dtype == HYB_F64 && t->dtype == HYB_F64, "two distinct FP64 functions are needed" );
+   Storage&          s   = *op->st;
+   const long long   n   = (long long) s.td.nC * s.L( level ).dev.stride;
+   std::unique_ptr< Function > inv( makeFunction( &s, level, level, HYB_F64 ) );
+   std::unique_ptr< Function > zero( makeFunction( &s, level, level, HYB_F64 ) );
+   launchInvDiag< double >( *op, level, zero->ptr< double >( level ), inv->ptr< double >( level ), nullptr );
+   double*       xp = x->ptr< double >( level );
+   double*       tp = t->ptr< double >( level );
+   const double* ip = inv->ptr< double >( level );
+   auto dot = [&]( const double* a, const double* b ) {
+      launchDot< double >( s, level, a, b, HYB_ALL, 1, nullptr );
+      HYB_CUDA( cudaMemcpy( s.hostScalar, s.scalars.p + 1, sizeof( double ), cudaMemcpyDeviceToHost ) );
+      return s.hostScalar[0];
+   };
+   // scale the slab: every replica and the zero padding alike
+   auto scale = [&]( double* dst, const double* src, double a ) {
+      const int g = int( std::max< long long >( 1, std::min< long long >( ( n + 255 ) / 256, (long long) s.numSMs * 8 ) ) );
+      k_scale_copy<<< g, 256 >>>( n, src, dst, a );
+      HYB_CHECK_LAUNCH();
+   };
+   // D^-1 A on All (chebyshev::InvDiagOperatorWrapper::apply)
+   auto invDiagA = [&]( const double* src, double* dst ) {
+      launchApply< double >( *op, level, src, dst, nullptr, HYB_ALL, kReplace, nullptr );
+      const int g = int( std::max< long long >( 1, std::min< long long >( ( n + 255 ) / 256, (long long) s.numSMs * 8 ) ) );
+      k_mul<<< g, 256 >>>( n, ip, dst );
+      HYB_CHECK_LAUNCH();
+   };
+   // estimateSpectralRadiusWithPowerIteration (SpectrumEstimation.hpp:57-81)
+   double norm = std::sqrt( dot( xp, xp ) );
+   scale( xp, xp, 1.0 / norm );
+   invDiagA( xp, tp );
+   double r = 0;
+   for ( int it = 1; it <= iterations; ++it )
+   {
+      norm = std::sqrt( dot( tp, tp ) );
+      scale( xp, tp, 1.0 / norm );
+      invDiagA( xp, tp );
+      r = dot( xp, tp );
+   }
+   HYB_CUDA( cudaDeviceSynchronize() );
+   *radius = r;
    HYB_API_END
 }
 

@@ -861,6 +861,73 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, Level
 }
 
 // ---------------------------------------------------------------------------
+// diag(A)^-1 at every closure point (all replicas; the full row's diagonal for macro-
+// primitive DoFs). zeros: a zero vector of the level, read as the operand of the rows
+// whose off-diagonal part is discarded. Cells' interiors on the first nCellBlocks blocks.
+// ---------------------------------------------------------------------------
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_inv_diag( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ zeros,
+                                                     T* __restrict__ out, int nCellBlocks )
+{
+   const Blk vb = launchBlk();
+   if ( vb.x < nCellBlocks )
+   {
+      const int nChunks = ( lv.nPts + 31 ) / 32;
+      HYB_CELL_LOOP( nChunks )
+      {
+         const int       cell = it_ / nChunks;
+         PointBatch< 1 > pb;
+         pb.load( lv.pts, lv.blk, lv.nPts, ( it_ - cell * nChunks ) * 32 + int( threadIdx.x & 31 ) );
+         InteriorOp< T, VAR > io;
+         io.load( op, cell );
+         T diag, off;
+         io.row( zeros + size_t( cell ) * lv.stride, pb.g[0], pb.no[0], diag, off );
+         if ( pb.valid[0] )
+            out[size_t( cell ) * lv.stride + pb.no[0].d[0] + pb.g[0]] = T( 1 ) / diag;
+      }
+      return;
+   }
+   const BdryLists bl = fullBdryLists( tp, lv );
+   HYB_BDRY_LANES( bl )
+   {
+      const LaneTask  tk = laneTask( tp, lv, bl, gt );
+      const BdryPoint p  = decodeBdry( tp, lv, tk.t );
+      T               diag, off;
+      bdryRowGroup< T, VAR >( tp, lv, op, zeros, p, tk, tk.valid, diag, off );
+      if ( tk.valid )
+         bdryWriteGroup( tp, lv, p, tk, out, T( 1 ) / diag );
+   }
+}
+
+// dst = a * src and dst *= w over a level's slabs (power iteration of the spectral radius
+// estimate)
+__global__ void k_scale_copy( long long n, const double* __restrict__ src, double* dst, double a )
+{
+   for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x )
+      dst[i] = a * src[i];
+}
+__global__ void k_mul( long long n, const double* __restrict__ w, double* dst )
+{
+   for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x )
+      dst[i] *= w[i];
+}
+
+// Chebyshev smoother update over a level's slabs: t = inv * t, x += w t (entries outside the
+// smoothed DoFs hold t = 0 and stay unchanged)
+template < typename T >
+__global__ void __launch_bounds__( 256 ) k_cheb_update( long long n, const T* __restrict__ inv, T* __restrict__ t,
+                                                        T* __restrict__ x, T w )
+{
+   HYB_PDL_PROLOGUE();
+   for ( long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x )
+   {
+      const T v = inv[i] * t[i];
+      t[i]      = v;
+      x[i] += w * v;
+   }
+}
+
+// ---------------------------------------------------------------------------
 // Weighted Jacobi (P1Operator::smooth_jac, P1Operator.hpp:424-440):
 // dst = src + relax * (rhs - A src) / diag(A)
 // ---------------------------------------------------------------------------

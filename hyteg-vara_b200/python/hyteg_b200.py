@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(PKG, "libhyteg_b200.so")
 INNER, DIRICHLET, NEUMANN, FREESLIP, ALL = 1, 2, 4, 8, 15
 REPLACE, ADD = 0, 1
 F64, F32 = 0, 1
-SMOOTHER_SOR, SMOOTHER_JACOBI, SMOOTHER_SYMMETRIC_SOR = 0, 1, 2
+SMOOTHER_SOR, SMOOTHER_JACOBI, SMOOTHER_SYMMETRIC_SOR, SMOOTHER_CHEBYSHEV = 0, 1, 2, 3
 CYCLE_V, CYCLE_W = 0, 1
 
 # the C ABI symbols (include/hyteg_b200.h); tests check that the library exports all of them
@@ -35,7 +35,8 @@ SYMBOLS = [
     "hyb_operator_create_divkgrad_rff", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
-    "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type",
+    "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
+    "hyb_chebyshev_coefficients", "hyb_operator_estimate_spectral_radius",
 ]
 
 COEFF_CONSTANT, COEFF_LOGNORMAL, COEFF_RADIAL = 0, 1, 2
@@ -118,6 +119,9 @@ def load(path=LIB_PATH):
         "hyb_storage_create_from_gmsh": (I, [ctypes.c_char_p, I, PP]),
         "hyb_operator_smooth_sor_backwards": (I, [P, P, P, D, I, I, P]),
         "hyb_gmg_set_cycle_type": (I, [P, I]),
+        "hyb_gmg_setup_chebyshev": (I, [P, I, D, D]),
+        "hyb_chebyshev_coefficients": (I, [I, D, D, P]),
+        "hyb_operator_estimate_spectral_radius": (I, [P, P, P, I, I, P]),
         "hyb_server_create": (I, [ctypes.c_size_t, I, I, PP]),
         "hyb_server_destroy": (I, [P]),
         "hyb_server_footprint": (I, [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
@@ -340,6 +344,12 @@ class _Operator:
     def smooth_gs_backwards(self, dst, rhs, level, flag, stream=None):
         self.smooth_sor_backwards(dst, rhs, 1.0, level, flag, stream)
 
+    def estimate_spectral_radius(self, x, tmp, level, iterations):
+        """chebyshev::estimateRadius: power iteration on D^-1 A (x is the start vector)."""
+        r = ctypes.c_double()
+        _check(load().hyb_operator_estimate_spectral_radius(self.h, x.h, tmp.h, level, iterations, ctypes.byref(r)))
+        return r.value
+
     def smooth_jac(self, dst, rhs, src, relax, level, flag, stream=None):
         _check(load().hyb_operator_smooth_jac(self.h, dst.h, rhs.h, src.h, float(relax), level, flag,
                                               _stream(stream)))
@@ -426,6 +436,13 @@ class GeometricMultigridSolver:
         if cycle_type != CYCLE_V:
             _check(load().hyb_gmg_set_cycle_type(self.h, cycle_type))
 
+    def setup_chebyshev(self, order, spectral_radius=None, lower=None, upper=None):
+        """ChebyshevSmoother::setupCoefficients(order, rho) -> [0.3 rho, 1.2 rho], or explicit
+        bounds of the eigenvalue interval of D^-1 A."""
+        if spectral_radius is not None:
+            lower, upper = 0.3 * spectral_radius, 1.2 * spectral_radius
+        _check(load().hyb_gmg_setup_chebyshev(self.h, order, float(lower), float(upper)))
+
     def close(self):
         if getattr(self, "h", None):
             try:
@@ -450,6 +467,12 @@ class GeometricMultigridSolver:
         _check(load().hyb_gmg_solve_to_tolerance(self.h, x.h, b.h, level, float(rel_tol), max_cycles, precision,
                                                  _p(hist), ctypes.byref(cyc), _stream(stream)))
         return hist[: cyc.value + 1]
+
+
+def chebyshev_coefficients(order, lower, upper):
+    out = np.zeros(order)
+    _check(load().hyb_chebyshev_coefficients(order, float(lower), float(upper), _p(out)))
+    return out
 
 
 def rff_features(seed, corr_len=0.2, modes=64):

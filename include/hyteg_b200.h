@@ -29,6 +29,8 @@
  *   hyb_cg_solve                  CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:66-135)
  *   hyb_gmg_create / hyb_gmg_solve  GeometricMultigridSolver ctor / solve (GeometricMultigridSolver.hpp:42-235)
  *   hyb_gmg_set_cycle_type        the CycleType argument of the GeometricMultigridSolver ctor (V or W)
+ *   hyb_gmg_setup_chebyshev       ChebyshevSmoother::setupCoefficients (ChebyshevSmoother.hpp)
+ *   hyb_operator_estimate_spectral_radius  chebyshev::estimateRadius (ChebyshevSmoother.hpp)
  *   hyb_gmg_solve_fmg             FullMultigridSolver::solve (src/hyteg/solvers/FullMultigridSolver.hpp)
  *   hyb_storage_create_from_gmsh  MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp)
  *
@@ -80,6 +82,9 @@ typedef enum
 #define HYB_SMOOTHER_SOR 0
 #define HYB_SMOOTHER_JACOBI 1
 #define HYB_SMOOTHER_SYMMETRIC_SOR 2
+/* ChebyshevSmoother (src/hyteg/solvers/ChebyshevSmoother.hpp): x += p(D^-1 A) D^-1 (b - A x),
+ * coefficients from hyb_gmg_setup_chebyshev before the first solve */
+#define HYB_SMOOTHER_CHEBYSHEV 3
 /* multigrid cycle types (GeometricMultigridSolver.hpp CycleType) */
 #define HYB_CYCLE_V 0
 #define HYB_CYCLE_W 1
@@ -205,6 +210,17 @@ int hyb_gmg_destroy( hyb_gmg* g );
 /* HYB_CYCLE_V (default) or HYB_CYCLE_W: with W the coarse-grid correction recurses twice
  * (GeometricMultigridSolver.hpp:201-204); applies to every later solve of this solver */
 int hyb_gmg_set_cycle_type( hyb_gmg* g, int cycle_type );
+/* ChebyshevSmoother::setupCoefficients(order, lowerBound, upperBound) (ChebyshevSmoother.hpp:98-188):
+ * order 1..5, eigenvalue interval [lower, upper] of D^-1 A (the reference's
+ * setupCoefficients(order, rho) uses [0.3 rho, 1.2 rho]) */
+int hyb_gmg_setup_chebyshev( hyb_gmg* g, int order, double lower, double upper );
+/* the coefficients w_0 .. w_{order-1} those calls use */
+int hyb_chebyshev_coefficients( int order, double lower, double upper, double* out );
+/* chebyshev::estimateRadius (ChebyshevSmoother.hpp:252-262): power iteration on D^-1 A with
+ * flag All (SpectrumEstimation.hpp:57-81); x (FP64) is the start vector and is overwritten,
+ * tmp (FP64) is scratch; blocking */
+int hyb_operator_estimate_spectral_radius( hyb_operator* op, hyb_function* x, hyb_function* tmp, int level,
+                                           int iterations, double* radius );
 /* one V-cycle on level (GeometricMultigridSolver::solve); b's coarser levels are scratch */
 int hyb_gmg_solve( hyb_gmg* g, hyb_function* x, hyb_function* b, int level, void* stream );
 /* blocking: cycles until ||b - Ax|| / ||b|| <= rel_tol (Inner|Neumann DoFs) or max_cycles.

@@ -198,6 +198,14 @@ class P1OperatorBase
    {
       smooth_sor_backwards( dst, rhs, V( 1 ), level, flag );
    }
+   // chebyshev::estimateRadius (power iteration on D^-1 A); x is the start vector
+   double estimateSpectralRadius( const P1Function< double >& x, const P1Function< double >& tmp, int level,
+                                  int iterations ) const
+   {
+      double r = 0;
+      hybCheck( hyb_operator_estimate_spectral_radius( h_, x.handle(), tmp.handle(), level, iterations, &r ) );
+      return r;
+   }
    template < typename V >
    void smooth_jac( const P1Function< V >& dst, const P1Function< V >& rhs, const P1Function< V >& src, V relax, int level,
                     DoFType flag ) const
@@ -313,6 +321,12 @@ class GeometricMultigridSolver
    void solveFullMultigrid( const P1Function< double >& x, const P1Function< double >& b, int level, int cyclesPerLevel = 1 )
    {
       hybCheck( hyb_gmg_solve_fmg( h_, x.handle(), b.handle(), level, cyclesPerLevel, nullptr ) );
+   }
+   // ChebyshevSmoother::setupCoefficients(order, spectralRadius) for a solver created with
+   // HYB_SMOOTHER_CHEBYSHEV
+   void setupChebyshev( int order, double spectralRadius )
+   {
+      hybCheck( hyb_gmg_setup_chebyshev( h_, order, 0.3 * spectralRadius, 1.2 * spectralRadius ) );
    }
    // cycles until ||b - Ax|| / ||b|| <= relTol; precision 64 (FP64) or 32 (FP32 inner cycles)
    std::vector< double > solveToTolerance( const P1Function< double >& x, const P1Function< double >& b, int level,

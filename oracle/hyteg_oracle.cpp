@@ -186,6 +186,7 @@ struct Oracle
    int                                    maxLevel;
    std::vector< Level >                   lv;
    std::vector< Op >                      ops;
+   std::vector< double >                  cheb; // Chebyshev smoother: omega_0 .. omega_{order-1}
 };
 
 void buildTopology( Oracle& o )
@@ -951,6 +952,91 @@ Oracle* H( void* h ) { return static_cast< Oracle* >( h ); }
 // ---------------------------------------------------------------------------
 // GMG (GeometricMultigridSolver.hpp:136-235)
 // ---------------------------------------------------------------------------
+// diag(A) of every DoF (the full row's diagonal: macro-primitive DoFs sum their cells)
+template < typename T >
+void invDiagT( const Oracle& o, const Op& op, const Level& lv, T* out )
+{
+   auto zero = []( i64 ) { return T( 0 ); };
+   for ( i64 d = 0; d < lv.offC; ++d )
+   {
+      T diag = 0, off = 0;
+      fullRow( o, op, lv, d, zero, diag, off );
+      out[d] = T( 1 ) / diag;
+   }
+   const i64 N = lv.N;
+   for ( i64 c = 0; c < i64( o.T.size() ); ++c )
+      for ( i64 z = 1; z <= N; ++z )
+         for ( i64 y = 1; y <= N - z; ++y )
+            for ( i64 x = 1; x <= N - y - z - 1; ++x )
+            {
+               T diag = 0, off = 0;
+               partialRow( o, op, lv, int( c ), x, y, z, zero, diag, off );
+               out[lv.cellMap[c][cellIdx( N + 1, x, y, z )]] = T( 1 ) / diag;
+            }
+}
+
+// ChebyshevSmoother::solve (src/hyteg/solvers/ChebyshevSmoother.hpp:49-96) on flag
+// Inner|Neumann: t = D^-1 (b - A x), x += w_0 t, then for k >= 1 t = D^-1 A t, x += w_k t.
+template < typename T >
+void chebyshevT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, const std::vector< double >& w )
+{
+   const int flag = ORC_INNER | ORC_NEUMANN;
+   std::vector< T > inv( lv.nDof ), t( lv.nDof, T( 0 ) ), t2( lv.nDof, T( 0 ) );
+   invDiagT( o, op, lv, inv.data() );
+   applyT( o, op, lv, x, t.data(), flag, false );
+   for ( i64 d = 0; d < lv.nDof; ++d )
+      if ( flagged( lv.bc[d], flag ) )
+      {
+         t[d] = inv[d] * ( b[d] - t[d] );
+         x[d] += T( w[0] ) * t[d];
+      }
+   for ( size_t k = 1; k < w.size(); ++k )
+   {
+      applyT( o, op, lv, t.data(), t2.data(), flag, false );
+      for ( i64 d = 0; d < lv.nDof; ++d )
+         if ( flagged( lv.bc[d], flag ) )
+         {
+            t[d] = inv[d] * t2[d];
+            x[d] += T( w[k] ) * t[d];
+         }
+   }
+}
+
+// Power-basis coefficients w_0 .. w_{k-1} of the Chebyshev smoother of order k for the
+// eigenvalue interval [lo, hi] of D^-1 A: the residual polynomial is
+// r(l) = T_k((th - l) / de) / T_k(th / de), th = (hi + lo) / 2, de = (hi - lo) / 2, T_k the
+// Chebyshev polynomial of the first kind (the polynomial smoother of Adams, Brezina, Hu and
+// Tuminaro, J. Comput. Phys. 188 (2003)), and x += p(D^-1 A) D^-1 r with
+// 1 - l p(l) = r(l). The polynomials are expanded with the three-term recurrence.
+void chebyshevCoefficients( int order, double lo, double hi, std::vector< double >& w )
+{
+   const double th = 0.5 * ( hi + lo ), de = 0.5 * ( hi - lo );
+   // s(l) = a + c l
+   const double a = th / de, c = -1.0 / de;
+   std::vector< double > tm( order + 1, 0.0 ), tc( order + 1, 0.0 ), tn( order + 1, 0.0 );
+   tm[0] = 1.0;          // T_0
+   tc[0] = a, tc[1] = c; // T_1
+   if ( order == 1 )
+      tn = tc;
+   for ( int n = 1; n < order; ++n )
+   {
+      std::fill( tn.begin(), tn.end(), 0.0 );
+      for ( int i = 0; i <= n; ++i )
+      {
+         tn[i] += 2 * a * tc[i];
+         tn[i + 1] += 2 * c * tc[i];
+      }
+      for ( int i = 0; i <= n; ++i )
+         tn[i] -= tm[i];
+      tm = tc;
+      tc = tn;
+   }
+   const double t0 = tn[0]; // T_k(th / de) = r's value at 0 before scaling
+   w.assign( order, 0.0 );
+   for ( int i = 1; i <= order; ++i )
+      w[i - 1] = -tn[i] / t0;
+}
+
 template < typename T >
 struct Hier
 {
@@ -981,6 +1067,7 @@ void smoothT( const Oracle& o, const GmgCfg& g, int level, T* x, const T* b )
       sorRefT( o, op, lv, x, b, T( g.relax ), flag, false );
       sorRefT( o, op, lv, x, b, T( g.relax ), flag, true );
       break;
+   case 5: chebyshevT( o, op, lv, x, b, o.cheb ); break;
    default:
       sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m, false );
       sorColoredT( o, op, lv, x, b, T( g.relax ), flag, g.labels, g.m, true );
@@ -1214,6 +1301,60 @@ void orc_prolongate( void* h, int coarseLevel, const double* coarse, double* fin
 void orc_restrict( void* h, int fineLevel, const double* fine, double* coarse, int flag )
 {
    restrictT( *H( h ), fineLevel, fine, coarse, flag );
+}
+
+void orc_chebyshev_coefficients( int order, double lower, double upper, double* out )
+{
+   std::vector< double > w;
+   chebyshevCoefficients( order, lower, upper, w );
+   std::copy( w.begin(), w.end(), out );
+}
+
+void orc_set_chebyshev( void* h, int order, double lower, double upper )
+{
+   chebyshevCoefficients( order, lower, upper, H( h )->cheb );
+}
+
+void orc_inv_diag( void* h, int op, int level, double* out )
+{
+   auto* o = H( h );
+   invDiagT( *o, o->ops[op], o->lv[level], out );
+}
+
+void orc_smooth_chebyshev( void* h, int op, int level, double* x, const double* b )
+{
+   auto* o = H( h );
+   chebyshevT( *o, o->ops[op], o->lv[level], x, b, o->cheb );
+}
+
+// estimateSpectralRadiusWithPowerIteration (src/hyteg/numerictools/SpectrumEstimation.hpp:57-81)
+// on D^-1 A (chebyshev::estimateRadius), flag All; x is the start vector and is overwritten
+double orc_spectral_radius( void* h, int op, int level, int iterations, double* x )
+{
+   auto*        o  = H( h );
+   const Op&    A  = o->ops[op];
+   const Level& lv = o->lv[level];
+   std::vector< double > inv( lv.nDof ), ax( lv.nDof );
+   invDiagT( *o, A, lv, inv.data() );
+   auto opApply = [&]( const double* src, double* dst ) {
+      applyT( *o, A, lv, src, dst, ORC_ALL, false );
+      for ( i64 d = 0; d < lv.nDof; ++d )
+         dst[d] *= inv[d];
+   };
+   double norm = std::sqrt( dotT( lv, x, x, ORC_ALL ) );
+   for ( i64 d = 0; d < lv.nDof; ++d )
+      x[d] /= norm;
+   opApply( x, ax.data() );
+   double radius = 0;
+   for ( int it = 1; it <= iterations; ++it )
+   {
+      norm = std::sqrt( dotT( lv, ax.data(), ax.data(), ORC_ALL ) );
+      for ( i64 d = 0; d < lv.nDof; ++d )
+         x[d] = ax[d] / norm;
+      opApply( x, ax.data() );
+      radius = dotT( lv, x, ax.data(), ORC_ALL );
+   }
+   return radius;
 }
 
 double orc_dot( void* h, int level, const double* a, const double* b, int flag )

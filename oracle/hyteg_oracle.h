@@ -54,11 +54,20 @@ void   orc_jacobi( void* h, int op, int level, double* x, const double* b, doubl
 void   orc_prolongate( void* h, int coarseLevel, const double* coarse, double* fine, int flag, int add );
 void   orc_restrict( void* h, int fineLevel, const double* fine, double* coarse, int flag );
 double orc_dot( void* h, int level, const double* a, const double* b, int flag );
+// ChebyshevSmoother: power-basis coefficients of order 1..5 for the eigenvalue interval
+// [lower, upper] of D^-1 A (setupCoefficients), the smoother step, diag(A)^-1, and
+// chebyshev::estimateRadius (power iteration on D^-1 A, flag All; x = start vector)
+void   orc_chebyshev_coefficients( int order, double lower, double upper, double* out );
+void   orc_set_chebyshev( void* h, int order, double lower, double upper );
+void   orc_smooth_chebyshev( void* h, int op, int level, double* x, const double* b );
+void   orc_inv_diag( void* h, int op, int level, double* out );
+double orc_spectral_radius( void* h, int op, int level, int iterations, double* x );
 int    orc_cg( void* h, int op, int level, double* x, const double* b, double tol, int maxIter );
 
 // V-cycle GMG (src/hyteg/solvers/GeometricMultigridSolver.hpp:127-235).
 // smoother: 0 = reference-order SOR, 1 = multicolour SOR (labels, m), 2 = weighted Jacobi,
-// 3 = reference-order symmetric SOR, 4 = multicolour symmetric SOR (SymmetricSORSmoother).
+// 3 = reference-order symmetric SOR, 4 = multicolour symmetric SOR (SymmetricSORSmoother),
+// 5 = Chebyshev (ChebyshevSmoother, coefficients from orc_set_chebyshev).
 // cycleType: 0 = V-cycle, 1 = W-cycle.
 // precision: 64 = plain FP64 cycles; 32 = FP32 inner V-cycles inside FP64 iterative refinement.
 // Runs until ||b-Ax||/||b|| <= relTol (Inner|Neumann DoFs) or maxCycles; history[k] =

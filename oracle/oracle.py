@@ -62,6 +62,12 @@ def lib():
         L.orc_dot.argtypes = [P, I, P, P, I]
         L.orc_cg.restype = I
         L.orc_cg.argtypes = [P, I, I, P, P, D, I]
+        L.orc_chebyshev_coefficients.argtypes = [I, D, D, P]
+        L.orc_set_chebyshev.argtypes = [P, I, D, D]
+        L.orc_smooth_chebyshev.argtypes = [P, I, I, P, P]
+        L.orc_inv_diag.argtypes = [P, I, I, P]
+        L.orc_spectral_radius.restype = D
+        L.orc_spectral_radius.argtypes = [P, I, I, I, P]
         L.orc_gmg_solve.restype = I
         L.orc_gmg_solve.argtypes = [P, I, I, I, P, P, I, I, D, I, P, I, D, I, D, I, P, I]
         _lib = L
@@ -131,6 +137,21 @@ class Oracle:
                               _p(lab), m, int(backwards))
         return x
 
+    def set_chebyshev(self, order, lower, upper):
+        lib().orc_set_chebyshev(self.h, order, lower, upper)
+
+    def smooth_chebyshev(self, x, b, level, op=0):
+        lib().orc_smooth_chebyshev(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)))
+        return x
+
+    def inv_diag(self, level, op=0):
+        out = np.zeros(self.n(level))
+        lib().orc_inv_diag(self.h, op, level, _p(out))
+        return out
+
+    def spectral_radius(self, level, iterations, x, op=0):
+        return lib().orc_spectral_radius(self.h, op, level, iterations, _p(x))
+
     def jacobi(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0):
         lib().orc_jacobi(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), relax, flag)
         return x
@@ -169,6 +190,12 @@ class Oracle:
 # Reference kernels compiled from the reference tree (oracle/_ref), for pinning
 # ---------------------------------------------------------------------------
 _ref = None
+
+
+def chebyshev_coefficients(order, lower, upper):
+    out = np.zeros(order)
+    lib().orc_chebyshev_coefficients(order, lower, upper, _p(out))
+    return out
 
 
 def ref_lib():

@@ -534,3 +534,61 @@ def test_w_cycle_symmetric_sor_to_tolerance(H, oracle_mod, setups, precision):
     orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=60, rel_tol=1e-13)
     err = np.abs(fx.get(L) - x).max() / np.abs(x).max()
     assert err < 1e-6, err
+
+
+def test_spectral_radius_estimate_matches_oracle(H, oracle_mod, setups):
+    """chebyshev::estimateRadius: the same power iteration on D^-1 A from the same start vector."""
+    st, orc, L = setups["cube211"]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    x0 = np.random.default_rng(12).uniform(0, 1, orc.n(L))
+    fx, ft = H.P1Function("x", st, 0, L), H.P1Function("t", st, 0, L)
+    fx.set(x0, L)
+    rho = A.estimate_spectral_radius(fx, ft, L, 25)
+    rho_ref = orc.spectral_radius(L, 25, x0.copy())
+    assert abs(rho - rho_ref) <= 1e-10 * rho_ref, (rho, rho_ref)
+
+
+@pytest.mark.parametrize("name", ["octahedron", "cube1", "cube211"])
+@pytest.mark.parametrize("order", [1, 3])
+def test_chebyshev_vcycle_matches_oracle(H, oracle_mod, setups, name, order):
+    """V(2,2) cycles with ChebyshevSmoother (the launched levels compute D^-1 once per level)
+    == the oracle's cycles with the same coefficients."""
+    O = oracle_mod
+    st, orc, L = setups[name]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    b = O.uniform_rhs(orc.coords_of(L), 0, 1 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fx.set(np.zeros(orc.n(L)), L)
+    fb.set(b, L)
+    rho = 1.9
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, smoother=H.SMOOTHER_CHEBYSHEV, coarse_tol=1e-14)
+    gmg.setup_chebyshev(order, rho)
+    orc.set_chebyshev(order, 0.3 * rho, 1.2 * rho)
+    x = np.zeros(orc.n(L))
+    for _ in range(2):
+        gmg.solve(fx, fb, L)
+        fb.set(b, L)
+        orc.gmg(x, b, 0, L, pre=2, post=2, smoother=5, coarse_tol=1e-14, max_cycles=1)
+        close(fx.get(L), x, 1e-10)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_chebyshev_solve_to_tolerance(H, oracle_mod, setups, precision):
+    """Chebyshev-smoothed cycles (order 3, radius from the GPU's own estimate) reach 1e-8,
+    FP64 and FP32-inner, and the solution matches the oracle's FP64 solve."""
+    O = oracle_mod
+    st, orc, L = setups["cube211"]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    fx, ft = H.P1Function("x", st, 0, L), H.P1Function("t", st, 0, L)
+    fx.set(np.random.default_rng(3).uniform(0, 1, orc.n(L)), L)
+    rho = A.estimate_spectral_radius(fx, ft, L, 30)
+    b = O.uniform_rhs(orc.coords_of(L), 0, 1 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, smoother=H.SMOOTHER_CHEBYSHEV)
+    gmg.setup_chebyshev(3, rho)
+    hist = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=40, precision=precision)
+    assert hist[-1] <= 1e-8, hist
+    x = np.zeros(orc.n(L))
+    orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=60, rel_tol=1e-13)
+    assert np.abs(fx.get(L) - x).max() / np.abs(x).max() < 1e-6

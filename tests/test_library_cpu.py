@@ -351,3 +351,23 @@ def test_mesh_primitive_counts_match_footprint_formula(tmp_path, kind, shape):
                          check=True).stdout.split()
     nV, nE, nF, nC = map(int, out)
     assert (nV, nE, nF) == mesh_primitives(*shape, mesh=kind)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
+def test_chebyshev_coefficients(lib, oracle_mod, order):
+    """ChebyshevSmoother::setupCoefficients: the product's power-basis coefficients equal the
+    oracle's, and 1 - l p(l) is the scaled Chebyshev polynomial T_k((th - l)/de)/T_k(th/de)
+    on the eigenvalue interval (host code, no device call)."""
+    import hyteg_b200 as H
+
+    rho = 1.7
+    lo, hi = 0.3 * rho, 1.2 * rho
+    w = H.chebyshev_coefficients(order, lo, hi)
+    np.testing.assert_allclose(w, oracle_mod.chebyshev_coefficients(order, lo, hi), rtol=1e-14)
+    th, de = (hi + lo) / 2, (hi - lo) / 2
+    lam = np.linspace(0.0, hi, 11)
+    r = 1 - lam * np.polyval(w[::-1], lam)
+    Tk = np.polynomial.chebyshev.Chebyshev.basis(order)
+    np.testing.assert_allclose(r, Tk((th - lam) / de) / Tk(th / de), atol=1e-12)
+    with pytest.raises(H.HybError):
+        H.chebyshev_coefficients(6, lo, hi)

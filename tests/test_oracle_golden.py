@@ -233,3 +233,25 @@ def test_gmg_convergence_symmetric_sor_and_w_cycles(oracle_mod, smoother, cycle)
         rates[cyc] = (hist[1:] / hist[:-1]) ** 2
         assert np.all(rates[cyc] < 3.2e-2), (cyc, rates[cyc])
     assert rates[cycle].max() <= rates["V"].max() * (1 + 1e-9)
+
+
+@pytest.mark.parametrize("order", [2, 3, 4])
+def test_gmg_convergence_chebyshev(oracle_mod, order):
+    """ChebyshevSmoother in the P1GMG3DConvergenceTest.cpp setting (regular_octahedron_8el,
+    levels 0..3, V(3,3)): coefficients from the power-iteration estimate of D^-1 A's spectral
+    radius (chebyshev::estimateRadius, [0.3 rho, 1.2 rho]); the estimate lies in the
+    interval's admissible range, and every cycle reduces the residual."""
+    O = oracle_mod
+    g = np.load(os.path.join(GOLD, "reference_meshes.npz"))
+    o = O.Oracle(g["regular_octahedron_8el_coords"], g["regular_octahedron_8el_tets"], 3)
+    rho = o.spectral_radius(3, 40, np.random.default_rng(1).uniform(0, 1, o.n(3)))
+    assert 1.0 < rho < 2.5  # D^-1 A of the P1 Laplacian: spectrum in (0, 2] plus boundary rows
+    o.set_chebyshev(order, 0.3 * rho, 1.2 * rho)
+    xyz = o.coords_of(3)
+    kind, bc = o.info(3)
+    x = np.random.default_rng(0).uniform(0, 1, o.n(3))
+    exact = np.sin(xyz[:, 0]) * np.sinh(xyz[:, 1]) * xyz[:, 2]
+    x[bc == O.DIRICHLET] = exact[bc == O.DIRICHLET]
+    _, hist = o.gmg(x, np.zeros(o.n(3)), 0, 3, pre=3, post=3, smoother=5, max_cycles=4)
+    ratios = hist[1:] / hist[:-1]
+    assert np.all(ratios < 0.1), ratios
