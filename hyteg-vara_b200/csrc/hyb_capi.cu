@@ -1569,12 +1569,13 @@ void launchProgram( Gmg& g, Function& x, Function& b, int top, cudaStream_t stre
       if ( p->x == &x && p->b == &b && p->dtype == dtype && p->top == top )
          prog = p.get();
    require( prog != nullptr, "program of the coarse V-cycle was not recorded" );
-   const Phase* ph = prog->phases.p;
-   const auto*  lt = (const LevelDev*) g.st->lvTable.p;
+   const Phase* ph  = prog->phases.p;
+   const auto*  lt  = (const LevelDev*) g.st->lvTable.p;
+   const int    nLv = int( g.st->lvTable.n );
    if ( g.op->variable )
-      pdlLaunch( k_program< T, true >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n );
+      pdlLaunch( k_program< T, true >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n, nLv );
    else
-      pdlLaunch( k_program< T, false >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n );
+      pdlLaunch( k_program< T, false >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n, nLv );
    HYB_CHECK_LAUNCH();
 }
 

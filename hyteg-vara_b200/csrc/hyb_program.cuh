@@ -66,18 +66,40 @@ __device__ __forceinline__ const OpDev< double >& phaseOp< double >( const Phase
 
 constexpr int kProgramThreads = 512;
 
+constexpr int kProgramLevels = 8; // level descriptors staged in shared memory
+
+// The phase descriptors are staged in shared memory one phase ahead (each thread of the
+// first warps loads one 8-byte word of the next descriptor while the current phase runs),
+// and the level descriptors once per launch: a phase then starts without a dependent L2
+// round trip for its own description.
 template < typename T, bool VAR >
 __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, const LevelDev* __restrict__ lvs,
-                                                                const Phase* __restrict__ prog, int nPhases )
+                                                                const Phase* __restrict__ prog, int nPhases, int nLv )
 {
+   static_assert( sizeof( Phase ) % 8 == 0 && sizeof( Phase ) / 8 <= kProgramThreads, "phase staging" );
+   static_assert( sizeof( LevelDev ) % 4 == 0 && sizeof( LevelDev ) / 4 <= kProgramThreads, "level staging" );
+   constexpr int       nWords = int( sizeof( Phase ) / 8 );
+   __shared__ double   red[32];
+   __shared__ Phase    sP[2];
+   __shared__ LevelDev sL[kProgramLevels];
    HYB_PDL_PROLOGUE();
-   __shared__ double red[32];
+   for ( int l = 0; l < kProgramLevels && l < nLv; ++l )
+      if ( threadIdx.x < sizeof( LevelDev ) / 4 )
+         reinterpret_cast< int* >( &sL[l] )[threadIdx.x] = reinterpret_cast< const int* >( lvs + l )[threadIdx.x];
+   if ( nPhases > 0 && threadIdx.x < nWords )
+      reinterpret_cast< unsigned long long* >( &sP[0] )[threadIdx.x] =
+          reinterpret_cast< const unsigned long long* >( prog )[threadIdx.x];
+   __syncthreads();
+   auto levelAt = [&]( int l ) -> const LevelDev& { return l < kProgramLevels ? sL[l] : lvs[l]; };
    for ( int ph = 0; ph < nPhases; ++ph )
    {
-      const Phase&   P      = prog[ph];
+      unsigned long long next = 0;
+      if ( ph + 1 < nPhases && threadIdx.x < nWords )
+         next = reinterpret_cast< const unsigned long long* >( prog + ph + 1 )[threadIdx.x];
+      const Phase&   P      = sP[ph & 1];
       const int      kind   = P.kind;
       const int      blocks = P.blocks;
-      const LevelDev lv     = lvs[P.level];
+      const LevelDev lv     = levelAt( P.level );
       for ( int b = int( blockIdx.x ); b < blocks; b += int( gridDim.x ) )
       {
          const Blk       vb{ b, blocks };
@@ -118,13 +140,13 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
             break;
          case kPhRestrict:
          {
-            const LevelDev& F = lvs[P.level + 1];
+            const LevelDev& F = levelAt( P.level + 1 );
             restrictBody< T >( vb, tp, lv, F.W, F.stride, (const T*) P.p0, (T*) P.p1, P.flag, P.cellBlocks );
             break;
          }
          case kPhProlongAdd:
          {
-            const LevelDev& C = lvs[P.level - 1];
+            const LevelDev& C = levelAt( P.level - 1 );
             prolongateBody< T, true >( vb, tp, lv, C.W, C.stride, (const T*) P.p0, (T*) P.p1, P.flag, P.cellBlocks );
             break;
          }
@@ -147,6 +169,10 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
          default: break;
          }
       }
+      // the next descriptor goes into the buffer the previous phase used (all threads have
+      // left that phase at the last barrier)
+      if ( ph + 1 < nPhases && threadIdx.x < nWords )
+         reinterpret_cast< unsigned long long* >( &sP[( ph + 1 ) & 1] )[threadIdx.x] = next;
       __syncthreads();
    }
 }
