@@ -115,7 +115,7 @@ inline cudaStream_t S( void* s ) { return reinterpret_cast< cudaStream_t >( s );
 // ---------------------------------------------------------------------------
 // Storage
 // ---------------------------------------------------------------------------
-// Row tables of a small level (SlabRow, constant operator): the surface lanes of each SOR
+// Row tables of a small level (SlabRow, any operator of the storage): the surface lanes of each SOR
 // colour, the interior points of each interior colour (cell-major), and all DoFs (the
 // surface lanes of the full lists, then every interior point) for residuals and CG.
 struct RowTables
@@ -918,18 +918,29 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
    if ( nb == 0 )
       return;
    const OpDev< T > od = op.dev< T >( l );
-   if ( !op.variable && ( mode == kResidual || mode == kReplace ) )
+   if ( mode == kResidual || mode == kReplace )
       if ( const RowTables* R = rowsIf( s, l ); R && R->full )
       {
          // small and middle levels: the precomputed rows (residual r = b - A u, or r = A u)
          const RowPass rp = rowPassAll( R );
          const int     g  = int( std::max< long >( 1, std::min< long >( ( rp.n + 127 ) / 128, long( s.numSMs ) * 8 ) ) );
+         T*            u  = const_cast< T* >( src );
+#define HYB_ROWS( M, V ) pdlLaunch( k_row_pass< T, M, V >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag )
          if ( mode == kResidual )
-            pdlLaunch( k_row_pass< T, kRowResidual >, dim3( g ), dim3( 128 ), 0, stream, rp, od.st, const_cast< T* >( src ),
-                       rhs, dst, T( 0 ), flag );
+         {
+            if ( op.variable )
+               HYB_ROWS( kRowResidual, true );
+            else
+               HYB_ROWS( kRowResidual, false );
+         }
          else
-            pdlLaunch( k_row_pass< T, kRowApply >, dim3( g ), dim3( 128 ), 0, stream, rp, od.st, const_cast< T* >( src ),
-                       rhs, dst, T( 0 ), flag );
+         {
+            if ( op.variable )
+               HYB_ROWS( kRowApply, true );
+            else
+               HYB_ROWS( kRowApply, false );
+         }
+#undef HYB_ROWS
          HYB_CHECK_LAUNCH();
          return;
       }
@@ -970,7 +981,7 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
    const auto&      L  = s.L( l );
    const OpDev< T > od = op.dev< T >( l );
    // interface passes: one launch per colour over that colour's surface DoFs
-   const RowTables* R = op.variable ? nullptr : rowsIf( s, l );
+   const RowTables* R = rowsIf( s, l );
    auto iface = [&]( int c ) {
       const int* co = &L.colourOff[4 * c];
       const long lanes = bdryLaneCount( co[1], co[2], co[3] );
@@ -980,9 +991,13 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       if ( R )
       {
          const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
-         pdlLaunch( k_row_pass< T, kRowSor >, dim3( nb ), dim3( 128 ), 0, stream,
-                    RowPass{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes }, od.st, u, rhs, (T*) nullptr,
-                    relax, flag );
+         const RowPass rp{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes };
+         if ( op.variable )
+            pdlLaunch( k_row_pass< T, kRowSor, true >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs, (T*) nullptr,
+                       relax, flag );
+         else
+            pdlLaunch( k_row_pass< T, kRowSor, false >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs, (T*) nullptr,
+                       relax, flag );
          HYB_CHECK_LAUNCH();
          return;
       }
@@ -1157,7 +1172,7 @@ void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch&
       cs.status.alloc( 4 );
    }
    const OpDev< double > od = op.dev< double >( l );
-   const RowPass         rp = op.variable ? RowPass{ nullptr, 0, 0, 0, 0 } : rowPassAll( rowsIf( s, l ) );
+   const RowPass         rp = rowPassAll( rowsIf( s, l ) );
    if ( op.variable )
       pdlLaunch( k_cg< true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
@@ -1368,7 +1383,7 @@ struct PhaseList
    // the row table of level l for the passes of this (constant) operator, built on first use
    const RowTables* rows( int l ) const
    {
-      const RowTables* R = g.op->variable ? nullptr : ensureRows( *g.st, l );
+      const RowTables* R = ensureRows( *g.st, l );
       return R && R->full ? R : nullptr;
    }
    int  flatBlocks( long n ) const
@@ -1677,9 +1692,8 @@ void ensureChebyshev( Gmg& g )
 void prepare( Gmg& g )
 {
    ensureChebyshev( g );
-   if ( !g.op->variable )
-      for ( int l = g.minL; l <= g.maxL; ++l )
-         ensureRows( *g.st, l );
+   for ( int l = g.minL; l <= g.maxL; ++l )
+      ensureRows( *g.st, l );
    if ( !g.cg.r )
    {
       g.cg.r.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );

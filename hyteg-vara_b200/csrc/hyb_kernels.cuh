@@ -402,7 +402,7 @@ struct PointBatch
 };
 
 // ---------------------------------------------------------------------------
-// Row tables of small levels (constant operator). On coarse levels a pass has little
+// Row tables of small levels. On coarse levels a pass has little
 // work, and its time is the length of one lane's dependent chain: the DoF from the list,
 // its embedding, class and stencil positions, then the loads. A row table stores the end
 // of that chain per lane -- the cell, the partial-stencil class, the DoF's boundary flag
@@ -509,9 +509,11 @@ enum RowMode : int
 };
 
 // one pass over the rows, lanes start, start + step, ... (start - lane and step multiples
-// of 32; the rows of one DoF are adjacent lanes of one warp)
-template < typename T, int MODE >
-__device__ __forceinline__ void rowPassBody( const RowPass& rp, const T* __restrict__ st, T* u, const T* b, T* r, T relax,
+// of 32; the rows of one DoF are adjacent lanes of one warp). Constant operator: the
+// partial stencil st[wsel + q]; variable operator: the row's positions drive the
+// incident micro-tets' matrices and nodal coefficients (the variable branch of partialRow).
+template < typename T, int MODE, bool VAR >
+__device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >& op, T* u, const T* b, T* r, T relax,
                                              int flag, long long start, long long step )
 {
    for ( long long gt = start; gt - ( threadIdx.x & 31 ) < rp.n; gt += step )
@@ -529,16 +531,44 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const T* __restr
       if ( active )
       {
          const T*       uc    = u + A.x;
-         const T*       w     = st + A.y;
          const uint32_t valid = uint32_t( A.z ) & 0xffffu;
          // pos[q] of the row: 16-bit halves of A.w, B.xyzw, C.xyz
          const uint32_t h[8] = { uint32_t( A.w ), uint32_t( B.x ), uint32_t( B.y ), uint32_t( B.z ),
                                  uint32_t( B.w ), uint32_t( C.x ), uint32_t( C.y ), uint32_t( C.z ) };
-         diag += w[0];
+         auto           pos  = [&]( int q ) { return int( ( q & 1 ) ? ( h[q >> 1] >> 16 ) : ( h[q >> 1] & 0xffffu ) ); };
+         if constexpr ( !VAR )
+         {
+            const T* w = op.st + A.y;
+            diag += w[0];
 #pragma unroll
-         for ( int q = 1; q < 15; ++q )
-            if ( valid & ( 1u << q ) )
-               off += w[q] * uc[( q & 1 ) ? ( h[q >> 1] >> 16 ) : ( h[q >> 1] & 0xffffu )];
+            for ( int q = 1; q < 15; ++q )
+               if ( valid & ( 1u << q ) )
+                  off += w[q] * uc[pos( q )];
+         }
+         else
+         {
+            const int      cls    = ( A.y / 15 ) & 15, cell = A.y / 240;
+            const T*       kv     = op.kap + A.x;
+            const T*       K      = op.K + size_t( cell ) * 96;
+            const uint32_t validT = kValidTets[cls];
+#pragma unroll
+            for ( int i = 0; i < 24; ++i )
+            {
+               const IncidentTet it = incidentTet( i );
+               if ( !( validT & ( 1u << i ) ) )
+                  continue;
+               const T  ks = kv[pos( it.q[0] )] + kv[pos( it.q[1] )] + kv[pos( it.q[2] )] + kv[pos( it.q[3] )];
+               const T* Kr = K + it.t * 16 + it.k * 4;
+#pragma unroll
+               for ( int j = 0; j < 4; ++j )
+               {
+                  if ( j == it.k )
+                     diag += ks * Kr[j];
+                  else
+                     off += ks * Kr[j] * uc[pos( it.q[j] )];
+               }
+            }
+         }
       }
       const int G = gt < rp.b1 ? 32 : gt < rp.b2 ? 8 : gt < rp.b3 ? 2 : 1;
       diag        = groupSum( diag, G );
@@ -556,13 +586,12 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const T* __restr
 }
 
 // a row pass as its own launch (levels between the program kernel's and the large ones)
-template < typename T, int MODE >
-__global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, const T* __restrict__ st, T* u, const T* b, T* r, T relax,
-                                                     int flag )
+template < typename T, int MODE, bool VAR >
+__global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, OpDev< T > op, T* u, const T* b, T* r, T relax, int flag )
 {
    HYB_PDL_PROLOGUE();
-   rowPassBody< T, MODE >( rp, st, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
-                           (long long) gridDim.x * blockDim.x );
+   rowPassBody< T, MODE, VAR >( rp, op, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
+                                (long long) gridDim.x * blockDim.x );
 }
 
 // Constant-stencil quad: the points x = 4g + r, r = 0..3, of row (y, z). Each of the seven
@@ -1502,8 +1531,8 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
    // the operator through the level's row table when there is one
    auto applyA = [&]( const double* src, double* dst ) {
       if ( rp.rows )
-         rowPassBody< double, kRowApply >( rp, op.st, const_cast< double* >( src ), nullptr, dst, 0.0, flag, threadIdx.x,
-                                           blockDim.x );
+         rowPassBody< double, kRowApply, VAR >( rp, op, const_cast< double* >( src ), nullptr, dst, 0.0, flag,
+                                                threadIdx.x, blockDim.x );
       else
          cgApplyAll< VAR >( tp, lv, op, src, dst, flag );
    };

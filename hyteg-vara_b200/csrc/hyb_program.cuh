@@ -108,16 +108,16 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
          {
          case kPhSorIface:
             if ( P.rp.rows )
-               rowPassBody< T, kRowSor >( P.rp, phaseOp< T >( P ).st, (T*) P.p0, (const T*) P.p1, nullptr, T( P.relax ),
-                                          P.flag, threadIdx.x, blockDim.x );
+               rowPassBody< T, kRowSor, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, nullptr,
+                                               T( P.relax ), P.flag, threadIdx.x, blockDim.x );
             else
                sorIfaceBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.flag,
                                        P.bl );
             break;
          case kPhSorInterior:
             if ( P.rp.rows )
-               rowPassBody< T, kRowSor >( P.rp, phaseOp< T >( P ).st, (T*) P.p0, (const T*) P.p1, nullptr, T( P.relax ),
-                                          0xff, threadIdx.x, blockDim.x );
+               rowPassBody< T, kRowSor, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, nullptr,
+                                               T( P.relax ), 0xff, threadIdx.x, blockDim.x );
             else
                sorInteriorBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.a0,
                                           P.a1, P.a2, P.cellBlocks );
@@ -132,8 +132,8 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
             break;
          case kPhResidual:
             if ( P.rp.rows )
-               rowPassBody< T, kRowResidual >( P.rp, phaseOp< T >( P ).st, (T*) P.p0, (const T*) P.p2, (T*) P.p1, T( 0 ),
-                                               P.flag, threadIdx.x, blockDim.x );
+               rowPassBody< T, kRowResidual, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p2, (T*) P.p1,
+                                                    T( 0 ), P.flag, threadIdx.x, blockDim.x );
             else
                applyBody< T, VAR, kResidual >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1,
                                                (const T*) P.p2, P.flag, P.cellBlocks );

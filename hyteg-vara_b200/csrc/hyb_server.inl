@@ -58,28 +58,6 @@ struct ServeKey
    {
       return mesh == HYB_MESH_SHELL ? 60l * ( nx - 1 ) * ( nx - 1 ) * ( ny - 1 ) : 6l * nx * ny * nz;
    }
-   // macro-vertices, -edges and -faces of the mesh. Cuboid (6 tets per cube): the grid's
-   // vertices and edges, one diagonal per grid face and per cube, two triangles per grid face
-   // and 6 inner triangles per cube. Shell (prisms between icosahedral spheres, 3 tets each):
-   // per sphere 10n^2+2 vertices, 30n^2 edges, 20n^2 triangles (n = ntan - 1); per layer gap
-   // a radial edge per sphere vertex and a diagonal per quad face (one per sphere edge), two
-   // triangles per quad face and two inner triangles per prism.
-   void primitives( long& nV, long& nE, long& nF ) const
-   {
-      if ( mesh == HYB_MESH_SHELL )
-      {
-         const long n = nx - 1, vs = 10 * n * n + 2, es = 30 * n * n, fs = 20 * n * n, gaps = ny - 1;
-         nV             = ny * vs;
-         nE             = ny * es + gaps * ( vs + es );
-         nF             = ny * fs + gaps * ( 2 * es + 2 * fs );
-         return;
-      }
-      const long X = nx, Y = ny, Z = nz;
-      const long gridFaces = X * Y * ( Z + 1 ) + X * ( Y + 1 ) * Z + ( X + 1 ) * Y * Z;
-      nV = ( X + 1 ) * ( Y + 1 ) * ( Z + 1 );
-      nE = X * ( Y + 1 ) * ( Z + 1 ) + ( X + 1 ) * Y * ( Z + 1 ) + ( X + 1 ) * ( Y + 1 ) * Z + gridFaces + X * Y * Z;
-      nF = 2 * gridFaces + 6 * X * Y * Z;
-   }
    bool operator==( const ServeKey& o ) const
    {
       return sameMesh( o ) && level == o.level && coeff == o.coeff && precision == o.precision;
@@ -133,31 +111,6 @@ size_t serveFootprint( const ServeKey& k, int meshMaxLevel )
    // an allowance of 64 KiB per level for the recorded phase list of the coarse-level
    // program kernel
    bytes += size_t( k.level + 1 ) * 65536;
-   // row tables (constant coefficient): the surface lanes of the mesh's primitives (32 per
-   // vertex, 8 per edge point, 2 per face point), each colour's edge and face ranges padded
-   // to whole warps (at most 16 colours); full tables on the small levels, the surface
-   // colours' rows only on the larger ones
-   if ( k.coeff == HYB_COEFF_CONSTANT )
-   {
-      long nV, nE, nF;
-      k.primitives( nV, nE, nF );
-      for ( int l = 0; l <= k.level; ++l )
-      {
-         const size_t N      = size_t( 1 ) << l;
-         const size_t S      = ( N + 1 ) * ( N + 2 ) * ( N + 3 ) / 6;
-         const long   points = long( nC * size_t( stridePad( int( S ) ) ) );
-         if ( points > std::max( rowTableMaxPoints(), rowIfaceMaxPoints() ) || stridePad( int( S ) ) >= 65536 )
-            continue;
-         const size_t nIntFace = N >= 3 ? ( N - 1 ) * ( N - 2 ) / 2 : 0;
-         const size_t nPts     = N >= 4 ? ( N - 1 ) * ( N - 2 ) * ( N - 3 ) / 6 : 0;
-         const size_t lanes    = 32 * size_t( nV ) + 8 * size_t( nE ) * ( N - 1 ) + 2 * size_t( nF ) * nIntFace;
-         const size_t iface    = lanes + 16 * 62;
-         if ( points <= rowTableMaxPoints() )
-            bytes += sizeof( SlabRow ) * ( iface + lanes + 62 + 2 * nC * nPts );
-         else
-            bytes += sizeof( SlabRow ) * iface;
-      }
-   }
    return bytes;
 }
 
@@ -265,6 +218,9 @@ struct Server
       m->st = std::make_unique< Storage >();
       buildStorage( *m->st, V, T, maxLevel );
       m->laplace.reset( makeLaplace( m->st.get(), 0, maxLevel ) );
+      // the mesh's row tables (shared by every hierarchy on it) belong to the mesh's bytes
+      for ( int l = 0; l <= maxLevel; ++l )
+         ensureRows( *m->st, l );
       m->bytes = size_t( g_deviceBytes.load() - before );
       account( (long long) m->bytes );
       meshes.push_back( std::move( m ) );
@@ -678,6 +634,17 @@ int hyb_server_stats( const hyb_server* s, size_t* peak, int* built, int* graphs
       *built = s->built;
    if ( graphs )
       *graphs = s->graphsCaptured();
+   HYB_API_END
+}
+
+int hyb_server_mesh_bytes( const hyb_server* s, size_t* bytes )
+{
+   HYB_API_BEGIN
+   require( s && bytes, "null argument" );
+   size_t sum = 0;
+   for ( auto& m : s->meshes )
+      sum += m->bytes;
+   *bytes = sum;
    HYB_API_END
 }
 

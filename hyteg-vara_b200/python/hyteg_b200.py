@@ -36,7 +36,7 @@ SYMBOLS = [
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
     "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
-    "hyb_chebyshev_coefficients", "hyb_operator_estimate_spectral_radius",
+    "hyb_chebyshev_coefficients", "hyb_operator_estimate_spectral_radius", "hyb_server_mesh_bytes",
 ]
 
 COEFF_CONSTANT, COEFF_LOGNORMAL, COEFF_RADIAL = 0, 1, 2
@@ -122,6 +122,7 @@ def load(path=LIB_PATH):
         "hyb_gmg_setup_chebyshev": (I, [P, I, D, D]),
         "hyb_chebyshev_coefficients": (I, [I, D, D, P]),
         "hyb_operator_estimate_spectral_radius": (I, [P, P, P, I, I, P]),
+        "hyb_server_mesh_bytes": (I, [P, P]),
         "hyb_server_create": (I, [ctypes.c_size_t, I, I, PP]),
         "hyb_server_destroy": (I, [P]),
         "hyb_server_footprint": (I, [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
@@ -540,4 +541,7 @@ class Server:
     def stats(self):
         peak, built, graphs = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int()
         _check(load().hyb_server_stats(self.h, ctypes.byref(peak), ctypes.byref(built), ctypes.byref(graphs)))
-        return {"peak_bytes": peak.value, "hierarchies_built": built.value, "graphs_captured": graphs.value}
+        mesh = ctypes.c_size_t()
+        _check(load().hyb_server_mesh_bytes(self.h, ctypes.byref(mesh)))
+        return {"peak_bytes": peak.value, "hierarchies_built": built.value, "graphs_captured": graphs.value,
+                "mesh_bytes": mesh.value}

@@ -308,6 +308,9 @@ int hyb_server_run( hyb_server* s, double time_limit_s );
 int hyb_server_result( const hyb_server* s, int id, hyb_request_result* out );
 /* peak device bytes held by the server, hierarchies built, graphs captured */
 int hyb_server_stats( const hyb_server* s, size_t* peak_bytes, int* hierarchies_built, int* graphs_captured );
+/* device bytes of the meshes the server holds (storage, Laplace operator, row tables),
+ * which are never evicted and are not part of a request's footprint */
+int hyb_server_mesh_bytes( const hyb_server* s, size_t* bytes );
 /* The random Fourier features the server draws for a lognormal request of this seed:
  * w (modes x 3) ~ N(0, 1/corr_len^2), phase (modes) ~ U[0, 2 pi), from a SplitMix64
  * stream and the Box-Muller transform (host only). */

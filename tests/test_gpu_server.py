@@ -120,8 +120,12 @@ def test_footprint_bound_and_tight_budget(H):
     reqs = [H.Server.request(2, 2, 2, 5, 1, p, s) for s, p in [(1, 32), (2, 64), (3, 32), (4, 64)]]
     probe = H.Server(1 << 40, max_level=5)
     need = max(probe.footprint(q) for q in reqs)
-    # room for the mesh (a few MB) and one hierarchy, not two
-    budget = need + need // 2
+    probe.submit(reqs[1])
+    probe.run(120)
+    mesh = probe.stats()["mesh_bytes"]  # storage, Laplace operator and row tables of the mesh
+    assert mesh > 0
+    # room for the mesh and one hierarchy, not two
+    budget = mesh + need + need // 2
     sv = H.Server(budget, max_active=4, max_level=5)
     ids = [sv.submit(q, arrival_s=0.0) for q in reqs]
     sv.run(120)

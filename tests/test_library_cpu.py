@@ -313,46 +313,6 @@ def test_gmsh_reader_rejects_unsupported_files(tmp_path, gmsh_exe):
         assert out.startswith("error"), (fname, out)
 
 
-PRIM_CHECK = r"""
-#include "topology.hpp"
-#include <cstdio>
-#include <cstdlib>
-using namespace hyb;
-int main( int argc, char** argv )
-{
-   // argv: kind (0 cuboid, 1 shell), nx ny nz (shell: ntan nrad 0); stdout: nV nE nF nC
-   std::vector< std::array< double, 3 > > V;
-   std::vector< std::array< int, 4 > >    T;
-   const double lo[3] = { 0, 0, 0 }, hi[3] = { 1, 1, 1 };
-   if ( atoi( argv[1] ) == 1 )
-      meshSphericalShell( atoi( argv[2] ), atoi( argv[3] ), 0.55, 1.0, V, T );
-   else
-      meshCuboid( atoi( argv[2] ), atoi( argv[3] ), atoi( argv[4] ), lo, hi, V, T );
-   Topology tp;
-   tp.build( V, T );
-   printf( "%zu %zu %zu %zu\n", V.size(), tp.E.size(), tp.F.size(), T.size() );
-   return 0;
-}
-"""
-
-
-@pytest.mark.parametrize("kind,shape", [(0, (1, 1, 1)), (0, (2, 2, 2)), (0, (3, 2, 1)), (1, (3, 2, 0)), (1, (5, 4, 0))])
-def test_mesh_primitive_counts_match_footprint_formula(tmp_path, kind, shape):
-    """The serving loop sizes row tables from closed-form vertex, edge and face counts of its
-    meshes; they equal the topology the storage builds."""
-    from test_server_cpu import mesh_primitives
-
-    src = tmp_path / "prim_check.cpp"
-    src.write_text(PRIM_CHECK)
-    exe = tmp_path / "prim_check"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(PKG, "csrc"), str(src),
-                    os.path.join(PKG, "csrc", "topology.cpp"), "-o", str(exe)], check=True)
-    out = subprocess.run([str(exe), str(kind)] + [str(v) for v in shape], capture_output=True, text=True,
-                         check=True).stdout.split()
-    nV, nE, nF, nC = map(int, out)
-    assert (nV, nE, nF) == mesh_primitives(*shape, mesh=kind)
-
-
 @pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
 def test_chebyshev_coefficients(lib, oracle_mod, order):
     """ChebyshevSmoother::setupCoefficients: the product's power-basis coefficients equal the

@@ -13,23 +13,6 @@ def H():
     return H
 
 
-def mesh_primitives(nx, ny, nz, mesh):
-    """Macro-vertices, -edges and -faces: counted by Euler's formula from the cells (cuboid:
-    V - E + F - C = 1 with E and F from the grid; shell: a sphere per radial layer)."""
-    if mesh == 1:
-        n = nx - 1
-        vs, es, fs = 10 * n * n + 2, 30 * n * n, 20 * n * n
-        nV, nE, nF = ny * vs, ny * es + (ny - 1) * (vs + es), ny * fs + (ny - 1) * (2 * es + 2 * fs)
-        assert nV - nE + nF - 60 * n * n * (ny - 1) == 2  # a thick sphere
-        return nV, nE, nF
-    grid_faces = nx * ny * (nz + 1) + nx * (ny + 1) * nz + (nx + 1) * ny * nz
-    nV = (nx + 1) * (ny + 1) * (nz + 1)
-    nE = nx * (ny + 1) * (nz + 1) + (nx + 1) * ny * (nz + 1) + (nx + 1) * (ny + 1) * nz + grid_faces + nx * ny * nz
-    nF = 2 * grid_faces + 6 * nx * ny * nz
-    assert nV - nE + nF - 6 * nx * ny * nz == 1  # a ball
-    return nV, nE, nF
-
-
 def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes=64, mesh=0):
     """Independent restatement of the per-request device bytes (the hierarchy's vectors per
     level, coefficient storage, coarse CG scratch, dot-product partials, features, the
@@ -42,18 +25,6 @@ def footprint_formula(nx, ny, nz, level, coeff, precision, mesh_max_level, modes
     b += nC * pad(4) * 8 * (5 if precision == 32 else 3)
     b += max(-(-closure(l) // 256) * nC for l in range(mesh_max_level + 1)) * 8
     b += (level + 1) * 65536  # phase-list allowance of the coarse-level program kernel
-    if coeff == 0:  # row tables (48-byte rows) of a constant operator: full, then surface only
-        nV, nE, nF = mesh_primitives(nx, ny, nz, mesh)
-        for l in range(level + 1):
-            N = 1 << l
-            points = nC * pad(closure(l))
-            if points > 4_000_000 or pad(closure(l)) >= 65536:
-                continue
-            n_int_face = (N - 1) * (N - 2) // 2 if N >= 3 else 0
-            n_pts = (N - 1) * (N - 2) * (N - 3) // 6 if N >= 4 else 0
-            lanes = 32 * nV + 8 * nE * (N - 1) + 2 * nF * n_int_face
-            iface = lanes + 16 * 62
-            b += 48 * (iface + lanes + 62 + 2 * nC * n_pts if points <= 400_000 else iface)
     return b + 16 + 16 + 4 * modes * 8
 
 
