@@ -828,6 +828,9 @@ __device__ __forceinline__ void sorInteriorBody( Blk vb, TopoDev tp, LevelDev lv
       io.load( op, cell );
       T*       uc = u + size_t( cell ) * lv.stride;
       const T* bc = rhs + size_t( cell ) * lv.stride;
+      // constant operator: the diagonal is the cell's stencil centre, one reciprocal per batch
+      // (the reference's macro-cell kernel multiplies by the inverse centre weight as well)
+      const T relaxInv = VAR ? relax : relax / io.w[0];
       T v[K];
 #pragma unroll
       for ( int k = 0; k < K; ++k )
@@ -835,7 +838,10 @@ __device__ __forceinline__ void sorInteriorBody( Blk vb, TopoDev tp, LevelDev lv
          T         diag, off;
          const int idx = pb.no[k].d[0] + pb.g[k];
          io.row( uc, pb.g[k], pb.no[k], diag, off );
-         v[k] = ( T( 1 ) - relax ) * uc[idx] + relax * ( bc[idx] - off ) / diag;
+         if constexpr ( VAR )
+            v[k] = ( T( 1 ) - relax ) * uc[idx] + relax * ( bc[idx] - off ) / diag;
+         else
+            v[k] = ( T( 1 ) - relax ) * uc[idx] + relaxInv * ( bc[idx] - off );
       }
       // the K points of a batch have one colour, so none reads another's new value
 #pragma unroll
@@ -868,9 +874,10 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, Level
    const int            cell = blockIdx.x;
    InteriorOp< T, VAR > io;
    io.load( op, cell );
-   T*       uc = u + size_t( cell ) * lv.stride;
-   const T* bc = rhs + size_t( cell ) * lv.stride;
-   const int off[5] = { o0, o1, o2, o3, o4 };
+   T*        uc       = u + size_t( cell ) * lv.stride;
+   const T*  bc       = rhs + size_t( cell ) * lv.stride;
+   const T   relaxInv = VAR ? relax : relax / io.w[0];
+   const int off[5]   = { o0, o1, o2, o3, o4 };
 #pragma unroll
    for ( int k = 0; k < kInteriorColours; ++k )
    {
@@ -883,7 +890,10 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, Level
          T             diag, offd;
          io.row( uc, g, no, diag, offd );
          const int idx = no.d[0] + g;
-         uc[idx]       = ( T( 1 ) - relax ) * uc[idx] + relax * ( bc[idx] - offd ) / diag;
+         if constexpr ( VAR )
+            uc[idx] = ( T( 1 ) - relax ) * uc[idx] + relax * ( bc[idx] - offd ) / diag;
+         else
+            uc[idx] = ( T( 1 ) - relax ) * uc[idx] + relaxInv * ( bc[idx] - offd );
       }
       __syncthreads();
    }
