@@ -540,7 +540,9 @@ def reference(args, rank, world):
 
 def single_op(args):
     """Run one level operation repeatedly (for ncu captures of a single kernel):
-    --op apply|residual|sor|sor32|restrict|prolong at --level on the bench mesh."""
+    --op apply|residual|sor|sor32|restrict|prolong at --level on the bench mesh, or
+    --op vcycle: FP64 V(3,3) cycles from --level down to level 0 (program kernel, row
+    passes of the middle levels, CG)."""
     import torch
 
     import build as B
@@ -566,6 +568,9 @@ def single_op(args):
     ops = {"apply": lambda: A.apply(b, y, L, F), "residual": lambda: A.residual(u, b, y, L, F),
            "sor": lambda: A.smooth_sor(u, b, 1.0, L, F), "sor32": lambda: A.smooth_sor(u, b, 1.0, L, F),
            "restrict": lambda: R.restrict(y, L, F), "prolong": lambda: P.prolongate_and_add(u, L - 1, F)}
+    if args.op == "vcycle":
+        gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+        ops["vcycle"] = lambda: gmg.solve(u, b, L)
     fn = ops[args.op]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -593,7 +598,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
-    ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong"],
+    ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong", "vcycle"],
                     help="profiling mode: repeat one level operation --steps times")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
