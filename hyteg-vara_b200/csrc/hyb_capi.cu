@@ -132,6 +132,7 @@ struct LevelHost
    std::unique_ptr< RowTables > rows; // built on first use (ensureRows)
    bool                         rowsTried = false;
    DevBuf< int32_t >  seg, xyz, blk, blkXYZ, pts, ptsC, quads, rowYZ;
+   DevBuf< int4 >     pro; // prolongation table (LevelDev::pro)
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
    std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
    int                cellBlocks   = 0;  // grid of the cell-interior row-segment loops
@@ -354,6 +355,58 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       d.blk  = lh->blk.p;
       d.pts  = lh->pts.p;
       d.ptsC = lh->ptsC.p;
+      // prolongation table: the two coarse endpoints of every block's points (pattern of
+      // interpolateFine), checked point by point against the closed-form indices
+      if ( l >= 1 && !blkXYZ.empty() )
+      {
+         const int           Wc = d.W / 2 + 1; // N / 2 + 1
+         std::vector< int4 > pro( 2 * blkXYZ.size() );
+         auto                ends = [&]( int x, int y, int z, int* A, int* B, bool& single ) {
+            const int px = x & 1, py = y & 1, pz = z & 1, pat = px | ( py << 1 ) | ( pz << 2 );
+            int       ox = 0, oy = 0, oz = 0;
+            switch ( pat )
+            {
+            case 0: break;
+            case 1: ox = 1; break;
+            case 2: oy = 1; break;
+            case 4: oz = 1; break;
+            case 3: ox = -1, oy = 1; break;
+            case 5: ox = -1, oz = 1; break;
+            case 6: oy = -1, oz = 1; break;
+            default: ox = -1, oy = 1, oz = -1; break;
+            }
+            single = pat == 0;
+            A[0] = ( x - ox ) >> 1, A[1] = ( y - oy ) >> 1, A[2] = ( z - oz ) >> 1;
+            B[0] = ( x + ox ) >> 1, B[1] = ( y + oy ) >> 1, B[2] = ( z + oz ) >> 1;
+         };
+         auto base = [&]( int X, int Y, int Z, int r ) { return rowStart( Wc, Y, Z ) + resOff( r, Wc - Y - Z ); };
+         for ( size_t b = 0; b < blkXYZ.size(); ++b )
+         {
+            const int x0 = blkXYZ[b] & 1023, y = ( blkXYZ[b] >> 10 ) & 1023, z = blkXYZ[b] >> 20;
+            int       A[3], B[3];
+            bool      single;
+            ends( x0, y, z, A, B, single );
+            pro[2 * b]     = make_int4( base( A[0], A[1], A[2], A[0] & 3 ), base( A[0], A[1], A[2], ( A[0] + 2 ) & 3 ), A[0],
+                                        base( B[0], B[1], B[2], B[0] & 3 ) );
+            pro[2 * b + 1] = make_int4( base( B[0], B[1], B[2], ( B[0] + 2 ) & 3 ), B[0], single ? 1 : 0, 0 );
+         }
+         for ( const int32_t e : pts )
+         {
+            const int  g = e & 255, b = e >> 8;
+            const int  x = ( blkXYZ[b] & 1023 ) + 4 * g, y = ( blkXYZ[b] >> 10 ) & 1023, z = blkXYZ[b] >> 20;
+            int        A[3], B[3];
+            bool       single;
+            ends( x, y, z, A, B, single );
+            const int4 P0 = pro[2 * b], P1 = pro[2 * b + 1];
+            const int  cA = ( ( g & 1 ) ? P0.y : P0.x ) + ( ( P0.z + 2 * g ) >> 2 );
+            const int  cB = ( ( g & 1 ) ? P1.x : P0.w ) + ( ( P1.y + 2 * g ) >> 2 );
+            require( cA == sidx( Wc, A[0], A[1], A[2] ) && ( single || cB == sidx( Wc, B[0], B[1], B[2] ) ) &&
+                         ( P1.z != 0 ) == single,
+                     "prolongation table disagrees with the closed-form indices" );
+         }
+         lh->pro.upload( pro );
+         d.pro = lh->pro.p;
+      }
       for ( int z = 0; z <= d.N; ++z )
          for ( int y = 0; y <= d.N - z; ++y )
             for ( int x = 0; x <= d.N - y - z; ++x )

@@ -69,6 +69,12 @@ struct LevelDev
    const int32_t* blkXYZ; // per block: x | y << 10 | z << 20 of its g = 0 point (x steps by 4)
    const int32_t* pts;
    const int32_t* ptsC;
+   // Prolongation from the next coarser level, per block b of the point table: the block's
+   // points x = x0 + 4g share a parity pattern, so each interpolates the coarse points
+   // A(g) and B(g) with x' = xA + 2g (xB + 2g) on fixed coarse rows. pro[2b] = {a0, a1, xA,
+   // b0}, pro[2b + 1] = {b1, xB, single, 0}: coarse index of A = (g odd ? a1 : a0) +
+   // ((xA + 2g) >> 2), of B likewise; single = 1 when the fine point is a coarse point.
+   const int4*    pro;
    // Interior quads for the constant-coefficient apply: entry g | row << 8 stands for the
    // points x = 4g .. 4g + 3 of interior row `row` (rowYZ[row] = y | z << 16), in storage
    // order; a quad holds at least one interior point.

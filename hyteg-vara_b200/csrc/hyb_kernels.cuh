@@ -1065,7 +1065,8 @@ __device__ __forceinline__ void prolongateBody( Blk vb, TopoDev tp, LevelDev lv,
    if ( vb.x < nCellBlocks )
    {
       // fine interior points from the point table: the points of one block share the
-      // parity pattern (x steps by 4), so the lanes of a block take one branch
+      // parity pattern (x steps by 4) and their coarse rows, whose positions the level's
+      // prolongation table holds (LevelDev::pro)
       constexpr int K       = 2;
       const int     nChunks = ( lv.nPts + 32 * K - 1 ) / ( 32 * K );
       HYB_CELL_LOOP( nChunks )
@@ -1081,11 +1082,12 @@ __device__ __forceinline__ void prolongateBody( Blk vb, TopoDev tp, LevelDev lv,
             const int i     = i0 + 32 * k;
             ok[k]           = i < lv.nPts;
             const int32_t e = __ldg( lv.pts + ( ok[k] ? i : lv.nPts - 1 ) );
-            const int     g = e & 255, b = e >> 8;
-            const int32_t p = __ldg( lv.blkXYZ + b );
-            const int     x = ( p & 1023 ) + 4 * g, y = ( p >> 10 ) & 1023, z = p >> 20;
-            fi[k]           = size_t( cell ) * lv.stride + __ldg( lv.blk + 16 * size_t( b ) ) + g;
-            v[k]            = interpolateFine( coarse + size_t( cell ) * strideC, Wc, x, y, z );
+            const int     g  = e & 255, b = e >> 8;
+            const int4    P0 = __ldg( lv.pro + 2 * b ), P1 = __ldg( lv.pro + 2 * b + 1 );
+            const T*      cc = coarse + size_t( cell ) * strideC;
+            fi[k]            = size_t( cell ) * lv.stride + __ldg( lv.blk + 16 * size_t( b ) ) + g;
+            const T a        = cc[( ( g & 1 ) ? P0.y : P0.x ) + ( ( P0.z + 2 * g ) >> 2 )];
+            v[k]             = P1.z ? a : T( 0.5 ) * ( a + cc[( ( g & 1 ) ? P1.x : P0.w ) + ( ( P1.y + 2 * g ) >> 2 )] );
          }
 #pragma unroll
          for ( int k = 0; k < K; ++k )
