@@ -379,16 +379,17 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
             A[0] = ( x - ox ) >> 1, A[1] = ( y - oy ) >> 1, A[2] = ( z - oz ) >> 1;
             B[0] = ( x + ox ) >> 1, B[1] = ( y + oy ) >> 1, B[2] = ( z + oz ) >> 1;
          };
-         auto base = [&]( int X, int Y, int Z, int r ) { return rowStart( Wc, Y, Z ) + resOff( r, Wc - Y - Z ); };
+         // slab position of the first point of residue r in coarse row (Y, Z)
+         auto base = [&]( int Y, int Z, int r ) { return rowStart( Wc, Y, Z ) + resOff( r, Wc - Y - Z ); };
          for ( size_t b = 0; b < blkXYZ.size(); ++b )
          {
             const int x0 = blkXYZ[b] & 1023, y = ( blkXYZ[b] >> 10 ) & 1023, z = blkXYZ[b] >> 20;
             int       A[3], B[3];
             bool      single;
             ends( x0, y, z, A, B, single );
-            pro[2 * b]     = make_int4( base( A[0], A[1], A[2], A[0] & 3 ), base( A[0], A[1], A[2], ( A[0] + 2 ) & 3 ), A[0],
-                                        base( B[0], B[1], B[2], B[0] & 3 ) );
-            pro[2 * b + 1] = make_int4( base( B[0], B[1], B[2], ( B[0] + 2 ) & 3 ), B[0], single ? 1 : 0, 0 );
+            pro[2 * b]     = make_int4( base( A[1], A[2], A[0] & 3 ), base( A[1], A[2], ( A[0] + 2 ) & 3 ), A[0],
+                                        base( B[1], B[2], B[0] & 3 ) );
+            pro[2 * b + 1] = make_int4( base( B[1], B[2], ( B[0] + 2 ) & 3 ), B[0], single ? 1 : 0, 0 );
          }
          for ( const int32_t e : pts )
          {
