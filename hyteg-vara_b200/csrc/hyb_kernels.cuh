@@ -339,6 +339,15 @@ struct InteriorOp
    const int nItems_ = tp.nC * ( NSEG );                                                                             \
    for ( int it_ = vb.x * wpb_ + int( threadIdx.x >> 5 ); it_ < nItems_; it_ += nCellBlocks * wpb_ )
 
+// The same items in block steps of S consecutive items per warp: block b's warps take the
+// items [b S w, (b + 1) S w) of each step (w warps per block), so they work on neighbouring
+// rows and share the rows around them in L1.
+#define HYB_CELL_LOOP_STRIP( NSEG, S )                                                                               \
+   const int wpb_ = int( blockDim.x >> 5 ), warp_ = int( threadIdx.x >> 5 );                                        \
+   const int nItems_ = tp.nC * ( NSEG ), step_ = ( S ) * wpb_;                                                      \
+   for ( int b0_ = vb.x * step_; b0_ < nItems_; b0_ += nCellBlocks * step_ )                                       \
+      for ( int it_ = b0_ + warp_; it_ < b0_ + step_ && it_ < nItems_; it_ += wpb_ )
+
 // ---------------------------------------------------------------------------
 // Cell-interior loops run over the level's interior point table: a warp takes 32
 // consecutive entries (consecutive storage positions, so every neighbour read is a
@@ -775,6 +784,10 @@ __global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_apply( TopoDev tp, Level
 // cell interiors. No two DoFs of one pass are coupled.
 // ---------------------------------------------------------------------------
 constexpr int kInteriorColours = 4;
+// consecutive interior batches a warp takes per block step at most (measured at level 7
+// on B200: 1 -> 435 us, 2 -> 428, 4 -> 413, 8 -> 422, 16 -> 476 us per FP64 sweep; on
+// smaller levels long strips leave blocks idle, so the strip shrinks with the work)
+constexpr int kInteriorStrip = 4;
 
 template < typename T, bool VAR >
 __device__ __forceinline__ void sorIfaceBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, T* u,
@@ -818,7 +831,9 @@ __device__ __forceinline__ void sorInteriorBody( Blk vb, TopoDev tp, LevelDev lv
    constexpr int  K       = interiorBatch< T, VAR >();
    const int32_t* pts     = lv.ptsC + begin;
    const int      nChunks = ( nPts + 32 * K - 1 ) / ( 32 * K );
-   HYB_CELL_LOOP( nChunks )
+   // strips only while every warp of the grid still gets at least one strip
+   const int strip = max( 1, min( kInteriorStrip, tp.nC * nChunks / ( nCellBlocks * int( blockDim.x >> 5 ) ) ) );
+   HYB_CELL_LOOP_STRIP( nChunks, strip )
    {
       const int       item = ( colour & 1 ) ? nItems_ - 1 - it_ : it_;
       const int       cell = item / nChunks;
