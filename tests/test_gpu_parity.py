@@ -592,3 +592,40 @@ def test_chebyshev_solve_to_tolerance(H, oracle_mod, setups, precision):
     x = np.zeros(orc.n(L))
     orc.gmg(x, b, 0, L, pre=3, post=3, smoother=0, max_cycles=60, rel_tol=1e-13)
     assert np.abs(fx.get(L) - x).max() / np.abs(x).max() < 1e-6
+
+
+@pytest.mark.parametrize("variable", [False, True])
+def test_row_table_and_lane_paths_agree(H, oracle_mod, variable):
+    """The surface SOR pass, the residual and the apply give the oracle's results both
+    through the lane-group path (a fresh storage: no row tables yet) and through the
+    precomputed rows (built by a solver's first cycle), for both operators."""
+    O = oracle_mod
+    c, t = O.mesh_cuboid(2, 1, 1, hi=(2.0, 1.0, 1.0))
+    L = 3
+    st = H.PrimitiveStorage(c, t, L)
+    orc = O.Oracle(c, t, L)
+    if variable:
+        kv = [O.grf_coefficient(orc.coords_of(l), seed=4) for l in range(L + 1)]
+        A, op = H.P1ElementwiseDivKGradOperator(st, 0, L, kv), orc.op_divkgrad(kv)
+    else:
+        A, op = H.P1ConstantLaplaceOperator(st, 0, L), 0
+    m, labels = st.colouring()
+    rng = np.random.default_rng(21)
+    x, b = rng.uniform(-1, 1, orc.n(L)), rng.uniform(-1, 1, orc.n(L))
+    ref_sor = orc.sor_colored(x.copy(), b, L, labels, m, relax=1.1, flag=1 | 4, op=op)
+    ref_res = b - orc.apply(x, L, flag=1 | 4, op=op)
+    kind, bc = orc.info(L)
+    inner = (bc == O.INNER) | (bc == O.NEUMANN)
+    for phase in ("lanes", "rows"):
+        if phase == "rows":
+            gmg = H.GeometricMultigridSolver(st, A, 0, L, 1, 1, 1.0)
+            fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+            gmg.solve(fx, fb, L)  # builds the row tables of every level
+        fu, fr, fo = (H.P1Function(n, st, 0, L) for n in "uro")
+        fu.set(x, L)
+        fr.set(b, L)
+        A.smooth_sor(fu, fr, 1.1, L, 1 | 4)
+        close(fu.get(L), ref_sor, 1e-11)
+        fu.set(x, L)
+        A.residual(fu, fr, fo, L, 1 | 4)
+        close(fo.get(L)[inner], ref_res[inner], 1e-11)
