@@ -380,11 +380,12 @@ __device__ __forceinline__ NbrOff blockNbr( const int32_t* __restrict__ blk, int
 // Interior points per lane and item: independent load chains that the warp keeps in
 // flight together (the loops are latency bound, not bandwidth bound, at one point per lane).
 // Measured on B200 at level 7, two beat one by 1.2-1.3x and beat four for FP32 (four cost
-// registers and with them resident warps).
+// registers and with them resident warps); three beat two by ~2 % for FP64 and lose ~5 %
+// for FP32.
 template < typename T, bool VAR >
 __host__ __device__ constexpr int interiorBatch()
 {
-   return VAR ? 1 : 2;
+   return VAR ? 1 : ( sizeof( T ) == 8 ? 3 : 2 );
 }
 
 // The K table entries i0 + 32 k of a point table. Entries past the end are clamped to the
