@@ -242,7 +242,7 @@ def ours(args, rank, world, local_rank):
     # DRAM bytes (read + write) per launch from ncu captures of the same kernels and workload
     # (the sum over the ten launches of one sweep): profiles/k_sor_fp64_fp32_level7_cube48.md,
     # profiles/k_apply_fp64_level7_cube48.md
-    sweep64_traffic, sweep32_traffic, apply_traffic = 1516.7e6, 900.5e6, 429.7e6
+    sweep64_traffic, sweep32_traffic, apply_traffic = 1510.5e6, 902.3e6, 429.7e6
     if (L, nc) != (7, 2):
         sweep64_traffic = sweep32_traffic = apply_traffic = None
 
