@@ -100,27 +100,30 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
       const int      kind   = P.kind;
       const int      blocks = P.blocks;
       const LevelDev lv     = levelAt( P.level );
-      for ( int b = int( blockIdx.x ); b < blocks; b += int( gridDim.x ) )
+      // row passes spread over every thread of the block
+      const bool rowPass = P.rp.rows && ( kind == kPhSorIface || kind == kPhSorInterior || kind == kPhResidual );
+      if ( rowPass )
+      {
+         const long long start = (long long) blockIdx.x * blockDim.x + threadIdx.x, step = (long long) gridDim.x * blockDim.x;
+         if ( kind == kPhResidual )
+            rowPassBody< T, kRowResidual, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p2, (T*) P.p1, T( 0 ),
+                                                 P.flag, start, step );
+         else
+            rowPassBody< T, kRowSor, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, nullptr, T( P.relax ),
+                                            kind == kPhSorIface ? P.flag : 0xff, start, step );
+      }
+      for ( int b = int( blockIdx.x ); !rowPass && b < blocks; b += int( gridDim.x ) )
       {
          const Blk       vb{ b, blocks };
          const long long t0 = (long long) b * blockDim.x + threadIdx.x, step = (long long) blocks * blockDim.x;
          switch ( kind )
          {
          case kPhSorIface:
-            if ( P.rp.rows )
-               rowPassBody< T, kRowSor, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, nullptr,
-                                               T( P.relax ), P.flag, threadIdx.x, blockDim.x );
-            else
-               sorIfaceBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.flag,
-                                       P.bl );
+            sorIfaceBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.flag, P.bl );
             break;
          case kPhSorInterior:
-            if ( P.rp.rows )
-               rowPassBody< T, kRowSor, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, nullptr,
-                                               T( P.relax ), 0xff, threadIdx.x, blockDim.x );
-            else
-               sorInteriorBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.a0,
-                                          P.a1, P.a2, P.cellBlocks );
+            sorInteriorBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p1, T( P.relax ), P.a0, P.a1,
+                                       P.a2, P.cellBlocks );
             break;
          case kPhJacobi:
             jacobiBody< T, VAR >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1, (const T*) P.p2, T( P.relax ),
@@ -131,12 +134,8 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
                ( (T*) P.p0 )[i] = ( (const T*) P.p1 )[i];
             break;
          case kPhResidual:
-            if ( P.rp.rows )
-               rowPassBody< T, kRowResidual, VAR >( P.rp, phaseOp< T >( P ), (T*) P.p0, (const T*) P.p2, (T*) P.p1,
-                                                    T( 0 ), P.flag, threadIdx.x, blockDim.x );
-            else
-               applyBody< T, VAR, kResidual >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1,
-                                               (const T*) P.p2, P.flag, P.cellBlocks );
+            applyBody< T, VAR, kResidual >( vb, tp, lv, phaseOp< T >( P ), (const T*) P.p0, (T*) P.p1, (const T*) P.p2,
+                                            P.flag, P.cellBlocks );
             break;
          case kPhRestrict:
          {
@@ -173,6 +172,7 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
       // left that phase at the last barrier)
       if ( ph + 1 < nPhases && threadIdx.x < nWords )
          reinterpret_cast< unsigned long long* >( &sP[( ph + 1 ) & 1] )[threadIdx.x] = next;
+      // a phase's results are read by other threads in the next one
       __syncthreads();
    }
 }
