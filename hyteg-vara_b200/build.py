@@ -8,7 +8,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = [os.path.join(HERE, "csrc", f) for f in ("hyb_capi.cu", "topology.cpp")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("hyb_device.cuh", "hyb_kernels.cuh", "hyb_program.cuh", "hyb_server.inl", "topology.hpp")] + \
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("hyb_device.cuh", "hyb_kernels.cuh", "hyb_program.cuh", "hyb_storage.inl", "hyb_launch.inl", "hyb_gmg.inl", "hyb_server.inl", "topology.hpp")] + \
     [os.path.join(os.path.dirname(HERE), "include", "hyteg_b200.h")]
 OUT = os.path.join(HERE, "libhyteg_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -1,0 +1,561 @@
+// Geometric multigrid: V/W-cycles, the small-level program, graph capture and replay.
+// (part of the single translation unit hyb_capi.cu, included inside namespace hyb)
+
+// ---------------------------------------------------------------------------
+// Geometric multigrid (GeometricMultigridSolver.hpp:136-235)
+// ---------------------------------------------------------------------------
+struct Gmg
+{
+   Storage*  st;
+   Operator* op;
+   int       minL, maxL, pre, post, smoother, coarseMaxIter;
+   int       cycleType = HYB_CYCLE_V;
+   double    relax, coarseTol;
+   std::unique_ptr< Function > tmp64;         // gmg_tmp
+   std::unique_ptr< Function > x32, b32, t32; // FP32 inner hierarchy (mixed precision)
+   std::unique_ptr< Function > r64;           // FP64 residual (mixed precision)
+   std::unique_ptr< Function > cx64, cb64;    // FP64 coarse-solve copies of the FP32 hierarchy
+   std::vector< double >       cheb;          // Chebyshev smoother: omega_0 .. omega_{order-1}
+   std::unique_ptr< Function > inv64, inv32;  // Chebyshev smoother: diag(A)^-1 per level
+   std::unique_ptr< Function > ch64, ch32;    // Chebyshev smoother: second temporary
+   CgScratch                   cg;
+   // reduction scratch of this solver, so that solvers sharing a storage can run on
+   // different streams at the same time: scalars[0] = ||r||^2, scalars[1] = ||b||^2
+   DevBuf< double >            partial, scalars;
+   double*                     hostScalar = nullptr; // pinned, 2 doubles
+   // Levels <= progTop of a V-cycle run as one program-kernel launch (-1: none), with one
+   // recorded phase list per (x, b, compute type, top level).
+   int progTop = -1;
+   struct Program
+   {
+      const void*     x;
+      const void*     b;
+      int             dtype, top, n;
+      DevBuf< Phase > phases;
+   };
+   std::vector< std::unique_ptr< Program > > programs;
+   cudaStream_t                cap = nullptr; // capture stream
+   // captured graphs keyed by (x, b, level, kind)
+   struct G
+   {
+      const void* x;
+      const void* b;
+      int         level, kind;
+      cudaGraphExec_t exec;
+      long long       kernels; // kernel launches captured in the graph
+   };
+   std::vector< G > graphs;
+
+   ~Gmg()
+   {
+      for ( auto& g : graphs )
+         cudaGraphExecDestroy( g.exec );
+      if ( cap )
+         cudaStreamDestroy( cap );
+      if ( hostScalar )
+         cudaFreeHost( hostScalar );
+   }
+};
+
+constexpr int kGmgFlag = HYB_INNER | HYB_NEUMANN;
+
+template < typename T >
+void smooth( Gmg& g, int l, T* x, const T* b, T* scratch, cudaStream_t stream )
+{
+   if ( g.smoother == HYB_SMOOTHER_SOR )
+      launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
+   else if ( g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR )
+   {
+      // SymmetricSORSmoother::solve (SymmetricSORSmoother.hpp:38-57): forward, then backwards
+      launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
+      launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream, true );
+   }
+   else if ( g.smoother == HYB_SMOOTHER_CHEBYSHEV )
+   {
+      // ChebyshevSmoother::solve (ChebyshevSmoother.hpp:49-96): t = D^-1 (b - A x), x += w_0 t,
+      // then t = D^-1 A t, x += w_k t. scratch (the solver's residual vector) and the second
+      // temporary are only written on Inner|Neumann DoFs, so they hold 0 elsewhere.
+      const bool      f64 = std::is_same< T, double >::value;
+      const T*        inv = ( f64 ? g.inv64 : g.inv32 )->template ptr< T >( l );
+      T*              t   = scratch;
+      T*              t2  = ( f64 ? g.ch64 : g.ch32 )->template ptr< T >( l );
+      launchApply< T >( *g.op, l, x, t, b, kGmgFlag, kResidual, stream );
+      launchChebUpdate< T >( *g.st, l, inv, t, x, T( g.cheb[0] ), stream );
+      for ( size_t k = 1; k < g.cheb.size(); ++k )
+      {
+         launchApply< T >( *g.op, l, t, t2, nullptr, kGmgFlag, kReplace, stream );
+         launchChebUpdate< T >( *g.st, l, inv, t2, x, T( g.cheb[k] ), stream );
+         std::swap( t, t2 );
+      }
+   }
+   else
+   {
+      // Jacobi needs the old iterate: scratch = x, then x = scratch + relax D^-1 (b - A scratch)
+      HYB_CUDA( cudaMemcpyAsync( scratch, x, size_t( g.st->td.nC ) * g.st->L( l ).dev.stride * sizeof( T ),
+                                 cudaMemcpyDeviceToDevice, stream ) );
+      launchJacobi< T >( *g.op, l, scratch, x, b, T( g.relax ), kGmgFlag, stream );
+   }
+}
+
+// coarse solve: FP64 CG; an FP32 hierarchy is solved through FP64 copies
+void coarseSolve( Gmg& g, double* x, const double* b, cudaStream_t stream )
+{
+   launchCg( *g.op, g.minL, x, b, g.cg, g.coarseTol, g.coarseMaxIter, stream );
+}
+void coarseSolve( Gmg& g, float* x, const float* b, cudaStream_t stream )
+{
+   const int l = g.minL;
+   launchConvert< double, float >( *g.st, l, g.cx64->ptr< double >( l ), x, stream );
+   launchConvert< double, float >( *g.st, l, g.cb64->ptr< double >( l ), b, stream );
+   launchCg( *g.op, l, g.cx64->ptr< double >( l ), g.cb64->ptr< double >( l ), g.cg, g.coarseTol, g.coarseMaxIter, stream );
+   launchConvert< float, double >( *g.st, l, x, g.cx64->ptr< double >( l ), stream );
+}
+
+// ---------------------------------------------------------------------------
+// Program-kernel V-cycle for the small levels: the phases mirror vcycle() below, launch
+// for launch, with each launch's grid as the phase's virtual grid.
+// ---------------------------------------------------------------------------
+// levels whose slabs hold at most this many points (all cells) run in the program kernel;
+// HYB_PROGRAM_MAX_POINTS overrides it (0: never)
+constexpr long kProgramMaxPoints = 4096;
+
+struct PhaseList
+{
+   const Gmg&           g;
+   std::vector< Phase > ph;
+
+   // one thread block runs the program: a phase has one virtual block for its cell-interior
+   // loop (if the launch it replaces has one) and one for its surface or flat loop
+   Phase& add( int kind, int level, int blocks, int cellBlocks )
+   {
+      Phase P{};
+      P.kind       = kind;
+      P.level      = level;
+      P.cellBlocks = cellBlocks > 0 ? 1 : 0;
+      P.blocks     = std::max( P.cellBlocks + ( blocks > cellBlocks ? 1 : 0 ), 1 );
+      P.op32       = g.op->dev< float >( level );
+      P.op64       = g.op->dev< double >( level );
+      ph.push_back( P );
+      return ph.back();
+   }
+   long slabElems( int l ) const { return long( g.st->td.nC ) * g.st->L( l ).dev.stride; }
+   // the row table of level l for the passes of this (constant) operator, built on first use
+   const RowTables* rows( int l ) const
+   {
+      const RowTables* R = ensureRows( *g.st, l );
+      return R && R->full ? R : nullptr;
+   }
+   int  flatBlocks( long n ) const
+   {
+      return int( std::min< long >( ( n + 127 ) / 128, long( g.st->numSMs ) * 8 ) );
+   }
+
+   template < typename T >
+   void smooth( int l, T* x, const T* b, T* scratch )
+   {
+      const Storage& s = *g.st;
+      const auto&    L = s.L( l );
+      if ( g.smoother == HYB_SMOOTHER_SOR || g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR )
+      {
+         auto iface = [&]( int c ) {
+            const int* co    = &L.colourOff[4 * c];
+            const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+            if ( lanes == 0 )
+               return;
+            const int32_t* list = L.colourList.p + co[0];
+            Phase&         P    = add( kPhSorIface, l, int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) ), 0 );
+            P.p0                = x;
+            P.p1                = const_cast< T* >( b );
+            P.relax             = g.relax;
+            P.flag              = kGmgFlag;
+            P.bl                = BdryLists{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+            if ( const RowTables* R = rows( l ) )
+            {
+               const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
+               P.rp          = RowPass{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes };
+               P.blocks      = 1;
+               P.cellBlocks  = 0;
+            }
+         };
+         auto interior = [&]( int c ) {
+            const int count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
+            if ( count == 0 )
+               return;
+            Phase& P = add( kPhSorInterior, l, L.colourBlocks, L.colourBlocks );
+            P.p0     = x;
+            P.p1     = const_cast< T* >( b );
+            P.relax  = g.relax;
+            P.a0     = c;
+            P.a1     = L.dev.ptsOff[c];
+            P.a2     = count;
+            if ( const RowTables* R = rows( l ) )
+            {
+               const long n = long( s.td.nC ) * count;
+               P.rp         = RowPass{ R->interior.p + long( s.td.nC ) * L.dev.ptsOff[c], n, 0, 0, 0 };
+               P.blocks     = 1;
+               P.cellBlocks = 0;
+            }
+         };
+         for ( int c = 0; c < s.td.m; ++c )
+            iface( c );
+         for ( int c = 0; c < kInteriorColours; ++c )
+            interior( c );
+         if ( g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR )
+         {
+            for ( int c = kInteriorColours - 1; c >= 0; --c )
+               interior( c );
+            for ( int c = s.td.m - 1; c >= 0; --c )
+               iface( c );
+         }
+      }
+      else
+      {
+         Phase& C = add( kPhCopy, l, flatBlocks( slabElems( l ) ), 0 );
+         C.p0     = scratch;
+         C.p1     = x;
+         C.n      = slabElems( l );
+         const int nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+         Phase&    P  = add( kPhJacobi, l, nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 ), nc );
+         P.p0         = scratch;
+         P.p1         = x;
+         P.p2         = const_cast< T* >( b );
+         P.relax      = g.relax;
+         P.flag       = kGmgFlag;
+      }
+   }
+
+   void cg( int l, double* x, const double* b )
+   {
+      Phase& P = add( kPhCg, l, 1, 0 );
+      P.p0     = x;
+      P.p1     = const_cast< double* >( b );
+      P.p2     = g.cg.r->ptr< double >( l );
+      P.p3     = g.cg.p->ptr< double >( l );
+      P.p4     = g.cg.ap->ptr< double >( l );
+      P.status = g.cg.status.p;
+      P.relax  = g.coarseTol;
+      P.a0     = g.coarseMaxIter;
+      P.rp     = rowPassAll( rows( l ) );
+   }
+
+   void coarse( double* x, const double* b ) { cg( g.minL, x, b ); }
+   void coarse( float* x, const float* b )
+   {
+      const int  l = g.minL;
+      const long n = slabElems( l );
+      Phase&     A = add( kPhToF64, l, flatBlocks( n ), 0 );
+      A.p0         = g.cx64->ptr< double >( l );
+      A.p1         = x;
+      A.n          = n;
+      Phase& B     = add( kPhToF64, l, flatBlocks( n ), 0 );
+      B.p0         = g.cb64->ptr< double >( l );
+      B.p1         = const_cast< float* >( b );
+      B.n          = n;
+      cg( l, g.cx64->ptr< double >( l ), g.cb64->ptr< double >( l ) );
+      Phase& C = add( kPhToF32, l, flatBlocks( n ), 0 );
+      C.p0     = x;
+      C.p1     = g.cx64->ptr< double >( l );
+      C.n      = n;
+   }
+
+   template < typename T >
+   void vcycle( Function& x, Function& b, Function& tmp, int l )
+   {
+      if ( l == g.minL )
+      {
+         coarse( x.ptr< T >( l ), b.ptr< T >( l ) );
+         return;
+      }
+      const Storage& s = *g.st;
+      for ( int i = 0; i < g.pre; ++i )
+         smooth< T >( l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ) );
+      {
+         const auto& L  = s.L( l );
+         const int   nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+         Phase&      P  = add( kPhResidual, l, nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 ), nc );
+         P.p0           = x.ptr< T >( l );
+         P.p1           = tmp.ptr< T >( l );
+         P.p2           = b.ptr< T >( l );
+         P.flag         = kGmgFlag;
+         if ( const RowTables* R = rows( l ) )
+         {
+            P.rp         = rowPassAll( R );
+            P.blocks     = 1;
+            P.cellBlocks = 0;
+         }
+      }
+      {
+         const auto& C  = s.L( l - 1 );
+         const int   nc = C.dev.nSeg > 0 ? C.cellBlocks : 0;
+         Phase&      P  = add( kPhRestrict, l - 1, nc + ( C.dev.nBdry > 0 ? C.bdryBlocks : 0 ), nc );
+         P.p0           = tmp.ptr< T >( l );
+         P.p1           = b.ptr< T >( l - 1 );
+         P.flag         = kGmgFlag;
+      }
+      {
+         Phase& P = add( kPhZero, l - 1, flatBlocks( slabElems( l - 1 ) ), 0 );
+         P.p0     = x.ptr< T >( l - 1 );
+         P.n      = slabElems( l - 1 );
+      }
+      vcycle< T >( x, b, tmp, l - 1 );
+      if ( g.cycleType == HYB_CYCLE_W )
+         vcycle< T >( x, b, tmp, l - 1 );
+      {
+         const auto& F  = s.L( l );
+         const int   nc = F.dev.nPts > 0 ? F.ptsBlocks : 0;
+         Phase&      P  = add( kPhProlongAdd, l, nc + ( F.dev.nBdry > 0 ? F.bdryBlocks : 0 ), nc );
+         P.p0           = x.ptr< T >( l - 1 );
+         P.p1           = x.ptr< T >( l );
+         P.flag         = kGmgFlag;
+      }
+      for ( int i = 0; i < g.post; ++i )
+         smooth< T >( l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ) );
+   }
+};
+
+// Record (once, outside any stream capture) the program of the sub-cycle at level `top`
+// for the V-cycle on (x, b, tmp) in type T.
+template < typename T >
+void ensureProgram( Gmg& g, Function& x, Function& b, Function& tmp, int top )
+{
+   const int dtype = std::is_same< T, double >::value ? HYB_F64 : HYB_F32;
+   for ( auto& p : g.programs )
+      if ( p->x == &x && p->b == &b && p->dtype == dtype && p->top == top )
+         return;
+   PhaseList pl{ g, {} };
+   pl.vcycle< T >( x, b, tmp, top );
+   auto prog   = std::make_unique< Gmg::Program >();
+   prog->x     = &x;
+   prog->b     = &b;
+   prog->dtype = dtype;
+   prog->top   = top;
+   prog->n     = int( pl.ph.size() );
+   prog->phases.upload( pl.ph );
+   g.programs.push_back( std::move( prog ) );
+}
+
+template < typename T >
+void launchProgram( Gmg& g, Function& x, Function& b, int top, cudaStream_t stream )
+{
+   const int           dtype = std::is_same< T, double >::value ? HYB_F64 : HYB_F32;
+   const Gmg::Program* prog  = nullptr;
+   for ( auto& p : g.programs )
+      if ( p->x == &x && p->b == &b && p->dtype == dtype && p->top == top )
+         prog = p.get();
+   require( prog != nullptr, "program of the coarse V-cycle was not recorded" );
+   const Phase* ph  = prog->phases.p;
+   const auto*  lt  = (const LevelDev*) g.st->lvTable.p;
+   const int    nLv = int( g.st->lvTable.n );
+   if ( g.op->variable )
+      pdlLaunch( k_program< T, true >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n, nLv );
+   else
+      pdlLaunch( k_program< T, false >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n, nLv );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void vcycle( Gmg& g, Function& x, Function& b, Function& tmp, int l, cudaStream_t stream )
+{
+   if ( l <= g.progTop )
+   {
+      launchProgram< T >( g, x, b, l, stream );
+      return;
+   }
+   if ( l == g.minL )
+   {
+      coarseSolve( g, x.ptr< T >( l ), b.ptr< T >( l ), stream );
+      return;
+   }
+   for ( int i = 0; i < g.pre; ++i )
+      smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
+   // tmp = b - A x ; restricted straight into b on the coarser level (b.assign(tmp) on flag)
+   launchApply< T >( *g.op, l, x.ptr< T >( l ), tmp.ptr< T >( l ), b.ptr< T >( l ), kGmgFlag, kResidual, stream );
+   launchRestrict< T >( *g.st, l, tmp.ptr< T >( l ), b.ptr< T >( l - 1 ), kGmgFlag, stream );
+   HYB_CUDA( cudaMemsetAsync( x.ptr< T >( l - 1 ), 0, x.levelBytes( l - 1 ), stream ) ); // x.interpolate(0, l-1)
+   vcycle< T >( g, x, b, tmp, l - 1, stream );
+   if ( g.cycleType == HYB_CYCLE_W ) // GeometricMultigridSolver.hpp:201-204
+      vcycle< T >( g, x, b, tmp, l - 1, stream );
+   launchProlongate< T >( *g.st, l - 1, x.ptr< T >( l - 1 ), x.ptr< T >( l ), kGmgFlag, true, stream );
+   for ( int i = 0; i < g.post; ++i )
+      smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
+}
+
+// Graph-captured work units.
+enum GraphKind : int
+{
+   kCycle64      = 0, // one FP64 V-cycle
+   kCycle64Norm  = 1, // FP64 V-cycle, then r = b - A x and ||r||^2 into scalar slot 0
+   kMixedStep    = 2, // FP32 V-cycle on A e = r (r from the previous step), x += e, new r and ||r||^2
+   kNorm64       = 3, // r = b - A x into gmg_tmp and ||r||^2
+   kNormMixed    = 4, // r = b - A x into the FP64 residual of the mixed solver and ||r||^2
+   kFmg64        = 8, // full multigrid, kFmg64 + c: c FP64 V-cycles per level (1 <= c <= 8)
+};
+
+void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s )
+{
+   if ( kind == kCycle64 || kind == kCycle64Norm )
+      vcycle< double >( g, x, b, *g.tmp64, l, s );
+   if ( kind == kMixedStep )
+   {
+      // FP32 V-cycle on the residual equation (mixedPrecisionIterativeRefinement.cpp:162-171)
+      launchConvert< float, double >( *g.st, l, g.b32->ptr< float >( l ), g.r64->ptr< double >( l ), s );
+      HYB_CUDA( cudaMemsetAsync( g.x32->ptr< float >( l ), 0, g.x32->levelBytes( l ), s ) );
+      vcycle< float >( g, *g.x32, *g.b32, *g.t32, l, s );
+      launchAddCorrection< float >( *g.st, l, x.ptr< double >( l ), g.x32->ptr< float >( l ), kGmgFlag, s );
+   }
+   if ( kind > kFmg64 && kind <= kFmg64 + 8 )
+   {
+      // FullMultigridSolver::solve (FullMultigridSolver.hpp:51-75) with linear FMG
+      // prolongation on inner and Neumann DoFs
+      for ( int lc = g.minL; lc <= l; ++lc )
+      {
+         for ( int c = 0; c < kind - kFmg64; ++c )
+            vcycle< double >( g, x, b, *g.tmp64, lc, s );
+         if ( lc < l )
+            launchProlongate< double >( *g.st, lc, x.ptr< double >( lc ), x.ptr< double >( lc + 1 ), kGmgFlag, false, s );
+      }
+      return;
+   }
+   if ( kind != kCycle64 )
+   {
+      Function& r = ( kind == kCycle64Norm || kind == kNorm64 ) ? *g.tmp64 : *g.r64;
+      launchApply< double >( *g.op, l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ), kGmgFlag, kResidual, s );
+      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, g.partial.p, g.scalars.p, s );
+   }
+}
+
+// everything a captured graph needs is allocated before capture begins
+// the Chebyshev smoother's inverse diagonals and temporaries for the hierarchies in use
+void ensureChebyshev( Gmg& g )
+{
+   if ( g.smoother != HYB_SMOOTHER_CHEBYSHEV )
+      return;
+   require( !g.cheb.empty(), "the Chebyshev smoother needs its coefficients (hyb_gmg_setup_chebyshev)" );
+   auto fill = [&]( std::unique_ptr< Function >& inv, std::unique_ptr< Function >& t2, int dtype ) {
+      if ( inv )
+         return;
+      inv.reset( makeFunction( g.st, g.minL, g.maxL, dtype ) );
+      t2.reset( makeFunction( g.st, g.minL, g.maxL, dtype ) );
+      for ( int l = g.minL; l <= g.maxL; ++l )
+         if ( dtype == HYB_F64 )
+            launchInvDiag< double >( *g.op, l, t2->ptr< double >( l ), inv->ptr< double >( l ), nullptr );
+         else
+            launchInvDiag< float >( *g.op, l, t2->ptr< float >( l ), inv->ptr< float >( l ), nullptr );
+      HYB_CUDA( cudaDeviceSynchronize() );
+   };
+   fill( g.inv64, g.ch64, HYB_F64 );
+   if ( g.x32 )
+      fill( g.inv32, g.ch32, HYB_F32 );
+}
+
+void prepare( Gmg& g )
+{
+   ensureChebyshev( g );
+   for ( int l = g.minL; l <= g.maxL; ++l )
+      ensureRows( *g.st, l );
+   if ( !g.cg.r )
+   {
+      g.cg.r.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
+      g.cg.p.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
+      g.cg.ap.reset( makeFunction( g.st, g.minL, g.minL, HYB_F64 ) );
+      g.cg.status.alloc( 4 );
+   }
+}
+
+void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int post, double relax, int smoother,
+              double coarseTol, int coarseMaxIter )
+{
+   g.st            = s;
+   g.op            = op;
+   g.minL          = minL;
+   g.maxL          = maxL;
+   g.pre           = pre;
+   g.post          = post;
+   g.relax         = relax;
+   g.smoother      = smoother;
+   g.coarseTol     = coarseTol;
+   g.coarseMaxIter = coarseMaxIter;
+   g.tmp64.reset( makeFunction( s, minL, maxL, HYB_F64 ) );
+   g.partial.alloc( s->partial.n );
+   g.scalars.alloc( 2 );
+   HYB_CUDA( cudaMallocHost( &g.hostScalar, 2 * sizeof( double ) ) );
+   long maxPoints = kProgramMaxPoints;
+   if ( const char* e = std::getenv( "HYB_PROGRAM_MAX_POINTS" ) )
+      maxPoints = std::atol( e );
+   g.progTop = -1;
+   for ( int l = minL; l <= maxL; ++l )
+      if ( long( s->td.nC ) * s->L( l ).dev.stride <= maxPoints )
+         g.progTop = l;
+   if ( smoother == HYB_SMOOTHER_CHEBYSHEV )
+      g.progTop = -1; // the program kernel has no Chebyshev phases
+}
+
+
+// the FP32 hierarchy and FP64 residual of the mixed-precision solver
+void ensureMixed( Gmg& g )
+{
+   if ( g.x32 )
+      return;
+   Storage* s = g.st;
+   g.x32.reset( makeFunction( s, g.minL, g.maxL, HYB_F32 ) );
+   g.b32.reset( makeFunction( s, g.minL, g.maxL, HYB_F32 ) );
+   g.t32.reset( makeFunction( s, g.minL, g.maxL, HYB_F32 ) );
+   g.r64.reset( makeFunction( s, g.minL, g.maxL, HYB_F64 ) );
+   g.cx64.reset( makeFunction( s, g.minL, g.minL, HYB_F64 ) );
+   g.cb64.reset( makeFunction( s, g.minL, g.minL, HYB_F64 ) );
+}
+
+void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t stream )
+{
+   for ( auto& G : g.graphs )
+      if ( G.x == &x && G.b == &b && G.level == l && G.kind == kind )
+      {
+         HYB_CUDA( cudaGraphLaunch( G.exec, stream ) );
+         g_launches.fetch_add( G.kernels, std::memory_order_relaxed );
+         return;
+      }
+   prepare( g );
+   if ( g.progTop >= g.minL )
+   {
+      const int top = std::min( l, g.progTop );
+      if ( kind == kCycle64 || kind == kCycle64Norm )
+         ensureProgram< double >( g, x, b, *g.tmp64, top );
+      if ( kind > kFmg64 && kind <= kFmg64 + 8 )
+         for ( int t = g.minL; t <= top; ++t )
+            ensureProgram< double >( g, x, b, *g.tmp64, t );
+      if ( kind == kMixedStep )
+         ensureProgram< float >( g, *g.x32, *g.b32, *g.t32, top );
+   }
+   if ( !g.cap )
+      HYB_CUDA( cudaStreamCreateWithFlags( &g.cap, cudaStreamNonBlocking ) );
+   // make the capture stream wait for prior work on the caller's stream
+   cudaEvent_t ev;
+   HYB_CUDA( cudaEventCreateWithFlags( &ev, cudaEventDisableTiming ) );
+   HYB_CUDA( cudaEventRecord( ev, stream ) );
+   HYB_CUDA( cudaStreamWaitEvent( g.cap, ev, 0 ) );
+   HYB_CUDA( cudaStreamSynchronize( g.cap ) );
+   HYB_CUDA( cudaEventDestroy( ev ) );
+   cudaGraph_t     graph = nullptr;
+   const long long before = g_launches.load();
+   HYB_CUDA( cudaStreamBeginCapture( g.cap, cudaStreamCaptureModeThreadLocal ) );
+   try
+   {
+      enqueue( g, x, b, l, kind, g.cap );
+   }
+   catch ( ... )
+   {
+      cudaStreamEndCapture( g.cap, &graph );
+      if ( graph )
+         cudaGraphDestroy( graph );
+      throw;
+   }
+   HYB_CUDA( cudaStreamEndCapture( g.cap, &graph ) );
+   const long long captured = g_launches.load() - before;
+   g_launches.fetch_sub( captured ); // counted when the graph runs
+   cudaGraphExec_t exec;
+   HYB_CUDA( cudaGraphInstantiate( &exec, graph, 0 ) );
+   HYB_CUDA( cudaGraphDestroy( graph ) );
+   g.graphs.push_back( { &x, &b, l, kind, exec, captured } );
+   HYB_CUDA( cudaGraphLaunch( exec, stream ) );
+   g_launches.fetch_add( captured );
+}

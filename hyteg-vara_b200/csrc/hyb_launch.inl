@@ -1,0 +1,476 @@
+// Kernel launchers of the level operations, row tables, coarse CG and the Chebyshev
+// coefficients.
+// (part of the single translation unit hyb_capi.cu, included inside namespace hyb)
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+inline int bdryBlocks( const LevelDev& d ) { return ( d.nBdry + kBdryThreads - 1 ) / kBdryThreads; }
+
+template < typename T >
+void launchFromDofs( const Storage& s, int l, T* slab, const T* dofs, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   pdlLaunch( k_from_dofs< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, slab, dofs );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchToDofs( const Storage& s, int l, const T* slab, T* dofs, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   pdlLaunch( k_to_dofs< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, slab, dofs );
+   HYB_CHECK_LAUNCH();
+}
+
+// Levels whose closure slabs hold at most this many points (all cells) get full row tables
+// (HYB_ROW_TABLE_MAX_POINTS overrides it, 0: none); larger levels up to the second bound
+// get the surface colours' rows only (HYB_ROW_IFACE_MAX_POINTS): their interior passes
+// are bandwidth bound and keep the interior point tables.
+constexpr long kRowTableMaxPoints = 400000;
+constexpr long kRowIfaceMaxPoints = 4000000;
+
+long envLong( const char* name, long dflt )
+{
+   const char* e = std::getenv( name );
+   return e ? std::atol( e ) : dflt;
+}
+long rowTableMaxPoints()
+{
+   static const long v = envLong( "HYB_ROW_TABLE_MAX_POINTS", kRowTableMaxPoints );
+   return v;
+}
+long rowIfaceMaxPoints()
+{
+   static const long v = envLong( "HYB_ROW_IFACE_MAX_POINTS", kRowIfaceMaxPoints );
+   return v;
+}
+
+// The row tables of level l, built on first use (not inside a stream capture); nullptr if
+// the level is too large, or if a DoF has more embeddings than its lane group (then the
+// passes keep the lane-group path).
+const RowTables* ensureRows( Storage& s, int l )
+{
+   LevelHost& L = *s.lv[size_t( l )];
+   if ( L.rowsTried )
+      return L.rows.get();
+   L.rowsTried = true;
+   const LevelDev& d      = L.dev;
+   const long      points = long( s.td.nC ) * d.stride;
+   if ( points > std::max( rowTableMaxPoints(), rowIfaceMaxPoints() ) || d.stride >= 65536 )
+      return nullptr;
+   auto R  = std::make_unique< RowTables >();
+   R->full = points <= rowTableMaxPoints();
+   DevBuf< int >    err;
+   err.alloc( 1 );
+   HYB_CUDA( cudaMemset( err.p, 0, sizeof( int ) ) );
+   auto grid = [&]( long n ) { return dim3( unsigned( std::max< long >( 1, std::min< long >( ( n + 255 ) / 256, 4096 ) ) ) ); };
+   // surface colours
+   long total = 0;
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      R->ifaceOff.push_back( total );
+      const int* co = &L.colourOff[4 * c];
+      total += bdryLaneCount( co[1], co[2], co[3] );
+   }
+   R->iface.alloc( size_t( std::max< long >( total, 1 ) ) );
+   for ( int c = 0; c < s.td.m; ++c )
+   {
+      const int* co    = &L.colourOff[4 * c];
+      const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+      if ( lanes == 0 )
+         continue;
+      const int32_t*  list = L.colourList.p + co[0];
+      const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+      k_rows_surface<<< grid( lanes ), 256 >>>( s.td, d, bl, lanes, R->iface.p + R->ifaceOff[size_t( c )], err.p );
+      HYB_CHECK_LAUNCH();
+   }
+   if ( !R->full )
+   {
+      int bad = 0;
+      HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
+      if ( bad )
+         return nullptr;
+      L.rows = std::move( R );
+      return L.rows.get();
+   }
+   // interior colours
+   const long nInt = long( s.td.nC ) * d.nPts;
+   R->interior.alloc( size_t( std::max< long >( nInt, 1 ) ) );
+   for ( int c = 0; c < kInteriorColours; ++c )
+   {
+      const int count = d.ptsOff[c + 1] - d.ptsOff[c];
+      if ( count == 0 )
+         continue;
+      k_rows_interior<<< grid( long( s.td.nC ) * count ), 256 >>>( s.td, d, d.ptsC + d.ptsOff[c], count,
+                                                                  R->interior.p + long( s.td.nC ) * d.ptsOff[c] );
+      HYB_CHECK_LAUNCH();
+   }
+   // all DoFs
+   const int       nv = s.td.nV, ne = s.td.nE * ( d.N - 1 ), nf = s.td.nF * d.nIntFace;
+   const BdryLists full{ nullptr, nullptr, nullptr, nv, ne, nf };
+   const long      surf = bdryLaneCount( nv, ne, nf );
+   R->allB1             = long( nv ) * 32;
+   R->allB2             = R->allB1 + ( long( ne ) * 8 + 31 ) / 32 * 32;
+   R->allB3             = surf;
+   R->allN              = surf + nInt;
+   R->all.alloc( size_t( std::max< long >( R->allN, 1 ) ) );
+   if ( surf > 0 )
+   {
+      k_rows_surface<<< grid( surf ), 256 >>>( s.td, d, full, surf, R->all.p, err.p );
+      HYB_CHECK_LAUNCH();
+   }
+   if ( nInt > 0 )
+   {
+      k_rows_interior<<< grid( nInt ), 256 >>>( s.td, d, d.pts, d.nPts, R->all.p + surf );
+      HYB_CHECK_LAUNCH();
+   }
+   int bad = 0;
+   HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
+   if ( bad )
+      return nullptr;
+   L.rows = std::move( R );
+   return L.rows.get();
+}
+
+// the row table of level l if it has been built (usable inside a capture)
+const RowTables* rowsIf( const Storage& s, int l ) { return s.lv[size_t( l )]->rows.get(); }
+
+RowPass rowPassAll( const RowTables* R )
+{
+   return R && R->full ? RowPass{ R->all.p, R->allN, R->allB1, R->allB2, R->allB3 } : RowPass{ nullptr, 0, 0, 0, 0 };
+}
+
+template < typename T >
+void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs, int flag, int mode, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.dev.nPts > 0 ? ( op.variable ? L.ptsBlocks : L.quadBlocks ) : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
+   if ( nb == 0 )
+      return;
+   const OpDev< T > od = op.dev< T >( l );
+   if ( mode == kResidual || mode == kReplace )
+      if ( const RowTables* R = rowsIf( s, l ); R && R->full )
+      {
+         // small and middle levels: the precomputed rows (residual r = b - A u, or r = A u)
+         const RowPass rp = rowPassAll( R );
+         const int     g  = int( std::max< long >( 1, std::min< long >( ( rp.n + 127 ) / 128, long( s.numSMs ) * 8 ) ) );
+         T*            u  = const_cast< T* >( src );
+#define HYB_ROWS( M, V ) pdlLaunch( k_row_pass< T, M, V >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag )
+         if ( mode == kResidual )
+         {
+            if ( op.variable )
+               HYB_ROWS( kRowResidual, true );
+            else
+               HYB_ROWS( kRowResidual, false );
+         }
+         else
+         {
+            if ( op.variable )
+               HYB_ROWS( kRowApply, true );
+            else
+               HYB_ROWS( kRowApply, false );
+         }
+#undef HYB_ROWS
+         HYB_CHECK_LAUNCH();
+         return;
+      }
+#define HYB_APPLY( VAR, MODE ) pdlLaunch( k_apply< T, VAR, MODE >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, flag, nc )
+   if ( op.variable )
+   {
+      if ( mode == kReplace )
+         HYB_APPLY( true, kReplace );
+      else if ( mode == kAdd )
+         HYB_APPLY( true, kAdd );
+      else
+         HYB_APPLY( true, kResidual );
+   }
+   else
+   {
+      if ( mode == kReplace )
+         HYB_APPLY( false, kReplace );
+      else if ( mode == kAdd )
+         HYB_APPLY( false, kAdd );
+      else
+         HYB_APPLY( false, kResidual );
+   }
+#undef HYB_APPLY
+   HYB_CHECK_LAUNCH();
+}
+
+// levels whose cells hold at most this many interior points run the four interior SOR
+// colours in one launch (a block per cell); HYB_FUSED_INTERIOR_MAX overrides it
+static const int kFusedInteriorMaxPoints = [] {
+   const char* e = std::getenv( "HYB_FUSED_INTERIOR_MAX" );
+   return e ? std::atoi( e ) : 4096;
+}();
+
+template < typename T >
+void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, cudaStream_t stream, bool backwards = false )
+{
+   const Storage&   s  = *op.st;
+   const auto&      L  = s.L( l );
+   const OpDev< T > od = op.dev< T >( l );
+   // interface passes: one launch per colour over that colour's surface DoFs
+   const RowTables* R = rowsIf( s, l );
+   auto iface = [&]( int c ) {
+      const int* co = &L.colourOff[4 * c];
+      const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+      if ( lanes == 0 )
+         return;
+      const int       nb   = int( std::min< long >( ( lanes + 127 ) / 128, long( s.numSMs ) * 8 ) );
+      if ( R )
+      {
+         const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
+         const RowPass rp{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes };
+         if ( op.variable )
+            pdlLaunch( k_row_pass< T, kRowSor, true >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs, (T*) nullptr,
+                       relax, flag );
+         else
+            pdlLaunch( k_row_pass< T, kRowSor, false >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs, (T*) nullptr,
+                       relax, flag );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
+      const int32_t*  list = L.colourList.p + co[0];
+      const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
+      if ( op.variable )
+         pdlLaunch( k_sor_iface< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
+      else
+         pdlLaunch( k_sor_iface< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
+      HYB_CHECK_LAUNCH();
+   };
+   // interior passes
+   auto interior = [&]() {
+      if ( L.dev.nPts == 0 )
+         return;
+      // small levels: the four interior colours in one launch, a block per cell
+      if ( L.dev.nPts <= kFusedInteriorMaxPoints )
+      {
+         const int* o  = L.dev.ptsOff;
+         const int  bw = backwards ? 1 : 0;
+         if ( op.variable )
+            pdlLaunch( k_sor_interior_cells< T, true >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, o[0], o[1], o[2], o[3], o[4], bw );
+         else
+            pdlLaunch( k_sor_interior_cells< T, false >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, o[0], o[1], o[2], o[3], o[4], bw );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
+      // one launch per colour
+      for ( int k = 0; k < kInteriorColours; ++k )
+      {
+         const int c     = backwards ? kInteriorColours - 1 - k : k;
+         const int begin = L.dev.ptsOff[c], count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
+         if ( count == 0 )
+            continue;
+         if ( op.variable )
+            pdlLaunch( k_sor_interior< T, true >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, c, begin, count, L.colourBlocks );
+         else
+            pdlLaunch( k_sor_interior< T, false >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
+                       relax, c, begin, count, L.colourBlocks );
+         HYB_CHECK_LAUNCH();
+      }
+   };
+   // forward: surface colours 0..m-1, then the interior colours 0..3; backwards (the
+   // multicolour smooth_sor_backwards, P1Operator.hpp:385-400): the same passes reversed
+   if ( !backwards )
+   {
+      for ( int c = 0; c < s.td.m; ++c )
+         iface( c );
+      interior();
+   }
+   else
+   {
+      interior();
+      for ( int c = s.td.m - 1; c >= 0; --c )
+         iface( c );
+   }
+}
+
+template < typename T >
+void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs, T relax, int flag, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
+   if ( nb == 0 )
+      return;
+   const OpDev< T > od = op.dev< T >( l );
+   if ( op.variable )
+      pdlLaunch( k_jacobi< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
+   else
+      pdlLaunch( k_jacobi< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchProlongate( const Storage& s, int coarseL, const T* coarse, T* fine, int flag, bool add, cudaStream_t stream )
+{
+   const auto& F  = s.L( coarseL + 1 );
+   const auto& C  = s.L( coarseL );
+   const int   nc = F.dev.nPts > 0 ? F.ptsBlocks : 0;
+   const int   nb = nc + ( F.dev.nBdry > 0 ? F.bdryBlocks : 0 );
+   if ( nb == 0 )
+      return;
+   if ( add )
+      pdlLaunch( k_prolongate< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
+   else
+      pdlLaunch( k_prolongate< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, F.dev, C.dev.W, C.dev.stride, coarse, fine, flag, nc );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchRestrict( const Storage& s, int fineL, const T* fine, T* coarse, int flag, cudaStream_t stream )
+{
+   const auto& F  = s.L( fineL );
+   const auto& C  = s.L( fineL - 1 );
+   const int   nc = C.dev.nSeg > 0 ? C.cellBlocks : 0;
+   const int   nb = nc + ( C.dev.nBdry > 0 ? C.bdryBlocks : 0 );
+   if ( nb == 0 )
+      return;
+   pdlLaunch( k_restrict< T >, dim3( nb ), dim3( 128 ), 0, stream, s.td, C.dev, F.dev.W, F.dev.stride, fine, coarse, flag, nc );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchLincomb( const Storage& s, int l, T* dst, int n, const double* sc, const T* const* src, bool add, int flag,
+                    cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   pdlLaunch( k_lincomb< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, dst, n, T( n > 0 ? sc[0] : 0 ), n > 0 ? src[0] : nullptr, T( n > 1 ? sc[1] : 0 ),
+       n > 1 ? src[1] : nullptr, T( n > 2 ? sc[2] : 0 ), n > 2 ? src[2] : nullptr, add ? 1 : 0, flag );
+   HYB_CHECK_LAUNCH();
+}
+
+// dot product into the device double `result`, with one partial sum per block in `partial`
+// (at least maxPartialSlots( s ) doubles)
+template < typename T >
+void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, double* partial, double* result,
+                cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   pdlLaunch( k_dot_partial< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, a, b, flag, partial );
+   HYB_CHECK_LAUNCH();
+   pdlLaunch( k_reduce_final, dim3( 1 ), dim3( 1024 ), 0, stream, partial, L.slabBlocks * s.td.nC, result );
+   HYB_CHECK_LAUNCH();
+}
+
+// dot product into the storage's device scalar slot `slot`
+template < typename T >
+void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, int slot, cudaStream_t stream )
+{
+   launchDot< T >( s, l, a, b, flag, s.partial.p, s.scalars.p + slot, stream );
+}
+
+template < typename TD, typename TS >
+void launchConvert( const Storage& s, int l, TD* dst, const TS* src, cudaStream_t stream )
+{
+   const auto&  L = s.L( l );
+   const size_t n = size_t( s.td.nC ) * L.dev.stride;
+   pdlLaunch( k_convert< TD, TS >, dim3( unsigned( ( n + 255 ) / 256 ) ), dim3( 256 ), 0, stream, L.dev, dst, src, s.td.nC );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchAddCorrection( const Storage& s, int l, double* x, const T* e, int flag, cudaStream_t stream )
+{
+   const auto& L = s.L( l );
+   pdlLaunch( k_add_correction< double, T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, x, e, flag );
+   HYB_CHECK_LAUNCH();
+}
+
+// Coarse CG in FP64 on device scratch (x, b given; r, p, ap scratch)
+struct CgScratch
+{
+   std::unique_ptr< Function > r, p, ap;
+   DevBuf< int >               status;
+};
+
+
+void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch& cs, double tol, int maxIter,
+               cudaStream_t stream )
+{
+   const Storage& s = *op.st;
+   if ( !cs.r || cs.r->minL > l || cs.r->maxL < l )
+   {
+      cs.r.reset( makeFunction( op.st, l, l, HYB_F64 ) );
+      cs.p.reset( makeFunction( op.st, l, l, HYB_F64 ) );
+      cs.ap.reset( makeFunction( op.st, l, l, HYB_F64 ) );
+      cs.status.alloc( 4 );
+   }
+   const OpDev< double > od = op.dev< double >( l );
+   const RowPass         rp = rowPassAll( rowsIf( s, l ) );
+   if ( op.variable )
+      pdlLaunch( k_cg< true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
+                                             cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
+   else
+      pdlLaunch( k_cg< false >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
+                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
+   HYB_CHECK_LAUNCH();
+}
+
+// ChebyshevSmoother::setupCoefficients (src/hyteg/solvers/ChebyshevSmoother.hpp:98-188):
+// the power-basis coefficients w_0 .. w_{k-1} of p with 1 - l p(l) = T_k((th - l) / de) /
+// T_k(th / de) on the eigenvalue interval [lower, upper] of D^-1 A (th, de its midpoint and
+// half width, T_k the Chebyshev polynomial of the first kind, expanded by its three-term
+// recurrence); the smoother adds p(D^-1 A) D^-1 (b - A x) to x. Orders 1 to 5.
+std::vector< double > chebyshevCoefficients( int order, double lower, double upper )
+{
+   require( order >= 1 && order <= 5, "Chebyshev order must be in [1, 5]" );
+   require( std::isfinite( lower ) && std::isfinite( upper ) && 0 < lower && lower < upper,
+            "Chebyshev bounds must satisfy 0 < lower < upper" );
+   const double th = 0.5 * ( upper + lower ), de = 0.5 * ( upper - lower );
+   const double a = th / de, c = -1.0 / de; // T_k's argument a + c l
+   std::vector< double > prev( order + 1, 0.0 ), cur( order + 1, 0.0 ), next( order + 1, 0.0 );
+   prev[0] = 1.0;
+   cur[0]  = a;
+   cur[1]  = c;
+   for ( int n = 1; n < order; ++n )
+   {
+      std::fill( next.begin(), next.end(), 0.0 );
+      for ( int i = 0; i <= n; ++i )
+      {
+         next[i] += 2 * a * cur[i] - prev[i];
+         next[i + 1] += 2 * c * cur[i];
+      }
+      prev.swap( cur );
+      cur.swap( next );
+   }
+   std::vector< double > w( order );
+   for ( int i = 1; i <= order; ++i )
+      w[i - 1] = -cur[i] / cur[0];
+   return w;
+}
+
+// diag(A)^-1 of level l into out (every replica)
+template < typename T >
+void launchInvDiag( const Operator& op, int l, const T* zeros, T* out, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
+   if ( nb == 0 )
+      return;
+   const OpDev< T > od = op.dev< T >( l );
+   if ( op.variable )
+      k_inv_diag< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
+   else
+      k_inv_diag< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
+   HYB_CHECK_LAUNCH();
+}
+
+template < typename T >
+void launchChebUpdate( const Storage& s, int l, const T* inv, T* t, T* x, T w, cudaStream_t stream )
+{
+   const long long n = (long long) s.td.nC * s.L( l ).dev.stride;
+   const int       g = int( std::max< long long >( 1, std::min< long long >( ( n + 255 ) / 256, (long long) s.numSMs * 8 ) ) );
+   pdlLaunch( k_cheb_update< T >, dim3( g ), dim3( 256 ), 0, stream, n, inv, t, x, w );
+   HYB_CHECK_LAUNCH();
+}
