@@ -963,10 +963,10 @@ int hyb_function_dot_noalloc( hyb_function* ah, hyb_function* bh, int level, int
    // every slot the reduction reads is rewritten by the first pass, so nothing is cleared
    if ( a->dtype == HYB_F64 )
       k_dot_partial< double ><<< dim3( L.slabBlocks, st.td.nC ), 256, 0, S( stream ) >>>(
-          st.td, L.dev, a->ptr< double >( level ), b->ptr< double >( level ), flag, scratch );
+          st.td, L.dev, a->ptr< double >( level ), b->ptr< double >( level ), flag, scratch, nullptr );
    else
       k_dot_partial< float ><<< dim3( L.slabBlocks, st.td.nC ), 256, 0, S( stream ) >>>(
-          st.td, L.dev, a->ptr< float >( level ), b->ptr< float >( level ), flag, scratch );
+          st.td, L.dev, a->ptr< float >( level ), b->ptr< float >( level ), flag, scratch, nullptr );
    HYB_CHECK_LAUNCH();
    k_reduce_final<<< 1, 1024, 0, S( stream ) >>>( scratch, int( slots ), out_device );
    HYB_CHECK_LAUNCH();

@@ -397,8 +397,8 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
       vcycle< double >( g, x, b, *g.tmp64, l, s );
    if ( kind == kMixedStep )
    {
-      // FP32 V-cycle on the residual equation (mixedPrecisionIterativeRefinement.cpp:162-171)
-      launchConvert< float, double >( *g.st, l, g.b32->ptr< float >( l ), g.r64->ptr< double >( l ), s );
+      // FP32 V-cycle on the residual equation (mixedPrecisionIterativeRefinement.cpp:162-171);
+      // the FP32 right-hand side was written with the previous residual's norm (below)
       HYB_CUDA( cudaMemsetAsync( g.x32->ptr< float >( l ), 0, g.x32->levelBytes( l ), s ) );
       vcycle< float >( g, *g.x32, *g.b32, *g.t32, l, s );
       launchAddCorrection< float >( *g.st, l, x.ptr< double >( l ), g.x32->ptr< float >( l ), kGmgFlag, s );
@@ -418,9 +418,12 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
    }
    if ( kind != kCycle64 )
    {
-      Function& r = ( kind == kCycle64Norm || kind == kNorm64 ) ? *g.tmp64 : *g.r64;
+      const bool mixed = kind == kMixedStep || kind == kNormMixed;
+      Function&  r     = mixed ? *g.r64 : *g.tmp64;
       launchApply< double >( *g.op, l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ), kGmgFlag, kResidual, s );
-      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, g.partial.p, g.scalars.p, s );
+      // ||r||^2; for the mixed solver the same pass writes the next FP32 right-hand side
+      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, g.partial.p, g.scalars.p, s,
+                           mixed ? g.b32->ptr< float >( l ) : nullptr );
    }
 }
 

@@ -1364,10 +1364,12 @@ __global__ void k_add_correction( TopoDev tp, LevelDev lv, T* __restrict__ x, co
    x[i] += T( e[i] );
 }
 
-// Partial dot products over the canonical replica of every DoF whose BC is in flag.
+// Partial dot products over the canonical replica of every DoF whose BC is in flag. With
+// cvt given, the pass also writes float(a) at every closure point (the mixed-precision
+// refinement's FP32 right-hand side from the FP64 residual, read once for both).
 template < typename T >
 __global__ void k_dot_partial( TopoDev tp, LevelDev lv, const T* __restrict__ a, const T* __restrict__ b, int flag,
-                               double* __restrict__ partial )
+                               double* __restrict__ partial, float* __restrict__ cvt )
 {
    HYB_PDL_PROLOGUE();
    __shared__ double red[32];
@@ -1376,6 +1378,8 @@ __global__ void k_dot_partial( TopoDev tp, LevelDev lv, const T* __restrict__ a,
    double    v    = 0;
    if ( idx < lv.S )
    {
+      if ( cvt )
+         cvt[size_t( cell ) * lv.stride + idx] = float( a[size_t( cell ) * lv.stride + idx] );
       const int p    = lv.xyz[idx];
       const int mask = classMask( lv.N, p & 1023, ( p >> 10 ) & 1023, p >> 20 );
       const ClassDev cd = tp.cls[cell * 16 + mask];

@@ -352,10 +352,11 @@ void launchLincomb( const Storage& s, int l, T* dst, int n, const double* sc, co
 // (at least maxPartialSlots( s ) doubles)
 template < typename T >
 void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, double* partial, double* result,
-                cudaStream_t stream )
+                cudaStream_t stream, float* cvt = nullptr )
 {
    const auto& L = s.L( l );
-   pdlLaunch( k_dot_partial< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, a, b, flag, partial );
+   pdlLaunch( k_dot_partial< T >, dim3( dim3( L.slabBlocks, s.td.nC ) ), dim3( 256 ), 0, stream, s.td, L.dev, a, b, flag, partial,
+              cvt );
    HYB_CHECK_LAUNCH();
    pdlLaunch( k_reduce_final, dim3( 1 ), dim3( 1024 ), 0, stream, partial, L.slabBlocks * s.td.nC, result );
    HYB_CHECK_LAUNCH();
