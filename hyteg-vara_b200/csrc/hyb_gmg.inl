@@ -419,11 +419,16 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
    if ( kind != kCycle64 )
    {
       const bool mixed = kind == kMixedStep || kind == kNormMixed;
-      Function&  r     = mixed ? *g.r64 : *g.tmp64;
+      float*     cvt   = mixed ? g.b32->ptr< float >( l ) : nullptr;
+      const RowTables* R = rowsIf( *g.st, l );
+      // ||r||^2 in the residual pass itself (r is not stored); for the mixed solver the same
+      // pass writes the next FP32 right-hand side
+      if ( !( R && R->full ) && launchResidualNorm< double >( *g.op, l, x.ptr< double >( l ), b.ptr< double >( l ), kGmgFlag,
+                                                              g.partial.p, g.partial.n, g.scalars.p, cvt, s ) )
+         return;
+      Function& r = mixed ? *g.r64 : *g.tmp64;
       launchApply< double >( *g.op, l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ), kGmgFlag, kResidual, s );
-      // ||r||^2; for the mixed solver the same pass writes the next FP32 right-hand side
-      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, g.partial.p, g.scalars.p, s,
-                           mixed ? g.b32->ptr< float >( l ) : nullptr );
+      launchDot< double >( *g.st, l, r.ptr< double >( l ), r.ptr< double >( l ), kGmgFlag, g.partial.p, g.scalars.p, s, cvt );
    }
 }
 

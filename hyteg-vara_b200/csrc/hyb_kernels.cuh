@@ -19,6 +19,8 @@ enum ApplyMode : int
    kReplace  = 0,
    kAdd      = 1,
    kResidual = 2, // dst = rhs - A src
+   kResidualNorm = 3, // r = rhs - A src is not stored: its squares over the owned active DoFs
+                      // accumulate into *acc, and float(r) goes to cvt when given
 };
 
 // Programmatic dependent launch: a kernel lets the next kernel of its stream be scheduled
@@ -660,7 +662,7 @@ __device__ __forceinline__ void quadApply( const T* u, const T w[15], const Sten
 template < typename T, bool VAR, int MODE >
 __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, const T* src,
                                                   T* dst, const T* rhs, int flag,
-                                                  int nCellBlocks )
+                                                  int nCellBlocks, double* acc = nullptr, float* cvt = nullptr )
 {
    if constexpr ( !VAR )
    {
@@ -695,8 +697,15 @@ __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDe
                   dst[idx] = ax[r];
                else if constexpr ( MODE == kAdd )
                   dst[idx] += ax[r];
-               else
+               else if constexpr ( MODE == kResidual )
                   dst[idx] = rhs[idx] - ax[r];
+               else
+               {
+                  const T res = rhs[idx] - ax[r];
+                  *acc += double( res ) * double( res );
+                  if ( cvt )
+                     cvt[idx] = float( res );
+               }
             }
          }
          return;
@@ -733,8 +742,15 @@ __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDe
                dst[idx] = ax[k];
             else if constexpr ( MODE == kAdd )
                dst[idx] += ax[k];
-            else
+            else if constexpr ( MODE == kResidual )
                dst[idx] = rhs[idx] - ax[k];
+            else
+            {
+               const T res = rhs[idx] - ax[k];
+               *acc += double( res ) * double( res );
+               if ( cvt )
+                  cvt[idx] = float( res );
+            }
          }
       }
       return;
@@ -758,6 +774,15 @@ __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDe
          v = dst[r0] + ax;
       else
          v = rhs[r0] - ax;
+      if constexpr ( MODE == kResidualNorm )
+      {
+         // the first embedding's lane counts the DoF once; every replica gets float(r)
+         if ( tk.sub == 0 )
+            *acc += double( v ) * double( v );
+         if ( cvt )
+            bdryWriteGroup( tp, lv, p, tk, cvt, float( v ) );
+         continue;
+      }
       // every lane of the group has read dst[r0] before any replica is written
       __syncwarp( __activemask() );
       bdryWriteGroup( tp, lv, p, tk, dst, v );
@@ -771,6 +796,25 @@ __global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_apply( TopoDev tp, Level
 {
    HYB_PDL_PROLOGUE();
    applyBody< T, VAR, MODE >( launchBlk(), tp, lv, op, src, dst, rhs, flag, nCellBlocks );
+}
+
+__device__ double blockSum( double v, double* red );
+
+// ||rhs - A src||^2 over the owned active DoFs without storing the residual: one partial
+// per block (summed by k_reduce_final in a fixed order); float(r) into cvt when given.
+template < typename T, bool VAR >
+__global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_residual_norm( TopoDev tp, LevelDev lv, OpDev< T > op,
+                                                                      const T* __restrict__ src, const T* __restrict__ rhs,
+                                                                      int flag, int nCellBlocks, double* __restrict__ partial,
+                                                                      float* __restrict__ cvt )
+{
+   HYB_PDL_PROLOGUE();
+   __shared__ double red[32];
+   double            acc = 0;
+   applyBody< T, VAR, kResidualNorm >( launchBlk(), tp, lv, op, src, nullptr, rhs, flag, nCellBlocks, &acc, cvt );
+   const double s = blockSum( acc, red );
+   if ( threadIdx.x == 0 )
+      partial[blockIdx.x] = s;
 }
 
 // ---------------------------------------------------------------------------

@@ -369,6 +369,30 @@ void launchDot( const Storage& s, int l, const T* a, const T* b, int flag, int s
    launchDot< T >( s, l, a, b, flag, s.partial.p, s.scalars.p + slot, stream );
 }
 
+// ||b - A x||^2 (owned DoFs on flag) into *result without storing the residual (levels
+// without full row tables), float(r) into cvt when given. Returns false, launching nothing,
+// when partial has fewer slots than the launch has blocks.
+template < typename T >
+bool launchResidualNorm( const Operator& op, int l, const T* x, const T* b, int flag, double* partial, size_t partialSlots,
+                         double* result, float* cvt, cudaStream_t stream )
+{
+   const Storage& s  = *op.st;
+   const auto&    L  = s.L( l );
+   const int      nc = L.dev.nPts > 0 ? ( op.variable ? L.ptsBlocks : L.quadBlocks ) : 0;
+   const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
+   if ( nb < 1 || size_t( nb ) > partialSlots )
+      return false;
+   const OpDev< T > od = op.dev< T >( l );
+   if ( op.variable )
+      pdlLaunch( k_residual_norm< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, x, b, flag, nc, partial, cvt );
+   else
+      pdlLaunch( k_residual_norm< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, x, b, flag, nc, partial, cvt );
+   HYB_CHECK_LAUNCH();
+   pdlLaunch( k_reduce_final, dim3( 1 ), dim3( 1024 ), 0, stream, partial, nb, result );
+   HYB_CHECK_LAUNCH();
+   return true;
+}
+
 template < typename TD, typename TS >
 void launchConvert( const Storage& s, int l, TD* dst, const TS* src, cudaStream_t stream )
 {
