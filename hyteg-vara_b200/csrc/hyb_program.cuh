@@ -99,7 +99,6 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
       const Phase&   P      = sP[ph & 1];
       const int      kind   = P.kind;
       const int      blocks = P.blocks;
-      const LevelDev lv     = levelAt( P.level );
       // row passes spread over every thread of the block
       const bool rowPass = P.rp.rows && ( kind == kPhSorIface || kind == kPhSorInterior || kind == kPhResidual );
       if ( rowPass )
@@ -114,6 +113,7 @@ __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, cons
       }
       for ( int b = int( blockIdx.x ); !rowPass && b < blocks; b += int( gridDim.x ) )
       {
+         const LevelDev& lv = levelAt( P.level );
          const Blk       vb{ b, blocks };
          const long long t0 = (long long) b * blockDim.x + threadIdx.x, step = (long long) blocks * blockDim.x;
          switch ( kind )
