@@ -163,9 +163,22 @@ struct Level
    std::vector< std::array< int32_t, 4 > > ent;
 };
 
+// IcosahedralShellMap of one macro-cell (src/hyteg/geometry/IcosahedralShellMap.hpp:286-303):
+// the ref/ray vertex pair on one radial ray, the two remaining vertices, the pair's radii.
+struct ShellMap
+{
+   std::array< double, 3 > ref, ray, thr, fou;
+   double                  radRef = 0, radRay = 0;
+};
+
 struct Op
 {
    bool variable = false;
+   // blending (p1_div_k_grad_blending_q3 on the IcosahedralShellMap): per-cell maps and the
+   // coefficient k(x) = exp( alpha (1 - |x|) ) of the mapped point
+   bool                    blend = false;
+   double                  alpha = 0;
+   std::vector< ShellMap > maps;
    // constant: stencil[level][cell][mask][15]
    std::vector< std::vector< std::array< std::array< double, 15 >, 16 > > > st;
    // variable: nodal k per level, element matrices K[level][cell][type][4][4]
@@ -382,6 +395,183 @@ void cellElementMatrices( const Oracle& o, int c, i64 N, std::array< std::array<
 }
 
 // ---------------------------------------------------------------------------
+// Blending: IcosahedralShellMap and the p1_div_k_grad_blending_q3 element matrix
+// ---------------------------------------------------------------------------
+using V3 = std::array< double, 3 >;
+inline V3     sub3( const V3& a, const V3& b ) { return { a[0] - b[0], a[1] - b[1], a[2] - b[2] }; }
+inline double dot3( const V3& a, const V3& b ) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline V3     cross3( const V3& a, const V3& b )
+{
+   return { a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0] };
+}
+
+// classifyTet + classifyVertices + findNonSkewTetInPrism
+// (src/hyteg/geometry/IcosahedralShellMap.hpp:299-344, 346-451, 454-492): the cell's vertices
+// are inner or outer by radius (within 0.1 % of the radial extent of the outer one); one outer
+// vertex = outwards, three = inwards, two = skew. The first vertex pair (in local order) whose
+// cross product vanishes relative to their radii (1e-14) lies on one ray. Outwards: ref = the
+// outer of the pair; inwards: ref = the inner one; thr = the last remaining local vertex, for
+// the other. A skew cell takes the map of the other cell at its first face (local order 012,
+// 013, 023, 123) that does not hold both pair vertices and has a second cell.
+bool classifyShell( const Oracle& o, const std::map< std::array< int, 3 >, std::vector< int > >& faceCells, int c,
+                    ShellMap& m, int depth )
+{
+   if ( depth > 16 )
+      return false;
+   const auto& t = o.T[size_t( c )];
+   double      rad[4], inner = 1e300, outer = 0;
+   for ( int k = 0; k < 4; ++k )
+   {
+      rad[k] = std::sqrt( dot3( o.V[t[k]], o.V[t[k]] ) );
+      inner  = std::min( inner, rad[k] );
+      outer  = std::max( outer, rad[k] );
+   }
+   const double eps    = ( outer - inner ) * 0.001;
+   int          nOuter = 0;
+   for ( int k = 0; k < 4; ++k )
+      nOuter += ( outer - rad[k] ) < eps ? 1 : 0;
+   if ( nOuter < 1 || nOuter > 3 )
+      return false;
+   int  iRef = -1, iRay = -1;
+   for ( int k = 0; k < 4 && iRef < 0; ++k )
+      for ( int j = k + 1; j < 4 && iRef < 0; ++j )
+      {
+         const V3 cr = cross3( o.V[t[k]], o.V[t[j]] );
+         bool     ok = true;
+         for ( int d = 0; d < 3; ++d )
+            ok = ok && std::abs( cr[d] ) / ( rad[k] * rad[j] ) <= 1e-14;
+         if ( ok )
+         {
+            iRef = k;
+            iRay = j;
+         }
+      }
+   if ( iRef < 0 )
+      return false;
+   if ( nOuter == 2 )
+   {
+      static const int kFace[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+      for ( const auto& f : kFace )
+      {
+         bool hasRef = false, hasRay = false;
+         for ( int a : f )
+         {
+            hasRef = hasRef || a == iRef;
+            hasRay = hasRay || a == iRay;
+         }
+         if ( hasRef && hasRay )
+            continue;
+         std::array< int, 3 > key = { t[f[0]], t[f[1]], t[f[2]] };
+         std::sort( key.begin(), key.end() );
+         for ( int other : faceCells.at( key ) )
+            if ( other != c )
+               return classifyShell( o, faceCells, other, m, depth + 1 );
+      }
+      return false;
+   }
+   int iThr = -1, iFor = -1;
+   for ( int k = 0; k < 4; ++k )
+      if ( k != iRef && k != iRay )
+         iThr = k;
+   for ( int k = 0; k < 4; ++k )
+      if ( k != iRef && k != iRay && k != iThr )
+         iFor = k;
+   if ( ( nOuter == 1 && rad[iRef] < rad[iRay] ) || ( nOuter == 3 && rad[iRef] > rad[iRay] ) )
+      std::swap( iRef, iRay );
+   m.ref    = o.V[t[iRef]];
+   m.ray    = o.V[t[iRay]];
+   m.thr    = o.V[t[iThr]];
+   m.fou    = o.V[t[iFor]];
+   m.radRef = std::sqrt( dot3( m.ref, m.ref ) );
+   m.radRay = std::sqrt( dot3( m.ray, m.ray ) );
+   return true;
+}
+
+// evalF (IcosahedralShellMap.hpp:99-136): the barycentric coordinate b of x with respect to
+// the ref vertex in the tet (ref, ray, thr, for) sets the new radius
+// radRay + |b| (radRef - radRay); x is scaled radially to it.
+V3 shellF( const ShellMap& m, const V3& x )
+{
+   const V3     nrm  = cross3( sub3( m.thr, m.ray ), sub3( m.fou, m.ray ) );
+   const double volT = dot3( sub3( m.ref, m.ray ), nrm ), volX = dot3( sub3( x, m.ray ), nrm );
+   const double bary = std::abs( volX / volT );
+   const double oldR = std::sqrt( dot3( x, x ) ), newR = m.radRay + bary * ( m.radRef - m.radRay );
+   return { x[0] * newR / oldR, x[1] * newR / oldR, x[2] * newR / oldR };
+}
+
+// evalDF (IcosahedralShellMap.hpp:173-223), derived from F(x) = x R(x) / |x| with
+// R = radRay + (radRef - radRay) volX / volT and grad volX = (thr - ray) x (for - ray):
+// DF = R/|x| (I - x x^T / |x|^2) + x (radRef - radRay) n^T / (volT |x|). Returns det DF.
+double shellDF( const ShellMap& m, const V3& x, double D[3][3] )
+{
+   const V3     nrm  = cross3( sub3( m.thr, m.ray ), sub3( m.fou, m.ray ) );
+   const double volT = dot3( sub3( m.ref, m.ray ), nrm ), volX = dot3( sub3( x, m.ray ), nrm );
+   const double s    = ( m.radRef - m.radRay ) / volT;
+   const double R    = m.radRay + s * volX;
+   const double r2 = dot3( x, x ), r = std::sqrt( r2 );
+   for ( int i = 0; i < 3; ++i )
+      for ( int j = 0; j < 3; ++j )
+         D[i][j] = R / r * ( ( i == j ? 1.0 : 0.0 ) - x[i] * x[j] / r2 ) + x[i] * s * nrm[j] / r;
+   return D[0][0] * ( D[1][1] * D[2][2] - D[1][2] * D[2][1] ) - D[0][1] * ( D[1][0] * D[2][2] - D[1][2] * D[2][0] ) +
+          D[0][2] * ( D[1][0] * D[2][1] - D[1][1] * D[2][0] );
+}
+
+// p1_div_k_grad_blending_q3::integrateAll, tetrahedron
+// (src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_blending_q3.cpp:412-1059):
+// A_ij = sum_q w_q k(F(xi_q)) |det J_aff| |det DF(xi_q)| (G_q g_i) . (G_q g_j), G_q = (DF J_aff)^-T,
+// g the reference gradients, the 5-point degree-3 rule (centroid, weight -2/15; the four
+// points with barycentric (1/2, 1/6, 1/6, 1/6), weight 3/40), xi_q the quadrature point in
+// computational coordinates; k(y) = exp( alpha (1 - |y|) ).
+void blendElementMatrix( const ShellMap& m, const V3 X[4], double alpha, double A[4][4] )
+{
+   const V3     e1 = sub3( X[1], X[0] ), e2 = sub3( X[2], X[0] ), e3 = sub3( X[3], X[0] );
+   const double detA = dot3( e1, cross3( e2, e3 ) );
+   // columns of J_aff^-T: the reference gradients of vertices 1..3 mapped to computational space
+   const V3 c1 = cross3( e2, e3 ), c2 = cross3( e3, e1 ), c3 = cross3( e1, e2 );
+   V3       ga[4];
+   for ( int d = 0; d < 3; ++d )
+   {
+      ga[1][d] = c1[d] / detA;
+      ga[2][d] = c2[d] / detA;
+      ga[3][d] = c3[d] / detA;
+      ga[0][d] = -( ga[1][d] + ga[2][d] + ga[3][d] );
+   }
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j )
+         A[i][j] = 0;
+   for ( int q = 0; q < 5; ++q )
+   {
+      double lam[4];
+      for ( int j = 0; j < 4; ++j )
+         lam[j] = q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 );
+      V3 xi = { 0, 0, 0 };
+      for ( int j = 0; j < 4; ++j )
+         for ( int d = 0; d < 3; ++d )
+            xi[d] += lam[j] * X[j][d];
+      double       D[3][3];
+      const double detD = shellDF( m, xi, D );
+      const V3     Fx   = shellF( m, xi );
+      const double k    = std::exp( alpha * ( 1.0 - std::sqrt( dot3( Fx, Fx ) ) ) );
+      // D^-T = cof(D) / det D
+      double C[3][3];
+      for ( int i = 0; i < 3; ++i )
+         for ( int j = 0; j < 3; ++j )
+         {
+            const int i1 = ( i + 1 ) % 3, i2 = ( i + 2 ) % 3, j1 = ( j + 1 ) % 3, j2 = ( j + 2 ) % 3;
+            C[i][j] = ( D[i1][j1] * D[i2][j2] - D[i1][j2] * D[i2][j1] ) / detD;
+         }
+      V3 g[4];
+      for ( int a = 0; a < 4; ++a )
+         for ( int i = 0; i < 3; ++i )
+            g[a][i] = C[i][0] * ga[a][0] + C[i][1] * ga[a][1] + C[i][2] * ga[a][2];
+      const double w = ( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * k * std::abs( detA ) * std::abs( detD );
+      for ( int i = 0; i < 4; ++i )
+         for ( int j = 0; j < 4; ++j )
+            A[i][j] += w * dot3( g[i], g[j] );
+   }
+}
+
+// ---------------------------------------------------------------------------
 // Row evaluation: the partial row of DoF at closure point p of cell c.
 // val(d) supplies the value of DoF d (current or snapshot, see smooth_sor).
 // ---------------------------------------------------------------------------
@@ -392,7 +582,7 @@ inline void partialRow( const Oracle& o, const Op& op, const Level& lv, int c, i
    const i64 N    = lv.N;
    const int mask = pointMask( N, x, y, z );
    const auto& map = lv.cellMap[c];
-   if ( !op.variable )
+   if ( !op.variable && !op.blend )
    {
       const auto& st = op.st[lv.L][c][mask];
       diag += T( st[0] );
@@ -402,6 +592,29 @@ inline void partialRow( const Oracle& o, const Op& op, const Level& lv, int c, i
          if ( !inClosure( N, xx, yy, zz ) )
             continue;
          off += T( st[q] ) * val( map[cellIdx( N + 1, xx, yy, zz )] );
+      }
+   }
+   else if ( op.blend )
+   {
+      for ( const auto& in : kIncident )
+      {
+         bool ok = true;
+         for ( int j = 0; j < 4 && ok; ++j )
+            ok = relAllowed( mask, in.rel[j] );
+         if ( !ok )
+            continue;
+         V3 X[4];
+         for ( int j = 0; j < 4; ++j )
+            X[j] = microCoord( o, c, N, x + in.rel[j][0], y + in.rel[j][1], z + in.rel[j][2] );
+         double A[4][4];
+         blendElementMatrix( op.maps[size_t( c )], X, op.alpha, A );
+         for ( int j = 0; j < 4; ++j )
+         {
+            if ( j == in.k )
+               diag += T( A[in.k][j] );
+            else
+               off += T( A[in.k][j] ) * val( map[cellIdx( N + 1, x + in.rel[j][0], y + in.rel[j][1], z + in.rel[j][2] )] );
+         }
       }
    }
    else
@@ -1259,6 +1472,77 @@ int orc_op_divkgrad( void* h, const double* const* nodalK )
    }
    o->ops.push_back( std::move( op ) );
    return int( o->ops.size() - 1 );
+}
+
+namespace {
+std::map< std::array< int, 3 >, std::vector< int > > faceCellLists( const Oracle& o )
+{
+   std::map< std::array< int, 3 >, std::vector< int > > fc;
+   static const int kFace[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+   for ( size_t c = 0; c < o.T.size(); ++c )
+      for ( const auto& f : kFace )
+      {
+         std::array< int, 3 > key = { o.T[c][f[0]], o.T[c][f[1]], o.T[c][f[2]] };
+         std::sort( key.begin(), key.end() );
+         fc[key].push_back( int( c ) );
+      }
+   return fc;
+}
+bool shellMaps( const Oracle& o, std::vector< ShellMap >& maps )
+{
+   const auto fc = faceCellLists( o );
+   maps.resize( o.T.size() );
+   for ( size_t c = 0; c < o.T.size(); ++c )
+      if ( !classifyShell( o, fc, int( c ), maps[c], 0 ) )
+         return false;
+   return true;
+}
+} // namespace
+
+int orc_op_blend_div_k_grad( void* h, double alpha )
+{
+   auto* o = H( h );
+   Op    op;
+   op.blend = true;
+   op.alpha = alpha;
+   if ( !shellMaps( *o, op.maps ) )
+      return -1;
+   o->ops.push_back( std::move( op ) );
+   return int( o->ops.size() - 1 );
+}
+
+int orc_shell_map_eval( void* h, int cell, const double* x, double* Fx, double* DF )
+{
+   std::vector< ShellMap > maps;
+   if ( !shellMaps( *H( h ), maps ) )
+      return -1;
+   const V3 p  = { x[0], x[1], x[2] };
+   const V3 f  = shellF( maps[size_t( cell )], p );
+   double   D[3][3];
+   shellDF( maps[size_t( cell )], p, D );
+   for ( int i = 0; i < 3; ++i )
+   {
+      Fx[i] = f[i];
+      for ( int j = 0; j < 3; ++j )
+         DF[3 * i + j] = D[i][j];
+   }
+   return 0;
+}
+
+int orc_blend_element_matrix( void* h, int cell, const double* X12, double alpha, double* out16 )
+{
+   std::vector< ShellMap > maps;
+   if ( !shellMaps( *H( h ), maps ) )
+      return -1;
+   V3 X[4];
+   for ( int j = 0; j < 4; ++j )
+      X[j] = { X12[3 * j], X12[3 * j + 1], X12[3 * j + 2] };
+   double A[4][4];
+   blendElementMatrix( maps[size_t( cell )], X, alpha, A );
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j )
+         out16[4 * i + j] = A[i][j];
+   return 0;
 }
 
 void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 )

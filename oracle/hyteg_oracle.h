@@ -43,6 +43,14 @@ int64_t orc_num_prims( void* h, int kind );
 // operators: 0 = constant P1 Laplace; then div-k-grad with nodal k per level
 int  orc_op_laplace( void* h );
 int  orc_op_divkgrad( void* h, const double* const* nodalK );
+// P1ElementwiseBlendingDivKGradOperator (p1_div_k_grad_blending_q3) on the macro-cells'
+// IcosahedralShellMaps with k(y) = exp( alpha (1 - |y|) ) of the mapped point; -1 if a cell
+// cannot be classified as a shell cell
+int  orc_op_blend_div_k_grad( void* h, double alpha );
+// the shell map of a cell at a computational point: F (3) and DF (3x3, row-major)
+int  orc_shell_map_eval( void* h, int cell, const double* x, double* Fx, double* DF );
+// the blended element matrix (4x4, row-major) of the micro-tet X (4 vertices x 3) in a cell
+int  orc_blend_element_matrix( void* h, int cell, const double* X12, double alpha, double* out16 );
 void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 );
 
 void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );

@@ -68,6 +68,12 @@ def lib():
         L.orc_inv_diag.argtypes = [P, I, I, P]
         L.orc_spectral_radius.restype = D
         L.orc_spectral_radius.argtypes = [P, I, I, I, P]
+        L.orc_op_blend_div_k_grad.restype = I
+        L.orc_op_blend_div_k_grad.argtypes = [P, D]
+        L.orc_shell_map_eval.restype = I
+        L.orc_shell_map_eval.argtypes = [P, I, P, P, P]
+        L.orc_blend_element_matrix.restype = I
+        L.orc_blend_element_matrix.argtypes = [P, I, P, D, P]
         L.orc_gmg_solve.restype = I
         L.orc_gmg_solve.argtypes = [P, I, I, I, P, P, I, I, D, I, P, I, D, I, D, I, P, I]
         _lib = L
@@ -114,6 +120,28 @@ class Oracle:
         self._keep = arrs
         ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
         return int(lib().orc_op_divkgrad(self.h, ptrs))
+
+    def op_blend_div_k_grad(self, alpha=0.0):
+        """P1ElementwiseBlendingDivKGradOperator on the cells' IcosahedralShellMaps,
+        k(y) = exp(alpha (1 - |y|)) at the mapped quadrature points."""
+        op = int(lib().orc_op_blend_div_k_grad(self.h, float(alpha)))
+        if op < 0:
+            raise ValueError("the mesh is not a spherical shell: a cell cannot be classified")
+        return op
+
+    def shell_map(self, cell, x):
+        F, DF = np.zeros(3), np.zeros(9)
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        if lib().orc_shell_map_eval(self.h, cell, _p(xx), _p(F), _p(DF)) != 0:
+            raise ValueError("the mesh is not a spherical shell")
+        return F, DF.reshape(3, 3)
+
+    def blend_element_matrix(self, cell, X, alpha=0.0):
+        A = np.zeros(16)
+        XX = np.ascontiguousarray(X, dtype=np.float64).reshape(12)
+        if lib().orc_blend_element_matrix(self.h, cell, _p(XX), float(alpha), _p(A)) != 0:
+            raise ValueError("the mesh is not a spherical shell")
+        return A.reshape(4, 4)
 
     def cell_stencil(self, level, cell, mask=0, op=0):
         out = np.zeros(15)
