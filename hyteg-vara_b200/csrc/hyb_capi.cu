@@ -525,6 +525,14 @@ int hyb_operator_create_divkgrad_rff( hyb_storage* s, int minL, int maxL, const 
    HYB_API_END
 }
 
+int hyb_operator_create_blend_divkgrad( hyb_storage* s, int minL, int maxL, double alpha, hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && out, "null argument" );
+   *out = reinterpret_cast< hyb_operator* >( makeBlendDivKGrad( ST( s ), minL, maxL, alpha ) );
+   HYB_API_END
+}
+
 int hyb_storage_dof_coords( const hyb_storage* s, int level, double* xyz )
 {
    HYB_API_BEGIN
@@ -649,7 +657,7 @@ int hyb_operator_cell_stencil( const hyb_operator* oh, int level, int cell, int 
    HYB_API_BEGIN
    const Operator* op = reinterpret_cast< const Operator* >( oh );
    require( op && out15, "null argument" );
-   require( !op->variable, "stencils are stored for constant-coefficient operators only" );
+   require( !op->variable && !op->blend, "stencils are stored for constant-coefficient operators only" );
    require( level >= op->minL && level <= op->maxL && cell >= 0 && cell < op->st->td.nC && mask >= 0 && mask < 16,
             "index out of range" );
    const auto& st = op->stHost[level - op->minL];

@@ -254,6 +254,13 @@ struct OpDev
    const T* K;   // variable coefficient: [nC][6][4][4] micro-tet matrices (1/4 folded in)
    const T* kap; // variable coefficient: nodal k, function layout
    int      stride;
+   // blending operator (curved shell): element matrices integrated on the fly per row
+   const double*  bcell;  // [nC][4][3] macro-cell vertex coordinates (computational domain)
+   const double*  bmap;   // [nC][8] shell map of the cell: ray vertex, n = (thr - ray) x (for - ray),
+                          // radRay, s = (radRef - radRay) / ((ref - ray) . n)
+   const int32_t* bxyz;   // closure index -> x | y<<10 | z<<20 of the level
+   double         balpha; // coefficient k(y) = exp( balpha (1 - |y|) )
+   int            bN;     // micro-edges per macro-edge (2^level)
 };
 
 // Partial row of the operator at closure point (x,y,z) of `cell`: the contributions

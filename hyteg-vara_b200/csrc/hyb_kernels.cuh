@@ -505,6 +505,156 @@ __global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, i
    }
 }
 
+// ---------------------------------------------------------------------------
+// Blending operator (P1ElementwiseBlendingDivKGradOperator: p1_div_k_grad_blending_q3 on the
+// IcosahedralShellMap, src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_blending_q3.cpp:412+,
+// src/hyteg/geometry/IcosahedralShellMap.hpp:99-223). The element matrix of a micro-tet
+// depends on its position, so a row integrates the matrices of its incident micro-tets on
+// the fly, always in FP64:
+//   A_kj = sum_q w_q k(F(xi_q)) |det J| |det DF(xi_q)| (G_q g_k) . (G_q g_j),  G_q = (DF J)^-T,
+// with the 5-point degree-3 rule (centroid: -2/15; barycentric (1/2,1/6,1/6,1/6): 3/40).
+// The shell map F(x) = x R(x)/|x|, R = radRay + s (x - ray) . n, has the rank-one Jacobian
+// DF = a I + u v^T (a = R/|x|, u = x/|x|, v = s n - R x/|x|^2), so det DF = a^2 (a + v.u) and
+// DF^-T c = (c - v (u.c)/(a + v.u)) / a; the 1/a^2 of the gradient product cancels against
+// det DF, leaving the weight w_q k_q |det J| |a + v.u|. k(y) = exp(alpha (1 - |y|)) with
+// |F(xi)| = R(xi).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const double X[4][3], int k, double alpha,
+                                             double row[4] )
+{
+   double e[3][3];
+#pragma unroll
+   for ( int j = 0; j < 3; ++j )
+#pragma unroll
+      for ( int d = 0; d < 3; ++d )
+         e[j][d] = X[j + 1][d] - X[0][d];
+   // columns of J^-T (the computational gradients of vertices 1..3), vertex 0 = minus their sum
+   double c[4][3];
+#pragma unroll
+   for ( int d = 0; d < 3; ++d )
+   {
+      const int d1 = ( d + 1 ) % 3, d2 = ( d + 2 ) % 3;
+      c[1][d] = e[1][d1] * e[2][d2] - e[1][d2] * e[2][d1];
+      c[2][d] = e[2][d1] * e[0][d2] - e[2][d2] * e[0][d1];
+      c[3][d] = e[0][d1] * e[1][d2] - e[0][d2] * e[1][d1];
+   }
+   const double detJ = e[0][0] * c[1][0] + e[0][1] * c[1][1] + e[0][2] * c[1][2];
+   const double inv  = 1.0 / detJ;
+#pragma unroll
+   for ( int d = 0; d < 3; ++d )
+   {
+      c[1][d] *= inv;
+      c[2][d] *= inv;
+      c[3][d] *= inv;
+      c[0][d] = -( c[1][d] + c[2][d] + c[3][d] );
+   }
+   const double ray[3] = { m[0], m[1], m[2] }, n[3] = { m[3], m[4], m[5] }, radRay = m[6], sc = m[7];
+#pragma unroll
+   for ( int j = 0; j < 4; ++j )
+      row[j] = 0.0;
+#pragma unroll
+   for ( int q = 0; q < 5; ++q )
+   {
+      double xi[3];
+#pragma unroll
+      for ( int d = 0; d < 3; ++d )
+      {
+         double acc = 0.0;
+#pragma unroll
+         for ( int j = 0; j < 4; ++j )
+            acc += ( q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][d];
+         xi[d] = acc;
+      }
+      const double r2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+      const double ir = rsqrt( r2 );
+      const double R  = radRay + sc * ( ( xi[0] - ray[0] ) * n[0] + ( xi[1] - ray[1] ) * n[1] + ( xi[2] - ray[2] ) * n[2] );
+      const double a  = R * ir;
+      double       u[3], v[3];
+#pragma unroll
+      for ( int d = 0; d < 3; ++d )
+      {
+         u[d] = xi[d] * ir;
+         v[d] = sc * n[d] - R * ir * ir * xi[d];
+      }
+      const double den = a + ( v[0] * u[0] + v[1] * u[1] + v[2] * u[2] );
+      const double kq  = alpha == 0.0 ? 1.0 : exp( alpha * ( 1.0 - R ) );
+      const double w   = ( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq * fabs( detJ ) * fabs( den );
+      const double iden = 1.0 / den;
+      // c' = c - v (u.c) / den for the row's vertex and every column vertex
+      double g[4][3];
+#pragma unroll
+      for ( int j = 0; j < 4; ++j )
+      {
+         const double uc = ( u[0] * c[j][0] + u[1] * c[j][1] + u[2] * c[j][2] ) * iden;
+#pragma unroll
+         for ( int d = 0; d < 3; ++d )
+            g[j][d] = c[j][d] - v[d] * uc;
+      }
+      double gk[3] = { 0, 0, 0 };
+#pragma unroll
+      for ( int j = 0; j < 4; ++j )
+         if ( j == k )
+         {
+            gk[0] = g[j][0];
+            gk[1] = g[j][1];
+            gk[2] = g[j][2];
+         }
+#pragma unroll
+      for ( int j = 0; j < 4; ++j )
+         row[j] += w * ( gk[0] * g[j][0] + gk[1] * g[j][1] + gk[2] * g[j][2] );
+   }
+}
+
+// diag and off-diagonal sum of the partial row of the closure point at slab position pos(0)
+// of `cell`: the blended matrices of the incident micro-tets allowed by the class (validT);
+// vertex coordinates as vertexdof::macrocell::coordinateFromIndex
+// (src/hyteg/p1functionspace/VertexDoFMacroCell.hpp:68-75): v0 + (v_k - v0)/N i_k.
+template < typename T, typename Pos >
+__device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int cell, uint32_t validT, Pos&& pos, T& diag,
+                                          T& off )
+{
+   const double* v  = op.bcell + size_t( cell ) * 12;
+   const double* m  = op.bmap + size_t( cell ) * 8;
+   const int     pk = op.bxyz[pos( 0 )];
+   const int     x = pk & 1023, y = ( pk >> 10 ) & 1023, z = pk >> 20;
+   double        h[3][3];
+#pragma unroll
+   for ( int j = 0; j < 3; ++j )
+#pragma unroll
+      for ( int d = 0; d < 3; ++d )
+         h[j][d] = ( v[3 * ( j + 1 ) + d] - v[d] ) / double( op.bN );
+   double dsum = 0.0, osum = 0.0;
+#pragma unroll 1
+   for ( int i = 0; i < 24; ++i )
+   {
+      if ( !( validT & ( 1u << i ) ) )
+         continue;
+      const IncidentTet it = incidentTet( i );
+      double            X[4][3];
+#pragma unroll
+      for ( int j = 0; j < 4; ++j )
+      {
+         const int q = it.q[j];
+         const int xx = x + offX( q ), yy = y + offY( q ), zz = z + offZ( q );
+#pragma unroll
+         for ( int d = 0; d < 3; ++d )
+            X[j][d] = v[d] + h[0][d] * double( xx ) + h[1][d] * double( yy ) + h[2][d] * double( zz );
+      }
+      double row[4];
+      blendTetRow( m, X, it.k, op.balpha, row );
+#pragma unroll
+      for ( int j = 0; j < 4; ++j )
+      {
+         if ( j == it.k )
+            dsum += row[j];
+         else
+            osum += row[j] * double( uc[pos( it.q[j] )] );
+      }
+   }
+   diag += T( dsum );
+   off += T( osum );
+}
+
 // the rows of a pass: lanes [0, b1) in groups of 32, [b1, b2) of 8, [b2, b3) of 2, the rest
 // single (b1, b2, b3 are multiples of 32, so a warp has one group size)
 struct RowPass
@@ -517,14 +667,15 @@ enum RowMode : int
 {
    kRowSor      = 0, // u = (1 - relax) u + relax (b - off) / diag
    kRowResidual = 1, // r = b - A u
-   kRowApply    = 2  // r = A u
+   kRowApply    = 2, // r = A u
+   kRowApplyAdd = 3  // r += A u
 };
 
 // one pass over the rows, lanes start, start + step, ... (start - lane and step multiples
 // of 32; the rows of one DoF are adjacent lanes of one warp). Constant operator: the
 // partial stencil st[wsel + q]; variable operator: the row's positions drive the
 // incident micro-tets' matrices and nodal coefficients (the variable branch of partialRow).
-template < typename T, int MODE, bool VAR >
+template < typename T, int MODE, bool VAR, bool BLEND = false >
 __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >& op, T* u, const T* b, T* r, T relax,
                                              int flag, long long start, long long step )
 {
@@ -548,7 +699,9 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
          const uint32_t h[8] = { uint32_t( A.w ), uint32_t( B.x ), uint32_t( B.y ), uint32_t( B.z ),
                                  uint32_t( B.w ), uint32_t( C.x ), uint32_t( C.y ), uint32_t( C.z ) };
          auto           pos  = [&]( int q ) { return int( ( q & 1 ) ? ( h[q >> 1] >> 16 ) : ( h[q >> 1] & 0xffffu ) ); };
-         if constexpr ( !VAR )
+         if constexpr ( BLEND )
+            blendRow( op, uc, A.y / 240, kValidTets[( A.y / 15 ) & 15], pos, diag, off );
+         else if constexpr ( !VAR )
          {
             const T* w = op.st + A.y;
             diag += w[0];
@@ -592,18 +745,20 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
          u[i] = ( T( 1 ) - relax ) * u[i] + relax * ( b[i] - off ) / diag;
       else if constexpr ( MODE == kRowResidual )
          r[i] = b[i] - ( diag * u[i] + off );
+      else if constexpr ( MODE == kRowApplyAdd )
+         r[i] += diag * u[i] + off;
       else
          r[i] = diag * u[i] + off;
    }
 }
 
 // a row pass as its own launch (levels between the program kernel's and the large ones)
-template < typename T, int MODE, bool VAR >
+template < typename T, int MODE, bool VAR, bool BLEND = false >
 __global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, OpDev< T > op, T* u, const T* b, T* r, T relax, int flag )
 {
    HYB_PDL_PROLOGUE();
-   rowPassBody< T, MODE, VAR >( rp, op, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
-                                (long long) gridDim.x * blockDim.x );
+   rowPassBody< T, MODE, VAR, BLEND >( rp, op, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
+                                       (long long) gridDim.x * blockDim.x );
 }
 
 // Constant-stencil quad: the points x = 4g + r, r = 0..3, of row (y, z). Each of the seven
@@ -1598,7 +1753,7 @@ __device__ void cgAxpby( const TopoDev& tp, const LevelDev& lv, double a, const 
 }
 
 // the whole CG in the calling thread block; red = 32 doubles of shared memory
-template < bool VAR >
+template < bool VAR, bool BLEND = false >
 __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< double >& op, double* x, const double* b,
                         double* r, double* p, double* ap, double tol, int maxIter, int* status, double* red,
                         const RowPass& rp )
@@ -1606,9 +1761,9 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
    const int flag = 1 | 4 | 8;
    // the operator through the level's row table when there is one
    auto applyA = [&]( const double* src, double* dst ) {
-      if ( rp.rows )
-         rowPassBody< double, kRowApply, VAR >( rp, op, const_cast< double* >( src ), nullptr, dst, 0.0, flag,
-                                                threadIdx.x, blockDim.x );
+      if ( BLEND || rp.rows )
+         rowPassBody< double, kRowApply, VAR, BLEND >( rp, op, const_cast< double* >( src ), nullptr, dst, 0.0, flag,
+                                                       threadIdx.x, blockDim.x );
       else
          cgApplyAll< VAR >( tp, lv, op, src, dst, flag );
    };
@@ -1657,14 +1812,14 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
    }
 }
 
-template < bool VAR >
+template < bool VAR, bool BLEND = false >
 __global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
                                                 double* r, double* p, double* ap, double tol, int maxIter, int* status,
                                                 RowPass rp )
 {
    HYB_PDL_PROLOGUE();
    __shared__ double red[32];
-   cgBody< VAR >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red, rp );
+   cgBody< VAR, BLEND >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red, rp );
 }
 
 } // namespace hyb

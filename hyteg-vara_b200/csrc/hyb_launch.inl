@@ -49,6 +49,8 @@ long rowIfaceMaxPoints()
 // The row tables of level l, built on first use (not inside a stream capture); nullptr if
 // the level is too large, or if a DoF has more embeddings than its lane group (then the
 // passes keep the lane-group path).
+std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool full );
+
 const RowTables* ensureRows( Storage& s, int l )
 {
    LevelHost& L = *s.lv[size_t( l )];
@@ -59,8 +61,32 @@ const RowTables* ensureRows( Storage& s, int l )
    const long      points = long( s.td.nC ) * d.stride;
    if ( points > std::max( rowTableMaxPoints(), rowIfaceMaxPoints() ) || d.stride >= 65536 )
       return nullptr;
+   L.rows = buildRows( s, l, points <= rowTableMaxPoints() );
+   return L.rows.get();
+}
+
+// full row tables of level l for blending operators (their only execution path)
+const RowTables* ensureBlendRows( Storage& s, int l )
+{
+   LevelHost& L = *s.lv[size_t( l )];
+   if ( L.blendRows )
+      return L.blendRows.get();
+   require( L.dev.stride < 65536,
+            "the blending operator supports levels whose cell closures have fewer than 65536 points (level <= 6)" );
+   L.blendRows = buildRows( s, l, true );
+   require( L.blendRows != nullptr, "row table construction failed (a DoF has more cells than its lane group)" );
+   return L.blendRows.get();
+}
+
+// the row tables of level l: the surface colours' rows, and with full also every colour's
+// interior rows and the rows of all DoFs; nullptr if a DoF has more embeddings than its lane
+// group has lanes
+std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool withInterior )
+{
+   LevelHost&      L = *s.lv[size_t( l )];
+   const LevelDev& d = L.dev;
    auto R  = std::make_unique< RowTables >();
-   R->full = points <= rowTableMaxPoints();
+   R->full = withInterior;
    DevBuf< int >    err;
    err.alloc( 1 );
    HYB_CUDA( cudaMemset( err.p, 0, sizeof( int ) ) );
@@ -91,8 +117,7 @@ const RowTables* ensureRows( Storage& s, int l )
       HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
       if ( bad )
          return nullptr;
-      L.rows = std::move( R );
-      return L.rows.get();
+      return R;
    }
    // interior colours
    const long nInt = long( s.td.nC ) * d.nPts;
@@ -129,8 +154,7 @@ const RowTables* ensureRows( Storage& s, int l )
    HYB_CUDA( cudaMemcpy( &bad, err.p, sizeof( int ), cudaMemcpyDeviceToHost ) );
    if ( bad )
       return nullptr;
-   L.rows = std::move( R );
-   return L.rows.get();
+   return R;
 }
 
 // the row table of level l if it has been built (usable inside a capture)
@@ -141,10 +165,38 @@ RowPass rowPassAll( const RowTables* R )
    return R && R->full ? RowPass{ R->all.p, R->allN, R->allB1, R->allB2, R->allB3 } : RowPass{ nullptr, 0, 0, 0, 0 };
 }
 
+// grid of a row pass over n rows (128 threads a block, at most 8 blocks per SM)
+inline int rowGrid( const Storage& s, long long n )
+{
+   return int( std::max< long long >( 1, std::min< long long >( ( n + 127 ) / 128, (long long) s.numSMs * 8 ) ) );
+}
+
+const RowTables& blendRowsOf( const Storage& s, int l )
+{
+   const RowTables* R = s.lv[size_t( l )]->blendRows.get();
+   require( R != nullptr && R->full, "the blending operator's row tables are missing" );
+   return *R;
+}
+
 template < typename T >
 void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs, int flag, int mode, cudaStream_t stream )
 {
    const Storage& s  = *op.st;
+   if ( op.blend )
+   {
+      const RowPass    rp = rowPassAll( &blendRowsOf( s, l ) );
+      const OpDev< T > od = op.dev< T >( l );
+      const int        g  = rowGrid( s, rp.n );
+      T*               u  = const_cast< T* >( src );
+      if ( mode == kResidual )
+         pdlLaunch( k_row_pass< T, kRowResidual, false, true >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
+      else if ( mode == kAdd )
+         pdlLaunch( k_row_pass< T, kRowApplyAdd, false, true >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
+      else
+         pdlLaunch( k_row_pass< T, kRowApply, false, true >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
+      HYB_CHECK_LAUNCH();
+      return;
+   }
    const auto&    L  = s.L( l );
    const int      nc = L.dev.nPts > 0 ? ( op.variable ? L.ptsBlocks : L.quadBlocks ) : 0;
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
@@ -213,6 +265,43 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
    const Storage&   s  = *op.st;
    const auto&      L  = s.L( l );
    const OpDev< T > od = op.dev< T >( l );
+   if ( op.blend )
+   {
+      // the same passes in the same order as below, every one through the blending rows
+      const RowTables& R    = blendRowsOf( s, l );
+      auto             pass = [&]( const RowPass& rp ) {
+         if ( rp.n == 0 )
+            return;
+         pdlLaunch( k_row_pass< T, kRowSor, false, true >, dim3( rowGrid( s, rp.n ) ), dim3( 128 ), 0, stream, rp, od, u,
+                    rhs, (T*) nullptr, relax, flag );
+         HYB_CHECK_LAUNCH();
+      };
+      auto surface = [&]( int c ) {
+         const int* co    = &L.colourOff[4 * c];
+         const long lanes = bdryLaneCount( co[1], co[2], co[3] );
+         const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
+         pass( RowPass{ R.iface.p + R.ifaceOff[size_t( c )], lanes, b1, b2, lanes } );
+      };
+      auto interiorColour = [&]( int c ) {
+         const long count = long( s.td.nC ) * ( L.dev.ptsOff[c + 1] - L.dev.ptsOff[c] );
+         pass( RowPass{ R.interior.p + long( s.td.nC ) * L.dev.ptsOff[c], count, 0, 0, 0 } );
+      };
+      if ( !backwards )
+      {
+         for ( int c = 0; c < s.td.m; ++c )
+            surface( c );
+         for ( int c = 0; c < kInteriorColours; ++c )
+            interiorColour( c );
+      }
+      else
+      {
+         for ( int c = kInteriorColours - 1; c >= 0; --c )
+            interiorColour( c );
+         for ( int c = s.td.m - 1; c >= 0; --c )
+            surface( c );
+      }
+      return;
+   }
    // interface passes: one launch per colour over that colour's surface DoFs
    const RowTables* R = rowsIf( s, l );
    auto iface = [&]( int c ) {
@@ -301,6 +390,7 @@ void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
+   require( !op.blend, "weighted Jacobi is not available for the blending operator (use SOR)" );
    const OpDev< T > od = op.dev< T >( l );
    if ( op.variable )
       pdlLaunch( k_jacobi< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
@@ -380,7 +470,7 @@ bool launchResidualNorm( const Operator& op, int l, const T* x, const T* b, int 
    const auto&    L  = s.L( l );
    const int      nc = L.dev.nPts > 0 ? ( op.variable ? L.ptsBlocks : L.quadBlocks ) : 0;
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
-   if ( nb < 1 || size_t( nb ) > partialSlots )
+   if ( op.blend || nb < 1 || size_t( nb ) > partialSlots )
       return false;
    const OpDev< T > od = op.dev< T >( l );
    if ( op.variable )
@@ -430,6 +520,13 @@ void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch&
       cs.status.alloc( 4 );
    }
    const OpDev< double > od = op.dev< double >( l );
+   if ( op.blend )
+   {
+      pdlLaunch( k_cg< false, true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ),
+                 cs.p->ptr< double >( l ), cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rowPassAll( &blendRowsOf( s, l ) ) );
+      HYB_CHECK_LAUNCH();
+      return;
+   }
    const RowPass         rp = rowPassAll( rowsIf( s, l ) );
    if ( op.variable )
       pdlLaunch( k_cg< true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
@@ -483,6 +580,7 @@ void launchInvDiag( const Operator& op, int l, const T* zeros, T* out, cudaStrea
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
+   require( !op.blend, "the Chebyshev smoother is not available for the blending operator (use SOR)" );
    const OpDev< T > od = op.dev< T >( l );
    if ( op.variable )
       k_inv_diag< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );

@@ -21,6 +21,7 @@ struct LevelHost
    LevelDev           dev{};
    std::unique_ptr< RowTables > rows; // built on first use (ensureRows)
    bool                         rowsTried = false;
+   std::unique_ptr< RowTables > blendRows; // full rows for blending operators (ensureBlendRows)
    DevBuf< int32_t >  seg, xyz, blk, blkXYZ, pts, ptsC, quads, rowYZ;
    DevBuf< int4 >     pro; // prolongation table (LevelDev::pro)
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
@@ -504,6 +505,10 @@ struct Operator
    Storage* st;
    int      minL, maxL;
    bool     variable = false;
+   // blending operator: per-cell shell maps, the coefficient's exponent, full row tables
+   bool             blend = false;
+   double           alpha = 0;
+   DevBuf< double > bmap;
    // per level (index l - minL)
    std::vector< std::unique_ptr< DevBuf< double > > > st64, K64;
    std::vector< std::unique_ptr< DevBuf< float > > >  st32, K32;
@@ -516,6 +521,17 @@ struct Operator
       require( l >= minL && l <= maxL, "level outside the operator's level range" );
       OpDev< T > o{};
       const int  i = l - minL;
+      o.stride     = st->L( l ).dev.stride;
+      if ( blend )
+      {
+         // no stencils or element matrices: the rows integrate the blended matrices
+         o.bcell  = st->cellCoords.p;
+         o.bmap   = bmap.p;
+         o.bxyz   = st->L( l ).dev.xyz;
+         o.balpha = alpha;
+         o.bN     = st->L( l ).dev.N;
+         return o;
+      }
       if constexpr ( std::is_same< T, double >::value )
       {
          o.st = variable ? nullptr : st64[i]->p;
@@ -528,7 +544,6 @@ struct Operator
          o.K  = variable ? K32[i]->p : nullptr;
          o.kap = variable ? kap32->ptr< float >( l ) : nullptr;
       }
-      o.stride = st->L( l ).dev.stride;
       return o;
    }
 };
@@ -569,6 +584,119 @@ Operator* makeLaplace( Storage* s, int minL, int maxL )
       op->st32.push_back( std::move( b32 ) );
       op->stHost.push_back( std::move( st ) );
    }
+   return op.release();
+}
+
+// IcosahedralShellMap of macro-cell c (src/hyteg/geometry/IcosahedralShellMap.hpp:299-492):
+// vertices are inner or outer by radius (within 0.1 % of the radial extent of the outer
+// one): one outer vertex = an outwards cell, three = inwards, two = skew. The first local
+// vertex pair whose cross product vanishes relative to their radii (1e-14) lies on one ray;
+// outwards: ref = the pair's outer vertex, inwards: its inner one; thr = the last other local
+// vertex, for = the remaining one. A skew cell takes the map of the second cell of its first
+// face (local order 012, 013, 023, 123) that does not hold both pair vertices. Stored as the
+// ray vertex, n = (thr - ray) x (for - ray), radRay and (radRef - radRay) / ((ref - ray) . n).
+bool shellMapOfCell( const Topology& tp, int c, double out[8], int depth = 0 )
+{
+   if ( depth > 16 )
+      return false;
+   const auto& t = tp.T[size_t( c )];
+   auto        norm = []( const std::array< double, 3 >& a ) { return std::sqrt( a[0] * a[0] + a[1] * a[1] + a[2] * a[2] ); };
+   double      rad[4], inner = 1e300, outer = 0;
+   for ( int k = 0; k < 4; ++k )
+   {
+      rad[k] = norm( tp.V[t[k]] );
+      inner  = std::min( inner, rad[k] );
+      outer  = std::max( outer, rad[k] );
+   }
+   const double eps    = ( outer - inner ) * 0.001;
+   int          nOuter = 0;
+   for ( int k = 0; k < 4; ++k )
+      nOuter += ( outer - rad[k] ) < eps ? 1 : 0;
+   if ( nOuter < 1 || nOuter > 3 )
+      return false;
+   int iRef = -1, iRay = -1;
+   for ( int k = 0; k < 4 && iRef < 0; ++k )
+      for ( int j = k + 1; j < 4 && iRef < 0; ++j )
+      {
+         const auto& a  = tp.V[t[k]];
+         const auto& b  = tp.V[t[j]];
+         const double cr[3] = { a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0] };
+         if ( std::abs( cr[0] ) / ( rad[k] * rad[j] ) <= 1e-14 && std::abs( cr[1] ) / ( rad[k] * rad[j] ) <= 1e-14 &&
+              std::abs( cr[2] ) / ( rad[k] * rad[j] ) <= 1e-14 )
+         {
+            iRef = k;
+            iRay = j;
+         }
+      }
+   if ( iRef < 0 )
+      return false;
+   if ( nOuter == 2 )
+   {
+      static const int kFace[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+      for ( const auto& f : kFace )
+      {
+         const bool hasRef = f[0] == iRef || f[1] == iRef || f[2] == iRef;
+         const bool hasRay = f[0] == iRay || f[1] == iRay || f[2] == iRay;
+         if ( hasRef && hasRay )
+            continue;
+         std::array< int, 3 > key = { t[f[0]], t[f[1]], t[f[2]] };
+         std::sort( key.begin(), key.end() );
+         for ( const Embedding& e : tp.fEmb[size_t( tp.faceId.at( key ) )] )
+            if ( e.cell != c )
+               return shellMapOfCell( tp, e.cell, out, depth + 1 );
+      }
+      return false;
+   }
+   int iThr = -1, iFor = -1;
+   for ( int k = 0; k < 4; ++k )
+      if ( k != iRef && k != iRay )
+         iThr = k;
+   for ( int k = 0; k < 4; ++k )
+      if ( k != iRef && k != iRay && k != iThr )
+         iFor = k;
+   if ( ( nOuter == 1 && rad[iRef] < rad[iRay] ) || ( nOuter == 3 && rad[iRef] > rad[iRay] ) )
+      std::swap( iRef, iRay );
+   const auto &ref = tp.V[t[iRef]], &ray = tp.V[t[iRay]], &thr = tp.V[t[iThr]], &fou = tp.V[t[iFor]];
+   const double b[3] = { thr[0] - ray[0], thr[1] - ray[1], thr[2] - ray[2] };
+   const double d[3] = { fou[0] - ray[0], fou[1] - ray[1], fou[2] - ray[2] };
+   const double n[3] = { b[1] * d[2] - b[2] * d[1], b[2] * d[0] - b[0] * d[2], b[0] * d[1] - b[1] * d[0] };
+   const double volT = ( ref[0] - ray[0] ) * n[0] + ( ref[1] - ray[1] ) * n[1] + ( ref[2] - ray[2] ) * n[2];
+   out[0] = ray[0];
+   out[1] = ray[1];
+   out[2] = ray[2];
+   out[3] = n[0];
+   out[4] = n[1];
+   out[5] = n[2];
+   out[6] = norm( ray );
+   out[7] = ( norm( ref ) - out[6] ) / volT;
+   return true;
+}
+
+const RowTables* ensureBlendRows( Storage& s, int l );
+
+// P1ElementwiseBlendingDivKGradOperator (src/hyteg/elementwiseoperators/P1ElementwiseOperator.hpp:349,
+// form p1_div_k_grad_blending_q3) on the cells' IcosahedralShellMaps with
+// k(y) = exp( alpha (1 - |y|) ) at the mapped quadrature points (alpha = 0: the Laplacian of
+// the curved shell). Every operation runs through full row tables, so the levels are
+// limited to cell closures below 65536 points (level 6).
+Operator* makeBlendDivKGrad( Storage* s, int minL, int maxL, double alpha )
+{
+   require( minL >= 0 && minL <= maxL && maxL <= s->maxLevel, "invalid level range" );
+   require( std::isfinite( alpha ), "alpha must be finite" );
+   auto op   = std::make_unique< Operator >();
+   op->st    = s;
+   op->minL  = minL;
+   op->maxL  = maxL;
+   op->blend = true;
+   op->alpha = alpha;
+   const int             nC = s->td.nC;
+   std::vector< double > maps( size_t( nC ) * 8 );
+   for ( int c = 0; c < nC; ++c )
+      require( shellMapOfCell( s->topo, c, &maps[size_t( c ) * 8] ),
+               "the mesh is not a spherical shell: a macro-cell has no shell map" );
+   op->bmap.upload( maps );
+   for ( int l = minL; l <= maxL; ++l )
+      ensureBlendRows( *s, l );
    return op.release();
 }
 

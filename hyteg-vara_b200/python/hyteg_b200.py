@@ -32,7 +32,7 @@ SYMBOLS = [
     "hyb_operator_smooth_sor", "hyb_operator_smooth_jac", "hyb_operator_cell_stencil", "hyb_prolongate",
     "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
-    "hyb_operator_create_divkgrad_rff", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
+    "hyb_operator_create_divkgrad_rff", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
     "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
@@ -114,6 +114,7 @@ def load(path=LIB_PATH):
         "hyb_function_dot_noalloc": (I, [P, P, I, I, P, P]),
         "hyb_function_fill_uniform_random": (I, [P, I, ctypes.c_uint64, D, P]),
         "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, D, PP]),
+        "hyb_operator_create_blend_divkgrad": (I, [P, I, I, D, PP]),
         "hyb_storage_create_spherical_shell": (I, [I, I, D, D, I, PP]),
         "hyb_gmg_solve_fmg": (I, [P, P, P, I, I, P]),
         "hyb_storage_create_from_gmsh": (I, [ctypes.c_char_p, I, PP]),
@@ -397,6 +398,20 @@ class P1ElementwiseDivKGradOperator(_Operator):
                                                        ctypes.byref(h)))
         op.h = h
         return op
+
+
+class P1ElementwiseBlendingDivKGradOperator(_Operator):
+    """P1ElementwiseOperator<p1_div_k_grad_blending_q3> on a spherical-shell mesh whose cells
+    carry the IcosahedralShellMap (IcosahedralShellMap::setMap); the coefficient is
+    k(y) = exp(alpha (1 - |y|)) at the mapped quadrature points (alpha = 0: Laplacian).
+    Element matrices are integrated on the device per row; levels up to 6."""
+
+    def __init__(self, storage, min_level, max_level, alpha=0.0):
+        self.storage = storage
+        h = ctypes.c_void_p()
+        _check(load().hyb_operator_create_blend_divkgrad(storage.h, min_level, max_level, float(alpha),
+                                                         ctypes.byref(h)))
+        self.h = h
 
 
 class P1toP1LinearProlongation:

@@ -19,6 +19,10 @@
  *   hyb_operator_create_laplace   P1ConstantLaplaceOperator (P1ConstantOperator.cpp:603-655 stencil assembly)
  *   hyb_operator_create_divkgrad  P1ElementwiseOperator<forms::p1_div_k_grad_affine_q3>
  *                                 (src/hyteg/elementwiseoperators/P1ElementwiseOperator.cpp:64-302)
+ *   hyb_operator_create_blend_divkgrad  P1ElementwiseBlendingDivKGradOperator
+ *                                 (src/hyteg/elementwiseoperators/P1ElementwiseOperator.hpp:349, form
+ *                                 p1_div_k_grad_blending_q3) with IcosahedralShellMap::setMap
+ *                                 (src/hyteg/geometry/IcosahedralShellMap.hpp:225-250)
  *   hyb_operator_apply            Operator::apply(src, dst, level, flag, updateType) (P1Operator.hpp:196)
  *   hyb_operator_smooth_sor       SORSmoothable::smooth_sor(dst, rhs, relax, level, flag) (P1Operator.hpp:343-422)
  *   hyb_operator_smooth_sor_backwards  SORBackwardsSmoothable::smooth_sor_backwards (P1Operator.hpp:424-431)
@@ -177,6 +181,14 @@ int hyb_operator_create_divkgrad_callback( hyb_storage* s, int min_level, int ma
  * micro-vertex of every level; blocking */
 int hyb_operator_create_divkgrad_rff( hyb_storage* s, int min_level, int max_level, const double* w,
                                       const double* phase, int modes, double sigma, double radial, hyb_operator** out );
+/* the curved-shell operator: every macro-cell of a spherical-shell mesh gets its
+ * IcosahedralShellMap, and the element matrices of p1_div_k_grad_blending_q3 (5-point rule,
+ * map Jacobian at the quadrature points) are integrated on the device per row, with
+ * k(y) = exp( alpha (1 - |y|) ) at the mapped points (alpha = 0: the Laplacian). Levels
+ * up to 6; apply, residual, (symmetric/backward) SOR, CG and GMG with SOR smoothers
+ * (no Jacobi or Chebyshev); HYB_ERR_ARG when a cell has no shell map */
+int hyb_operator_create_blend_divkgrad( hyb_storage* s, int min_level, int max_level, double alpha,
+                                        hyb_operator** out );
 int hyb_operator_destroy( hyb_operator* op );
 int hyb_operator_apply( hyb_operator* op, hyb_function* src, hyb_function* dst, int level, int flag, int update,
                         void* stream );

@@ -1,0 +1,147 @@
+"""Curved-shell (blending) operator on the GPU against the CPU oracle: every macro-cell of a
+spherical shell carries its IcosahedralShellMap and the element matrices of
+p1_div_k_grad_blending_q3 are integrated per row on the device. Apply (replace, add,
+residual), multicolour SOR forward and backward, the coarse CG and V-cycles must match the
+oracle (whose map and form are pinned to the reference's compiled code) to 1e-12 for
+applies, 1e-11 for sweeps and 1e-10 for cycles, the tolerances of the other parity tests."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def shell(oracle_mod):
+    import hyteg_b200 as H
+
+    H.load()
+    L = 3
+    st = H.PrimitiveStorage.spherical_shell(3, 2, 0.55, 1.0, L)
+    coords, tets = st.mesh()
+    orc = oracle_mod.Oracle(coords, tets, L)
+    return H, st, orc, L
+
+
+def close(a, b, rtol):
+    err = np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+    assert err <= rtol, f"max relative error {err:.3e} > {rtol:.1e}"
+
+
+@pytest.mark.parametrize("alpha", [0.0, 5.0])
+def test_blend_apply_matches_oracle(shell, alpha):
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, alpha)
+    op = orc.op_blend_div_k_grad(alpha)
+    rng = np.random.default_rng(21)
+    for level in range(L + 1):
+        x = rng.uniform(-1, 1, orc.n(level))
+        y = rng.uniform(-1, 1, orc.n(level))
+        fs, fd = H.P1Function("s", st, 0, L), H.P1Function("d", st, 0, L)
+        fs.set(x, level)
+        _, bc = orc.info(level)
+        for flag in (H.ALL, H.INNER):
+            A.apply(fs, fd, level, flag)
+            mask = (bc & flag) != 0
+            if mask.any():
+                close(fd.get(level)[mask], orc.apply(x, level, flag=flag, op=op)[mask], 1e-12)
+        fd.set(y, level)
+        A.apply(fs, fd, level, H.ALL, update=H.ADD)
+        close(fd.get(level), y + orc.apply(x, level, flag=H.ALL, op=op), 1e-12)
+
+
+def test_blend_residual_and_cg_match_oracle(shell):
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    rng = np.random.default_rng(22)
+    level = 2
+    x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+    fx, fb, fr = (H.P1Function(n, st, 0, L) for n in "xbr")
+    fx.set(x, level)
+    fb.set(b, level)
+    A.residual(fx, fb, fr, level, 1 | 4)
+    _, bc = orc.info(level)
+    inner = (bc & (1 | 4)) != 0
+    close(fr.get(level)[inner], (b - orc.apply(x, level, op=op))[inner], 1e-12)
+    # coarse CG on level 1 (zero Dirichlet values)
+    bb = rng.uniform(-1, 1, orc.n(1))
+    _, bc1 = orc.info(1)
+    bb[(bc1 & (1 | 4)) == 0] = 0
+    fx.set(np.zeros(orc.n(1)), 1)
+    fb.set(bb, 1)
+    it, conv = H.CGSolver(1e-13, 1000).solve(A, fx, fb, 1)
+    assert conv
+    xr = np.zeros(orc.n(1))
+    orc.cg(xr, bb, 1, tol=1e-13, op=op)
+    close(fx.get(1), xr, 1e-10)
+
+
+@pytest.mark.parametrize("backwards", [False, True])
+def test_blend_multicolour_sor_matches_oracle(shell, backwards):
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    m, labels = st.colouring()
+    rng = np.random.default_rng(23)
+    for level in range(1, L + 1):
+        x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+        fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+        fx.set(x, level)
+        fb.set(b, level)
+        for _ in range(2):
+            if backwards:
+                A.smooth_sor_backwards(fx, fb, 1.1, level, 1 | 4)
+            else:
+                A.smooth_sor(fx, fb, 1.1, level, 1 | 4)
+            orc.sor_colored(x, b, level, labels, m, relax=1.1, flag=1 | 4, op=op, backwards=backwards)
+        close(fx.get(level), x, 1e-11)
+
+
+@pytest.mark.parametrize("smoother", ["SOR", "SYMMETRIC_SOR"])
+def test_blend_vcycle_matches_oracle(shell, smoother):
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    m, labels = st.colouring()
+    rng = np.random.default_rng(24)
+    b = rng.uniform(-1, 1, orc.n(L))
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    code = {"SOR": (H.SMOOTHER_SOR, 1), "SYMMETRIC_SOR": (H.SMOOTHER_SYMMETRIC_SOR, 4)}[smoother]
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, smoother=code[0])
+    x = np.zeros(orc.n(L))
+    for _ in range(2):
+        gmg.solve(fx, fb, L)
+    orc.gmg(x, b, 0, L, pre=2, post=2, relax=1.0, smoother=code[1], labels=labels, m=m, coarse_tol=1e-12,
+            max_cycles=2, op=op)
+    close(fx.get(L), x, 1e-10)
+
+
+def test_blend_mixed_precision_solve_converges(shell):
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    rng = np.random.default_rng(25)
+    b = rng.uniform(-1, 1, orc.n(L))
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0)
+    hist = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=40, precision=32)
+    assert hist[-1] <= 1e-8 * hist[0]
+    _, bc = orc.info(L)
+    inner = (bc & (1 | 4)) != 0
+    r = (b - orc.apply(fx.get(L), L, op=op))[inner]
+    assert np.linalg.norm(r) <= 1.01e-8 * np.linalg.norm(b[inner])
+
+
+def test_blend_rejects_other_meshes_and_smoothers(shell):
+    H, st, orc, L = shell
+    cube = H.PrimitiveStorage.cuboid(1, 1, 1, 2)
+    with pytest.raises(RuntimeError):
+        H.P1ElementwiseBlendingDivKGradOperator(cube, 0, 2, 0.0)
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 0.0)
+    with pytest.raises(RuntimeError):
+        H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, smoother=H.SMOOTHER_CHEBYSHEV)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    with pytest.raises(RuntimeError):
+        A.smooth_jac(fx, fb, fb, 0.6, L, 1 | 4)
