@@ -257,6 +257,11 @@ def ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         shell = spherical_shell(args, H, I, stream)
 
+    blend = None
+    if not args.no_blend:
+        torch.cuda.synchronize()
+        blend = blended_shell(args, H, stream)
+
     serve = None
     if not args.no_serve:
         torch.cuda.synchronize()
@@ -293,7 +298,7 @@ def ours(args, rank, world, local_rank):
             "roofline_sor_fp32": dict(roof(sor32_gbs, sweep32_traffic, "ncu, profiles/k_sor_fp64_fp32_level7_cube48.md"),
                                       kernel="k_sor_iface + k_sor_interior (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
-            "variable_coefficient": varcoef, "spherical_shell": shell, "serving": serve,
+            "variable_coefficient": varcoef, "spherical_shell": shell, "blended_shell": blend, "serving": serve,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -419,6 +424,71 @@ def spherical_shell(args, H, I, stream, ntan=5, nrad=4, L=6):
             "error_mixed_vs_fp64_solution": err, "as_serving_requests": served}
 
 
+# FP64 flops of one blended micro-tet row evaluation (blendTetRow plus the four vertex
+# positions): the map Jacobian, its rank-one inverse and the five quadrature points
+BLEND_FLOPS_PER_TET_ROW = 830
+FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (CUDA cores), nominal; no measured FP64 peak on this pool
+
+
+def blended_shell(args, H, stream, ntan=5, nrad=4, L=5):
+    """The curved shell: the mesh of the spherical-shell leg with every macro-cell carrying
+    its IcosahedralShellMap, -div(k grad u) = f with p1_div_k_grad_blending_q3 element
+    matrices integrated on the device per row, k = exp(5 (1 - |x|)) at the mapped points,
+    f ~ U[-1,1] seeded; V(2,2) cycles, mixed precision and FP64 to 1e-8, and the FP64
+    apply's arithmetic rate (4 N^3 micro-tet rows per cell and apply)."""
+    import torch
+
+    sh = stream.cuda_stream
+    t0 = time.perf_counter()
+    st = H.PrimitiveStorage.spherical_shell(ntan, nrad, 0.55, 1.0, L)
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    setup_s = time.perf_counter() - t0
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, coarse_tol=1e-12)
+    u, b = H.P1Function("u", st, 0, L), H.P1Function("f", st, 0, L)
+    b.fill_uniform_random(L, 0, float(1 << 20), stream=sh)
+    out = {}
+    for prec in (32, 64):
+        u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+        gmg.solve_to_tolerance(u, b, L, TOL, max_cycles=2, precision=prec, stream=sh)
+        torch.cuda.synchronize()
+        u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hist = gmg.solve_to_tolerance(u, b, L, TOL, max_cycles=100, precision=prec, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[prec] = (e0.elapsed_time(e1), len(hist) - 1, float(hist[-1]))
+    y = H.P1Function("y", st, L, L)
+    for _ in range(2):
+        A.apply(b, y, L, H.ALL, stream=sh)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(stream)
+    for _ in range(reps):
+        A.apply(b, y, L, H.ALL, stream=sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_apply = e0.elapsed_time(e1) / reps / 1e3
+    n_cells = 60 * (ntan - 1) ** 2 * (nrad - 1)
+    flops = 4 * (1 << L) ** 3 * n_cells * BLEND_FLOPS_PER_TET_ROW
+    ndofs = st.num_dofs(L)
+    del gmg, A, u, b, y, st
+    torch.cuda.synchronize()
+    return {"workload": f"curved spherical shell ntan={ntan} nrad={nrad} r in [0.55, 1], {n_cells} macro-tets with "
+                        f"IcosahedralShellMap, level {L}, p1_div_k_grad_blending_q3 with k=exp(5(1-|x|)), "
+                        f"V(2,2) multicolour SOR, to rel. residual 1e-8",
+            "dofs": ndofs, "setup_s": setup_s,
+            "time_to_tol_ms": {"mixed": out[32][0], "fp64": out[64][0]},
+            "cycles": {"mixed": out[32][1], "fp64": out[64][1]},
+            "final_rel_residual": {"mixed": out[32][2], "fp64": out[64][2]},
+            "apply": {"kernel": "k_row_pass<double, kRowApply, blend> (FP64 apply, all rows)", "ms": t_apply * 1e3,
+                      "bound": "fp64", "achieved_tflops": flops / t_apply / 1e12,
+                      "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_source": "nominal",
+                      "frac": flops / t_apply / 1e12 / FP64_NOMINAL_TFLOPS,
+                      "flops_per_apply": flops, "flops_per_tet_row": BLEND_FLOPS_PER_TET_ROW}}
+
+
 def serve_stream(n, rate, seed, levels=(3, 7), cubes=(1, 4)):
     """Open-loop request stream: Poisson arrivals at `rate` per second; per request a
     cuboid mesh of c x c x c macro-cubes (c uniform in `cubes`), a level uniform in
@@ -542,7 +612,8 @@ def single_op(args):
     """Run one level operation repeatedly (for ncu captures of a single kernel):
     --op apply|residual|sor|sor32|restrict|prolong at --level on the bench mesh, or
     --op vcycle: FP64 V(3,3) cycles from --level down to level 0 (program kernel, row
-    passes of the middle levels, CG)."""
+    passes of the middle levels, CG); --op blend_apply: the blending operator's FP64 apply
+    on the curved shell (ntan 5, nrad 4) at --level."""
     import torch
 
     import build as B
@@ -551,6 +622,20 @@ def single_op(args):
 
     B.build()
     L, nc = args.level, args.cubes
+    if args.op == "blend_apply":
+        # the curved shell (ntan 5, nrad 4) with the blending operator, FP64 apply
+        st = H.PrimitiveStorage.spherical_shell(5, 4, 0.55, 1.0, L)
+        A = H.P1ElementwiseBlendingDivKGradOperator(st, L, L, 5.0)
+        b, y = H.P1Function("b", st, L, L), H.P1Function("y", st, L, L)
+        b.fill_uniform_random(L, 0, float(1 << 20))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            A.apply(b, y, L, H.ALL)
+        torch.cuda.synchronize()
+        print(json.dumps({"op": args.op, "level": L, "dofs": st.num_dofs(L), "reps": args.steps,
+                          "us_per_call_wall": (time.perf_counter() - t0) / args.steps * 1e6}))
+        return
     st = H.PrimitiveStorage.cuboid(nc, nc, nc, L)
     A = H.P1ConstantLaplaceOperator(st, 0, L)
     dt = H.F32 if args.op == "sor32" else H.F64
@@ -593,12 +678,14 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-varcoef", action="store_true", help="skip the variable-coefficient leg")
     ap.add_argument("--no-shell", action="store_true", help="skip the spherical-shell leg")
+    ap.add_argument("--no-blend", action="store_true", help="skip the curved-shell (blending operator) leg")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving-stream leg")
     ap.add_argument("--rate", type=float, default=200.0, help="serving arrival rate, requests/s")
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
-    ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong", "vcycle"],
+    ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong", "vcycle",
+                                                       "blend_apply"],
                     help="profiling mode: repeat one level operation --steps times")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

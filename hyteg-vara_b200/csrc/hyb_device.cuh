@@ -122,6 +122,14 @@ __host__ __device__ constexpr IncidentTet incidentTet( int i )
                                 { 5, 0, 0, 1, 14, 5 },  { 5, 1, 2, 0, 11, 9 },   { 5, 2, 13, 12, 0, 7 }, { 5, 3, 6, 10, 8, 0 } };
    return IncidentTet{ tab[i][0], tab[i][1], { tab[i][2], tab[i][3], tab[i][4], tab[i][5] } };
 }
+// the incident-tet table in constant memory, for loops that index it at run time (a
+// warp's lanes read the same entry: a broadcast)
+__constant__ const IncidentTet kIncidentTets[24] = {
+   incidentTet( 0 ),  incidentTet( 1 ),  incidentTet( 2 ),  incidentTet( 3 ),  incidentTet( 4 ),  incidentTet( 5 ),
+   incidentTet( 6 ),  incidentTet( 7 ),  incidentTet( 8 ),  incidentTet( 9 ),  incidentTet( 10 ), incidentTet( 11 ),
+   incidentTet( 12 ), incidentTet( 13 ), incidentTet( 14 ), incidentTet( 15 ), incidentTet( 16 ), incidentTet( 17 ),
+   incidentTet( 18 ), incidentTet( 19 ), incidentTet( 20 ), incidentTet( 21 ), incidentTet( 22 ), incidentTet( 23 ) };
+
 
 __host__ __device__ __forceinline__ int tetSize( int w ) { return ( w + 2 ) * ( w + 1 ) * w / 6; }
 // first index of row (y, z) in a closure of width W

@@ -510,7 +510,7 @@ __global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, i
 // IcosahedralShellMap, src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_blending_q3.cpp:412+,
 // src/hyteg/geometry/IcosahedralShellMap.hpp:99-223). The element matrix of a micro-tet
 // depends on its position, so a row integrates the matrices of its incident micro-tets on
-// the fly, always in FP64:
+// the fly:
 //   A_kj = sum_q w_q k(F(xi_q)) |det J| |det DF(xi_q)| (G_q g_k) . (G_q g_j),  G_q = (DF J)^-T,
 // with the 5-point degree-3 rule (centroid: -2/15; barycentric (1/2,1/6,1/6,1/6): 3/40).
 // The shell map F(x) = x R(x)/|x|, R = radRay + s (x - ray) . n, has the rank-one Jacobian
@@ -519,17 +519,17 @@ __global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, i
 // det DF, leaving the weight w_q k_q |det J| |a + v.u|. k(y) = exp(alpha (1 - |y|)) with
 // |F(xi)| = R(xi).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const double X[4][3], int k, double alpha,
-                                             double row[4] )
+template < typename C >
+__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C X[4][3], int k, C alpha, C row[4] )
 {
-   double e[3][3];
+   C e[3][3];
 #pragma unroll
    for ( int j = 0; j < 3; ++j )
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
          e[j][d] = X[j + 1][d] - X[0][d];
    // columns of J^-T (the computational gradients of vertices 1..3), vertex 0 = minus their sum
-   double c[4][3];
+   C c[4][3];
 #pragma unroll
    for ( int d = 0; d < 3; ++d )
    {
@@ -538,8 +538,8 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
       c[2][d] = e[2][d1] * e[0][d2] - e[2][d2] * e[0][d1];
       c[3][d] = e[0][d1] * e[1][d2] - e[0][d2] * e[1][d1];
    }
-   const double detJ = e[0][0] * c[1][0] + e[0][1] * c[1][1] + e[0][2] * c[1][2];
-   const double inv  = 1.0 / detJ;
+   const C detJ = e[0][0] * c[1][0] + e[0][1] * c[1][1] + e[0][2] * c[1][2];
+   const C inv  = C( 1 ) / detJ;
 #pragma unroll
    for ( int d = 0; d < 3; ++d )
    {
@@ -548,49 +548,50 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
       c[3][d] *= inv;
       c[0][d] = -( c[1][d] + c[2][d] + c[3][d] );
    }
-   const double ray[3] = { m[0], m[1], m[2] }, n[3] = { m[3], m[4], m[5] }, radRay = m[6], sc = m[7];
+   const C ray[3] = { C( m[0] ), C( m[1] ), C( m[2] ) }, n[3] = { C( m[3] ), C( m[4] ), C( m[5] ) };
+   const C radRay = C( m[6] ), sc = C( m[7] );
 #pragma unroll
    for ( int j = 0; j < 4; ++j )
-      row[j] = 0.0;
+      row[j] = C( 0 );
 #pragma unroll
    for ( int q = 0; q < 5; ++q )
    {
-      double xi[3];
+      C xi[3];
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
       {
-         double acc = 0.0;
+         C acc = C( 0 );
 #pragma unroll
          for ( int j = 0; j < 4; ++j )
-            acc += ( q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][d];
+            acc += C( q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][d];
          xi[d] = acc;
       }
-      const double r2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
-      const double ir = rsqrt( r2 );
-      const double R  = radRay + sc * ( ( xi[0] - ray[0] ) * n[0] + ( xi[1] - ray[1] ) * n[1] + ( xi[2] - ray[2] ) * n[2] );
-      const double a  = R * ir;
-      double       u[3], v[3];
+      const C r2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+      const C ir = rsqrt( r2 );
+      const C R  = radRay + sc * ( ( xi[0] - ray[0] ) * n[0] + ( xi[1] - ray[1] ) * n[1] + ( xi[2] - ray[2] ) * n[2] );
+      const C a  = R * ir;
+      C       u[3], v[3];
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
       {
          u[d] = xi[d] * ir;
          v[d] = sc * n[d] - R * ir * ir * xi[d];
       }
-      const double den = a + ( v[0] * u[0] + v[1] * u[1] + v[2] * u[2] );
-      const double kq  = alpha == 0.0 ? 1.0 : exp( alpha * ( 1.0 - R ) );
-      const double w   = ( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq * fabs( detJ ) * fabs( den );
-      const double iden = 1.0 / den;
+      const C den  = a + ( v[0] * u[0] + v[1] * u[1] + v[2] * u[2] );
+      const C kq   = alpha == C( 0 ) ? C( 1 ) : exp( alpha * ( C( 1 ) - R ) );
+      const C w    = C( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq * fabs( detJ ) * fabs( den );
+      const C iden = C( 1 ) / den;
       // c' = c - v (u.c) / den for the row's vertex and every column vertex
-      double g[4][3];
+      C g[4][3];
 #pragma unroll
       for ( int j = 0; j < 4; ++j )
       {
-         const double uc = ( u[0] * c[j][0] + u[1] * c[j][1] + u[2] * c[j][2] ) * iden;
+         const C uc = ( u[0] * c[j][0] + u[1] * c[j][1] + u[2] * c[j][2] ) * iden;
 #pragma unroll
          for ( int d = 0; d < 3; ++d )
             g[j][d] = c[j][d] - v[d] * uc;
       }
-      double gk[3] = { 0, 0, 0 };
+      C gk[3] = { C( 0 ), C( 0 ), C( 0 ) };
 #pragma unroll
       for ( int j = 0; j < 4; ++j )
          if ( j == k )
@@ -608,29 +609,35 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
 // diag and off-diagonal sum of the partial row of the closure point at slab position pos(0)
 // of `cell`: the blended matrices of the incident micro-tets allowed by the class (validT);
 // vertex coordinates as vertexdof::macrocell::coordinateFromIndex
-// (src/hyteg/p1functionspace/VertexDoFMacroCell.hpp:68-75): v0 + (v_k - v0)/N i_k.
+// (src/hyteg/p1functionspace/VertexDoFMacroCell.hpp:68-75): v0 + (v_k - v0)/N i_k. The
+// integration runs in the row type: FP64 rows reproduce the reference's matrices, FP32 rows
+// (the single-precision V-cycles of the mixed solver) evaluate them in FP32.
 template < typename T, typename Pos >
 __device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int cell, uint32_t validT, Pos&& pos, T& diag,
                                           T& off )
 {
+   using C          = T;
    const double* v  = op.bcell + size_t( cell ) * 12;
    const double* m  = op.bmap + size_t( cell ) * 8;
    const int     pk = op.bxyz[pos( 0 )];
    const int     x = pk & 1023, y = ( pk >> 10 ) & 1023, z = pk >> 20;
-   double        h[3][3];
+   C             h[3][3], v0[3];
 #pragma unroll
    for ( int j = 0; j < 3; ++j )
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
-         h[j][d] = ( v[3 * ( j + 1 ) + d] - v[d] ) / double( op.bN );
-   double dsum = 0.0, osum = 0.0;
+         h[j][d] = C( ( v[3 * ( j + 1 ) + d] - v[d] ) / double( op.bN ) );
+#pragma unroll
+   for ( int d = 0; d < 3; ++d )
+      v0[d] = C( v[d] );
+   C dsum = C( 0 ), osum = C( 0 );
 #pragma unroll 1
    for ( int i = 0; i < 24; ++i )
    {
       if ( !( validT & ( 1u << i ) ) )
          continue;
-      const IncidentTet it = incidentTet( i );
-      double            X[4][3];
+      const IncidentTet it = kIncidentTets[i];
+      C                 X[4][3];
 #pragma unroll
       for ( int j = 0; j < 4; ++j )
       {
@@ -638,21 +645,21 @@ __device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int
          const int xx = x + offX( q ), yy = y + offY( q ), zz = z + offZ( q );
 #pragma unroll
          for ( int d = 0; d < 3; ++d )
-            X[j][d] = v[d] + h[0][d] * double( xx ) + h[1][d] * double( yy ) + h[2][d] * double( zz );
+            X[j][d] = v0[d] + h[0][d] * C( xx ) + h[1][d] * C( yy ) + h[2][d] * C( zz );
       }
-      double row[4];
-      blendTetRow( m, X, it.k, op.balpha, row );
+      C row[4];
+      blendTetRow< C >( m, X, it.k, C( op.balpha ), row );
 #pragma unroll
       for ( int j = 0; j < 4; ++j )
       {
          if ( j == it.k )
             dsum += row[j];
          else
-            osum += row[j] * double( uc[pos( it.q[j] )] );
+            osum += row[j] * uc[pos( it.q[j] )];
       }
    }
-   diag += T( dsum );
-   off += T( osum );
+   diag += dsum;
+   off += osum;
 }
 
 // the rows of a pass: lanes [0, b1) in groups of 32, [b1, b2) of 8, [b2, b3) of 2, the rest
@@ -675,6 +682,8 @@ enum RowMode : int
 // of 32; the rows of one DoF are adjacent lanes of one warp). Constant operator: the
 // partial stencil st[wsel + q]; variable operator: the row's positions drive the
 // incident micro-tets' matrices and nodal coefficients (the variable branch of partialRow).
+constexpr int kBlendMaxThreads = 256; // block size bound of the blended row passes
+
 template < typename T, int MODE, bool VAR, bool BLEND = false >
 __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >& op, T* u, const T* b, T* r, T relax,
                                              int flag, long long start, long long step )
@@ -700,7 +709,20 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
                                  uint32_t( B.w ), uint32_t( C.x ), uint32_t( C.y ), uint32_t( C.z ) };
          auto           pos  = [&]( int q ) { return int( ( q & 1 ) ? ( h[q >> 1] >> 16 ) : ( h[q >> 1] & 0xffffu ) ); };
          if constexpr ( BLEND )
-            blendRow( op, uc, A.y / 240, kValidTets[( A.y / 15 ) & 15], pos, diag, off );
+         {
+            // the blended row loops over its micro-tets at run time: the row's positions go
+            // through shared memory (a local array indexed at run time would live in local
+            // memory); blocks of at most kBlendMaxThreads threads
+            __shared__ uint32_t sPos[8][kBlendMaxThreads];
+#pragma unroll
+            for ( int w = 0; w < 8; ++w )
+               sPos[w][threadIdx.x] = h[w];
+            auto spos = [&]( int q ) {
+               const uint32_t v = sPos[q >> 1][threadIdx.x];
+               return int( ( q & 1 ) ? ( v >> 16 ) : ( v & 0xffffu ) );
+            };
+            blendRow( op, uc, A.y / 240, kValidTets[( A.y / 15 ) & 15], spos, diag, off );
+         }
          else if constexpr ( !VAR )
          {
             const T* w = op.st + A.y;
@@ -759,6 +781,16 @@ __global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, OpDev< T > op, 
    HYB_PDL_PROLOGUE();
    rowPassBody< T, MODE, VAR, BLEND >( rp, op, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
                                        (long long) gridDim.x * blockDim.x );
+}
+
+// the blended row pass (FP64 arithmetic bound; four blocks of 128 threads per SM)
+template < typename T, int MODE >
+__global__ void __launch_bounds__( 128, 4 ) k_row_pass_blend( RowPass rp, OpDev< T > op, T* u, const T* b, T* r, T relax,
+                                                              int flag )
+{
+   HYB_PDL_PROLOGUE();
+   rowPassBody< T, MODE, false, true >( rp, op, u, b, r, relax, flag, (long long) blockIdx.x * blockDim.x + threadIdx.x,
+                                        (long long) gridDim.x * blockDim.x );
 }
 
 // Constant-stencil quad: the points x = 4g + r, r = 0..3, of row (y, z). Each of the seven

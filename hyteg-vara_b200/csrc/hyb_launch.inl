@@ -189,11 +189,11 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
       const int        g  = rowGrid( s, rp.n );
       T*               u  = const_cast< T* >( src );
       if ( mode == kResidual )
-         pdlLaunch( k_row_pass< T, kRowResidual, false, true >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
+         pdlLaunch( k_row_pass_blend< T, kRowResidual >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
       else if ( mode == kAdd )
-         pdlLaunch( k_row_pass< T, kRowApplyAdd, false, true >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
+         pdlLaunch( k_row_pass_blend< T, kRowApplyAdd >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
       else
-         pdlLaunch( k_row_pass< T, kRowApply, false, true >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
+         pdlLaunch( k_row_pass_blend< T, kRowApply >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag );
       HYB_CHECK_LAUNCH();
       return;
    }
@@ -272,7 +272,7 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       auto             pass = [&]( const RowPass& rp ) {
          if ( rp.n == 0 )
             return;
-         pdlLaunch( k_row_pass< T, kRowSor, false, true >, dim3( rowGrid( s, rp.n ) ), dim3( 128 ), 0, stream, rp, od, u,
+         pdlLaunch( k_row_pass_blend< T, kRowSor >, dim3( rowGrid( s, rp.n ) ), dim3( 128 ), 0, stream, rp, od, u,
                     rhs, (T*) nullptr, relax, flag );
          HYB_CHECK_LAUNCH();
       };

@@ -239,6 +239,21 @@ class P1ElementwiseDivKGradOperator : public P1OperatorBase
    }
 };
 
+/// P1ElementwiseBlendingDivKGradOperator on a spherical-shell storage whose cells carry the
+/// IcosahedralShellMap (the reference sets it with IcosahedralShellMap::setMap); the
+/// coefficient is k(y) = exp( alpha (1 - |y|) ) at the mapped quadrature points, alpha = 0
+/// gives the shell's Laplacian. Levels up to 6; smooth with (symmetric) SOR.
+class P1ElementwiseBlendingDivKGradOperator : public P1OperatorBase
+{
+ public:
+   using srcType = P1Function< double >;
+   P1ElementwiseBlendingDivKGradOperator( const std::shared_ptr< PrimitiveStorage >& storage, int minLevel, int maxLevel,
+                                          double alpha = 0.0 )
+   {
+      hybCheck( hyb_operator_create_blend_divkgrad( storage->handle(), minLevel, maxLevel, alpha, &h_ ) );
+   }
+};
+
 template < typename V = double >
 class P1toP1LinearProlongation
 {

@@ -49,6 +49,20 @@ def test_blend_apply_matches_oracle(shell, alpha):
         close(fd.get(level), y + orc.apply(x, level, flag=H.ALL, op=op), 1e-12)
 
 
+def test_blend_apply_fp32_close_to_oracle(shell):
+    """FP32 rows (the mixed solver's single-precision cycles) integrate in FP32."""
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    rng = np.random.default_rng(26)
+    x = rng.uniform(-1, 1, orc.n(L))
+    fs, fd = H.P1Function("s", st, 0, L, H.F32), H.P1Function("d", st, 0, L, H.F32)
+    fs.set(x.astype(np.float32), L)
+    A.apply(fs, fd, L, H.ALL)
+    close(fd.get(L).astype(np.float64), orc.apply(x.astype(np.float32).astype(np.float64), L, flag=H.ALL, op=op),
+          5e-5)
+
+
 def test_blend_residual_and_cg_match_oracle(shell):
     H, st, orc, L = shell
     A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
