@@ -515,9 +515,9 @@ __global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, i
 // with the 5-point degree-3 rule (centroid: -2/15; barycentric (1/2,1/6,1/6,1/6): 3/40).
 // The shell map F(x) = x R(x)/|x|, R = radRay + s (x - ray) . n, has the rank-one Jacobian
 // DF = a I + u v^T (a = R/|x|, u = x/|x|, v = s n - R x/|x|^2), so det DF = a^2 (a + v.u) and
-// DF^-T c = (c - v (u.c)/(a + v.u)) / a; the 1/a^2 of the gradient product cancels against
-// det DF, leaving the weight w_q k_q |det J| |a + v.u|. k(y) = exp(alpha (1 - |y|)) with
-// |F(xi)| = R(xi).
+// DF^-T c = (c - v (u.c)/(a + v.u)) / a, with a + v.u = s (n.x)/|x|; the 1/a^2 of the
+// gradient product cancels against det DF, leaving the weight w_q k_q |det J| |s n.x| / |x|.
+// k(y) = exp(alpha (1 - |y|)) with |F(xi)| = R(xi).
 // ---------------------------------------------------------------------------
 template < typename C >
 __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C X[4][3], int k, C alpha, C row[4] )
@@ -548,8 +548,9 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
       c[3][d] *= inv;
       c[0][d] = -( c[1][d] + c[2][d] + c[3][d] );
    }
-   const C ray[3] = { C( m[0] ), C( m[1] ), C( m[2] ) }, n[3] = { C( m[3] ), C( m[4] ), C( m[5] ) };
-   const C radRay = C( m[6] ), sc = C( m[7] );
+   const C n[3] = { C( m[3] ), C( m[4] ), C( m[5] ) }, sc = C( m[7] );
+   // R(x) = R0 + s n.x
+   const C R0 = C( m[6] ) - sc * ( n[0] * C( m[0] ) + n[1] * C( m[1] ) + n[2] * C( m[2] ) );
 #pragma unroll
    for ( int j = 0; j < 4; ++j )
       row[j] = C( 0 );
@@ -566,30 +567,27 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
             acc += C( q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][d];
          xi[d] = acc;
       }
-      const C r2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
-      const C ir = rsqrt( r2 );
-      const C R  = radRay + sc * ( ( xi[0] - ray[0] ) * n[0] + ( xi[1] - ray[1] ) * n[1] + ( xi[2] - ray[2] ) * n[2] );
-      const C a  = R * ir;
-      C       u[3], v[3];
+      const C r2  = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+      const C ir  = rsqrt( r2 );
+      const C snx = sc * ( n[0] * xi[0] + n[1] * xi[1] + n[2] * xi[2] );
+      const C R   = R0 + snx;
+      // a + v.u = s (n.x) / |x|
+      C v[3];
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
-      {
-         u[d] = xi[d] * ir;
          v[d] = sc * n[d] - R * ir * ir * xi[d];
-      }
-      const C den  = a + ( v[0] * u[0] + v[1] * u[1] + v[2] * u[2] );
-      const C kq   = alpha == C( 0 ) ? C( 1 ) : exp( alpha * ( C( 1 ) - R ) );
-      const C w    = C( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq * fabs( detJ ) * fabs( den );
-      const C iden = C( 1 ) / den;
-      // c' = c - v (u.c) / den for the row's vertex and every column vertex
+      const C kq = alpha == C( 0 ) ? C( 1 ) : exp( alpha * ( C( 1 ) - R ) );
+      const C w  = C( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq * fabs( detJ ) * fabs( snx ) * ir;
+      const C t  = C( 1 ) / snx;
+      // c' = c - v (u.c) / (a + v.u) = c - v (x.c) / (s n.x) for the row's vertex and every column vertex
       C g[4][3];
 #pragma unroll
       for ( int j = 0; j < 4; ++j )
       {
-         const C uc = ( u[0] * c[j][0] + u[1] * c[j][1] + u[2] * c[j][2] ) * iden;
+         const C xc = ( xi[0] * c[j][0] + xi[1] * c[j][1] + xi[2] * c[j][2] ) * t;
 #pragma unroll
          for ( int d = 0; d < 3; ++d )
-            g[j][d] = c[j][d] - v[d] * uc;
+            g[j][d] = c[j][d] - v[d] * xc;
       }
       C gk[3] = { C( 0 ), C( 0 ), C( 0 ) };
 #pragma unroll
