@@ -519,9 +519,27 @@ __global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, i
 // gradient product cancels against det DF, leaving the weight w_q k_q |det J| |s n.x| / |x|.
 // k(y) = exp(alpha (1 - |y|)) with |F(xi)| = R(xi).
 // ---------------------------------------------------------------------------
+constexpr int kBlendMaxThreads = 256; // block size bound of the blended row passes
+
+// kv[j] = exp(alpha (1 - R(X_j)) / 12) at the tet's vertices (alpha != 0): R is affine, so
+// at the quadrature points k = exp(alpha (1 - R)) is a product of integer powers of them
+// (centroid: (k0 k1 k2 k3)^3; the point weighted 1/2 on vertex j: kj^6 times the others^2)
 template < typename C >
-__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C X[4][3], int k, C alpha, C row[4] )
+__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C X[4][3], int k, C alpha,
+                                             const C kv[4], C row[4] )
 {
+   C kq5[5] = { C( 1 ), C( 1 ), C( 1 ), C( 1 ), C( 1 ) };
+   if ( alpha != C( 0 ) )
+   {
+      const C P = kv[0] * kv[1] * kv[2] * kv[3], P2 = P * P;
+      kq5[0] = P2 * P;
+#pragma unroll
+      for ( int j = 0; j < 4; ++j )
+      {
+         const C k2 = kv[j] * kv[j];
+         kq5[j + 1] = P2 * ( k2 * k2 );
+      }
+   }
    C e[3][3];
 #pragma unroll
    for ( int j = 0; j < 3; ++j )
@@ -570,14 +588,13 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
       const C r2  = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
       const C ir  = rsqrt( r2 );
       const C snx = sc * ( n[0] * xi[0] + n[1] * xi[1] + n[2] * xi[2] );
-      const C R   = R0 + snx;
+      const C R   = R0 + snx; // |F(xi)|
       // a + v.u = s (n.x) / |x|
       C v[3];
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
          v[d] = sc * n[d] - R * ir * ir * xi[d];
-      const C kq = alpha == C( 0 ) ? C( 1 ) : exp( alpha * ( C( 1 ) - R ) );
-      const C w  = C( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq * fabs( detJ ) * fabs( snx ) * ir;
+      const C w  = C( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq5[q] * fabs( detJ ) * fabs( snx ) * ir;
       const C t  = C( 1 ) / snx;
       // c' = c - v (u.c) / (a + v.u) = c - v (x.c) / (s n.x) for the row's vertex and every column vertex
       C g[4][3];
@@ -628,6 +645,24 @@ __device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int
 #pragma unroll
    for ( int d = 0; d < 3; ++d )
       v0[d] = C( v[d] );
+   // the coefficient's factors at the 15 stencil points (shared memory: indexed at run time)
+   __shared__ C sK[15][kBlendMaxThreads];
+   const C      alpha = C( op.balpha );
+   if ( alpha != C( 0 ) )
+   {
+      const C sc = C( m[7] ), n[3] = { C( m[3] ), C( m[4] ), C( m[5] ) };
+      const C R0 = C( m[6] ) - sc * ( n[0] * C( m[0] ) + n[1] * C( m[1] ) + n[2] * C( m[2] ) );
+#pragma unroll
+      for ( int q = 0; q < 15; ++q )
+      {
+         C p[3];
+#pragma unroll
+         for ( int d = 0; d < 3; ++d )
+            p[d] = v0[d] + h[0][d] * C( x + offX( q ) ) + h[1][d] * C( y + offY( q ) ) + h[2][d] * C( z + offZ( q ) );
+         const C R             = R0 + sc * ( n[0] * p[0] + n[1] * p[1] + n[2] * p[2] );
+         sK[q][threadIdx.x] = exp( alpha * ( C( 1 ) - R ) * C( 1.0 / 12.0 ) );
+      }
+   }
    C dsum = C( 0 ), osum = C( 0 );
 #pragma unroll 1
    for ( int i = 0; i < 24; ++i )
@@ -645,8 +680,12 @@ __device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int
          for ( int d = 0; d < 3; ++d )
             X[j][d] = v0[d] + h[0][d] * C( xx ) + h[1][d] * C( yy ) + h[2][d] * C( zz );
       }
-      C row[4];
-      blendTetRow< C >( m, X, it.k, C( op.balpha ), row );
+      C row[4], kv[4] = { C( 1 ), C( 1 ), C( 1 ), C( 1 ) };
+      if ( alpha != C( 0 ) )
+#pragma unroll
+         for ( int j = 0; j < 4; ++j )
+            kv[j] = sK[it.q[j]][threadIdx.x];
+      blendTetRow< C >( m, X, it.k, alpha, kv, row );
 #pragma unroll
       for ( int j = 0; j < 4; ++j )
       {
@@ -680,8 +719,6 @@ enum RowMode : int
 // of 32; the rows of one DoF are adjacent lanes of one warp). Constant operator: the
 // partial stencil st[wsel + q]; variable operator: the row's positions drive the
 // incident micro-tets' matrices and nodal coefficients (the variable branch of partialRow).
-constexpr int kBlendMaxThreads = 256; // block size bound of the blended row passes
-
 template < typename T, int MODE, bool VAR, bool BLEND = false >
 __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >& op, T* u, const T* b, T* r, T relax,
                                              int flag, long long start, long long step )
