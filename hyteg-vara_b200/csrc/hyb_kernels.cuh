@@ -818,9 +818,10 @@ __global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, OpDev< T > op, 
                                        (long long) gridDim.x * blockDim.x );
 }
 
-// the blended row pass (FP64 arithmetic bound; four blocks of 128 threads per SM)
+// the blended row pass (arithmetic bound; FP64: three blocks of 128 threads per SM without
+// spills measured faster than four with them, FP32 fits four)
 template < typename T, int MODE >
-__global__ void __launch_bounds__( 128, 4 ) k_row_pass_blend( RowPass rp, OpDev< T > op, T* u, const T* b, T* r, T relax,
+__global__ void __launch_bounds__( 128, sizeof( T ) == 8 ? 3 : 4 ) k_row_pass_blend( RowPass rp, OpDev< T > op, T* u, const T* b, T* r, T relax,
                                                               int flag )
 {
    HYB_PDL_PROLOGUE();
