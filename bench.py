@@ -482,7 +482,7 @@ def blended_shell(args, H, stream, ntan=5, nrad=4, L=5):
             "time_to_tol_ms": {"mixed": out[32][0], "fp64": out[64][0]},
             "cycles": {"mixed": out[32][1], "fp64": out[64][1]},
             "final_rel_residual": {"mixed": out[32][2], "fp64": out[64][2]},
-            "apply": {"kernel": "k_row_pass<double, kRowApply, blend> (FP64 apply, all rows)", "ms": t_apply * 1e3,
+            "apply": {"kernel": "k_row_pass_blend<double, kRowApply> (FP64 apply, all rows)", "ms": t_apply * 1e3,
                       "bound": "fp64", "achieved_tflops": flops / t_apply / 1e12,
                       "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_source": "nominal",
                       "frac": flops / t_apply / 1e12 / FP64_NOMINAL_TFLOPS,
