@@ -497,12 +497,7 @@ void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int
    if ( smoother == HYB_SMOOTHER_CHEBYSHEV )
       g.progTop = -1; // the program kernel has no Chebyshev phases
    if ( op->blend )
-   {
-      // blending operators run every level as row-pass launches
-      require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_SYMMETRIC_SOR,
-               "the blending operator smooths with (symmetric) SOR" );
-      g.progTop = -1;
-   }
+      g.progTop = -1; // blending operators run every level as row-pass launches
 }
 
 

@@ -712,7 +712,9 @@ enum RowMode : int
    kRowSor      = 0, // u = (1 - relax) u + relax (b - off) / diag
    kRowResidual = 1, // r = b - A u
    kRowApply    = 2, // r = A u
-   kRowApplyAdd = 3  // r += A u
+   kRowApplyAdd = 3, // r += A u
+   kRowJacobi   = 4, // r = u + relax (b - A u) / diag (u the old iterate, read only)
+   kRowInvDiag  = 5  // r = 1 / diag
 };
 
 // one pass over the rows, lanes start, start + step, ... (start - lane and step multiples
@@ -804,6 +806,10 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
          r[i] = b[i] - ( diag * u[i] + off );
       else if constexpr ( MODE == kRowApplyAdd )
          r[i] += diag * u[i] + off;
+      else if constexpr ( MODE == kRowJacobi )
+         r[i] = u[i] + relax * ( b[i] - off - diag * u[i] ) / diag;
+      else if constexpr ( MODE == kRowInvDiag )
+         r[i] = T( 1 ) / diag;
       else
          r[i] = diag * u[i] + off;
    }

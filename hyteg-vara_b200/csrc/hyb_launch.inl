@@ -390,8 +390,15 @@ void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
-   require( !op.blend, "weighted Jacobi is not available for the blending operator (use SOR)" );
    const OpDev< T > od = op.dev< T >( l );
+   if ( op.blend )
+   {
+      const RowPass rp = rowPassAll( &blendRowsOf( s, l ) );
+      pdlLaunch( k_row_pass_blend< T, kRowJacobi >, dim3( rowGrid( s, rp.n ) ), dim3( 128 ), 0, stream, rp, od,
+                 const_cast< T* >( src ), rhs, dst, relax, flag );
+      HYB_CHECK_LAUNCH();
+      return;
+   }
    if ( op.variable )
       pdlLaunch( k_jacobi< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
    else
@@ -580,8 +587,15 @@ void launchInvDiag( const Operator& op, int l, const T* zeros, T* out, cudaStrea
    const int      nb = nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 );
    if ( nb == 0 )
       return;
-   require( !op.blend, "the Chebyshev smoother is not available for the blending operator (use SOR)" );
    const OpDev< T > od = op.dev< T >( l );
+   if ( op.blend )
+   {
+      const RowPass rp = rowPassAll( &blendRowsOf( s, l ) );
+      k_row_pass_blend< T, kRowInvDiag ><<< rowGrid( s, rp.n ), 128, 0, stream >>>( rp, od, const_cast< T* >( zeros ),
+                                                                                   nullptr, out, T( 0 ), kAll );
+      HYB_CHECK_LAUNCH();
+      return;
+   }
    if ( op.variable )
       k_inv_diag< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
    else

@@ -242,7 +242,7 @@ class P1ElementwiseDivKGradOperator : public P1OperatorBase
 /// P1ElementwiseBlendingDivKGradOperator on a spherical-shell storage whose cells carry the
 /// IcosahedralShellMap (the reference sets it with IcosahedralShellMap::setMap); the
 /// coefficient is k(y) = exp( alpha (1 - |y|) ) at the mapped quadrature points, alpha = 0
-/// gives the shell's Laplacian. Levels up to 6; smooth with (symmetric) SOR.
+/// gives the shell's Laplacian. Levels up to 6.
 class P1ElementwiseBlendingDivKGradOperator : public P1OperatorBase
 {
  public:

@@ -3,7 +3,8 @@ spherical shell carries its IcosahedralShellMap and the element matrices of
 p1_div_k_grad_blending_q3 are integrated per row on the device. Apply (replace, add,
 residual), multicolour SOR forward and backward, the coarse CG and V-cycles must match the
 oracle (whose map and form are pinned to the reference's compiled code) to 1e-12 for
-applies, 1e-11 for sweeps and 1e-10 for cycles, the tolerances of the other parity tests."""
+applies, 1e-11 for sweeps and 1e-10 for cycles, the tolerances of the other parity tests;
+so must weighted Jacobi, the spectral radius estimate and Chebyshev-smoothed cycles."""
 import numpy as np
 import pytest
 
@@ -148,14 +149,51 @@ def test_blend_mixed_precision_solve_converges(shell):
     assert np.linalg.norm(r) <= 1.01e-8 * np.linalg.norm(b[inner])
 
 
-def test_blend_rejects_other_meshes_and_smoothers(shell):
+def test_blend_jacobi_matches_oracle(shell):
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    rng = np.random.default_rng(27)
+    x, b = rng.uniform(-1, 1, orc.n(L)), rng.uniform(-1, 1, orc.n(L))
+    fs, fd, fb = (H.P1Function(n, st, 0, L) for n in "sdb")
+    fs.set(x, L)
+    fd.set(x, L)
+    fb.set(b, L)
+    A.smooth_jac(fd, fb, fs, 0.7, L, 1 | 4)
+    close(fd.get(L), orc.jacobi(x.copy(), b, L, relax=0.7, flag=1 | 4, op=op), 1e-12)
+
+
+def test_blend_chebyshev_vcycle_matches_oracle(shell):
+    """Chebyshev smoothing on the curved shell: the inverse diagonal and the applies run
+    through the blended rows; the spectral radius estimate is the power iteration on D^-1 A."""
+    H, st, orc, L = shell
+    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 5.0)
+    op = orc.op_blend_div_k_grad(5.0)
+    fx, ft = H.P1Function("x", st, 0, L), H.P1Function("t", st, 0, L)
+    start = np.random.default_rng(28).uniform(0, 1, orc.n(L))
+    fx.set(start, L)
+    rho = A.estimate_spectral_radius(fx, ft, L, 20)
+    rho_ref = orc.spectral_radius(L, 20, start.copy(), op=op)
+    assert abs(rho - rho_ref) <= 1e-10 * rho_ref
+    b = np.random.default_rng(29).uniform(-1, 1, orc.n(L))
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, smoother=H.SMOOTHER_CHEBYSHEV, coarse_tol=1e-14)
+    gmg.setup_chebyshev(3, rho)
+    orc.set_chebyshev(3, 0.3 * rho, 1.2 * rho)
+    x = np.zeros(orc.n(L))
+    for _ in range(2):
+        gmg.solve(fx, fb, L)
+        fb.set(b, L)
+        orc.gmg(x, b, 0, L, pre=2, post=2, smoother=5, coarse_tol=1e-14, max_cycles=1, op=op)
+        close(fx.get(L), x, 1e-10)
+
+
+def test_blend_rejects_other_meshes(shell):
     H, st, orc, L = shell
     cube = H.PrimitiveStorage.cuboid(1, 1, 1, 2)
     with pytest.raises(RuntimeError):
         H.P1ElementwiseBlendingDivKGradOperator(cube, 0, 2, 0.0)
-    A = H.P1ElementwiseBlendingDivKGradOperator(st, 0, L, 0.0)
-    with pytest.raises(RuntimeError):
-        H.GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0, smoother=H.SMOOTHER_CHEBYSHEV)
-    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
-    with pytest.raises(RuntimeError):
-        A.smooth_jac(fx, fb, fb, 0.6, L, 1 | 4)
+    coarse_only = H.PrimitiveStorage.spherical_shell(2, 2, 0.55, 1.0, 7)
+    with pytest.raises(RuntimeError):  # level 7 closures exceed the 16-bit row positions
+        H.P1ElementwiseBlendingDivKGradOperator(coarse_only, 7, 7, 0.0)
