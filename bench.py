@@ -613,7 +613,7 @@ def single_op(args):
     --op apply|residual|sor|sor32|restrict|prolong at --level on the bench mesh, or
     --op vcycle: FP64 V(3,3) cycles from --level down to level 0 (program kernel, row
     passes of the middle levels, CG); --op blend_apply: the blending operator's FP64 apply
-    on the curved shell (ntan 5, nrad 4) at --level."""
+    on the curved shell (ntan 5, nrad 4) at --level (blend_apply32: FP32 rows)."""
     import torch
 
     import build as B
@@ -622,12 +622,13 @@ def single_op(args):
 
     B.build()
     L, nc = args.level, args.cubes
-    if args.op == "blend_apply":
-        # the curved shell (ntan 5, nrad 4) with the blending operator, FP64 apply
+    if args.op in ("blend_apply", "blend_apply32"):
+        # the curved shell (ntan 5, nrad 4) with the blending operator, FP64 (FP32) apply
         st = H.PrimitiveStorage.spherical_shell(5, 4, 0.55, 1.0, L)
         A = H.P1ElementwiseBlendingDivKGradOperator(st, L, L, 5.0)
-        b, y = H.P1Function("b", st, L, L), H.P1Function("y", st, L, L)
-        b.fill_uniform_random(L, 0, float(1 << 20))
+        bt = H.F32 if args.op == "blend_apply32" else H.F64
+        b, y = H.P1Function("b", st, L, L, bt), H.P1Function("y", st, L, L, bt)
+        b.interpolate(1.0, L, flag=H.ALL)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -685,7 +686,7 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=16)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--op", default=None, choices=["apply", "residual", "sor", "sor32", "restrict", "prolong", "vcycle",
-                                                       "blend_apply"],
+                                                       "blend_apply", "blend_apply32"],
                     help="profiling mode: repeat one level operation --steps times")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

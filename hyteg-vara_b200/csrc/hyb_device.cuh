@@ -122,6 +122,29 @@ __host__ __device__ constexpr IncidentTet incidentTet( int i )
                                 { 5, 0, 0, 1, 14, 5 },  { 5, 1, 2, 0, 11, 9 },   { 5, 2, 13, 12, 0, 7 }, { 5, 3, 6, 10, 8, 0 } };
    return IncidentTet{ tab[i][0], tab[i][1], { tab[i][2], tab[i][3], tab[i][4], tab[i][5] } };
 }
+// the three vertices of incident tet i other than the row's point (offsets in the tet's
+// vertex order): with the row's point as vertex 0, the row of the element matrix is row 0
+struct IncidentOthers
+{
+   int q[3];
+};
+__host__ __device__ constexpr IncidentOthers incidentOthers( int i )
+{
+   const IncidentTet it = incidentTet( i );
+   IncidentOthers    o{ { 0, 0, 0 } };
+   int               n = 0;
+   for ( int j = 0; j < 4; ++j )
+      if ( j != it.k )
+         o.q[n++] = it.q[j];
+   return o;
+}
+__constant__ const IncidentOthers kIncidentOthers[24] = {
+   incidentOthers( 0 ),  incidentOthers( 1 ),  incidentOthers( 2 ),  incidentOthers( 3 ),  incidentOthers( 4 ),
+   incidentOthers( 5 ),  incidentOthers( 6 ),  incidentOthers( 7 ),  incidentOthers( 8 ),  incidentOthers( 9 ),
+   incidentOthers( 10 ), incidentOthers( 11 ), incidentOthers( 12 ), incidentOthers( 13 ), incidentOthers( 14 ),
+   incidentOthers( 15 ), incidentOthers( 16 ), incidentOthers( 17 ), incidentOthers( 18 ), incidentOthers( 19 ),
+   incidentOthers( 20 ), incidentOthers( 21 ), incidentOthers( 22 ), incidentOthers( 23 ) };
+
 // the incident-tet table in constant memory, for loops that index it at run time (a
 // warp's lanes read the same entry: a broadcast)
 __constant__ const IncidentTet kIncidentTets[24] = {

@@ -663,37 +663,41 @@ __device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int
          sK[q][threadIdx.x] = exp( alpha * ( C( 1 ) - R ) * C( 1.0 / 12.0 ) );
       }
    }
-   C dsum = C( 0 ), osum = C( 0 );
+   // the row's point is vertex 0 of every incident tet (the element matrix is equivariant
+   // under relabelling its vertices), so the row is row 0
+   C P[3];
+#pragma unroll
+   for ( int d = 0; d < 3; ++d )
+      P[d] = v0[d] + h[0][d] * C( x ) + h[1][d] * C( y ) + h[2][d] * C( z );
+   const C k0   = alpha != C( 0 ) ? sK[0][threadIdx.x] : C( 1 );
+   C       dsum = C( 0 ), osum = C( 0 );
 #pragma unroll 1
    for ( int i = 0; i < 24; ++i )
    {
       if ( !( validT & ( 1u << i ) ) )
          continue;
-      const IncidentTet it = kIncidentTets[i];
-      C                 X[4][3];
+      const IncidentOthers it = kIncidentOthers[i];
+      C                    X[4][3], kv[4] = { k0, C( 1 ), C( 1 ), C( 1 ) };
 #pragma unroll
-      for ( int j = 0; j < 4; ++j )
+      for ( int d = 0; d < 3; ++d )
+         X[0][d] = P[d];
+#pragma unroll
+      for ( int j = 1; j < 4; ++j )
       {
-         const int q = it.q[j];
+         const int q  = it.q[j - 1];
          const int xx = x + offX( q ), yy = y + offY( q ), zz = z + offZ( q );
 #pragma unroll
          for ( int d = 0; d < 3; ++d )
             X[j][d] = v0[d] + h[0][d] * C( xx ) + h[1][d] * C( yy ) + h[2][d] * C( zz );
+         if ( alpha != C( 0 ) )
+            kv[j] = sK[q][threadIdx.x];
       }
-      C row[4], kv[4] = { C( 1 ), C( 1 ), C( 1 ), C( 1 ) };
-      if ( alpha != C( 0 ) )
+      C row[4];
+      blendTetRow< C >( m, X, 0, alpha, kv, row );
+      dsum += row[0];
 #pragma unroll
-         for ( int j = 0; j < 4; ++j )
-            kv[j] = sK[it.q[j]][threadIdx.x];
-      blendTetRow< C >( m, X, it.k, alpha, kv, row );
-#pragma unroll
-      for ( int j = 0; j < 4; ++j )
-      {
-         if ( j == it.k )
-            dsum += row[j];
-         else
-            osum += row[j] * uc[pos( it.q[j] )];
-      }
+      for ( int j = 1; j < 4; ++j )
+         osum += row[j] * uc[pos( it.q[j - 1] )];
    }
    diag += dsum;
    off += osum;
