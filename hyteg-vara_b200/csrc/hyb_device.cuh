@@ -126,16 +126,23 @@ __host__ __device__ constexpr IncidentTet incidentTet( int i )
 // vertex order): with the row's point as vertex 0, the row of the element matrix is row 0
 struct IncidentOthers
 {
-   int q[3];
+   int   q[3];    // stencil offset indices
+   float d[3][3]; // their lattice offsets (x, y, z) from the row's point
 };
 __host__ __device__ constexpr IncidentOthers incidentOthers( int i )
 {
    const IncidentTet it = incidentTet( i );
-   IncidentOthers    o{ { 0, 0, 0 } };
+   IncidentOthers    o{ { 0, 0, 0 }, { { 0, 0, 0 }, { 0, 0, 0 }, { 0, 0, 0 } } };
    int               n = 0;
    for ( int j = 0; j < 4; ++j )
       if ( j != it.k )
-         o.q[n++] = it.q[j];
+      {
+         o.q[n]    = it.q[j];
+         o.d[n][0] = float( offX( it.q[j] ) );
+         o.d[n][1] = float( offY( it.q[j] ) );
+         o.d[n][2] = float( offZ( it.q[j] ) );
+         ++n;
+      }
    return o;
 }
 __constant__ const IncidentOthers kIncidentOthers[24] = {

@@ -525,9 +525,10 @@ constexpr int kBlendMaxThreads = 256; // block size bound of the blended row pas
 // at the quadrature points k = exp(alpha (1 - R)) is a product of integer powers of them
 // (centroid: (k0 k1 k2 k3)^3; the point weighted 1/2 on vertex j: kj^6 times the others^2)
 template < typename C >
-__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C X[4][3], int k, C alpha,
+__device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C P[3], const C e[3][3], C alpha,
                                              const C kv[4], C row[4] )
 {
+   constexpr int k = 0; // the row's point is vertex 0
    C kq5[5] = { C( 1 ), C( 1 ), C( 1 ), C( 1 ), C( 1 ) };
    if ( alpha != C( 0 ) )
    {
@@ -540,12 +541,6 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
          kq5[j + 1] = P2 * ( k2 * k2 );
       }
    }
-   C e[3][3];
-#pragma unroll
-   for ( int j = 0; j < 3; ++j )
-#pragma unroll
-      for ( int d = 0; d < 3; ++d )
-         e[j][d] = X[j + 1][d] - X[0][d];
    // columns of J^-T (the computational gradients of vertices 1..3), vertex 0 = minus their sum
    C c[4][3];
 #pragma unroll
@@ -575,14 +570,15 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
 #pragma unroll
    for ( int q = 0; q < 5; ++q )
    {
+      // xi = X0 + sum_j lambda_j (X_j - X0)
       C xi[3];
 #pragma unroll
       for ( int d = 0; d < 3; ++d )
       {
-         C acc = C( 0 );
+         C acc = P[d];
 #pragma unroll
-         for ( int j = 0; j < 4; ++j )
-            acc += C( q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][d];
+         for ( int j = 1; j < 4; ++j )
+            acc += C( q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ) ) * e[j - 1][d];
          xi[d] = acc;
       }
       const C r2  = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
@@ -676,24 +672,20 @@ __device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int
    {
       if ( !( validT & ( 1u << i ) ) )
          continue;
-      const IncidentOthers it = kIncidentOthers[i];
-      C                    X[4][3], kv[4] = { k0, C( 1 ), C( 1 ), C( 1 ) };
+      const IncidentOthers& it = kIncidentOthers[i];
+      C                     e[3][3], kv[4] = { k0, C( 1 ), C( 1 ), C( 1 ) };
 #pragma unroll
-      for ( int d = 0; d < 3; ++d )
-         X[0][d] = P[d];
-#pragma unroll
-      for ( int j = 1; j < 4; ++j )
+      for ( int j = 0; j < 3; ++j )
       {
-         const int q  = it.q[j - 1];
-         const int xx = x + offX( q ), yy = y + offY( q ), zz = z + offZ( q );
+         const C dx = C( it.d[j][0] ), dy = C( it.d[j][1] ), dz = C( it.d[j][2] );
 #pragma unroll
          for ( int d = 0; d < 3; ++d )
-            X[j][d] = v0[d] + h[0][d] * C( xx ) + h[1][d] * C( yy ) + h[2][d] * C( zz );
+            e[j][d] = h[0][d] * dx + h[1][d] * dy + h[2][d] * dz;
          if ( alpha != C( 0 ) )
-            kv[j] = sK[q][threadIdx.x];
+            kv[j + 1] = sK[it.q[j]][threadIdx.x];
       }
       C row[4];
-      blendTetRow< C >( m, X, 0, alpha, kv, row );
+      blendTetRow< C >( m, P, e, alpha, kv, row );
       dsum += row[0];
 #pragma unroll
       for ( int j = 1; j < 4; ++j )
