@@ -424,9 +424,10 @@ def spherical_shell(args, H, I, stream, ntan=5, nrad=4, L=6):
             "error_mixed_vs_fp64_solution": err, "as_serving_requests": served}
 
 
-# FP64 flops of one blended micro-tet row evaluation (blendTetRow plus the four vertex
-# positions): the map Jacobian, its rank-one inverse and the five quadrature points
-BLEND_FLOPS_PER_TET_ROW = 830
+# flops of one blended micro-tet row evaluation as the kernel formulates it (edges 54,
+# inverse Jacobian 51, coefficient products 25, five quadrature points 124 each, row
+# accumulation 7): the map Jacobian's rank-one inverse and the 5-point rule
+BLEND_FLOPS_PER_TET_ROW = 750
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (CUDA cores), nominal; no measured FP64 peak on this pool
 
 
