@@ -425,9 +425,9 @@ def spherical_shell(args, H, I, stream, ntan=5, nrad=4, L=6):
 
 
 # flops of one blended micro-tet row evaluation as the kernel formulates it (edges 54,
-# inverse Jacobian 51, coefficient products 25, five quadrature points 124 each, row
-# accumulation 7): the map Jacobian's rank-one inverse and the 5-point rule
-BLEND_FLOPS_PER_TET_ROW = 750
+# inverse Jacobian 42, coefficient products 25, five quadrature points 111 each, row sums
+# and accumulation 10): the map Jacobian's rank-one inverse and the 5-point rule
+BLEND_FLOPS_PER_TET_ROW = 690
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (CUDA cores), nominal; no measured FP64 peak on this pool
 
 

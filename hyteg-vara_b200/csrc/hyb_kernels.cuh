@@ -528,7 +528,7 @@ template < typename C >
 __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const C P[3], const C e[3][3], C alpha,
                                              const C kv[4], C row[4] )
 {
-   constexpr int k = 0; // the row's point is vertex 0
+   // the row's point is vertex 0
    C kq5[5] = { C( 1 ), C( 1 ), C( 1 ), C( 1 ), C( 1 ) };
    if ( alpha != C( 0 ) )
    {
@@ -541,7 +541,8 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
          kq5[j + 1] = P2 * ( k2 * k2 );
       }
    }
-   // columns of J^-T (the computational gradients of vertices 1..3), vertex 0 = minus their sum
+   // columns of J^-T (the computational gradients of vertices 1..3; vertex 0's is minus their
+   // sum, so its mapped gradient is minus the sum of the others' and the row sums to zero)
    C c[4][3];
 #pragma unroll
    for ( int d = 0; d < 3; ++d )
@@ -559,7 +560,6 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
       c[1][d] *= inv;
       c[2][d] *= inv;
       c[3][d] *= inv;
-      c[0][d] = -( c[1][d] + c[2][d] + c[3][d] );
    }
    const C n[3] = { C( m[3] ), C( m[4] ), C( m[5] ) }, sc = C( m[7] );
    // R(x) = R0 + s n.x
@@ -592,29 +592,24 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
          v[d] = sc * n[d] - R * ir * ir * xi[d];
       const C w  = C( q == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kq5[q] * fabs( detJ ) * fabs( snx ) * ir;
       const C t  = C( 1 ) / snx;
-      // c' = c - v (u.c) / (a + v.u) = c - v (x.c) / (s n.x) for the row's vertex and every column vertex
+      // c' = c - v (u.c) / (a + v.u) = c - v (x.c) / (s n.x) for vertices 1..3; vertex 0: minus their sum
       C g[4][3];
 #pragma unroll
-      for ( int j = 0; j < 4; ++j )
+      for ( int j = 1; j < 4; ++j )
       {
          const C xc = ( xi[0] * c[j][0] + xi[1] * c[j][1] + xi[2] * c[j][2] ) * t;
 #pragma unroll
          for ( int d = 0; d < 3; ++d )
             g[j][d] = c[j][d] - v[d] * xc;
       }
-      C gk[3] = { C( 0 ), C( 0 ), C( 0 ) };
 #pragma unroll
-      for ( int j = 0; j < 4; ++j )
-         if ( j == k )
-         {
-            gk[0] = g[j][0];
-            gk[1] = g[j][1];
-            gk[2] = g[j][2];
-         }
+      for ( int d = 0; d < 3; ++d )
+         g[0][d] = -( g[1][d] + g[2][d] + g[3][d] );
 #pragma unroll
-      for ( int j = 0; j < 4; ++j )
-         row[j] += w * ( gk[0] * g[j][0] + gk[1] * g[j][1] + gk[2] * g[j][2] );
+      for ( int j = 1; j < 4; ++j )
+         row[j] += w * ( g[0][0] * g[j][0] + g[0][1] * g[j][1] + g[0][2] * g[j][2] );
    }
+   row[0] = -( row[1] + row[2] + row[3] );
 }
 
 // diag and off-diagonal sum of the partial row of the closure point at slab position pos(0)
