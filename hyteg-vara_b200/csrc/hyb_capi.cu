@@ -930,7 +930,9 @@ constexpr int kNoAllocSlots = 131072;
 static __device__ __align__( 256 ) double g_noAllocPartial[kNoAllocSlots];
 
 // In host code the array's name is only a host-side stand-in, not a device address: the
-// address is looked up once per device, with that device current.
+// address is looked up once per device, with that device current, and cached for the
+// rest of the process. A cudaDeviceReset (or anything else that destroys the device's
+// primary context) invalidates the cached address; do not call the entry point after one.
 double* noAllocScratch()
 {
    static std::mutex mu;
@@ -958,6 +960,18 @@ int hyb_function_dot_noalloc( hyb_function* ah, hyb_function* bh, int level, int
    Function *a = FN( ah ), *b = FN( bh );
    require( out_device, "null result pointer" );
    sameStorage( a, b );
+   {
+      // the scratch array used is the current device's: the functions and the result must
+      // live there too (a host pointer would only fail later, asynchronously)
+      int dev = 0;
+      HYB_CUDA( cudaGetDevice( &dev ) );
+      require( dev == a->st->device, "the functions live on device " + std::to_string( a->st->device ) +
+                                         ", the current device is " + std::to_string( dev ) );
+      cudaPointerAttributes pa{};
+      HYB_CUDA( cudaPointerGetAttributes( &pa, out_device ) );
+      require( ( pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged ) && pa.device == dev,
+               "out_device must be device (or managed) memory of the current device" );
+   }
    require( a->dtype == b->dtype, "dtypes differ" );
    checkLevel( a, level );
    checkLevel( b, level );

@@ -39,6 +39,7 @@ struct Storage
    Topology                              topo;
    int                                   maxLevel = 0;
    int                                   numSMs   = 148;
+   int                                   device   = 0; // the CUDA device the storage lives on
    DevBuf< ClassDev >                    cls;
    DevBuf< int32_t >                     fEmb, eEmbOff, eEmb, vEmbOff, vEmb;
    DevBuf< uint8_t >                     fBc, eBc, vBc;
@@ -84,6 +85,7 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       int dev = 0;
       HYB_CUDA( cudaGetDevice( &dev ) );
       HYB_CUDA( cudaDeviceGetAttribute( &s.numSMs, cudaDevAttrMultiProcessorCount, dev ) );
+      s.device = dev;
    }
    s.topo.build( V, T );
    s.topo.computeColouring();

@@ -161,7 +161,11 @@ int hyb_function_copy_convert( hyb_function* dst, hyb_function* src, int level, 
  * written to the device double `out_device`. The first call on a device looks up the
  * array's device address with that device current; make that first call before any
  * stream capture. All calls share the array and it keeps the last call's contents:
- * calls that overlap on the GPU (other streams, other host threads) race. */
+ * calls that overlap on the GPU (other streams, other host threads) race, and so do
+ * CUDA graphs captured from this call: their partial sums go to the same array, so such
+ * a graph must not run concurrently with another call or graph of this entry point.
+ * The functions and out_device must live on the current device (HYB_EINVAL otherwise);
+ * the looked-up address is cached, so do not call this after a cudaDeviceReset. */
 int hyb_function_dot_noalloc( hyb_function* a, hyb_function* b, int level, int flag, double* out_device, void* stream );
 
 /* ---- operators ---- */

@@ -23,11 +23,19 @@ INNER, DIRICHLET, NEUMANN, FREESLIP, ALL = 1, 2, 4, 8, 15
 _lib = None
 
 
+def reference_root():
+    """The reference checkout named by HYTEG_REFERENCE_ROOT, or None when it is unset or
+    holds no source tree (the compiled reference pieces are then not built)."""
+    root = os.environ.get("HYTEG_REFERENCE_ROOT")
+    return root if root and os.path.isdir(os.path.join(root, "src")) else None
+
+
 def build(ref=False):
-    """Compile the oracle (and, when the reference tree is present, oracle/_ref)."""
+    """Compile the oracle (and, when the reference tree is available, oracle/_ref)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    root = reference_root()
+    if ref and root:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF_ROOT=" + root], check=True)
 
 
 def lib():

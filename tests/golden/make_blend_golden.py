@@ -7,7 +7,7 @@ oracle/_ref/libhyteg_refblend.so, on the spherical shell ntan = 3, nrad = 2, rad
 Per cell: the map at one seeded interior point, and the element matrix of one level-2
 micro-tet for k = 1 (alpha = 0) and k = exp(5 (1 - |x|)) (alpha = 5).
 
-    make -C oracle ref && python tests/golden/make_blend_golden.py
+    HYTEG_REFERENCE_ROOT=<reference checkout> make -C oracle ref && python tests/golden/make_blend_golden.py
 """
 import ctypes
 import os

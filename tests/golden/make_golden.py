@@ -1,7 +1,6 @@
 """Generate the golden fixtures that pin the CPU oracle to the reference.
 
-Run in a checkout where the reference source tree is present (default
-/root/reference). It compiles the reference's own generated macro-cell kernels
+Run with HYTEG_REFERENCE_ROOT naming the reference source tree. It compiles the reference's own generated macro-cell kernels
 and its FEniCS P1 diffusion form, unchanged, into oracle/_ref/ (oracle/Makefile
 target "ref"), runs them on seeded inputs and writes tests/golden/*.npz.
 The tests then compare the oracle against these files; neither the tests nor
@@ -96,9 +95,11 @@ def cell_neighbour_counts(tets):
 
 
 def main():
+    if not O.reference_root():
+        sys.exit("set HYTEG_REFERENCE_ROOT to the reference checkout")
     O.build(ref=True)
     R = O.ref_lib()
-    assert R is not None, "reference kernels not built (is the reference tree present?)"
+    assert R is not None, "reference kernels not built"
     rng = np.random.default_rng(0)
 
     # 1) element stiffness of random tetrahedra
@@ -173,7 +174,7 @@ def main():
     print("golden fixtures written to", HERE)
 
 
-REF_ROOT = os.environ.get("HYTEG_REFERENCE_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("HYTEG_REFERENCE_ROOT")
 
 
 def read_gmsh(path):
