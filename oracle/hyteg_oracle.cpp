@@ -147,6 +147,23 @@ void p1Stiffness( const std::array< std::array< double, 3 >, 4 >& X, double K[4]
       *absDetOut = std::fabs( det );
 }
 
+// The 5-point degree-3 rule of p1_div_k_grad_affine_q3::integrateAll, tetrahedron
+// (src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_affine_q3.cpp:179-381): the centroid
+// with weight -2/15 and the four points with barycentric coordinates (1/2, 1/6, 1/6, 1/6)
+// (the 1/2 on vertex a) with weight 3/40, on the reference tetrahedron of volume 1/6; the
+// element matrix is |det J| sum_q w_q k(x_q) grad(phi_i).grad(phi_j).
+// Barycentric coordinates of point q (q = 0 centroid, q = a + 1 the point weighted on a).
+inline double divKGradBary( int q, int j ) { return q == 0 ? 0.25 : ( j == q - 1 ? 0.5 : 1.0 / 6.0 ); }
+inline double divKGradWeight( int q ) { return q == 0 ? -2.0 / 15.0 : 3.0 / 40.0; }
+// 6 sum_q w_q kq[q] (the factor on the stiffness K_ij = |T| grad.grad, |det J| = 6 |T|)
+inline double divKGradScale( const double kq[5] )
+{
+   double s = 0;
+   for ( int q = 0; q < 5; ++q )
+      s += divKGradWeight( q ) * kq[q];
+   return 6.0 * s;
+}
+
 // ---------------------------------------------------------------------------
 // Topology
 // ---------------------------------------------------------------------------
@@ -183,6 +200,10 @@ struct Op
    std::vector< std::vector< std::array< std::array< double, 15 >, 16 > > > st;
    // variable: nodal k per level, element matrices K[level][cell][type][4][4]
    std::vector< std::vector< double > > k;
+   // variable, coefficient given as a function (the reference form's callback): per level and
+   // cell, 6 sum_q w_q k(x_q) of every micro-tet at index type * closure size + closure index
+   // of its vertex 0 (empty: the nodal coefficient k above is used)
+   std::vector< std::vector< std::vector< double > > > kq6;
    std::vector< std::vector< std::array< std::array< std::array< double, 4 >, 4 >, 6 > > > K;
 };
 
@@ -378,8 +399,21 @@ std::array< double, 3 > microCoord( const Oracle& o, int c, i64 N, i64 x, i64 y,
    return p;
 }
 
-// Element matrices of the six micro-tet shapes of a cell at level L.
-void cellElementMatrices( const Oracle& o, int c, i64 N, std::array< std::array< std::array< double, 4 >, 4 >, 6 >& K )
+// P1 element mass matrix M_ij = |T| (1 + delta_ij) / 20 (the exact integral that
+// P1ElementwiseMassOperator's form computes)
+void p1Mass( const std::array< std::array< double, 3 >, 4 >& X, double M[4][4] )
+{
+   double K[4][4], absDet = 0;
+   p1Stiffness( X, K, &absDet );
+   const double vol = absDet / 6.0;
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j )
+         M[i][j] = vol * ( i == j ? 2.0 : 1.0 ) / 20.0;
+}
+
+// Element matrices of the six micro-tet shapes of a cell at level L (stiffness, or mass).
+void cellElementMatrices( const Oracle& o, int c, i64 N, std::array< std::array< std::array< double, 4 >, 4 >, 6 >& K,
+                          bool mass = false )
 {
    for ( int t = 0; t < 6; ++t )
    {
@@ -387,7 +421,10 @@ void cellElementMatrices( const Oracle& o, int c, i64 N, std::array< std::array<
       for ( int j = 0; j < 4; ++j )
          X[j] = microCoord( o, c, N, kMicro[t][j][0], kMicro[t][j][1], kMicro[t][j][2] );
       double Km[4][4];
-      p1Stiffness( X, Km );
+      if ( mass )
+         p1Mass( X, Km );
+      else
+         p1Stiffness( X, Km );
       for ( int i = 0; i < 4; ++i )
          for ( int j = 0; j < 4; ++j )
             K[t][i][j] = Km[i][j];
@@ -635,17 +672,22 @@ inline void partialRow( const Oracle& o, const Op& op, const Level& lv, int c, i
          // (src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_affine_q3.cpp:179+) with the
          // coefficient callback = P1 interpolant of the nodal k: centroid weight -2/15, four
          // points (1/2,1/6,1/6,1/6) with weight 3/40, all times |det J| = 6|T|.
-         double kq[5];
-         kq[0] = 0.25 * ( kv[dof[0]] + kv[dof[1]] + kv[dof[2]] + kv[dof[3]] );
-         for ( int a = 0; a < 4; ++a )
+         double scale; // K holds |T| grad.grad = |detJ|/6 grad.grad
+         if ( !op.kq6.empty() )
+            scale = op.kq6[lv.L][c][size_t( in.t ) * size_t( lv.S ) +
+                                    size_t( cellIdx( N + 1, x + in.rel[0][0], y + in.rel[0][1], z + in.rel[0][2] ) )];
+         else
          {
-            double s = 0;
-            for ( int j = 0; j < 4; ++j )
-               s += ( j == a ? 0.5 : 1.0 / 6.0 ) * kv[dof[j]];
-            kq[a + 1] = s;
+            double kq[5];
+            for ( int q = 0; q < 5; ++q )
+            {
+               double s = 0;
+               for ( int j = 0; j < 4; ++j )
+                  s += divKGradBary( q, j ) * kv[dof[j]];
+               kq[q] = s;
+            }
+            scale = divKGradScale( kq );
          }
-         const double quad = -2.0 / 15.0 * kq[0] + 3.0 / 40.0 * ( kq[1] + kq[2] + kq[3] + kq[4] );
-         const double scale = 6.0 * quad; // K holds |T| grad.grad = |detJ|/6 grad.grad
          for ( int j = 0; j < 4; ++j )
          {
             const double a = scale * K[in.t][in.k][j];
@@ -1419,9 +1461,11 @@ void orc_cell_closure_map( void* h, int level, int cell, int32_t* out )
    std::memcpy( out, m.data(), m.size() * sizeof( int32_t ) );
 }
 
-int orc_op_laplace( void* h )
+namespace {
+// operator with a constant element matrix per micro-tet shape (stiffness or mass): the
+// stencils of every cell and class mask
+int constantOperator( Oracle* o, bool mass )
 {
-   auto* o = H( h );
    Op op;
    op.variable = false;
    op.st.resize( o->maxLevel + 1 );
@@ -1432,7 +1476,7 @@ int orc_op_laplace( void* h )
       for ( size_t c = 0; c < o->T.size(); ++c )
       {
          std::array< std::array< std::array< double, 4 >, 4 >, 6 > K;
-         cellElementMatrices( *o, int( c ), N, K );
+         cellElementMatrices( *o, int( c ), N, K, mass );
          for ( int mask = 0; mask < 16; ++mask )
          {
             auto& st = op.st[L][c][mask];
@@ -1450,6 +1494,81 @@ int orc_op_laplace( void* h )
                   st[offsetId( in.rel[j][0], in.rel[j][1], in.rel[j][2] )] += K[in.t][in.k][j];
             }
          }
+      }
+   }
+   o->ops.push_back( std::move( op ) );
+   return int( o->ops.size() - 1 );
+}
+} // namespace
+
+int orc_op_laplace( void* h ) { return constantOperator( H( h ), false ); }
+
+int orc_op_mass( void* h ) { return constantOperator( H( h ), true ); }
+
+// P1ElementwiseOperator< p1_div_k_grad_affine_q3 > with the coefficient as the form's callback,
+// evaluated at the 5 quadrature points of every micro-tet on every level, as the reference
+// assembles it (P1ElementwiseOperator.cpp:64-221 calling integrateAll per micro-tet):
+//   kind 1: tanh(2 (x - 1/2)) + 2 (ElementwiseDivKGradCGConvergenceTest);
+//   kind 2: exp( radial (1 - |x|) + sigma sqrt(2/M) sum_m cos( w_m . x + phase_m ) ), the random-
+//           Fourier-feature field of the benchmarks (w: M x 3, phase: M).
+int orc_op_divkgrad_callback( void* h, int kind, const double* w, const double* phase, int modes, double sigma,
+                              double radial )
+{
+   auto* o = H( h );
+   if ( kind != 1 && kind != 2 )
+      return -1;
+   auto kfun = [&]( const double* x ) {
+      if ( kind == 1 )
+         return std::tanh( 2.0 * ( x[0] - 0.5 ) ) + 2.0;
+      double g = 0;
+      for ( int m = 0; m < modes; ++m )
+         g += std::cos( w[3 * m] * x[0] + w[3 * m + 1] * x[1] + w[3 * m + 2] * x[2] + phase[m] );
+      const double r = std::sqrt( x[0] * x[0] + x[1] * x[1] + x[2] * x[2] );
+      return std::exp( radial * ( 1.0 - r ) + sigma * std::sqrt( 2.0 / modes ) * g );
+   };
+   Op op;
+   op.variable = true;
+   op.k.resize( o->maxLevel + 1 );
+   op.K.resize( o->maxLevel + 1 );
+   op.kq6.resize( o->maxLevel + 1 );
+   for ( int L = 0; L <= o->maxLevel; ++L )
+   {
+      const i64 N = i64( 1 ) << L, S = o->lv[L].S;
+      op.k[L].assign( o->lv[L].nDof, 0.0 );
+      op.K[L].resize( o->T.size() );
+      op.kq6[L].resize( o->T.size() );
+#pragma omp parallel for schedule( dynamic )
+      for ( size_t c = 0; c < o->T.size(); ++c )
+      {
+         cellElementMatrices( *o, int( c ), N, op.K[L][c] );
+         auto& kc = op.kq6[L][c];
+         kc.assign( size_t( 6 * S ), 0.0 );
+         for ( int t = 0; t < 6; ++t )
+            for ( i64 az = 0; az <= N; ++az )
+               for ( i64 ay = 0; ay + az <= N; ++ay )
+                  for ( i64 ax = 0; ax + ay + az <= N; ++ax )
+                  {
+                     bool inside = true;
+                     for ( int j = 0; j < 4 && inside; ++j )
+                        inside = inClosure( N, ax + kMicro[t][j][0], ay + kMicro[t][j][1], az + kMicro[t][j][2] );
+                     if ( !inside )
+                        continue;
+                     std::array< double, 3 > X[4];
+                     for ( int j = 0; j < 4; ++j )
+                        X[j] = microCoord( *o, int( c ), N, ax + kMicro[t][j][0], ay + kMicro[t][j][1],
+                                           az + kMicro[t][j][2] );
+                     double kq[5];
+                     for ( int q = 0; q < 5; ++q )
+                     {
+                        double x[3] = { 0, 0, 0 };
+                        for ( int j = 0; j < 4; ++j )
+                           for ( int d = 0; d < 3; ++d )
+                              x[d] += divKGradBary( q, j ) * X[j][d];
+                        kq[q] = kfun( x );
+                     }
+                     kc[size_t( t ) * size_t( S ) + size_t( cellIdx( N + 1, ax + kMicro[t][0][0], ay + kMicro[t][0][1],
+                                                                     az + kMicro[t][0][2] ) )] = divKGradScale( kq );
+                  }
       }
    }
    o->ops.push_back( std::move( op ) );
@@ -1542,6 +1661,37 @@ int orc_blend_element_matrix( void* h, int cell, const double* X12, double alpha
    for ( int i = 0; i < 4; ++i )
       for ( int j = 0; j < 4; ++j )
          out16[4 * i + j] = A[i][j];
+   return 0;
+}
+
+int orc_divkgrad_element_matrix( const double* X12, int kind, const double* k4, double* out16 )
+{
+   std::array< std::array< double, 3 >, 4 > X;
+   for ( int j = 0; j < 4; ++j )
+      X[j] = { X12[3 * j], X12[3 * j + 1], X12[3 * j + 2] };
+   double kq[5];
+   for ( int q = 0; q < 5; ++q )
+   {
+      double x[3] = { 0, 0, 0 }, kl = 0;
+      for ( int j = 0; j < 4; ++j )
+      {
+         for ( int d = 0; d < 3; ++d )
+            x[d] += divKGradBary( q, j ) * X[j][d];
+         kl += divKGradBary( q, j ) * k4[j];
+      }
+      if ( kind == 0 )
+         kq[q] = kl; // the P1 interpolant of the nodal values k4
+      else if ( kind == 1 )
+         kq[q] = std::tanh( 2.0 * ( x[0] - 0.5 ) ) + 2.0; // ElementwiseDivKGradCGConvergenceTest's k
+      else
+         return -1;
+   }
+   double K[4][4];
+   p1Stiffness( X, K );
+   const double sc = divKGradScale( kq );
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j )
+         out16[4 * i + j] = sc * K[i][j];
    return 0;
 }
 

@@ -43,6 +43,13 @@ int64_t orc_num_prims( void* h, int kind );
 // operators: 0 = constant P1 Laplace; then div-k-grad with nodal k per level
 int  orc_op_laplace( void* h );
 int  orc_op_divkgrad( void* h, const double* const* nodalK );
+// P1ElementwiseMassOperator (exact P1 mass matrix |T| (1 + delta_ij) / 20 per micro-tet)
+int  orc_op_mass( void* h );
+// P1ElementwiseOperator< p1_div_k_grad_affine_q3 > with the coefficient evaluated as the form's
+// callback at every micro-tet's quadrature points on every level (the reference's assembly):
+// kind 1 tanh(2 (x - 1/2)) + 2; kind 2 exp(radial (1 - |x|) + sigma sqrt(2/M) sum cos(w.x + phase))
+int  orc_op_divkgrad_callback( void* h, int kind, const double* w, const double* phase, int modes, double sigma,
+                               double radial );
 // P1ElementwiseBlendingDivKGradOperator (p1_div_k_grad_blending_q3) on the macro-cells'
 // IcosahedralShellMaps with k(y) = exp( alpha (1 - |y|) ) of the mapped point; -1 if a cell
 // cannot be classified as a shell cell
@@ -51,6 +58,10 @@ int  orc_op_blend_div_k_grad( void* h, double alpha );
 int  orc_shell_map_eval( void* h, int cell, const double* x, double* Fx, double* DF );
 // the blended element matrix (4x4, row-major) of the micro-tet X (4 vertices x 3) in a cell
 int  orc_blend_element_matrix( void* h, int cell, const double* X12, double alpha, double* out16 );
+// p1_div_k_grad_affine_q3::integrateAll (tetrahedron) restated: X12 the 4 vertices, the
+// coefficient the P1 interpolant of the nodal values k4 (kind 0) or tanh(2 (x - 1/2)) + 2 of
+// ElementwiseDivKGradCGConvergenceTest (kind 1) at the rule's points
+int  orc_divkgrad_element_matrix( const double* X12, int kind, const double* k4, double* out16 );
 void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 );
 
 void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );

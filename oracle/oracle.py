@@ -82,6 +82,12 @@ def lib():
         L.orc_shell_map_eval.argtypes = [P, I, P, P, P]
         L.orc_blend_element_matrix.restype = I
         L.orc_blend_element_matrix.argtypes = [P, I, P, D, P]
+        L.orc_divkgrad_element_matrix.restype = I
+        L.orc_divkgrad_element_matrix.argtypes = [P, I, P, P]
+        L.orc_op_divkgrad_callback.restype = I
+        L.orc_op_divkgrad_callback.argtypes = [P, I, P, P, I, D, D]
+        L.orc_op_mass.restype = I
+        L.orc_op_mass.argtypes = [P]
         L.orc_gmg_solve.restype = I
         L.orc_gmg_solve.argtypes = [P, I, I, I, P, P, I, I, D, I, P, I, D, I, D, I, P, I]
         _lib = L
@@ -128,6 +134,23 @@ class Oracle:
         self._keep = arrs
         ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
         return int(lib().orc_op_divkgrad(self.h, ptrs))
+
+    def op_divkgrad_callback(self, kind, w=None, phase=None, sigma=1.0, radial=0.0):
+        """The variable-coefficient operator as the reference assembles it: the coefficient
+        evaluated as the form's callback at the quadrature points of every micro-tet on every
+        level (kind 1: tanh(2 (x - 1/2)) + 2; kind 2: exp(radial (1 - |x|) + sigma sqrt(2/M)
+        sum_m cos(w_m . x + phase_m)))."""
+        w = np.ascontiguousarray(np.zeros((1, 3)) if w is None else w, np.float64).reshape(-1, 3)
+        ph = np.ascontiguousarray(np.zeros(1) if phase is None else phase, np.float64).ravel()
+        op = int(lib().orc_op_divkgrad_callback(self.h, int(kind), _p(w), _p(ph), len(ph), float(sigma),
+                                                float(radial)))
+        if op < 0:
+            raise ValueError("unknown coefficient kind")
+        return op
+
+    def op_mass(self):
+        """P1ElementwiseMassOperator (exact P1 mass matrix per micro-tet)."""
+        return int(lib().orc_op_mass(self.h))
 
     def op_blend_div_k_grad(self, alpha=0.0):
         """P1ElementwiseBlendingDivKGradOperator on the cells' IcosahedralShellMaps,
@@ -226,6 +249,17 @@ class Oracle:
 # Reference kernels compiled from the reference tree (oracle/_ref), for pinning
 # ---------------------------------------------------------------------------
 _ref = None
+
+
+def divkgrad_element_matrix(X, kind=0, k4=None):
+    """The oracle's restatement of p1_div_k_grad_affine_q3::integrateAll on the tetrahedron X
+    (4 x 3): kind 0 with the P1 interpolant of the nodal values k4, kind 1 with
+    k(x) = tanh(2 (x - 1/2)) + 2."""
+    a = np.zeros(16)
+    k = np.ascontiguousarray(np.ones(4) if k4 is None else k4, np.float64)
+    if lib().orc_divkgrad_element_matrix(_p(np.ascontiguousarray(X, np.float64)), int(kind), _p(k), _p(a)) != 0:
+        raise ValueError("unknown coefficient kind")
+    return a.reshape(4, 4)
 
 
 def chebyshev_coefficients(order, lower, upper):
