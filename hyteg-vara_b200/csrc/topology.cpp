@@ -488,19 +488,17 @@ void readGmsh( const std::string& path, std::vector< std::array< double, 3 > >& 
    T.assign( cells.begin(), cells.end() );
 }
 
-// Thick spherical shell (the mesh family of MeshInfo::meshSphericalShell,
-// src/hyteg/mesh/MeshGenSphericalShell.cpp:579-690): the 20 faces of the icosahedron are
-// each cut into (ntan - 1)^2 triangles, projected onto the unit sphere, and the sphere is
-// repeated on nrad radii evenly spaced in [rmin, rmax]; every prism between two radii is
-// split into three tetrahedra. This gives the reference's cell count,
-// 60 (ntan - 1)^2 (nrad - 1), and vertex count, (10 (ntan - 1)^2 + 2) nrad, with affine
-// macro-cells, but the triangulation of the sphere is this function's own (uniform
-// barycentric subdivision of the icosahedron faces), not the reference's diamond meshing.
-// Shared sphere points are computed once, from a canonical key, so coincident vertices
-// are bitwise equal. Prism split: with the triangle's vertices in ascending id order
-// (0, 1, 2) and b/t its bottom/top copies, the tetrahedra (b0 b1 b2 t2), (b0 b1 t1 t2),
-// (b0 t0 t1 t2) cut every quadrilateral side from its lower-id bottom vertex to its
-// higher-id top vertex, so neighbouring prisms agree on the shared diagonal.
+// Thick spherical shell: MeshInfo::meshSphericalShell( ntan, nrad, rmin, rmax ) with the
+// reference's default meshing SHELLMESH_CLASSIC (src/hyteg/mesh/MeshGenSphericalShell.cpp:
+// 577-900), restated. The unit sphere is the icosahedron seen as ten "diamonds" (pairs of
+// triangles sharing an edge, five around each pole), each refined by repeated arc midpoints
+// into an ntan x ntan grid of nodes (ntan - 1 a power of two); the nodes are scaled to nrad
+// equidistant radii. Vertex ids: the north pole of every radius, then the south poles, then
+// radius by radius the other nodes diamond by diamond. Every grid square between two radii
+// is a prism-like local cell of 8 vertices split into 6 tetrahedra by fixed tables (one for
+// each hemisphere). Cells come out in the order of the reference's cell map: sorted by their
+// vertex-id lists. The tables (icosahedral nodes, diamond corners, local-cell offsets, the
+// two tetrahedron splits) must be the reference's for the meshes to be the same.
 void meshSphericalShell( int ntan, int nrad, double rmin, double rmax, std::vector< std::array< double, 3 > >& V,
                          std::vector< std::array< int, 4 > >& T )
 {
@@ -508,101 +506,129 @@ void meshSphericalShell( int ntan, int nrad, double rmin, double rmax, std::vect
       throw std::invalid_argument( "meshSphericalShell: need ntan >= 2 and nrad >= 2" );
    if ( !( rmin > 0 ) || !( rmin < rmax ) )
       throw std::invalid_argument( "meshSphericalShell: need 0 < rmin < rmax" );
-   const int    n   = ntan - 1;
-   const double phi = ( 1.0 + std::sqrt( 5.0 ) ) / 2.0;
-   // icosahedron: cyclic permutations of (0, +-1, +-phi)
-   std::vector< std::array< double, 3 > > ico;
-   for ( int a : { -1, 1 } )
-      for ( int b : { -1, 1 } )
-      {
-         ico.push_back( { 0.0, double( a ), b * phi } );
-         ico.push_back( { double( a ), b * phi, 0.0 } );
-         ico.push_back( { b * phi, 0.0, double( a ) } );
-      }
-   auto dist2 = [&]( int i, int j ) {
-      double d = 0;
-      for ( int k = 0; k < 3; ++k )
-         d += ( ico[i][k] - ico[j][k] ) * ( ico[i][k] - ico[j][k] );
-      return d;
-   };
-   // faces: triples of mutually adjacent vertices (edge length 2)
-   std::vector< std::array< int, 3 > > faces;
-   for ( int i = 0; i < 12; ++i )
-      for ( int j = i + 1; j < 12; ++j )
-         for ( int k = j + 1; k < 12; ++k )
-            if ( std::fabs( dist2( i, j ) - 4 ) < 1e-9 && std::fabs( dist2( i, k ) - 4 ) < 1e-9 &&
-                 std::fabs( dist2( j, k ) - 4 ) < 1e-9 )
-               faces.push_back( { i, j, k } );
-   if ( faces.size() != 20 )
-      throw std::logic_error( "meshSphericalShell: icosahedron construction failed" );
-   // sphere points by canonical key: (kind, a, b, c) with kind 0 vertex (a), 1 edge point
-   // (a < b, c steps from a), 2 face point (face a, i = b, j = c)
-   std::map< std::array< int, 4 >, int >  key2id;
-   std::vector< std::array< double, 3 > > S;
-   auto point = [&]( const std::array< int, 4 >& key, const std::array< double, 3 >& x ) {
-      auto it = key2id.find( key );
-      if ( it != key2id.end() )
-         return it->second;
-      const double r = std::sqrt( x[0] * x[0] + x[1] * x[1] + x[2] * x[2] );
-      S.push_back( { x[0] / r, x[1] / r, x[2] / r } );
-      key2id[key] = int( S.size() ) - 1;
-      return int( S.size() ) - 1;
-   };
-   auto mix = [&]( int a, double wa, int b, double wb, int c, double wc ) {
-      std::array< double, 3 > x;
-      for ( int k = 0; k < 3; ++k )
-         x[k] = ( ico[a][k] * wa + ico[b][k] * wb + ico[c][k] * wc ) / n;
-      return x;
-   };
-   std::vector< std::array< int, 3 > > tris;
-   for ( int f = 0; f < 20; ++f )
-   {
-      const int a = faces[f][0], b = faces[f][1], c = faces[f][2]; // ascending
-      auto      P = [&]( int i, int j ) {
-         const int wa = n - i - j, wb = i, wc = j;
-         if ( wb == 0 && wc == 0 )
-            return point( { 0, a, 0, 0 }, ico[a] );
-         if ( wa == 0 && wc == 0 )
-            return point( { 0, b, 0, 0 }, ico[b] );
-         if ( wa == 0 && wb == 0 )
-            return point( { 0, c, 0, 0 }, ico[c] );
-         if ( wc == 0 )
-            return point( { 1, a, b, wb }, mix( a, wa, b, wb, c, 0 ) );
-         if ( wb == 0 )
-            return point( { 1, a, c, wc }, mix( a, wa, c, wc, b, 0 ) );
-         if ( wa == 0 )
-            return point( { 1, b, c, wc }, mix( b, wb, c, wc, a, 0 ) );
-         return point( { 2, f, i, j }, mix( a, wa, b, wb, c, wc ) );
-      };
-      for ( int j = 0; j < n; ++j )
-         for ( int i = 0; i + j < n; ++i )
-         {
-            tris.push_back( { P( i, j ), P( i + 1, j ), P( i, j + 1 ) } );
-            if ( i + j + 1 < n )
-               tris.push_back( { P( i + 1, j ), P( i + 1, j + 1 ), P( i, j + 1 ) } );
-         }
-   }
-   const int nS = int( S.size() );
-   V.clear();
-   T.clear();
+   const int n1 = ntan - 1;
+   if ( ( n1 & ( n1 - 1 ) ) != 0 )
+      throw std::invalid_argument( "meshSphericalShell: ntan - 1 must be a power of two" );
+   std::vector< double > radius( static_cast< size_t >( nrad ), 0.0 );
    for ( int l = 0; l < nrad; ++l )
+      radius[size_t( l )] = rmin + ( ( rmax - rmin ) / double( nrad - 1 ) ) * double( l );
+
+   // the twelve icosahedral nodes: poles 0 and 11, an upper ring 1..5 and a lower ring 6..10
+   // of pentagons, each ring counter-clockwise
+   double       ico[12][3];
+   const double fifthPi = 0.4 * std::asin( 1.0 );
+   const double w       = 2.0 * std::acos( 1.0 / ( 2.0 * std::sin( fifthPi ) ) );
+   const double cw = std::cos( w ), sw = std::sin( w );
+   ico[0][0] = 0.0, ico[0][1] = 0.0, ico[0][2] = 1.0;
+   ico[11][0] = 0.0, ico[11][1] = 0.0, ico[11][2] = -1.0;
+   for ( int k = 1; k <= 5; ++k )
    {
-      const double r = rmin + ( rmax - rmin ) * l / ( nrad - 1 );
-      for ( const auto& x : S )
-         V.push_back( { r * x[0], r * x[1], r * x[2] } );
+      const double up = 2.0 * ( double( k ) - 0.5 ) * fifthPi, lo = 2.0 * ( double( k ) - 1 ) * fifthPi;
+      ico[k][0] = sw * std::cos( up ), ico[k][1] = sw * std::sin( up ), ico[k][2] = cw;
+      ico[k + 5][0] = sw * std::cos( lo ), ico[k + 5][1] = sw * std::sin( lo ), ico[k + 5][2] = -cw;
    }
-   for ( auto t : tris )
+   // diamond corners: pole, then counter-clockwise (left, bottom, right on the north side)
+   static const int diamond[10][4] = { { 0, 5, 6, 1 },   { 0, 1, 7, 2 },  { 0, 2, 8, 3 },  { 0, 3, 9, 4 },
+                                       { 0, 4, 10, 5 },  { 11, 7, 1, 6 }, { 11, 8, 2, 7 }, { 11, 9, 3, 8 },
+                                       { 11, 10, 4, 9 }, { 11, 6, 5, 10 } };
+   // unit-sphere node (i1, i2) of diamond d: arc midpoints, level by level
+   std::vector< double > node( size_t( ntan ) * ntan * 10 * 3, 0.0 );
+   auto nd = [&]( int i1, int i2, int d ) { return &node[( ( size_t( i1 ) * ntan + i2 ) * 10 + d ) * 3]; };
+   auto midpoint = [&]( double* out, const double* p, const double* q ) {
+      const double x = p[0] + q[0], y = p[1] + q[1], z = p[2] + q[2];
+      const double s = std::sqrt( x * x + y * y + z * z );
+      out[0] = x / s, out[1] = y / s, out[2] = z / s;
+   };
+   for ( int d = 0; d < 10; ++d )
    {
-      std::sort( t.begin(), t.end() );
-      for ( int l = 0; l + 1 < nrad; ++l )
+      const int left = d < 5 ? 1 : 3, right = d < 5 ? 3 : 1; // mirrored on the south side
+      std::copy( ico[diamond[d][0]], ico[diamond[d][0]] + 3, nd( 0, 0, d ) );
+      std::copy( ico[diamond[d][left]], ico[diamond[d][left]] + 3, nd( n1, 0, d ) );
+      std::copy( ico[diamond[d][2]], ico[diamond[d][2]] + 3, nd( n1, n1, d ) );
+      std::copy( ico[diamond[d][right]], ico[diamond[d][right]] + 3, nd( 0, n1, d ) );
+      for ( int m = 1; m < n1; m *= 2 )
       {
-         const int b0 = l * nS + t[0], b1 = l * nS + t[1], b2 = l * nS + t[2];
-         const int t0 = b0 + nS, t1 = b1 + nS, t2 = b2 + nS;
-         T.push_back( { b0, b1, b2, t2 } );
-         T.push_back( { b0, b1, t1, t2 } );
-         T.push_back( { b0, t0, t1, t2 } );
+         const int l = n1 / m, h = l / 2;
+         for ( int a = 0; a <= m; ++a ) // along i2 on the lines i1 = a l
+            for ( int b = 0; b < m; ++b )
+               midpoint( nd( a * l, b * l + h, d ), nd( a * l, b * l, d ), nd( a * l, b * l + l, d ) );
+         for ( int a = 0; a <= m; ++a ) // along i1 on the lines i2 = a l
+            for ( int b = 0; b < m; ++b )
+               midpoint( nd( b * l + h, a * l, d ), nd( b * l, a * l, d ), nd( b * l + l, a * l, d ) );
+         for ( int a = 0; a < m; ++a ) // the diagonals (i1 - h, i2 + h) -- (i1 + h, i2 - h)
+            for ( int b = 0; b < m; ++b )
+               midpoint( nd( a * l + h, b * l + h, d ), nd( a * l, b * l + l, d ), nd( a * l + l, b * l, d ) );
       }
    }
+   // vertex id of grid node (s1, s2) of diamond d on radius r; nodes on a diamond's left
+   // edges are stored with the neighbouring diamond that owns them
+   const int perLayer = 10 * n1 * n1;
+   auto      vertexId = [&]( int s1, int s2, int d, int r ) {
+      if ( s1 == 0 && s2 == 0 )
+         return d < 5 ? r : nrad + r;
+      if ( s2 == 0 )
+      {
+         s2 = s1;
+         s1 = 0;
+         d  = d < 5 ? ( d + 4 ) % 5 : ( d + 4 ) % 5 + 5;
+      }
+      else if ( s1 == n1 )
+      {
+         s1 = n1 - s2;
+         s2 = n1;
+         d  = d < 5 ? ( d + 4 ) % 5 + 5 : d % 5;
+      }
+      return 2 * nrad + r * perLayer + d * n1 * n1 + ( s2 - 1 ) * n1 + s1;
+   };
+   V.assign( size_t( ( perLayer + 2 ) * nrad ), { 0.0, 0.0, 0.0 } );
+   for ( int id = 0; id < ( perLayer + 2 ) * nrad; ++id )
+   {
+      int s1 = 0, s2 = 0, d = 0, r = 0;
+      if ( id < nrad )
+         r = id;
+      else if ( id < 2 * nrad )
+         d = 5, r = id - nrad;
+      else
+      {
+         int k = id - 2 * nrad;
+         r     = k / perLayer;
+         k -= r * perLayer;
+         d = k / ( n1 * n1 );
+         k -= d * n1 * n1;
+         s2 = k / n1 + 1;
+         s1 = k - ( s2 - 1 ) * n1;
+      }
+      const double* u = nd( s1, s2, d );
+      V[size_t( id )] = { u[0] * radius[size_t( r )], u[1] * radius[size_t( r )], u[2] * radius[size_t( r )] };
+   }
+   // local cell of grid square (s1, s2) between radii r and r + 1: corner k at offsets
+   // (ds1, ds2, dr) (ds1 and ds2 swapped on the south side), split into six tetrahedra
+   static const int corner[8][3] = { { 0, 0, 1 }, { 1, 0, 1 }, { 1, 1, 1 }, { 0, 1, 1 },
+                                     { 0, 0, 0 }, { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 } };
+   static const int north[6][4]  = { { 0, 1, 3, 7 }, { 4, 7, 5, 0 }, { 0, 5, 1, 7 },
+                                     { 1, 2, 3, 6 }, { 5, 7, 6, 1 }, { 3, 6, 7, 1 } };
+   static const int south[6][4]  = { { 4, 7, 5, 1 }, { 0, 1, 3, 4 }, { 4, 3, 7, 1 },
+                                     { 7, 6, 5, 2 }, { 3, 1, 2, 7 }, { 5, 2, 1, 7 } };
+   std::vector< std::array< int, 4 > > cells;
+   for ( int r = 0; r + 1 < nrad; ++r )
+      for ( int d = 0; d < 10; ++d )
+         for ( int s2 = 0; s2 < n1; ++s2 )
+            for ( int s1 = 0; s1 < n1; ++s1 )
+            {
+               int v[8];
+               for ( int k = 0; k < 8; ++k )
+               {
+                  const int a = d <= 4 ? corner[k][0] : corner[k][1], b = d <= 4 ? corner[k][1] : corner[k][0];
+                  v[k] = vertexId( s1 + a, s2 + b, d, r + corner[k][2] );
+               }
+               for ( int t = 0; t < 6; ++t )
+               {
+                  const int( &tab )[4] = d <= 4 ? north[t] : south[t];
+                  cells.push_back( { v[tab[0]], v[tab[1]], v[tab[2]], v[tab[3]] } );
+               }
+            }
+   std::sort( cells.begin(), cells.end() );
+   T = cells;
 }
 
 } // namespace hyb

@@ -192,7 +192,8 @@ class PrimitiveStorage:
 
     @classmethod
     def spherical_shell(cls, ntan, nrad, rmin, rmax, max_level):
-        """MeshInfo::meshSphericalShell(ntan, nrad, rmin, rmax) family (own sphere triangulation)."""
+        """MeshInfo::meshSphericalShell(ntan, nrad, rmin, rmax) (SHELLMESH_CLASSIC; ntan - 1 a power
+        of two): the reference's vertices, cells and cell order."""
         st = cls.__new__(cls)
         h = ctypes.c_void_p()
         _check(load().hyb_storage_create_spherical_shell(ntan, nrad, float(rmin), float(rmax), max_level,

@@ -8,8 +8,9 @@
  *                                 setMeshBoundaryFlagsOnBoundary(1,0,true) + PrimitiveStorage
  *                                 (src/hyteg/primitivestorage/SetupPrimitiveStorage.hpp:52,136)
  *   hyb_storage_create_cuboid     MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:34-160)
- *   hyb_storage_create_spherical_shell  MeshInfo::meshSphericalShell (MeshGenSphericalShell.cpp:579-690;
- *                                 same cell and vertex counts, own sphere triangulation)
+ *   hyb_storage_create_spherical_shell  MeshInfo::meshSphericalShell with SHELLMESH_CLASSIC
+ *                                 (src/hyteg/mesh/MeshGenSphericalShell.cpp:577-900): the same
+ *                                 vertices, cells and cell order
  *   hyb_function_create           P1Function<V>(name, storage, minLevel, maxLevel)
  *                                 (src/hyteg/p1functionspace/P1Function.hpp:26-27)
  *   hyb_function_interpolate_const  VertexDoFFunction::interpolate(constant, level, flag)
@@ -109,8 +110,10 @@ int     hyb_storage_create( const double* coords, int64_t num_vertices, const in
 /* MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp): a Gmsh 2.2 ASCII file,
  * vertices in file-id order, tetrahedra in the reference's cell order */
 int     hyb_storage_create_from_gmsh( const char* path, int max_level, hyb_storage** out );
-/* thick spherical shell: icosahedral sphere with (ntan - 1)^2 triangles per icosahedron
- * face on nrad radii in [rmin, rmax], prisms split into three tetrahedra */
+/* thick spherical shell, the reference's SHELLMESH_CLASSIC meshing: the icosahedron's ten
+ * diamonds refined by arc midpoints into ntan x ntan nodes (ntan - 1 a power of two) on nrad
+ * equidistant radii in [rmin, rmax], every grid cell between two radii split into six
+ * tetrahedra; vertex ids and cell order as MeshInfo::meshSphericalShell numbers them */
 int     hyb_storage_create_spherical_shell( int ntan, int nrad, double rmin, double rmax, int max_level, hyb_storage** out );
 int     hyb_storage_create_cuboid( int nx, int ny, int nz, const double* lo3, const double* hi3, int max_level,
                                    hyb_storage** out );
