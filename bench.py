@@ -93,6 +93,18 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def profile_figure(name, key):
+    """A figure recorded as `key = value` in an ncu summary under profiles/ (None if absent)."""
+    import re
+
+    try:
+        text = open(os.path.join(ROOT, "profiles", name)).read()
+    except OSError:
+        return None
+    m = re.search(r"\b" + re.escape(key) + r"\s*=\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
 def rank_reduce(vals, op, world, device):
     """All-reduce floats over the ranks of the default process group ("max" for times,
     "sum" for throughputs); identity on a single rank. Every rank calls it in the same
@@ -239,10 +251,12 @@ def ours(args, rank, world, local_rank):
         return {"bound": "hbm", "achieved": round(a, 1), "peak": peak, "unit": "GB/s", "frac": round(a / peak, 3),
                 "peak_source": peak_kind, "traffic": t_bytes, "traffic_source": t_src}
 
-    # DRAM bytes (read + write) per launch from ncu captures of the same kernels and workload
-    # (the sum over the ten launches of one sweep): profiles/k_sor_fp64_fp32_level7_cube48.md,
-    # profiles/k_apply_fp64_level7_cube48.md
-    sweep64_traffic, sweep32_traffic, apply_traffic = 1510.5e6, 902.3e6, 429.7e6
+    # DRAM bytes (read + write) per launch from the warm-cache ncu captures of the same kernels
+    # and workload that profiles/ summarises (one sweep = the sum over its ten launches)
+    sweep_prof, apply_prof = "k_sor_fp64_fp32_level7_cube48.md", "k_apply_fp64_level7_cube48.md"
+    sweep64_traffic = profile_figure(sweep_prof, "fp64_sweep_bytes")
+    sweep32_traffic = profile_figure(sweep_prof, "fp32_sweep_bytes")
+    apply_traffic = profile_figure(apply_prof, "fp64_apply_bytes")
     if (L, nc) != (7, 2):
         sweep64_traffic = sweep32_traffic = apply_traffic = None
 
@@ -290,12 +304,12 @@ def ours(args, rank, world, local_rank):
             "final_rel_residual": {"mixed": float(hist_mixed[-1][-1]), "fp64": float(hist_fp64[-1][-1])},
             "error_mixed_vs_fp64_solution": err_mixed,
             "dof_updates_per_s_fp64": world * n_unknowns * sum(cyc_fp64) / (t_fp64 / 1e3),
-            "roofline": dict(roof(sor_gbs, sweep64_traffic, "ncu, profiles/k_sor_fp64_fp32_level7_cube48.md"),
+            "roofline": dict(roof(sor_gbs, sweep64_traffic, "ncu (warm caches), profiles/" + sweep_prof),
                              kernel="k_sor_iface + k_sor_interior (one FP64 multicolour SOR sweep, 10 launches, level 7)",
                              ms=t_sor * 1e3),
-            "roofline_apply": dict(roof(apply_gbs, apply_traffic, "ncu, profiles/k_apply_fp64_level7_cube48.md"),
+            "roofline_apply": dict(roof(apply_gbs, apply_traffic, "ncu (warm caches), profiles/" + apply_prof),
                                    kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
-            "roofline_sor_fp32": dict(roof(sor32_gbs, sweep32_traffic, "ncu, profiles/k_sor_fp64_fp32_level7_cube48.md"),
+            "roofline_sor_fp32": dict(roof(sor32_gbs, sweep32_traffic, "ncu (warm caches), profiles/" + sweep_prof),
                                       kernel="k_sor_iface + k_sor_interior (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "variable_coefficient": varcoef, "spherical_shell": shell, "blended_shell": blend, "serving": serve,
@@ -556,7 +570,7 @@ def cpu_baseline(args, steps=1):
     import oracle as O
 
     cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    threads = O.set_threads(cores)
     c, t = O.mesh_cuboid(args.cubes, args.cubes, args.cubes)
     orc = O.Oracle(c, t, args.level)
     L = args.level
@@ -567,15 +581,21 @@ def cpu_baseline(args, steps=1):
     t0 = time.perf_counter()
     orc.gmg(x, b, 0, L, smoother=0, max_cycles=steps)
     dt = time.perf_counter() - t0
-    return {"value": n_unknowns * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": n_unknowns * steps / dt, "unit": UNIT, "cores": threads, "host_cores": cores, "threads": threads,
+            "kind": "port",
             "sample": f"{steps} FP64 V(3,3) cycle(s) at level {L} on the {6 * args.cubes ** 3}-tet mesh, "
-                      f"reference SOR ordering, {dt:.2f} s"}
+                      f"reference SOR ordering, {threads} OpenMP threads, {dt:.2f} s"}
 
 
 def reference(args, rank, world):
-    """The reference's algorithm on the host CPU (oracle port; the reference itself cannot be
-    built here: its waLBerla and Eigen submodules and MPI are absent). Each step is one FP64
-    V(3,3) cycle of the workload."""
+    """The reference's algorithm on the host CPU: the oracle port (the reference itself cannot
+    be built here: its waLBerla and Eigen submodules and MPI are absent), FP64 with the
+    reference's staged lexicographic SOR, OpenMP over all host threads (the count is stated).
+    Each timed step is one V(3,3) cycle of the workload (a bounded sample; the unit is the
+    same DoF-updates/s per V-cycle as ours). Besides the K timed cycles, the line reports one
+    whole FP64 solve from zero to relative residual 1e-8 (its cycles and seconds: the
+    time-to-tolerance form of the metric) and one cycle on a single thread (the reference's
+    default build has no OpenMP)."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -583,6 +603,7 @@ def reference(args, rank, world):
     import oracle as O
 
     cores = os.cpu_count() or 1
+    threads = O.set_threads(cores)
     c, t = O.mesh_cuboid(args.cubes, args.cubes, args.cubes)
     L = args.level
     orc = O.Oracle(c, t, L)
@@ -598,13 +619,32 @@ def reference(args, rank, world):
         orc.gmg(x, b, 0, L, smoother=0, max_cycles=1)
     dt = time.perf_counter() - t0
     value = n_unknowns * args.steps / dt
+    # one whole solve to tolerance from the zero guess
+    x[:] = 0
+    t0 = time.perf_counter()
+    _, hist = orc.gmg(x, b, 0, L, smoother=0, max_cycles=60, rel_tol=TOL)
+    t_tol = time.perf_counter() - t0
+    # one cycle on one thread
+    O.set_threads(1)
+    x[:] = 0
+    t0 = time.perf_counter()
+    orc.gmg(x, b, 0, L, smoother=0, max_cycles=1)
+    t_one = time.perf_counter() - t0
+    O.set_threads(threads)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"Poisson, {args.cubes}^3 cuboid ({6 * args.cubes ** 3} macro-tets), level {L}, "
-                                   f"one FP64 V(3,3) cycle per step, reference SOR ordering"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} V-cycles at level {L}"},
+            "config": {"workload": f"Poisson, {args.cubes}x{args.cubes}x{args.cubes} cuboid "
+                                   f"({6 * args.cubes ** 3} macro-tets), level {L}, FP64 V(3,3) cycles, "
+                                   f"reference SOR ordering (one cycle per timed step)",
+                       "unknowns": n_unknowns, "threads": threads, "host_cores": cores},
+            "time_to_tol_s": {"fp64": t_tol, "cycles": len(hist) - 1, "final_rel_residual": float(hist[-1]),
+                              "dof_updates_per_s": n_unknowns * (len(hist) - 1) / t_tol},
+            "single_thread": {"dof_updates_per_s": n_unknowns / t_one, "s_per_cycle": t_one},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "host_cores": cores, "threads": threads,
+                             "kind": "port",
+                             "sample": f"{args.steps} FP64 V(3,3) cycles at level {L}, reference SOR ordering, "
+                                       f"{threads} OpenMP threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

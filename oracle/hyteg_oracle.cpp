@@ -13,6 +13,9 @@
 // (src/hyteg/p1functionspace/P1Elements.hpp:464-526 calculateStencilInMacroCellForm_new,
 //  P1Operator.hpp:1045-1175 apply_edge / apply_face3D).
 #include "hyteg_oracle.h"
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include <algorithm>
 #include <array>
@@ -1662,6 +1665,18 @@ int orc_blend_element_matrix( void* h, int cell, const double* X12, double alpha
       for ( int j = 0; j < 4; ++j )
          out16[4 * i + j] = A[i][j];
    return 0;
+}
+
+int orc_set_threads( int n )
+{
+#ifdef _OPENMP
+   if ( n > 0 )
+      omp_set_num_threads( n );
+   return omp_get_max_threads();
+#else
+   (void) n;
+   return 1;
+#endif
 }
 
 int orc_divkgrad_element_matrix( const double* X12, int kind, const double* k4, double* out16 )

@@ -62,6 +62,8 @@ int  orc_blend_element_matrix( void* h, int cell, const double* X12, double alph
 // coefficient the P1 interpolant of the nodal values k4 (kind 0) or tanh(2 (x - 1/2)) + 2 of
 // ElementwiseDivKGradCGConvergenceTest (kind 1) at the rule's points
 int  orc_divkgrad_element_matrix( const double* X12, int kind, const double* k4, double* out16 );
+// OpenMP threads of the oracle's parallel loops (n > 0 sets them); the count in effect
+int  orc_set_threads( int n );
 void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 );
 
 void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );

@@ -82,6 +82,8 @@ def lib():
         L.orc_shell_map_eval.argtypes = [P, I, P, P, P]
         L.orc_blend_element_matrix.restype = I
         L.orc_blend_element_matrix.argtypes = [P, I, P, D, P]
+        L.orc_set_threads.restype = I
+        L.orc_set_threads.argtypes = [I]
         L.orc_divkgrad_element_matrix.restype = I
         L.orc_divkgrad_element_matrix.argtypes = [P, I, P, P]
         L.orc_op_divkgrad_callback.restype = I
@@ -249,6 +251,11 @@ class Oracle:
 # Reference kernels compiled from the reference tree (oracle/_ref), for pinning
 # ---------------------------------------------------------------------------
 _ref = None
+
+
+def set_threads(n):
+    """Number of OpenMP threads of the oracle's parallel loops; returns the count in effect."""
+    return int(lib().orc_set_threads(int(n)))
 
 
 def divkgrad_element_matrix(X, kind=0, k4=None):
