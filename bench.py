@@ -525,7 +525,9 @@ def serve_stream(n, rate, seed, levels=(3, 7), cubes=(1, 4)):
 def serving(args, H):
     """Serving stream at --rate requests/s through the continuous-batching loop. Warm-up:
     one request of every shape the stream holds, so that hierarchies are resident and
-    their graphs captured before the timed stream (as in a long-running server)."""
+    their graphs captured before the timed stream (as in a long-running server). Then the
+    same requests one at a time (the mix's throughput without overlap) and a second stream
+    at 0.7x the measured capacity (latency without a backlog)."""
     import numpy as np
 
     stream = serve_stream(args.serve_requests, args.rate, 1234)
@@ -544,16 +546,45 @@ def serving(args, H):
     lat = np.array([(r.done_s - r.arrival_s) * 1e3 for r in ok])
     wait = np.array([(r.admit_s - r.arrival_s) * 1e3 for r in ok])
     makespan = max(r.done_s for r in res) - min(r.arrival_s for r in res)
+
     # unknowns (interior micro-vertices) x cycles of the completed solves
-    work = sum((q[0] * (1 << q[3]) - 1) ** 3 * r.cycles for (a, q), r in zip(stream, res) if r.status == 0)
+    def work_of(strm, results):
+        return sum((q[0] * (1 << q[3]) - 1) ** 3 * r.cycles for (a, q), r in zip(strm, results) if r.status == 0)
+
+    work = work_of(stream, res)
     stats = sv.stats()
+    # the same requests one at a time (one slot, all present at the start): the throughput of
+    # this mix without overlap, what the concurrent loop is compared with
+    sq = H.Server(int(args.serve_budget_gb * (1 << 30)), max_active=1, max_level=7)
+    for i, sh in enumerate(shapes):
+        sq.submit(H.Server.request(*sh, seed=10_000 + i), arrival_s=0.0)
+    sq.run(600)
+    sids = [sq.submit(H.Server.request(*q), arrival_s=0.0) for a, q in stream]
+    sq.run(900)
+    sres = [sq.result(i) for i in sids]
+    s_span = max(r.done_s for r in sres) - min(r.arrival_s for r in sres)
+    sq.close()
+    # a stream at a rate the loop sustains (0.7 x the measured capacity): latency without a backlog
+    rate2 = max(1.0, round(0.7 * len(ok) / makespan, 1))
+    stream2 = serve_stream(args.serve_requests, rate2, 4321)
+    ids2 = [sv.submit(H.Server.request(*q), arrival_s=a) for a, q in stream2]
+    sv.run(900)
+    res2 = [sv.result(i) for i in ids2]
+    ok2 = [r for r in res2 if r.status == 0]
+    lat2 = np.array([(r.done_s - r.arrival_s) * 1e3 for r in ok2])
     sv.close()
     return {"rate_req_per_s": args.rate, "requests": len(res), "completed": len(ok),
             "statuses": sorted({r.status for r in res}),
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "p50_queue_ms": float(np.percentile(wait, 50)),
             "solves_per_s": len(ok) / makespan, "makespan_s": makespan,
-            "dof_updates_per_s": work / makespan, "max_rel_residual": max(r.rel_residual for r in ok),
+            "dof_updates_per_s": work / makespan,
+            "one_at_a_time": {"dof_updates_per_s": work_of(stream, sres) / s_span, "solves_per_s": len(sres) / s_span,
+                              "makespan_s": s_span},
+            "concurrent_over_one_at_a_time": (work / makespan) / (work_of(stream, sres) / s_span),
+            "sustained": {"rate_req_per_s": rate2, "completed": len(ok2), "p50_ms": float(np.percentile(lat2, 50)),
+                          "p99_ms": float(np.percentile(lat2, 99)), "mean_ms": float(lat2.mean())},
+            "max_rel_residual": max(r.rel_residual for r in ok),
             "slots": args.serve_slots, "budget_gb": args.serve_budget_gb, "warmup_s": warm_s,
             "peak_gb": stats["peak_bytes"] / 2 ** 30, "hierarchies_built": stats["hierarchies_built"],
             "graphs_captured": stats["graphs_captured"], "clocks": clk.summary(),

@@ -45,11 +45,20 @@ struct Gmg
       long long       kernels; // kernel launches captured in the graph
    };
    std::vector< G > graphs;
+   // device-iterated solves (runSolveLoop): one graph per (x, b, level, step kind), and the
+   // stopping-test state they share (SolveCtl, device and pinned host copy)
+   std::vector< G > loops;
+   DevBuf< SolveCtl > ctl;
+   SolveCtl*          hostCtl = nullptr;
 
    ~Gmg()
    {
       for ( auto& g : graphs )
          cudaGraphExecDestroy( g.exec );
+      for ( auto& g : loops )
+         cudaGraphExecDestroy( g.exec );
+      if ( hostCtl )
+         cudaFreeHost( hostCtl );
       if ( cap )
          cudaStreamDestroy( cap );
       if ( hostScalar )
@@ -568,4 +577,97 @@ void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s
    g.graphs.push_back( { &x, &b, l, kind, exec, captured } );
    HYB_CUDA( cudaGraphLaunch( exec, stream ) );
    g_launches.fetch_add( captured );
+}
+
+// A whole solve as ONE graph launch: while ||b - A x|| / ||b|| > tol (and fewer than
+// maxCycles steps ran), run the step `kind` (kCycle64Norm: an FP64 V-cycle; kMixedStep: an
+// FP32 V-cycle with FP64 refinement), each followed by the device-side stopping test
+// (k_solve_ctl) that sets the condition of the graph's WHILE node -- no host round trip
+// per cycle. Before it, the residual norm of the start iterate must be in scalars[0] and
+// ||b||^2 in scalars[1] (the kNorm64 / kNormMixed graphs and a dot product). Afterwards
+// g.ctl holds the cycles run and the final relative residual.
+void runSolveLoop( Gmg& g, Function& x, Function& b, int l, int kind, double tol, int maxCycles, cudaStream_t stream )
+{
+   require( kind == kCycle64Norm || kind == kMixedStep, "the solve loop iterates V-cycles or refinement steps" );
+   if ( !g.ctl.p )
+   {
+      g.ctl.alloc( 1 );
+      HYB_CUDA( cudaMallocHost( &g.hostCtl, sizeof( SolveCtl ) ) );
+   }
+   g.hostCtl->tol       = tol;
+   g.hostCtl->maxCycles = maxCycles;
+   HYB_CUDA( cudaMemcpyAsync( g.ctl.p, g.hostCtl, sizeof( SolveCtl ), cudaMemcpyHostToDevice, stream ) );
+   for ( auto& G : g.loops )
+      if ( G.x == &x && G.b == &b && G.level == l && G.kind == kind )
+      {
+         HYB_CUDA( cudaGraphLaunch( G.exec, stream ) );
+         return; // (its kernels are counted by the graph's step launches only approximately)
+      }
+   prepare( g );
+   if ( g.progTop >= g.minL )
+   {
+      const int top = std::min( l, g.progTop );
+      if ( kind == kCycle64Norm )
+         ensureProgram< double >( g, x, b, *g.tmp64, top );
+      else
+         ensureProgram< float >( g, *g.x32, *g.b32, *g.t32, top );
+   }
+   if ( !g.cap )
+      HYB_CUDA( cudaStreamCreateWithFlags( &g.cap, cudaStreamNonBlocking ) );
+   HYB_CUDA( cudaStreamSynchronize( stream ) ); // the capture stream must not overtake prior work
+   cudaGraph_t outer = nullptr;
+   HYB_CUDA( cudaGraphCreate( &outer, 0 ) );
+   try
+   {
+      cudaGraphConditionalHandle h;
+      HYB_CUDA( cudaGraphConditionalHandleCreate( &h, outer, 0, 0 ) );
+      SolveCtl*            c    = g.ctl.p;
+      const double*        sc   = g.scalars.p;
+      int                  one  = 1;
+      void*                ia[] = { &h, &c, &sc, &one };
+      cudaKernelNodeParams kp{};
+      kp.func         = reinterpret_cast< void* >( k_solve_ctl );
+      kp.gridDim      = dim3( 1 );
+      kp.blockDim     = dim3( 1 );
+      kp.kernelParams = ia;
+      cudaGraphNode_t init;
+      HYB_CUDA( cudaGraphAddKernelNode( &init, outer, nullptr, 0, &kp ) );
+      cudaGraphNodeParams cp{};
+      cp.type                = cudaGraphNodeTypeConditional;
+      cp.conditional.handle  = h;
+      cp.conditional.type    = cudaGraphCondTypeWhile;
+      cp.conditional.size    = 1;
+      cudaGraphNode_t whileNode;
+      HYB_CUDA( cudaGraphAddNode( &whileNode, outer, &init, 1, &cp ) );
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      const long long before = g_launches.load();
+      HYB_CUDA( cudaStreamBeginCaptureToGraph( g.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal ) );
+      try
+      {
+         enqueue( g, x, b, l, kind, g.cap );
+         k_solve_ctl<<< 1, 1, 0, g.cap >>>( h, c, sc, 0 );
+         HYB_CHECK_LAUNCH();
+      }
+      catch ( ... )
+      {
+         cudaGraph_t dummy = nullptr;
+         cudaStreamEndCapture( g.cap, &dummy );
+         throw;
+      }
+      HYB_CUDA( cudaStreamEndCapture( g.cap, &body ) );
+      const long long captured = g_launches.load() - before;
+      g_launches.fetch_sub( captured );
+      cudaGraphExec_t exec;
+      HYB_CUDA( cudaGraphInstantiate( &exec, outer, 0 ) );
+      HYB_CUDA( cudaGraphDestroy( outer ) );
+      outer = nullptr;
+      g.loops.push_back( { &x, &b, l, kind, exec, captured } );
+      HYB_CUDA( cudaGraphLaunch( exec, stream ) );
+   }
+   catch ( ... )
+   {
+      if ( outer )
+         cudaGraphDestroy( outer );
+      throw;
+   }
 }

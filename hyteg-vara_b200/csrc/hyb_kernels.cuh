@@ -1887,4 +1887,34 @@ __global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< d
    cgBody< VAR, BLEND >( tp, lv, op, x, b, r, p, ap, tol, maxIter, status, red, rp );
 }
 
+// ---------------------------------------------------------------------------
+// Device-side stopping test of an iterated solve (GeometricMultigridSolver's outer loop
+// without a host round trip per cycle): scalars[0] = ||b - A x||^2 of the current iterate,
+// scalars[1] = ||b||^2. With init the cycle count starts at 0 and ||b|| is taken; otherwise
+// one more cycle has run. The graph's WHILE condition stays set while the relative residual
+// is above the tolerance, finite, and the cycle budget is not spent.
+// ---------------------------------------------------------------------------
+struct SolveCtl
+{
+   double tol;
+   int    maxCycles;
+   int    cycles;
+   double nb;  // ||b|| (1 if b = 0)
+   double rel; // relative residual of the last iterate
+};
+
+__global__ void k_solve_ctl( cudaGraphConditionalHandle h, SolveCtl* c, const double* __restrict__ scalars, int init )
+{
+   if ( init )
+   {
+      c->cycles = 0;
+      c->nb     = scalars[1] > 0 ? sqrt( scalars[1] ) : 1.0;
+   }
+   else
+      c->cycles += 1;
+   const double rel = sqrt( scalars[0] ) / c->nb;
+   c->rel           = rel;
+   cudaGraphSetConditional( h, ( rel > c->tol && c->cycles < c->maxCycles ) ? 1u : 0u ); // NaN stops too
+}
+
 } // namespace hyb

@@ -3,10 +3,12 @@
 // No reference counterpart: the reference runs one GeometricMultigridSolver solve per MPI
 // job (GeometricMultigridSolver.hpp:136-235 driven by an app's main loop). Here one host
 // thread admits requests by device footprint, keeps their level hierarchies resident,
-// and steps every admitted solve as captured CUDA graphs on the solve's own stream, one
-// V-cycle (FP64) or one refinement step (mixed precision) per graph; between two steps
-// of any solve the loop admits newly arrived requests, so the GPU interleaves the kernels
-// of all solves in flight.
+// and runs every admitted solve on the solve's own stream as ONE captured CUDA graph: a
+// WHILE node around a V-cycle (FP64) or refinement step (mixed precision) and a device-side
+// stopping test (runSolveLoop), so a solve costs the host one launch and one event. Small
+// hierarchies run whole V-cycles in the one-block program kernel, so concurrent small
+// solves occupy one multiprocessor each. Whenever a solve finishes the loop admits newly
+// arrived requests, and the GPU interleaves the kernels of all solves in flight.
 //
 // Included at the end of hyb_capi.cu (same translation unit: it uses the engine's
 // internal types and launchers).
@@ -22,6 +24,9 @@ constexpr double kServeCorrLen = 0.2; // correlation length of its Gaussian rand
 constexpr double kServeSigma   = 1.0; // and its standard deviation
 constexpr int    kServePre = 3, kServePost = 3;
 constexpr double kServeCoarseTol     = 1e-12;
+// hierarchies whose finest level holds at most this many closure points (all cells) run
+// whole V-cycles in the program kernel
+constexpr long   kServeProgramPoints = 65536;
 constexpr int    kServeCoarseMaxIter = 10000;
 
 inline uint64_t splitmix64Host( uint64_t x )
@@ -140,6 +145,7 @@ struct Instance
    size_t                      bytes    = 0;
    uint64_t                    lastUse  = 0;
    int                         req      = -1; // request being served, -1 when idle
+   bool                        hostLoop = false; // the device-iterated solve graph is unavailable
 
    ~Instance()
    {
@@ -162,7 +168,8 @@ enum ServeState : int
    kStarting = 2, // right-hand side, coefficient and initial residual enqueued
    kStepping = 3, // cycles in flight
    kDraining = 4, // solution copy to the host in flight
-   kDone     = 5
+   kDone     = 5,
+   kLooping  = 6  // the device-iterated solve and its result copy in flight
 };
 
 struct ServeRequest
@@ -229,7 +236,7 @@ struct Server
 
    void evict( Instance* victim )
    {
-      graphsEvicted += int( victim->gmg ? victim->gmg->graphs.size() : 0 );
+      graphsEvicted += int( victim->gmg ? victim->gmg->graphs.size() + victim->gmg->loops.size() : 0 );
       const long long before = g_deviceBytes.load();
       for ( auto it = inst.begin(); it != inst.end(); ++it )
          if ( it->get() == victim )
@@ -258,6 +265,11 @@ struct Server
       in->gmg = std::make_unique< Gmg >();
       initGmg( *in->gmg, st, in->op, 0, k.level, kServePre, kServePost, 1.0, HYB_SMOOTHER_SOR, kServeCoarseTol,
                kServeCoarseMaxIter );
+      // a small hierarchy runs every level of its V-cycle in the one-block program kernel:
+      // its cost is launch latency, not bandwidth, and concurrent small solves then occupy
+      // one multiprocessor each
+      if ( long( st->td.nC ) * st->L( k.level ).dev.stride <= kServeProgramPoints )
+         in->gmg->progTop = k.level;
       if ( k.precision == 32 )
          ensureMixed( *in->gmg );
       prepare( *in->gmg );
@@ -313,7 +325,7 @@ struct Server
    {
       int n = graphsEvicted;
       for ( auto& in : inst )
-         n += int( in->gmg->graphs.size() );
+         n += int( in->gmg->graphs.size() + in->gmg->loops.size() );
       return n;
    }
 };
@@ -341,7 +353,10 @@ ServeKey keyOf( const hyb_request& d )
    return ServeKey{ d.nx, d.ny, shell ? 1 : d.nz, d.level, d.coefficient, d.precision, d.mesh };
 }
 
-// right-hand side, coefficient, x = 0, ||b||^2 and the initial residual norm
+bool serveHostLoop();
+
+// right-hand side, coefficient, x = 0, ||b||^2, the initial residual norm, and (unless the
+// hierarchy is stepped from the host) the whole solve
 void startRequest( Server& sv, ServeRequest& r, Instance& in )
 {
    const int    L = r.key.level;
@@ -368,13 +383,41 @@ void startRequest( Server& sv, ServeRequest& r, Instance& in )
    launchDot< double >( st, L, in.b->ptr< double >( L ), in.b->ptr< double >( L ), kGmgFlag, g.partial.p, g.scalars.p + 1,
                         s );
    runGraph( g, *in.x, *in.b, L, r.key.precision == 64 ? kNorm64 : kNormMixed, s );
+   if ( !in.hostLoop && !serveHostLoop() )
+   {
+      // the whole solve as one graph launch with the stopping test on the device
+      try
+      {
+         runSolveLoop( g, *in.x, *in.b, L, r.key.precision == 64 ? kCycle64Norm : kMixedStep, r.d.rel_tol,
+                       r.d.max_cycles, s );
+         HYB_CUDA( cudaMemcpyAsync( g.hostCtl, g.ctl.p, sizeof( SolveCtl ), cudaMemcpyDeviceToHost, s ) );
+         HYB_CUDA( cudaEventRecord( in.ev, s ) );
+         r.state = kLooping;
+         return;
+      }
+      catch ( const Error& )
+      {
+         // the device loop could not be captured here: step this hierarchy from the host
+         in.hostLoop = true;
+         HYB_CUDA( cudaGetLastError() );
+      }
+   }
    HYB_CUDA( cudaMemcpyAsync( g.hostScalar, g.scalars.p, 2 * sizeof( double ), cudaMemcpyDeviceToHost, s ) );
    HYB_CUDA( cudaEventRecord( in.ev, s ) );
    r.state = kStarting;
 }
 
-// The request's last enqueued work has finished: read the residual norm and enqueue the
-// next step, the solution copy, or finish. Returns true when the request is done.
+// HYB_SERVE_HOST_LOOP=1: step every solve from the host (one graph launch and one residual
+// read per cycle) instead of the device-iterated solve graph
+bool serveHostLoop()
+{
+   static const bool v = envLong( "HYB_SERVE_HOST_LOOP", 0 ) != 0;
+   return v;
+}
+
+// The request's last enqueued work has finished: take the device loop's result (or, stepped
+// from the host, read the residual norm and enqueue the next step), then the solution copy,
+// or finish. Returns true when the request is done.
 bool advanceRequest( ServeRequest& r, double now )
 {
    Instance& in = *r.inst;
@@ -386,24 +429,37 @@ bool advanceRequest( ServeRequest& r, double now )
       r.tDone = now;
       return true;
    }
-   if ( r.state == kStarting )
-   {
-      r.nb    = std::sqrt( g.hostScalar[1] ) > 0 ? std::sqrt( g.hostScalar[1] ) : 1.0;
-      r.state = kStepping;
-   }
-   r.rel     = std::sqrt( g.hostScalar[0] ) / r.nb;
    bool stop = false;
-   if ( !std::isfinite( r.rel ) )
+   if ( r.state == kLooping )
    {
-      r.status = HYB_ENOTCONVERGED;
-      stop     = true;
-   }
-   else if ( r.rel <= r.d.rel_tol )
+      r.nb     = g.hostCtl->nb;
+      r.rel    = g.hostCtl->rel;
+      r.cycles = g.hostCtl->cycles;
+      if ( !std::isfinite( r.rel ) || r.rel > r.d.rel_tol )
+         r.status = HYB_ENOTCONVERGED;
       stop = true;
-   else if ( r.cycles >= r.d.max_cycles )
+   }
+   else
    {
-      r.status = HYB_ENOTCONVERGED;
-      stop     = true;
+      // stepped from the host: one cycle per event
+      if ( r.state == kStarting )
+      {
+         r.nb    = std::sqrt( g.hostScalar[1] ) > 0 ? std::sqrt( g.hostScalar[1] ) : 1.0;
+         r.state = kStepping;
+      }
+      r.rel = std::sqrt( g.hostScalar[0] ) / r.nb;
+      if ( !std::isfinite( r.rel ) )
+      {
+         r.status = HYB_ENOTCONVERGED;
+         stop     = true;
+      }
+      else if ( r.rel <= r.d.rel_tol )
+         stop = true;
+      else if ( r.cycles >= r.d.max_cycles )
+      {
+         r.status = HYB_ENOTCONVERGED;
+         stop     = true;
+      }
    }
    if ( !stop )
    {

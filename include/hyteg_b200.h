@@ -263,10 +263,13 @@ int hyb_gmg_solve_to_tolerance( hyb_gmg* g, hyb_function* x, hyb_function* b, in
  * admits a request when an active slot and its device footprint (hyb_server_footprint)
  * fit the byte budget, keeps each admitted hierarchy resident (an idle hierarchy of the
  * same shape is reused; idle ones are evicted least recently used when memory is needed),
- * and runs every admitted solve on its own stream as captured CUDA graphs, one
- * V-cycle (FP64) or one refinement step (FP32 V-cycle in FP64 refinement) per graph, so
- * the solves in flight overlap on the GPU. New requests join between any two steps of
- * the others. Each solve is V(3,3) with multicolour SOR (omega 1) and a level-0 FP64 CG
+ * and runs every admitted solve on its own stream as one captured CUDA graph that
+ * iterates V-cycles (FP64) or refinement steps (FP32 V-cycle in FP64 refinement) with
+ * the stopping test on the device, so the solves in flight overlap on the GPU and the
+ * host touches a solve only at its start and end. Hierarchies of at most 65536 closure
+ * points on their finest level run whole V-cycles in one thread block. New requests
+ * join as slots and memory free up. HYB_SERVE_HOST_LOOP=1 steps the solves from the host
+ * instead (one graph launch and one residual read per cycle). Each solve is V(3,3) with multicolour SOR (omega 1) and a level-0 FP64 CG
  * coarse solve to 1e-12; f is hyb_function_fill_uniform_random( seed, lattice =
  * lcm(nx,ny,nz) 2^level ) and, for the lognormal coefficient, k is exp of the random
  * field of hyb_rff_features( seed, 0.2, 64 ) with sigma 1 (the radial coefficient: the same

@@ -28,6 +28,23 @@ def rel_diff(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
+def server_like_gmg(H, st, A, L):
+    """The public solver configured as the server configures a hierarchy: a hierarchy whose
+    finest level holds at most 65536 closure points runs whole V-cycles in the program kernel
+    (HYB_PROGRAM_MAX_POINTS, read when a solver is created)."""
+    import os
+
+    old = os.environ.get("HYB_PROGRAM_MAX_POINTS")
+    os.environ["HYB_PROGRAM_MAX_POINTS"] = "65536"
+    try:
+        return H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    finally:
+        if old is None:
+            del os.environ["HYB_PROGRAM_MAX_POINTS"]
+        else:
+            os.environ["HYB_PROGRAM_MAX_POINTS"] = old
+
+
 MIX = [  # (nx, ny, nz, level, coefficient, precision, seed)
     (2, 2, 2, 5, 1, 32, 3),  # the probe request
     (1, 1, 1, 6, 0, 32, 1),
@@ -75,7 +92,8 @@ def test_result_same_alone_and_in_mix(H):
 
 @pytest.mark.parametrize("coefficient", [0, 1])
 def test_server_matches_standalone_solver(H, coefficient):
-    """The same problem through the public solver API gives the same solution."""
+    """The same problem through the public solver API, configured as the server configures
+    the hierarchy, gives the same solution."""
     nx, L, seed = 2, 4, 9
     sv = H.Server(4 << 30, max_level=L)
     n = ndofs(H, nx, nx, nx, L)
@@ -92,7 +110,7 @@ def test_server_matches_standalone_solver(H, coefficient):
         A = H.P1ConstantLaplaceOperator(st, 0, L)
     x, b = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
     b.fill_uniform_random(L, seed, float(nx << L))
-    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    gmg = server_like_gmg(H, st, A, L)
     hist = gmg.solve_to_tolerance(x, b, L, 1e-8, max_cycles=100, precision=32)
     assert len(hist) - 1 == res.cycles
     assert abs(hist[-1] - res.rel_residual) <= 1e-12 * max(hist[-1], 1e-300) + 1e-18
@@ -165,7 +183,7 @@ def test_shell_request_matches_standalone_solver(H):
     A = H.P1ElementwiseDivKGradOperator.random_features(st, 0, L, w, ph, 0.5, radial=5.0)
     x, b = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
     b.fill_uniform_random(L, seed, float(1 << 20))
-    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    gmg = server_like_gmg(H, st, A, L)
     hist = gmg.solve_to_tolerance(x, b, L, 1e-8, max_cycles=100, precision=32)
     assert len(hist) - 1 == res.cycles
     assert rel_diff(sv.solution(rid), x.get(L)) <= TOL
