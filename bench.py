@@ -722,6 +722,10 @@ def single_op(args):
             b.set(f.astype("float32"), lv)
             u.set((0.1 * f).astype("float32"), lv)
     F = H.INNER | H.NEUMANN
+    # a solver's first cycle builds the levels' row tables, as in every solve
+    x64, b64 = H.P1Function("x64", st, 0, L), H.P1Function("b64", st, 0, L)
+    H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0).solve(x64, b64, L)
+    del x64, b64
     P, R = H.P1toP1LinearProlongation(), H.P1toP1LinearRestriction()
     ops = {"apply": lambda: A.apply(b, y, L, F), "residual": lambda: A.residual(u, b, y, L, F),
            "sor": lambda: A.smooth_sor(u, b, 1.0, L, F), "sor32": lambda: A.smooth_sor(u, b, 1.0, L, F),
