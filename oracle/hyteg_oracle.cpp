@@ -791,8 +791,11 @@ inline void sorUpdate( T& x, T b, T diag, T off, T relax )
 // of the last three, so a stage reads its own closure current and everything else from
 // the state at the start of that stage; inside each primitive the lexicographic order is
 // reversed (sor_3D_macrocell_P1_backwards.cpp:52-57, sor_3D_macroface_P1_backwards.cpp).
+// stages: bit 0 vertices, 1 edges, 2 faces, 3 cells (15 = the whole sweep; a single stage
+// isolates one primitive type's sweep for comparison with that type's generated kernel).
 template < typename T >
-void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag, bool backwards )
+void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, T relax, int flag, bool backwards,
+              int stages = 15 )
 {
    const i64 N = lv.N;
    std::vector< T > xs( x, x + lv.nDof );
@@ -890,20 +893,28 @@ void sorRefT( const Oracle& o, const Op& op, const Level& lv, T* x, const T* b, 
    };
    if ( !backwards )
    {
-      vertices();
-      edges();
-      faces();
-      cells();
+      if ( stages & 1 )
+         vertices();
+      if ( stages & 2 )
+         edges();
+      if ( stages & 4 )
+         faces();
+      if ( stages & 8 )
+         cells();
    }
    else
    {
-      cells();
+      if ( stages & 8 )
+         cells();
       refresh();
-      faces();
+      if ( stages & 4 )
+         faces();
       refresh();
-      edges();
+      if ( stages & 2 )
+         edges();
       refresh();
-      vertices();
+      if ( stages & 1 )
+         vertices();
    }
 }
 
@@ -1727,6 +1738,13 @@ void orc_sor_ref( void* h, int op, int level, double* x, const double* b, double
 {
    auto* o = H( h );
    sorRefT( *o, o->ops[op], o->lv[level], x, b, relax, flag, backwards != 0 );
+}
+
+void orc_sor_ref_stages( void* h, int op, int level, double* x, const double* b, double relax, int flag, int backwards,
+                         int stages )
+{
+   auto* o = H( h );
+   sorRefT( *o, o->ops[op], o->lv[level], x, b, relax, flag, backwards != 0, stages );
 }
 
 void orc_sor_colored( void* h, int op, int level, double* x, const double* b, double relax, int flag, const int* labels,

@@ -69,6 +69,10 @@ void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* o
 void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );
 // backwards != 0: smooth_sor_backwards (P1Operator.hpp:424-431)
 void   orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag, int backwards );
+// One or more stages of that sweep: bit 0 macro-vertices, 1 macro-edges, 2 macro-faces,
+// 3 macro-cells (15 = orc_sor_ref).
+void   orc_sor_ref_stages( void* h, int op, int level, double* x, const double* b, double relax, int flag,
+                           int backwards, int stages );
 void   orc_sor_colored( void* h, int op, int level, double* x, const double* b, double relax, int flag,
                         const int* labels, int m, int backwards );
 void   orc_jacobi( void* h, int op, int level, double* x, const double* b, double relax, int flag );

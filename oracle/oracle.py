@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libhyteg_refkernels.so")
+REF_FACE_LIB = os.path.join(HERE, "_ref", "libhyteg_refface.so")
 
 INNER, DIRICHLET, NEUMANN, FREESLIP, ALL = 1, 2, 4, 8, 15
 
@@ -35,7 +36,8 @@ def build(ref=False):
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     root = reference_root()
     if ref and root:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF_ROOT=" + root], check=True)
+        jobs = str(max(1, min(8, os.cpu_count() or 1)))
+        subprocess.run(["make", "-s", "-j", jobs, "-C", HERE, "ref", "REF_ROOT=" + root], check=True)
 
 
 def lib():
@@ -62,6 +64,7 @@ def lib():
         L.orc_cell_stencil.argtypes = [P, I, I, I, I, P]
         L.orc_apply.argtypes = [P, I, I, P, P, I, I]
         L.orc_sor_ref.argtypes = [P, I, I, P, P, D, I, I]
+        L.orc_sor_ref_stages.argtypes = [P, I, I, P, P, D, I, I, I]
         L.orc_sor_colored.argtypes = [P, I, I, P, P, D, I, P, I, I]
         L.orc_jacobi.argtypes = [P, I, I, P, P, D, I]
         L.orc_prolongate.argtypes = [P, I, P, P, I, I]
@@ -187,9 +190,11 @@ class Oracle:
         lib().orc_apply(self.h, op, level, _p(src), _p(dst), flag, int(add))
         return dst
 
-    def sor_ref(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0, backwards=False):
-        lib().orc_sor_ref(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), relax, flag,
-                          int(backwards))
+    def sor_ref(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0, backwards=False, stages=15):
+        """smooth_sor / smooth_sor_backwards; `stages` selects the primitive sweeps to run
+        (bit 0 vertices, 1 edges, 2 faces, 3 cells)."""
+        lib().orc_sor_ref_stages(self.h, op, level, _p(x), _p(np.ascontiguousarray(b, np.float64)), relax, flag,
+                                 int(backwards), int(stages))
         return x
 
     def sor_colored(self, x, b, level, labels, m, relax=1.0, flag=INNER | NEUMANN, op=0, backwards=False):
@@ -289,6 +294,25 @@ def ref_lib():
         R.ref_p1_tet_diffusion.argtypes = [P, P]
         _ref = R
     return _ref
+
+
+_ref_face = None
+
+
+def ref_face_lib():
+    """The reference's generated macro-face kernels (oracle/ref_face_abi.cpp), or None."""
+    global _ref_face
+    if _ref_face is None:
+        if not os.path.exists(REF_FACE_LIB):
+            return None
+        R = ctypes.CDLL(REF_FACE_LIB)
+        P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        R.ref_face_apply.argtypes = [P, P, P, I, P, P, I]
+        R.ref_face_sor.argtypes = [P, P, P, P, I, P, P, D, P, P, I]
+        R.ref_cell_to_face.argtypes = [P, P, I, P]
+        R.ref_face_to_cell.argtypes = [P, P, I, P]
+        _ref_face = R
+    return _ref_face
 
 
 # ---------------------------------------------------------------------------
