@@ -34,6 +34,9 @@ struct Gmg
       DevBuf< Phase > phases;
    };
    std::vector< std::unique_ptr< Program > > programs;
+   // whole-solve programs for k_solve_batch (ensureSolveProgram), keyed by (x, b, level =
+   // top, step kind in dtype)
+   std::vector< std::unique_ptr< Program > > solvePrograms;
    cudaStream_t                cap = nullptr; // capture stream
    // captured graphs keyed by (x, b, level, kind)
    struct G
@@ -245,6 +248,54 @@ struct PhaseList
       P.relax  = g.coarseTol;
       P.a0     = g.coarseMaxIter;
       P.rp     = rowPassAll( rows( l ) );
+   }
+
+   // phases of a whole solve (k_solve_batch)
+   void residual64( int l, double* x, double* r, const double* b )
+   {
+      const auto& L  = g.st->L( l );
+      const int   nc = L.dev.nPts > 0 ? L.ptsBlocks : 0;
+      Phase&      P  = add( kPhResidual, l, nc + ( L.dev.nBdry > 0 ? L.bdryBlocks : 0 ), nc );
+      P.p0           = x;
+      P.p1           = r;
+      P.p2           = const_cast< double* >( b );
+      P.flag         = kGmgFlag;
+      if ( const RowTables* R = rows( l ) )
+      {
+         P.rp         = rowPassAll( R );
+         P.blocks     = 1;
+         P.cellBlocks = 0;
+      }
+   }
+   void dot( int l, const double* a, const double* b, float* cvt, int slot )
+   {
+      Phase& P = add( kPhDot, l, 1, 0 );
+      P.p0     = const_cast< double* >( a );
+      P.p1     = const_cast< double* >( b );
+      P.p2     = cvt;
+      P.flag   = kGmgFlag;
+      P.a0     = slot;
+   }
+   void zero32( int l, float* p )
+   {
+      Phase& P = add( kPhZero, l, flatBlocks( slabElems( l ) ), 0 );
+      P.p0     = p;
+      P.n      = slabElems( l );
+      P.dtype  = HYB_F32;
+   }
+   void addCorr( int l, double* x, const float* e )
+   {
+      Phase& P = add( kPhAddCorr, l, 1, 0 );
+      P.p0     = x;
+      P.p1     = const_cast< float* >( e );
+      P.flag   = kGmgFlag;
+   }
+   void ctl( SolveCtl* c, int loopStart, int init )
+   {
+      Phase& P = add( kPhCtl, 0, 1, 0 );
+      P.p0     = c;
+      P.a0     = loopStart;
+      P.a1     = init;
    }
 
    void coarse( double* x, const double* b ) { cg( g.minL, x, b ); }
@@ -669,5 +720,103 @@ void runSolveLoop( Gmg& g, Function& x, Function& b, int l, int kind, double tol
       if ( outer )
          cudaGraphDestroy( outer );
       throw;
+   }
+}
+
+// Record (once, outside any stream capture) the whole solve of (x, b) at level l as one
+// program for k_solve_batch: ||b||^2, the start residual and its norm (with the FP32
+// right-hand side for mixed precision), the stopping test, then the loop of V-cycles
+// (kCycle64Norm) or refinement steps (kMixedStep: x32 = 0, FP32 V-cycle, x += x32), each
+// followed by the residual norm and the test, which jumps back to the loop's start while
+// ||r|| / ||b|| > tol and fewer than maxCycles steps ran. The phases mirror enqueue() and
+// runSolveLoop() operation for operation; the whole V-cycle must fit the program kernel
+// (l <= progTop). Returns the program, whose tolerance and cycle limit sit in g.ctl.
+const Gmg::Program* ensureSolveProgram( Gmg& g, Function& x, Function& b, int l, int kind )
+{
+   require( kind == kCycle64Norm || kind == kMixedStep, "a solve program iterates V-cycles or refinement steps" );
+   for ( auto& p : g.solvePrograms )
+      if ( p->x == &x && p->b == &b && p->dtype == kind && p->top == l )
+         return p.get();
+   require( g.progTop >= l && l > g.minL, "a batched solve needs its whole V-cycle in the program kernel" );
+   prepare( g );
+   if ( !g.ctl.p )
+   {
+      g.ctl.alloc( 1 );
+      HYB_CUDA( cudaMallocHost( &g.hostCtl, sizeof( SolveCtl ) ) );
+   }
+   const bool mixed = kind == kMixedStep;
+   if ( mixed )
+      ensureMixed( g );
+   Function& r   = mixed ? *g.r64 : *g.tmp64;
+   float*    cvt = mixed ? g.b32->ptr< float >( l ) : nullptr;
+   PhaseList pl{ g, {} };
+   pl.dot( l, b.ptr< double >( l ), b.ptr< double >( l ), nullptr, 1 );
+   pl.residual64( l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ) );
+   pl.dot( l, r.ptr< double >( l ), r.ptr< double >( l ), cvt, 0 );
+   const size_t init = pl.ph.size();
+   pl.ctl( g.ctl.p, 0, 1 );
+   const int loopStart = int( pl.ph.size() );
+   if ( mixed )
+   {
+      pl.zero32( l, g.x32->ptr< float >( l ) );
+      const size_t c0 = pl.ph.size();
+      pl.vcycle< float >( *g.x32, *g.b32, *g.t32, l );
+      for ( size_t i = c0; i < pl.ph.size(); ++i )
+         pl.ph[i].dtype = HYB_F32;
+      pl.addCorr( l, x.ptr< double >( l ), g.x32->ptr< float >( l ) );
+   }
+   else
+      pl.vcycle< double >( x, b, *g.tmp64, l );
+   pl.residual64( l, x.ptr< double >( l ), r.ptr< double >( l ), b.ptr< double >( l ) );
+   pl.dot( l, r.ptr< double >( l ), r.ptr< double >( l ), cvt, 0 );
+   pl.ctl( g.ctl.p, loopStart, 0 );
+   pl.ph[init].a0 = loopStart;
+   auto prog   = std::make_unique< Gmg::Program >();
+   prog->x     = &x;
+   prog->b     = &b;
+   prog->dtype = kind;
+   prog->top   = l;
+   prog->n     = int( pl.ph.size() );
+   prog->phases.upload( pl.ph );
+   g.solvePrograms.push_back( std::move( prog ) );
+   return g.solvePrograms.back().get();
+}
+
+// Up to kSolveBatchMax solves in one launch of k_solve_batch (one block each); every job's
+// SolveCtl must hold its tolerance and cycle limit in stream order before the launch.
+constexpr int kSolveBatchMax = 64;
+struct SolveBatch
+{
+   SolveJob job[kSolveBatchMax];
+};
+
+template < bool VAR >
+__global__ void __launch_bounds__( kProgramThreads ) k_solve_batch( const __grid_constant__ SolveBatch batch )
+{
+   // the job table travels in the launch's parameters, so no buffer outlives the launch
+   solveBatchBody< VAR >( batch.job );
+}
+
+// The job of one recorded solve program (ensureSolveProgram) of g.
+SolveJob solveJob( const Gmg& g, const Gmg::Program& p )
+{
+   return SolveJob{ g.st->td, (const LevelDev*) g.st->lvTable.p, p.phases.p, int( g.st->lvTable.n ), p.n };
+}
+
+// Every job in launches of at most kSolveBatchMax blocks; var selects the operator kind
+// (every job of the call must have that kind).
+void launchSolveBatch( const std::vector< SolveJob >& jobs, bool var, cudaStream_t stream )
+{
+   for ( size_t i0 = 0; i0 < jobs.size(); i0 += kSolveBatchMax )
+   {
+      const int  n = int( std::min< size_t >( kSolveBatchMax, jobs.size() - i0 ) );
+      SolveBatch B{};
+      for ( int i = 0; i < n; ++i )
+         B.job[i] = jobs[i0 + size_t( i )];
+      if ( var )
+         k_solve_batch< true ><<< n, kProgramThreads, 0, stream >>>( B );
+      else
+         k_solve_batch< false ><<< n, kProgramThreads, 0, stream >>>( B );
+      HYB_CHECK_LAUNCH();
    }
 }

@@ -6,8 +6,10 @@
 // and runs every admitted solve on the solve's own stream as ONE captured CUDA graph: a
 // WHILE node around a V-cycle (FP64) or refinement step (mixed precision) and a device-side
 // stopping test (runSolveLoop), so a solve costs the host one launch and one event. Small
-// hierarchies run whole V-cycles in the one-block program kernel, so concurrent small
-// solves occupy one multiprocessor each. Whenever a solve finishes the loop admits newly
+// hierarchies (whole V-cycles in the one-block program kernel) are batched instead: the
+// small requests admitted in one round of the loop run in ONE launch of k_solve_batch, a
+// thread block per solve carrying it from its start residual to its tolerance, so a batch
+// of small solves costs one launch in all. Whenever a solve finishes the loop admits newly
 // arrived requests, and the GPU interleaves the kernels of all solves in flight.
 //
 // Included at the end of hyb_capi.cu (same translation unit: it uses the engine's
@@ -146,6 +148,8 @@ struct Instance
    uint64_t                    lastUse  = 0;
    int                         req      = -1; // request being served, -1 when idle
    bool                        hostLoop = false; // the device-iterated solve graph is unavailable
+   bool                        batch    = false; // solved in k_solve_batch with the small solves admitted beside it
+   const Gmg::Program*         solveProg = nullptr; // its whole-solve program (batch)
 
    ~Instance()
    {
@@ -187,12 +191,40 @@ struct ServeRequest
    Instance*   inst      = nullptr;
 };
 
+bool serveBatch();
+bool serveHostLoop();
+
 struct Server
 {
    size_t                                    budget    = 0;
    int                                       maxActive = 1, maxLevel = 0;
    size_t                                    used = 0, peak = 0;
    int                                       built = 0, graphsEvicted = 0;
+   int                                       batches = 0, batchedSolves = 0; // k_solve_batch launches, solves in them
+   std::vector< cudaStream_t >               batchStreams; // batches of small solves, round robin
+   int                                       batchNext = 0;
+
+   ~Server()
+   {
+      for ( cudaStream_t b : batchStreams )
+      {
+         cudaStreamSynchronize( b );
+         cudaStreamDestroy( b );
+      }
+   }
+
+   cudaStream_t nextBatchStream()
+   {
+      constexpr int kBatchStreams = 8;
+      if ( batchStreams.empty() )
+         for ( int i = 0; i < kBatchStreams; ++i )
+         {
+            cudaStream_t b;
+            HYB_CUDA( cudaStreamCreateWithFlags( &b, cudaStreamNonBlocking ) );
+            batchStreams.push_back( b );
+         }
+      return batchStreams[size_t( batchNext++ % kBatchStreams )];
+   }
    uint64_t                                  tick  = 0;
    std::vector< std::unique_ptr< MeshEntry > > meshes;
    std::vector< std::unique_ptr< Instance > >  inst;
@@ -285,6 +317,13 @@ struct Server
          else
             ensureProgram< double >( g, *in->x, *in->b, *g.tmp64, top );
       }
+      // a hierarchy whose whole V-cycle runs in the program kernel is solved by k_solve_batch
+      // together with the other small solves admitted at the same time
+      if ( g.progTop >= k.level && serveBatch() && !serveHostLoop() )
+      {
+         in->solveProg = ensureSolveProgram( g, *in->x, *in->b, k.level, k.precision == 64 ? kCycle64Norm : kMixedStep );
+         in->batch     = true;
+      }
       in->feat.alloc( 4 * kServeModes );
       HYB_CUDA( cudaMallocHost( &in->featHost, 4 * kServeModes * sizeof( double ) ) );
       HYB_CUDA( cudaStreamCreateWithFlags( &in->stream, cudaStreamNonBlocking ) );
@@ -355,17 +394,15 @@ ServeKey keyOf( const hyb_request& d )
 
 bool serveHostLoop();
 
-// right-hand side, coefficient, x = 0, ||b||^2, the initial residual norm, and (unless the
-// hierarchy is stepped from the host) the whole solve
-void startRequest( Server& sv, ServeRequest& r, Instance& in )
+// the request's right-hand side, coefficient and x = 0, on stream s
+void setupRequest( Server& sv, ServeRequest& r, Instance& in, cudaStream_t s )
 {
-   const int    L = r.key.level;
-   cudaStream_t s = in.stream;
-   Storage&     st = *in.mesh->st;
-   in.req          = int( &r - sv.reqs.data() );
-   in.lastUse      = ++sv.tick;
-   r.inst          = &in;
-   r.served        = in.bytes;
+   const int L = r.key.level;
+   Storage&  st = *in.mesh->st;
+   in.req       = int( &r - sv.reqs.data() );
+   in.lastUse   = ++sv.tick;
+   r.inst       = &in;
+   r.served     = in.bytes;
    if ( r.key.coeff != HYB_COEFF_CONSTANT )
    {
       const bool radial = r.key.coeff == HYB_COEFF_RADIAL;
@@ -379,6 +416,16 @@ void startRequest( Server& sv, ServeRequest& r, Instance& in )
        st.td, Lh.dev, st.cellCoords.p, st.cellOrder.p, in.b->ptr< double >( L ), r.d.seed, serveLattice( r.key ) );
    HYB_CHECK_LAUNCH();
    HYB_CUDA( cudaMemsetAsync( in.x->ptr< double >( L ), 0, in.x->levelBytes( L ), s ) );
+}
+
+// set-up, ||b||^2, the initial residual norm, and (unless the hierarchy is stepped from the
+// host) the whole solve as one device-iterated graph
+void startRequest( Server& sv, ServeRequest& r, Instance& in )
+{
+   const int    L = r.key.level;
+   cudaStream_t s = in.stream;
+   Storage&     st = *in.mesh->st;
+   setupRequest( sv, r, in, s );
    Gmg& g = *in.gmg;
    launchDot< double >( st, L, in.b->ptr< double >( L ), in.b->ptr< double >( L ), kGmgFlag, g.partial.p, g.scalars.p + 1,
                         s );
@@ -405,6 +452,49 @@ void startRequest( Server& sv, ServeRequest& r, Instance& in )
    HYB_CUDA( cudaMemcpyAsync( g.hostScalar, g.scalars.p, 2 * sizeof( double ), cudaMemcpyDeviceToHost, s ) );
    HYB_CUDA( cudaEventRecord( in.ev, s ) );
    r.state = kStarting;
+}
+
+// Start the small solves admitted together: their set-up and ONE k_solve_batch launch (per
+// operator kind) on a stream of the batch pool, which runs each solve to its tolerance in
+// its own thread block; then every solve's stopping-test state back to the host.
+void startBatch( Server& sv, const std::vector< int >& ids )
+{
+   cudaStream_t            s = sv.nextBatchStream();
+   std::vector< SolveJob > jobs[2];
+   for ( int id : ids )
+   {
+      ServeRequest& r  = sv.reqs[size_t( id )];
+      Instance&     in = *r.inst;
+      setupRequest( sv, r, in, s );
+      Gmg& g               = *in.gmg;
+      g.hostCtl->tol       = r.d.rel_tol;
+      g.hostCtl->maxCycles = r.d.max_cycles;
+      HYB_CUDA( cudaMemcpyAsync( g.ctl.p, g.hostCtl, sizeof( SolveCtl ), cudaMemcpyHostToDevice, s ) );
+      jobs[in.op->variable ? 1 : 0].push_back( solveJob( g, *in.solveProg ) );
+   }
+   for ( int v = 0; v < 2; ++v )
+      if ( !jobs[v].empty() )
+      {
+         launchSolveBatch( jobs[v], v == 1, s );
+         sv.batches += int( ( jobs[v].size() + kSolveBatchMax - 1 ) / kSolveBatchMax );
+      }
+   for ( int id : ids )
+   {
+      ServeRequest& r  = sv.reqs[size_t( id )];
+      Instance&     in = *r.inst;
+      HYB_CUDA( cudaMemcpyAsync( in.gmg->hostCtl, in.gmg->ctl.p, sizeof( SolveCtl ), cudaMemcpyDeviceToHost, s ) );
+      HYB_CUDA( cudaEventRecord( in.ev, s ) );
+      r.state = kLooping;
+   }
+   sv.batchedSolves += int( ids.size() );
+}
+
+// HYB_SERVE_BATCH=0: solve small hierarchies one device-iterated graph each instead of in
+// k_solve_batch
+bool serveBatch()
+{
+   static const bool v = envLong( "HYB_SERVE_BATCH", 1 ) != 0;
+   return v;
 }
 
 // HYB_SERVE_HOST_LOOP=1: step every solve from the host (one graph launch and one residual
@@ -516,7 +606,9 @@ void runServer( Server& sv, double timeLimit )
          sv.reqs[order[next]].state = kQueued;
          queue.push_back( order[next++] );
       }
-      // admission in arrival order, as slots and memory allow
+      // admission in arrival order, as slots and memory allow; small solves admitted in
+      // the same round start as one batch
+      std::vector< int > batch;
       while ( !queue.empty() && int( running.size() ) < sv.maxActive )
       {
          ServeRequest& r  = sv.reqs[queue.front()];
@@ -534,9 +626,19 @@ void runServer( Server& sv, double timeLimit )
          }
          queue.pop_front();
          r.tAdmit = elapsed();
-         startRequest( sv, r, *in );
-         running.push_back( int( &r - sv.reqs.data() ) );
+         const int id = int( &r - sv.reqs.data() );
+         if ( in->batch )
+         {
+            r.inst = in;
+            in->req = id; // taken: a later request of the round must not acquire it
+            batch.push_back( id );
+         }
+         else
+            startRequest( sv, r, *in );
+         running.push_back( id );
       }
+      if ( !batch.empty() )
+         startBatch( sv, batch );
       bool progressed = false;
       for ( size_t i = 0; i < running.size(); )
       {
@@ -690,6 +792,17 @@ int hyb_server_stats( const hyb_server* s, size_t* peak, int* built, int* graphs
       *built = s->built;
    if ( graphs )
       *graphs = s->graphsCaptured();
+   HYB_API_END
+}
+
+int hyb_server_batch_stats( const hyb_server* s, int* batches, int* batched_solves )
+{
+   HYB_API_BEGIN
+   require( s, "null argument" );
+   if ( batches )
+      *batches = s->batches;
+   if ( batched_solves )
+      *batched_solves = s->batchedSolves;
    HYB_API_END
 }
 

@@ -33,7 +33,7 @@ SYMBOLS = [
     "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
     "hyb_operator_create_divkgrad_rff", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
-    "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_rff_features",
+    "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_server_batch_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
     "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
     "hyb_chebyshev_coefficients", "hyb_operator_estimate_spectral_radius", "hyb_server_mesh_bytes",
@@ -131,6 +131,7 @@ def load(path=LIB_PATH):
         "hyb_server_run": (I, [P, D]),
         "hyb_server_result": (I, [P, I, ctypes.POINTER(RequestResult)]),
         "hyb_server_stats": (I, [P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "hyb_server_batch_stats": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "hyb_rff_features": (I, [ctypes.c_uint64, D, I, P, P]),
     }
     for name, (res, args) in sig.items():
@@ -559,5 +560,7 @@ class Server:
         _check(load().hyb_server_stats(self.h, ctypes.byref(peak), ctypes.byref(built), ctypes.byref(graphs)))
         mesh = ctypes.c_size_t()
         _check(load().hyb_server_mesh_bytes(self.h, ctypes.byref(mesh)))
+        batches, batched = ctypes.c_int(), ctypes.c_int()
+        _check(load().hyb_server_batch_stats(self.h, ctypes.byref(batches), ctypes.byref(batched)))
         return {"peak_bytes": peak.value, "hierarchies_built": built.value, "graphs_captured": graphs.value,
-                "mesh_bytes": mesh.value}
+                "mesh_bytes": mesh.value, "batches": batches.value, "batched_solves": batched.value}

@@ -331,6 +331,14 @@ int hyb_server_run( hyb_server* s, double time_limit_s );
 int hyb_server_result( const hyb_server* s, int id, hyb_request_result* out );
 /* peak device bytes held by the server, hierarchies built, graphs captured */
 int hyb_server_stats( const hyb_server* s, size_t* peak_bytes, int* hierarchies_built, int* graphs_captured );
+/* Launches of the batched whole-solve kernel and the solves they carried. Hierarchies whose
+ * whole V-cycle fits the one-block program kernel (at most 65536 closure points on the
+ * finest level) are solved together: the small requests admitted in one round of the loop
+ * go into ONE kernel launch, a thread block per solve, which runs each solve from its
+ * start residual to its tolerance on the device (HYB_SERVE_BATCH=0 solves them one
+ * device-iterated graph each instead). No reference counterpart (the reference runs one
+ * solve per job). */
+int hyb_server_batch_stats( const hyb_server* s, int* batches, int* batched_solves );
 /* device bytes of the meshes the server holds (storage, Laplace operator, row tables),
  * which are never evicted and are not part of a request's footprint */
 int hyb_server_mesh_bytes( const hyb_server* s, size_t* bytes );

@@ -90,6 +90,45 @@ def test_result_same_alone_and_in_mix(H):
     assert st["peak_bytes"] <= 8 << 30
 
 
+SMALL = [  # (nx, ny, nz, level, coefficient, precision, seed): whole V-cycles in the program kernel
+    (1, 1, 1, 3, 0, 64, 11),
+    (1, 1, 1, 4, 1, 64, 12),
+    (1, 1, 1, 5, 0, 32, 13),
+    (2, 2, 2, 4, 1, 32, 14),
+    (2, 1, 1, 4, 0, 64, 15),
+    (1, 2, 1, 3, 1, 32, 16),
+]
+
+
+def test_small_solves_batched_in_one_launch(H):
+    """Small requests admitted together run as ONE batched whole-solve launch per operator
+    kind (a thread block per solve, every cycle and stopping test on the device); each
+    result equals the public solver's on the same problem: same cycle count, residual and
+    solution within the tolerance of the other serving tests."""
+    sv = H.Server(8 << 30, max_active=16, max_level=5)
+    ids = [sv.submit(H.Server.request(*q), keep_solution=True, num_dofs=ndofs(H, *q[:4])) for q in SMALL]
+    sv.run(300)
+    st = sv.stats()
+    assert st["batched_solves"] == len(SMALL)
+    assert st["batches"] == 2  # constant and lognormal coefficients: one launch each
+    for rid, (nx, ny, nz, L, coefficient, precision, seed) in zip(ids, SMALL):
+        res = sv.result(rid)
+        assert res.status == 0 and res.rel_residual <= 1e-8, (nx, ny, nz, L, res.status, res.rel_residual)
+        storage = H.PrimitiveStorage.cuboid(nx, ny, nz, L)
+        if coefficient:
+            w, ph = H.rff_features(seed, 0.2, 64)
+            A = H.P1ElementwiseDivKGradOperator.random_features(storage, 0, L, w, ph, 1.0)
+        else:
+            A = H.P1ConstantLaplaceOperator(storage, 0, L)
+        x, b = H.P1Function("x", storage, 0, L), H.P1Function("b", storage, 0, L)
+        b.fill_uniform_random(L, seed, float(np.lcm.reduce([nx, ny, nz]) << L))
+        gmg = server_like_gmg(H, storage, A, L)
+        hist = gmg.solve_to_tolerance(x, b, L, 1e-8, max_cycles=100, precision=precision)
+        assert len(hist) - 1 == res.cycles, (nx, ny, nz, L)
+        assert abs(hist[-1] - res.rel_residual) <= 1e-12 * max(hist[-1], 1e-300) + 1e-18
+        assert rel_diff(sv.solution(rid), x.get(L)) <= TOL, (nx, ny, nz, L)
+
+
 @pytest.mark.parametrize("coefficient", [0, 1])
 def test_server_matches_standalone_solver(H, coefficient):
     """The same problem through the public solver API, configured as the server configures
