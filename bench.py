@@ -587,7 +587,8 @@ def serving(args, H):
             "max_rel_residual": max(r.rel_residual for r in ok),
             "slots": args.serve_slots, "budget_gb": args.serve_budget_gb, "warmup_s": warm_s,
             "peak_gb": stats["peak_bytes"] / 2 ** 30, "hierarchies_built": stats["hierarchies_built"],
-            "graphs_captured": stats["graphs_captured"], "clocks": clk.summary(),
+            "graphs_captured": stats["graphs_captured"], "batched_solves": stats["batched_solves"],
+            "batch_launches": stats["batches"], "clocks": clk.summary(),
             "workload": "Poisson arrivals; c x c x c cubes c~U{1..4}, level~U{3..7}, k constant or lognormal "
                         "(exp of GRF, corr. 0.2, sigma 1), seeded f, mixed V(3,3) to 1e-8; latency = arrival "
                         "to result on the host"}
