@@ -743,6 +743,41 @@ int hyb_gmg_destroy( hyb_gmg* g )
    HYB_API_END
 }
 
+int hyb_gmg_set_timing( hyb_gmg* gh, int enable )
+{
+   HYB_API_BEGIN
+   Gmg* g = static_cast< Gmg* >( static_cast< hyb_gmg_s* >( gh ) );
+   require( g != nullptr, "null argument" );
+   g->timing = enable != 0;
+   HYB_API_END
+}
+
+int hyb_gmg_timing_reset( hyb_gmg* gh )
+{
+   HYB_API_BEGIN
+   Gmg* g = static_cast< Gmg* >( static_cast< hyb_gmg_s* >( gh ) );
+   require( g != nullptr, "null argument" );
+   g->tt.reset();
+   HYB_API_END
+}
+
+int hyb_gmg_timing_json( hyb_gmg* gh, char* buf, size_t capacity, size_t* length )
+{
+   HYB_API_BEGIN
+   Gmg* g = static_cast< Gmg* >( static_cast< hyb_gmg_s* >( gh ) );
+   require( g != nullptr && length != nullptr, "null argument" );
+   g->tt.collect();
+   std::string out;
+   TimingTree::json( g->tt.root, out );
+   *length = out.size();
+   if ( buf )
+   {
+      require( capacity > out.size(), "buffer too small for the timing tree (length holds the size needed)" );
+      std::memcpy( buf, out.c_str(), out.size() + 1 );
+   }
+   HYB_API_END
+}
+
 int hyb_gmg_set_cycle_type( hyb_gmg* gh, int cycleType )
 {
    HYB_API_BEGIN

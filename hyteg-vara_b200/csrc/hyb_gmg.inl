@@ -2,6 +2,142 @@
 // (part of the single translation unit hyb_capi.cu, included inside namespace hyb)
 
 // ---------------------------------------------------------------------------
+// Timing tree: the nested stage timers of the reference's solver (waLBerla WcTimingTree
+// owned by the PrimitiveStorage; start/stop in GeometricMultigridSolver.hpp:129-233) with
+// the same node names and nesting, measured on the device: start and stop record CUDA
+// events on the solve's stream, and collect() waits for the last one and adds each pair's
+// elapsed time to its node.
+// ---------------------------------------------------------------------------
+struct TimingNode
+{
+   std::string                                name;
+   TimingNode*                                parent = nullptr;
+   std::vector< std::unique_ptr< TimingNode > > kids;
+   double                                     total = 0, minT = 0, maxT = 0; // seconds
+   long                                       count = 0;
+};
+
+struct TimingTree
+{
+   TimingNode root;
+   TimingNode* cur = &root;
+   struct Open
+   {
+      TimingNode* node;
+      cudaEvent_t start;
+   };
+   struct Pending
+   {
+      TimingNode* node;
+      cudaEvent_t start, stop;
+   };
+   std::vector< Open >        open;
+   std::vector< Pending >     pending;
+   std::vector< cudaEvent_t > pool;
+
+   TimingTree() = default;
+   TimingTree( const TimingTree& ) = delete;
+   TimingTree& operator=( const TimingTree& ) = delete;
+   ~TimingTree()
+   {
+      for ( auto& p : pending )
+      {
+         cudaEventSynchronize( p.stop );
+         pool.push_back( p.start );
+         pool.push_back( p.stop );
+      }
+      for ( auto& o : open )
+         pool.push_back( o.start );
+      for ( cudaEvent_t e : pool )
+         cudaEventDestroy( e );
+   }
+   cudaEvent_t event()
+   {
+      if ( !pool.empty() )
+      {
+         cudaEvent_t e = pool.back();
+         pool.pop_back();
+         return e;
+      }
+      cudaEvent_t e;
+      HYB_CUDA( cudaEventCreate( &e ) );
+      return e;
+   }
+   void start( const std::string& name, cudaStream_t s )
+   {
+      TimingNode* child = nullptr;
+      for ( auto& k : cur->kids )
+         if ( k->name == name )
+            child = k.get();
+      if ( !child )
+      {
+         cur->kids.push_back( std::make_unique< TimingNode >() );
+         child         = cur->kids.back().get();
+         child->name   = name;
+         child->parent = cur;
+      }
+      const cudaEvent_t e = event();
+      HYB_CUDA( cudaEventRecord( e, s ) );
+      open.push_back( { child, e } );
+      cur = child;
+   }
+   void stop( const std::string& name, cudaStream_t s )
+   {
+      require( !open.empty() && open.back().node->name == name, "timing tree: stop of a timer that is not open" );
+      const cudaEvent_t e = event();
+      HYB_CUDA( cudaEventRecord( e, s ) );
+      pending.push_back( { open.back().node, open.back().start, e } );
+      open.pop_back();
+      cur = cur->parent;
+   }
+   // wait for the recorded events and add their intervals to the nodes
+   void collect()
+   {
+      if ( pending.empty() )
+         return;
+      HYB_CUDA( cudaEventSynchronize( pending.back().stop ) );
+      for ( auto& p : pending )
+      {
+         HYB_CUDA( cudaEventSynchronize( p.stop ) ); // events of other streams complete on their own
+         float ms = 0;
+         HYB_CUDA( cudaEventElapsedTime( &ms, p.start, p.stop ) );
+         const double t = 1e-3 * double( ms );
+         TimingNode&  n = *p.node;
+         n.minT         = n.count == 0 ? t : std::min( n.minT, t );
+         n.maxT         = n.count == 0 ? t : std::max( n.maxT, t );
+         n.total += t;
+         ++n.count;
+         pool.push_back( p.start );
+         pool.push_back( p.stop );
+      }
+      pending.clear();
+   }
+   void reset()
+   {
+      require( open.empty(), "timing tree: reset while a timer is open" );
+      collect();
+      root.kids.clear();
+      cur = &root;
+   }
+   // {"<name>": {"total": s, "average": s, "min": s, "max": s, "count": n, "children": {...}}, ...}
+   static void json( const TimingNode& n, std::string& out )
+   {
+      out += "{";
+      for ( size_t i = 0; i < n.kids.size(); ++i )
+      {
+         const TimingNode& k = *n.kids[i];
+         char              buf[256];
+         std::snprintf( buf, sizeof( buf ), "\"total\": %.9g, \"average\": %.9g, \"min\": %.9g, \"max\": %.9g, \"count\": %ld",
+                        k.total, k.count ? k.total / double( k.count ) : 0.0, k.minT, k.maxT, k.count );
+         out += ( i ? ", \"" : "\"" ) + k.name + "\": {" + buf + ", \"children\": ";
+         json( k, out );
+         out += "}";
+      }
+      out += "}";
+   }
+};
+
+// ---------------------------------------------------------------------------
 // Geometric multigrid (GeometricMultigridSolver.hpp:136-235)
 // ---------------------------------------------------------------------------
 struct Gmg
@@ -53,6 +189,20 @@ struct Gmg
    std::vector< G > loops;
    DevBuf< SolveCtl > ctl;
    SolveCtl*          hostCtl = nullptr;
+   // stage timers (hyb_gmg_set_timing): while on, solves run launch by launch, without
+   // graphs or the program kernel, and every stage records device events
+   bool       timing = false;
+   TimingTree tt;
+   void tstart( const std::string& name, cudaStream_t s )
+   {
+      if ( timing )
+         tt.start( name, s );
+   }
+   void tstop( const std::string& name, cudaStream_t s )
+   {
+      if ( timing )
+         tt.stop( name, s );
+   }
 
    ~Gmg()
    {
@@ -416,28 +566,49 @@ void launchProgram( Gmg& g, Function& x, Function& b, int top, cudaStream_t stre
 template < typename T >
 void vcycle( Gmg& g, Function& x, Function& b, Function& tmp, int l, cudaStream_t stream )
 {
-   if ( l <= g.progTop )
+   if ( l <= g.progTop && !g.timing )
    {
       launchProgram< T >( g, x, b, l, stream );
       return;
    }
+   const std::string lname = "Level " + std::to_string( l );
    if ( l == g.minL )
    {
+      g.tstart( lname, stream );
+      g.tstart( "Coarse Grid Solver", stream );
       coarseSolve( g, x.ptr< T >( l ), b.ptr< T >( l ), stream );
+      g.tstop( "Coarse Grid Solver", stream );
+      g.tstop( lname, stream );
       return;
    }
+   g.tstart( lname, stream );
    for ( int i = 0; i < g.pre; ++i )
+   {
+      g.tstart( "Smoother", stream );
       smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
+      g.tstop( "Smoother", stream );
+   }
    // tmp = b - A x ; restricted straight into b on the coarser level (b.assign(tmp) on flag)
    launchApply< T >( *g.op, l, x.ptr< T >( l ), tmp.ptr< T >( l ), b.ptr< T >( l ), kGmgFlag, kResidual, stream );
+   g.tstart( "Restriction", stream );
    launchRestrict< T >( *g.st, l, tmp.ptr< T >( l ), b.ptr< T >( l - 1 ), kGmgFlag, stream );
+   g.tstop( "Restriction", stream );
    HYB_CUDA( cudaMemsetAsync( x.ptr< T >( l - 1 ), 0, x.levelBytes( l - 1 ), stream ) ); // x.interpolate(0, l-1)
+   g.tstop( lname, stream );
    vcycle< T >( g, x, b, tmp, l - 1, stream );
    if ( g.cycleType == HYB_CYCLE_W ) // GeometricMultigridSolver.hpp:201-204
       vcycle< T >( g, x, b, tmp, l - 1, stream );
+   g.tstart( lname, stream );
+   g.tstart( "Prolongation", stream );
    launchProlongate< T >( *g.st, l - 1, x.ptr< T >( l - 1 ), x.ptr< T >( l ), kGmgFlag, true, stream );
+   g.tstop( "Prolongation", stream );
    for ( int i = 0; i < g.post; ++i )
+   {
+      g.tstart( "Smoother", stream );
       smooth< T >( g, l, x.ptr< T >( l ), b.ptr< T >( l ), tmp.ptr< T >( l ), stream );
+      g.tstop( "Smoother", stream );
+   }
+   g.tstop( lname, stream );
 }
 
 // Graph-captured work units.
@@ -454,13 +625,19 @@ enum GraphKind : int
 void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s )
 {
    if ( kind == kCycle64 || kind == kCycle64Norm )
+   {
+      g.tstart( "Geometric Multigrid Solver", s );
       vcycle< double >( g, x, b, *g.tmp64, l, s );
+      g.tstop( "Geometric Multigrid Solver", s );
+   }
    if ( kind == kMixedStep )
    {
       // FP32 V-cycle on the residual equation (mixedPrecisionIterativeRefinement.cpp:162-171);
       // the FP32 right-hand side was written with the previous residual's norm (below)
       HYB_CUDA( cudaMemsetAsync( g.x32->ptr< float >( l ), 0, g.x32->levelBytes( l ), s ) );
+      g.tstart( "Geometric Multigrid Solver", s );
       vcycle< float >( g, *g.x32, *g.b32, *g.t32, l, s );
+      g.tstop( "Geometric Multigrid Solver", s );
       launchAddCorrection< float >( *g.st, l, x.ptr< double >( l ), g.x32->ptr< float >( l ), kGmgFlag, s );
    }
    if ( kind > kFmg64 && kind <= kFmg64 + 8 )
@@ -470,7 +647,11 @@ void enqueue( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t s 
       for ( int lc = g.minL; lc <= l; ++lc )
       {
          for ( int c = 0; c < kind - kFmg64; ++c )
+         {
+            g.tstart( "Geometric Multigrid Solver", s );
             vcycle< double >( g, x, b, *g.tmp64, lc, s );
+            g.tstop( "Geometric Multigrid Solver", s );
+         }
          if ( lc < l )
             launchProlongate< double >( *g.st, lc, x.ptr< double >( lc ), x.ptr< double >( lc + 1 ), kGmgFlag, false, s );
       }
@@ -577,6 +758,13 @@ void ensureMixed( Gmg& g )
 
 void runGraph( Gmg& g, Function& x, Function& b, int l, int kind, cudaStream_t stream )
 {
+   if ( g.timing )
+   {
+      // timed: launch by launch, so that the stage events sit between the stages' kernels
+      prepare( g );
+      enqueue( g, x, b, l, kind, stream );
+      return;
+   }
    for ( auto& G : g.graphs )
       if ( G.x == &x && G.b == &b && G.level == l && G.kind == kind )
       {

@@ -36,6 +36,7 @@ SYMBOLS = [
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_server_batch_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
     "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
+    "hyb_gmg_set_timing", "hyb_gmg_timing_json", "hyb_gmg_timing_reset",
     "hyb_chebyshev_coefficients", "hyb_operator_estimate_spectral_radius", "hyb_server_mesh_bytes",
 ]
 
@@ -120,6 +121,9 @@ def load(path=LIB_PATH):
         "hyb_storage_create_from_gmsh": (I, [ctypes.c_char_p, I, PP]),
         "hyb_operator_smooth_sor_backwards": (I, [P, P, P, D, I, I, P]),
         "hyb_gmg_set_cycle_type": (I, [P, I]),
+        "hyb_gmg_set_timing": (I, [P, I]),
+        "hyb_gmg_timing_json": (I, [P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+        "hyb_gmg_timing_reset": (I, [P]),
         "hyb_gmg_setup_chebyshev": (I, [P, I, D, D]),
         "hyb_chebyshev_coefficients": (I, [I, D, D, P]),
         "hyb_operator_estimate_spectral_radius": (I, [P, P, P, I, I, P]),
@@ -474,6 +478,24 @@ class GeometricMultigridSolver:
 
     def solve(self, x, b, level, stream=None):
         _check(load().hyb_gmg_solve(self.h, x.h, b.h, level, _stream(stream)))
+
+    def set_timing(self, enable=True):
+        """Stage timers in the reference's timing-tree shape (device events); while on, solves
+        run launch by launch."""
+        _check(load().hyb_gmg_set_timing(self.h, int(bool(enable))))
+
+    def timing(self):
+        """The accumulated timing tree: {name: {total, average, min, max, count, children}}."""
+        import json
+
+        n = ctypes.c_size_t()
+        _check(load().hyb_gmg_timing_json(self.h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        _check(load().hyb_gmg_timing_json(self.h, buf, n.value + 1, ctypes.byref(n)))
+        return json.loads(buf.value.decode())
+
+    def reset_timing(self):
+        _check(load().hyb_gmg_timing_reset(self.h))
 
     def solve_fmg(self, x, b, level, cycles_per_level=1, stream=None):
         """FullMultigridSolver::solve: b must hold the right-hand side on every level."""

@@ -230,6 +230,22 @@ int hyb_gmg_destroy( hyb_gmg* g );
 /* HYB_CYCLE_V (default) or HYB_CYCLE_W: with W the coarse-grid correction recurses twice
  * (GeometricMultigridSolver.hpp:201-204); applies to every later solve of this solver */
 int hyb_gmg_set_cycle_type( hyb_gmg* g, int cycle_type );
+/* Stage timers in the shape of the reference's timing tree (the WcTimingTree that
+ * GeometricMultigridSolver.hpp:129-233 starts and stops): "Geometric Multigrid Solver" per
+ * V-cycle, with children "Level l" (started twice per cycle: before and after the coarse
+ * correction), and under those "Smoother", "Restriction", "Prolongation" and, on the
+ * coarsest level, "Coarse Grid Solver". The residual sits in its level's own time, as in
+ * the reference. The times come from CUDA events recorded on the solve's stream. While
+ * timing is on, solves run launch by launch, without CUDA graphs or the one-block program
+ * kernel, so every level has its own nodes; off (the default) costs nothing. */
+int hyb_gmg_set_timing( hyb_gmg* g, int enable );
+/* The accumulated tree as JSON, {"<name>": {"total": s, "average": s, "min": s, "max": s,
+ * "count": n, "children": {...}}, ...}. Waits for the recorded events. *length receives the
+ * size without the terminating NUL; buf may be NULL to ask for it, else capacity must
+ * exceed it (HYB_EINVAL otherwise). */
+int hyb_gmg_timing_json( hyb_gmg* g, char* buf, size_t capacity, size_t* length );
+/* clears the accumulated times (no timer may be open) */
+int hyb_gmg_timing_reset( hyb_gmg* g );
 /* ChebyshevSmoother::setupCoefficients(order, lowerBound, upperBound) (ChebyshevSmoother.hpp:98-188):
  * order 1..5, eigenvalue interval [lower, upper] of D^-1 A (the reference's
  * setupCoefficients(order, rho) uses [0.3 rho, 1.2 rho]) */
