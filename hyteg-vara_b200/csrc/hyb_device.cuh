@@ -296,7 +296,6 @@ struct OpDev
    const double*  bcell;  // [nC][4][3] macro-cell vertex coordinates (computational domain)
    const double*  bmap;   // [nC][8] shell map of the cell: ray vertex, n = (thr - ray) x (for - ray),
                           // radRay, s = (radRef - radRay) / ((ref - ray) . n)
-   const int32_t* bxyz;   // closure index -> x | y<<10 | z<<20 of the level
    double         balpha; // coefficient k(y) = exp( balpha (1 - |y|) )
    int            bN;     // micro-edges per macro-edge (2^level)
 };

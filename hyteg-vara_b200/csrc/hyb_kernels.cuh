@@ -421,15 +421,21 @@ struct PointBatch
 // and the slab positions of the 15 neighbours -- so a pass reads one row (three 16-byte
 // loads), gathers, and sums the group as before.
 // ---------------------------------------------------------------------------
+// Rows of the constant and variable operators: base = cell * stride and pos[q] the slab
+// position of neighbour q within the cell (16 bits: closures below 65536 points, level <= 6).
+// Rows of the blending operator ("relative" rows): base = cell * stride + the point's own slab
+// position, pos[q] the signed offset of neighbour q from the point (pos[0] = 0), which fits
+// 16 bits through level 7 (a neighbour is at most a z-slice and a row away), and xyz the
+// point's logical coordinates, which the on-the-fly integration needs.
 struct SlabRow
 {
-   int32_t  base;    // cell * stride; -1: no row (padding lane)
+   int32_t  base;    // see above; -1: no row (padding lane)
    int32_t  wsel;    // (cell * 16 + class) * 15: the partial stencil of the row
    uint16_t valid;   // neighbour mask of the class
    uint8_t  bc;      // boundary flag of the DoF
    uint8_t  pad0;
-   uint16_t pos[15]; // slab positions of the neighbours within the cell, pos[0] = the point
-   uint16_t pad1[3];
+   uint16_t pos[15]; // neighbour positions (absolute in the cell, or relative to the point)
+   uint16_t xyz[3];  // the point's x, y, z
 };
 static_assert( sizeof( SlabRow ) == 48, "three 16-byte loads per row" );
 
@@ -440,7 +446,7 @@ __device__ __forceinline__ SlabRow noRow()
    return R;
 }
 
-__device__ __forceinline__ SlabRow makeRow( const LevelDev& lv, int c, int x, int y, int z, uint8_t bc )
+__device__ __forceinline__ SlabRow makeRow( const LevelDev& lv, int c, int x, int y, int z, uint8_t bc, bool rel )
 {
    SlabRow           R{};
    const int         mask  = classMask( lv.N, x, y, z );
@@ -450,18 +456,22 @@ __device__ __forceinline__ SlabRow makeRow( const LevelDev& lv, int c, int x, in
    for ( int q = 0; q < 15; ++q )
    {
       const int xq = x + offX( q ), k = offRow( q );
-      R.pos[q]     = uint16_t( ( valid & ( 1u << q ) ) ? S.start[k] + resOff( xq & 3, S.len[k] ) + ( xq >> 2 ) : self );
+      const int p  = ( valid & ( 1u << q ) ) ? S.start[k] + resOff( xq & 3, S.len[k] ) + ( xq >> 2 ) : self;
+      R.pos[q]     = uint16_t( rel ? p - self : p );
    }
-   R.base  = c * lv.stride;
-   R.wsel  = ( c * 16 + mask ) * 15;
-   R.valid = uint16_t( valid );
-   R.bc    = bc;
+   R.base   = c * lv.stride + ( rel ? self : 0 );
+   R.wsel   = ( c * 16 + mask ) * 15;
+   R.valid  = uint16_t( valid );
+   R.bc     = bc;
+   R.xyz[0] = uint16_t( x );
+   R.xyz[1] = uint16_t( y );
+   R.xyz[2] = uint16_t( z );
    return R;
 }
 
 // one row per lane of the surface lists bl, in the lane order of HYB_BDRY_LANES; *err is
 // set when a lane's DoF has more embeddings than its group has lanes
-__global__ void k_rows_surface( TopoDev tp, LevelDev lv, BdryLists bl, long n, SlabRow* out, int* err )
+__global__ void k_rows_surface( TopoDev tp, LevelDev lv, BdryLists bl, long n, SlabRow* out, int* err, int rel )
 {
    for ( long gt = long( blockIdx.x ) * blockDim.x + threadIdx.x; gt < n; gt += long( gridDim.x ) * blockDim.x )
    {
@@ -477,7 +487,7 @@ __global__ void k_rows_surface( TopoDev tp, LevelDev lv, BdryLists bl, long n, S
          {
             int c, x, y, z;
             embeddingCoords( embAt( tp, p.kind, p.prim, tk.sub ), p.kind, lv.N, p.i, p.j, c, x, y, z );
-            R = makeRow( lv, c, x, y, z, primBc( tp, p.kind, p.prim ) );
+            R = makeRow( lv, c, x, y, z, primBc( tp, p.kind, p.prim ), rel != 0 );
          }
       }
       out[gt] = R;
@@ -485,7 +495,7 @@ __global__ void k_rows_surface( TopoDev tp, LevelDev lv, BdryLists bl, long n, S
 }
 
 // one row per (cell, entry) of an interior point list, cell-major; interior points are Inner
-__global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, int nList, SlabRow* out )
+__global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, int nList, SlabRow* out, int rel )
 {
    const long n = long( tp.nC ) * nList;
    for ( long t = long( blockIdx.x ) * blockDim.x + threadIdx.x; t < n; t += long( gridDim.x ) * blockDim.x )
@@ -494,13 +504,18 @@ __global__ void k_rows_interior( TopoDev tp, LevelDev lv, const int32_t* list, i
       const int32_t e    = list[t - long( cell ) * nList];
       const int     g    = e & 255;
       const NbrOff  no   = blockNbr( lv.blk, e >> 8 );
+      const int32_t p0   = lv.blkXYZ[e >> 8]; // x | y << 10 | z << 20 of the block's g = 0 point
+      const int     self = no.d[0] + g;
       SlabRow       R{};
-      R.base  = cell * lv.stride;
+      R.base  = cell * lv.stride + ( rel ? self : 0 );
       R.wsel  = cell * 16 * 15;
       R.valid = 0x7fff;
       R.bc    = 1; // Inner
       for ( int q = 0; q < 15; ++q )
-         R.pos[q] = uint16_t( no.d[q] + g );
+         R.pos[q] = uint16_t( rel ? no.d[q] - no.d[0] : no.d[q] + g );
+      R.xyz[0] = uint16_t( ( p0 & 1023 ) + 4 * g );
+      R.xyz[1] = uint16_t( ( p0 >> 10 ) & 1023 );
+      R.xyz[2] = uint16_t( p0 >> 20 );
       out[t] = R;
    }
 }
@@ -612,21 +627,19 @@ __device__ __forceinline__ void blendTetRow( const double* __restrict__ m, const
    row[0] = -( row[1] + row[2] + row[3] );
 }
 
-// diag and off-diagonal sum of the partial row of the closure point at slab position pos(0)
-// of `cell`: the blended matrices of the incident micro-tets allowed by the class (validT);
+// diag and off-diagonal sum of the partial row of the closure point (x, y, z) of `cell`,
+// whose neighbours are read at uc[pos(q)]: the blended matrices of the incident micro-tets allowed by the class (validT);
 // vertex coordinates as vertexdof::macrocell::coordinateFromIndex
 // (src/hyteg/p1functionspace/VertexDoFMacroCell.hpp:68-75): v0 + (v_k - v0)/N i_k. The
 // integration runs in the row type: FP64 rows reproduce the reference's matrices, FP32 rows
 // (the single-precision V-cycles of the mixed solver) evaluate them in FP32.
 template < typename T, typename Pos >
-__device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int cell, uint32_t validT, Pos&& pos, T& diag,
-                                          T& off )
+__device__ __forceinline__ void blendRow( const OpDev< T >& op, const T* uc, int cell, int x, int y, int z, uint32_t validT,
+                                          Pos&& pos, T& diag, T& off )
 {
    using C          = T;
    const double* v  = op.bcell + size_t( cell ) * 12;
    const double* m  = op.bmap + size_t( cell ) * 8;
-   const int     pk = op.bxyz[pos( 0 )];
-   const int     x = pk & 1023, y = ( pk >> 10 ) & 1023, z = pk >> 20;
    C             h[3][3], v0[3];
 #pragma unroll
    for ( int j = 0; j < 3; ++j )
@@ -745,11 +758,14 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
 #pragma unroll
             for ( int w = 0; w < 8; ++w )
                sPos[w][threadIdx.x] = h[w];
+            // relative rows: signed offsets from the point (uc), its x, y, z in C.z's upper
+            // and C.w's halves
             auto spos = [&]( int q ) {
                const uint32_t v = sPos[q >> 1][threadIdx.x];
-               return int( ( q & 1 ) ? ( v >> 16 ) : ( v & 0xffffu ) );
+               return int( int16_t( ( q & 1 ) ? ( v >> 16 ) : ( v & 0xffffu ) ) );
             };
-            blendRow( op, uc, A.y / 240, kValidTets[( A.y / 15 ) & 15], spos, diag, off );
+            blendRow( op, uc, A.y / 240, int( uint32_t( C.z ) >> 16 ), int( uint32_t( C.w ) & 0xffffu ),
+                      int( uint32_t( C.w ) >> 16 ), kValidTets[( A.y / 15 ) & 15], spos, diag, off );
          }
          else if constexpr ( !VAR )
          {

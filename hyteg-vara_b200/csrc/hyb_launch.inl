@@ -49,7 +49,7 @@ long rowIfaceMaxPoints()
 // The row tables of level l, built on first use (not inside a stream capture); nullptr if
 // the level is too large, or if a DoF has more embeddings than its lane group (then the
 // passes keep the lane-group path).
-std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool full );
+std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool full, bool relative = false );
 
 const RowTables* ensureRows( Storage& s, int l )
 {
@@ -71,9 +71,12 @@ const RowTables* ensureBlendRows( Storage& s, int l )
    LevelHost& L = *s.lv[size_t( l )];
    if ( L.blendRows )
       return L.blendRows.get();
-   require( L.dev.stride < 65536,
-            "the blending operator supports levels whose cell closures have fewer than 65536 points (level <= 6)" );
-   L.blendRows = buildRows( s, l, true );
+   // relative rows: a neighbour's offset from its point (at most a z-slice and a row) must fit
+   // 16 signed bits, and cell * stride + position 32 signed bits
+   const long W = L.dev.W;
+   require( W * ( W + 1 ) / 2 + 2 * W < 32768, "the blending operator supports levels up to 7" );
+   require( long( s.td.nC ) * L.dev.stride < ( 1l << 31 ), "too many cells for the blending operator at this level" );
+   L.blendRows = buildRows( s, l, true, true );
    require( L.blendRows != nullptr, "row table construction failed (a DoF has more cells than its lane group)" );
    return L.blendRows.get();
 }
@@ -81,7 +84,7 @@ const RowTables* ensureBlendRows( Storage& s, int l )
 // the row tables of level l: the surface colours' rows, and with full also every colour's
 // interior rows and the rows of all DoFs; nullptr if a DoF has more embeddings than its lane
 // group has lanes
-std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool withInterior )
+std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool withInterior, bool relative )
 {
    LevelHost&      L = *s.lv[size_t( l )];
    const LevelDev& d = L.dev;
@@ -108,7 +111,8 @@ std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool withInterior )
          continue;
       const int32_t*  list = L.colourList.p + co[0];
       const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
-      k_rows_surface<<< grid( lanes ), 256 >>>( s.td, d, bl, lanes, R->iface.p + R->ifaceOff[size_t( c )], err.p );
+      k_rows_surface<<< grid( lanes ), 256 >>>( s.td, d, bl, lanes, R->iface.p + R->ifaceOff[size_t( c )], err.p,
+                                               int( relative ) );
       HYB_CHECK_LAUNCH();
    }
    if ( !R->full )
@@ -128,7 +132,8 @@ std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool withInterior )
       if ( count == 0 )
          continue;
       k_rows_interior<<< grid( long( s.td.nC ) * count ), 256 >>>( s.td, d, d.ptsC + d.ptsOff[c], count,
-                                                                  R->interior.p + long( s.td.nC ) * d.ptsOff[c] );
+                                                                  R->interior.p + long( s.td.nC ) * d.ptsOff[c],
+                                                                  int( relative ) );
       HYB_CHECK_LAUNCH();
    }
    // all DoFs
@@ -142,12 +147,12 @@ std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool withInterior )
    R->all.alloc( size_t( std::max< long >( R->allN, 1 ) ) );
    if ( surf > 0 )
    {
-      k_rows_surface<<< grid( surf ), 256 >>>( s.td, d, full, surf, R->all.p, err.p );
+      k_rows_surface<<< grid( surf ), 256 >>>( s.td, d, full, surf, R->all.p, err.p, int( relative ) );
       HYB_CHECK_LAUNCH();
    }
    if ( nInt > 0 )
    {
-      k_rows_interior<<< grid( nInt ), 256 >>>( s.td, d, d.pts, d.nPts, R->all.p + surf );
+      k_rows_interior<<< grid( nInt ), 256 >>>( s.td, d, d.pts, d.nPts, R->all.p + surf, int( relative ) );
       HYB_CHECK_LAUNCH();
    }
    int bad = 0;

@@ -529,7 +529,6 @@ struct Operator
          // no stencils or element matrices: the rows integrate the blended matrices
          o.bcell  = st->cellCoords.p;
          o.bmap   = bmap.p;
-         o.bxyz   = st->L( l ).dev.xyz;
          o.balpha = alpha;
          o.bN     = st->L( l ).dev.N;
          return o;

@@ -192,7 +192,7 @@ int hyb_operator_create_divkgrad_rff( hyb_storage* s, int min_level, int max_lev
  * IcosahedralShellMap, and the element matrices of p1_div_k_grad_blending_q3 (5-point rule,
  * map Jacobian at the quadrature points) are integrated on the device per row, with
  * k(y) = exp( alpha (1 - |y|) ) at the mapped points (alpha = 0: the Laplacian). Levels
- * up to 6; apply, residual, (symmetric/backward) SOR, weighted Jacobi, the inverse
+ * up to 7; apply, residual, (symmetric/backward) SOR, weighted Jacobi, the inverse
  * diagonal (Chebyshev smoother, spectral radius estimate), CG and GMG; an error when a cell
  * has no shell map */
 int hyb_operator_create_blend_divkgrad( hyb_storage* s, int min_level, int max_level, double alpha,

@@ -1740,6 +1740,21 @@ void orc_sor_ref( void* h, int op, int level, double* x, const double* b, double
    sorRefT( *o, o->ops[op], o->lv[level], x, b, relax, flag, backwards != 0 );
 }
 
+void orc_apply_rows( void* h, int op, int level, const double* src, const int64_t* dofs, int64_t n, double* out )
+{
+   auto*        o  = H( h );
+   const Op&    O  = o->ops[op];
+   const Level& lv = o->lv[level];
+#pragma omp parallel for schedule( dynamic, 16 )
+   for ( int64_t i = 0; i < n; ++i )
+   {
+      const i64 d    = dofs[i];
+      double    diag = 0, off = 0;
+      fullRow( *o, O, lv, d, [src]( i64 k ) { return src[k]; }, diag, off );
+      out[i] = diag * src[d] + off;
+   }
+}
+
 void orc_sor_ref_stages( void* h, int op, int level, double* x, const double* b, double relax, int flag, int backwards,
                          int stages )
 {

@@ -67,6 +67,8 @@ int  orc_set_threads( int n );
 void orc_cell_stencil( void* h, int op, int level, int cell, int mask, double* out15 );
 
 void   orc_apply( void* h, int op, int level, const double* src, double* dst, int flag, int add );
+// (A src)[dofs[i]] for the listed DoFs only (every flag), for spot checks on large levels
+void   orc_apply_rows( void* h, int op, int level, const double* src, const int64_t* dofs, int64_t n, double* out );
 // backwards != 0: smooth_sor_backwards (P1Operator.hpp:424-431)
 void   orc_sor_ref( void* h, int op, int level, double* x, const double* b, double relax, int flag, int backwards );
 // One or more stages of that sweep: bit 0 macro-vertices, 1 macro-edges, 2 macro-faces,

@@ -65,6 +65,7 @@ def lib():
         L.orc_apply.argtypes = [P, I, I, P, P, I, I]
         L.orc_sor_ref.argtypes = [P, I, I, P, P, D, I, I]
         L.orc_sor_ref_stages.argtypes = [P, I, I, P, P, D, I, I, I]
+        L.orc_apply_rows.argtypes = [P, I, I, P, P, I64, P]
         L.orc_sor_colored.argtypes = [P, I, I, P, P, D, I, P, I, I]
         L.orc_jacobi.argtypes = [P, I, I, P, P, D, I]
         L.orc_prolongate.argtypes = [P, I, P, P, I, I]
@@ -189,6 +190,14 @@ class Oracle:
         dst = np.zeros_like(src) if dst is None else dst
         lib().orc_apply(self.h, op, level, _p(src), _p(dst), flag, int(add))
         return dst
+
+    def apply_rows(self, src, level, dofs, op=0):
+        """(A src) at the listed DoFs only."""
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        dofs = np.ascontiguousarray(dofs, dtype=np.int64)
+        out = np.zeros(len(dofs))
+        lib().orc_apply_rows(self.h, op, level, _p(src), _p(dofs), len(dofs), _p(out))
+        return out
 
     def sor_ref(self, x, b, level, relax=1.0, flag=INNER | NEUMANN, op=0, backwards=False, stages=15):
         """smooth_sor / smooth_sor_backwards; `stages` selects the primitive sweeps to run

@@ -155,3 +155,13 @@ def test_face_sor_stage_matches_generated_face_kernels(oracle_mod, gold, level):
             assert not np.allclose(r, x0[fds[fi][ip]])  # the kernel did run on this face
             np.testing.assert_allclose(xs[fds[fi][ip]], r, rtol=0, atol=1e-12 * (1 + np.abs(r).max()),
                                        err_msg=f"face {f} relax {relax} backwards {bw}")
+
+
+def test_apply_rows_equals_apply(oracle_mod, gold):
+    """The oracle's row spot check (used on levels too large for a full oracle apply) is the
+    full apply restricted to the listed DoFs."""
+    O = oracle_mod
+    o = O.Oracle(gold["coords"], gold["tets"], 4)
+    x = gold["x_L4"]
+    dofs = np.arange(o.n(4))[::7]
+    np.testing.assert_array_equal(o.apply_rows(x, 4, dofs), o.apply(x, 4, flag=O.ALL)[dofs])
