@@ -410,7 +410,7 @@ class P1ElementwiseBlendingDivKGradOperator(_Operator):
     """P1ElementwiseOperator<p1_div_k_grad_blending_q3> on a spherical-shell mesh whose cells
     carry the IcosahedralShellMap (IcosahedralShellMap::setMap); the coefficient is
     k(y) = exp(alpha (1 - |y|)) at the mapped quadrature points (alpha = 0: Laplacian).
-    Element matrices are integrated on the device per row; levels up to 6."""
+    Element matrices are integrated on the device per row; levels up to 7."""
 
     def __init__(self, storage, min_level, max_level, alpha=0.0):
         self.storage = storage
