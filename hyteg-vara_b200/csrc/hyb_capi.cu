@@ -515,6 +515,23 @@ int hyb_operator_create_divkgrad_callback( hyb_storage* s, int minL, int maxL, d
    HYB_API_END
 }
 
+int hyb_operator_create_divkgrad_quadrature( hyb_storage* s, int minL, int maxL, int kind, const double* w,
+                                             const double* phase, int modes, double sigma, double radial,
+                                             hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && out, "null argument" );
+   require( kind == 1 || kind == 2, "coefficient kind must be 1 (tanh) or 2 (random features)" );
+   if ( kind == 2 )
+   {
+      require( w && phase, "null argument" );
+      require( modes > 0 && modes <= 4096, "modes must be in [1, 4096]" );
+   }
+   *out = reinterpret_cast< hyb_operator* >(
+       makeDivKGradQuadrature( ST( s ), minL, maxL, kind, w, phase, modes, sigma, radial ) );
+   HYB_API_END
+}
+
 int hyb_operator_create_divkgrad_rff( hyb_storage* s, int minL, int maxL, const double* w, const double* phase,
                                       int modes, double sigma, double radial, hyb_operator** out )
 {

@@ -291,6 +291,11 @@ struct OpDev
    const T* st;  // constant coefficient: [nC][16][15] partial stencils per class
    const T* K;   // variable coefficient: [nC][6][4][4] micro-tet matrices (1/4 folded in)
    const T* kap; // variable coefficient: nodal k, function layout
+   // variable coefficient integrated at quadrature points (the reference form's callback):
+   // per cell 6 slabs (one per micro-tet type) holding, at the slab position of a micro-tet's
+   // vertex 0, 24 sum_q w_q k(x_q) -- the factor on its matrix K (which has the 1/4 folded
+   // in) that replaces the sum of the 4 nodal values; null: nodal k (kap)
+   const T* kq;
    int      stride;
    // blending operator (curved shell): element matrices integrated on the fly per row
    const double*  bcell;  // [nC][4][3] macro-cell vertex coordinates (computational domain)
@@ -301,8 +306,10 @@ struct OpDev
 };
 
 // Partial row of the operator at closure point (x,y,z) of `cell`: the contributions
-// of the micro-tets of this cell only. u = the cell's slab.
-template < typename T, bool VAR >
+// of the micro-tets of this cell only. u = the cell's slab. VAR (throughout the kernels):
+// 0 constant stencils, 1 variable coefficient from nodal values (OpDev::kap), 2 variable
+// coefficient integrated at quadrature points (OpDev::kq).
+template < typename T, int VAR >
 __device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* u, int cell, int W, int x, int y,
                                             int z, T& diag, T& off )
 {
@@ -330,6 +337,7 @@ __device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* u, in
    else
    {
       const T*       kv    = op.kap + size_t( cell ) * op.stride;
+      const T*       kqc   = VAR == 2 ? op.kq + size_t( cell ) * 6 * op.stride : nullptr;
       const T*       K     = op.K + size_t( cell ) * 96;
       const uint32_t validT = kValidTets[mask];
 #pragma unroll
@@ -338,7 +346,11 @@ __device__ __forceinline__ void partialRow( const OpDev< T >& op, const T* u, in
          const IncidentTet it = incidentTet( i );
          if ( !( validT & ( 1u << i ) ) )
             continue;
-         const T ks = kv[pos[it.q[0]]] + kv[pos[it.q[1]]] + kv[pos[it.q[2]]] + kv[pos[it.q[3]]];
+         T ks;
+         if constexpr ( VAR == 2 )
+            ks = kqc[size_t( it.t ) * op.stride + pos[it.q[0]]];
+         else
+            ks = kv[pos[it.q[0]]] + kv[pos[it.q[1]]] + kv[pos[it.q[2]]] + kv[pos[it.q[3]]];
          const T* Kr = K + it.t * 16 + it.k * 4;
 #pragma unroll
          for ( int j = 0; j < 4; ++j )

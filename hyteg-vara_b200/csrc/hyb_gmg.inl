@@ -556,6 +556,7 @@ void launchProgram( Gmg& g, Function& x, Function& b, int top, cudaStream_t stre
    const Phase* ph  = prog->phases.p;
    const auto*  lt  = (const LevelDev*) g.st->lvTable.p;
    const int    nLv = int( g.st->lvTable.n );
+   require( varKind( *g.op ) != 2, "the program kernel does not take coefficients at quadrature points" );
    if ( g.op->variable )
       pdlLaunch( k_program< T, true >, dim3( 1 ), dim3( kProgramThreads ), 0, stream, g.st->td, lt, ph, prog->n, nLv );
    else
@@ -739,6 +740,8 @@ void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int
       g.progTop = -1; // the program kernel has no Chebyshev phases
    if ( op->blend )
       g.progTop = -1; // blending operators run every level as row-pass launches
+   if ( varKind( *op ) == 2 )
+      g.progTop = -1; // the program kernel is built for nodal coefficients only
 }
 
 
@@ -978,7 +981,7 @@ struct SolveBatch
    SolveJob job[kSolveBatchMax];
 };
 
-template < bool VAR >
+template < int VAR >
 __global__ void __launch_bounds__( kProgramThreads ) k_solve_batch( const __grid_constant__ SolveBatch batch )
 {
    // the job table travels in the launch's parameters, so no buffer outlives the launch

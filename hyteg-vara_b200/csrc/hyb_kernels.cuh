@@ -97,7 +97,7 @@ __device__ __forceinline__ uint8_t primBc( const TopoDev& tp, int kind, int prim
 }
 
 // Full row (sum of partial rows over adjacent cells) of a boundary DoF.
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __device__ __forceinline__ void bdryRow( const TopoDev& tp, const LevelDev& lv, const OpDev< T >& op, const T* u,
                                          const BdryPoint& p, T& diag, T& off )
 {
@@ -196,7 +196,7 @@ __device__ __forceinline__ T groupSum( T v, int G )
 }
 
 // Partial rows of the group's adjacent cells, summed over the group (all lanes get it).
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __device__ __forceinline__ void bdryRowGroup( const TopoDev& tp, const LevelDev& lv, const OpDev< T >& op, const T* u,
                                               const BdryPoint& p, const LaneTask& tk, bool active, T& diag, T& off )
 {
@@ -243,13 +243,15 @@ __device__ __forceinline__ Blk launchBlk() { return Blk{ int( blockIdx.x ), int(
 // ---------------------------------------------------------------------------
 // Interior stencil evaluation with all 15 neighbours inside the cell
 // ---------------------------------------------------------------------------
-template < typename T, bool VAR >
+template < typename T, int VAR >
 struct InteriorOp
 {
    T w[15];       // constant operator: the class-0 stencil of the cell
    T ku[36];      // variable operator: the 6 off-diagonal entries (pairs 01 02 03 12 13 23)
                   // of each of the cell's 6 micro-tet matrices, held in registers
    const T* kv;   // variable operator: nodal k slab of the cell
+   const T* kqc;  // variable operator at quadrature points: the cell's 6 micro-tet factor slabs
+   int      kqs;  // their stride
 
    // index of the unordered vertex pair (a, b), a != b, in the order 01 02 03 12 13 23
    __host__ __device__ static constexpr int pairIdx( int a, int b )
@@ -277,7 +279,9 @@ struct InteriorOp
 #pragma unroll
                for ( int b = a + 1; b < 4; ++b )
                   ku[6 * t + pairIdx( a, b )] = K[t * 16 + a * 4 + b];
-         kv = op.kap + size_t( cell ) * op.stride;
+         kv  = op.kap + size_t( cell ) * op.stride;
+         kqc = VAR == 2 ? op.kq + size_t( cell ) * 6 * op.stride : nullptr;
+         kqs = op.stride;
       }
    }
 
@@ -293,6 +297,34 @@ struct InteriorOp
          for ( int q = 1; q < 15; ++q )
             s += w[q] * u[no.d[q] + g];
          off = s;
+      }
+      else if constexpr ( VAR == 2 )
+      {
+         // one quadrature factor per incident micro-tet, at its vertex 0
+         T uq[15];
+#pragma unroll
+         for ( int q = 0; q < 15; ++q )
+            uq[q] = u[no.d[q] + g];
+         T d = 0, s = 0;
+#pragma unroll
+         for ( int i = 0; i < 24; ++i )
+         {
+            const IncidentTet it = incidentTet( i );
+            const T ks = kqc[it.t * kqs + no.d[it.q[0]] + g];
+            T       rowsum = 0, acc = 0;
+#pragma unroll
+            for ( int j = 0; j < 4; ++j )
+               if ( j != it.k )
+               {
+                  const T c = ku[6 * it.t + pairIdx( it.k, j )];
+                  rowsum += c;
+                  acc += c * uq[it.q[j]];
+               }
+            d -= ks * rowsum;
+            s += ks * acc;
+         }
+         diag = d;
+         off  = s;
       }
       else
       {
@@ -384,7 +416,7 @@ __device__ __forceinline__ NbrOff blockNbr( const int32_t* __restrict__ blk, int
 // Measured on B200 at level 7, two beat one by 1.2-1.3x and beat four for FP32 (four cost
 // registers and with them resident warps); three beat two by ~2 % for FP64 and lose ~5 %
 // for FP32.
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __host__ __device__ constexpr int interiorBatch()
 {
    return VAR ? 1 : ( sizeof( T ) == 8 ? 3 : 2 );
@@ -725,7 +757,7 @@ enum RowMode : int
 // of 32; the rows of one DoF are adjacent lanes of one warp). Constant operator: the
 // partial stencil st[wsel + q]; variable operator: the row's positions drive the
 // incident micro-tets' matrices and nodal coefficients (the variable branch of partialRow).
-template < typename T, int MODE, bool VAR, bool BLEND = false >
+template < typename T, int MODE, int VAR, bool BLEND = false >
 __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >& op, T* u, const T* b, T* r, T relax,
                                              int flag, long long start, long long step )
 {
@@ -780,6 +812,7 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
          {
             const int      cls    = ( A.y / 15 ) & 15, cell = A.y / 240;
             const T*       kv     = op.kap + A.x;
+            const T*       kqc    = VAR == 2 ? op.kq + size_t( cell ) * 6 * op.stride : nullptr;
             const T*       K      = op.K + size_t( cell ) * 96;
             const uint32_t validT = kValidTets[cls];
 #pragma unroll
@@ -788,7 +821,11 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
                const IncidentTet it = incidentTet( i );
                if ( !( validT & ( 1u << i ) ) )
                   continue;
-               const T  ks = kv[pos( it.q[0] )] + kv[pos( it.q[1] )] + kv[pos( it.q[2] )] + kv[pos( it.q[3] )];
+               T ks;
+               if constexpr ( VAR == 2 )
+                  ks = kqc[size_t( it.t ) * op.stride + pos( it.q[0] )];
+               else
+                  ks = kv[pos( it.q[0] )] + kv[pos( it.q[1] )] + kv[pos( it.q[2] )] + kv[pos( it.q[3] )];
                const T* Kr = K + it.t * 16 + it.k * 4;
 #pragma unroll
                for ( int j = 0; j < 4; ++j )
@@ -823,7 +860,7 @@ __device__ __forceinline__ void rowPassBody( const RowPass& rp, const OpDev< T >
 }
 
 // a row pass as its own launch (levels between the program kernel's and the large ones)
-template < typename T, int MODE, bool VAR, bool BLEND = false >
+template < typename T, int MODE, int VAR, bool BLEND = false >
 __global__ void __launch_bounds__( 128 ) k_row_pass( RowPass rp, OpDev< T > op, T* u, const T* b, T* r, T relax, int flag )
 {
    HYB_PDL_PROLOGUE();
@@ -895,7 +932,7 @@ __device__ __forceinline__ void quadApply( const T* u, const T w[15], const Sten
 // apply / residual (P1Operator::apply, P1Operator.hpp:196-324;
 // P1ElementwiseOperator::apply, P1ElementwiseOperator.cpp:64-221)
 // ---------------------------------------------------------------------------
-template < typename T, bool VAR, int MODE >
+template < typename T, int VAR, int MODE >
 __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, const T* src,
                                                   T* dst, const T* rhs, int flag,
                                                   int nCellBlocks, double* acc = nullptr, float* cvt = nullptr )
@@ -1025,7 +1062,7 @@ __device__ __forceinline__ void applyBody( Blk vb, TopoDev tp, LevelDev lv, OpDe
    }
 }
 
-template < typename T, bool VAR, int MODE >
+template < typename T, int VAR, int MODE >
 __global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_apply( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
                                                   T* __restrict__ dst, const T* __restrict__ rhs, int flag,
                                                   int nCellBlocks )
@@ -1038,7 +1075,7 @@ __device__ double blockSum( double v, double* red );
 
 // ||rhs - A src||^2 over the owned active DoFs without storing the residual: one partial
 // per block (summed by k_reduce_final in a fixed order); float(r) into cvt when given.
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( 128, VAR ? 3 : 8 ) k_residual_norm( TopoDev tp, LevelDev lv, OpDev< T > op,
                                                                       const T* __restrict__ src, const T* __restrict__ rhs,
                                                                       int flag, int nCellBlocks, double* __restrict__ partial,
@@ -1070,7 +1107,7 @@ constexpr int kInteriorColours = 4;
 // smaller levels long strips leave blocks idle, so the strip shrinks with the work)
 constexpr int kInteriorStrip = 4;
 
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __device__ __forceinline__ void sorIfaceBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, T* u,
                                                       const T* rhs, T relax, int flag, BdryLists bl )
 {
@@ -1092,7 +1129,7 @@ __device__ __forceinline__ void sorIfaceBody( Blk vb, TopoDev tp, LevelDev lv, O
    }
 }
 
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( 128, VAR ? 4 : 8 ) k_sor_iface( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                       const T* __restrict__ rhs, T relax, int flag, BdryLists bl )
 {
@@ -1104,7 +1141,7 @@ __global__ void __launch_bounds__( 128, VAR ? 4 : 8 ) k_sor_iface( TopoDev tp, L
 // residue block r = (c - 2y - 3z) mod 4, one contiguous run of the row; the colour's point
 // table lists them in storage order. Odd colours walk the cells in reverse order, so a
 // pass starts on the data the previous pass touched last (still in L2).
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __device__ __forceinline__ void sorInteriorBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, T* u,
                                                          const T* rhs, T relax, int colour, int begin,
                                                          int nPts, int nCellBlocks )
@@ -1147,7 +1184,7 @@ __device__ __forceinline__ void sorInteriorBody( Blk vb, TopoDev tp, LevelDev lv
    }
 }
 
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                          const T* __restrict__ rhs, T relax, int colour, int begin,
                                                          int nPts, int nCellBlocks )
@@ -1161,7 +1198,7 @@ __global__ void __launch_bounds__( 128 ) k_sor_interior( TopoDev tp, LevelDev lv
 // points of different cells are never coupled, so no other block's progress matters; on
 // small levels, where a colour pass has little work, this saves three launches per sweep.
 // backwards != 0 runs the colours 3..0 (the backward sweep of a symmetric SOR step).
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                                const T* __restrict__ rhs, T relax, int o0, int o1, int o2,
                                                                int o3, int o4, int backwards )
@@ -1200,7 +1237,7 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, Level
 // primitive DoFs). zeros: a zero vector of the level, read as the operand of the rows
 // whose off-diagonal part is discarded. Cells' interiors on the first nCellBlocks blocks.
 // ---------------------------------------------------------------------------
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( 128 ) k_inv_diag( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ zeros,
                                                      T* __restrict__ out, int nCellBlocks )
 {
@@ -1266,7 +1303,7 @@ __global__ void __launch_bounds__( 256 ) k_cheb_update( long long n, const T* __
 // Weighted Jacobi (P1Operator::smooth_jac, P1Operator.hpp:424-440):
 // dst = src + relax * (rhs - A src) / diag(A)
 // ---------------------------------------------------------------------------
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __device__ __forceinline__ void jacobiBody( Blk vb, TopoDev tp, LevelDev lv, OpDev< T > op, const T* src,
                                                    T* dst, const T* rhs, T relax, int flag,
                                                    int nCellBlocks )
@@ -1317,7 +1354,7 @@ __device__ __forceinline__ void jacobiBody( Blk vb, TopoDev tp, LevelDev lv, OpD
    }
 }
 
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( 128 ) k_jacobi( TopoDev tp, LevelDev lv, OpDev< T > op, const T* __restrict__ src,
                                                    T* __restrict__ dst, const T* __restrict__ rhs, T relax, int flag,
                                                    int nCellBlocks )
@@ -1603,6 +1640,95 @@ __global__ void k_fill_rff_coefficient( TopoDev tp, LevelDev lv, const double* _
    dst[size_t( cell ) * lv.stride + idx] = T( exp( radial * ( 1.0 - r ) + sigma * sqrt( 2.0 / modes ) * g ) );
 }
 
+// Coefficient functions of the quadrature-point operator (the reference form's callback):
+// kind 1: tanh(2 (x - 1/2)) + 2 (ElementwiseDivKGradCGConvergenceTest.cpp:41-137);
+// kind 2: exp( radial (1 - |x|) + sigma sqrt(2/M) sum_m cos( w_m . x + phase_m ) ), the random
+// Fourier-feature field (w: M x 3, phase: M).
+struct CoefFn
+{
+   int           kind, modes;
+   double        sigma, radial;
+   const double* w;
+   const double* phase;
+};
+
+__device__ __forceinline__ double coefValue( const CoefFn& f, const double p[3] )
+{
+   if ( f.kind == 1 )
+      return tanh( 2.0 * ( p[0] - 0.5 ) ) + 2.0;
+   double g = 0;
+   for ( int m = 0; m < f.modes; ++m )
+      g += cos( f.w[3 * m] * p[0] + f.w[3 * m + 1] * p[1] + f.w[3 * m + 2] * p[2] + f.phase[m] );
+   const double r = sqrt( p[0] * p[0] + p[1] * p[1] + p[2] * p[2] );
+   return exp( f.radial * ( 1.0 - r ) + f.sigma * sqrt( 2.0 / f.modes ) * g );
+}
+
+// nodal values of a coefficient function (closure layout)
+__global__ void k_fill_coefficient( LevelDev lv, const double* __restrict__ cellCoords,
+                                    const int32_t* __restrict__ cellOrder, double* __restrict__ dst, CoefFn f )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int pk   = lv.xyz[idx];
+   double    p[3];
+   closurePosition( cellCoords, cellOrder, cell, lv.N, pk & 1023, ( pk >> 10 ) & 1023, pk >> 20, p );
+   dst[size_t( cell ) * lv.stride + idx] = coefValue( f, p );
+}
+
+// The quadrature factors of OpDev::kq: for every micro-tet (type t, vertex 0 at closure point
+// idx) inside the closure, 24 sum_q w_q k(x_q) with the 5-point degree-3 rule of
+// p1_div_k_grad_affine_q3 (centroid, weight -2/15; the points with barycentric coordinates
+// (1/2, 1/6, 1/6, 1/6), weight 3/40; p1_div_k_grad_affine_q3.cpp:179+). Slots of micro-tets
+// that leave the closure are set to 0 and never read.
+__global__ void k_fill_tet_factors( LevelDev lv, const double* __restrict__ cellCoords,
+                                    const int32_t* __restrict__ cellOrder, double* __restrict__ dst, CoefFn f )
+{
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( idx >= lv.S )
+      return;
+   const int cell = blockIdx.y;
+   const int pk   = lv.xyz[idx];
+   const int x = pk & 1023, y = ( pk >> 10 ) & 1023, z = pk >> 20;
+   for ( int t = 0; t < 6; ++t )
+   {
+      // the micro-tet of type t with this point as its vertex 0 (role 0 of incidentTet)
+      int q[4] = { 0, 0, 0, 0 };
+      for ( int i = 0; i < 24; ++i )
+      {
+         const IncidentTet it = incidentTet( i );
+         if ( it.t == t && it.k == 0 )
+            for ( int j = 0; j < 4; ++j )
+               q[j] = it.q[j];
+      }
+      double X[4][3];
+      bool   inside = true;
+      for ( int j = 0; j < 4 && inside; ++j )
+      {
+         const int xx = x + offX( q[j] ), yy = y + offY( q[j] ), zz = z + offZ( q[j] );
+         inside       = xx >= 0 && yy >= 0 && zz >= 0 && xx + yy + zz <= lv.N;
+         if ( inside )
+            closurePosition( cellCoords, cellOrder, cell, lv.N, xx, yy, zz, X[j] );
+      }
+      double s = 0;
+      if ( inside )
+         for ( int qp = 0; qp < 5; ++qp )
+         {
+            double p[3];
+            for ( int d = 0; d < 3; ++d )
+            {
+               double acc = 0;
+               for ( int j = 0; j < 4; ++j )
+                  acc += ( qp == 0 ? 0.25 : ( j == qp - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][d];
+               p[d] = acc;
+            }
+            s += ( qp == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * coefValue( f, p );
+         }
+      dst[( size_t( cell ) * 6 + t ) * lv.stride + idx] = 24.0 * s;
+   }
+}
+
 // VertexDoFFunction::interpolate(constant, level, flag)
 template < typename T >
 __global__ void k_fill( TopoDev tp, LevelDev lv, T* __restrict__ dst, T value, int flag )
@@ -1761,7 +1887,7 @@ __global__ void k_to_dofs( TopoDev tp, LevelDev lv, const T* __restrict__ slab, 
 // thousand DoFs); scalars stay on the device, so it can be captured in a CUDA graph.
 // status[0] = iterations, status[1] = 1 if converged, 2 if the budget ran out.
 // ---------------------------------------------------------------------------
-template < bool VAR >
+template < int VAR >
 __device__ void cgApplyAll( const TopoDev& tp, const LevelDev& lv, const OpDev< double >& op, const double* src,
                             double* dst, int flag )
 {
@@ -1834,7 +1960,7 @@ __device__ void cgAxpby( const TopoDev& tp, const LevelDev& lv, double a, const 
 }
 
 // the whole CG in the calling thread block; red = 32 doubles of shared memory
-template < bool VAR, bool BLEND = false >
+template < int VAR, bool BLEND = false >
 __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< double >& op, double* x, const double* b,
                         double* r, double* p, double* ap, double tol, int maxIter, int* status, double* red,
                         const RowPass& rp )
@@ -1893,7 +2019,7 @@ __device__ void cgBody( const TopoDev& tp, const LevelDev& lv, const OpDev< doub
    }
 }
 
-template < bool VAR, bool BLEND = false >
+template < int VAR, bool BLEND = false >
 __global__ void __launch_bounds__( 256 ) k_cg( TopoDev tp, LevelDev lv, OpDev< double > op, double* x, const double* b,
                                                 double* r, double* p, double* ap, double tol, int maxIter, int* status,
                                                 RowPass rp )

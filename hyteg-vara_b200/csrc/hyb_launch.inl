@@ -35,6 +35,21 @@ long envLong( const char* name, long dflt )
    const char* e = std::getenv( name );
    return e ? std::atol( e ) : dflt;
 }
+// The VAR template argument of an operator's kernels: 0 constant stencils, 1 variable
+// coefficient from nodal values, 2 variable coefficient at quadrature points. withVar calls
+// f with it as a compile-time constant (std::integral_constant).
+inline int varKind( const Operator& op ) { return !op.variable ? 0 : ( op.kq64.empty() ? 1 : 2 ); }
+template < typename F >
+void withVar( const Operator& op, F&& f )
+{
+   switch ( varKind( op ) )
+   {
+   case 2: f( std::integral_constant< int, 2 >{} ); break;
+   case 1: f( std::integral_constant< int, 1 >{} ); break;
+   default: f( std::integral_constant< int, 0 >{} ); break;
+   }
+}
+
 long rowTableMaxPoints()
 {
    static const long v = envLong( "HYB_ROW_TABLE_MAX_POINTS", kRowTableMaxPoints );
@@ -216,43 +231,26 @@ void launchApply( const Operator& op, int l, const T* src, T* dst, const T* rhs,
          const int     g  = int( std::max< long >( 1, std::min< long >( ( rp.n + 127 ) / 128, long( s.numSMs ) * 8 ) ) );
          T*            u  = const_cast< T* >( src );
 #define HYB_ROWS( M, V ) pdlLaunch( k_row_pass< T, M, V >, dim3( g ), dim3( 128 ), 0, stream, rp, od, u, rhs, dst, T( 0 ), flag )
-         if ( mode == kResidual )
-         {
-            if ( op.variable )
-               HYB_ROWS( kRowResidual, true );
+         withVar( op, [&]( auto V ) {
+            if ( mode == kResidual )
+               HYB_ROWS( kRowResidual, decltype( V )::value );
             else
-               HYB_ROWS( kRowResidual, false );
-         }
-         else
-         {
-            if ( op.variable )
-               HYB_ROWS( kRowApply, true );
-            else
-               HYB_ROWS( kRowApply, false );
-         }
+               HYB_ROWS( kRowApply, decltype( V )::value );
+         } );
 #undef HYB_ROWS
          HYB_CHECK_LAUNCH();
          return;
       }
 #define HYB_APPLY( VAR, MODE ) pdlLaunch( k_apply< T, VAR, MODE >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, flag, nc )
-   if ( op.variable )
-   {
+   withVar( op, [&]( auto V ) {
+      constexpr int var = decltype( V )::value;
       if ( mode == kReplace )
-         HYB_APPLY( true, kReplace );
+         HYB_APPLY( var, kReplace );
       else if ( mode == kAdd )
-         HYB_APPLY( true, kAdd );
+         HYB_APPLY( var, kAdd );
       else
-         HYB_APPLY( true, kResidual );
-   }
-   else
-   {
-      if ( mode == kReplace )
-         HYB_APPLY( false, kReplace );
-      else if ( mode == kAdd )
-         HYB_APPLY( false, kAdd );
-      else
-         HYB_APPLY( false, kResidual );
-   }
+         HYB_APPLY( var, kResidual );
+   } );
 #undef HYB_APPLY
    HYB_CHECK_LAUNCH();
 }
@@ -319,21 +317,19 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       {
          const long b1 = long( co[1] ) * 32, b2 = b1 + ( long( co[2] ) * 8 + 31 ) / 32 * 32;
          const RowPass rp{ R->iface.p + R->ifaceOff[size_t( c )], lanes, b1, b2, lanes };
-         if ( op.variable )
-            pdlLaunch( k_row_pass< T, kRowSor, true >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs, (T*) nullptr,
-                       relax, flag );
-         else
-            pdlLaunch( k_row_pass< T, kRowSor, false >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs, (T*) nullptr,
-                       relax, flag );
+         withVar( op, [&]( auto V ) {
+            pdlLaunch( k_row_pass< T, kRowSor, decltype( V )::value >, dim3( nb ), dim3( 128 ), 0, stream, rp, od, u, rhs,
+                       (T*) nullptr, relax, flag );
+         } );
          HYB_CHECK_LAUNCH();
          return;
       }
       const int32_t*  list = L.colourList.p + co[0];
       const BdryLists bl{ list, list + co[1], list + co[1] + co[2], co[1], co[2], co[3] };
-      if ( op.variable )
-         pdlLaunch( k_sor_iface< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
-      else
-         pdlLaunch( k_sor_iface< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs, relax, flag, bl );
+      withVar( op, [&]( auto V ) {
+         pdlLaunch( k_sor_iface< T, decltype( V )::value >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
+                    relax, flag, bl );
+      } );
       HYB_CHECK_LAUNCH();
    };
    // interior passes
@@ -345,12 +341,10 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
       {
          const int* o  = L.dev.ptsOff;
          const int  bw = backwards ? 1 : 0;
-         if ( op.variable )
-            pdlLaunch( k_sor_interior_cells< T, true >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
-                       relax, o[0], o[1], o[2], o[3], o[4], bw );
-         else
-            pdlLaunch( k_sor_interior_cells< T, false >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td, L.dev, od, u, rhs,
-                       relax, o[0], o[1], o[2], o[3], o[4], bw );
+         withVar( op, [&]( auto V ) {
+            pdlLaunch( k_sor_interior_cells< T, decltype( V )::value >, dim3( s.td.nC ), dim3( 256 ), 0, stream, s.td,
+                       L.dev, od, u, rhs, relax, o[0], o[1], o[2], o[3], o[4], bw );
+         } );
          HYB_CHECK_LAUNCH();
          return;
       }
@@ -361,12 +355,10 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
          const int begin = L.dev.ptsOff[c], count = L.dev.ptsOff[c + 1] - L.dev.ptsOff[c];
          if ( count == 0 )
             continue;
-         if ( op.variable )
-            pdlLaunch( k_sor_interior< T, true >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
-                       relax, c, begin, count, L.colourBlocks );
-         else
-            pdlLaunch( k_sor_interior< T, false >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td, L.dev, od, u, rhs,
-                       relax, c, begin, count, L.colourBlocks );
+         withVar( op, [&]( auto V ) {
+            pdlLaunch( k_sor_interior< T, decltype( V )::value >, dim3( L.colourBlocks ), dim3( 128 ), 0, stream, s.td,
+                       L.dev, od, u, rhs, relax, c, begin, count, L.colourBlocks );
+         } );
          HYB_CHECK_LAUNCH();
       }
    };
@@ -404,10 +396,10 @@ void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs
       HYB_CHECK_LAUNCH();
       return;
    }
-   if ( op.variable )
-      pdlLaunch( k_jacobi< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
-   else
-      pdlLaunch( k_jacobi< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs, relax, flag, nc );
+   withVar( op, [&]( auto V ) {
+      pdlLaunch( k_jacobi< T, decltype( V )::value >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, src, dst, rhs,
+                 relax, flag, nc );
+   } );
    HYB_CHECK_LAUNCH();
 }
 
@@ -485,10 +477,10 @@ bool launchResidualNorm( const Operator& op, int l, const T* x, const T* b, int 
    if ( op.blend || nb < 1 || size_t( nb ) > partialSlots )
       return false;
    const OpDev< T > od = op.dev< T >( l );
-   if ( op.variable )
-      pdlLaunch( k_residual_norm< T, true >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, x, b, flag, nc, partial, cvt );
-   else
-      pdlLaunch( k_residual_norm< T, false >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, x, b, flag, nc, partial, cvt );
+   withVar( op, [&]( auto V ) {
+      pdlLaunch( k_residual_norm< T, decltype( V )::value >, dim3( nb ), dim3( 128 ), 0, stream, s.td, L.dev, od, x, b,
+                 flag, nc, partial, cvt );
+   } );
    HYB_CHECK_LAUNCH();
    pdlLaunch( k_reduce_final, dim3( 1 ), dim3( 1024 ), 0, stream, partial, nb, result );
    HYB_CHECK_LAUNCH();
@@ -540,12 +532,11 @@ void launchCg( const Operator& op, int l, double* x, const double* b, CgScratch&
       return;
    }
    const RowPass         rp = rowPassAll( rowsIf( s, l ) );
-   if ( op.variable )
-      pdlLaunch( k_cg< true >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
-                                             cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
-   else
-      pdlLaunch( k_cg< false >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b, cs.r->ptr< double >( l ), cs.p->ptr< double >( l ),
-                                              cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p, rp );
+   withVar( op, [&]( auto V ) {
+      pdlLaunch( k_cg< decltype( V )::value >, dim3( 1 ), dim3( 256 ), 0, stream, s.td, s.L( l ).dev, od, x, b,
+                 cs.r->ptr< double >( l ), cs.p->ptr< double >( l ), cs.ap->ptr< double >( l ), tol, maxIter, cs.status.p,
+                 rp );
+   } );
    HYB_CHECK_LAUNCH();
 }
 
@@ -601,10 +592,9 @@ void launchInvDiag( const Operator& op, int l, const T* zeros, T* out, cudaStrea
       HYB_CHECK_LAUNCH();
       return;
    }
-   if ( op.variable )
-      k_inv_diag< T, true ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
-   else
-      k_inv_diag< T, false ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
+   withVar( op, [&]( auto V ) {
+      k_inv_diag< T, decltype( V )::value ><<< nb, 128, 0, stream >>>( s.td, L.dev, od, zeros, out, nc );
+   } );
    HYB_CHECK_LAUNCH();
 }
 

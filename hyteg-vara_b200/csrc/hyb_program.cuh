@@ -77,7 +77,7 @@ constexpr int kProgramLevels = 8; // level descriptors staged in shared memory
 // One phase of a program, run by the program's thread blocks (block pb of npb): a row pass
 // spreads its rows over every thread, any other phase steps through its virtual blocks.
 // sL holds the first kProgramLevels level descriptors (staged in shared memory), lvs all.
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __device__ __forceinline__ void runPhase( const TopoDev& tp, const Phase& P, const LevelDev* sL,
                                           const LevelDev* __restrict__ lvs, double* red, int pb, int npb )
 {
@@ -159,7 +159,7 @@ __device__ __forceinline__ void runPhase( const TopoDev& tp, const Phase& P, con
 // first warps loads one 8-byte word of the next descriptor while the current phase runs),
 // and the level descriptors once per launch: a phase then starts without a dependent L2
 // round trip for its own description.
-template < typename T, bool VAR >
+template < typename T, int VAR >
 __global__ void __launch_bounds__( kProgramThreads ) k_program( TopoDev tp, const LevelDev* __restrict__ lvs,
                                                                 const Phase* __restrict__ prog, int nPhases, int nLv )
 {
@@ -232,7 +232,7 @@ __device__ __forceinline__ void dotPhase( const TopoDev& tp, const LevelDev& lv,
       *slot = s;
 }
 
-template < bool VAR >
+template < int VAR >
 __device__ __forceinline__ void solveBatchBody( const SolveJob* jobs )
 {
    constexpr int       nWords = int( sizeof( Phase ) / 8 );

@@ -516,6 +516,9 @@ struct Operator
    std::vector< std::unique_ptr< DevBuf< float > > >  st32, K32;
    std::vector< std::vector< double > >               stHost; // [nC*16*15]
    std::unique_ptr< Function >                        kap64, kap32;
+   // coefficient integrated at quadrature points: per level [nC][6][stride] factors (OpDev::kq)
+   std::vector< std::unique_ptr< DevBuf< double > > > kq64;
+   std::vector< std::unique_ptr< DevBuf< float > > >  kq32;
 
    template < typename T >
    OpDev< T > dev( int l ) const
@@ -538,12 +541,14 @@ struct Operator
          o.st = variable ? nullptr : st64[i]->p;
          o.K  = variable ? K64[i]->p : nullptr;
          o.kap = variable ? kap64->ptr< double >( l ) : nullptr;
+         o.kq  = kq64.empty() ? nullptr : kq64[i]->p;
       }
       else
       {
          o.st = variable ? nullptr : st32[i]->p;
          o.K  = variable ? K32[i]->p : nullptr;
          o.kap = variable ? kap32->ptr< float >( l ) : nullptr;
+         o.kq  = kq32.empty() ? nullptr : kq32[i]->p;
       }
       return o;
    }
@@ -789,6 +794,49 @@ Operator* makeDivKGradRff( Storage* s, int minL, int maxL, const double* w, cons
    dp.upload( std::vector< double >( phase, phase + modes ) );
    std::unique_ptr< Operator > op( makeDivKGradWith( s, minL, maxL, []( int, double* ) {} ) );
    fillRff( *op, dw.p, dp.p, modes, sigma, radial, 0 );
+   HYB_CUDA( cudaDeviceSynchronize() );
+   return op.release();
+}
+
+// The variable-coefficient operator with the coefficient evaluated as the reference's form
+// does it: the callback k at the 5 quadrature points of every micro-tet on every level
+// (p1_div_k_grad_affine_q3::integrateAll, src/hyteg/forms/form_hyteg_generated/p1/
+// p1_div_k_grad_affine_q3.cpp:179+, applied per level by P1ElementwiseOperator.cpp:64-221).
+// k is one of the functions of CoefFn (kind 1 tanh, kind 2 random features); its nodal
+// values are kept as well (for callers that read the operator's coefficient).
+Operator* makeDivKGradQuadrature( Storage* s, int minL, int maxL, int kind, const double* w, const double* phase,
+                                  int modes, double sigma, double radial )
+{
+   require( kind == 1 || kind == 2, "coefficient kind must be 1 (tanh) or 2 (random features)" );
+   require( kind == 1 || ( modes > 0 && w && phase ), "random-feature parameters missing" );
+   DevBuf< double > dw, dp;
+   if ( kind == 2 )
+   {
+      dw.upload( std::vector< double >( w, w + 3 * modes ) );
+      dp.upload( std::vector< double >( phase, phase + modes ) );
+   }
+   const CoefFn f{ kind, kind == 2 ? modes : 0, sigma, radial, dw.p, dp.p };
+   std::unique_ptr< Operator > op( makeDivKGradWith( s, minL, maxL, []( int, double* ) {} ) );
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      const auto&  L = s->L( l );
+      const size_t n = size_t( s->td.nC ) * 6 * L.dev.stride;
+      k_fill_coefficient<<< dim3( L.slabBlocks, s->td.nC ), 256 >>>( L.dev, s->cellCoords.p, s->cellOrder.p,
+                                                                      op->kap64->ptr< double >( l ), f );
+      HYB_CHECK_LAUNCH();
+      launchConvert< float, double >( *s, l, op->kap32->ptr< float >( l ), op->kap64->ptr< double >( l ), 0 );
+      auto q64 = std::make_unique< DevBuf< double > >();
+      auto q32 = std::make_unique< DevBuf< float > >();
+      q64->alloc( n );
+      q32->alloc( n );
+      k_fill_tet_factors<<< dim3( L.slabBlocks, s->td.nC ), 256 >>>( L.dev, s->cellCoords.p, s->cellOrder.p, q64->p, f );
+      HYB_CHECK_LAUNCH();
+      pdlLaunch( k_convert< float, double >, dim3( unsigned( ( n + 255 ) / 256 ) ), dim3( 256 ), 0, 0, L.dev, q32->p,
+                 q64->p, 6 * s->td.nC );
+      HYB_CHECK_LAUNCH();
+      op->kq64.push_back( std::move( q64 ) );
+      op->kq32.push_back( std::move( q32 ) );
+   }
    HYB_CUDA( cudaDeviceSynchronize() );
    return op.release();
 }

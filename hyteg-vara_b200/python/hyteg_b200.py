@@ -32,7 +32,7 @@ SYMBOLS = [
     "hyb_operator_smooth_sor", "hyb_operator_smooth_jac", "hyb_operator_cell_stencil", "hyb_prolongate",
     "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
-    "hyb_operator_create_divkgrad_rff", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
+    "hyb_operator_create_divkgrad_rff", "hyb_operator_create_divkgrad_quadrature", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_server_batch_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
     "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
@@ -115,6 +115,7 @@ def load(path=LIB_PATH):
         "hyb_function_dot_noalloc": (I, [P, P, I, I, P, P]),
         "hyb_function_fill_uniform_random": (I, [P, I, ctypes.c_uint64, D, P]),
         "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, D, PP]),
+        "hyb_operator_create_divkgrad_quadrature": (I, [P, I, I, I, P, P, I, D, D, PP]),
         "hyb_operator_create_blend_divkgrad": (I, [P, I, I, D, PP]),
         "hyb_storage_create_spherical_shell": (I, [I, I, D, D, I, PP]),
         "hyb_gmg_solve_fmg": (I, [P, P, P, I, I, P]),
@@ -402,6 +403,26 @@ class P1ElementwiseDivKGradOperator(_Operator):
         _check(load().hyb_operator_create_divkgrad_rff(storage.h, min_level, max_level, w.ctypes.data,
                                                        phase.ctypes.data, w.shape[0], float(sigma), float(radial),
                                                        ctypes.byref(h)))
+        op.h = h
+        return op
+
+    @classmethod
+    def quadrature(cls, storage, min_level, max_level, kind, w=None, phase=None, sigma=1.0, radial=0.0):
+        """The coefficient callback evaluated as the reference's form does: k at the 5
+        quadrature points of every micro-tet on every level. kind 1: tanh(2 (x - 1/2)) + 2;
+        kind 2: the random-feature field of random_features (w, phase, sigma, radial)."""
+        op = cls.__new__(cls)
+        op.storage = storage
+        h = ctypes.c_void_p()
+        if kind == 2:
+            w = np.ascontiguousarray(w, np.float64).reshape(-1, 3)
+            phase = np.ascontiguousarray(phase, np.float64).ravel()
+            assert w.shape[0] == phase.shape[0]
+            wp, pp, m = w.ctypes.data, phase.ctypes.data, w.shape[0]
+        else:
+            wp, pp, m = None, None, 0
+        _check(load().hyb_operator_create_divkgrad_quadrature(storage.h, min_level, max_level, kind, wp, pp, m,
+                                                              float(sigma), float(radial), ctypes.byref(h)))
         op.h = h
         return op
 

@@ -188,6 +188,18 @@ int hyb_operator_create_divkgrad_callback( hyb_storage* s, int min_level, int ma
  * micro-vertex of every level; blocking */
 int hyb_operator_create_divkgrad_rff( hyb_storage* s, int min_level, int max_level, const double* w,
                                       const double* phase, int modes, double sigma, double radial, hyb_operator** out );
+/* P1ElementwiseOperator< p1_div_k_grad_affine_q3 > with its coefficient callback as the
+ * reference evaluates it (p1_div_k_grad_affine_q3.cpp:179+, per level from
+ * P1ElementwiseOperator.cpp:64-221): k at the 5 quadrature points of every micro-tet on every
+ * level, where the nodal operators above take the level's P1 interpolant. The factors
+ * 24 sum_q w_q k(x_q) are computed once per level on the device and kept (6 values per
+ * closure point and cell, FP64 and FP32), so an application reads one factor per incident
+ * micro-tet. kind 1: k = tanh(2 (x - 1/2)) + 2 (ElementwiseDivKGradCGConvergenceTest's
+ * coefficient; w, phase, modes, sigma, radial ignored); kind 2: the random-feature field of
+ * hyb_operator_create_divkgrad_rff. Every smoother, CG and GMG accept it; blocking */
+int hyb_operator_create_divkgrad_quadrature( hyb_storage* s, int min_level, int max_level, int kind, const double* w,
+                                             const double* phase, int modes, double sigma, double radial,
+                                             hyb_operator** out );
 /* the curved-shell operator: every macro-cell of a spherical-shell mesh gets its
  * IcosahedralShellMap, and the element matrices of p1_div_k_grad_blending_q3 (5-point rule,
  * map Jacobian at the quadrature points) are integrated on the device per row, with
