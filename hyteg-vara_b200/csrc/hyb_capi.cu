@@ -515,6 +515,17 @@ int hyb_operator_create_divkgrad_callback( hyb_storage* s, int minL, int maxL, d
    HYB_API_END
 }
 
+int hyb_operator_create_divkgrad_callback_quadrature( hyb_storage* s, int minL, int maxL,
+                                                      double ( *kfun )( const double*, void* ), void* ctx,
+                                                      hyb_operator** out )
+{
+   HYB_API_BEGIN
+   require( s && out && kfun, "null argument" );
+   require( minL >= 0 && minL <= maxL && maxL <= ST( s )->maxLevel, "invalid level range" );
+   *out = reinterpret_cast< hyb_operator* >( makeDivKGradCallbackQuadrature( ST( s ), minL, maxL, kfun, ctx ) );
+   HYB_API_END
+}
+
 int hyb_operator_create_divkgrad_quadrature( hyb_storage* s, int minL, int maxL, int kind, const double* w,
                                              const double* phase, int modes, double sigma, double radial,
                                              hyb_operator** out )

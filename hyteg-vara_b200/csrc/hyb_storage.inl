@@ -841,6 +841,98 @@ Operator* makeDivKGradQuadrature( Storage* s, int minL, int maxL, int kind, cons
    return op.release();
 }
 
+// The quadrature-point operator with a host callback: for every micro-tet (type t, vertex 0
+// at closure point (x, y, z)) of every cell and level, k at the 5 quadrature points of
+// p1_div_k_grad_affine_q3's rule (centroid, weight -2/15; barycentric (1/2, 1/6, 1/6, 1/6),
+// weight 3/40), the factor 24 sum_q w_q k(x_q) at slab position (cell * 6 + t) * stride +
+// sidx(x, y, z); micro-vertex coordinates v0 + (v_j - v0) i_j / N
+// (vertexdof::macrocell::coordinateFromIndex, VertexDoFMacroCell.hpp:68-75). The nodal values
+// of the same callback are kept as well.
+void dofCoords( const Topology& tp, int l, std::vector< double >& out );
+
+Operator* makeDivKGradCallbackQuadrature( Storage* s, int minL, int maxL, double ( *kfun )( const double*, void* ),
+                                          void* ctx )
+{
+   const Topology& tp = s->topo;
+   std::vector< std::vector< double > > nodal;
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      std::vector< double > xyz;
+      dofCoords( tp, l, xyz );
+      std::vector< double > kv( xyz.size() / 3 );
+      for ( size_t i = 0; i < kv.size(); ++i )
+         kv[i] = kfun( &xyz[3 * i], ctx );
+      nodal.push_back( std::move( kv ) );
+   }
+   std::unique_ptr< Operator > op( makeDivKGrad( s, minL, maxL, nodal ) );
+   const int nC = s->td.nC;
+   // the micro-tet of type t with vertex 0 at a point: role 0 of the incident-tet table
+   int q[6][4];
+   for ( int i = 0; i < 24; ++i )
+   {
+      const IncidentTet it = incidentTet( i );
+      if ( it.k == 0 )
+         for ( int j = 0; j < 4; ++j )
+            q[it.t][j] = it.q[j];
+   }
+   for ( int l = minL; l <= maxL; ++l )
+   {
+      const LevelDev& d = s->L( l ).dev;
+      const int       N = d.N;
+      std::vector< double > f( size_t( nC ) * 6 * d.stride, 0.0 );
+      for ( int c = 0; c < nC; ++c )
+      {
+         const auto& T = tp.T[size_t( c )];
+         double      v0[3], h[3][3];
+         for ( int k = 0; k < 3; ++k )
+         {
+            v0[k] = tp.V[size_t( T[0] )][k];
+            for ( int j = 0; j < 3; ++j )
+               h[j][k] = ( tp.V[size_t( T[j + 1] )][k] - v0[k] ) / N;
+         }
+         for ( int z = 0; z <= N; ++z )
+            for ( int y = 0; y + z <= N; ++y )
+               for ( int x = 0; x + y + z <= N; ++x )
+                  for ( int t = 0; t < 6; ++t )
+                  {
+                     double X[4][3];
+                     bool   inside = true;
+                     for ( int j = 0; j < 4 && inside; ++j )
+                     {
+                        const int xx = x + offX( q[t][j] ), yy = y + offY( q[t][j] ), zz = z + offZ( q[t][j] );
+                        inside       = xx >= 0 && yy >= 0 && zz >= 0 && xx + yy + zz <= N;
+                        for ( int k = 0; k < 3 && inside; ++k )
+                           X[j][k] = v0[k] + h[0][k] * xx + h[1][k] * yy + h[2][k] * zz;
+                     }
+                     if ( !inside )
+                        continue;
+                     double sum = 0;
+                     for ( int qp = 0; qp < 5; ++qp )
+                     {
+                        double p[3];
+                        for ( int k = 0; k < 3; ++k )
+                        {
+                           double acc = 0;
+                           for ( int j = 0; j < 4; ++j )
+                              acc += ( qp == 0 ? 0.25 : ( j == qp - 1 ? 0.5 : 1.0 / 6.0 ) ) * X[j][k];
+                           p[k] = acc;
+                        }
+                        sum += ( qp == 0 ? -2.0 / 15.0 : 3.0 / 40.0 ) * kfun( p, ctx );
+                     }
+                     f[( size_t( c ) * 6 + t ) * d.stride + size_t( sidx( d.W, x, y, z ) )] = 24.0 * sum;
+                  }
+      }
+      auto q64 = std::make_unique< DevBuf< double > >();
+      q64->upload( f );
+      std::vector< float > f32( f.begin(), f.end() );
+      auto q32 = std::make_unique< DevBuf< float > >();
+      q32->upload( f32 );
+      op->kq64.push_back( std::move( q64 ) );
+      op->kq32.push_back( std::move( q32 ) );
+   }
+   return op.release();
+}
+
 // Coordinates of every micro-vertex of a level in the canonical DoF order
 // (vertexdof::macrocell::coordinateFromIndex, VertexDoFMacroCell.hpp:68-75, and its
 // face/edge analogues), evaluated on the host.

@@ -32,7 +32,8 @@ SYMBOLS = [
     "hyb_operator_smooth_sor", "hyb_operator_smooth_jac", "hyb_operator_cell_stencil", "hyb_prolongate",
     "hyb_restrict", "hyb_cg_solve", "hyb_gmg_create", "hyb_gmg_destroy", "hyb_gmg_solve",
     "hyb_gmg_solve_to_tolerance", "hyb_function_dot_noalloc", "hyb_function_fill_uniform_random",
-    "hyb_operator_create_divkgrad_rff", "hyb_operator_create_divkgrad_quadrature", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
+    "hyb_operator_create_divkgrad_rff", "hyb_operator_create_divkgrad_quadrature",
+    "hyb_operator_create_divkgrad_callback_quadrature", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_server_batch_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
     "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
@@ -58,6 +59,8 @@ class RequestResult(ctypes.Structure):
                 ("footprint_bytes", ctypes.c_size_t)]
 
 _lib = None
+# double k(const double* xyz, void* ctx): a coefficient callback
+KFUN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
 
 
 class HybError(RuntimeError):
@@ -116,6 +119,7 @@ def load(path=LIB_PATH):
         "hyb_function_fill_uniform_random": (I, [P, I, ctypes.c_uint64, D, P]),
         "hyb_operator_create_divkgrad_rff": (I, [P, I, I, P, P, I, D, D, PP]),
         "hyb_operator_create_divkgrad_quadrature": (I, [P, I, I, I, P, P, I, D, D, PP]),
+        "hyb_operator_create_divkgrad_callback_quadrature": (I, [P, I, I, KFUN, P, PP]),
         "hyb_operator_create_blend_divkgrad": (I, [P, I, I, D, PP]),
         "hyb_storage_create_spherical_shell": (I, [I, I, D, D, I, PP]),
         "hyb_gmg_solve_fmg": (I, [P, P, P, I, I, P]),
@@ -403,6 +407,19 @@ class P1ElementwiseDivKGradOperator(_Operator):
         _check(load().hyb_operator_create_divkgrad_rff(storage.h, min_level, max_level, w.ctypes.data,
                                                        phase.ctypes.data, w.shape[0], float(sigma), float(radial),
                                                        ctypes.byref(h)))
+        op.h = h
+        return op
+
+    @classmethod
+    def callback_quadrature(cls, storage, min_level, max_level, k):
+        """Any coefficient k(xyz) -> float, called on the host at the 5 quadrature points of
+        every micro-tet on every level (the reference form's callback semantics)."""
+        op = cls.__new__(cls)
+        op.storage = storage
+        op._kfun = KFUN(lambda xyz, ctx: float(k(np.ctypeslib.as_array(xyz, shape=(3,)))))
+        h = ctypes.c_void_p()
+        _check(load().hyb_operator_create_divkgrad_callback_quadrature(storage.h, min_level, max_level, op._kfun,
+                                                                       None, ctypes.byref(h)))
         op.h = h
         return op
 

@@ -200,6 +200,12 @@ int hyb_operator_create_divkgrad_rff( hyb_storage* s, int min_level, int max_lev
 int hyb_operator_create_divkgrad_quadrature( hyb_storage* s, int min_level, int max_level, int kind, const double* w,
                                              const double* phase, int modes, double sigma, double radial,
                                              hyb_operator** out );
+/* The same with any coefficient callback k(x) (P1ElementwiseOperator< p1_div_k_grad_affine_q3 >
+ * with form(callback)): k is called on the host at the 5 quadrature points of every micro-tet
+ * of every level (and at every micro-vertex, for the nodal values); blocking */
+int hyb_operator_create_divkgrad_callback_quadrature( hyb_storage* s, int min_level, int max_level,
+                                                      double ( *k )( const double* xyz, void* ctx ), void* ctx,
+                                                      hyb_operator** out );
 /* the curved-shell operator: every macro-cell of a spherical-shell mesh gets its
  * IcosahedralShellMap, and the element matrices of p1_div_k_grad_blending_q3 (5-point rule,
  * map Jacobian at the quadrature points) are integrated on the device per row, with

@@ -228,21 +228,34 @@ class P1ConstantLaplaceOperator : public P1OperatorBase
 };
 
 // P1ElementwiseOperator< forms::p1_div_k_grad_affine_q3 > with the coefficient as a callback
+/// Where the coefficient callback is evaluated: at every micro-vertex (its P1 interpolant
+/// integrated exactly; the fast default), or at the 5 quadrature points of every micro-tet as
+/// the reference's p1_div_k_grad_affine_q3 form does (the reference's element matrices).
+enum class CoefficientAt
+{
+   Vertices,
+   QuadraturePoints
+};
+
 class P1ElementwiseDivKGradOperator : public P1OperatorBase
 {
  public:
    using srcType = P1Function< double >;
    P1ElementwiseDivKGradOperator( const std::shared_ptr< PrimitiveStorage >& storage, int minLevel, int maxLevel,
-                                  double ( *k )( const double* xyz, void* ctx ), void* ctx = nullptr )
+                                  double ( *k )( const double* xyz, void* ctx ), void* ctx = nullptr,
+                                  CoefficientAt at = CoefficientAt::Vertices )
    {
-      hybCheck( hyb_operator_create_divkgrad_callback( storage->handle(), minLevel, maxLevel, k, ctx, &h_ ) );
+      if ( at == CoefficientAt::QuadraturePoints )
+         hybCheck( hyb_operator_create_divkgrad_callback_quadrature( storage->handle(), minLevel, maxLevel, k, ctx, &h_ ) );
+      else
+         hybCheck( hyb_operator_create_divkgrad_callback( storage->handle(), minLevel, maxLevel, k, ctx, &h_ ) );
    }
 };
 
 /// P1ElementwiseBlendingDivKGradOperator on a spherical-shell storage whose cells carry the
 /// IcosahedralShellMap (the reference sets it with IcosahedralShellMap::setMap); the
 /// coefficient is k(y) = exp( alpha (1 - |y|) ) at the mapped quadrature points, alpha = 0
-/// gives the shell's Laplacian. Levels up to 6.
+/// gives the shell's Laplacian. Levels up to 7.
 class P1ElementwiseBlendingDivKGradOperator : public P1OperatorBase
 {
  public:

@@ -134,3 +134,22 @@ def test_reference_cg_convergence_with_reference_coefficient_semantics(oracle_mo
     uo = u0.copy()
     orc.cg(uo, f, level, tol=1e-12, max_iter=1000, op=orc.op_divkgrad_callback(1))
     close(u, uo, 1e-9)
+
+
+def test_host_callback_quadrature_matches_oracle_and_device_factors(cube):
+    """Any coefficient callback, evaluated on the host at every micro-tet's quadrature points
+    (hyb_operator_create_divkgrad_callback_quadrature): with tanh(2 (x - 1/2)) + 2 its apply
+    matches the oracle's callback operator (1e-12) and the device-evaluated kind 1 (1e-13)."""
+    H, st, orc, L, w, ph = cube
+    A = H.P1ElementwiseDivKGradOperator.callback_quadrature(st, 0, L, lambda p: np.tanh(2.0 * (p[0] - 0.5)) + 2.0)
+    Ad = H.P1ElementwiseDivKGradOperator.quadrature(st, 0, L, 1)
+    op = orc.op_divkgrad_callback(1)
+    rng = np.random.default_rng(41)
+    for level in range(L + 1):
+        x = rng.uniform(-1, 1, orc.n(level))
+        fs, fd, fe = (H.P1Function(n, st, 0, L) for n in "sde")
+        fs.set(x, level)
+        A.apply(fs, fd, level, H.ALL)
+        Ad.apply(fs, fe, level, H.ALL)
+        close(fd.get(level), orc.apply(x, level, flag=H.ALL, op=op), 1e-12)
+        close(fd.get(level), fe.get(level), 1e-13)
