@@ -819,8 +819,12 @@ int hyb_gmg_set_cycle_type( hyb_gmg* gh, int cycleType )
    HYB_CUDA( cudaDeviceSynchronize() );
    for ( auto& gr : g->graphs )
       cudaGraphExecDestroy( gr.exec );
+   for ( auto& gr : g->loops )
+      cudaGraphExecDestroy( gr.exec );
    g->graphs.clear();
+   g->loops.clear();
    g->programs.clear();
+   g->solvePrograms.clear();
    g->cycleType = cycleType;
    HYB_API_END
 }
