@@ -660,6 +660,25 @@ int hyb_operator_smooth_sor_backwards( hyb_operator* oh, hyb_function* dh, hyb_f
    HYB_API_END
 }
 
+int hyb_operator_smooth_sor_reference_order( hyb_operator* oh, hyb_function* dh, hyb_function* rh, double relax,
+                                             int level, int flag, int backwards, void* stream )
+{
+   HYB_API_BEGIN
+   Operator* op = OP( oh );
+   Function *u = FN( dh ), *b = FN( rh );
+   checkOpFn( op, u, level );
+   checkOpFn( op, b, level );
+   require( u != b, "smooth_sor_reference_order needs distinct dst and rhs" );
+   require( u->dtype == b->dtype, "dtypes differ" );
+   if ( u->dtype == HYB_F64 )
+      launchSorReference< double >( *op, level, u->ptr< double >( level ), b->ptr< double >( level ), relax, flag,
+                                    op->st->snapScratch< double >( level ), S( stream ), backwards != 0 );
+   else
+      launchSorReference< float >( *op, level, u->ptr< float >( level ), b->ptr< float >( level ), float( relax ), flag,
+                                   op->st->snapScratch< float >( level ), S( stream ), backwards != 0 );
+   HYB_API_END
+}
+
 int hyb_operator_smooth_jac( hyb_operator* oh, hyb_function* dh, hyb_function* rh, hyb_function* sh, double relax, int level,
                              int flag, void* stream )
 {
@@ -756,7 +775,8 @@ int hyb_gmg_create( hyb_storage* s, hyb_operator* oh, int minL, int maxL, int pr
    require( minL >= op->minL && maxL <= op->maxL && minL <= maxL, "GMG levels outside the operator's level range" );
    require( pre >= 0 && post >= 0, "smoothing steps must be non-negative" );
    require( smoother == HYB_SMOOTHER_SOR || smoother == HYB_SMOOTHER_JACOBI || smoother == HYB_SMOOTHER_SYMMETRIC_SOR ||
-                smoother == HYB_SMOOTHER_CHEBYSHEV,
+                smoother == HYB_SMOOTHER_CHEBYSHEV || smoother == HYB_SMOOTHER_SOR_REFERENCE_ORDER ||
+                smoother == HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER,
             "unknown smoother" );
    auto g = std::make_unique< hyb_gmg_s >();
    initGmg( *g, ST( s ), op, minL, maxL, pre, post, relax, smoother, coarseTol, coarseMaxIter );

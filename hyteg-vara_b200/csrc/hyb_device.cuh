@@ -81,6 +81,17 @@ struct LevelDev
    int            nQuads;
    const int32_t* quads;
    const int32_t* rowYZ;
+   // Hyperplanes of the reference-order (lexicographic) SOR: the cell-interior points
+   // x | y << 10 | z << 20 grouped by t = x + 2y + 3z (hyperplane t at [lexCellOff[t],
+   // lexCellOff[t + 1])), and the face-interior points i | j << 16 grouped by t = i + 2j. Every
+   // stencil coupling changes t in the direction of the lexicographic order (x fastest, then
+   // y, then z; in a face i, then j), so updating the hyperplanes in increasing t equals the
+   // lexicographic sweep, and the points of one hyperplane are independent.
+   int            nLexCellT, nLexFaceT;
+   const int32_t* lexCell;
+   const int32_t* lexCellOff;
+   const int32_t* lexFace;
+   const int32_t* lexFaceOff;
 };
 
 // 15 stencil offsets, order shared with the oracle and the C ABI

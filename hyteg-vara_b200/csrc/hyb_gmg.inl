@@ -232,6 +232,14 @@ void smooth( Gmg& g, int l, T* x, const T* b, T* scratch, cudaStream_t stream )
       launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream );
       launchSor< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, stream, true );
    }
+   else if ( g.smoother == HYB_SMOOTHER_SOR_REFERENCE_ORDER || g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER )
+   {
+      // the reference's own sweep order; scratch (the solver's residual vector) holds the
+      // start-of-sweep snapshot
+      launchSorReference< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, scratch, stream, false );
+      if ( g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER )
+         launchSorReference< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, scratch, stream, true );
+   }
    else if ( g.smoother == HYB_SMOOTHER_CHEBYSHEV )
    {
       // ChebyshevSmoother::solve (ChebyshevSmoother.hpp:49-96): t = D^-1 (b - A x), x += w_0 t,
@@ -736,8 +744,9 @@ void initGmg( Gmg& g, Storage* s, Operator* op, int minL, int maxL, int pre, int
    for ( int l = minL; l <= maxL; ++l )
       if ( long( s->td.nC ) * s->L( l ).dev.stride <= maxPoints )
          g.progTop = l;
-   if ( smoother == HYB_SMOOTHER_CHEBYSHEV )
-      g.progTop = -1; // the program kernel has no Chebyshev phases
+   if ( smoother == HYB_SMOOTHER_CHEBYSHEV || smoother == HYB_SMOOTHER_SOR_REFERENCE_ORDER ||
+        smoother == HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER )
+      g.progTop = -1; // the program kernel has no Chebyshev or reference-order SOR phases
    if ( op->blend )
       g.progTop = -1; // blending operators run every level as row-pass launches
    if ( varKind( *op ) == 2 )

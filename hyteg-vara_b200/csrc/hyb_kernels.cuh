@@ -1233,6 +1233,230 @@ __global__ void __launch_bounds__( 256 ) k_sor_interior_cells( TopoDev tp, Level
 }
 
 // ---------------------------------------------------------------------------
+// Reference-order SOR (P1Operator::smooth_sor, P1Operator.hpp:352-422; smooth_sor_backwards
+// :385-400): the staged lexicographic sweep V -> E -> F -> C of the reference, in which a
+// macro-vertex, -edge or -face reads its own closure's current values and every other DoF as
+// it was at the start of the sweep (the ghost layers filled before it), and a macro-cell
+// reads its whole closure current. The stages run as kernels on the level and on `snap`, a
+// copy of the level taken when the sweep starts (and again before each of the last three
+// stages of a backward sweep):
+//   vertices: independent given the snapshot (lane groups);
+//   edges:    a warp per edge walks its points in order, a lane per adjacent cell;
+//   faces:    a block per face walks the hyperplanes t = i + 2j of its points;
+//   cells:    a block per cell walks the hyperplanes t = x + 2y + 3z (LevelDev::lexCell).
+// The hyperplane orders equal the lexicographic order on every coupled pair, so the result
+// is the reference's sweep up to the summation order of a row.
+// ---------------------------------------------------------------------------
+
+// partialRow of (x, y, z) in `cell` with neighbour q read from the cell's slab of u when
+// own(b0, b1, b2, b3) holds for its barycentric micro-coordinates, else from snap's
+template < typename T, int VAR, typename Own >
+__device__ __forceinline__ void partialRowSel( const OpDev< T >& op, const T* u, const T* snap, int cell, int W, int x,
+                                               int y, int z, Own&& own, T& diag, T& off )
+{
+   const int         N     = W - 1;
+   const int         mask  = classMask( N, x, y, z );
+   const uint32_t    valid = kValidOffsets[mask];
+   const StencilRows R     = stencilRows( W, y, z );
+   int               pos[15];
+   bool              cur[15];
+#pragma unroll
+   for ( int q = 0; q < 15; ++q )
+   {
+      const int xq = x + offX( q ), yq = y + offY( q ), zq = z + offZ( q ), k = offRow( q );
+      const bool v = ( valid & ( 1u << q ) ) != 0;
+      pos[q]       = v ? R.start[k] + resOff( xq & 3, R.len[k] ) + ( xq >> 2 ) : 0;
+      cur[q]       = v && own( N - xq - yq - zq, xq, yq, zq );
+   }
+   auto val = [&]( int q ) { return cur[q] ? u[pos[q]] : snap[pos[q]]; };
+   if constexpr ( !VAR )
+   {
+      const T* st = op.st + ( size_t( cell ) * 16 + mask ) * 15;
+      diag += st[0];
+#pragma unroll
+      for ( int q = 1; q < 15; ++q )
+         if ( valid & ( 1u << q ) )
+            off += st[q] * val( q );
+   }
+   else
+   {
+      const T*       kv     = op.kap + size_t( cell ) * op.stride;
+      const T*       K      = op.K + size_t( cell ) * 96;
+      const uint32_t validT = kValidTets[mask];
+#pragma unroll
+      for ( int i = 0; i < 24; ++i )
+      {
+         const IncidentTet it = incidentTet( i );
+         if ( !( validT & ( 1u << i ) ) )
+            continue;
+         T ks;
+         if constexpr ( VAR == 2 )
+            ks = op.kq[( size_t( cell ) * 6 + it.t ) * op.stride + pos[it.q[0]]];
+         else
+            ks = kv[pos[it.q[0]]] + kv[pos[it.q[1]]] + kv[pos[it.q[2]]] + kv[pos[it.q[3]]];
+         const T* Kr = K + it.t * 16 + it.k * 4;
+#pragma unroll
+         for ( int j = 0; j < 4; ++j )
+         {
+            if ( j == it.k )
+               diag += ks * Kr[j];
+            else
+               off += ks * Kr[j] * val( it.q[j] );
+         }
+      }
+   }
+}
+
+// vertex stage: every vertex from the snapshot (its own value is the snapshot's too)
+template < typename T, int VAR >
+__global__ void __launch_bounds__( 128 ) k_sorref_vertices( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                            const T* __restrict__ snap, const T* __restrict__ rhs, T relax,
+                                                            int flag )
+{
+   const Blk       vb          = launchBlk();
+   const int       nCellBlocks = 0;
+   const BdryLists bl{ nullptr, nullptr, nullptr, tp.nV, 0, 0 };
+   HYB_BDRY_LANES( bl )
+   {
+      const LaneTask  tk     = laneTask( tp, lv, bl, gt );
+      const BdryPoint p      = decodeBdry( tp, lv, tk.t );
+      const bool      active = tk.valid && ( primBc( tp, p.kind, p.prim ) & flag );
+      T               diag, off;
+      bdryRowGroup< T, VAR >( tp, lv, op, snap, p, tk, active, diag, off );
+      if ( !active )
+         continue;
+      const size_t r0 = bdryReplica< T >( tp, lv, p, 0 );
+      bdryWriteGroup( tp, lv, p, tk, u, ( T( 1 ) - relax ) * snap[r0] + relax * ( rhs[r0] - off ) / diag );
+   }
+}
+
+// edge stage: warp w of the grid takes edge w and walks its points i = 1 .. N-1 (backwards:
+// N-1 .. 1); lane l takes the edge's embeddings l, l + 32, ...
+template < typename T, int VAR >
+__global__ void __launch_bounds__( 128 ) k_sorref_edges( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                         const T* __restrict__ snap, const T* __restrict__ rhs, T relax,
+                                                         int flag, int backwards )
+{
+   const int e    = int( ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5 );
+   const int lane = int( threadIdx.x & 31 );
+   if ( e >= tp.nE || lv.N < 2 || !( primBc( tp, 1, e ) & flag ) )
+      return;
+   const int ne = numEmb( tp, 1, e );
+   for ( int s = 0; s < lv.N - 1; ++s )
+   {
+      const int i    = backwards ? lv.N - 1 - s : s + 1;
+      T         diag = 0, off = 0;
+      for ( int k = lane; k < ne; k += 32 )
+      {
+         const int32_t packed = embAt( tp, 1, e, k );
+         const int     k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3;
+         // the edge's closure in this cell: barycentric coordinates zero off k0 and k1
+         auto own = [&]( int b0, int b1, int b2, int b3 ) {
+            const int b[4] = { b0, b1, b2, b3 };
+            for ( int m = 0; m < 4; ++m )
+               if ( m != k0 && m != k1 && b[m] != 0 )
+                  return false;
+            return true;
+         };
+         int c, x, y, z;
+         embeddingCoords( packed, 1, lv.N, i, 0, c, x, y, z );
+         partialRowSel< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z, own,
+                                  diag, off );
+      }
+      diag            = groupSum( diag, 32 );
+      off             = groupSum( off, 32 );
+      const BdryPoint p{ 1, e, i, 0 };
+      const size_t    r0 = bdryReplica< T >( tp, lv, p, 0 );
+      const T         v  = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
+      __syncwarp();
+      for ( int k = lane; k < ne; k += 32 )
+         u[bdryReplica< T >( tp, lv, p, k )] = v;
+      __syncwarp(); // the next point reads this one's replicas
+   }
+}
+
+// face stage: block f takes face f and walks its hyperplanes t = i + 2j (backwards: the
+// reverse); two lanes per point, one per adjacent cell
+template < typename T, int VAR >
+__global__ void __launch_bounds__( 256 ) k_sorref_faces( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                         const T* __restrict__ snap, const T* __restrict__ rhs, T relax,
+                                                         int flag, int backwards )
+{
+   const int f = int( blockIdx.x );
+   if ( !( primBc( tp, 2, f ) & flag ) )
+      return;
+   const int     sub    = int( threadIdx.x & 1 );
+   const int     ne     = numEmb( tp, 2, f );
+   const int32_t packed = sub < ne ? embAt( tp, 2, f, sub ) : 0;
+   const int     k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3, k2 = ( packed >> 28 ) & 3;
+   const int     o  = 6 - k0 - k1 - k2; // the cell-local vertex opposite the face
+   auto          own = [&]( int b0, int b1, int b2, int b3 ) {
+      const int b[4] = { b0, b1, b2, b3 };
+      return b[o] == 0;
+   };
+   const int pairs = int( blockDim.x >> 1 );
+   for ( int s = 0; s < lv.nLexFaceT; ++s )
+   {
+      const int t  = backwards ? lv.nLexFaceT - 1 - s : s;
+      const int p0 = lv.lexFaceOff[t], p1 = lv.lexFaceOff[t + 1];
+      // whole warps take the same number of rounds, so the pair sums run on full warps
+      const int rounds = ( p1 - p0 + pairs - 1 ) / pairs;
+      for ( int r = 0; r < rounds; ++r )
+      {
+         const int  k     = p0 + r * pairs + int( threadIdx.x >> 1 );
+         const bool valid = k < p1;
+         T          diag = 0, off = 0;
+         size_t     rep = 0;
+         if ( valid && sub < ne )
+         {
+            const int32_t ij = lv.lexFace[k];
+            int           c, x, y, z;
+            embeddingCoords( packed, 2, lv.N, ij & 0xffff, ij >> 16, c, x, y, z );
+            rep = size_t( c ) * lv.stride + sidx( lv.W, x, y, z );
+            partialRowSel< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z,
+                                     own, diag, off );
+         }
+         diag             = groupSum( diag, 2 );
+         off              = groupSum( off, 2 );
+         const size_t r0  = __shfl_sync( 0xffffffffu, rep, int( threadIdx.x & 30 ) );
+         T            v   = 0;
+         if ( valid )
+            v = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
+         __syncwarp();
+         if ( valid && sub < ne )
+            u[rep] = v;
+      }
+      __syncthreads(); // the next hyperplane reads this one's values
+   }
+}
+
+// cell stage: block c takes cell c's interior and walks its hyperplanes t = x + 2y + 3z
+// (backwards: the reverse), reading its closure current; interior points are Inner
+template < typename T, int VAR >
+__global__ void __launch_bounds__( 256 ) k_sorref_cells( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                         const T* __restrict__ rhs, T relax, int backwards )
+{
+   const int c  = int( blockIdx.x );
+   T*        uc = u + size_t( c ) * lv.stride;
+   const T*  bc = rhs + size_t( c ) * lv.stride;
+   for ( int s = 0; s < lv.nLexCellT; ++s )
+   {
+      const int t  = backwards ? lv.nLexCellT - 1 - s : s;
+      const int p0 = lv.lexCellOff[t], p1 = lv.lexCellOff[t + 1];
+      for ( int k = p0 + int( threadIdx.x ); k < p1; k += int( blockDim.x ) )
+      {
+         const int32_t xyz = lv.lexCell[k];
+         const int     x = xyz & 1023, y = ( xyz >> 10 ) & 1023, z = xyz >> 20;
+         T             diag = 0, off = 0;
+         partialRow< T, VAR >( op, uc, c, lv.W, x, y, z, diag, off );
+         const int i = sidx( lv.W, x, y, z );
+         uc[i]       = ( T( 1 ) - relax ) * uc[i] + relax * ( bc[i] - off ) / diag;
+      }
+      __syncthreads();
+   }
+}
+
+// ---------------------------------------------------------------------------
 // diag(A)^-1 at every closure point (all replicas; the full row's diagonal for macro-
 // primitive DoFs). zeros: a zero vector of the level, read as the operand of the rows
 // whose off-diagonal part is discarded. Cells' interiors on the first nCellBlocks blocks.

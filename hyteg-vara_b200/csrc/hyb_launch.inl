@@ -378,6 +378,78 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
    }
 }
 
+// Reference-order SOR (k_sorref_*): the staged lexicographic sweep of the reference's
+// smooth_sor / smooth_sor_backwards (P1Operator.hpp:352-431). snap is a level-sized scratch
+// in T that takes the start-of-sweep copy (and, backwards, the copy before each later
+// stage). Macro-cell interiors are Inner DoFs: they move when flag has HYB_INNER.
+template < typename T >
+void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, T* snap, cudaStream_t stream,
+                         bool backwards )
+{
+   require( !op.blend, "the reference-order SOR takes the stencil and coefficient operators" );
+   const Storage&   s     = *op.st;
+   const auto&      L     = s.L( l );
+   const OpDev< T > od    = op.dev< T >( l );
+   const size_t     bytes = size_t( s.td.nC ) * L.dev.stride * sizeof( T );
+   const int        bw    = backwards ? 1 : 0;
+   auto snapshot = [&]() { HYB_CUDA( cudaMemcpyAsync( snap, u, bytes, cudaMemcpyDeviceToDevice, stream ) ); };
+   auto vertices = [&]() {
+      if ( s.td.nV == 0 )
+         return;
+      withVar( op, [&]( auto V ) {
+         k_sorref_vertices< T, decltype( V )::value ><<< ( s.td.nV * 32 + 127 ) / 128, 128, 0, stream >>>(
+             s.td, L.dev, od, u, snap, rhs, relax, flag );
+      } );
+      HYB_CHECK_LAUNCH();
+   };
+   auto edges = [&]() {
+      if ( s.td.nE == 0 || L.dev.N < 2 )
+         return;
+      withVar( op, [&]( auto V ) {
+         k_sorref_edges< T, decltype( V )::value ><<< ( s.td.nE * 32 + 127 ) / 128, 128, 0, stream >>>(
+             s.td, L.dev, od, u, snap, rhs, relax, flag, bw );
+      } );
+      HYB_CHECK_LAUNCH();
+   };
+   auto faces = [&]() {
+      if ( s.td.nF == 0 || L.dev.nIntFace == 0 )
+         return;
+      withVar( op, [&]( auto V ) {
+         k_sorref_faces< T, decltype( V )::value ><<< s.td.nF, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax,
+                                                                                   flag, bw );
+      } );
+      HYB_CHECK_LAUNCH();
+   };
+   auto cells = [&]() {
+      if ( !( flag & HYB_INNER ) || L.dev.nPts == 0 )
+         return;
+      withVar( op, [&]( auto V ) {
+         k_sorref_cells< T, decltype( V )::value ><<< s.td.nC, 256, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, bw );
+      } );
+      HYB_CHECK_LAUNCH();
+   };
+   snapshot();
+   if ( !backwards )
+   {
+      vertices();
+      edges();
+      faces();
+      cells();
+   }
+   else
+   {
+      // C -> F -> E -> V with the ghost layers (here: the snapshot) refreshed before each of
+      // the last three stages
+      cells();
+      snapshot();
+      faces();
+      snapshot();
+      edges();
+      snapshot();
+      vertices();
+   }
+}
+
 template < typename T >
 void launchJacobi( const Operator& op, int l, const T* src, T* dst, const T* rhs, T relax, int flag, cudaStream_t stream )
 {

@@ -19,6 +19,8 @@ INNER, DIRICHLET, NEUMANN, FREESLIP, ALL = 1, 2, 4, 8, 15
 REPLACE, ADD = 0, 1
 F64, F32 = 0, 1
 SMOOTHER_SOR, SMOOTHER_JACOBI, SMOOTHER_SYMMETRIC_SOR, SMOOTHER_CHEBYSHEV = 0, 1, 2, 3
+# SORSmoother / SymmetricSORSmoother in the reference's own sweep order
+SMOOTHER_SOR_REFERENCE_ORDER, SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER = 4, 5
 CYCLE_V, CYCLE_W = 0, 1
 
 # the C ABI symbols (include/hyteg_b200.h); tests check that the library exports all of them
@@ -36,7 +38,7 @@ SYMBOLS = [
     "hyb_operator_create_divkgrad_callback_quadrature", "hyb_operator_create_blend_divkgrad", "hyb_server_create", "hyb_server_destroy", "hyb_server_footprint",
     "hyb_server_submit", "hyb_server_run", "hyb_server_result", "hyb_server_stats", "hyb_server_batch_stats", "hyb_rff_features",
     "hyb_storage_create_spherical_shell", "hyb_gmg_solve_fmg", "hyb_storage_create_from_gmsh",
-    "hyb_operator_smooth_sor_backwards", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
+    "hyb_operator_smooth_sor_backwards", "hyb_operator_smooth_sor_reference_order", "hyb_gmg_set_cycle_type", "hyb_gmg_setup_chebyshev",
     "hyb_gmg_set_timing", "hyb_gmg_timing_json", "hyb_gmg_timing_reset",
     "hyb_chebyshev_coefficients", "hyb_operator_estimate_spectral_radius", "hyb_server_mesh_bytes",
 ]
@@ -125,6 +127,7 @@ def load(path=LIB_PATH):
         "hyb_gmg_solve_fmg": (I, [P, P, P, I, I, P]),
         "hyb_storage_create_from_gmsh": (I, [ctypes.c_char_p, I, PP]),
         "hyb_operator_smooth_sor_backwards": (I, [P, P, P, D, I, I, P]),
+        "hyb_operator_smooth_sor_reference_order": (I, [P, P, P, D, I, I, I, P]),
         "hyb_gmg_set_cycle_type": (I, [P, I]),
         "hyb_gmg_set_timing": (I, [P, I]),
         "hyb_gmg_timing_json": (I, [P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
@@ -350,6 +353,12 @@ class _Operator:
     def smooth_sor_backwards(self, dst, rhs, relax, level, flag, stream=None):
         _check(load().hyb_operator_smooth_sor_backwards(self.h, dst.h, rhs.h, float(relax), level, flag,
                                                         _stream(stream)))
+
+    def smooth_sor_reference_order(self, dst, rhs, relax, level, flag, backwards=False, stream=None):
+        """One SOR sweep in the reference's V -> E -> F -> C lexicographic order
+        (smooth_sor / smooth_sor_backwards, P1Operator.hpp:352-431)."""
+        _check(load().hyb_operator_smooth_sor_reference_order(self.h, dst.h, rhs.h, float(relax), level, flag,
+                                                              int(bool(backwards)), _stream(stream)))
 
     def smooth_gs(self, dst, rhs, level, flag, stream=None):
         self.smooth_sor(dst, rhs, 1.0, level, flag, stream)

@@ -27,6 +27,8 @@
  *   hyb_operator_apply            Operator::apply(src, dst, level, flag, updateType) (P1Operator.hpp:196)
  *   hyb_operator_smooth_sor       SORSmoothable::smooth_sor(dst, rhs, relax, level, flag) (P1Operator.hpp:343-422)
  *   hyb_operator_smooth_sor_backwards  SORBackwardsSmoothable::smooth_sor_backwards (P1Operator.hpp:424-431)
+ *   hyb_operator_smooth_sor_reference_order  smooth_sor / smooth_sor_backwards in the reference's
+ *                                 own V -> E -> F -> C lexicographic order (P1Operator.hpp:352-431)
  *   hyb_operator_smooth_jac       WeightedJacobiSmoothable::smooth_jac (P1Operator.hpp:424-440)
  *   hyb_prolongate                P1toP1LinearProlongation::prolongate / prolongateAndAdd
  *                                 (src/hyteg/gridtransferoperators/P1toP1LinearProlongation.cpp:194-410)
@@ -90,6 +92,10 @@ typedef enum
 /* ChebyshevSmoother (src/hyteg/solvers/ChebyshevSmoother.hpp): x += p(D^-1 A) D^-1 (b - A x),
  * coefficients from hyb_gmg_setup_chebyshev before the first solve */
 #define HYB_SMOOTHER_CHEBYSHEV 3
+/* SORSmoother / SymmetricSORSmoother with the reference's own sweep order
+ * (hyb_operator_smooth_sor_reference_order) instead of the multicolour order */
+#define HYB_SMOOTHER_SOR_REFERENCE_ORDER 4
+#define HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER 5
 /* multigrid cycle types (GeometricMultigridSolver.hpp CycleType) */
 #define HYB_CYCLE_V 0
 #define HYB_CYCLE_W 1
@@ -228,6 +234,13 @@ int hyb_operator_smooth_sor( hyb_operator* op, hyb_function* dst, hyb_function* 
  * order (interior colours 3..0, then the surface colours m-1..0) */
 int hyb_operator_smooth_sor_backwards( hyb_operator* op, hyb_function* dst, hyb_function* rhs, double relax, int level,
                                        int flag, void* stream );
+/* one SOR sweep in the reference's order (P1Operator.hpp:352-431): macro-vertices, -edges,
+ * -faces, then -cells (backwards != 0: cells, faces, edges, vertices), each primitive
+ * lexicographic (backwards: reversed) and reading its own closure's current values and every
+ * other DoF as it was when the sweep (backwards: the stage) began; stencil and coefficient
+ * operators (not the blending operator) */
+int hyb_operator_smooth_sor_reference_order( hyb_operator* op, hyb_function* dst, hyb_function* rhs, double relax,
+                                             int level, int flag, int backwards, void* stream );
 /* dst = src + relax * diag(A)^-1 (rhs - A src) */
 int hyb_operator_smooth_jac( hyb_operator* op, hyb_function* dst, hyb_function* rhs, hyb_function* src, double relax,
                              int level, int flag, void* stream );

@@ -188,6 +188,15 @@ class P1OperatorBase
    {
       hybCheck( hyb_operator_smooth_sor_backwards( h_, dst.handle(), rhs.handle(), double( relax ), level, flag, nullptr ) );
    }
+   // smooth_sor / smooth_sor_backwards in the reference's own staged lexicographic order
+   // (macro-vertices, -edges, -faces, -cells) instead of the multicolour order
+   template < typename V >
+   void smooth_sor_reference_order( const P1Function< V >& dst, const P1Function< V >& rhs, V relax, int level,
+                                    DoFType flag, bool backwards = false ) const
+   {
+      hybCheck( hyb_operator_smooth_sor_reference_order( h_, dst.handle(), rhs.handle(), double( relax ), level, flag,
+                                                         backwards ? 1 : 0, nullptr ) );
+   }
    template < typename V >
    void smooth_gs( const P1Function< V >& dst, const P1Function< V >& rhs, int level, DoFType flag ) const
    {
@@ -320,8 +329,9 @@ enum class CycleType
 };
 
 // V- or W-cycle with SOR smoothing (SORSmoother, relax; HYB_SMOOTHER_SYMMETRIC_SOR for
-// SymmetricSORSmoother, HYB_SMOOTHER_JACOBI for WeightedJacobiSmoother) and an FP64 CG
-// coarse solve.
+// SymmetricSORSmoother, HYB_SMOOTHER_JACOBI for WeightedJacobiSmoother;
+// HYB_SMOOTHER_SOR_REFERENCE_ORDER and HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER for the two
+// SOR smoothers in the reference's sweep order) and an FP64 CG coarse solve.
 template < typename OperatorType >
 class GeometricMultigridSolver
 {
