@@ -296,6 +296,30 @@ def ours(args, rank, world, local_rank):
     if (L, nc) != (7, 2):
         sweep64_traffic = sweep32_traffic = apply_traffic = None
 
+    # The reference's own SOR order on the GPU (hyb_operator_smooth_sor_reference_order): the
+    # same FP64 algorithm, with the same iterates up to rounding, as the reference arm times
+    # on the host; one solve from zero to 1e-8 and one level-7 sweep.
+    ref_order = None
+    if not args.no_reference_order:
+        g_ref = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, smoother=H.SMOOTHER_SOR_REFERENCE_ORDER,
+                                           coarse_tol=1e-12)
+
+        def solve_ref():
+            u.interpolate(0.0, L, flag=H.ALL, stream=sh)
+            return g_ref.solve_to_tolerance(u, b, L, TOL, max_cycles=60, precision=64, stream=sh)
+
+        solve_ref()
+        t_ref, h_ref = timed(solve_ref, 1)
+        cyc_ref = len(h_ref[0]) - 1
+        t_sweep_ref = kernel_time(lambda: A.smooth_sor_reference_order(u, b, 1.0, L, H.INNER | H.NEUMANN, stream=sh),
+                                  reps=5)
+        ref_order = {"smoother": "SOR in the reference's staged lexicographic order (V, E, F, C), FP64",
+                     "time_to_tol_ms": t_ref, "cycles": cyc_ref, "final_rel_residual": float(h_ref[0][-1]),
+                     "dof_updates_per_s": world * n_unknowns * cyc_ref / (t_ref / 1e3),
+                     "sweep_ms": t_sweep_ref * 1e3, "sweep_level": L,
+                     "multicolour_sweep_ms": t_sor * 1e3}
+        del g_ref
+
     varcoef = None
     if not args.no_varcoef:
         del y, u32, b32
@@ -347,6 +371,7 @@ def ours(args, rank, world, local_rank):
                                    kernel="k_apply (FP64 stencil apply, level 7)", ms=t_apply * 1e3),
             "roofline_sor_fp32": dict(roof(sor32_gbs, sweep32_traffic, "ncu (warm caches), profiles/" + sweep_prof),
                                       kernel="k_sor_iface + k_sor_interior (FP32 sweep, level 7)", ms=t_sor32 * 1e3),
+            "reference_order_fp64": ref_order,
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "variable_coefficient": varcoef, "spherical_shell": shell, "blended_shell": blend, "serving": serve,
         }
@@ -818,6 +843,8 @@ def main():
     ap.add_argument("--no-varcoef", action="store_true", help="skip the variable-coefficient leg")
     ap.add_argument("--no-shell", action="store_true", help="skip the spherical-shell leg")
     ap.add_argument("--no-blend", action="store_true", help="skip the curved-shell (blending operator) leg")
+    ap.add_argument("--no-reference-order", action="store_true",
+                    help="skip the FP64 solve with SOR in the reference's own order")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving-stream leg")
     ap.add_argument("--rate", type=float, default=200.0, help="serving arrival rate, requests/s")
     ap.add_argument("--serve-requests", type=int, default=100)

@@ -1331,7 +1331,8 @@ __global__ void __launch_bounds__( 128 ) k_sorref_vertices( TopoDev tp, LevelDev
 }
 
 // edge stage: warp w of the grid takes edge w and walks its points i = 1 .. N-1 (backwards:
-// N-1 .. 1); lane l takes the edge's embeddings l, l + 32, ...
+// N-1 .. 1); lane l takes the edge's embeddings l, l + 32, ...; lane 0 (embedding 0) reads
+// the point's value and right-hand side alongside its neighbours
 template < typename T, int VAR >
 __global__ void __launch_bounds__( 128 ) k_sorref_edges( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                          const T* __restrict__ snap, const T* __restrict__ rhs, T relax,
@@ -1341,17 +1342,19 @@ __global__ void __launch_bounds__( 128 ) k_sorref_edges( TopoDev tp, LevelDev lv
    const int lane = int( threadIdx.x & 31 );
    if ( e >= tp.nE || lv.N < 2 || !( primBc( tp, 1, e ) & flag ) )
       return;
-   const int ne = numEmb( tp, 1, e );
+   const int     ne      = numEmb( tp, 1, e );
+   const int32_t packed0 = lane < ne ? embAt( tp, 1, e, lane ) : 0;
    for ( int s = 0; s < lv.N - 1; ++s )
    {
       const int i    = backwards ? lv.N - 1 - s : s + 1;
-      T         diag = 0, off = 0;
+      T         diag = 0, off = 0, own = 0, bb = 0;
+      size_t    rep = 0;
       for ( int k = lane; k < ne; k += 32 )
       {
-         const int32_t packed = embAt( tp, 1, e, k );
+         const int32_t packed = k == lane ? packed0 : embAt( tp, 1, e, k );
          const int     k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3;
          // the edge's closure in this cell: barycentric coordinates zero off k0 and k1
-         auto own = [&]( int b0, int b1, int b2, int b3 ) {
+         auto own_ = [&]( int b0, int b1, int b2, int b3 ) {
             const int b[4] = { b0, b1, b2, b3 };
             for ( int m = 0; m < 4; ++m )
                if ( m != k0 && m != k1 && b[m] != 0 )
@@ -1360,23 +1363,32 @@ __global__ void __launch_bounds__( 128 ) k_sorref_edges( TopoDev tp, LevelDev lv
          };
          int c, x, y, z;
          embeddingCoords( packed, 1, lv.N, i, 0, c, x, y, z );
-         partialRowSel< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z, own,
+         const size_t r = size_t( c ) * lv.stride + sidx( lv.W, x, y, z );
+         if ( k == lane )
+            rep = r;
+         if ( k == 0 )
+         {
+            own = u[r];
+            bb  = rhs[r];
+         }
+         partialRowSel< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z, own_,
                                   diag, off );
       }
-      diag            = groupSum( diag, 32 );
-      off             = groupSum( off, 32 );
-      const BdryPoint p{ 1, e, i, 0 };
-      const size_t    r0 = bdryReplica< T >( tp, lv, p, 0 );
-      const T         v  = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
-      __syncwarp();
-      for ( int k = lane; k < ne; k += 32 )
-         u[bdryReplica< T >( tp, lv, p, k )] = v;
+      diag = groupSum( diag, 32 );
+      off  = groupSum( off, 32 );
+      T v  = lane == 0 ? ( T( 1 ) - relax ) * own + relax * ( bb - off ) / diag : T( 0 );
+      v    = __shfl_sync( 0xffffffffu, v, 0 );
+      if ( lane < ne )
+         u[rep] = v;
+      for ( int k = lane + 32; k < ne; k += 32 )
+         u[bdryReplica< T >( tp, lv, BdryPoint{ 1, e, i, 0 }, k )] = v;
       __syncwarp(); // the next point reads this one's replicas
    }
 }
 
 // face stage: block f takes face f and walks its hyperplanes t = i + 2j (backwards: the
-// reverse); two lanes per point, one per adjacent cell
+// reverse); two lanes per point, one per adjacent cell; the first reads the point's value
+// and right-hand side alongside its neighbours
 template < typename T, int VAR >
 __global__ void __launch_bounds__( 256 ) k_sorref_faces( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                          const T* __restrict__ snap, const T* __restrict__ rhs, T relax,
@@ -1390,7 +1402,7 @@ __global__ void __launch_bounds__( 256 ) k_sorref_faces( TopoDev tp, LevelDev lv
    const int32_t packed = sub < ne ? embAt( tp, 2, f, sub ) : 0;
    const int     k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3, k2 = ( packed >> 28 ) & 3;
    const int     o  = 6 - k0 - k1 - k2; // the cell-local vertex opposite the face
-   auto          own = [&]( int b0, int b1, int b2, int b3 ) {
+   auto          own_ = [&]( int b0, int b1, int b2, int b3 ) {
       const int b[4] = { b0, b1, b2, b3 };
       return b[o] == 0;
    };
@@ -1405,7 +1417,7 @@ __global__ void __launch_bounds__( 256 ) k_sorref_faces( TopoDev tp, LevelDev lv
       {
          const int  k     = p0 + r * pairs + int( threadIdx.x >> 1 );
          const bool valid = k < p1;
-         T          diag = 0, off = 0;
+         T          diag = 0, off = 0, own = 0, bb = 0;
          size_t     rep = 0;
          if ( valid && sub < ne )
          {
@@ -1413,16 +1425,18 @@ __global__ void __launch_bounds__( 256 ) k_sorref_faces( TopoDev tp, LevelDev lv
             int           c, x, y, z;
             embeddingCoords( packed, 2, lv.N, ij & 0xffff, ij >> 16, c, x, y, z );
             rep = size_t( c ) * lv.stride + sidx( lv.W, x, y, z );
+            if ( sub == 0 )
+            {
+               own = u[rep];
+               bb  = rhs[rep];
+            }
             partialRowSel< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z,
-                                     own, diag, off );
+                                     own_, diag, off );
          }
-         diag             = groupSum( diag, 2 );
-         off              = groupSum( off, 2 );
-         const size_t r0  = __shfl_sync( 0xffffffffu, rep, int( threadIdx.x & 30 ) );
-         T            v   = 0;
-         if ( valid )
-            v = ( T( 1 ) - relax ) * u[r0] + relax * ( rhs[r0] - off ) / diag;
-         __syncwarp();
+         diag = groupSum( diag, 2 );
+         off  = groupSum( off, 2 );
+         T v  = valid && sub == 0 ? ( T( 1 ) - relax ) * own + relax * ( bb - off ) / diag : T( 0 );
+         v    = __shfl_sync( 0xffffffffu, v, int( threadIdx.x & 30 ) );
          if ( valid && sub < ne )
             u[rep] = v;
       }
@@ -1432,9 +1446,12 @@ __global__ void __launch_bounds__( 256 ) k_sorref_faces( TopoDev tp, LevelDev lv
 
 // cell stage: block c takes cell c's interior and walks its hyperplanes t = x + 2y + 3z
 // (backwards: the reverse), reading its closure current; interior points are Inner
+// (1024 threads for the stencil operator, whose rows fit 64 registers; 512 for the others)
+__host__ __device__ constexpr int sorRefCellThreads( int var ) { return var == 0 ? 1024 : 512; }
 template < typename T, int VAR >
-__global__ void __launch_bounds__( 256 ) k_sorref_cells( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                         const T* __restrict__ rhs, T relax, int backwards )
+__global__ void __launch_bounds__( sorRefCellThreads( VAR ) ) k_sorref_cells( TopoDev tp, LevelDev lv, OpDev< T > op,
+                                                                        T* __restrict__ u, const T* __restrict__ rhs,
+                                                                        T relax, int backwards )
 {
    const int c  = int( blockIdx.x );
    T*        uc = u + size_t( c ) * lv.stride;
@@ -1447,10 +1464,11 @@ __global__ void __launch_bounds__( 256 ) k_sorref_cells( TopoDev tp, LevelDev lv
       {
          const int32_t xyz = lv.lexCell[k];
          const int     x = xyz & 1023, y = ( xyz >> 10 ) & 1023, z = xyz >> 20;
+         const int     i   = sidx( lv.W, x, y, z );
+         const T       own = uc[i], bb = bc[i];
          T             diag = 0, off = 0;
          partialRow< T, VAR >( op, uc, c, lv.W, x, y, z, diag, off );
-         const int i = sidx( lv.W, x, y, z );
-         uc[i]       = ( T( 1 ) - relax ) * uc[i] + relax * ( bc[i] - off ) / diag;
+         uc[i] = ( T( 1 ) - relax ) * own + relax * ( bb - off ) / diag;
       }
       __syncthreads();
    }

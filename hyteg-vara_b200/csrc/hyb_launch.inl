@@ -424,7 +424,7 @@ void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax,
       if ( !( flag & HYB_INNER ) || L.dev.nPts == 0 )
          return;
       withVar( op, [&]( auto V ) {
-         k_sorref_cells< T, decltype( V )::value ><<< s.td.nC, 256, 0, stream >>>( s.td, L.dev, od, u, rhs, relax, bw );
+         k_sorref_cells< T, decltype( V )::value ><<< s.td.nC, sorRefCellThreads( decltype( V )::value ), 0, stream >>>( s.td, L.dev, od, u, rhs, relax, bw );
       } );
       HYB_CHECK_LAUNCH();
    };
