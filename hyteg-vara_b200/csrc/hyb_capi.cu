@@ -672,10 +672,14 @@ int hyb_operator_smooth_sor_reference_order( hyb_operator* oh, hyb_function* dh,
    require( u->dtype == b->dtype, "dtypes differ" );
    if ( u->dtype == HYB_F64 )
       launchSorReference< double >( *op, level, u->ptr< double >( level ), b->ptr< double >( level ), relax, flag,
-                                    op->st->snapScratch< double >( level ), S( stream ), backwards != 0 );
+                                    op->st->snapScratch< double >( level ),
+                                    op->st->sorCoefScratch< double >( sorRefCoefElems( *op->st, level ) ), S( stream ),
+                                    backwards != 0 );
    else
       launchSorReference< float >( *op, level, u->ptr< float >( level ), b->ptr< float >( level ), float( relax ), flag,
-                                   op->st->snapScratch< float >( level ), S( stream ), backwards != 0 );
+                                   op->st->snapScratch< float >( level ),
+                                   op->st->sorCoefScratch< float >( sorRefCoefElems( *op->st, level ) ), S( stream ),
+                                   backwards != 0 );
    HYB_API_END
 }
 

@@ -88,10 +88,18 @@ struct LevelDev
    // y, then z; in a face i, then j), so updating the hyperplanes in increasing t equals the
    // lexicographic sweep, and the points of one hyperplane are independent.
    int            nLexCellT, nLexFaceT;
+   int            nLexCell, lexCellMax; // interior points; most points on one hyperplane
    const int32_t* lexCell;
    const int32_t* lexCellOff;
    const int32_t* lexFace;
    const int32_t* lexFaceOff;
+   // for the point at lexCell[k]: the positions, within their own hyperplanes, of the
+   // interior neighbours updated before it (16 int16 = two int4 per point: [0..6] forward,
+   // [8..14] backwards; -1 where the
+   // neighbour lies on the closure; offsets sorRefEarlier(0, m) forwards and
+   // sorRefEarlier(1, m) backwards); only where the ring of the cell wavefront fits
+   const int4*    lexCellNbr;
+   const int32_t* lexOfPts; // hyperplane-list position of each point of `pts`
 };
 
 // 15 stencil offsets, order shared with the oracle and the C ABI
@@ -106,6 +114,16 @@ __host__ __device__ constexpr int offY( int q )
 __host__ __device__ constexpr int offZ( int q )
 {
    return q == 5 ? 1 : q == 6 ? -1 : q == 9 ? 1 : q == 10 ? -1 : q == 11 ? 1 : q == 12 ? -1 : q == 13 ? -1 : q == 14 ? 1 : 0;
+}
+
+// hyperplane step t(q) = offX + 2 offY + 3 offZ of each offset (never 0, |t| <= 3), and the
+// seven offsets of each sweep direction whose neighbours a lexicographic sweep updates
+// before the point: t(q) < 0 forwards, t(q) > 0 backwards
+__host__ __device__ constexpr int offT( int q ) { return offX( q ) + 2 * offY( q ) + 3 * offZ( q ); }
+__host__ __device__ constexpr int sorRefEarlier( int backwards, int m )
+{
+   return backwards ? ( m == 0 ? 1 : m == 1 ? 3 : m == 2 ? 5 : m == 3 ? 7 : m == 4 ? 9 : m == 5 ? 11 : 14 )
+                    : ( m == 0 ? 2 : m == 1 ? 4 : m == 2 ? 6 : m == 3 ? 8 : m == 4 ? 10 : m == 5 ? 12 : 13 );
 }
 
 // valid offsets (bit q) of a point of class mask (offset stays inside the closure)

@@ -154,6 +154,7 @@ struct Gmg
    std::vector< double >       cheb;          // Chebyshev smoother: omega_0 .. omega_{order-1}
    std::unique_ptr< Function > inv64, inv32;  // Chebyshev smoother: diag(A)^-1 per level
    std::unique_ptr< Function > ch64, ch32;    // Chebyshev smoother: second temporary
+   DevBuf< char >              sorCoef;       // reference-order SOR: face couplings
    CgScratch                   cg;
    // reduction scratch of this solver, so that solvers sharing a storage can run on
    // different streams at the same time: scalars[0] = ||r||^2, scalars[1] = ||b||^2
@@ -236,9 +237,10 @@ void smooth( Gmg& g, int l, T* x, const T* b, T* scratch, cudaStream_t stream )
    {
       // the reference's own sweep order; scratch (the solver's residual vector) holds the
       // start-of-sweep snapshot
-      launchSorReference< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, scratch, stream, false );
+      T* coef = reinterpret_cast< T* >( g.sorCoef.p );
+      launchSorReference< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, scratch, coef, stream, false );
       if ( g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER )
-         launchSorReference< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, scratch, stream, true );
+         launchSorReference< T >( *g.op, l, x, b, T( g.relax ), kGmgFlag, scratch, coef, stream, true );
    }
    else if ( g.smoother == HYB_SMOOTHER_CHEBYSHEV )
    {
@@ -709,6 +711,20 @@ void ensureChebyshev( Gmg& g )
 void prepare( Gmg& g )
 {
    ensureChebyshev( g );
+   if ( g.smoother == HYB_SMOOTHER_SOR_REFERENCE_ORDER || g.smoother == HYB_SMOOTHER_SYMMETRIC_SOR_REFERENCE_ORDER )
+   {
+      // tables, kernel attributes and this solver's own face-coupling scratch (FP64 sizes
+      // cover FP32), all before any graph is captured
+      size_t n = 0;
+      for ( int l = g.minL; l <= g.maxL; ++l )
+      {
+         sorRefPrepare< double >( *g.st, l );
+         sorRefPrepare< float >( *g.st, l );
+         n = std::max( n, sorRefCoefElems( *g.st, l ) );
+      }
+      if ( g.sorCoef.n < std::max< size_t >( n, 1 ) * sizeof( double ) )
+         g.sorCoef.alloc( std::max< size_t >( n, 1 ) * sizeof( double ) );
+   }
    for ( int l = g.minL; l <= g.maxL; ++l )
       ensureRows( *g.st, l );
    if ( !g.cg.r )

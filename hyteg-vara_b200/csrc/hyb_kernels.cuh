@@ -1475,6 +1475,433 @@ __global__ void __launch_bounds__( sorRefCellThreads( VAR ) ) k_sorref_cells( To
 }
 
 // ---------------------------------------------------------------------------
+// Reference-order SOR as an affine precompute and a short recurrence. Inside one stage a
+// point's new value is x_p = c0_p + sum_{q in E(p)} a_pq x_q, where E(p) holds the points of
+// the same primitive that the lexicographic walk updates before p and that p couples to
+// (one on an edge, three in a face, seven in a cell), and c0_p collects everything else:
+// its old value, its right-hand side and the neighbours read as they were when the stage
+// began. c0 and a need no order, so every point computes them at once; the walk then runs
+// over on-chip memory only: the edge's points in shared memory, the face's interior in
+// shared memory, and for a cell a ring of the last four hyperplanes (every coupling offset
+// moves t by 1 to 3). The products are those of the plain walk in another summation order.
+// ---------------------------------------------------------------------------
+constexpr int kFromSnap = -1, kFromU = -2; // partialRowSplit neighbour classes (else slot 0..2)
+
+// partialRow of (x, y, z) in `cell` split by cls(b0, b1, b2, b3) of each neighbour's
+// barycentric micro-coordinates: kFromSnap and kFromU add weight * value (from snap, from u)
+// to pre, a slot s in 0..2 adds the weight to a[s]
+template < typename T, int VAR, typename Cls >
+__device__ __forceinline__ void partialRowSplit( const OpDev< T >& op, const T* u, const T* snap, int cell, int W, int x,
+                                                 int y, int z, Cls&& cls, T& diag, T& pre, T ( &a )[3] )
+{
+   const int         N     = W - 1;
+   const int         mask  = classMask( N, x, y, z );
+   const uint32_t    valid = kValidOffsets[mask];
+   const StencilRows R     = stencilRows( W, y, z );
+   int               pos[15];
+   int               cl[15];
+#pragma unroll
+   for ( int q = 0; q < 15; ++q )
+   {
+      const int  xq = x + offX( q ), yq = y + offY( q ), zq = z + offZ( q ), k = offRow( q );
+      const bool v  = ( valid & ( 1u << q ) ) != 0;
+      pos[q]        = v ? R.start[k] + resOff( xq & 3, R.len[k] ) + ( xq >> 2 ) : 0;
+      cl[q]         = v ? cls( N - xq - yq - zq, xq, yq, zq ) : kFromSnap;
+   }
+   auto acc = [&]( int q, T w ) {
+      const int c = cl[q];
+      if ( c == 0 )
+         a[0] += w;
+      else if ( c == 1 )
+         a[1] += w;
+      else if ( c == 2 )
+         a[2] += w;
+      else
+         pre += w * ( c == kFromU ? u[pos[q]] : snap[pos[q]] );
+   };
+   if constexpr ( !VAR )
+   {
+      const T* st = op.st + ( size_t( cell ) * 16 + mask ) * 15;
+      diag += st[0];
+#pragma unroll
+      for ( int q = 1; q < 15; ++q )
+         if ( valid & ( 1u << q ) )
+            acc( q, st[q] );
+   }
+   else
+   {
+      const T*       kv     = op.kap + size_t( cell ) * op.stride;
+      const T*       K      = op.K + size_t( cell ) * 96;
+      const uint32_t validT = kValidTets[mask];
+#pragma unroll
+      for ( int i = 0; i < 24; ++i )
+      {
+         const IncidentTet it = incidentTet( i );
+         if ( !( validT & ( 1u << i ) ) )
+            continue;
+         T ks;
+         if constexpr ( VAR == 2 )
+            ks = op.kq[( size_t( cell ) * 6 + it.t ) * op.stride + pos[it.q[0]]];
+         else
+            ks = kv[pos[it.q[0]]] + kv[pos[it.q[1]]] + kv[pos[it.q[2]]] + kv[pos[it.q[3]]];
+         const T* Kr = K + it.t * 16 + it.k * 4;
+#pragma unroll
+         for ( int j = 0; j < 4; ++j )
+         {
+            if ( j == it.k )
+               diag += ks * Kr[j];
+            else
+               acc( it.q[j], ks * Kr[j] );
+         }
+      }
+   }
+}
+
+// canonical index of face-interior point (i, j): rows j = 1 .. N-2 of N-1-j points
+__device__ __forceinline__ int faceInteriorIdx( int N, int i, int j )
+{
+   return ( j - 1 ) * ( N - 1 ) - ( ( j - 1 ) * j ) / 2 + ( i - 1 );
+}
+__device__ __forceinline__ bool faceInterior( int N, int i, int j ) { return i >= 1 && j >= 1 && i + j <= N - 1; }
+
+// edge stage: warp w of the block takes edge blockIdx.x * warps + w; shared memory holds
+// c0 and a of the edge's N - 1 points per warp; lane 0 runs the recurrence
+template < typename T, int VAR >
+__global__ void __launch_bounds__( 128 ) k_sorref_edges_fast( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                              const T* __restrict__ snap, const T* __restrict__ rhs,
+                                                              T relax, int flag, int backwards )
+{
+   extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
+   const int warp = int( threadIdx.x >> 5 ), lane = int( threadIdx.x & 31 );
+   const int e    = int( blockIdx.x ) * int( blockDim.x >> 5 ) + warp;
+   const int n    = lv.N - 1;
+   T*        c0   = reinterpret_cast< T* >( sorRefSmem ) + size_t( warp ) * 2 * n;
+   T*        aa   = c0 + n;
+   if ( e >= tp.nE || n < 1 || !( primBc( tp, 1, e ) & flag ) )
+      return;
+   const int ne = numEmb( tp, 1, e );
+   for ( int i = 1 + lane; i <= n; i += 32 )
+   {
+      const int ie   = backwards ? i + 1 : i - 1; // the point the walk updates just before i
+      T         diag = 0, pre = 0, a[3] = { 0, 0, 0 }, own = 0, bb = 0;
+      for ( int k = 0; k < ne; ++k )
+      {
+         const int32_t packed = embAt( tp, 1, e, k );
+         const int     k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3;
+         auto          cls = [&]( int b0, int b1, int b2, int b3 ) {
+            const int b[4] = { b0, b1, b2, b3 };
+            for ( int m = 0; m < 4; ++m )
+               if ( m != k0 && m != k1 && b[m] != 0 )
+                  return kFromSnap; // off the edge's closure
+            return ( b[k1] == ie && ie >= 1 && ie <= n ) ? 0 : kFromU;
+         };
+         int c, x, y, z;
+         embeddingCoords( packed, 1, lv.N, i, 0, c, x, y, z );
+         if ( k == 0 )
+         {
+            const size_t r = size_t( c ) * lv.stride + sidx( lv.W, x, y, z );
+            own            = u[r];
+            bb             = rhs[r];
+         }
+         partialRowSplit< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z,
+                                    cls, diag, pre, a );
+      }
+      c0[i - 1] = ( T( 1 ) - relax ) * own + relax * ( bb - pre ) / diag;
+      aa[i - 1] = -relax * a[0] / diag;
+   }
+   __syncwarp();
+   if ( lane == 0 )
+   {
+      T prev = 0; // a is 0 at the first point: the point before it is a vertex
+      for ( int s = 0; s < n; ++s )
+      {
+         const int i = backwards ? n - s : s + 1;
+         prev        = c0[i - 1] + aa[i - 1] * prev;
+         c0[i - 1]   = prev;
+      }
+   }
+   __syncwarp();
+   for ( int i = 1 + lane; i <= n; i += 32 )
+   {
+      const T v = c0[i - 1];
+      for ( int k = 0; k < ne; ++k )
+         u[bdryReplica< T >( tp, lv, BdryPoint{ 1, e, i, 0 }, k )] = v;
+   }
+}
+
+// face stage, first kernel: c0 and the three couplings of every face-interior point of
+// every face whose flag matches, two lanes (adjacent cells) per point, grid-wide;
+// coef[(f * nIntFace + idx) * 4 + {0, 1, 2, 3}] = a0, a1, a2, c0 (idx: canonical index)
+template < typename T, int VAR >
+__global__ void __launch_bounds__( 256 ) k_sorref_faces_pre( TopoDev tp, LevelDev lv, OpDev< T > op,
+                                                             const T* __restrict__ u, const T* __restrict__ snap,
+                                                             const T* __restrict__ rhs, T relax, int flag,
+                                                             int backwards, T* __restrict__ coef )
+{
+   const int  N = lv.N, nI = lv.nIntFace;
+   const long total = long( tp.nF ) * nI * 2;
+   const int  sg    = backwards ? 1 : -1;
+   // whole warps run the loop together (the pair sums shuffle over full warps)
+   for ( long g = long( blockIdx.x ) * blockDim.x + threadIdx.x; g - ( threadIdx.x & 31 ) < total;
+         g += long( gridDim.x ) * blockDim.x )
+   {
+      const bool valid = g < total;
+      const long pt    = valid ? g >> 1 : 0;
+      const int  f = int( pt / nI ), k = int( pt - long( f ) * nI ), sub = int( g & 1 );
+      const bool act   = valid && ( primBc( tp, 2, f ) & flag );
+      const int  ne    = numEmb( tp, 2, f );
+      T          diag = 0, pre = 0, a[3] = { 0, 0, 0 }, own = 0, bb = 0;
+      const int32_t ij = lv.lexFace[k];
+      const int     i = ij & 0xffff, j = ij >> 16;
+      if ( act && sub < ne )
+      {
+         const int32_t packed = embAt( tp, 2, f, sub );
+         const int     k0 = ( packed >> 24 ) & 3, k1 = ( packed >> 26 ) & 3, k2 = ( packed >> 28 ) & 3;
+         const int     o  = 6 - k0 - k1 - k2; // the cell-local vertex opposite the face
+         auto          cls = [&]( int b0, int b1, int b2, int b3 ) {
+            const int b[4] = { b0, b1, b2, b3 };
+            if ( b[o] != 0 )
+               return kFromSnap; // off the face's closure
+            const int di = b[k1] - i, dj = b[k2] - j;
+            if ( !faceInterior( N, b[k1], b[k2] ) )
+               return kFromU; // the face's edges and vertices
+            if ( di == sg && dj == 0 )
+               return 0;
+            if ( di == 0 && dj == sg )
+               return 1;
+            if ( di == -sg && dj == sg )
+               return 2;
+            return kFromU; // face points the walk reaches later
+         };
+         int c, x, y, z;
+         embeddingCoords( packed, 2, N, i, j, c, x, y, z );
+         if ( sub == 0 )
+         {
+            const size_t rep = size_t( c ) * lv.stride + sidx( lv.W, x, y, z );
+            own              = u[rep];
+            bb               = rhs[rep];
+         }
+         partialRowSplit< T, VAR >( op, u + size_t( c ) * lv.stride, snap + size_t( c ) * lv.stride, c, lv.W, x, y, z,
+                                    cls, diag, pre, a );
+      }
+      diag = groupSum( diag, 2 );
+      pre  = groupSum( pre, 2 );
+      a[0] = groupSum( a[0], 2 );
+      a[1] = groupSum( a[1], 2 );
+      a[2] = groupSum( a[2], 2 );
+      if ( act && sub == 0 )
+      {
+         T* cf   = coef + ( size_t( f ) * nI + faceInteriorIdx( N, i, j ) ) * 4;
+         const T m = -relax / diag;
+         cf[0]   = m * a[0];
+         cf[1]   = m * a[1];
+         cf[2]   = m * a[2];
+         cf[3]   = ( T( 1 ) - relax ) * own + relax * ( bb - pre ) / diag;
+      }
+   }
+}
+
+// the k-th point of face hyperplane t = i + 2j (j ascending), or false past its end
+__device__ __forceinline__ bool faceHyperplanePoint( int N, int t, int k, int& i, int& j )
+{
+   const int jlo = max( 1, t - N + 1 ), jhi = min( N - 2, ( t - 1 ) / 2 );
+   j             = jlo + k;
+   i             = t - 2 * j;
+   return j <= jhi;
+}
+
+// face stage, second kernel: block f walks face f's hyperplanes over the shared array X of
+// its interior (c0, then the new values), the couplings of the next hyperplane's points
+// loaded while the current one is updated; then it writes every replica
+template < typename T >
+__global__ void __launch_bounds__( 128 ) k_sorref_faces_wave( TopoDev tp, LevelDev lv, T* __restrict__ u,
+                                                              const T* __restrict__ coef, int flag, int backwards )
+{
+   extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
+   T*        X = reinterpret_cast< T* >( sorRefSmem );
+   const int f = int( blockIdx.x );
+   if ( !( primBc( tp, 2, f ) & flag ) )
+      return;
+   const int N = lv.N, nI = lv.nIntFace, bd = int( blockDim.x ), nT = 2 * N + 1;
+   const T*  cf = coef + size_t( f ) * nI * 4;
+   for ( int k = int( threadIdx.x ); k < nI; k += bd )
+      X[k] = cf[4 * k + 3];
+   const int sg = backwards ? 1 : -1;
+   // this thread's first point of the current and of the next hyperplane, with couplings
+   struct Item
+   {
+      int  i, j, idx;
+      T    a0, a1, a2;
+      bool ok;
+   };
+   auto fetch = [&]( int s, int r ) {
+      Item it{ 0, 0, 0, 0, 0, 0, false };
+      if ( s < nT && faceHyperplanePoint( N, backwards ? nT - 1 - s : s, int( threadIdx.x ) + r * bd, it.i, it.j ) )
+      {
+         it.idx = faceInteriorIdx( N, it.i, it.j );
+         it.a0  = cf[4 * it.idx];
+         it.a1  = cf[4 * it.idx + 1];
+         it.a2  = cf[4 * it.idx + 2];
+         it.ok  = true;
+      }
+      return it;
+   };
+   // couplings to (i + sg, j), (i, j + sg), (i - sg, j + sg): the points updated before
+   auto update = [&]( const Item& it ) {
+      T v = X[it.idx];
+      if ( faceInterior( N, it.i + sg, it.j ) )
+         v += it.a0 * X[faceInteriorIdx( N, it.i + sg, it.j )];
+      if ( faceInterior( N, it.i, it.j + sg ) )
+         v += it.a1 * X[faceInteriorIdx( N, it.i, it.j + sg )];
+      if ( faceInterior( N, it.i - sg, it.j + sg ) )
+         v += it.a2 * X[faceInteriorIdx( N, it.i - sg, it.j + sg )];
+      X[it.idx] = v;
+   };
+   __syncthreads();
+   Item nxt = fetch( 0, 0 );
+   for ( int s = 0; s < nT; ++s )
+   {
+      const Item cur = nxt;
+      nxt            = fetch( s + 1, 0 );
+      if ( cur.ok )
+         update( cur );
+      // hyperplanes longer than the block (levels above 8) take further rounds unprefetched
+      for ( int r = 1;; ++r )
+      {
+         const Item more = fetch( s, r );
+         if ( !more.ok )
+            break;
+         update( more );
+      }
+      __syncthreads();
+   }
+   // every replica: two lanes per point, one per adjacent cell
+   const int     sub    = int( threadIdx.x & 1 );
+   const int     ne     = numEmb( tp, 2, f );
+   const int32_t packed = sub < ne ? embAt( tp, 2, f, sub ) : 0;
+   if ( sub < ne )
+      for ( int k = int( threadIdx.x >> 1 ); k < nI; k += bd >> 1 )
+      {
+         const int32_t ij = lv.lexFace[k];
+         const int     i = ij & 0xffff, j = ij >> 16;
+         int           c, x, y, z;
+         embeddingCoords( packed, 2, N, i, j, c, x, y, z );
+         u[size_t( c ) * lv.stride + sidx( lv.W, x, y, z )] = X[faceInteriorIdx( N, i, j )];
+      }
+}
+
+// cell stage, stencil operator: c0 of every interior point of every cell, in storage order
+// (the point tables), into snap at the point's hyperplane-list position within its cell's
+// slab (snap's entries are not read again before the next snapshot)
+template < typename T >
+__global__ void __launch_bounds__( 256 ) k_sorref_cells_pre( TopoDev tp, LevelDev lv, OpDev< T > op,
+                                                             const T* __restrict__ u, T* __restrict__ snap,
+                                                             const T* __restrict__ rhs, T relax, int backwards )
+{
+   const long total = long( tp.nC ) * lv.nPts;
+   const int  N     = lv.N;
+   for ( long gi = long( blockIdx.x ) * blockDim.x + threadIdx.x; gi < total; gi += long( gridDim.x ) * blockDim.x )
+   {
+      const int      c   = int( gi / lv.nPts );
+      const int      k   = int( gi - long( c ) * lv.nPts );
+      const int32_t  e   = lv.pts[k];
+      const int      b   = e >> 8, g = e & 255;
+      const int32_t  p0  = lv.blkXYZ[b];
+      const int      x = ( p0 & 1023 ) + 4 * g, y = ( p0 >> 10 ) & 1023, z = p0 >> 20;
+      const int32_t* nb  = lv.blk + 16 * b;
+      const T*       uc  = u + size_t( c ) * lv.stride;
+      const T*       st  = op.st + size_t( c ) * 16 * 15; // interior points are class 0
+      T              pre = 0;
+#pragma unroll
+      for ( int q = 1; q < 15; ++q )
+      {
+         const int  xq = x + offX( q ), yq = y + offY( q ), zq = z + offZ( q );
+         const bool earlier  = backwards ? offT( q ) > 0 : offT( q ) < 0;
+         const bool interior = xq >= 1 && yq >= 1 && zq >= 1 && xq + yq + zq <= N - 1;
+         if ( !( earlier && interior ) )
+            pre += st[q] * uc[nb[q] + g];
+      }
+      const size_t i = size_t( c ) * lv.stride + size_t( nb[0] + g );
+      snap[size_t( c ) * lv.stride + size_t( lv.lexOfPts[k] )] =
+          ( T( 1 ) - relax ) * u[i] + relax * ( rhs[i] - pre ) / st[0];
+   }
+}
+
+// cell stage, stencil operator: block c walks cell c's hyperplanes; the new values of the
+// last four hyperplanes stay in a shared ring, indexed by position within the hyperplane;
+// each thread loads its next point's c0, neighbour positions and coordinates while it
+// updates the current one
+template < typename T >
+__global__ void __launch_bounds__( 1024 ) k_sorref_cells_wave( LevelDev lv, OpDev< T > op, T* __restrict__ u,
+                                                               const T* __restrict__ snap, T relax, int backwards )
+{
+   extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
+   T*           ring = reinterpret_cast< T* >( sorRefSmem );
+   __shared__ T aq[8];
+   const int    c  = int( blockIdx.x );
+   const T*     st = op.st + size_t( c ) * 16 * 15;
+   if ( threadIdx.x < 7 )
+      aq[threadIdx.x] = -relax * st[sorRefEarlier( backwards, int( threadIdx.x ) )] / st[0];
+   T*        uc = u + size_t( c ) * lv.stride;
+   const T*  sc = snap + size_t( c ) * lv.stride;
+   const int M = lv.lexCellMax, nT = lv.nLexCellT, bd = int( blockDim.x );
+   struct Item
+   {
+      int  k, t, i;
+      int4 nb;
+      T    c0;
+      bool ok;
+   };
+   auto fetch = [&]( int s, int r ) {
+      Item it{};
+      it.ok = false;
+      if ( s >= nT )
+         return it;
+      it.t        = backwards ? nT - 1 - s : s;
+      const int p0 = lv.lexCellOff[it.t], p1 = lv.lexCellOff[it.t + 1];
+      it.k         = p0 + int( threadIdx.x ) + r * bd;
+      if ( it.k < p1 )
+      {
+         const int32_t xyz = lv.lexCell[it.k];
+         it.i              = sidx( lv.W, xyz & 1023, ( xyz >> 10 ) & 1023, xyz >> 20 );
+         it.nb             = lv.lexCellNbr[2 * it.k + backwards];
+         it.c0             = sc[it.k];
+         it.k -= p0;
+         it.ok = true;
+      }
+      return it;
+   };
+   auto update = [&]( const Item& it ) {
+      const int16_t* p = reinterpret_cast< const int16_t* >( &it.nb );
+      T              v = it.c0;
+#pragma unroll
+      for ( int m = 0; m < 7; ++m )
+         if ( p[m] >= 0 )
+            v += aq[m] * ring[( ( it.t + offT( sorRefEarlier( backwards, m ) ) ) & 3 ) * M + p[m]];
+      ring[( it.t & 3 ) * M + it.k] = v;
+      uc[it.i]                      = v;
+   };
+   __syncthreads();
+   Item nxt = fetch( 0, 0 );
+   for ( int s = 0; s < nT; ++s )
+   {
+      const Item cur = nxt;
+      nxt            = fetch( s + 1, 0 );
+      if ( cur.ok )
+         update( cur );
+      // hyperplanes longer than the block take further rounds, unprefetched
+      for ( int r = 1;; ++r )
+      {
+         const Item more = fetch( s, r );
+         if ( !more.ok )
+            break;
+         update( more );
+      }
+      __syncthreads();
+   }
+}
+
+// ---------------------------------------------------------------------------
 // diag(A)^-1 at every closure point (all replicas; the full row's diagonal for macro-
 // primitive DoFs). zeros: a zero vector of the level, read as the operand of the rows
 // whose off-diagonal part is discarded. Cells' interiors on the first nCellBlocks blocks.

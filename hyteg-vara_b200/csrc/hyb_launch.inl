@@ -66,6 +66,113 @@ long rowIfaceMaxPoints()
 // passes keep the lane-group path).
 std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool full, bool relative = false );
 
+// Bytes of shared memory the reference-order SOR's face and cell wavefronts need on level l
+// in T, and the most a block may take; above it the stages run the plain hyperplane kernels.
+constexpr size_t kSorRefMaxSmem = 200 * 1024;
+template < typename T >
+size_t sorRefFaceSmem( const LevelDev& d ) { return size_t( d.nIntFace ) * sizeof( T ); }
+template < typename T >
+size_t sorRefCellSmem( const LevelDev& d ) { return size_t( 4 ) * d.lexCellMax * sizeof( T ); }
+
+// Hyperplane tables of the reference-order SOR (LevelDev::lex*), built on first use: the
+// cell-interior points x | y << 10 | z << 20 grouped by t = x + 2y + 3z, the face-interior
+// points i | j << 16 grouped by t = i + 2j, and, where the cell wavefront's ring fits
+// (FP32 sizes the check, so both precisions can use it where FP64 does), each interior
+// point's earlier neighbours as positions within their hyperplanes.
+void ensureLex( Storage& s, int l )
+{
+   LevelHost& lh = *s.lv.at( size_t( l ) );
+   if ( lh.lexBuilt )
+      return;
+   LevelDev& d = lh.dev;
+   const int N = d.N;
+   require( N <= 1023, "the reference-order SOR's tables take levels up to 9" );
+   for ( int m = 0; m < 7; ++m )
+      require( offT( sorRefEarlier( 0, m ) ) < 0 && offT( sorRefEarlier( 1, m ) ) > 0, "offset order" );
+   std::vector< std::vector< int32_t > > cellT( size_t( 3 * N + 1 ) ), faceT( size_t( 2 * N + 1 ) );
+   for ( int z = 1; z <= N; ++z )
+      for ( int y = 1; y + z <= N - 2; ++y )
+         for ( int x = 1; x + y + z <= N - 1; ++x )
+            cellT[size_t( x + 2 * y + 3 * z )].push_back( x | ( y << 10 ) | ( z << 20 ) );
+   for ( int j = 1; j <= N - 2; ++j )
+      for ( int i = 1; i + j <= N - 1; ++i )
+         faceT[size_t( i + 2 * j )].push_back( i | ( j << 16 ) );
+   auto flatten = [&]( const std::vector< std::vector< int32_t > >& byT, std::vector< int32_t >& p,
+                       std::vector< int32_t >& o ) {
+      o.assign( 1, 0 );
+      for ( const auto& v : byT )
+      {
+         p.insert( p.end(), v.begin(), v.end() );
+         o.push_back( int32_t( p.size() ) );
+      }
+   };
+   std::vector< int32_t > cp, co, fp, fo;
+   flatten( cellT, cp, co );
+   flatten( faceT, fp, fo );
+   int maxPts = 0;
+   for ( const auto& v : cellT )
+      maxPts = std::max( maxPts, int( v.size() ) );
+   lh.lexCell.upload( cp );
+   lh.lexCellOff.upload( co );
+   lh.lexFace.upload( fp );
+   lh.lexFaceOff.upload( fo );
+   d.nLexCellT  = int( cellT.size() );
+   d.nLexFaceT  = int( faceT.size() );
+   d.nLexCell   = int( cp.size() );
+   d.lexCellMax = maxPts;
+   d.lexCell    = lh.lexCell.p;
+   d.lexCellOff = lh.lexCellOff.p;
+   d.lexFace    = lh.lexFace.p;
+   d.lexFaceOff = lh.lexFaceOff.p;
+   d.lexCellNbr = nullptr;
+   d.lexOfPts   = nullptr;
+   if ( !cp.empty() && sorRefCellSmem< float >( d ) <= kSorRefMaxSmem )
+   {
+      // position of every interior point within its hyperplane
+      const size_t W = size_t( N ) + 1;
+      std::vector< int32_t > posIn( W * W * W, -1 );
+      for ( const auto& v : cellT )
+         for ( size_t k = 0; k < v.size(); ++k )
+         {
+            const int32_t q = v[k];
+            posIn[( size_t( q >> 20 ) * W + size_t( ( q >> 10 ) & 1023 ) ) * W + size_t( q & 1023 )] = int32_t( k );
+         }
+      std::vector< int16_t > nb( cp.size() * 16, int16_t( -1 ) );
+      for ( size_t k = 0; k < cp.size(); ++k )
+      {
+         const int x = cp[k] & 1023, y = ( cp[k] >> 10 ) & 1023, z = cp[k] >> 20;
+         for ( int bw = 0; bw < 2; ++bw )
+            for ( int m = 0; m < 7; ++m )
+            {
+               const int q  = sorRefEarlier( bw, m );
+               const int xq = x + offX( q ), yq = y + offY( q ), zq = z + offZ( q );
+               if ( xq >= 1 && yq >= 1 && zq >= 1 && xq + yq + zq <= N - 1 )
+                  nb[k * 16 + size_t( bw * 8 + m )] =
+                      int16_t( posIn[( size_t( zq ) * W + size_t( yq ) ) * W + size_t( xq )] );
+            }
+      }
+      std::vector< int4 > nb4( cp.size() * 2 );
+      std::memcpy( nb4.data(), nb.data(), nb.size() * sizeof( int16_t ) );
+      lh.lexCellNbr.upload( nb4 );
+      d.lexCellNbr = lh.lexCellNbr.p;
+      // hyperplane-list position of each entry of the point table (storage order)
+      require( d.nPts == int( cp.size() ), "point tables disagree" );
+      std::vector< int32_t > pts( size_t( d.nPts ) ), bx( lh.blkXYZ.n );
+      HYB_CUDA( cudaMemcpy( pts.data(), d.pts, pts.size() * sizeof( int32_t ), cudaMemcpyDeviceToHost ) );
+      HYB_CUDA( cudaMemcpy( bx.data(), lh.blkXYZ.p, bx.size() * sizeof( int32_t ), cudaMemcpyDeviceToHost ) );
+      std::vector< int32_t > lop( pts.size() );
+      for ( size_t k = 0; k < pts.size(); ++k )
+      {
+         const int32_t p0 = bx[size_t( pts[k] >> 8 )];
+         const int x = ( p0 & 1023 ) + 4 * ( pts[k] & 255 ), y = ( p0 >> 10 ) & 1023, z = p0 >> 20;
+         lop[k] = co[size_t( x + 2 * y + 3 * z )] + posIn[( size_t( z ) * W + size_t( y ) ) * W + size_t( x )];
+      }
+      lh.lexOfPts.upload( lop );
+      d.lexOfPts = lh.lexOfPts.p;
+   }
+   lh.lexBuilt = true;
+}
+
 const RowTables* ensureRows( Storage& s, int l )
 {
    LevelHost& L = *s.lv[size_t( l )];
@@ -378,20 +485,44 @@ void launchSor( const Operator& op, int l, T* u, const T* rhs, T relax, int flag
    }
 }
 
-// Reference-order SOR (k_sorref_*): the staged lexicographic sweep of the reference's
-// smooth_sor / smooth_sor_backwards (P1Operator.hpp:352-431). snap is a level-sized scratch
-// in T that takes the start-of-sweep copy (and, backwards, the copy before each later
-// stage). Macro-cell interiors are Inner DoFs: they move when flag has HYB_INNER.
+// Elements of the face-coupling scratch the reference-order SOR needs on level l
+inline size_t sorRefCoefElems( const Storage& s, int l ) { return size_t( s.td.nF ) * s.L( l ).dev.nIntFace * 4; }
+
+// Everything the reference-order SOR on level l needs before a launch (and before a graph
+// that holds one is captured): the hyperplane tables and the opt-in to more than 48 KB of
+// dynamic shared memory for the wavefront kernels.
 template < typename T >
-void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, T* snap, cudaStream_t stream,
-                         bool backwards )
+void sorRefPrepare( Storage& s, int l )
+{
+   ensureLex( s, l );
+   static const bool attrs = [] {
+      const int mx = int( kSorRefMaxSmem );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_faces_wave< T >, cudaFuncAttributeMaxDynamicSharedMemorySize, mx ) );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_cells_wave< T >, cudaFuncAttributeMaxDynamicSharedMemorySize, mx ) );
+      return true;
+   }();
+   (void) attrs;
+}
+
+// Reference-order SOR: the staged lexicographic sweep of the reference's smooth_sor /
+// smooth_sor_backwards (P1Operator.hpp:352-431). snap is a level-sized scratch in T that
+// takes the start-of-sweep copy (and, backwards, the copy before each later stage); coef
+// holds sorRefCoefElems(s, l) elements of T for the face couplings. Macro-cell interiors are Inner DoFs: they move when flag has HYB_INNER. Each stage runs
+// as affine precompute + on-chip recurrence (k_sorref_*_fast, k_sorref_cells_pre/_wave)
+// where its shared memory fits, else as the plain hyperplane walk (k_sorref_edges/_faces/
+// _cells; also with HYB_SORREF_SIMPLE=1, and for the cells of coefficient operators).
+template < typename T >
+void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax, int flag, T* snap, T* coef,
+                         cudaStream_t stream, bool backwards )
 {
    require( !op.blend, "the reference-order SOR takes the stencil and coefficient operators" );
-   const Storage&   s     = *op.st;
-   const auto&      L     = s.L( l );
-   const OpDev< T > od    = op.dev< T >( l );
-   const size_t     bytes = size_t( s.td.nC ) * L.dev.stride * sizeof( T );
-   const int        bw    = backwards ? 1 : 0;
+   Storage& s = *op.st;
+   sorRefPrepare< T >( s, l );
+   const auto&      L      = s.L( l );
+   const OpDev< T > od     = op.dev< T >( l );
+   const size_t     bytes  = size_t( s.td.nC ) * L.dev.stride * sizeof( T );
+   const int        bw     = backwards ? 1 : 0;
+   static const bool simple = envLong( "HYB_SORREF_SIMPLE", 0 ) != 0;
    auto snapshot = [&]() { HYB_CUDA( cudaMemcpyAsync( snap, u, bytes, cudaMemcpyDeviceToDevice, stream ) ); };
    auto vertices = [&]() {
       if ( s.td.nV == 0 )
@@ -405,26 +536,65 @@ void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax,
    auto edges = [&]() {
       if ( s.td.nE == 0 || L.dev.N < 2 )
          return;
+      if ( simple )
+      {
+         withVar( op, [&]( auto V ) {
+            k_sorref_edges< T, decltype( V )::value ><<< ( s.td.nE * 32 + 127 ) / 128, 128, 0, stream >>>(
+                s.td, L.dev, od, u, snap, rhs, relax, flag, bw );
+         } );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
+      // four warps (edges) per block while their c0 and a fit 48 KB, else one
+      const size_t perWarp = size_t( 2 ) * ( L.dev.N - 1 ) * sizeof( T );
+      const int    warps   = perWarp * 4 <= 48 * 1024 ? 4 : 1;
       withVar( op, [&]( auto V ) {
-         k_sorref_edges< T, decltype( V )::value ><<< ( s.td.nE * 32 + 127 ) / 128, 128, 0, stream >>>(
-             s.td, L.dev, od, u, snap, rhs, relax, flag, bw );
+         k_sorref_edges_fast< T, decltype( V )::value ><<< ( s.td.nE + warps - 1 ) / warps, 32 * warps,
+                                                           perWarp * warps, stream >>>( s.td, L.dev, od, u, snap, rhs,
+                                                                                        relax, flag, bw );
       } );
       HYB_CHECK_LAUNCH();
    };
    auto faces = [&]() {
       if ( s.td.nF == 0 || L.dev.nIntFace == 0 )
          return;
+      const size_t sm = sorRefFaceSmem< T >( L.dev );
+      if ( simple || sm > kSorRefMaxSmem )
+      {
+         withVar( op, [&]( auto V ) {
+            k_sorref_faces< T, decltype( V )::value ><<< s.td.nF, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs,
+                                                                                      relax, flag, bw );
+         } );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
+      const long lanes = long( s.td.nF ) * L.dev.nIntFace * 2;
+      const int  nb    = int( std::min< long >( ( lanes + 255 ) / 256, long( s.numSMs ) * 8 ) );
       withVar( op, [&]( auto V ) {
-         k_sorref_faces< T, decltype( V )::value ><<< s.td.nF, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax,
-                                                                                   flag, bw );
+         k_sorref_faces_pre< T, decltype( V )::value ><<< nb, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax,
+                                                                                  flag, bw, coef );
       } );
+      HYB_CHECK_LAUNCH();
+      k_sorref_faces_wave< T ><<< s.td.nF, 128, sm, stream >>>( s.td, L.dev, u, coef, flag, bw );
       HYB_CHECK_LAUNCH();
    };
    auto cells = [&]() {
-      if ( !( flag & HYB_INNER ) || L.dev.nPts == 0 )
+      if ( !( flag & HYB_INNER ) || L.dev.nLexCell == 0 )
          return;
+      const size_t sm = sorRefCellSmem< T >( L.dev );
+      if ( !simple && varKind( op ) == 0 && L.dev.lexCellNbr && sm <= kSorRefMaxSmem )
+      {
+         const long total = long( s.td.nC ) * L.dev.nPts;
+         const int  nb    = int( std::min< long >( ( total + 255 ) / 256, long( s.numSMs ) * 8 ) );
+         k_sorref_cells_pre< T ><<< nb, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax, bw );
+         HYB_CHECK_LAUNCH();
+         k_sorref_cells_wave< T ><<< s.td.nC, 1024, sm, stream >>>( L.dev, od, u, snap, relax, bw );
+         HYB_CHECK_LAUNCH();
+         return;
+      }
       withVar( op, [&]( auto V ) {
-         k_sorref_cells< T, decltype( V )::value ><<< s.td.nC, sorRefCellThreads( decltype( V )::value ), 0, stream >>>( s.td, L.dev, od, u, rhs, relax, bw );
+         k_sorref_cells< T, decltype( V )::value >
+             <<< s.td.nC, sorRefCellThreads( decltype( V )::value ), 0, stream >>>( s.td, L.dev, od, u, rhs, relax, bw );
       } );
       HYB_CHECK_LAUNCH();
    };

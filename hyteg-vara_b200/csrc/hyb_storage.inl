@@ -23,7 +23,10 @@ struct LevelHost
    bool                         rowsTried = false;
    std::unique_ptr< RowTables > blendRows; // full rows for blending operators (ensureBlendRows)
    DevBuf< int32_t >  seg, xyz, blk, blkXYZ, pts, ptsC, quads, rowYZ;
-   DevBuf< int32_t >  lexCell, lexCellOff, lexFace, lexFaceOff; // LevelDev::lex*
+   DevBuf< int32_t >  lexCell, lexCellOff, lexFace, lexFaceOff; // LevelDev::lex* (ensureLex)
+   DevBuf< int4 >     lexCellNbr;                                  // LevelDev::lexCellNbr
+   DevBuf< int32_t >  lexOfPts;                                    // LevelDev::lexOfPts
+   bool               lexBuilt = false;
    DevBuf< int4 >     pro; // prolongation table (LevelDev::pro)
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
    std::vector< int > colourOff;         // per colour: offset, #vertex, #edge, #face DoFs
@@ -76,6 +79,19 @@ struct Storage
          sorSnap.alloc( bytes );
       }
       return reinterpret_cast< T* >( sorSnap.p );
+   }
+
+   DevBuf< char > sorCoef; // face couplings of the reference-order SOR's C ABI calls (grow-only)
+   template < typename T >
+   T* sorCoefScratch( size_t n )
+   {
+      const size_t bytes = std::max< size_t >( n, 1 ) * sizeof( T );
+      if ( sorCoef.n < bytes )
+      {
+         HYB_CUDA( cudaDeviceSynchronize() ); // the old buffer may still be in use by queued sweeps
+         sorCoef.alloc( bytes );
+      }
+      return reinterpret_cast< T* >( sorCoef.p );
    }
 
    ~Storage()
@@ -249,36 +265,6 @@ void buildStorage( Storage& s, const std::vector< std::array< double, 3 > >& V, 
       }
       d.ptsOff[kInteriorColours] = int( ptsFlat.size() );
       d.nPts                     = int( pts.size() );
-      {
-         // hyperplanes of the reference-order SOR (LevelDev::lexCell, lexFace)
-         const int N = d.N;
-         std::vector< std::vector< int32_t > > cellT( size_t( 3 * N + 1 ) ), faceT( size_t( 2 * N + 1 ) );
-         for ( int z = 1; z <= N; ++z )
-            for ( int y = 1; y + z <= N - 2; ++y )
-               for ( int x = 1; x + y + z <= N - 1; ++x )
-                  cellT[size_t( x + 2 * y + 3 * z )].push_back( x | ( y << 10 ) | ( z << 20 ) );
-         for ( int j = 1; j <= N - 2; ++j )
-            for ( int i = 1; i + j <= N - 1; ++i )
-               faceT[size_t( i + 2 * j )].push_back( i | ( j << 16 ) );
-         auto flatten = [&]( const std::vector< std::vector< int32_t > >& byT, DevBuf< int32_t >& pts,
-                             DevBuf< int32_t >& off ) {
-            std::vector< int32_t > p, o( 1, 0 );
-            for ( const auto& v : byT )
-            {
-               p.insert( p.end(), v.begin(), v.end() );
-               o.push_back( int32_t( p.size() ) );
-            }
-            pts.upload( p );
-            off.upload( o );
-            return int( byT.size() );
-         };
-         d.nLexCellT  = flatten( cellT, lh->lexCell, lh->lexCellOff );
-         d.nLexFaceT  = flatten( faceT, lh->lexFace, lh->lexFaceOff );
-         d.lexCell    = lh->lexCell.p;
-         d.lexCellOff = lh->lexCellOff.p;
-         d.lexFace    = lh->lexFace.p;
-         d.lexFaceOff = lh->lexFaceOff.p;
-      }
       d.nQuads = int( quads.size() );
       lh->quads.upload( quads );
       lh->rowYZ.upload( rowYZ );

@@ -1,12 +1,20 @@
 """The SOR sweep in the reference's own order (hyb_operator_smooth_sor_reference_order):
 macro-vertices, -edges, -faces, then -cells (backwards: the reverse, with the ghost layers
 refreshed between stages), each primitive lexicographic and reading only its own closure's
-current values (P1Operator.hpp:352-431). On the GPU the edges walk their points in order,
-the faces and cells their hyperplanes i + 2j and x + 2y + 3z. Checked against the oracle's
-reference-order sweep, whose face stage is pinned to the generated macro-face kernels: one
-sweep 1e-11 (the multicolour sweep's tolerance), FP32 1e-5; V(3,3) cycles with the forward
-and the symmetric smoother 1e-10 against the oracle's cycles with smoother 0 and 3."""
+current values (P1Operator.hpp:352-431). On the GPU each stage computes the affine part of
+every point's update at once and then walks the edge's points, the face's hyperplanes
+i + 2j and the cell's hyperplanes x + 2y + 3z over on-chip memory (k_sorref_*_fast,
+k_sorref_cells_pre/_wave); the plain walks (k_sorref_edges/_faces/_cells) run the cells of
+coefficient operators, the stages whose shared memory would not fit, and everything under
+HYB_SORREF_SIMPLE=1 (tested in a subprocess). Checked against the oracle's reference-order
+sweep, whose face stage is pinned to the generated macro-face kernels: one sweep 1e-11 (the
+multicolour sweep's tolerance), also at level 7 on the benchmarked 48-tet mesh; FP32 1e-5;
+V(3,3) cycles with the forward and the symmetric smoother 1e-10 against the oracle's cycles
+with smoother 0 and 3."""
+import json
 import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -132,3 +140,82 @@ def test_vcycles_match_oracle(setups, smoother, oracle_smoother, kind):
                        max_cycles=60, rel_tol=1e-8, op=op)
     assert len(hist) == len(h_ref), (hist, h_ref)
     close(np.asarray(hist), np.asarray(h_ref), 1e-6)
+
+
+def test_level7_cube48_sweeps(setups, oracle_mod):
+    """Forward then backward sweep on the 2x2x2 cuboid at level 7 (16.97 M DoFs; the face
+    wavefront takes 64 KB of shared memory, the cell ring 44 KB)."""
+    H, O, _ = setups
+    c, t = O.mesh_cuboid(2, 2, 2)
+    L = 7
+    st, orc = H.PrimitiveStorage(c, t, L), O.Oracle(c, t, L)
+    A = H.P1ConstantLaplaceOperator(st, L, L)
+    rng = np.random.default_rng(29)
+    x, b = rng.uniform(-1, 1, orc.n(L)), rng.uniform(-1, 1, orc.n(L))
+    fu, fb = H.P1Function("u", st, L, L), H.P1Function("b", st, L, L)
+    fu.set(x, L)
+    fb.set(b, L)
+    for backwards in (False, True):
+        A.smooth_sor_reference_order(fu, fb, 1.0, L, H.INNER | H.NEUMANN, backwards=backwards)
+        orc.sor_ref(x, b, L, backwards=backwards)
+        close(fu.get(L), x, 1e-11)
+
+
+def test_mixed_precision_solve(setups):
+    """The mixed-precision solver with the reference-order smoother (FP32 sweeps) reaches 1e-8
+    and agrees with the oracle's tightly converged FP64 solution to 1e-6."""
+    H, O, S = setups
+    st, orc, L = S["cube211"]
+    A = H.P1ConstantLaplaceOperator(st, 0, L)
+    b = O.uniform_rhs(orc.coords_of(L), 3, 2 << L)
+    fx, fb = H.P1Function("x", st, 0, L), H.P1Function("b", st, 0, L)
+    fb.set(b, L)
+    gmg = H.GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0, smoother=H.SMOOTHER_SOR_REFERENCE_ORDER)
+    hist = gmg.solve_to_tolerance(fx, fb, L, 1e-8, max_cycles=60, precision=32)
+    assert hist[-1] <= 1e-8
+    xr = np.zeros(orc.n(L))
+    orc.gmg(xr, b, 0, L, pre=3, post=3, smoother=0, max_cycles=100, rel_tol=1e-13)
+    close(fx.get(L), xr, 1e-6)
+
+
+def _simple_errors():
+    """The plain hyperplane kernels (HYB_SORREF_SIMPLE=1): sweeps on the 2x1x1 cuboid at
+    levels 3 and 4, Laplacian and nodal coefficient, both directions; prints the errors."""
+    import hyteg_b200 as H
+    import oracle as O
+
+    H.load()
+    L = 4
+    c, t = O.mesh_cuboid(2, 1, 1, hi=(2.0, 1.0, 1.0))
+    st, orc = H.PrimitiveStorage(c, t, L), O.Oracle(c, t, L)
+    errs = {}
+    rng = np.random.default_rng(37)
+    for kind in ("laplace", "nodal"):
+        A, op = operators(H, O, st, orc, L, kind)
+        for level in (3, 4):
+            for backwards in (False, True):
+                x, b = rng.uniform(-1, 1, orc.n(level)), rng.uniform(-1, 1, orc.n(level))
+                fu, fb = H.P1Function("u", st, 0, L), H.P1Function("b", st, 0, L)
+                fu.set(x, level)
+                fb.set(b, level)
+                A.smooth_sor_reference_order(fu, fb, 0.8, level, H.ALL, backwards=backwards)
+                xr = orc.sor_ref(x.copy(), b, level, relax=0.8, flag=H.ALL, op=op, backwards=backwards)
+                errs[f"{kind}_L{level}_bw{int(backwards)}"] = float(np.abs(fu.get(level) - xr).max() /
+                                                                    np.abs(xr).max())
+    print("SIMPLE_ERRORS " + json.dumps(errs))
+
+
+def test_plain_walk_kernels_in_subprocess():
+    env = dict(os.environ, HYB_SORREF_SIMPLE="1")
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--simple-errors"], env=env, cwd=ROOT,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("SIMPLE_ERRORS ")][-1]
+    for k, e in json.loads(line.split(" ", 1)[1]).items():
+        assert e <= 1e-11, f"{k}: {e:.3e}"
+
+
+if __name__ == "__main__" and "--simple-errors" in sys.argv:
+    for sub in ("oracle", os.path.join("hyteg-vara_b200", "python")):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    _simple_errors()
