@@ -93,13 +93,14 @@ struct LevelDev
    const int32_t* lexCellOff;
    const int32_t* lexFace;
    const int32_t* lexFaceOff;
-   // for the point at lexCell[k]: the positions, within their own hyperplanes, of the
-   // interior neighbours updated before it (16 int16 = two int4 per point: [0..6] forward,
-   // [8..14] backwards; -1 where the
-   // neighbour lies on the closure; offsets sorRefEarlier(0, m) forwards and
-   // sorRefEarlier(1, m) backwards); only where the ring of the cell wavefront fits
+   // for the point at lexCell[k]: the positions, within their own hyperplanes, of the seven
+   // interior neighbours a sweep updates before it, as 7 int16 in one int4 (m = 0..6 for
+   // offset sorRefEarlier(bw, m); -1 where the neighbour lies on the closure), forward
+   // entries at [k], backward entries at [nLexCell + k]; only where the ring of the cell
+   // wavefront fits
    const int4*    lexCellNbr;
    const int32_t* lexOfPts; // hyperplane-list position of each point of `pts`
+   const int32_t* lexSidx;  // storage index of the point at lexCell[k]
 };
 
 // 15 stencil offsets, order shared with the oracle and the C ABI

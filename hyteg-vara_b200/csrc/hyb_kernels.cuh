@@ -1564,23 +1564,23 @@ __device__ __forceinline__ int faceInteriorIdx( int N, int i, int j )
 }
 __device__ __forceinline__ bool faceInterior( int N, int i, int j ) { return i >= 1 && j >= 1 && i + j <= N - 1; }
 
-// edge stage: warp w of the block takes edge blockIdx.x * warps + w; shared memory holds
-// c0 and a of the edge's N - 1 points per warp; lane 0 runs the recurrence
-template < typename T, int VAR >
+// edge stage: block e takes edge e; shared memory holds c0 and a of the edge's N - 1
+// points, a thread per point computes them, thread 0 runs the recurrence
+template < typename T, int VAR, int BW >
 __global__ void __launch_bounds__( 128 ) k_sorref_edges_fast( TopoDev tp, LevelDev lv, OpDev< T > op, T* __restrict__ u,
                                                               const T* __restrict__ snap, const T* __restrict__ rhs,
-                                                              T relax, int flag, int backwards )
+                                                              T relax, int flag )
 {
+   constexpr int backwards = BW;
    extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
-   const int warp = int( threadIdx.x >> 5 ), lane = int( threadIdx.x & 31 );
-   const int e    = int( blockIdx.x ) * int( blockDim.x >> 5 ) + warp;
-   const int n    = lv.N - 1;
-   T*        c0   = reinterpret_cast< T* >( sorRefSmem ) + size_t( warp ) * 2 * n;
-   T*        aa   = c0 + n;
-   if ( e >= tp.nE || n < 1 || !( primBc( tp, 1, e ) & flag ) )
+   const int e  = int( blockIdx.x );
+   const int n  = lv.N - 1;
+   T*        c0 = reinterpret_cast< T* >( sorRefSmem );
+   T*        aa = c0 + n;
+   if ( n < 1 || !( primBc( tp, 1, e ) & flag ) )
       return;
    const int ne = numEmb( tp, 1, e );
-   for ( int i = 1 + lane; i <= n; i += 32 )
+   for ( int i = 1 + int( threadIdx.x ); i <= n; i += int( blockDim.x ) )
    {
       const int ie   = backwards ? i + 1 : i - 1; // the point the walk updates just before i
       T         diag = 0, pre = 0, a[3] = { 0, 0, 0 }, own = 0, bb = 0;
@@ -1609,8 +1609,8 @@ __global__ void __launch_bounds__( 128 ) k_sorref_edges_fast( TopoDev tp, LevelD
       c0[i - 1] = ( T( 1 ) - relax ) * own + relax * ( bb - pre ) / diag;
       aa[i - 1] = -relax * a[0] / diag;
    }
-   __syncwarp();
-   if ( lane == 0 )
+   __syncthreads();
+   if ( threadIdx.x == 0 )
    {
       T prev = 0; // a is 0 at the first point: the point before it is a vertex
       for ( int s = 0; s < n; ++s )
@@ -1620,24 +1620,23 @@ __global__ void __launch_bounds__( 128 ) k_sorref_edges_fast( TopoDev tp, LevelD
          c0[i - 1]   = prev;
       }
    }
-   __syncwarp();
-   for ( int i = 1 + lane; i <= n; i += 32 )
+   __syncthreads();
+   for ( int t = int( threadIdx.x ); t < n * ne; t += int( blockDim.x ) )
    {
-      const T v = c0[i - 1];
-      for ( int k = 0; k < ne; ++k )
-         u[bdryReplica< T >( tp, lv, BdryPoint{ 1, e, i, 0 }, k )] = v;
+      const int i = t / ne + 1, k = t - ( i - 1 ) * ne;
+      u[bdryReplica< T >( tp, lv, BdryPoint{ 1, e, i, 0 }, k )] = c0[i - 1];
    }
 }
 
 // face stage, first kernel: c0 and the three couplings of every face-interior point of
 // every face whose flag matches, two lanes (adjacent cells) per point, grid-wide;
 // coef[(f * nIntFace + idx) * 4 + {0, 1, 2, 3}] = a0, a1, a2, c0 (idx: canonical index)
-template < typename T, int VAR >
+template < typename T, int VAR, int BW >
 __global__ void __launch_bounds__( 256 ) k_sorref_faces_pre( TopoDev tp, LevelDev lv, OpDev< T > op,
                                                              const T* __restrict__ u, const T* __restrict__ snap,
-                                                             const T* __restrict__ rhs, T relax, int flag,
-                                                             int backwards, T* __restrict__ coef )
+                                                             const T* __restrict__ rhs, T relax, int flag, T* __restrict__ coef )
 {
+   constexpr int backwards = BW;
    const int  N = lv.N, nI = lv.nIntFace;
    const long total = long( tp.nF ) * nI * 2;
    const int  sg    = backwards ? 1 : -1;
@@ -1710,94 +1709,15 @@ __device__ __forceinline__ bool faceHyperplanePoint( int N, int t, int k, int& i
    return j <= jhi;
 }
 
-// face stage, second kernel: block f walks face f's hyperplanes over the shared array X of
-// its interior (c0, then the new values), the couplings of the next hyperplane's points
-// loaded while the current one is updated; then it writes every replica
-template < typename T >
-__global__ void __launch_bounds__( 128 ) k_sorref_faces_wave( TopoDev tp, LevelDev lv, T* __restrict__ u,
-                                                              const T* __restrict__ coef, int flag, int backwards )
-{
-   extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
-   T*        X = reinterpret_cast< T* >( sorRefSmem );
-   const int f = int( blockIdx.x );
-   if ( !( primBc( tp, 2, f ) & flag ) )
-      return;
-   const int N = lv.N, nI = lv.nIntFace, bd = int( blockDim.x ), nT = 2 * N + 1;
-   const T*  cf = coef + size_t( f ) * nI * 4;
-   for ( int k = int( threadIdx.x ); k < nI; k += bd )
-      X[k] = cf[4 * k + 3];
-   const int sg = backwards ? 1 : -1;
-   // this thread's first point of the current and of the next hyperplane, with couplings
-   struct Item
-   {
-      int  i, j, idx;
-      T    a0, a1, a2;
-      bool ok;
-   };
-   auto fetch = [&]( int s, int r ) {
-      Item it{ 0, 0, 0, 0, 0, 0, false };
-      if ( s < nT && faceHyperplanePoint( N, backwards ? nT - 1 - s : s, int( threadIdx.x ) + r * bd, it.i, it.j ) )
-      {
-         it.idx = faceInteriorIdx( N, it.i, it.j );
-         it.a0  = cf[4 * it.idx];
-         it.a1  = cf[4 * it.idx + 1];
-         it.a2  = cf[4 * it.idx + 2];
-         it.ok  = true;
-      }
-      return it;
-   };
-   // couplings to (i + sg, j), (i, j + sg), (i - sg, j + sg): the points updated before
-   auto update = [&]( const Item& it ) {
-      T v = X[it.idx];
-      if ( faceInterior( N, it.i + sg, it.j ) )
-         v += it.a0 * X[faceInteriorIdx( N, it.i + sg, it.j )];
-      if ( faceInterior( N, it.i, it.j + sg ) )
-         v += it.a1 * X[faceInteriorIdx( N, it.i, it.j + sg )];
-      if ( faceInterior( N, it.i - sg, it.j + sg ) )
-         v += it.a2 * X[faceInteriorIdx( N, it.i - sg, it.j + sg )];
-      X[it.idx] = v;
-   };
-   __syncthreads();
-   Item nxt = fetch( 0, 0 );
-   for ( int s = 0; s < nT; ++s )
-   {
-      const Item cur = nxt;
-      nxt            = fetch( s + 1, 0 );
-      if ( cur.ok )
-         update( cur );
-      // hyperplanes longer than the block (levels above 8) take further rounds unprefetched
-      for ( int r = 1;; ++r )
-      {
-         const Item more = fetch( s, r );
-         if ( !more.ok )
-            break;
-         update( more );
-      }
-      __syncthreads();
-   }
-   // every replica: two lanes per point, one per adjacent cell
-   const int     sub    = int( threadIdx.x & 1 );
-   const int     ne     = numEmb( tp, 2, f );
-   const int32_t packed = sub < ne ? embAt( tp, 2, f, sub ) : 0;
-   if ( sub < ne )
-      for ( int k = int( threadIdx.x >> 1 ); k < nI; k += bd >> 1 )
-      {
-         const int32_t ij = lv.lexFace[k];
-         const int     i = ij & 0xffff, j = ij >> 16;
-         int           c, x, y, z;
-         embeddingCoords( packed, 2, N, i, j, c, x, y, z );
-         u[size_t( c ) * lv.stride + sidx( lv.W, x, y, z )] = X[faceInteriorIdx( N, i, j )];
-      }
-}
-
 // cell stage, stencil operator: c0 of every interior point of every cell, in storage order
 // (the point tables), into snap at the point's hyperplane-list position within its cell's
 // slab (snap's entries are not read again before the next snapshot)
-template < typename T >
+template < typename T, int BW >
 __global__ void __launch_bounds__( 256 ) k_sorref_cells_pre( TopoDev tp, LevelDev lv, OpDev< T > op,
                                                              const T* __restrict__ u, T* __restrict__ snap,
-                                                             const T* __restrict__ rhs, T relax, int backwards )
+                                                             const T* __restrict__ rhs, T relax )
 {
+   constexpr int backwards = BW;
    const long total = long( tp.nC ) * lv.nPts;
    const int  N     = lv.N;
    for ( long gi = long( blockIdx.x ) * blockDim.x + threadIdx.x; gi < total; gi += long( gridDim.x ) * blockDim.x )
@@ -1831,10 +1751,11 @@ __global__ void __launch_bounds__( 256 ) k_sorref_cells_pre( TopoDev tp, LevelDe
 // last four hyperplanes stay in a shared ring, indexed by position within the hyperplane;
 // each thread loads its next point's c0, neighbour positions and coordinates while it
 // updates the current one
-template < typename T >
+template < typename T, int BW >
 __global__ void __launch_bounds__( 1024 ) k_sorref_cells_wave( LevelDev lv, OpDev< T > op, T* __restrict__ u,
-                                                               const T* __restrict__ snap, T relax, int backwards )
+                                                               const T* __restrict__ snap, T relax )
 {
+   constexpr int backwards = BW;
    extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
    T*           ring = reinterpret_cast< T* >( sorRefSmem );
    __shared__ T aq[8];
@@ -1864,7 +1785,7 @@ __global__ void __launch_bounds__( 1024 ) k_sorref_cells_wave( LevelDev lv, OpDe
       {
          const int32_t xyz = lv.lexCell[it.k];
          it.i              = sidx( lv.W, xyz & 1023, ( xyz >> 10 ) & 1023, xyz >> 20 );
-         it.nb             = lv.lexCellNbr[2 * it.k + backwards];
+         it.nb             = lv.lexCellNbr[size_t( backwards ) * lv.nLexCell + it.k];
          it.c0             = sc[it.k];
          it.k -= p0;
          it.ok = true;
@@ -1899,6 +1820,199 @@ __global__ void __launch_bounds__( 1024 ) k_sorref_cells_wave( LevelDev lv, OpDe
       }
       __syncthreads();
    }
+}
+
+// Asynchronous global -> shared copies (cp.async, groups committed and awaited in order)
+template < int B >
+__device__ __forceinline__ void cpAsync( void* dst, const void* src )
+{
+   const unsigned d = unsigned( __cvta_generic_to_shared( dst ) );
+   if constexpr ( B == 16 )
+      asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"( d ), "l"( src ) : "memory" );
+   else
+      asm volatile( "cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"( d ), "l"( src ), "n"( B ) : "memory" );
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile( "cp.async.commit_group;\n" ::: "memory" ); }
+template < int N >
+__device__ __forceinline__ void cpAsyncWait()
+{
+   asm volatile( "cp.async.wait_group %0;\n" ::"n"( N ) : "memory" );
+}
+
+// Stages in flight of the staged wavefronts: the operands of hyperplane s + ahead are copied
+// while hyperplane s is updated, into one of ahead + 1 shared stages (faces: six ahead; cells:
+// two, as a cell hyperplane holds up to ~N^2/8 points, 1985 at level 7)
+constexpr int kSorRefAhead = 6, kSorRefCellAhead = 2;
+
+// shared bytes of k_sorref_cells_stage on a level: ring, stages, hyperplane offsets
+template < typename T >
+__host__ __device__ inline size_t sorRefCellStageSmem( int M, int nT )
+{
+   return size_t( 4 ) * M * sizeof( T ) + size_t( kSorRefCellAhead + 1 ) * M * ( 16 + sizeof( T ) ) +
+          size_t( nT + 1 ) * 4;
+}
+
+// cell stage, stencil operator, staged: as k_sorref_cells_wave, with each hyperplane's c0 and
+// neighbour positions copied to shared memory kSorRefCellAhead hyperplanes ahead. The new
+// values go back over c0 in snap, in hyperplane order (contiguous stores);
+// k_sorref_cells_scatter then moves them to u in storage order.
+template < typename T, int BW >
+__global__ void __launch_bounds__( 1024 ) k_sorref_cells_stage( LevelDev lv, OpDev< T > op, T* __restrict__ snap,
+                                                                T relax )
+{
+   constexpr int backwards = BW;
+   constexpr int A = kSorRefCellAhead, S = A + 1;
+   extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
+   const int     M = lv.lexCellMax, nT = lv.nLexCellT, bd = int( blockDim.x ), tid = int( threadIdx.x );
+   T*            ring = reinterpret_cast< T* >( sorRefSmem );
+   int4*         stNb = reinterpret_cast< int4* >( sorRefSmem + size_t( 4 ) * M * sizeof( T ) );
+   T*            stC0 = reinterpret_cast< T* >( stNb + size_t( S ) * M );
+   int32_t*      offS = reinterpret_cast< int32_t* >( stC0 + size_t( S ) * M );
+   __shared__ T  aq[8];
+   const int     c  = int( blockIdx.x );
+   const T*      st = op.st + size_t( c ) * 16 * 15;
+   if ( tid < 7 )
+      aq[tid] = -relax * st[sorRefEarlier( backwards, tid )] / st[0];
+   for ( int k = tid; k <= nT; k += bd )
+      offS[k] = lv.lexCellOff[k];
+   T*          sc     = snap + size_t( c ) * lv.stride;
+   const int4* nbBase = lv.lexCellNbr + size_t( backwards ) * lv.nLexCell;
+   __syncthreads();
+   auto issue = [&]( int s ) {
+      if ( s < nT )
+      {
+         const int t  = backwards ? nT - 1 - s : s;
+         const int p0 = offS[t], n = offS[t + 1] - p0, sg = ( s % S ) * M;
+         for ( int k = tid; k < n; k += bd )
+         {
+            cpAsync< 16 >( &stNb[sg + k], &nbBase[p0 + k] );
+            cpAsync< int( sizeof( T ) ) >( &stC0[sg + k], &sc[p0 + k] );
+         }
+      }
+      cpAsyncCommit();
+   };
+   for ( int d = 0; d < A; ++d )
+      issue( d );
+   for ( int s = 0; s < nT; ++s )
+   {
+      cpAsyncWait< A - 1 >(); // this thread's copies of hyperplane s have landed
+      __syncthreads();        // everyone's, and hyperplane s - 1's ring entries
+      issue( s + A );         // into the stage hyperplane s - 1 used
+      const int t = backwards ? nT - 1 - s : s;
+      const int p0 = offS[t], n = offS[t + 1] - p0, sg = ( s % S ) * M;
+      for ( int k = tid; k < n; k += bd )
+      {
+         const int4     nb = stNb[sg + k];
+         const int16_t* p  = reinterpret_cast< const int16_t* >( &nb );
+         T              v  = stC0[sg + k];
+#pragma unroll
+         for ( int m = 0; m < 7; ++m )
+            if ( p[m] >= 0 )
+               v += aq[m] * ring[( ( t + offT( sorRefEarlier( backwards, m ) ) ) & 3 ) * M + p[m]];
+         ring[( t & 3 ) * M + k] = v;
+         sc[p0 + k]              = v; // its c0 was copied to the stage before
+      }
+   }
+   cpAsyncWait< 0 >();
+}
+
+// cell stage: the new interior values from snap (hyperplane order) to u (storage order)
+template < typename T >
+__global__ void __launch_bounds__( 256 ) k_sorref_cells_scatter( TopoDev tp, LevelDev lv, T* __restrict__ u,
+                                                                 const T* __restrict__ snap )
+{
+   const long total = long( tp.nC ) * lv.nPts;
+   for ( long gi = long( blockIdx.x ) * blockDim.x + threadIdx.x; gi < total; gi += long( gridDim.x ) * blockDim.x )
+   {
+      const int     c = int( gi / lv.nPts ), k = int( gi - long( c ) * lv.nPts );
+      const int32_t e = lv.pts[k];
+      u[size_t( c ) * lv.stride + size_t( lv.blk[16 * ( e >> 8 )] + ( e & 255 ) )] =
+          snap[size_t( c ) * lv.stride + size_t( lv.lexOfPts[k] )];
+   }
+}
+
+// face stage, second kernel: block f walks face f's hyperplanes t = i + 2j over the shared
+// array X of its interior (c0, then the new values), with the couplings of each
+// hyperplane's points copied to shared memory kSorRefAhead hyperplanes ahead; then it
+// writes every replica
+template < typename T, int BW >
+__global__ void __launch_bounds__( 128 ) k_sorref_faces_stage( TopoDev tp, LevelDev lv, T* __restrict__ u,
+                                                               const T* __restrict__ coef, int flag )
+{
+   constexpr int backwards = BW;
+   constexpr int S = kSorRefAhead + 1;
+   extern __shared__ __align__( 16 ) unsigned char sorRefSmem[];
+   const int     f = int( blockIdx.x );
+   if ( !( primBc( tp, 2, f ) & flag ) )
+      return;
+   const int N = lv.N, nI = lv.nIntFace, bd = int( blockDim.x ), tid = int( threadIdx.x ), nT = 2 * N + 1;
+   const int P = N / 2 + 1; // most points on one hyperplane
+   T*        stA = reinterpret_cast< T* >( sorRefSmem ); // [S][P][4]: a0, a1, a2, c0
+   T*        X   = stA + size_t( S ) * P * 4;
+   const T*  cf  = coef + size_t( f ) * nI * 4;
+   for ( int k = tid; k < nI; k += bd )
+      cpAsync< int( sizeof( T ) ) >( &X[k], &cf[4 * k + 3] );
+   cpAsyncCommit();
+   cpAsyncWait< 0 >();
+   const int sg = backwards ? 1 : -1;
+   auto issue = [&]( int s ) {
+      if ( s < nT )
+      {
+         const int t = backwards ? nT - 1 - s : s;
+         int       i, j;
+         for ( int k = tid; faceHyperplanePoint( N, t, k, i, j ); k += bd )
+         {
+            const T* src = cf + 4 * size_t( faceInteriorIdx( N, i, j ) );
+            T*       dst = stA + ( size_t( s % S ) * P + k ) * 4;
+            if constexpr ( sizeof( T ) == 8 )
+            {
+               cpAsync< 16 >( dst, src );
+               cpAsync< 8 >( dst + 2, src + 2 );
+            }
+            else
+               cpAsync< 16 >( dst, src );
+         }
+      }
+      cpAsyncCommit();
+   };
+   __syncthreads();
+   for ( int d = 0; d < kSorRefAhead; ++d )
+      issue( d );
+   for ( int s = 0; s < nT; ++s )
+   {
+      cpAsyncWait< kSorRefAhead - 1 >();
+      __syncthreads();
+      issue( s + kSorRefAhead );
+      const int t = backwards ? nT - 1 - s : s;
+      int       i, j;
+      for ( int k = tid; faceHyperplanePoint( N, t, k, i, j ); k += bd )
+      {
+         const T*  a   = stA + ( size_t( s % S ) * P + k ) * 4;
+         const int idx = faceInteriorIdx( N, i, j );
+         T         v   = X[idx];
+         if ( faceInterior( N, i + sg, j ) )
+            v += a[0] * X[faceInteriorIdx( N, i + sg, j )];
+         if ( faceInterior( N, i, j + sg ) )
+            v += a[1] * X[faceInteriorIdx( N, i, j + sg )];
+         if ( faceInterior( N, i - sg, j + sg ) )
+            v += a[2] * X[faceInteriorIdx( N, i - sg, j + sg )];
+         X[idx] = v;
+      }
+   }
+   cpAsyncWait< 0 >();
+   __syncthreads();
+   // every replica: two lanes per point, one per adjacent cell, row by row
+   const int     sub    = tid & 1;
+   const int     ne     = numEmb( tp, 2, f );
+   const int32_t packed = sub < ne ? embAt( tp, 2, f, sub ) : 0;
+   if ( sub < ne )
+      for ( int j = 1; j <= N - 2; ++j )
+         for ( int i = 1 + ( tid >> 1 ); i + j <= N - 1; i += bd >> 1 )
+         {
+            int c, x, y, z;
+            embeddingCoords( packed, 2, N, i, j, c, x, y, z );
+            u[size_t( c ) * lv.stride + sidx( lv.W, x, y, z )] = X[faceInteriorIdx( N, i, j )];
+         }
 }
 
 // ---------------------------------------------------------------------------

@@ -68,7 +68,7 @@ std::unique_ptr< RowTables > buildRows( Storage& s, int l, bool full, bool relat
 
 // Bytes of shared memory the reference-order SOR's face and cell wavefronts need on level l
 // in T, and the most a block may take; above it the stages run the plain hyperplane kernels.
-constexpr size_t kSorRefMaxSmem = 200 * 1024;
+constexpr size_t kSorRefMaxSmem = 220 * 1024;
 template < typename T >
 size_t sorRefFaceSmem( const LevelDev& d ) { return size_t( d.nIntFace ) * sizeof( T ); }
 template < typename T >
@@ -113,6 +113,13 @@ void ensureLex( Storage& s, int l )
    for ( const auto& v : cellT )
       maxPts = std::max( maxPts, int( v.size() ) );
    lh.lexCell.upload( cp );
+   {
+      std::vector< int32_t > si( cp.size() );
+      for ( size_t k = 0; k < cp.size(); ++k )
+         si[k] = sidx( N + 1, cp[k] & 1023, ( cp[k] >> 10 ) & 1023, cp[k] >> 20 );
+      lh.lexSidx.upload( si );
+      d.lexSidx = lh.lexSidx.p;
+   }
    lh.lexCellOff.upload( co );
    lh.lexFace.upload( fp );
    lh.lexFaceOff.upload( fo );
@@ -151,8 +158,13 @@ void ensureLex( Storage& s, int l )
                       int16_t( posIn[( size_t( zq ) * W + size_t( yq ) ) * W + size_t( xq )] );
             }
       }
+      // two blocks of int4: all points' forward entries, then all points' backward entries
       std::vector< int4 > nb4( cp.size() * 2 );
-      std::memcpy( nb4.data(), nb.data(), nb.size() * sizeof( int16_t ) );
+      for ( size_t k = 0; k < cp.size(); ++k )
+      {
+         std::memcpy( &nb4[k], &nb[k * 16], sizeof( int4 ) );
+         std::memcpy( &nb4[cp.size() + k], &nb[k * 16 + 8], sizeof( int4 ) );
+      }
       lh.lexCellNbr.upload( nb4 );
       d.lexCellNbr = lh.lexCellNbr.p;
       // hyperplane-list position of each entry of the point table (storage order)
@@ -497,8 +509,13 @@ void sorRefPrepare( Storage& s, int l )
    ensureLex( s, l );
    static const bool attrs = [] {
       const int mx = int( kSorRefMaxSmem );
-      HYB_CUDA( cudaFuncSetAttribute( k_sorref_faces_wave< T >, cudaFuncAttributeMaxDynamicSharedMemorySize, mx ) );
-      HYB_CUDA( cudaFuncSetAttribute( k_sorref_cells_wave< T >, cudaFuncAttributeMaxDynamicSharedMemorySize, mx ) );
+      const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_cells_wave< T, 0 >, a, mx ) );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_cells_wave< T, 1 >, a, mx ) );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_faces_stage< T, 0 >, a, mx ) );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_faces_stage< T, 1 >, a, mx ) );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_cells_stage< T, 0 >, a, mx ) );
+      HYB_CUDA( cudaFuncSetAttribute( k_sorref_cells_stage< T, 1 >, a, mx ) );
       return true;
    }();
    (void) attrs;
@@ -523,6 +540,13 @@ void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax,
    const size_t     bytes  = size_t( s.td.nC ) * L.dev.stride * sizeof( T );
    const int        bw     = backwards ? 1 : 0;
    static const bool simple = envLong( "HYB_SORREF_SIMPLE", 0 ) != 0;
+   // the fast kernels take the direction as a template argument
+   auto withBw = [&]( auto&& f ) {
+      if ( backwards )
+         f( std::integral_constant< int, 1 >() );
+      else
+         f( std::integral_constant< int, 0 >() );
+   };
    auto snapshot = [&]() { HYB_CUDA( cudaMemcpyAsync( snap, u, bytes, cudaMemcpyDeviceToDevice, stream ) ); };
    auto vertices = [&]() {
       if ( s.td.nV == 0 )
@@ -545,20 +569,23 @@ void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax,
          HYB_CHECK_LAUNCH();
          return;
       }
-      // four warps (edges) per block while their c0 and a fit 48 KB, else one
-      const size_t perWarp = size_t( 2 ) * ( L.dev.N - 1 ) * sizeof( T );
-      const int    warps   = perWarp * 4 <= 48 * 1024 ? 4 : 1;
+      // a block per edge; c0 and a of its points: 2 (N - 1) values, 16 KB at level 10 in FP64
+      const size_t sm = size_t( 2 ) * ( L.dev.N - 1 ) * sizeof( T );
       withVar( op, [&]( auto V ) {
-         k_sorref_edges_fast< T, decltype( V )::value ><<< ( s.td.nE + warps - 1 ) / warps, 32 * warps,
-                                                           perWarp * warps, stream >>>( s.td, L.dev, od, u, snap, rhs,
-                                                                                        relax, flag, bw );
+         withBw( [&]( auto B ) {
+            k_sorref_edges_fast< T, decltype( V )::value, decltype( B )::value >
+                <<< s.td.nE, 128, sm, stream >>>( s.td, L.dev, od, u, snap, rhs, relax, flag );
+         } );
       } );
       HYB_CHECK_LAUNCH();
    };
    auto faces = [&]() {
       if ( s.td.nF == 0 || L.dev.nIntFace == 0 )
          return;
-      const size_t sm = sorRefFaceSmem< T >( L.dev );
+      // the face's interior plus the couplings of kSorRefAhead + 1 hyperplanes of at most
+      // N / 2 + 1 points
+      const size_t sm =
+          sorRefFaceSmem< T >( L.dev ) + size_t( kSorRefAhead + 1 ) * ( L.dev.N / 2 + 1 ) * 4 * sizeof( T );
       if ( simple || sm > kSorRefMaxSmem )
       {
          withVar( op, [&]( auto V ) {
@@ -571,11 +598,15 @@ void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax,
       const long lanes = long( s.td.nF ) * L.dev.nIntFace * 2;
       const int  nb    = int( std::min< long >( ( lanes + 255 ) / 256, long( s.numSMs ) * 8 ) );
       withVar( op, [&]( auto V ) {
-         k_sorref_faces_pre< T, decltype( V )::value ><<< nb, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax,
-                                                                                  flag, bw, coef );
+         withBw( [&]( auto B ) {
+            k_sorref_faces_pre< T, decltype( V )::value, decltype( B )::value >
+                <<< nb, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax, flag, coef );
+         } );
       } );
       HYB_CHECK_LAUNCH();
-      k_sorref_faces_wave< T ><<< s.td.nF, 128, sm, stream >>>( s.td, L.dev, u, coef, flag, bw );
+      withBw( [&]( auto B ) {
+         k_sorref_faces_stage< T, decltype( B )::value ><<< s.td.nF, 128, sm, stream >>>( s.td, L.dev, u, coef, flag );
+      } );
       HYB_CHECK_LAUNCH();
    };
    auto cells = [&]() {
@@ -586,9 +617,24 @@ void launchSorReference( const Operator& op, int l, T* u, const T* rhs, T relax,
       {
          const long total = long( s.td.nC ) * L.dev.nPts;
          const int  nb    = int( std::min< long >( ( total + 255 ) / 256, long( s.numSMs ) * 8 ) );
-         k_sorref_cells_pre< T ><<< nb, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs, relax, bw );
+         withBw( [&]( auto B ) {
+            k_sorref_cells_pre< T, decltype( B )::value ><<< nb, 256, 0, stream >>>( s.td, L.dev, od, u, snap, rhs,
+                                                                                    relax );
+         } );
          HYB_CHECK_LAUNCH();
-         k_sorref_cells_wave< T ><<< s.td.nC, 1024, sm, stream >>>( L.dev, od, u, snap, relax, bw );
+         const size_t smStage = sorRefCellStageSmem< T >( L.dev.lexCellMax, L.dev.nLexCellT );
+         withBw( [&]( auto B ) {
+            if ( smStage <= kSorRefMaxSmem )
+            {
+               k_sorref_cells_stage< T, decltype( B )::value ><<< s.td.nC, 1024, smStage, stream >>>( L.dev, od, snap,
+                                                                                                       relax );
+               HYB_CHECK_LAUNCH();
+               k_sorref_cells_scatter< T ><<< nb, 256, 0, stream >>>( s.td, L.dev, u, snap );
+            }
+            else
+               k_sorref_cells_wave< T, decltype( B )::value ><<< s.td.nC, 1024, sm, stream >>>( L.dev, od, u, snap,
+                                                                                                relax );
+         } );
          HYB_CHECK_LAUNCH();
          return;
       }

@@ -25,7 +25,7 @@ struct LevelHost
    DevBuf< int32_t >  seg, xyz, blk, blkXYZ, pts, ptsC, quads, rowYZ;
    DevBuf< int32_t >  lexCell, lexCellOff, lexFace, lexFaceOff; // LevelDev::lex* (ensureLex)
    DevBuf< int4 >     lexCellNbr;                                  // LevelDev::lexCellNbr
-   DevBuf< int32_t >  lexOfPts;                                    // LevelDev::lexOfPts
+   DevBuf< int32_t >  lexOfPts, lexSidx;                           // LevelDev::lexOfPts, lexSidx
    bool               lexBuilt = false;
    DevBuf< int4 >     pro; // prolongation table (LevelDev::pro)
    DevBuf< int32_t >  colourList;        // surface-DoF indices grouped by SOR colour
