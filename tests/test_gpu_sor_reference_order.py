@@ -3,10 +3,11 @@ macro-vertices, -edges, -faces, then -cells (backwards: the reverse, with the gh
 refreshed between stages), each primitive lexicographic and reading only its own closure's
 current values (P1Operator.hpp:352-431). On the GPU each stage computes the affine part of
 every point's update at once and then walks the edge's points, the face's hyperplanes
-i + 2j and the cell's hyperplanes x + 2y + 3z over on-chip memory (k_sorref_*_fast,
-k_sorref_cells_pre/_wave); the plain walks (k_sorref_edges/_faces/_cells) run the cells of
-coefficient operators, the stages whose shared memory would not fit, and everything under
-HYB_SORREF_SIMPLE=1 (tested in a subprocess). Checked against the oracle's reference-order
+i + 2j and the cell's hyperplanes x + 2y + 3z over on-chip memory (k_sorref_edges_fast,
+k_sorref_faces_pre/_stage, k_sorref_cells_pre/_stage/_scatter); the plain walks
+(k_sorref_edges/_faces/_cells) run the cells of coefficient operators, the stages whose
+shared memory would not fit, and everything under HYB_SORREF_SIMPLE=1 (tested in a
+subprocess). Checked against the oracle's reference-order
 sweep, whose face stage is pinned to the generated macro-face kernels: one sweep 1e-11 (the
 multicolour sweep's tolerance), also at level 7 on the benchmarked 48-tet mesh; FP32 1e-5;
 V(3,3) cycles with the forward and the symmetric smoother 1e-10 against the oracle's cycles
