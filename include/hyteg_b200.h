@@ -238,7 +238,9 @@ int hyb_operator_smooth_sor_backwards( hyb_operator* op, hyb_function* dst, hyb_
  * -faces, then -cells (backwards != 0: cells, faces, edges, vertices), each primitive
  * lexicographic (backwards: reversed) and reading its own closure's current values and every
  * other DoF as it was when the sweep (backwards: the stage) began; stencil and coefficient
- * operators (not the blending operator) */
+ * operators (not the blending operator). The call keeps the sweep's start-of-stage copy and
+ * the face couplings in scratch buffers of the storage: calls on one storage must not
+ * overlap in time (a GMG solver with a reference-order smoother has its own) */
 int hyb_operator_smooth_sor_reference_order( hyb_operator* op, hyb_function* dst, hyb_function* rhs, double relax,
                                              int level, int flag, int backwards, void* stream );
 /* dst = src + relax * diag(A)^-1 (rhs - A src) */
