@@ -220,3 +220,27 @@ if __name__ == "__main__" and "--simple-errors" in sys.argv:
     for sub in ("oracle", os.path.join("hyteg-vara_b200", "python")):
         sys.path.insert(0, os.path.join(ROOT, sub))
     _simple_errors()
+
+
+def test_level8_single_tet_fp32_ring_walk(setups, oracle_mod):
+    """FP32 at level 8 on one macro-tet: the face interior and its staged couplings fit shared
+    memory (k_sorref_faces_stage), the cell walk's ring fits but its staging does not, so the
+    cells run the ring walk with register prefetch (k_sorref_cells_wave). Forward then
+    backward against the oracle's FP64 sweeps of the same FP32-rounded inputs (FP32
+    tolerance 2e-5)."""
+    H, O, _ = setups
+    g = np.load(os.path.join(GOLD, "reference_meshes.npz"))
+    c, t = g["tet_1el_coords"], g["tet_1el_tets"]
+    L = 8
+    st, orc = H.PrimitiveStorage(c, t, L), O.Oracle(c, t, L)
+    A = H.P1ConstantLaplaceOperator(st, L, L)
+    rng = np.random.default_rng(43)
+    x = rng.uniform(-1, 1, orc.n(L)).astype(np.float32).astype(np.float64)
+    b = rng.uniform(-1, 1, orc.n(L)).astype(np.float32).astype(np.float64)
+    fu, fb = H.P1Function("u", st, L, L, H.F32), H.P1Function("b", st, L, L, H.F32)
+    fu.set(x.astype(np.float32), L)
+    fb.set(b.astype(np.float32), L)
+    for backwards in (False, True):
+        A.smooth_sor_reference_order(fu, fb, 1.0, L, H.INNER | H.NEUMANN, backwards=backwards)
+        orc.sor_ref(x, b, L, backwards=backwards)
+        close(fu.get(L).astype(np.float64), x, 2e-5)
